@@ -1,0 +1,77 @@
+"""ctypes binding of libappearance_cuda.so (include/appearance_cuda.h).
+
+The library is built in-tree by appearance_b200/build.py.  Loading fails with
+an exception when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libappearance_cuda.so")
+
+AP_OK, AP_E_INVALID, AP_E_OOM, AP_E_CUDA, AP_E_TIMEOUT, AP_E_UNSUPPORTED, AP_E_NO_SCENE = range(7)
+
+EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error", "ap_set_config",
+           "ap_world_action", "ap_scene_upload", "ap_set_camera_matrices", "ap_render_hdr", "ap_render_device",
+           "ap_device_framebuffer", "ap_trace_rays", "ap_read_buffer", "ap_bvh_stats"]
+
+U32, F32, P = ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p
+
+
+class FrameConfig(ctypes.Structure):
+    _fields_ = [("max_bounces", U32), ("sample_count", U32), ("restir_di", U32), ("restir_gi", U32),
+                ("svgf", U32), ("firefly_filter", U32), ("taa", U32), ("di_area_samples", U32),
+                ("di_bsdf_samples", U32), ("di_temporal_m_factor", F32), ("di_spatial_passes", U32),
+                ("di_spatial_samples", U32), ("di_unbiased", U32), ("gi_temporal_m_cap", F32),
+                ("gi_spatial_passes", U32), ("gi_spatial_samples", U32), ("gi_unbiased", U32),
+                ("svgf_max_history", U32), ("svgf_atrous_passes", U32), ("taa_history_influence", F32)]
+
+
+class Mesh(ctypes.Structure):
+    _fields_ = [("first_vertex", U32), ("num_vertices", U32), ("first_index", U32), ("num_indices", U32),
+                ("material_idx", U32), ("emissive", U32)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("positions", P), ("normals", P), ("num_vertices", U32), ("indices", P), ("tri_material", P),
+                ("num_tris", U32), ("meshes", P), ("num_meshes", U32), ("materials", P), ("num_materials", U32),
+                ("env", P), ("env_w", U32), ("env_h", U32), ("sun", F32 * 8)]
+
+
+class FrameStats(ctypes.Structure):
+    _fields_ = [("gpu_ms", ctypes.c_double), ("extension_rays", ctypes.c_uint64), ("width", U32),
+                ("height", U32), ("frame_idx", U32)]
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python appearance_b200/build.py` (nvcc, sm_100a)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.ap_frame_config_default.argtypes = [ctypes.POINTER(FrameConfig)]
+    L.ap_create.restype = P
+    L.ap_create.argtypes = [ctypes.POINTER(FrameConfig), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.ap_destroy.argtypes = [P]
+    L.ap_last_error.restype = ctypes.c_char_p
+    L.ap_last_error.argtypes = [P]
+    L.ap_set_config.argtypes = [P, ctypes.POINTER(FrameConfig)]
+    L.ap_world_action.argtypes = [P, U32, P, ctypes.c_size_t]
+    L.ap_scene_upload.argtypes = [P, ctypes.POINTER(SceneDesc)]
+    L.ap_set_camera_matrices.argtypes = [P, P]
+    L.ap_render_hdr.argtypes = [P, U32, U32, U32, U32, P, ctypes.c_size_t, ctypes.POINTER(FrameStats)]
+    L.ap_render_device.argtypes = [P, U32, U32, ctypes.POINTER(FrameStats)]
+    L.ap_device_framebuffer.restype = P
+    L.ap_device_framebuffer.argtypes = [P]
+    L.ap_trace_rays.argtypes = [P, P, P, U32, ctypes.c_int, P]
+    L.ap_read_buffer.argtypes = [P, U32, P, ctypes.c_size_t]
+    L.ap_bvh_stats.argtypes = [P, P]
+    _lib = L
+    return L

@@ -1,0 +1,585 @@
+// C-ABI implementation (include/appearance_cuda.h): handle, scene upload and
+// BVH build, camera, frame encode and readback.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/appearance_cuda.h"
+#include "bvh_build.h"
+#include "dev_common.cuh"
+#include "frame.cuh"
+#include "traverse.cuh"
+
+namespace {
+
+using namespace ap;
+
+static_assert(sizeof(ap_frame_config) == sizeof(FrameConfig), "config layout");
+static_assert(sizeof(ap_material) == sizeof(MaterialDev), "material layout");
+
+struct DeviceScene {
+  void* nodes = nullptr;
+  void* tris = nullptr;
+  void* positions = nullptr;
+  void* normals = nullptr;
+  void* indices = nullptr;
+  void* tri_material = nullptr;
+  void* tri_instance = nullptr;
+  void* instances = nullptr;
+  void* materials = nullptr;
+  void* emissive_instances = nullptr;
+  void* emissive_cdf = nullptr;
+  void* env = nullptr;
+  DevScene view{};
+  BvhStats stats{};
+  bool valid = false;
+  void release() {
+    void** all[] = {&nodes, &tris, &positions, &normals, &indices, &tri_material, &tri_instance,
+                    &instances, &materials, &emissive_instances, &emissive_cdf, &env};
+    for (void** p : all) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+    valid = false;
+  }
+};
+
+struct Handle {
+  FrameConfig cfg{};
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  DeviceScene scene;
+  void* frame_mem = nullptr;
+  size_t frame_bytes = 0;
+  uint32_t W = 0, H = 0;
+  FrameBuffers fb{};
+  uint32_t frame_idx = 0;
+  // camera
+  bool explicit_mats = false;
+  Mats mats{};
+  double cam_transform[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  float fov = 60.0f, znear = 0.1f, zfar = 300.0f;  // Camera::default (appearance-camera/src/lib.rs)
+  bool have_prev = false;
+  double prev_vp[16] = {0};
+  // scratch for ap_trace_rays
+  void* trace_mem = nullptr;
+  size_t trace_bytes = 0;
+  uint64_t ext_rays = 0;
+};
+
+int fail(Handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int check_cuda(Handle* h, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return AP_OK;
+  if (e == cudaErrorMemoryAllocation) return fail(h, AP_E_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+  return fail(h, AP_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+int upload(Handle* h, void** dst, const T* src, size_t count) {
+  size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+  int rc = check_cuda(h, cudaMalloc(dst, bytes), "cudaMalloc");
+  if (rc) return rc;
+  if (count) rc = check_cuda(h, cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice), "upload");
+  return rc;
+}
+
+__global__ void k_pack_normals(const float* n, uint32_t count, uint32_t* out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) out[i] = pack_oct30(f3(n[3 * i], n[3 * i + 1], n[3 * i + 2]));
+}
+
+// ---- camera: glam perspective_rh / look_to_rh in double, rounded once ----
+void mat_mul(const double* a, const double* b, double* out) {  // column-major
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) {
+      double s = 0.0;
+      for (int k = 0; k < 4; ++k) s += a[k * 4 + r] * b[c * 4 + k];
+      out[c * 4 + r] = s;
+    }
+}
+bool mat_inv(const double* m, double* out) {  // Gauss-Jordan, column-major in/out
+  double a[4][8];
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      a[r][c] = m[c * 4 + r];
+      a[r][c + 4] = r == c ? 1.0 : 0.0;
+    }
+  for (int c = 0; c < 4; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 4; ++r)
+      if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+    if (std::fabs(a[piv][c]) < 1e-300) return false;
+    for (int k = 0; k < 8; ++k) std::swap(a[c][k], a[piv][k]);
+    double inv = 1.0 / a[c][c];
+    for (int k = 0; k < 8; ++k) a[c][k] *= inv;
+    for (int r = 0; r < 4; ++r)
+      if (r != c) {
+        double f = a[r][c];
+        for (int k = 0; k < 8; ++k) a[r][k] -= f * a[c][k];
+      }
+  }
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) out[c * 4 + r] = a[r][c + 4];
+  return true;
+}
+
+void camera_from_transform(Handle* hd, uint32_t w, uint32_t h, double* view, double* proj) {
+  // CameraUpdate (lib.rs:285-294): rotation + translation of the transform;
+  // Transform::get_view_matrix = look_to_rh(t, R*(0,0,-1), R*(0,1,0)).
+  const double* m = hd->cam_transform;
+  double cx[3] = {m[0], m[1], m[2]}, cy[3] = {m[4], m[5], m[6]}, cz[3] = {m[8], m[9], m[10]};
+  auto nrm = [](double* v) {
+    double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (l > 0) { v[0] /= l; v[1] /= l; v[2] /= l; }
+  };
+  nrm(cx); nrm(cy); nrm(cz);
+  double t[3] = {m[12], m[13], m[14]};
+  // view = inverse(rigid(R, t)): rows of R, translation -R^T t
+  double v[16] = {cx[0], cy[0], cz[0], 0, cx[1], cy[1], cz[1], 0, cx[2], cy[2], cz[2], 0,
+                  -(cx[0] * t[0] + cx[1] * t[1] + cx[2] * t[2]),
+                  -(cy[0] * t[0] + cy[1] * t[1] + cy[2] * t[2]),
+                  -(cz[0] * t[0] + cz[1] * t[1] + cz[2] * t[2]), 1};
+  std::memcpy(view, v, sizeof(v));
+  double f = 1.0 / std::tan(0.5 * (double)hd->fov * M_PI / 180.0);
+  double aspect = (double)w / (double)h;
+  double r = (double)hd->zfar / ((double)hd->znear - (double)hd->zfar);
+  double p[16] = {f / aspect, 0, 0, 0, 0, f, 0, 0, 0, 0, r, -1, 0, 0, r * hd->znear, 0};
+  std::memcpy(proj, p, sizeof(p));
+}
+
+void compute_mats(Handle* hd, uint32_t w, uint32_t h) {
+  if (hd->explicit_mats) return;
+  double view[16], proj[16], vp[16], iv[16], ip[16];
+  camera_from_transform(hd, w, h, view, proj);
+  mat_mul(proj, view, vp);
+  mat_inv(view, iv);
+  mat_inv(proj, ip);
+  const double* pvp = hd->have_prev ? hd->prev_vp : vp;
+  for (int i = 0; i < 16; ++i) {
+    hd->mats.inv_view[i] = (float)iv[i];
+    hd->mats.inv_proj[i] = (float)ip[i];
+    hd->mats.view_proj[i] = (float)vp[i];
+    hd->mats.prev_view_proj[i] = (float)pvp[i];
+  }
+  std::memcpy(hd->prev_vp, vp, sizeof(vp));
+  hd->have_prev = true;
+}
+
+int ensure_frame(Handle* h, uint32_t w, uint32_t hgt) {
+  if (h->frame_mem && h->W == w && h->H == hgt) return AP_OK;
+  if (h->frame_mem) cudaFree(h->frame_mem);
+  h->frame_mem = nullptr;
+  size_t bytes = frame_buffer_bytes(w, hgt);
+  int rc = check_cuda(h, cudaMalloc(&h->frame_mem, bytes), "frame buffers");
+  if (rc) return rc;
+  rc = check_cuda(h, cudaMemsetAsync(h->frame_mem, 0, bytes, h->stream), "frame buffers");
+  if (rc) return rc;
+  h->frame_bytes = bytes;
+  frame_buffers_carve(h->frame_mem, w, hgt, &h->fb);
+  h->W = w;
+  h->H = hgt;
+  h->frame_idx = 0;  // SizedResources::new restarts the temporal state
+  return AP_OK;
+}
+
+int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats) {
+  if (w == 0 || hgt == 0 || (uint64_t)w * hgt > (1ull << 28)) return fail(h, AP_E_INVALID, "bad resolution");
+  if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  const FrameConfig& c = h->cfg;
+  if (c.sample_count == 0 || c.max_bounces == 0 || c.max_bounces > 64 || c.di_area_samples > 1024 ||
+      c.di_bsdf_samples > 16 || c.svgf_atrous_passes > 8 || c.di_spatial_samples > 64 || c.gi_spatial_samples > 64 ||
+      c.di_spatial_passes > 16 || c.gi_spatial_passes > 16)
+    return fail(h, AP_E_INVALID, "frame config out of range");
+  int rc = ensure_frame(h, w, hgt);
+  if (rc) return rc;
+  compute_mats(h, w, hgt);
+  cudaEventRecord(h->ev0, h->stream);
+  encode_frame(h->scene.view, h->fb, h->cfg, h->mats, w, hgt, h->frame_idx, h->num_sms, h->stream);
+  cudaEventRecord(h->ev1, h->stream);
+  rc = check_cuda(h, cudaGetLastError(), "frame launch");
+  if (rc) return rc;
+  rc = check_cuda(h, cudaEventSynchronize(h->ev1), "frame");
+  if (rc) return rc;
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  if (stats) {
+    stats->gpu_ms = ms;
+    stats->extension_rays = 0;
+    stats->width = w;
+    stats->height = hgt;
+    stats->frame_idx = h->frame_idx;
+  }
+  h->frame_idx += 1;
+  return AP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ap_frame_config_default(ap_frame_config* c) {
+  if (!c) return;
+  c->max_bounces = 2;
+  c->sample_count = 1;
+  c->restir_di = 1;
+  c->restir_gi = 1;
+  c->svgf = 0;
+  c->firefly_filter = 1;
+  c->taa = 0;
+  c->di_area_samples = 4;
+  c->di_bsdf_samples = 1;
+  c->di_temporal_m_factor = 20.0f;
+  c->di_spatial_passes = 1;
+  c->di_spatial_samples = 3;
+  c->di_unbiased = 1;
+  c->gi_temporal_m_cap = 30.0f;
+  c->gi_spatial_passes = 0;
+  c->gi_spatial_samples = 5;
+  c->gi_unbiased = 1;
+  c->svgf_max_history = 24;
+  c->svgf_atrous_passes = 5;
+  c->taa_history_influence = 0.8f;
+}
+
+void* ap_create(const ap_frame_config* cfg, int device, int* err) {
+  int dummy;
+  if (!err) err = &dummy;
+  *err = AP_OK;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    *err = AP_E_CUDA;
+    return nullptr;
+  }
+  Handle* h = new Handle();
+  h->device = device;
+  if (cfg) std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
+  else ap_frame_config_default(reinterpret_cast<ap_frame_config*>(&h->cfg));
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    *err = AP_E_CUDA;
+    delete h;
+    return nullptr;
+  }
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+  return h;
+}
+
+void ap_destroy(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  h->scene.release();
+  if (h->frame_mem) cudaFree(h->frame_mem);
+  if (h->trace_mem) cudaFree(h->trace_mem);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+const char* ap_last_error(const void* hp) {
+  const Handle* h = static_cast<const Handle*>(hp);
+  return h ? h->err.c_str() : "null handle";
+}
+
+int ap_set_config(void* hp, const ap_frame_config* cfg) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !cfg) return AP_E_INVALID;
+  std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
+  // a new configuration starts a new frame sequence: drop the temporal state
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  if (h->frame_mem) cudaFree(h->frame_mem);
+  h->frame_mem = nullptr;
+  h->W = h->H = 0;
+  h->frame_idx = 0;
+  h->have_prev = false;
+  return AP_OK;
+}
+
+int ap_world_action(void* hp, uint32_t ty, const void* bytes, size_t len) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  switch (ty) {
+    case 0: {  // CameraUpdateData {Mat4, fov, near, far, pad}
+      if (!bytes || len != 80) return fail(h, AP_E_INVALID, "CameraUpdate expects 80 bytes");
+      const float* f = static_cast<const float*>(bytes);
+      for (int i = 0; i < 16; ++i) h->cam_transform[i] = f[i];
+      h->fov = f[16];
+      h->znear = f[17];
+      h->zfar = f[18];
+      h->explicit_mats = false;
+      return AP_OK;
+    }
+    case 4:  // Clear
+      if (!bytes || len != 4) return fail(h, AP_E_INVALID, "Clear expects 4 bytes");
+      cudaSetDevice(h->device);
+      cudaStreamSynchronize(h->stream);
+      h->scene.release();
+      return AP_OK;
+    case 1:
+    case 2:
+    case 3:
+      return fail(h, AP_E_UNSUPPORTED, "SpawnModel/TransformModel/DestroyModel name glTF assets; upload meshes with ap_scene_upload");
+    default:
+      return fail(h, AP_E_INVALID, "unknown world action type");
+  }
+}
+
+int ap_scene_upload(void* hp, const ap_scene_desc* d) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !d) return AP_E_INVALID;
+  if (!d->positions || !d->normals || !d->indices || !d->tri_material || !d->meshes || !d->materials)
+    return fail(h, AP_E_INVALID, "scene: null array");
+  if (d->num_meshes == 0 || d->num_materials == 0) return fail(h, AP_E_INVALID, "scene: no meshes or materials");
+  // validate mesh ranges
+  uint64_t tri_total = 0;
+  for (uint32_t m = 0; m < d->num_meshes; ++m) {
+    const ap_mesh& me = d->meshes[m];
+    if (me.num_indices % 3 != 0 || (uint64_t)me.first_index + me.num_indices > 3ull * d->num_tris ||
+        (uint64_t)me.first_vertex + me.num_vertices > d->num_vertices || me.material_idx >= d->num_materials)
+      return fail(h, AP_E_INVALID, "scene: mesh " + std::to_string(m) + " out of range");
+    if (me.first_index != 3 * tri_total) return fail(h, AP_E_INVALID, "scene: meshes must be contiguous in index order");
+    tri_total += me.num_indices / 3;
+  }
+  if (tri_total != d->num_tris) return fail(h, AP_E_INVALID, "scene: meshes do not cover all triangles");
+  for (uint32_t m = 0; m < d->num_meshes; ++m) {
+    const ap_mesh& me = d->meshes[m];
+    for (uint32_t i = 0; i < me.num_indices; ++i)
+      if (d->indices[me.first_index + i] >= me.num_vertices) return fail(h, AP_E_INVALID, "scene: index out of range");
+    for (uint32_t t = 0; t < me.num_indices / 3; ++t)
+      if (me.material_idx + d->tri_material[me.first_index / 3 + t] >= d->num_materials)
+        return fail(h, AP_E_INVALID, "scene: triangle material out of range");
+  }
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  h->scene.release();
+  // flattened world triangles, instances, emissive list and CDF (vertex_pool.rs:307-348)
+  std::vector<float> tv(9 * (size_t)d->num_tris);
+  std::vector<InstanceDev> inst(d->num_meshes);
+  std::vector<uint32_t> tri_inst(d->num_tris);
+  std::vector<uint32_t> emissive;
+  uint32_t num_emissive_tris = 0;
+  uint32_t g = 0;
+  for (uint32_t m = 0; m < d->num_meshes; ++m) {
+    const ap_mesh& me = d->meshes[m];
+    InstanceDev& in = inst[m];
+    std::memset(&in, 0, sizeof(in));
+    in.first_vertex = me.first_vertex;
+    in.first_index = me.first_index;
+    in.num_indices = me.num_indices;
+    in.material_idx = me.material_idx;
+    in.emissive_idx = 0xFFFFFFFFu;
+    in.first_global_tri = g;
+    if (me.emissive) {
+      in.emissive_idx = (uint32_t)emissive.size();
+      emissive.push_back(m);
+      num_emissive_tris += me.num_indices / 3;
+    }
+    for (uint32_t t = 0; t < me.num_indices / 3; ++t, ++g) {
+      tri_inst[g] = m;
+      for (int k = 0; k < 3; ++k) {
+        const float* p = d->positions + 3 * (size_t)(me.first_vertex + d->indices[me.first_index + 3 * t + k]);
+        tv[9 * (size_t)g + 3 * k + 0] = p[0];
+        tv[9 * (size_t)g + 3 * k + 1] = p[1];
+        tv[9 * (size_t)g + 3 * k + 2] = p[2];
+      }
+    }
+  }
+  std::vector<float> cdf;
+  float acc = 0.0f;
+  for (uint32_t e : emissive) {
+    float pdf = (float)(inst[e].num_indices / 3) / (float)num_emissive_tris;
+    acc = acc + pdf;
+    cdf.push_back(acc);
+  }
+  WideBvh bvh;
+  std::string berr;
+  if (!build_wide_bvh(tv.data(), d->num_tris, (uint32_t)kTraversalStack, &bvh, &berr))
+    return fail(h, AP_E_INVALID, "BVH build: " + berr);
+  std::vector<float4> pos4(d->num_vertices);
+  for (uint32_t i = 0; i < d->num_vertices; ++i)
+    pos4[i] = make_float4(d->positions[3 * i], d->positions[3 * i + 1], d->positions[3 * i + 2], 0.0f);
+  DeviceScene& s = h->scene;
+  int rc = 0;
+  void* nrm_f = nullptr;
+  if ((rc = upload(h, &s.nodes, bvh.nodes.data(), bvh.nodes.size())) ||
+      (rc = upload(h, &s.tris, bvh.tris.data(), bvh.tris.size())) ||
+      (rc = upload(h, &s.positions, pos4.data(), pos4.size())) ||
+      (rc = upload(h, &nrm_f, d->normals, 3 * (size_t)d->num_vertices)) ||
+      (rc = check_cuda(h, cudaMalloc(&s.normals, std::max<size_t>(4 * (size_t)d->num_vertices, 16)), "normals")) ||
+      (rc = upload(h, &s.indices, d->indices, 3 * (size_t)d->num_tris)) ||
+      (rc = upload(h, &s.tri_material, d->tri_material, d->num_tris)) ||
+      (rc = upload(h, &s.tri_instance, tri_inst.data(), tri_inst.size())) ||
+      (rc = upload(h, &s.instances, inst.data(), inst.size())) ||
+      (rc = upload(h, &s.materials, reinterpret_cast<const MaterialDev*>(d->materials), d->num_materials)) ||
+      (rc = upload(h, &s.emissive_instances, emissive.data(), emissive.size())) ||
+      (rc = upload(h, &s.emissive_cdf, cdf.data(), cdf.size()))) {
+    if (nrm_f) cudaFree(nrm_f);
+    s.release();
+    return rc;
+  }
+  if (d->num_vertices)
+    k_pack_normals<<<(d->num_vertices + 255) / 256, 256, 0, h->stream>>>(static_cast<const float*>(nrm_f), d->num_vertices,
+                                                                           static_cast<uint32_t*>(s.normals));
+  rc = check_cuda(h, cudaStreamSynchronize(h->stream), "pack normals");
+  cudaFree(nrm_f);
+  if (rc) {
+    s.release();
+    return rc;
+  }
+  if (d->env && d->env_w && d->env_h) {
+    if ((rc = upload(h, &s.env, d->env, 3 * (size_t)d->env_w * d->env_h))) {
+      s.release();
+      return rc;
+    }
+  }
+  DevScene& v = s.view;
+  v.nodes = static_cast<const uint4*>(s.nodes);
+  v.tris = static_cast<const float4*>(s.tris);
+  v.positions = static_cast<const float4*>(s.positions);
+  v.normals = static_cast<const uint32_t*>(s.normals);
+  v.indices = static_cast<const uint32_t*>(s.indices);
+  v.tri_material = static_cast<const uint32_t*>(s.tri_material);
+  v.tri_instance = static_cast<const uint32_t*>(s.tri_instance);
+  v.instances = static_cast<const InstanceDev*>(s.instances);
+  v.materials = static_cast<const MaterialDev*>(s.materials);
+  v.emissive_instances = static_cast<const uint32_t*>(s.emissive_instances);
+  v.emissive_cdf = static_cast<const float*>(s.emissive_cdf);
+  v.num_emissive_instances = (uint32_t)emissive.size();
+  v.num_emissive_tris = num_emissive_tris;
+  v.env = static_cast<const float*>(s.env);
+  v.env_w = s.env ? d->env_w : 0;
+  v.env_h = s.env ? d->env_h : 0;
+  std::memcpy(&v.sun, d->sun, sizeof(SunDev));
+  v.num_tris = d->num_tris;
+  s.stats = bvh.stats;
+  s.valid = true;
+  return AP_OK;
+}
+
+int ap_set_camera_matrices(void* hp, const float* m) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !m) return AP_E_INVALID;
+  std::memcpy(&h->mats, m, sizeof(Mats));
+  h->explicit_mats = true;
+  return AP_OK;
+}
+
+int ap_render_hdr(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32_t row_end, float* out,
+                  size_t out_bytes, ap_frame_stats* stats) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  if (row_start >= row_end || row_end > hgt) return fail(h, AP_E_INVALID, "bad row range");
+  size_t need = (size_t)(row_end - row_start) * w * 3 * sizeof(float);
+  if (!out || out_bytes < need) return fail(h, AP_E_INVALID, "output buffer too small");
+  cudaSetDevice(h->device);
+  int rc = render_common(h, w, hgt, stats);
+  if (rc) return rc;
+  rc = check_cuda(h, cudaMemcpyAsync(out, h->fb.out_rgb + (size_t)row_start * w * 3, need, cudaMemcpyDeviceToHost, h->stream),
+                  "readback");
+  if (rc) return rc;
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "readback");
+}
+
+int ap_render_device(void* hp, uint32_t w, uint32_t hgt, ap_frame_stats* stats) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  cudaSetDevice(h->device);
+  return render_common(h, w, hgt, stats);
+}
+
+const float* ap_device_framebuffer(const void* hp) {
+  const Handle* h = static_cast<const Handle*>(hp);
+  return h ? h->fb.out_rgb : nullptr;
+}
+
+int ap_trace_rays(void* hp, const float* origins_tmax, const float* dirs, uint32_t n, int any_hit, uint32_t* out4) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  if (!origins_tmax || !dirs || !out4) return fail(h, AP_E_INVALID, "null buffer");
+  if (n == 0) return AP_OK;
+  cudaSetDevice(h->device);
+  size_t need = (size_t)n * 48 + 256;
+  if (h->trace_bytes < need) {
+    if (h->trace_mem) cudaFree(h->trace_mem);
+    h->trace_mem = nullptr;
+    int rc = check_cuda(h, cudaMalloc(&h->trace_mem, need), "trace scratch");
+    if (rc) return rc;
+    h->trace_bytes = need;
+  }
+  char* p = static_cast<char*>(h->trace_mem);
+  float4* o = reinterpret_cast<float4*>(p);
+  float4* dd = reinterpret_cast<float4*>(p + (size_t)n * 16);
+  uint4* out = reinterpret_cast<uint4*>(p + (size_t)n * 32);
+  uint32_t* cursor = reinterpret_cast<uint32_t*>(p + (size_t)n * 48);
+  cudaMemcpyAsync(o, origins_tmax, (size_t)n * 16, cudaMemcpyHostToDevice, h->stream);
+  cudaMemcpyAsync(dd, dirs, (size_t)n * 16, cudaMemcpyHostToDevice, h->stream);
+  launch_trace_batch(h->scene.view, o, dd, n, any_hit, out, cursor, h->num_sms, h->stream);
+  int rc = check_cuda(h, cudaGetLastError(), "trace launch");
+  if (rc) return rc;
+  cudaMemcpyAsync(out4, out, (size_t)n * 16, cudaMemcpyDeviceToHost, h->stream);
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "trace");
+}
+
+int ap_read_buffer(void* hp, uint32_t which, uint32_t* out, size_t out_bytes) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !out) return AP_E_INVALID;
+  if (!h->frame_mem) return fail(h, AP_E_INVALID, "no frame rendered");
+  size_t P = (size_t)h->W * h->H;
+  uint32_t cur = (h->frame_idx + 1) & 1u;  // parity of the last rendered frame
+  cudaSetDevice(h->device);
+  struct Part { const void* ptr; size_t stride; };
+  std::vector<Part> parts;
+  size_t words = 0;
+  switch (which) {
+    case 0: parts = {{h->fb.radiance, 4}}; words = 1; break;
+    case 1: parts = {{h->fb.payload, 16}}; words = 4; break;
+    case 2: parts = {{h->fb.gb_a[cur], 16}, {h->fb.gb_b[cur], 16}}; words = 8; break;
+    case 3: parts = {{h->fb.di_a, 16}, {h->fb.di_b, 16}}; words = 8; break;
+    case 4: parts = {{h->fb.gi_a, 16}, {h->fb.gi_b, 16}}; words = 8; break;
+    case 5: parts = {{h->fb.ctx, 16}}; words = 4; break;
+    case 7: parts = {{h->fb.rays, 16}}; words = 4; break;
+    default: return fail(h, AP_E_INVALID, "unknown buffer");
+  }
+  if (out_bytes < P * words * 4) return fail(h, AP_E_INVALID, "output buffer too small");
+  size_t col = 0;
+  for (const Part& pt : parts) {
+    size_t pw = pt.stride / 4;
+    int rc = check_cuda(h, cudaMemcpy2DAsync(out + col, words * 4, pt.ptr, pt.stride, pt.stride, P,
+                                             cudaMemcpyDeviceToHost, h->stream),
+                        "read buffer");
+    if (rc) return rc;
+    col += pw;
+  }
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "read buffer");
+}
+
+int ap_bvh_stats(void* hp, uint32_t* out8) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !out8) return AP_E_INVALID;
+  if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  const BvhStats& s = h->scene.stats;
+  out8[0] = s.num_nodes;
+  out8[1] = s.num_tris;
+  out8[2] = s.max_depth;
+  out8[3] = s.max_stack;
+  std::memcpy(&out8[4], &s.build_ms, 8);
+  out8[6] = 0;
+  out8[7] = 0;
+  return AP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1253 @@
+// Wavefront path-tracing frame for sm_100a.
+//
+// Pass structure and per-pixel arithmetic follow PathTracerGpu::render
+// (crates/appearance-path-tracer-gpu/src/lib.rs:314-615) and its WGSL passes;
+// the data layout and scheduling are this library's own:
+//   * per-pixel state in 16-byte SoA records (frame.cuh);
+//   * the path-extension ray of every bounce is traced by a persistent kernel
+//     that fetches 32 rays per warp from a compacted queue of live paths;
+//   * live paths are re-queued by warp ballot + popc + one atomic per warp;
+//   * shading, next-event estimation, the GI candidate path and ReSTIR
+//     resampling trace their short rays inline (traverse.cuh);
+//   * the a-trous filter stages each 16x16 tile with its 2*2^i halo through
+//     shared memory.
+#include <algorithm>
+
+#include "dev_shade.cuh"
+#include "frame.cuh"
+#include "traverse.cuh"
+
+namespace ap {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+struct Consts {
+  uint32_t W, H, P;
+  uint32_t bounce, seed, frame_idx, qin, qout;
+  FrameConfig cfg;
+};
+
+APD float3 ray_dir(const float4 r) { return unpack_oct30(__float_as_uint(r.w)); }
+APD float3 ray_org(const float4 r) { return f3(r.x, r.y, r.z); }
+
+// ---- hit attributes (trace.wgsl:101-201) ----
+struct Surface {
+  uint32_t material_idx;
+  float3 hit_point, n;
+  bool back_face;
+  Frame frame;
+};
+APD Surface surface(const DevScene& s, const Hit& h, float3 origin, float3 direction, const MaterialDev** mat) {
+  Surface sf;
+  uint32_t inst_idx = s.tri_instance[h.tri];
+  const InstanceDev in = s.instances[inst_idx];
+  uint32_t prim = h.tri - in.first_global_tri;
+  float bx = 1.0f - h.u - h.v;
+  uint32_t fi = in.first_index + prim * 3;
+  float3 n0 = unpack_oct30(s.normals[in.first_vertex + s.indices[fi + 0]]);
+  float3 n1 = unpack_oct30(s.normals[in.first_vertex + s.indices[fi + 1]]);
+  float3 n2 = unpack_oct30(s.normals[in.first_vertex + s.indices[fi + 2]]);
+  sf.material_idx = in.material_idx + s.tri_material[in.first_index / 3 + prim];
+  *mat = s.materials + sf.material_idx;
+  float3 hit_n = normalize(n0 * bx + n1 * h.u + n2 * h.v);
+  sf.hit_point = origin + direction * h.t;
+  float3 w_out = -direction;
+  sf.back_face = dot(w_out, hit_n) < 0.0f;
+  float3 ff = sf.back_face ? hit_n * -1.0f : hit_n;
+  sf.n = ff;
+  sf.frame.n = ff;
+  sf.frame.t2w = onb(ff);
+  if ((*mat)->clearcoat > 0.0f) {
+    sf.frame.cc_t2w = onb(ff);
+  } else {
+    sf.frame.cc_t2w.c0 = f3s(0.0f);
+    sf.frame.cc_t2w.c1 = f3s(0.0f);
+    sf.frame.cc_t2w.c2 = f3s(0.0f);
+  }
+  return sf;
+}
+
+APD bool shadow_ray(const DevScene& s, float3 origin, float3 dir, float d, float3 n) {
+  return !trace_any(s, origin + n * 1e-4f, dir, d - 1e-4f * 2.0f);
+}
+
+// ---- Nee::sample_ris (helpers/nee.wgsl:122-237) ----
+APD DiRes sample_ris(const DevScene& s, const FrameConfig& cfg, float3 hit, float3 wo, const Frame& fr,
+                     const Bsdf& b, float t, bool back_face, uint32_t& rng) {
+  const uint32_t NA = cfg.di_area_samples, NB = cfg.di_bsdf_samples;
+  DiRes res;
+  res.M = res.W = res.wsum = res.phat = 0.0f;
+  res.s = ls_empty();
+  LightEval sel{f3s(0.0f), f3s(0.0f)};
+  uint32_t n_iter = NA > NB ? NA : NB;
+  for (uint32_t i = 0; i < n_iter; ++i) {
+    float area_pdf = 0.0f, area_phat = 0.0f;
+    LightSample area_s{make_float2(0.0f, 0.0f), 0u, 0u};
+    LightEval area_e{f3s(0.0f), f3s(0.0f)};
+    if (i < NA) {
+      float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng), r3 = rnd(rng), r4 = rnd(rng);
+      area_s = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), &area_pdf);
+      area_e = load_eval(s, area_s, hit);
+      float3 wi = normalize(area_e.point - hit);
+      float wdn = dot(wi, fr.n);
+      if (wdn > 0.0f && area_pdf > 0.0f) {
+        float sp = 0.0f;
+        float3 refl = disney_eval(b, fr, wo, wi, &sp);
+        if (sp > 0.0f) area_phat = luma(refl * wdn * area_e.emission);
+      }
+    }
+    float bsdf_pdf = 0.0f, bsdf_phat = 0.0f;
+    LightSample bsdf_s = ls_empty();
+    LightEval bsdf_e{f3s(0.0f), f3s(0.0f)};
+    if (i < NB) {
+      float3 wi = f3s(0.0f);
+      float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng);
+      float3 refl = disney_sample(b, fr, wo, t, back_face, r0, r1, r2, &wi, &bsdf_pdf);
+      float wdn = dm::fabs_(dot(wi, fr.n));
+      float3 contribution = wdn * refl;
+      if (dot(contribution, contribution) > 0.0f) {
+        Hit h;
+        if (trace_closest(s, hit + fr.n * 1e-4f, wi, 1000.0f, h)) {
+          const InstanceDev in = s.instances[s.tri_instance[h.tri]];
+          if (in.emissive_idx != kU32Max)
+            bsdf_s = LightSample{make_float2(h.u, h.v), in.emissive_idx, h.tri - in.first_global_tri};
+        } else {
+          bsdf_s = LightSample{inverse_direction_to_sun(s.sun, wi), kU32Max - 1, 0u};
+        }
+        if (!ls_is_empty(bsdf_s)) {
+          bsdf_e = load_eval(s, bsdf_s, hit);
+          bsdf_phat = luma(contribution * bsdf_e.emission);
+        }
+      }
+    }
+    if (i < NA) {
+      float aw = 0.0f;
+      if (area_pdf > 0.0f) {
+        float mis = area_pdf / ((float)NA * area_pdf + (float)NB * bsdf_pdf);
+        aw = mis * area_phat * (1.0f / dm::fmax(area_pdf, 1e-8f));
+      }
+      if (di_update(res, aw, rng, area_s, area_phat)) sel = area_e;
+    }
+    if (i < NB) {
+      float bw = 0.0f;
+      if (bsdf_pdf > 0.0f) {
+        float mis = bsdf_pdf / ((float)NB * bsdf_pdf + (float)NA * area_pdf);
+        bw = mis * bsdf_phat * (1.0f / dm::fmax(bsdf_pdf, 1e-8f));
+      }
+      if (di_update(res, bw, rng, bsdf_s, bsdf_phat)) sel = bsdf_e;
+    }
+  }
+  if (res.phat > 1e-6f) {
+    float3 dir = normalize(sel.point - hit);
+    float d = dist(sel.point, hit);
+    if (shadow_ray(s, hit, dir, d, fr.n)) res.W = (1.0f / res.phat) * res.wsum;
+  }
+  return res;
+}
+
+// ---- InlinePathTracer::trace with the approx() config (inline_path_tracer.wgsl:51-256) ----
+APD float3 inline_trace(const DevScene& s, float3 origin, float3 direction, float3 throughput, float3* first_hit,
+                        uint32_t& rng) {
+  float3 acc = f3s(0.0f);
+  Hit h;
+  if (trace_closest(s, origin + direction * 1e-4f, direction, 1000.0f - 1e-4f * 2.0f, h)) {
+    const MaterialDev* m;
+    Surface sf = surface(s, h, origin, direction, &m);
+    Bsdf b = load_bsdf(m);
+    float3 wo = -direction;
+    float pdf = 0.0f;
+    float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng), r3 = rnd(rng), r4 = rnd(rng);
+    LightSample ls = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), &pdf);
+    float W = 1.0f / pdf;
+    if (W > 0.0f) {
+      LightEval ev = load_eval(s, ls, sf.hit_point);
+      float3 sdir = normalize(ev.point - sf.hit_point);
+      float sd = dist(ev.point, sf.hit_point);
+      float ndl = dot(sdir, sf.n);
+      if (ndl > 0.0f && shadow_ray(s, sf.hit_point, sdir, sd, sf.n)) {
+        float sp = 0.0f;
+        float3 refl = disney_eval(b, sf.frame, wo, sdir, &sp);
+        acc = acc + throughput * refl * ev.emission * ndl * W;
+      }
+    }
+    *first_hit = sf.hit_point;
+    return acc;
+  }
+  *first_hit = origin + direction * 1000.0f;
+  return acc + throughput * sky_radiance(s, direction, true);
+}
+
+// ---- InlinePathTracer::sample_ris (inline_path_tracer.wgsl:258-296) ----
+APD GiRes gi_sample_ris(const DevScene& s, float3 hit, float3 wo, const Frame& fr, const Bsdf& b, float3 T,
+                        float t, bool back_face, uint32_t& rng) {
+  GiRes res;
+  res.M = res.W = res.wsum = res.phat = 0.0f;
+  res.point = f3s(0.0f);
+  res.phat_rng = 0u;
+  float3 wi = f3s(0.0f);
+  float pdf = 0.0f;
+  float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng);
+  float3 refl = disney_sample(b, fr, wo, t, back_face, r0, r1, r2, &wi, &pdf);
+  if (pdf > 1e-6f) {
+    float cos_in = dm::fabs_(dot(wi, fr.n));
+    float3 local = cos_in * refl;
+    float3 tr = T * local;
+    uint32_t phat_rng = rng;
+    float3 point = f3s(0.0f);
+    float3 contribution = inline_trace(s, hit, wi, tr, &point, rng);
+    float phat = luma(contribution);
+    gi_update(res, phat / pdf, rng, point, phat, phat_rng);
+  }
+  if (res.phat > 0.0f && res.M * res.wsum > 0.0f) res.W = (1.0f / res.phat) * (1.0f / res.M * res.wsum);
+  return res;
+}
+
+APD Frame ctx_frame(const uint4 c) {
+  Frame fr;
+  fr.n = unpack_oct30(c.z);
+  fr.t2w = onb(fr.n);
+  fr.cc_t2w = onb(unpack_oct30(c.w));
+  return fr;
+}
+
+// GiReservoir::phat (inline_path_tracer.wgsl:299-331)
+APD float gi_phat(const DevScene& s, const GiRes& r, const uint4 c, float3 T, float3 hit, float3 wo) {
+  Bsdf b = load_bsdf(s.materials + c.x);
+  Frame fr = ctx_frame(c);
+  float3 wi = normalize(r.point - hit);
+  float sp = 0.0f;
+  float3 refl = disney_eval(b, fr, wo, wi, &sp);
+  float cos_in = dm::fabs_(dot(wi, fr.n));
+  float3 local = cos_in * refl;
+  float3 gi_origin = hit + wi * 0.0001f;
+  float3 tr = T * local;
+  uint32_t prng = r.phat_rng;
+  float3 pt;
+  return luma(inline_trace(s, gi_origin, wi, tr, &pt, prng));
+}
+
+// LightSample::phat (di_reservoir.wgsl:58-97)
+APD float ls_phat(const DevScene& s, const LightSample& l, const uint4 c, float3 hit, float3 wo, bool vis) {
+  LightEval ev = load_eval(s, l, hit);
+  Bsdf b = load_bsdf(s.materials + c.x);
+  Frame fr = ctx_frame(c);
+  float3 wi = normalize(ev.point - hit);
+  float wdn = dot(wi, fr.n);
+  if (wdn > 0.0f) {
+    bool visible = true;
+    if (vis) visible = shadow_ray(s, hit, wi, dist(ev.point, hit), fr.n);
+    if (visible) {
+      float sp = 0.0f;
+      float3 refl = disney_eval(b, fr, wo, wi, &sp);
+      return luma(refl * wdn * ev.emission);
+    }
+  }
+  return 0.0f;
+}
+
+APD DiRes di_new() {
+  DiRes r;
+  r.M = r.W = r.wsum = r.phat = 0.0f;
+  r.s = ls_empty();
+  return r;
+}
+APD GiRes gi_new() {
+  GiRes r;
+  r.M = r.W = r.wsum = r.phat = 0.0f;
+  r.point = f3s(0.0f);
+  r.phat_rng = 0u;
+  return r;
+}
+
+// ---- kernels ----------------------------------------------------------------
+
+APD void mul4(const float* m, float v0, float v1, float v2, float v3, float out[4]) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r) out[r] = m[r] * v0 + m[4 + r] * v1 + m[8 + r] * v2 + m[12 + r] * v3;
+}
+
+// raygen.wgsl:21-39
+__global__ void k_raygen(FrameBuffers fb, uint32_t W, uint32_t H, Mats mats) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  float ux = (((float)x + 0.5f) / (float)W) * 2.0f - 1.0f;
+  float uy = (((float)y + 0.5f) / (float)H) * 2.0f - 1.0f;
+  uy = -uy;
+  float o[4], t[4], d[4];
+  mul4(mats.inv_view, 0.0f, 0.0f, 0.0f, 1.0f, o);
+  mul4(mats.inv_proj, ux, uy, 1.0f, 1.0f, t);
+  float3 tn = normalize(f3(t[0], t[1], t[2]));
+  mul4(mats.inv_view, tn.x, tn.y, tn.z, 0.0f, d);
+  fb.rays[y * W + x] = make_float4(o[0], o[1], o[2], __uint_as_float(pack_oct30(f3(d[0], d[1], d[2]))));
+}
+
+// Persistent closest-hit kernel for the path-extension rays: each warp takes
+// 32 consecutive queue entries per atomic.  Bounce 0 traces every pixel.
+__global__ void __launch_bounds__(kBlock) k_extend(DevScene s, FrameBuffers fb, Consts c) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
+  const uint32_t* q = fb.queue[c.qin];
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&fb.counters[2], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= count) break;
+    uint32_t i = base + lane;
+    if (i < count) {
+      uint32_t id = c.bounce == 0 ? i : q[i];
+      float4 r = fb.rays[id];
+      float3 o = ray_org(r), d = ray_dir(r);
+      Hit h;
+      trace_closest(s, o + d * 1e-4f, d, 1000.0f, h);
+      fb.hits[id] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.u), __float_as_uint(h.v), h.tri);
+    }
+  }
+}
+
+APD float2 velocity_of(const Mats& m, float3 p) {
+  float cs[4], ps[4];
+  mul4(m.view_proj, p.x, p.y, p.z, 1.0f, cs);
+  mul4(m.prev_view_proj, p.x, p.y, p.z, 1.0f, ps);
+  float px = (ps[0] / ps[3] + 1.0f) / 2.0f, py = 1.0f - (ps[1] / ps[3] + 1.0f) / 2.0f;
+  float cx = (cs[0] / cs[3] + 1.0f) / 2.0f, cy = 1.0f - (cs[1] / cs[3] + 1.0f) / 2.0f;
+  return make_float2(cx - px, cy - py);
+}
+
+// trace.wgsl:62-262 after the closest hit (taken from fb.hits).
+__global__ void __launch_bounds__(kBlock) k_shade(DevScene s, FrameBuffers fb, Consts c, Mats mats) {
+  const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
+  const uint32_t* q = fb.queue[c.qin];
+  const uint32_t cur = c.frame_idx & 1u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t id = c.bounce == 0 ? i : q[i];
+    float4 ray = fb.rays[id];
+    float3 origin = ray_org(ray), direction = ray_dir(ray);
+    uint4 pl = fb.payload[id];
+    if (c.bounce == 0) {
+      pl.x = pack_rgb9e5(f3s(1.0f));
+      pl.y = pcg_hash(id ^ xor_shift(c.seed));
+      pl.z = __float_as_uint(0.0f);
+    }
+    if (__uint_as_float(pl.z) < 0.0f) continue;
+    float3 acc = unpack_rgb9e5(fb.radiance[id]);
+    float3 T = unpack_rgb9e5(pl.x);
+    uint32_t rng = pl.y;
+    float3 g_pos = f3s(0.0f), g_n = f3s(0.0f), g_alb = f3s(0.0f);
+    float g_depth = 0.0f;
+    float2 vel = make_float2(0.0f, 0.0f);
+    uint4 hr = fb.hits[id];
+    Hit h{__uint_as_float(hr.x), __uint_as_float(hr.y), __uint_as_float(hr.z), hr.w};
+    float t_out;
+    if (h.tri != kNoHit) {
+      float depth_ws = 0.0f + h.t;
+      const MaterialDev* m;
+      Surface sf = surface(s, h, origin, direction, &m);
+      float3 emission = ld3(m->emission);
+      if (c.bounce == 0) acc = acc + T * emission;
+      float3 wo = -direction;
+      Bsdf b = load_bsdf(m);
+      if (c.bounce == 0) {
+        g_pos = sf.hit_point;
+        g_depth = depth_ws;
+        g_n = sf.n;
+        g_alb = ld3(m->color) + emission;
+        vel = velocity_of(mats, sf.hit_point);
+      }
+      DiRes dr = sample_ris(s, c.cfg, sf.hit_point, wo, sf.frame, b, h.t, sf.back_face, rng);
+      fb.di_a[id] = di_pack_a(dr);
+      fb.di_b[id] = di_pack_b(dr);
+      fb.ctx[id] = make_uint4(sf.material_idx, pack_rgb9e5(T), pack_oct30(sf.n), pack_oct30(sf.frame.cc_t2w.c2));
+      t_out = depth_ws;
+      if (c.bounce + 1 < c.cfg.max_bounces) {
+        bool killed = false;
+        if (c.bounce > 1) {
+          float rr = dm::fmax(T.x, dm::fmax(T.y, T.z));
+          if (rr < rnd(rng)) {
+            t_out = -1.0f;
+            killed = true;
+          } else {
+            T = T * (1.0f / rr);
+          }
+        }
+        if (!killed) {
+          GiRes gr = gi_sample_ris(s, sf.hit_point, wo, sf.frame, b, T, h.t, sf.back_face, rng);
+          fb.gi_a[id] = gi_pack_a(gr);
+          fb.gi_b[id] = gi_pack_b(gr);
+        }
+      }
+    } else {
+      g_alb = f3s(1.0f);
+      acc = acc + T * sky_radiance(s, direction, true);
+      t_out = -1.0f;
+    }
+    fb.radiance[id] = pack_rgb9e5(acc);
+    fb.payload[id] = make_uint4(pack_rgb9e5(T), rng, __float_as_uint(t_out), 0u);
+    if (c.bounce == 0) {
+      fb.gb_a[cur][id] = make_uint4(__float_as_uint(g_pos.x), __float_as_uint(g_pos.y), __float_as_uint(g_pos.z),
+                                    __float_as_uint(g_depth));
+      fb.gb_b[cur][id] = make_uint4(pack_oct30(g_n), pack_rgb9e5(g_alb), __float_as_uint(vel.x), __float_as_uint(vel.y));
+    }
+  }
+}
+
+// apply_di.wgsl:48-111
+__global__ void __launch_bounds__(kBlock) k_apply_di(DevScene s, FrameBuffers fb, Consts c) {
+  const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
+  const uint32_t* q = fb.queue[c.qin];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t id = c.bounce == 0 ? i : q[i];
+    uint4 pl = fb.payload[id];
+    float pt = __uint_as_float(pl.z);
+    if (pt < 0.0f) continue;
+    DiRes dr = di_unpack(fb.di_a[id], fb.di_b[id]);
+    if (dr.W == 0.0f) continue;
+    float4 ray = fb.rays[id];
+    float3 origin = ray_org(ray), direction = ray_dir(ray);
+    uint4 cx = fb.ctx[id];
+    float3 acc = unpack_rgb9e5(fb.radiance[id]);
+    float3 T = unpack_rgb9e5(cx.y);
+    Bsdf b = load_bsdf(s.materials + cx.x);
+    float3 hit = origin + direction * pt;
+    Frame fr = ctx_frame(cx);
+    LightEval ev = load_eval(s, dr.s, hit);
+    float3 sdir = normalize(ev.point - hit);
+    float sd = dist(ev.point, hit);
+    float ndl = dot(sdir, fr.n);
+    if (ndl > 0.0f && shadow_ray(s, hit, sdir, sd, fr.n)) {
+      float sp = 0.0f;
+      float3 refl = disney_eval(b, fr, -direction, sdir, &sp);
+      acc = acc + T * refl * ev.emission * ndl * dr.W;
+    }
+    fb.radiance[id] = pack_rgb9e5(acc);
+  }
+}
+
+// apply_gi.wgsl:44-99, plus re-queueing of the live paths (warp ballot, one
+// atomic per warp) for the next bounce.
+__global__ void __launch_bounds__(kBlock) k_apply_gi(DevScene s, FrameBuffers fb, Consts c) {
+  const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
+  const uint32_t* q = fb.queue[c.qin];
+  uint32_t* qo = fb.queue[c.qout];
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t start = blockIdx.x * blockDim.x + threadIdx.x;
+  // every lane of a warp runs the same number of iterations (ballot below)
+  uint32_t iters = (count + stride - 1) / stride;
+  for (uint32_t it = 0; it < iters; ++it) {
+    uint32_t i = start + it * stride;
+    bool alive = false;
+    uint32_t id = 0;
+    if (i < count) {
+      id = c.bounce == 0 ? i : q[i];
+      uint4 pl = fb.payload[id];
+      float pt = __uint_as_float(pl.z);
+      if (pt >= 0.0f) {
+        float4 ray = fb.rays[id];
+        float3 origin = ray_org(ray), direction = ray_dir(ray);
+        float3 hit = origin + direction * pt;
+        GiRes gr = gi_unpack(fb.gi_a[id], fb.gi_b[id]);
+        if (gr.W > 0.0f) {
+          uint4 cx = fb.ctx[id];
+          float3 T = unpack_rgb9e5(pl.x);
+          Bsdf b = load_bsdf(s.materials + cx.x);
+          Frame fr = ctx_frame(cx);
+          float3 wi = normalize(gr.point - hit);
+          float sp = 0.0f;
+          float3 refl = disney_eval(b, fr, -direction, wi, &sp);
+          float cos_in = dm::fabs_(dot(fr.n, wi));
+          T = T * (refl * cos_in * gr.W);
+          pl.x = pack_rgb9e5(T);
+          fb.rays[id] = make_float4(hit.x, hit.y, hit.z, __uint_as_float(pack_oct30(wi)));
+          alive = true;
+        } else {
+          pl.z = __float_as_uint(-1.0f);
+        }
+        fb.payload[id] = pl;
+      }
+    }
+    uint32_t ballot = __ballot_sync(0xffffffffu, alive);
+    if (ballot) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&fb.counters[c.qout], (uint32_t)__popc(ballot));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (alive) qo[base + __popc(ballot & ((1u << lane) - 1u))] = id;
+    }
+  }
+}
+
+// ---- ReSTIR ---------------------------------------------------------------
+
+struct GT {
+  float3 pos;
+  float depth;
+  float3 n;
+  float3 albedo;
+};
+APD GT gt_load(const uint4* a, const uint4* b, uint32_t id) {
+  uint4 x = a[id], y = b[id];
+  return GT{f3(__uint_as_float(x.x), __uint_as_float(x.y), __uint_as_float(x.z)), __uint_as_float(x.w),
+            unpack_oct30(y.x), unpack_rgb9e5(y.y)};
+}
+// GBuffer::sample_prev_gbuffer (gbuffer_bindings.wgsl:20-50)
+APD GT sample_prev_gbuffer(const uint4* a, const uint4* b, uint32_t W, uint32_t H, float2 pos) {
+  uint32_t ix = dm::f2u(floorf(pos.x)), iy = dm::f2u(floorf(pos.y));
+  float fx = dm::fract(pos.x), fy = dm::fract(pos.y);
+  uint32_t x1 = min(ix + 1, W - 1), y1 = min(iy + 1, H - 1);
+  GT t00 = gt_load(a, b, iy * W + ix), t10 = gt_load(a, b, iy * W + x1);
+  GT t01 = gt_load(a, b, y1 * W + ix), t11 = gt_load(a, b, y1 * W + x1);
+  GT r;
+  r.pos = mix3(mix3(t00.pos, t10.pos, fx), mix3(t01.pos, t11.pos, fx), fy);
+  r.depth = mixf(mixf(t00.depth, t10.depth, fx), mixf(t01.depth, t11.depth, fx), fy);
+  r.n = normalize(mix3(mix3(t00.n, t10.n, fx), mix3(t01.n, t11.n, fx), fy));
+  r.albedo = mix3(mix3(t00.albedo, t10.albedo, fx), mix3(t01.albedo, t11.albedo, fx), fy);
+  return r;
+}
+APD bool history_valid(const GT& cur, const GT& prev) {
+  bool ds = dm::fabs_(cur.depth - prev.depth) <= 0.1f * prev.depth;
+  bool ns = dot(cur.n, prev.n) > 0.906f;
+  return ds && ns;
+}
+APD bool prev_point(const FrameBuffers& fb, uint32_t cur, uint32_t x, uint32_t y, uint32_t W, uint32_t H, float2* out) {
+  uint4 gb = fb.gb_b[cur][y * W + x];
+  float vx = __uint_as_float(gb.z), vy = __uint_as_float(gb.w);
+  float px = (float)x - ((float)W * vx), py = (float)y - ((float)H * vy);
+  *out = make_float2(px, py);
+  return px >= 0.0f && py >= 0.0f && px <= (float)(W - 1) && py <= (float)(H - 1);
+}
+APD uint32_t stochastic_prev_id(float2 p, float r0, float r1, uint32_t W, uint32_t H) {
+  uint32_t px = dm::f2u(floorf(p.x + r0)), py = dm::f2u(floorf(p.y + r1));
+  unsigned long long id = (unsigned long long)py * W + px;
+  unsigned long long last = (unsigned long long)W * H - 1ull;
+  return (uint32_t)(id < last ? id : last);
+}
+APD DiRes di_combine(const DiRes& r1, const DiRes& r2, uint32_t& rng) {
+  DiRes c = di_new();
+  di_update(c, r1.phat * r1.W * r1.M, rng, r1.s, r1.phat);
+  di_update(c, r2.phat * r2.W * r2.M, rng, r2.s, r2.phat);
+  c.M = r1.M + r2.M;
+  if (c.phat > 1e-6f && c.M * c.wsum > 1e-6f) c.W = (1.0f / c.phat) * (1.0f / c.M * c.wsum);
+  return c;
+}
+APD GiRes gi_combine(const GiRes& r1, const GiRes& r2, uint32_t& rng) {
+  GiRes c = gi_new();
+  gi_update(c, r1.phat * r1.W * r1.M, rng, r1.point, r1.phat, r1.phat_rng);
+  gi_update(c, r2.phat * r2.W * r2.M, rng, r2.point, r2.phat, r2.phat_rng);
+  c.M = r1.M + r2.M;
+  if (c.phat > 0.0f && c.M * c.wsum > 0.0f) c.W = (1.0f / c.phat) * (1.0f / c.M * c.wsum);
+  return c;
+}
+
+// restir_di_temporal.wgsl:68-176 (BILINEAR = false)
+__global__ void k_di_temporal(DevScene s, FrameBuffers fb, Consts c, const uint4* in_a, const uint4* in_b,
+                              uint4* out_a, uint4* out_b, const uint4* prev_a, const uint4* prev_b,
+                              uint4* pout_a, uint4* pout_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  uint32_t id = y * c.W + x;
+  uint4 pl = fb.payload[id];
+  float pt = __uint_as_float(pl.z);
+  if (pt < 0.0f) return;
+  const uint32_t cur = c.frame_idx & 1u;
+  uint32_t rng = pl.y;
+  float4 ray = fb.rays[id];
+  float3 direction = ray_dir(ray);
+  float3 hit = ray_org(ray) + direction * pt;
+  uint4 cx = fb.ctx[id];
+  DiRes r = di_unpack(in_a[id], in_b[id]);
+  float2 pp;
+  if (prev_point(fb, cur, x, y, c.W, c.H, &pp)) {
+    GT g = gt_load(fb.gb_a[cur], fb.gb_b[cur], id);
+    GT pg = sample_prev_gbuffer(fb.gb_a[cur ^ 1u], fb.gb_b[cur ^ 1u], c.W, c.H, pp);
+    if (history_valid(g, pg)) {
+      float r0 = rnd(rng), r1 = rnd(rng);
+      uint32_t pid = stochastic_prev_id(pp, r0, r1, c.W, c.H);
+      DiRes pr = di_unpack(prev_a[pid], prev_b[pid]);
+      pr.M = dm::fmin(pr.M, c.cfg.di_temporal_m_factor * r.M);
+      pr.phat = ls_phat(s, pr.s, cx, hit, -direction, c.cfg.di_unbiased > 0);
+      r = di_combine(r, pr, rng);
+    }
+  }
+  out_a[id] = di_pack_a(r);
+  out_b[id] = di_pack_b(r);
+  if (c.cfg.di_spatial_passes == 0) {
+    pout_a[id] = di_pack_a(r);
+    pout_b[id] = di_pack_b(r);
+  }
+  pl.y = rng;
+  fb.payload[id] = pl;
+}
+
+// restir_gi_temporal.wgsl:67-116
+__global__ void k_gi_temporal(DevScene s, FrameBuffers fb, Consts c, const uint4* in_a, const uint4* in_b,
+                              uint4* out_a, uint4* out_b, const uint4* prev_a, const uint4* prev_b,
+                              uint4* pout_a, uint4* pout_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  uint32_t id = y * c.W + x;
+  uint4 pl = fb.payload[id];
+  float pt = __uint_as_float(pl.z);
+  if (pt < 0.0f) return;
+  const uint32_t cur = c.frame_idx & 1u;
+  uint32_t rng = pl.y;
+  float3 T = unpack_rgb9e5(pl.x);
+  float4 ray = fb.rays[id];
+  float3 direction = ray_dir(ray);
+  float3 hit = ray_org(ray) + direction * pt;
+  uint4 cx = fb.ctx[id];
+  GiRes r = gi_unpack(in_a[id], in_b[id]);
+  float2 pp;
+  if (prev_point(fb, cur, x, y, c.W, c.H, &pp)) {
+    float r0 = rnd(rng), r1 = rnd(rng);
+    uint32_t pid = stochastic_prev_id(pp, r0, r1, c.W, c.H);
+    GT g = gt_load(fb.gb_a[cur], fb.gb_b[cur], id);
+    GT pg = sample_prev_gbuffer(fb.gb_a[cur ^ 1u], fb.gb_b[cur ^ 1u], c.W, c.H, pp);
+    if (history_valid(g, pg)) {
+      GiRes pr = gi_unpack(prev_a[pid], prev_b[pid]);
+      pr.M = dm::fmin(pr.M, c.cfg.gi_temporal_m_cap);
+      pr.phat = gi_phat(s, pr, cx, T, hit, -direction);
+      r = gi_combine(r, pr, rng);
+    }
+  }
+  out_a[id] = gi_pack_a(r);
+  out_b[id] = gi_pack_b(r);
+  if (c.cfg.gi_spatial_passes == 0) {
+    pout_a[id] = gi_pack_a(r);
+    pout_b[id] = gi_pack_b(r);
+  }
+  pl.y = rng;
+  fb.payload[id] = pl;
+}
+
+APD uint32_t mirror(int x, int mx) {
+  int v = ((x + mx) % (2 * mx)) - mx;
+  return (uint32_t)(v < 0 ? -v : v);
+}
+APD float ign_animated(uint32_t px, uint32_t py, uint32_t frame) {
+  uint32_t fid = frame % 64u;
+  float x = (float)px + 5.588238f * (float)fid;
+  float y = (float)py + 5.588238f * (float)fid;
+  return dm::fract(52.9829189f * dm::fract(0.06711056f * x + 0.00583715f * y));
+}
+APD float depth_cs(float d, float zn, float zf) {
+  float zl = (d - zn) / zf;
+  return (zn * zf) / (zf - zl * (zf - zn));
+}
+
+// restir_di_spatial.wgsl:70-163 (GI = false) and restir_gi_spatial.wgsl:71-166 (GI = true)
+template <bool GI>
+__global__ void k_spatial(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx, uint32_t pass_count,
+                          uint32_t nsamples, uint32_t unbiased, const uint4* in_a, const uint4* in_b, uint4* out_a,
+                          uint4* out_b, uint4* prev_a, uint4* prev_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  uint32_t id = y * c.W + x;
+  uint4 pl = fb.payload[id];
+  float pt = __uint_as_float(pl.z);
+  if (pt < 0.0f) return;
+  const uint32_t cur = c.frame_idx & 1u;
+  const uint4* ga = fb.gb_a[cur];
+  const uint4* gbb = fb.gb_b[cur];
+  uint32_t rng = pl.y;
+  float3 T = unpack_rgb9e5(pl.x);
+  float4 ray = fb.rays[id];
+  float3 direction = ray_dir(ray);
+  float3 hit = ray_org(ray) + direction * pt;
+  uint4 cx = fb.ctx[id];
+  float cdepth = depth_cs(__uint_as_float(ga[id].w), 0.001f, 10000.0f);
+  float3 cn = unpack_oct30(gbb[id].x);
+  float radius = (float)(c.W + c.H) / 2.0f * 0.05f;
+  uint32_t frame_arg = GI ? c.seed * 3u + pass_idx : c.seed * pass_count + pass_idx;
+  float roff = ign_animated(x, y, frame_arg);
+  uint32_t psx = pass_idx == 0 ? (x >> 2) : (x >> 1);
+  uint32_t psy = pass_idx == 0 ? (y >> 2) : (y >> 1);
+  uint32_t aseed = hash_combine(psx, hash_combine(psy, frame_arg));
+  float aoff = __uint2float_rn(aseed) * (1.0f / 4294967296.0f) * kTwoPi;
+  const float golden = 2.39996322972865332f;
+  DiRes rdi;
+  GiRes rgi;
+  if (GI) rgi = gi_unpack(in_a[id], in_b[id]);
+  else rdi = di_unpack(in_a[id], in_b[id]);
+  float3 wo = -direction;
+  for (uint32_t i = 0; i < nsamples; ++i) {
+    float angle = (float)i * golden + aoff;
+    float cr = dm::pow_((float)i / (float)nsamples, 0.5f) * radius + roff;
+    float sa, ca;
+    dm::sincos_(angle, &sa, &ca);
+    int ox = dm::f2i(cr * ca), oy = dm::f2i(cr * sa);
+    // mirror_pixel (restir_*_spatial.wgsl:59-68) can return the resolution itself
+    // (one past the edge, an out-of-bounds read in the reference): clamp to the edge
+    uint32_t nx = min(mirror((int)x + ox, (int)c.W), c.W - 1), ny = min(mirror((int)y + oy, (int)c.H), c.H - 1);
+    uint32_t nid = ny * c.W + nx;
+    if (nid == id) continue;
+    bool valid = true;
+    uint4 nga = ga[nid];
+    float ndepth = __uint_as_float(nga.w);
+    if (ndepth == 0.0f) {
+      valid = false;
+    } else {
+      float nd = depth_cs(ndepth, 0.001f, 10000.0f);
+      bool vd = (dm::fabs_(cdepth - nd) / cdepth) < 0.1f;
+      bool vn = dot(cn, unpack_oct30(gbb[nid].x)) > 0.906f;
+      valid = vd && vn;
+    }
+    if (valid) {
+      float3 npos = f3(__uint_as_float(nga.x), __uint_as_float(nga.y), __uint_as_float(nga.z));
+      if (!GI) {
+        DiRes nr = di_unpack(in_a[nid], in_b[nid]);
+        nr.phat = ls_phat(s, nr.s, cx, hit, wo, unbiased > 0);
+        valid = nr.phat > 0.0f;
+        if (!unbiased) {
+          rdi = di_combine(rdi, nr, rng);
+        } else {
+          float3 nwo = -ray_dir(fb.rays[nid]);
+          uint4 ncx = fb.ctx[nid];
+          DiRes cmb = di_new();
+          di_update(cmb, rdi.phat * rdi.W * rdi.M, rng, rdi.s, rdi.phat);
+          di_update(cmb, nr.phat * nr.W * nr.M, rng, nr.s, nr.phat);
+          cmb.M = rdi.M + nr.M;
+          float z = 0.0f;
+          if (ls_phat(s, cmb.s, cx, hit, wo, true) > 0.0f) z = z + rdi.M;
+          if (ls_phat(s, cmb.s, ncx, npos, nwo, true) > 0.0f) z = z + nr.M;
+          if (cmb.phat > 1e-6f && z * cmb.wsum > 1e-6f) cmb.W = (1.0f / cmb.phat) * (1.0f / z * cmb.wsum);
+          rdi = cmb;
+        }
+      } else {
+        GiRes nr = gi_unpack(in_a[nid], in_b[nid]);
+        nr.phat = gi_phat(s, nr, cx, T, hit, wo);
+        valid = nr.phat > 0.0f;
+        if (!unbiased) {
+          rgi = gi_combine(rgi, nr, rng);
+        } else {
+          float3 nwo = -ray_dir(fb.rays[nid]);
+          float3 nT = unpack_rgb9e5(fb.payload[nid].x);
+          uint4 ncx = fb.ctx[nid];
+          GiRes cmb = gi_new();
+          gi_update(cmb, rgi.phat * rgi.W * rgi.M, rng, rgi.point, rgi.phat, rgi.phat_rng);
+          gi_update(cmb, nr.phat * nr.W * nr.M, rng, nr.point, nr.phat, nr.phat_rng);
+          cmb.M = rgi.M + nr.M;
+          float z = 0.0f;
+          if (gi_phat(s, cmb, cx, T, hit, wo) > 0.0f) z = z + rgi.M;
+          if (gi_phat(s, cmb, ncx, nT, npos, nwo) > 0.0f) z = z + nr.M;
+          if (cmb.phat > 0.0f && z * cmb.wsum > 0.0f) cmb.W = (1.0f / cmb.phat) * (1.0f / z * cmb.wsum);
+          rgi = cmb;
+        }
+      }
+    }
+    if (!valid) radius = dm::fmax(radius * 0.5f, 3.0f);
+  }
+  if (GI) {
+    out_a[id] = gi_pack_a(rgi);
+    out_b[id] = gi_pack_b(rgi);
+    if (pass_idx == pass_count - 1) {
+      prev_a[id] = gi_pack_a(rgi);
+      prev_b[id] = gi_pack_b(rgi);
+    }
+  } else {
+    out_a[id] = di_pack_a(rdi);
+    out_b[id] = di_pack_b(rdi);
+    if (pass_idx == pass_count - 1) {
+      prev_a[id] = di_pack_a(rdi);
+      prev_b[id] = di_pack_b(rdi);
+    }
+  }
+  pl.y = rng;
+  fb.payload[id] = pl;
+}
+
+// ---- denoising -------------------------------------------------------------
+
+// demodulate_radiance.wgsl:24-42
+__global__ void k_demodulate(FrameBuffers fb, uint32_t P, uint32_t cur, const uint32_t* in, uint32_t* out,
+                             int remodulate) {
+  uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= P) return;
+  float3 alb = unpack_rgb9e5(fb.gb_b[cur][id].y);
+  float3 r = unpack_rgb9e5(in[id]);
+  if (remodulate) r = r * alb;
+  else r = f3(alb.x > 0.0f ? r.x / alb.x : 0.0f, alb.y > 0.0f ? r.y / alb.y : 0.0f, alb.z > 0.0f ? r.z / alb.z : 0.0f);
+  out[id] = pack_rgb9e5(r);
+}
+
+// firefly_filter.wgsl:20-85; neighbours come from the unfiltered copy `src`.
+__global__ void k_firefly(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t cur, const uint32_t* src, uint32_t* dst) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  uint32_t id = y * W + x;
+  const uint4* ga = fb.gb_a[cur];
+  if (__uint_as_float(ga[id].w) == 0.0f) return;
+  float3 curc = unpack_rgb9e5(src[id]);
+  float min_l = dm::F32_MAX, max_l = 0.0f;
+  float3 min_c = curc, max_c = f3s(0.0f);
+  float cl = luma(curc);
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy) {
+      if (dx == 0 && dy == 0) continue;
+      int sx = (int)x + dx, sy = (int)y + dy;
+      if (sx < 0 || sy < 0 || sx >= (int)W || sy >= (int)H) continue;
+      uint32_t sid = (uint32_t)sy * W + (uint32_t)sx;
+      if (__uint_as_float(ga[sid].w) == 0.0f) continue;
+      float3 nc = unpack_rgb9e5(src[sid]);
+      float nl = luma(nc);
+      if (nl < min_l) {
+        min_l = nl;
+        min_c = nc;
+      } else if (nl > max_l) {
+        max_l = nl;
+        max_c = nc;
+      }
+    }
+  float3 rec = cl < min_l ? min_c : (cl > max_l ? max_c : curc);
+  if (min_l > max_l) rec = curc;
+  dst[id] = pack_rgb9e5(rec);
+}
+
+// svgf_temporal.wgsl:87-139
+__global__ void k_svgf_temporal(FrameBuffers fb, Consts c, const uint32_t* demod, uint32_t* out_rad,
+                                const float2* in_mom, float2* out_mom, float* out_var) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  uint32_t id = y * c.W + x;
+  const uint32_t cur = c.frame_idx & 1u;
+  GT g = gt_load(fb.gb_a[cur], fb.gb_b[cur], id);
+  float3 rad = unpack_rgb9e5(demod[id]);
+  if (g.depth == 0.0f) {
+    out_rad[id] = pack_rgb9e5(rad);
+    return;
+  }
+  float mx = luma(rad);
+  float my = sqr(mx);
+  float3 trad = f3s(0.0f);
+  float tmx = 0.0f, tmy = 0.0f;
+  uint32_t count = 0;
+  float2 pp;
+  if (prev_point(fb, cur, x, y, c.W, c.H, &pp)) {
+    GT pg = sample_prev_gbuffer(fb.gb_a[cur ^ 1u], fb.gb_b[cur ^ 1u], c.W, c.H, pp);
+    if (history_valid(g, pg)) {
+      uint32_t ix = dm::f2u(floorf(pp.x)), iy = dm::f2u(floorf(pp.y));
+      float fx = dm::fract(pp.x), fy = dm::fract(pp.y);
+      uint32_t x1 = min(ix + 1, c.W - 1), y1 = min(iy + 1, c.H - 1);
+      uint32_t i00 = iy * c.W + ix, i10 = iy * c.W + x1, i01 = y1 * c.W + ix, i11 = y1 * c.W + x1;
+      float3 c0 = mix3(unpack_rgb9e5(fb.svgf_hist[i00]), unpack_rgb9e5(fb.svgf_hist[i10]), fx);
+      float3 c1 = mix3(unpack_rgb9e5(fb.svgf_hist[i01]), unpack_rgb9e5(fb.svgf_hist[i11]), fx);
+      trad = mix3(c0, c1, fy);
+      float2 m00 = in_mom[i00], m10 = in_mom[i10], m01 = in_mom[i01], m11 = in_mom[i11];
+      float m0x = mixf(m00.x, m10.x, fx), m0y = mixf(m00.y, m10.y, fx);
+      float m1x = mixf(m01.x, m11.x, fx), m1y = mixf(m01.y, m11.y, fx);
+      tmx = mixf(m0x, m1x, fy);
+      tmy = mixf(m0y, m1y, fy);
+      count = min(fb.svgf_count[id] + 1u, c.cfg.svgf_max_history);
+    }
+  }
+  float alpha = 1.0f / (1.0f + (float)count);
+  tmx = mixf(tmx, mx, alpha);
+  tmy = mixf(tmy, my, alpha);
+  trad = mix3(trad, rad, alpha);
+  out_var[id] = dm::fmax(tmy - sqr(tmx), 0.0f);
+  out_rad[id] = pack_rgb9e5(trad);
+  out_mom[id] = make_float2(tmx, tmy);
+  fb.svgf_count[id] = count;
+}
+
+// svgf_atrous.wgsl:48-117.  A 16x16 block stages radiance, variance, normal
+// and depth of its tile plus a halo of 2*step pixels in shared memory when the
+// halo is small (steps 1, 2, 4); larger steps read through L1/L2.
+constexpr int kAtrousTile = 16;
+template <int STEP>
+__global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t cur,
+                                                uint32_t pass_idx, const uint32_t* in_rad, uint32_t* out_rad,
+                                                const float* in_var, float* out_var) {
+  constexpr int HALO = 2 * STEP;
+  constexpr int SW = kAtrousTile + 2 * HALO;
+  constexpr bool kShared = STEP <= 4;
+  __shared__ uint4 s_px[kShared ? SW * SW : 1];  // radiance, variance bits, normal, depth bits
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x0 = blockIdx.x * kAtrousTile, y0 = blockIdx.y * kAtrousTile;
+  const uint4* ga = fb.gb_a[cur];
+  const uint4* gbb = fb.gb_b[cur];
+  if (kShared) {
+    for (int k = ty * kAtrousTile + tx; k < SW * SW; k += kAtrousTile * kAtrousTile) {
+      int sx = x0 - HALO + (k % SW), sy = y0 - HALO + (k / SW);
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (sx >= 0 && sy >= 0 && sx < (int)W && sy < (int)H) {
+        uint32_t sid = (uint32_t)sy * W + (uint32_t)sx;
+        v = make_uint4(in_rad[sid], __float_as_uint(in_var[sid]), gbb[sid].x, ga[sid].w);
+      }
+      s_px[k] = v;
+    }
+    __syncthreads();
+  }
+  int x = x0 + tx, y = y0 + ty;
+  if (x >= (int)W || y >= (int)H) return;
+  uint32_t id = (uint32_t)y * W + (uint32_t)x;
+  auto fetch = [&](int px, int py) -> uint4 {
+    if (kShared) return s_px[(py - y0 + HALO) * SW + (px - x0 + HALO)];
+    uint32_t sid = (uint32_t)py * W + (uint32_t)px;
+    return make_uint4(in_rad[sid], __float_as_uint(in_var[sid]), gbb[sid].x, ga[sid].w);
+  };
+  uint4 cpx = fetch(x, y);
+  float cdepth = __uint_as_float(cpx.w);
+  if (cdepth == 0.0f) return;
+  float3 cn = unpack_oct30(cpx.z);
+  const float KW[3] = {3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
+  float3 rsum = unpack_rgb9e5(cpx.x);
+  float vsum = __uint_as_float(cpx.y);
+  float wsum = 1.0f;
+  float cl = luma(rsum);
+  float cv = vsum;
+  float lum_den = dm::fmax(4.0f * dm::sqrt_(cv), 1e-8f);
+  for (int dy = -2; dy <= 2; ++dy)
+    for (int dx = -2; dx <= 2; ++dx) {
+      if (dy == 0 && dx == 0) continue;
+      int sx = x + dx * STEP, sy = y + dy * STEP;
+      if (sx < 0 || sy < 0 || sx >= (int)W || sy >= (int)H) continue;
+      uint4 spx = fetch(sx, sy);
+      float sdepth = __uint_as_float(spx.w);
+      if (sdepth == 0.0f) continue;
+      float3 srad = unpack_rgb9e5(spx.x);
+      float sl = luma(srad);
+      float nw = dm::pow_(dm::fmax(dot(cn, unpack_oct30(spx.z)), 0.0f), 128.0f);
+      float dd = dm::fabs_(cdepth - sdepth);
+      float dw = dm::exp_(-sqr(dd) / (2.0f * sqr(0.1f)));
+      float ld = dm::fabs_(cl - sl);
+      float lw = dm::exp_(-ld / lum_den);
+      float w = nw * dw * lw;
+      w = w * (KW[dx < 0 ? -dx : dx] * KW[dy < 0 ? -dy : dy]);
+      rsum = rsum + srad * w;
+      vsum = vsum + __uint_as_float(spx.y) * sqr(w);
+      wsum = wsum + w;
+    }
+  rsum = rsum / wsum;
+  vsum = vsum / sqr(wsum);
+  uint32_t packed = pack_rgb9e5(rsum);
+  out_rad[id] = packed;
+  out_var[id] = vsum;
+  if (pass_idx == 0) fb.svgf_hist[id] = packed;
+}
+
+// taa.wgsl:67-171; neighbours come from the pre-TAA copy `src`.
+APD float mitchell(float x_, float B, float C) {
+  float x = dm::fabs_(2.0f * x_);
+  float ods = 1.0f / 6.0f;
+  if (x > 1.0f)
+    return ((-B - 6.0f * C) * x * x * x + (6.0f * B + 30.0f * C) * x * x + (-12.0f * B - 48.0f * C) * x +
+            (8.0f * B + 24.0f * C)) * ods;
+  return ((12.0f - 9.0f * B - 6.0f * C) * x * x * x + (-18.0f + 12.0f * B + 6.0f * C) * x * x + (6.0f - 2.0f * B)) *
+         ods;
+}
+__global__ void k_taa(FrameBuffers fb, Consts c, const uint32_t* src, uint32_t* dst, const uint32_t* prevb) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  uint32_t id = y * c.W + x;
+  const uint32_t cur = c.frame_idx & 1u;
+  float cdepth = __uint_as_float(fb.gb_a[cur][id].w);
+  if (cdepth == 0.0f) return;
+  float3 curc = unpack_rgb9e5(src[id]);
+  float wsum = sqr(mitchell(0.0f, 0.33f, 0.33f));
+  float3 rec = curc * wsum;
+  float3 m1 = curc, m2 = curc * curc;
+  float cnt = 1.0f;
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy) {
+      if (dx == 0 && dy == 0) continue;
+      int sx = (int)x + dx, sy = (int)y + dy;
+      if (sx < 0 || sy < 0 || sx >= (int)c.W || sy >= (int)c.H) continue;
+      uint32_t sid = (uint32_t)sy * c.W + (uint32_t)sx;
+      float3 sc = vmax(unpack_rgb9e5(src[sid]), f3s(0.0f));
+      float w = mitchell((float)dx, 0.33f, 0.33f) * mitchell((float)dy, 0.33f, 0.33f);
+      w = w * (1.0f / (1.0f + luma(sc)));
+      rec = rec + sc * w;
+      wsum = wsum + w;
+      m1 = m1 + sc;
+      m2 = m2 + sc * sc;
+      cnt = cnt + 1.0f;
+    }
+  rec = rec / dm::fmax(wsum, 1e-5f);
+  float3 hist;
+  uint32_t pid;
+  float2 pp;
+  if (prev_point(fb, cur, x, y, c.W, c.H, &pp)) {
+    uint32_t fx = dm::f2u(floorf(pp.x)), fy = dm::f2u(floorf(pp.y));
+    uint32_t cxp = dm::f2u(ceilf(pp.x)), cyp = dm::f2u(ceilf(pp.y));
+    pid = fy * c.W + fx;
+    uint32_t i00 = min(fy, c.H - 1) * c.W + min(fx, c.W - 1);
+    uint32_t i10 = min(cyp, c.H - 1) * c.W + min(fx, c.W - 1);
+    uint32_t i01 = min(fy, c.H - 1) * c.W + min(cxp, c.W - 1);
+    uint32_t i11 = min(cyp, c.H - 1) * c.W + min(cxp, c.W - 1);
+    float3 h00 = unpack_rgb9e5(prevb[i00]), h10 = unpack_rgb9e5(prevb[i10]);
+    float3 h01 = unpack_rgb9e5(prevb[i01]), h11 = unpack_rgb9e5(prevb[i11]);
+    float tx = dm::fract(pp.x), ty = dm::fract(pp.y);
+    float3 a = h00 * (1.0f - tx) + h10 * tx;
+    float3 b = h01 * (1.0f - tx) + h11 * tx;
+    hist = a * (1.0f - ty) + b * ty;
+  } else {
+    hist = unpack_rgb9e5(prevb[id]);
+    pid = id;
+  }
+  float pdepth = __uint_as_float(fb.gb_a[cur ^ 1u][pid].w);
+  float cdcs = depth_cs(cdepth, 0.001f, 10000.0f), pdcs = depth_cs(pdepth, 0.001f, 10000.0f);
+  bool vdd = (dm::fabs_(cdcs - pdcs) / cdcs) < 0.1f;
+  float3 mean = m1 / cnt;
+  float3 sd = vabs(m2 - (m1 * m1) / cnt);
+  sd = sd / (cnt - 1.0f);
+  sd = vsqrt(sd);
+  float3 lo = mean - sd, hi = mean + sd;
+  float3 center = 0.5f * (hi + lo);
+  float3 ext = 0.5f * (hi - lo);
+  float3 rtc = hist - center;
+  float3 rtcu = vabs(rtc / ext);
+  float mxv = dm::fmax(rtcu.x, dm::fmax(rtcu.y, rtcu.z));
+  float3 clipped = mxv > 1.0f ? center + rtc / mxv : hist;
+  float blend = 1.0f - (c.cfg.taa_history_influence * (vdd ? 1.0f : 0.0f));
+  float cw = dm::saturate(blend * (1.0f / (1.0f + luma(rec))));
+  float hw = dm::saturate((1.0f - blend) * (1.0f / (1.0f + luma(clipped))));
+  rec = (cw * rec + hw * clipped) / (cw + hw);
+  dst[id] = pack_rgb9e5(rec);
+}
+
+// resolve.wgsl:48-49 (before the tonemap): linear HDR = radiance / sample_count.
+__global__ void k_resolve(FrameBuffers fb, uint32_t P, float inv_count_den) {
+  uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= P) return;
+  float3 r = unpack_rgb9e5(fb.radiance[id]);
+  r = r / inv_count_den;
+  fb.out_rgb[3 * id + 0] = r.x;
+  fb.out_rgb[3 * id + 1] = r.y;
+  fb.out_rgb[3 * id + 2] = r.z;
+}
+
+// Batch traversal for tests and the traversal benchmark (persistent, warp fetch).
+__global__ void __launch_bounds__(kBlock) k_trace_batch(DevScene s, const float4* origins, const float4* dirs,
+                                                        uint32_t n, int any_hit, uint4* out, uint32_t* cursor) {
+  const uint32_t lane = threadIdx.x & 31;
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(cursor, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    uint32_t i = base + lane;
+    if (i < n) {
+      float4 o = origins[i], d = dirs[i];
+      float3 oo = f3(o.x, o.y, o.z), dd = f3(d.x, d.y, d.z);
+      if (any_hit) {
+        bool occ = trace_any(s, oo, dd, o.w);
+        out[i] = make_uint4(occ ? 1u : 0u, 0u, 0u, 0u);
+      } else {
+        Hit h;
+        trace_closest(s, oo, dd, o.w, h);
+        out[i] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.u), __float_as_uint(h.v), h.tri);
+      }
+    }
+  }
+}
+
+template <typename T>
+T* carve(char*& p, size_t count) {
+  T* r = reinterpret_cast<T*>(p);
+  p += ((count * sizeof(T) + 255) / 256) * 256;
+  return r;
+}
+
+}  // namespace
+
+size_t frame_buffer_bytes(uint32_t W, uint32_t H) {
+  FrameBuffers fb;
+  char* p = nullptr;
+  size_t P = (size_t)W * H;
+  (void)fb;
+  size_t n = 0;
+  auto add = [&](size_t bytes) { n += ((bytes + 255) / 256) * 256; };
+  add(P * 16);  // rays
+  add(P * 16);  // payload
+  add(P * 4);   // radiance
+  add(P * 16);  // hits
+  for (int i = 0; i < 6; ++i) add(P * 16);  // di a,b inter a,b prev a,b[0]
+  add(P * 16); add(P * 16);                 // di prev [1] a,b
+  add(P * 16);                              // ctx
+  for (int i = 0; i < 6; ++i) add(P * 16);  // gi
+  add(P * 16); add(P * 16);
+  for (int i = 0; i < 4; ++i) add(P * 16);  // gbuffer
+  add(P * 4); add(P * 4);                   // demod
+  add(P * 4); add(P * 4);                   // svgf rad
+  add(P * 8); add(P * 8);                   // moments
+  add(P * 4); add(P * 4);                   // variance
+  add(P * 4); add(P * 4);                   // count, hist
+  add(P * 4);                               // snapshot
+  add(P * 4); add(P * 4);                   // queues
+  add(64 * 4);                              // counters
+  add(P * 12);                              // out rgb
+  (void)p;
+  return n;
+}
+
+void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
+  char* p = static_cast<char*>(base);
+  size_t P = (size_t)W * H;
+  fb->rays = carve<float4>(p, P);
+  fb->payload = carve<uint4>(p, P);
+  fb->radiance = carve<uint32_t>(p, P);
+  fb->hits = carve<uint4>(p, P);
+  fb->di_a = carve<uint4>(p, P);
+  fb->di_b = carve<uint4>(p, P);
+  fb->di_inter_a = carve<uint4>(p, P);
+  fb->di_inter_b = carve<uint4>(p, P);
+  fb->di_prev_a[0] = carve<uint4>(p, P);
+  fb->di_prev_b[0] = carve<uint4>(p, P);
+  fb->di_prev_a[1] = carve<uint4>(p, P);
+  fb->di_prev_b[1] = carve<uint4>(p, P);
+  fb->ctx = carve<uint4>(p, P);
+  fb->gi_a = carve<uint4>(p, P);
+  fb->gi_b = carve<uint4>(p, P);
+  fb->gi_inter_a = carve<uint4>(p, P);
+  fb->gi_inter_b = carve<uint4>(p, P);
+  fb->gi_prev_a[0] = carve<uint4>(p, P);
+  fb->gi_prev_b[0] = carve<uint4>(p, P);
+  fb->gi_prev_a[1] = carve<uint4>(p, P);
+  fb->gi_prev_b[1] = carve<uint4>(p, P);
+  fb->gb_a[0] = carve<uint4>(p, P);
+  fb->gb_b[0] = carve<uint4>(p, P);
+  fb->gb_a[1] = carve<uint4>(p, P);
+  fb->gb_b[1] = carve<uint4>(p, P);
+  fb->demod[0] = carve<uint32_t>(p, P);
+  fb->demod[1] = carve<uint32_t>(p, P);
+  fb->svgf_rad[0] = carve<uint32_t>(p, P);
+  fb->svgf_rad[1] = carve<uint32_t>(p, P);
+  fb->svgf_mom[0] = carve<float2>(p, P);
+  fb->svgf_mom[1] = carve<float2>(p, P);
+  fb->svgf_var[0] = carve<float>(p, P);
+  fb->svgf_var[1] = carve<float>(p, P);
+  fb->svgf_count = carve<uint32_t>(p, P);
+  fb->svgf_hist = carve<uint32_t>(p, P);
+  fb->snapshot = carve<uint32_t>(p, P);
+  fb->queue[0] = carve<uint32_t>(p, P);
+  fb->queue[1] = carve<uint32_t>(p, P);
+  fb->counters = carve<uint32_t>(p, 64);
+  fb->out_rgb = carve<float>(p, 3 * P);
+}
+
+void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
+                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t st) {
+  const uint32_t P = W * H;
+  const uint32_t cur = frame_idx & 1u;
+  dim3 b2(16, 16), g2((W + 15) / 16, (H + 15) / 16);
+  const int persistent_blocks = num_sms * 8;  // 8 x 128 threads per SM
+  const int linear_blocks = (int)std::min<uint32_t>((P + kBlock - 1) / kBlock, (uint32_t)num_sms * 16u);
+  Consts c;
+  c.W = W;
+  c.H = H;
+  c.P = P;
+  c.frame_idx = frame_idx;
+  c.cfg = cfg;
+  cudaMemsetAsync(fb.radiance, 0, (size_t)P * 4, st);
+  for (uint32_t sample = 0; sample < cfg.sample_count; ++sample) {
+    c.seed = frame_idx * cfg.sample_count + sample;
+    k_raygen<<<g2, b2, 0, st>>>(fb, W, H, mats);
+    for (uint32_t i = 0; i < cfg.max_bounces; ++i) {
+      c.bounce = i;
+      c.qin = i & 1u;
+      c.qout = (i + 1) & 1u;
+      cudaMemsetAsync(fb.counters + 2, 0, 4, st);
+      k_extend<<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
+      k_shade<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c, mats);
+      if (i == 0) {
+        if (cfg.restir_di) {
+          uint4* pin_a = fb.di_prev_a[cur];
+          uint4* pin_b = fb.di_prev_b[cur];
+          uint4* pout_a = fb.di_prev_a[cur ^ 1u];
+          uint4* pout_b = fb.di_prev_b[cur ^ 1u];
+          k_di_temporal<<<g2, b2, 0, st>>>(scene, fb, c, fb.di_a, fb.di_b, fb.di_inter_a, fb.di_inter_b, pin_a, pin_b,
+                                           pout_a, pout_b);
+          uint32_t n = cfg.di_spatial_passes;
+          for (uint32_t k = 0; k < n; ++k) {
+            bool odd = (k % 2) != 0;
+            k_spatial<false><<<g2, b2, 0, st>>>(scene, fb, c, k, n, cfg.di_spatial_samples, cfg.di_unbiased,
+                                                odd ? fb.di_a : fb.di_inter_a, odd ? fb.di_b : fb.di_inter_b,
+                                                odd ? fb.di_inter_a : fb.di_a, odd ? fb.di_inter_b : fb.di_b, pout_a,
+                                                pout_b);
+          }
+          if (n % 2 == 0) {
+            cudaMemcpyAsync(fb.di_a, fb.di_inter_a, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(fb.di_b, fb.di_inter_b, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+          }
+        }
+        if (cfg.restir_gi) {
+          uint4* pin_a = fb.gi_prev_a[cur];
+          uint4* pin_b = fb.gi_prev_b[cur];
+          uint4* pout_a = fb.gi_prev_a[cur ^ 1u];
+          uint4* pout_b = fb.gi_prev_b[cur ^ 1u];
+          k_gi_temporal<<<g2, b2, 0, st>>>(scene, fb, c, fb.gi_a, fb.gi_b, fb.gi_inter_a, fb.gi_inter_b, pin_a, pin_b,
+                                           pout_a, pout_b);
+          uint32_t n = cfg.gi_spatial_passes;
+          if (n == 0) {
+            cudaMemcpyAsync(fb.gi_a, fb.gi_inter_a, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(fb.gi_b, fb.gi_inter_b, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+          }
+          for (uint32_t k = 0; k < n; ++k) {
+            bool odd = (k % 2) != 0;
+            k_spatial<true><<<g2, b2, 0, st>>>(scene, fb, c, k, n, cfg.gi_spatial_samples, cfg.gi_unbiased,
+                                               odd ? fb.gi_a : fb.gi_inter_a, odd ? fb.gi_b : fb.gi_inter_b,
+                                               odd ? fb.gi_inter_a : fb.gi_a, odd ? fb.gi_inter_b : fb.gi_b, pout_a,
+                                               pout_b);
+          }
+          if (n > 0 && n % 2 == 0) {
+            cudaMemcpyAsync(fb.gi_a, fb.gi_inter_a, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(fb.gi_b, fb.gi_inter_b, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+          }
+        }
+      }
+      k_apply_di<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
+      if (i + 1 < cfg.max_bounces) {
+        cudaMemsetAsync(fb.counters + c.qout, 0, 4, st);
+        k_apply_gi<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
+      }
+    }
+  }
+  // demodulate -> firefly -> SVGF -> TAA -> remodulate -> resolve (lib.rs:492-576)
+  const int lb = (int)((P + 255) / 256);
+  uint32_t* dcur = fb.demod[cur];
+  uint32_t* dprev = fb.demod[cur ^ 1u];
+  k_demodulate<<<lb, 256, 0, st>>>(fb, P, cur, fb.radiance, dcur, 0);
+  if (cfg.firefly_filter) {
+    cudaMemcpyAsync(fb.snapshot, dcur, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
+    k_firefly<<<g2, b2, 0, st>>>(fb, W, H, cur, fb.snapshot, dcur);
+  }
+  if (cfg.svgf) {
+    uint32_t f = frame_idx;
+    k_svgf_temporal<<<g2, b2, 0, st>>>(fb, c, dcur, fb.svgf_rad[(f + 1) % 2], fb.svgf_mom[f % 2],
+                                       fb.svgf_mom[(f + 1) % 2], fb.svgf_var[(f + 1) % 2]);
+    for (uint32_t i = 0; i < cfg.svgf_atrous_passes; ++i) {
+      const uint32_t* in_rad = fb.svgf_rad[(f + 1 + i) % 2];
+      uint32_t* out_rad = fb.svgf_rad[(f + i) % 2];
+      const float* in_var = fb.svgf_var[(f + 1 + i) % 2];
+      float* out_var = fb.svgf_var[(f + i) % 2];
+      dim3 bt(kAtrousTile, kAtrousTile), gt((W + kAtrousTile - 1) / kAtrousTile, (H + kAtrousTile - 1) / kAtrousTile);
+      switch (i) {
+        case 0: k_atrous<1><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+        case 1: k_atrous<2><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+        case 2: k_atrous<4><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+        case 3: k_atrous<8><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+        case 4: k_atrous<16><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+        case 5: k_atrous<32><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+        case 6: k_atrous<64><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+        default: k_atrous<128><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+      }
+      if (i == cfg.svgf_atrous_passes - 1)
+        cudaMemcpyAsync(dcur, out_rad, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
+    }
+  }
+  if (cfg.taa && frame_idx > 0) {
+    cudaMemcpyAsync(fb.snapshot, dcur, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
+    k_taa<<<g2, b2, 0, st>>>(fb, c, fb.snapshot, dcur, dprev);
+  }
+  k_demodulate<<<lb, 256, 0, st>>>(fb, P, cur, dcur, fb.radiance, 1);
+  k_resolve<<<lb, 256, 0, st>>>(fb, P, (float)cfg.sample_count);
+}
+
+void launch_trace_batch(const DevScene& scene, const float4* origins, const float4* dirs, uint32_t n, int any_hit,
+                        uint4* out, uint32_t* cursor, int num_sms, cudaStream_t st) {
+  cudaMemsetAsync(cursor, 0, 4, st);
+  k_trace_batch<<<num_sms * 8, kBlock, 0, st>>>(scene, origins, dirs, n, any_hit, out, cursor);
+}
+
+}  // namespace ap

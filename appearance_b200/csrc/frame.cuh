@@ -1,0 +1,72 @@
+// Per-frame device buffers, constants and kernel launchers of the wavefront
+// path tracer (one frame = PathTracerGpu::render, crates/appearance-path-
+// tracer-gpu/src/lib.rs:314-615).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "scene_layout.h"
+
+namespace ap {
+
+// Same field order as ap_frame_config (include/appearance_cuda.h).
+struct FrameConfig {
+  uint32_t max_bounces, sample_count;
+  uint32_t restir_di, restir_gi, svgf, firefly_filter, taa;
+  uint32_t di_area_samples, di_bsdf_samples;
+  float di_temporal_m_factor;
+  uint32_t di_spatial_passes, di_spatial_samples, di_unbiased;
+  float gi_temporal_m_cap;
+  uint32_t gi_spatial_passes, gi_spatial_samples, gi_unbiased;
+  uint32_t svgf_max_history, svgf_atrous_passes;
+  float taa_history_influence;
+};
+
+// Per-pixel state, structure-of-arrays, every record 4 or 16 bytes so that a
+// warp reads whole 128-byte lines.
+struct FrameBuffers {
+  float4* rays;        // origin.xyz, oct30 direction bits
+  uint4* payload;      // throughput rgb9e5, rng, t bits, unused
+  uint32_t* radiance;  // rgb9e5
+  uint4* hits;         // t, u, v bits, global triangle id (extension stage)
+  uint4 *di_a, *di_b;  // DiReservoir: (M, W, wsum, phat), (uv, emissive instance, triangle)
+  uint4 *di_inter_a, *di_inter_b, *di_prev_a[2], *di_prev_b[2];
+  uint4* ctx;          // LightSampleCtx: material, throughput, n, clearcoat n
+  uint4 *gi_a, *gi_b;  // GiReservoir: (M, W, wsum, phat), (point.xyz, phat_rng)
+  uint4 *gi_inter_a, *gi_inter_b, *gi_prev_a[2], *gi_prev_b[2];
+  uint4 *gb_a[2], *gb_b[2];  // G-buffer: (pos.xyz, depth), (n oct30, albedo rgb9e5, velocity.xy)
+  uint32_t* demod[2];
+  uint32_t* svgf_rad[2];
+  float2* svgf_mom[2];
+  float* svgf_var[2];
+  uint32_t* svgf_count;
+  uint32_t* svgf_hist;
+  uint32_t* snapshot;  // pre-filter copy for the firefly filter and TAA
+  uint32_t* queue[2];  // active path ids (ping-pong)
+  uint32_t* counters;  // [0..1] queue sizes, [2] work cursor, [3..] statistics
+  float* out_rgb;      // linear HDR output, 3 floats per pixel (device)
+};
+
+struct Mats {
+  float inv_view[16], inv_proj[16], view_proj[16], prev_view_proj[16];
+};
+
+struct FrameStats {
+  unsigned long long rays_extend, rays_secondary;
+};
+
+size_t frame_buffer_bytes(uint32_t W, uint32_t H);
+// Carves `base` (frame_buffer_bytes(W,H) bytes, zeroed by the caller) into buffers.
+void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb);
+
+// Encodes one frame on `stream`.  `frame_idx` selects the ping-pong parity.
+void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
+                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t stream);
+
+// Closest / any hit for a batch of rays (parity tests and traversal bench).
+// rays: origin.xyz + tmax (float4), dirs: float4; out: t, u, v, tri bits.
+void launch_trace_batch(const DevScene& scene, const float4* origins, const float4* dirs, uint32_t n,
+                        int any_hit, uint4* out, uint32_t* cursor, int num_sms, cudaStream_t stream);
+
+}  // namespace ap

@@ -1,0 +1,255 @@
+// Software ray traversal of the compressed 8-wide BVH (scene_layout.h) and the
+// watertight ray/triangle test, for sm_100a (no RT cores).
+//
+// Node layout and quantisation follow the compressed-wide-BVH idea of
+// H. Ylitie, T. Karras, S. Laine, "Efficient Incoherent Ray Traversal on GPUs
+// Through Compressed Wide BVHs", HPG 2017: one 80-byte node holds 8 child
+// boxes quantised to 8 bits per plane relative to a per-node origin and
+// power-of-two scale, read with five 128-bit loads.  Traversal is nearest-child-
+// first with the other hit children pushed with their entry distance and
+// culled on pop.  The triangle test is Woop/Benthin/Wald (JCGT 2013) in the same
+// operation order as the CPU oracle, so closest-hit results are bit-identical:
+// the closest hit is the minimum of (t, global triangle id) over all triangles
+// that pass the test, which no traversal order can change.
+#pragma once
+
+#include "dev_common.cuh"
+#include "scene_layout.h"
+
+namespace ap {
+
+constexpr int kTraversalStack = 96;
+constexpr uint32_t kNoHit = 0xFFFFFFFFu;
+
+struct Hit {
+  float t, u, v;
+  uint32_t tri;  // global triangle id or kNoHit
+};
+
+struct RayPre {
+  float3 o, d;
+  int kx, ky, kz;
+  float sx, sy, sz;
+  float3 inv;  // box-test reciprocal direction (zero components replaced)
+};
+
+APD float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+APD RayPre ray_pre(float3 o, float3 d) {
+  RayPre r;
+  r.o = o;
+  r.d = d;
+  float ax = dm::fabs_(d.x), ay = dm::fabs_(d.y), az = dm::fabs_(d.z);
+  int kz = 0;
+  float m = ax;
+  if (ay > m) { kz = 1; m = ay; }
+  if (az > m) { kz = 2; }
+  int kx = kz + 1 == 3 ? 0 : kz + 1;
+  int ky = kx + 1 == 3 ? 0 : kx + 1;
+  if (comp(d, kz) < 0.0f) { int t = kx; kx = ky; ky = t; }
+  r.kx = kx;
+  r.ky = ky;
+  r.kz = kz;
+  float dz = comp(d, kz);
+  r.sx = comp(d, kx) / dz;
+  r.sy = comp(d, ky) / dz;
+  r.sz = 1.0f / dz;
+  const float tiny = 1e-20f;
+  float dx = dm::fabs_(d.x) < tiny ? copysignf(tiny, d.x) : d.x;
+  float dy = dm::fabs_(d.y) < tiny ? copysignf(tiny, d.y) : d.y;
+  float dzz = dm::fabs_(d.z) < tiny ? copysignf(tiny, d.z) : d.z;
+  r.inv = f3(1.0f / dx, 1.0f / dy, 1.0f / dzz);
+  return r;
+}
+
+// Watertight test; same expressions as the oracle (intersect_tri).
+APD bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float tmin, float tmax,
+                       float& t, float& u, float& v) {
+  float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+  float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
+  float Ax = comp(A, r.kx) - r.sx * Akz, Ay = comp(A, r.ky) - r.sy * Akz;
+  float Bx = comp(B, r.kx) - r.sx * Bkz, By = comp(B, r.ky) - r.sy * Bkz;
+  float Cx = comp(C, r.kx) - r.sx * Ckz, Cy = comp(C, r.ky) - r.sy * Ckz;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  float det = U + V + W;
+  if (det == 0.0f) return false;
+  float Az = r.sz * Akz, Bz = r.sz * Bkz, Cz = r.sz * Ckz;
+  float T = U * Az + V * Bz + W * Cz;
+  float rcp = 1.0f / det;
+  float tt = T * rcp;
+  if (!(tt >= tmin && tt <= tmax)) return false;
+  t = tt;
+  u = V * rcp;
+  v = W * rcp;
+  return true;
+}
+
+APD float byte_f(uint32_t word, int k) { return __uint2float_rn((word >> (8 * k)) & 0xffu); }
+
+// Box tests of the 8 children of one node.  Returns the hit mask; tnear[] gets
+// the entry distance of each hit child.  Bounds are widened by a relative
+// 2^-21 so that no child containing a triangle hit inside [tmin, tmax] is culled
+// by rounding in the slab arithmetic.
+template <bool kClosest>
+APD uint32_t node_children(const uint4 w0, const uint4 w2, const uint4 w3, const uint4 w4,
+                           const RayPre& r, float tmin, float tmax, float tnear[8]) {
+  float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+  float sxs = __uint_as_float((w0.w & 0xffu) << 23);
+  float sys = __uint_as_float(((w0.w >> 8) & 0xffu) << 23);
+  float szs = __uint_as_float(((w0.w >> 16) & 0xffu) << 23);
+  float ax = sxs * r.inv.x, ay = sys * r.inv.y, az = szs * r.inv.z;
+  float bx = (px - r.o.x) * r.inv.x, by = (py - r.o.y) * r.inv.y, bz = (pz - r.o.z) * r.inv.z;
+  const float grow = 1.0f + 4.8e-7f;
+  uint32_t mask = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    uint32_t lox = i < 4 ? w2.x : w2.y, loy = i < 4 ? w2.z : w2.w;
+    uint32_t loz = i < 4 ? w3.x : w3.y, hix = i < 4 ? w3.z : w3.w;
+    uint32_t hiy = i < 4 ? w4.x : w4.y, hiz = i < 4 ? w4.z : w4.w;
+    int k = i & 3;
+    float x0 = fmaf(byte_f(lox, k), ax, bx), x1 = fmaf(byte_f(hix, k), ax, bx);
+    float y0 = fmaf(byte_f(loy, k), ay, by), y1 = fmaf(byte_f(hiy, k), ay, by);
+    float z0 = fmaf(byte_f(loz, k), az, bz), z1 = fmaf(byte_f(hiz, k), az, bz);
+    float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+    float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fmaxf(z0, z1));
+    tf = tf * (tf > 0.0f ? grow : 1.0f / grow);
+    tn = tn * (tn > 0.0f ? 1.0f / grow : grow);
+    tnear[i] = tn;
+    if (tn <= tf && tn <= tmax * grow) mask |= 1u << i;
+  }
+  return mask;
+}
+
+APD uint32_t meta_of(const uint4 w1, int i) { return ((i < 4 ? w1.z : w1.w) >> (8 * (i & 3))) & 0xffu; }
+
+// Closest hit in [0, tmax] (returns false on miss).  Tie rule: smaller t, then
+// smaller global triangle id.
+APD bool trace_closest(const DevScene& s, float3 o, float3 d, float tmax, Hit& hit) {
+  RayPre r = ray_pre(o, d);
+  hit.t = tmax;
+  hit.u = 0.0f;
+  hit.v = 0.0f;
+  hit.tri = kNoHit;
+  uint2 stack[kTraversalStack];
+  int sp = 0;
+  uint32_t node = 0;
+  bool have = true;
+  while (true) {
+    if (!have) {
+      if (sp == 0) break;
+      uint2 e = stack[--sp];
+      if (__uint_as_float(e.y) > hit.t * (1.0f + 4.8e-7f)) continue;
+      node = e.x;
+    }
+    have = false;
+    const uint4* np = s.nodes + 5 * (size_t)node;
+    uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
+          w4 = __ldg(np + 4);
+    float tnear[8];
+    uint32_t mask = node_children<true>(w0, w2, w3, w4, r, 0.0f, hit.t, tnear);
+    // leaves first (their hits shrink hit.t before the inner children are ordered)
+    uint32_t todo = mask;
+    while (todo) {
+      int i = __ffs(todo) - 1;
+      todo &= todo - 1;
+      uint32_t meta = meta_of(w1, i);
+      if ((meta & 0xe0u) == 0) continue;
+      uint32_t first = w1.y + (meta & 0x1fu);
+      uint32_t cnt = __popc(meta >> 5);
+      for (uint32_t k = 0; k < cnt; ++k) {
+        const float4* tp = s.tris + 3 * (size_t)(first + k);
+        float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float t, u, v;
+        if (intersect_tri(r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), 0.0f, hit.t, t, u, v)) {
+          uint32_t gid = __float_as_uint(a.w);
+          if (t < hit.t || gid < hit.tri) {  // t <= hit.t here: strict or tie
+            hit.t = t;
+            hit.u = u;
+            hit.v = v;
+            hit.tri = gid;
+          }
+        }
+      }
+    }
+    // inner children: continue with the nearest, push the rest
+    float best_t = 3.4e38f;
+    int best_i = -1;
+    todo = mask;
+    while (todo) {
+      int i = __ffs(todo) - 1;
+      todo &= todo - 1;
+      uint32_t meta = meta_of(w1, i);
+      if ((meta & 0xf0u) != 0x10u) continue;
+      if (tnear[i] > hit.t * (1.0f + 4.8e-7f)) continue;
+      if (tnear[i] < best_t) {
+        if (best_i >= 0 && sp < kTraversalStack)
+          stack[sp++] = make_uint2(w1.x + (meta_of(w1, best_i) & 7u), __float_as_uint(best_t));
+        best_t = tnear[i];
+        best_i = i;
+      } else if (sp < kTraversalStack) {
+        stack[sp++] = make_uint2(w1.x + (meta & 7u), __float_as_uint(tnear[i]));
+      }
+    }
+    if (best_i >= 0) {
+      node = w1.x + (meta_of(w1, best_i) & 7u);
+      have = true;
+    }
+  }
+  return hit.tri != kNoHit;
+}
+
+// Any hit in [0, tmax] (shadow rays: terminate on first hit).  Same stack
+// discipline as trace_closest (continue with one inner child, push the rest),
+// so the build-time bound on stack depth (BvhStats::max_stack) covers both.
+APD bool trace_any(const DevScene& s, float3 o, float3 d, float tmax) {
+  RayPre r = ray_pre(o, d);
+  uint32_t stack[kTraversalStack];
+  int sp = 0;
+  uint32_t node = 0;
+  bool have = true;
+  while (true) {
+    if (!have) {
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+    have = false;
+    const uint4* np = s.nodes + 5 * (size_t)node;
+    uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
+          w4 = __ldg(np + 4);
+    float tnear[8];
+    uint32_t mask = node_children<false>(w0, w2, w3, w4, r, 0.0f, tmax, tnear);
+    uint32_t todo = mask;
+    while (todo) {
+      int i = __ffs(todo) - 1;
+      todo &= todo - 1;
+      uint32_t meta = meta_of(w1, i);
+      if ((meta & 0xe0u) != 0) {
+        uint32_t first = w1.y + (meta & 0x1fu);
+        uint32_t cnt = __popc(meta >> 5);
+        for (uint32_t k = 0; k < cnt; ++k) {
+          const float4* tp = s.tris + 3 * (size_t)(first + k);
+          float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+          float t, u, v;
+          if (intersect_tri(r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), 0.0f, tmax, t, u, v))
+            return true;
+        }
+      } else if (!have) {
+        node = w1.x + (meta & 7u);
+        have = true;
+      } else if (sp < kTraversalStack) {
+        stack[sp++] = w1.x + (meta & 7u);
+      }
+    }
+  }
+  return false;
+}
+
+}  // namespace ap

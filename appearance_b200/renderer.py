@@ -1,0 +1,161 @@
+"""Host-side mirror of the reference's renderer interface.
+
+`PathTracer` follows PathTracerGpu (crates/appearance-path-tracer-gpu/src/
+lib.rs:247-615) and the NodeRenderer trait it is used through
+(crates/appearance-render-loop/src/node.rs:14-25):
+
+    handle_visible_world_action(ty, bytes)     NodeRenderer::visible_world_action
+    render(resolution, start_row, end_row, cb) NodeRenderer::render
+
+plus the calls a synthetic-scene host needs (upload_scene, set_camera).  All
+work runs in libappearance_cuda.so on the GPU; errors raise RendererError with
+the library's message.
+"""
+from __future__ import annotations
+
+import ctypes
+import struct
+
+import numpy as np
+
+from . import _native, presets
+from .scenes import Scene, camera_matrices
+
+
+class RendererError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def config_struct(cfg: dict | None) -> _native.FrameConfig:
+    c = _native.FrameConfig()
+    _native.load().ap_frame_config_default(ctypes.byref(c))
+    for k, v in (cfg or {}).items():
+        setattr(c, k, v)
+    return c
+
+
+class PathTracer:
+    """One renderer instance (one CUDA stream, persistent temporal state)."""
+
+    def __init__(self, config: dict | None = None, device: int = 0):
+        self._lib = _native.load()
+        err = ctypes.c_int(0)
+        self._cfg = config_struct(config if config is not None else presets.FAITHFUL)
+        self._h = self._lib.ap_create(ctypes.byref(self._cfg), device, ctypes.byref(err))
+        if not self._h:
+            raise RendererError(err.value, "ap_create failed (no CUDA device?)")
+        self._scene_keep = None
+        self._eye = None
+        self.last_stats = _native.FrameStats()
+
+    # -- error plumbing
+    def _check(self, rc: int):
+        if rc != _native.AP_OK:
+            raise RendererError(rc, self._lib.ap_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ap_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- configuration
+    def set_config(self, config: dict):
+        self._cfg = config_struct(config)
+        self._check(self._lib.ap_set_config(self._h, ctypes.byref(self._cfg)))
+
+    # -- world
+    def handle_visible_world_action(self, ty: int, data: bytes):
+        """VisibleWorldActionType::from_ty_and_bytes wire format (visible_world_action.rs:87-96)."""
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        self._check(self._lib.ap_world_action(self._h, ty, buf, len(data)))
+
+    @staticmethod
+    def camera_update_bytes(transform_col_major, fov_deg: float, near: float, far: float) -> bytes:
+        """Packs CameraUpdateData {Mat4, fov, near, far, pad} (visible_world_action.rs:9-15)."""
+        m = np.asarray(transform_col_major, np.float32).reshape(16)
+        return m.tobytes() + struct.pack("<fffI", fov_deg, near, far, 0)
+
+    def upload_scene(self, scene: Scene):
+        keep = dict(pos=np.ascontiguousarray(scene.positions, np.float32),
+                    nrm=np.ascontiguousarray(scene.normals, np.float32),
+                    idx=np.ascontiguousarray(scene.indices, np.uint32),
+                    tm=np.ascontiguousarray(scene.tri_material, np.uint32),
+                    mesh=np.ascontiguousarray(scene.meshes, np.uint32),
+                    mat=np.ascontiguousarray(scene.materials, np.float32),
+                    env=None if scene.env is None else np.ascontiguousarray(scene.env, np.float32))
+        d = _native.SceneDesc()
+        d.positions, d.normals = _ptr(keep["pos"]), _ptr(keep["nrm"])
+        d.num_vertices = keep["pos"].shape[0]
+        d.indices, d.tri_material = _ptr(keep["idx"]), _ptr(keep["tm"])
+        d.num_tris = keep["idx"].shape[0]
+        d.meshes, d.num_meshes = _ptr(keep["mesh"]), keep["mesh"].shape[0]
+        d.materials, d.num_materials = _ptr(keep["mat"]), keep["mat"].shape[0]
+        if keep["env"] is not None:
+            d.env, d.env_h, d.env_w = _ptr(keep["env"]), keep["env"].shape[0], keep["env"].shape[1]
+        for i in range(8):
+            d.sun[i] = float(scene.sun[i])
+        self._check(self._lib.ap_scene_upload(self._h, ctypes.byref(d)))
+
+    def set_camera_matrices(self, mats: np.ndarray):
+        m = np.ascontiguousarray(mats, np.float32).reshape(64)
+        self._check(self._lib.ap_set_camera_matrices(self._h, _ptr(m)))
+
+    def set_camera(self, eye, target, fov, near, far, width, height, prev_view_proj=None):
+        """Look-at camera; returns this frame's view_proj (float64) for the next frame's motion."""
+        mats, vp = camera_matrices(eye, target, fov, near, far, width, height, prev_view_proj)
+        self.set_camera_matrices(mats)
+        return vp
+
+    # -- rendering
+    def render(self, resolution, start_row: int = 0, end_row: int | None = None, result_callback=None) -> np.ndarray:
+        """NodeRenderer::render: linear HDR RGB f32 rows [start_row, end_row) of a
+        resolution=(width, height) frame.  The callback, when given, receives the
+        rows as bytes (the reference passes &[u8]) and the array is returned."""
+        w, h = int(resolution[0]), int(resolution[1])
+        end_row = h if end_row is None else end_row
+        out = np.empty((end_row - start_row, w, 3), np.float32)
+        self._check(self._lib.ap_render_hdr(self._h, w, h, start_row, end_row, _ptr(out), out.nbytes,
+                                            ctypes.byref(self.last_stats)))
+        if result_callback is not None:
+            result_callback(out.tobytes())
+        return out
+
+    def render_device(self, width: int, height: int) -> float:
+        """Renders into the device framebuffer only; returns the frame's GPU ms."""
+        self._check(self._lib.ap_render_device(self._h, width, height, ctypes.byref(self.last_stats)))
+        return self.last_stats.gpu_ms
+
+    def device_framebuffer_ptr(self) -> int:
+        return int(self._lib.ap_device_framebuffer(self._h) or 0)
+
+    def trace_rays(self, origins: np.ndarray, dirs: np.ndarray, tmax, any_hit: bool = False) -> np.ndarray:
+        """Closest (t, u, v, tri) or any-hit queries; returns (n, 4) uint32 words."""
+        n = origins.shape[0]
+        o4 = np.zeros((n, 4), np.float32)
+        o4[:, :3] = origins
+        o4[:, 3] = tmax
+        d4 = np.zeros((n, 4), np.float32)
+        d4[:, :3] = dirs
+        out = np.zeros((n, 4), np.uint32)
+        self._check(self._lib.ap_trace_rays(self._h, _ptr(o4), _ptr(d4), n, 1 if any_hit else 0, _ptr(out)))
+        return out
+
+    def read_buffer(self, which: int, words: int, pixels: int) -> np.ndarray:
+        out = np.zeros((pixels, words), np.uint32)
+        self._check(self._lib.ap_read_buffer(self._h, which, _ptr(out), out.nbytes))
+        return out
+
+    def bvh_stats(self) -> dict:
+        out = np.zeros(8, np.uint32)
+        self._check(self._lib.ap_bvh_stats(self._h, _ptr(out)))
+        return dict(nodes=int(out[0]), tris=int(out[1]), max_depth=int(out[2]), max_stack=int(out[3]),
+                    build_ms=float(out[4:6].view(np.float64)[0]))

@@ -1,0 +1,177 @@
+/* C ABI of the B200 path-tracing frame: the boundary a host (Rust over FFI,
+ * C++, or Python ctypes) binds in place of the reference's GPU renderer.
+ *
+ * Reference interfaces replaced:
+ *   NodeRenderer::visible_world_action / NodeRenderer::render
+ *       crates/appearance-render-loop/src/node.rs:14-25
+ *   DistributedRenderer (its NodeRenderer impl)
+ *       crates/appearance-distributed-renderer/src/lib.rs:60-82
+ *   PathTracerGpu::new / handle_visible_world_action / render
+ *       crates/appearance-path-tracer-gpu/src/lib.rs:260-302, 314-615
+ *   PathTracerGpuConfig (+ the pass literals of render)
+ *       crates/appearance-path-tracer-gpu/src/lib.rs:220-245, 413-545
+ *   VisibleWorldActionType wire format
+ *       crates/appearance-world/src/visible_world_action.rs:9-125
+ *
+ * Ownership: the library owns all device memory and the per-handle temporal
+ * state (reservoirs, G-buffers, SVGF/TAA history); the caller owns every host
+ * buffer it passes, and no pointer escapes a call.  A handle is used by one
+ * host thread at a time.  Every entry point returns an AP_* status; none
+ * aborts.  ap_last_error() describes the last failure of a handle.
+ */
+#ifndef APPEARANCE_CUDA_H
+#define APPEARANCE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  AP_OK = 0,
+  AP_E_INVALID = 1,     /* bad argument, size or state */
+  AP_E_OOM = 2,         /* device allocation failed */
+  AP_E_CUDA = 3,        /* CUDA runtime error (message in ap_last_error) */
+  AP_E_TIMEOUT = 4,     /* a bounded device wait ran out */
+  AP_E_UNSUPPORTED = 5, /* valid request this library does not implement */
+  AP_E_NO_SCENE = 6     /* render before any geometry was uploaded */
+};
+
+/* PathTracerGpuConfig plus the literals the reference hard-codes in render()
+ * and in its shaders.  ap_frame_config_default() gives the reference values. */
+typedef struct ap_frame_config {
+  uint32_t max_bounces;         /* 2   lib.rs:235 */
+  uint32_t sample_count;        /* 1   lib.rs:236 */
+  uint32_t restir_di;           /* 1   lib.rs:238 */
+  uint32_t restir_gi;           /* 1   lib.rs:239 */
+  uint32_t svgf;                /* 0   lib.rs:240 */
+  uint32_t firefly_filter;      /* 1   lib.rs:241 */
+  uint32_t taa;                 /* 0   lib.rs:242 */
+  uint32_t di_area_samples;     /* 4   helpers/nee.wgsl:125 */
+  uint32_t di_bsdf_samples;     /* 1   helpers/nee.wgsl:126 */
+  float di_temporal_m_factor;   /* 20  restir_di_temporal.wgsl:159 */
+  uint32_t di_spatial_passes;   /* 1   lib.rs:417 */
+  uint32_t di_spatial_samples;  /* 3   restir_di_spatial.wgsl:15 */
+  uint32_t di_unbiased;         /* 1   lib.rs:419 */
+  float gi_temporal_m_cap;      /* 30  restir_gi_temporal.wgsl:100 */
+  uint32_t gi_spatial_passes;   /* 0   lib.rs:441 */
+  uint32_t gi_spatial_samples;  /* 5   restir_gi_spatial.wgsl:16 */
+  uint32_t gi_unbiased;         /* 1   lib.rs:443 */
+  uint32_t svgf_max_history;    /* 24  lib.rs:522 */
+  uint32_t svgf_atrous_passes;  /* 5   lib.rs:523 */
+  float taa_history_influence;  /* 0.8 lib.rs:538 */
+} ap_frame_config;
+
+/* MaterialDescriptor (shared/material/material_pool.wgsl:6-41) without the
+ * texture slots; 26 floats. */
+typedef struct ap_material {
+  float color[3];
+  float metallic, roughness;
+  float emission[3];
+  float transmission, eta, subsurface;
+  float absorption[3];
+  float specular;
+  float specular_tint[3];
+  float anisotropic, sheen;
+  float sheen_tint[3];
+  float clearcoat, clearcoat_roughness, alpha_cutoff;
+} ap_material;
+
+/* One mesh of the scene (a VertexPoolSlice, shared/vertex_pool.wgsl:3-12). */
+typedef struct ap_mesh {
+  uint32_t first_vertex, num_vertices; /* into positions/normals */
+  uint32_t first_index, num_indices;   /* into indices (3 per triangle) */
+  uint32_t material_idx;               /* first material of the mesh */
+  uint32_t emissive;                   /* 1: mesh takes part in light sampling */
+} ap_mesh;
+
+/* A whole scene: world-space vertex pool, per-triangle material indices
+ * relative to the mesh's material_idx, materials, an optional equirect
+ * environment (RGB f32, env_w x env_h) and the analytic sun (SunInfo,
+ * scene_resources/sky.rs:11-22: direction xyz, size, color xyz, intensity). */
+typedef struct ap_scene_desc {
+  const float* positions;        /* 3 floats per vertex */
+  const float* normals;          /* 3 floats per vertex, unit length */
+  uint32_t num_vertices;
+  const uint32_t* indices;       /* 3 per triangle, relative to the mesh's first_vertex */
+  const uint32_t* tri_material;  /* 1 per triangle */
+  uint32_t num_tris;
+  const ap_mesh* meshes;
+  uint32_t num_meshes;
+  const ap_material* materials;
+  uint32_t num_materials;
+  const float* env;              /* may be NULL (black sky) */
+  uint32_t env_w, env_h;
+  float sun[8];
+} ap_scene_desc;
+
+typedef struct ap_frame_stats {
+  double gpu_ms;            /* device time of the frame (CUDA events) */
+  uint64_t extension_rays;  /* closest-hit rays of the path-extension stage */
+  uint32_t width, height;
+  uint32_t frame_idx;
+} ap_frame_stats;
+
+/* Fills the reference defaults (PathTracerGpuConfig::default + pass literals). */
+void ap_frame_config_default(ap_frame_config* cfg);
+
+/* PathTracerGpu::new (lib.rs:260-281).  Returns NULL and sets *err on failure. */
+void* ap_create(const ap_frame_config* cfg, int device, int* err);
+void ap_destroy(void* handle);
+const char* ap_last_error(const void* handle);
+/* Replaces the frame configuration and restarts the frame sequence (the
+ * temporal state is dropped, the next frame is frame 0). */
+int ap_set_config(void* handle, const ap_frame_config* cfg);
+
+/* NodeRenderer::visible_world_action (node.rs:16): `ty` and `bytes` exactly as
+ * VisibleWorldActionType::from_ty_and_bytes (visible_world_action.rs:87-96).
+ * 0 CameraUpdate {Mat4 transform, fov deg, near, far, pad} is applied;
+ * 4 Clear drops the scene; 1 SpawnModel / 2 TransformModel / 3 DestroyModel
+ * name glTF assets and entity uuids, which this library does not load:
+ * they return AP_E_UNSUPPORTED (use ap_scene_upload). */
+int ap_world_action(void* handle, uint32_t ty, const void* bytes, size_t len);
+
+/* Uploads (replaces) the scene and builds its wide BVH. */
+int ap_scene_upload(void* handle, const ap_scene_desc* desc);
+
+/* Explicit camera: inv_view, inv_proj, view_proj, prev_view_proj as 4
+ * column-major float[16], used for the next render (overrides CameraUpdate). */
+int ap_set_camera_matrices(void* handle, const float* mats16x4);
+
+/* NodeRenderer::render (node.rs:18-24) / PathTracerGpu::render: renders one
+ * frame of w x h pixels and writes linear HDR RGB f32 (radiance / sample
+ * count, before the reference's tonemap, resolve.wgsl:48-50) for rows
+ * [row_start, row_end) to `out_rgb` (3 floats per pixel, row-major).
+ * Synchronous: returns when `out_rgb` holds the result. */
+int ap_render_hdr(void* handle, uint32_t w, uint32_t h, uint32_t row_start, uint32_t row_end, float* out_rgb,
+                  size_t out_bytes, ap_frame_stats* stats);
+
+/* Renders one frame into the device-resident framebuffer only (no copy to
+ * the host); ap_device_framebuffer() returns its device address. */
+int ap_render_device(void* handle, uint32_t w, uint32_t h, ap_frame_stats* stats);
+const float* ap_device_framebuffer(const void* handle);
+
+/* Closest-hit (any_hit = 0) or any-hit (1) queries against the uploaded BVH.
+ * origins_tmax: n x {ox, oy, oz, tmax}; dirs: n x {dx, dy, dz, unused};
+ * out: n x {t, u, v, triangle id} (as raw 32-bit words; any-hit: {hit, 0,0,0}).
+ * Host buffers; tmin is 0. */
+int ap_trace_rays(void* handle, const float* origins_tmax, const float* dirs, uint32_t n, int any_hit,
+                  uint32_t* out4);
+
+/* Copies a per-pixel state buffer of the last frame to the host, for
+ * stage-by-stage comparisons: 0 radiance (1 word), 1 payload (4), 2 current
+ * G-buffer (8), 3 DI reservoirs (8), 4 GI reservoirs (8), 5 light-sample
+ * context (4), 7 rays (4). */
+int ap_read_buffer(void* handle, uint32_t which, uint32_t* out, size_t out_bytes);
+
+/* BVH statistics of the uploaded scene: nodes, triangles, max depth, max
+ * traversal stack, build ms (as double bits in out[4..5]). */
+int ap_bvh_stats(void* handle, uint32_t* out8);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APPEARANCE_CUDA_H */

@@ -1,0 +1,146 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py load
+this module; the shipped library never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+class FrameConfig(ctypes.Structure):
+    """Same field order as ap_frame_config (include/appearance_cuda.h) plus threads."""
+    _fields_ = [(n, t) for n, t in [
+        ("max_bounces", ctypes.c_uint32), ("sample_count", ctypes.c_uint32),
+        ("restir_di", ctypes.c_uint32), ("restir_gi", ctypes.c_uint32), ("svgf", ctypes.c_uint32),
+        ("firefly_filter", ctypes.c_uint32), ("taa", ctypes.c_uint32),
+        ("di_area_samples", ctypes.c_uint32), ("di_bsdf_samples", ctypes.c_uint32),
+        ("di_temporal_m_factor", ctypes.c_float),
+        ("di_spatial_passes", ctypes.c_uint32), ("di_spatial_samples", ctypes.c_uint32),
+        ("di_unbiased", ctypes.c_uint32),
+        ("gi_temporal_m_cap", ctypes.c_float),
+        ("gi_spatial_passes", ctypes.c_uint32), ("gi_spatial_samples", ctypes.c_uint32),
+        ("gi_unbiased", ctypes.c_uint32),
+        ("svgf_max_history", ctypes.c_uint32), ("svgf_atrous_passes", ctypes.c_uint32),
+        ("taa_history_influence", ctypes.c_float),
+        ("threads", ctypes.c_uint32)]]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        P, U, F = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_float
+        L.orc_scene_new.restype = P
+        L.orc_scene_new.argtypes = [P, P, U, P, P, U, P, U, P, U, P, U, U, P]
+        L.orc_scene_free.argtypes = [P]
+        L.orc_closest.argtypes = [P, P, P, U, F, U, P, P]
+        L.orc_any.argtypes = [P, P, P, P, U, U, P]
+        L.orc_frame_new.restype = P
+        L.orc_frame_new.argtypes = [P, U, U, P]
+        L.orc_frame_free.argtypes = [P]
+        L.orc_frame_render.argtypes = [P, P, P]
+        L.orc_frame_buffer.argtypes = [P, U, P]
+        L.orc_frame_rays_cast.restype = ctypes.c_uint64
+        L.orc_frame_rays_cast.argtypes = [P]
+        L.orc_rgb9e5_pack.restype = U
+        L.orc_rgb9e5_pack.argtypes = [P]
+        L.orc_rgb9e5_unpack.argtypes = [U, P]
+        L.orc_oct30_pack.restype = U
+        L.orc_oct30_pack.argtypes = [P]
+        L.orc_oct30_unpack.argtypes = [U, P]
+        for n in ("orc_pcg_hash", "orc_xor_shift"):
+            getattr(L, n).restype = U
+            getattr(L, n).argtypes = [U]
+        L.orc_hash_combine.restype = U
+        L.orc_hash_combine.argtypes = [U, U]
+        L.orc_disney.argtypes = [P] * 7
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class OracleScene:
+    def __init__(self, scene):
+        L = lib()
+        self._keep = dict(
+            pos=np.ascontiguousarray(scene.positions, np.float32),
+            nrm=np.ascontiguousarray(scene.normals, np.float32),
+            idx=np.ascontiguousarray(scene.indices, np.uint32),
+            tm=np.ascontiguousarray(scene.tri_material, np.uint32),
+            mesh=np.ascontiguousarray(scene.meshes, np.uint32),
+            mat=np.ascontiguousarray(scene.materials, np.float32),
+            env=None if scene.env is None else np.ascontiguousarray(scene.env, np.float32),
+            sun=np.ascontiguousarray(scene.sun, np.float32))
+        k = self._keep
+        env_h, env_w = (0, 0) if k["env"] is None else k["env"].shape[:2]
+        self.ptr = L.orc_scene_new(_p(k["pos"]), _p(k["nrm"]), k["pos"].shape[0], _p(k["idx"]), _p(k["tm"]),
+                                   k["idx"].shape[0], _p(k["mesh"]), k["mesh"].shape[0], _p(k["mat"]),
+                                   k["mat"].shape[0], _p(k["env"]), env_w, env_h, _p(k["sun"]))
+
+    def closest(self, origins, dirs, tmax=1000.0, threads=0):
+        n = origins.shape[0]
+        out = np.zeros((n, 4), np.float32)
+        counts = np.zeros(2, np.uint64)
+        lib().orc_closest(self.ptr, _p(np.ascontiguousarray(origins, np.float32)),
+                          _p(np.ascontiguousarray(dirs, np.float32)), n, tmax, threads or os.cpu_count(),
+                          _p(out), _p(counts))
+        return out, counts
+
+    def any(self, origins, dirs, tmax, threads=0):
+        n = origins.shape[0]
+        out = np.zeros(n, np.uint8)
+        lib().orc_any(self.ptr, _p(np.ascontiguousarray(origins, np.float32)),
+                      _p(np.ascontiguousarray(dirs, np.float32)), _p(np.ascontiguousarray(tmax, np.float32)),
+                      n, threads or os.cpu_count(), _p(out))
+        return out
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().orc_scene_free(self.ptr)
+            self.ptr = None
+
+
+class OracleFrame:
+    """Persistent frame state (reservoir, G-buffer and SVGF history) of one view."""
+
+    def __init__(self, oscene: OracleScene, width: int, height: int, cfg: dict, threads: int = 0):
+        c = FrameConfig(**{k: v for k, v in cfg.items()}, threads=threads or os.cpu_count())
+        self.scene = oscene
+        self.w, self.h = width, height
+        self.ptr = lib().orc_frame_new(oscene.ptr, width, height, ctypes.byref(c))
+
+    def render(self, mats: np.ndarray) -> np.ndarray:
+        out = np.zeros((self.h, self.w, 3), np.float32)
+        lib().orc_frame_render(self.ptr, _p(np.ascontiguousarray(mats, np.float32)), _p(out))
+        return out
+
+    def buffer(self, which: int, words: int) -> np.ndarray:
+        out = np.zeros((self.h * self.w, words), np.uint32)
+        lib().orc_frame_buffer(self.ptr, which, _p(out))
+        return out
+
+    def rays_cast(self) -> int:
+        return int(lib().orc_frame_rays_cast(self.ptr))
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().orc_frame_free(self.ptr)
+            self.ptr = None
