@@ -71,6 +71,7 @@ struct Handle {
   void* trace_mem = nullptr;
   size_t trace_bytes = 0;
   uint64_t ext_rays = 0;
+  FrameProfiler prof;
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -192,7 +193,7 @@ int ensure_frame(Handle* h, uint32_t w, uint32_t hgt) {
   return AP_OK;
 }
 
-int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats) {
+int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats, FrameProfiler* prof = nullptr) {
   if (w == 0 || hgt == 0 || (uint64_t)w * hgt > (1ull << 28)) return fail(h, AP_E_INVALID, "bad resolution");
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
   const FrameConfig& c = h->cfg;
@@ -204,8 +205,10 @@ int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats) {
   if (rc) return rc;
   compute_mats(h, w, hgt);
   cudaEventRecord(h->ev0, h->stream);
-  encode_frame(h->scene.view, h->fb, h->cfg, h->mats, w, hgt, h->frame_idx, h->num_sms, h->stream);
+  int launches = encode_frame(h->scene.view, h->fb, h->cfg, h->mats, w, hgt, h->frame_idx, h->num_sms, h->stream, prof);
   cudaEventRecord(h->ev1, h->stream);
+  uint32_t rays = 0;
+  cudaMemcpyAsync(&rays, h->fb.counters + 3, 4, cudaMemcpyDeviceToHost, h->stream);
   rc = check_cuda(h, cudaGetLastError(), "frame launch");
   if (rc) return rc;
   rc = check_cuda(h, cudaEventSynchronize(h->ev1), "frame");
@@ -214,7 +217,8 @@ int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats) {
   cudaEventElapsedTime(&ms, h->ev0, h->ev1);
   if (stats) {
     stats->gpu_ms = ms;
-    stats->extension_rays = 0;
+    stats->extension_rays = rays;
+    stats->kernel_launches = (uint32_t)launches;
     stats->width = w;
     stats->height = hgt;
     stats->frame_idx = h->frame_idx;
@@ -282,6 +286,8 @@ void ap_destroy(void* hp) {
   h->scene.release();
   if (h->frame_mem) cudaFree(h->frame_mem);
   if (h->trace_mem) cudaFree(h->trace_mem);
+  if (h->prof.created)
+    for (int i = 0; i <= FrameProfiler::kMax; ++i) cudaEventDestroy(h->prof.ev[i]);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -565,6 +571,37 @@ int ap_read_buffer(void* hp, uint32_t which, uint32_t* out, size_t out_bytes) {
     col += pw;
   }
   return check_cuda(h, cudaStreamSynchronize(h->stream), "read buffer");
+}
+
+int ap_profile_frame(void* hp, uint32_t w, uint32_t hgt, double* kind_ms, uint32_t* kind_count, const char** names,
+                     uint32_t max_kinds, uint32_t* num_kinds, ap_frame_stats* stats) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !kind_ms || !kind_count || !num_kinds) return AP_E_INVALID;
+  cudaSetDevice(h->device);
+  if (!h->prof.created) {
+    for (int i = 0; i <= FrameProfiler::kMax; ++i)
+      if (cudaEventCreate(&h->prof.ev[i]) != cudaSuccess) return fail(h, AP_E_CUDA, "profiler events");
+    h->prof.created = true;
+  }
+  int rc = render_common(h, w, hgt, stats, &h->prof);
+  if (rc) return rc;
+  uint32_t nk = std::min<uint32_t>(max_kinds, (uint32_t)K_NUM_KINDS);
+  for (uint32_t k = 0; k < nk; ++k) {
+    kind_ms[k] = 0.0;
+    kind_count[k] = 0;
+    if (names) names[k] = kernel_kind_name((int)k);
+  }
+  for (int i = 0; i < h->prof.n; ++i) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, h->prof.ev[i], h->prof.ev[i + 1]);
+    int k = h->prof.kind[i];
+    if (k >= 0 && (uint32_t)k < nk) {
+      kind_ms[k] += ms;
+      kind_count[k] += 1;
+    }
+  }
+  *num_kinds = nk;
+  return AP_OK;
 }
 
 int ap_bvh_stats(void* hp, uint32_t* out8) {

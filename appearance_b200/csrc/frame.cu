@@ -73,80 +73,6 @@ APD bool shadow_ray(const DevScene& s, float3 origin, float3 dir, float d, float
   return !trace_any(s, origin + n * 1e-4f, dir, d - 1e-4f * 2.0f);
 }
 
-// ---- Nee::sample_ris (helpers/nee.wgsl:122-237) ----
-APD DiRes sample_ris(const DevScene& s, const FrameConfig& cfg, float3 hit, float3 wo, const Frame& fr,
-                     const Bsdf& b, float t, bool back_face, uint32_t& rng) {
-  const uint32_t NA = cfg.di_area_samples, NB = cfg.di_bsdf_samples;
-  DiRes res;
-  res.M = res.W = res.wsum = res.phat = 0.0f;
-  res.s = ls_empty();
-  LightEval sel{f3s(0.0f), f3s(0.0f)};
-  uint32_t n_iter = NA > NB ? NA : NB;
-  for (uint32_t i = 0; i < n_iter; ++i) {
-    float area_pdf = 0.0f, area_phat = 0.0f;
-    LightSample area_s{make_float2(0.0f, 0.0f), 0u, 0u};
-    LightEval area_e{f3s(0.0f), f3s(0.0f)};
-    if (i < NA) {
-      float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng), r3 = rnd(rng), r4 = rnd(rng);
-      area_s = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), &area_pdf);
-      area_e = load_eval(s, area_s, hit);
-      float3 wi = normalize(area_e.point - hit);
-      float wdn = dot(wi, fr.n);
-      if (wdn > 0.0f && area_pdf > 0.0f) {
-        float sp = 0.0f;
-        float3 refl = disney_eval(b, fr, wo, wi, &sp);
-        if (sp > 0.0f) area_phat = luma(refl * wdn * area_e.emission);
-      }
-    }
-    float bsdf_pdf = 0.0f, bsdf_phat = 0.0f;
-    LightSample bsdf_s = ls_empty();
-    LightEval bsdf_e{f3s(0.0f), f3s(0.0f)};
-    if (i < NB) {
-      float3 wi = f3s(0.0f);
-      float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng);
-      float3 refl = disney_sample(b, fr, wo, t, back_face, r0, r1, r2, &wi, &bsdf_pdf);
-      float wdn = dm::fabs_(dot(wi, fr.n));
-      float3 contribution = wdn * refl;
-      if (dot(contribution, contribution) > 0.0f) {
-        Hit h;
-        if (trace_closest(s, hit + fr.n * 1e-4f, wi, 1000.0f, h)) {
-          const InstanceDev in = s.instances[s.tri_instance[h.tri]];
-          if (in.emissive_idx != kU32Max)
-            bsdf_s = LightSample{make_float2(h.u, h.v), in.emissive_idx, h.tri - in.first_global_tri};
-        } else {
-          bsdf_s = LightSample{inverse_direction_to_sun(s.sun, wi), kU32Max - 1, 0u};
-        }
-        if (!ls_is_empty(bsdf_s)) {
-          bsdf_e = load_eval(s, bsdf_s, hit);
-          bsdf_phat = luma(contribution * bsdf_e.emission);
-        }
-      }
-    }
-    if (i < NA) {
-      float aw = 0.0f;
-      if (area_pdf > 0.0f) {
-        float mis = area_pdf / ((float)NA * area_pdf + (float)NB * bsdf_pdf);
-        aw = mis * area_phat * (1.0f / dm::fmax(area_pdf, 1e-8f));
-      }
-      if (di_update(res, aw, rng, area_s, area_phat)) sel = area_e;
-    }
-    if (i < NB) {
-      float bw = 0.0f;
-      if (bsdf_pdf > 0.0f) {
-        float mis = bsdf_pdf / ((float)NB * bsdf_pdf + (float)NA * area_pdf);
-        bw = mis * bsdf_phat * (1.0f / dm::fmax(bsdf_pdf, 1e-8f));
-      }
-      if (di_update(res, bw, rng, bsdf_s, bsdf_phat)) sel = bsdf_e;
-    }
-  }
-  if (res.phat > 1e-6f) {
-    float3 dir = normalize(sel.point - hit);
-    float d = dist(sel.point, hit);
-    if (shadow_ray(s, hit, dir, d, fr.n)) res.W = (1.0f / res.phat) * res.wsum;
-  }
-  return res;
-}
-
 // ---- InlinePathTracer::trace with the approx() config (inline_path_tracer.wgsl:51-256) ----
 APD float3 inline_trace(const DevScene& s, float3 origin, float3 direction, float3 throughput, float3* first_hit,
                         uint32_t& rng) {
@@ -177,31 +103,6 @@ APD float3 inline_trace(const DevScene& s, float3 origin, float3 direction, floa
   }
   *first_hit = origin + direction * 1000.0f;
   return acc + throughput * sky_radiance(s, direction, true);
-}
-
-// ---- InlinePathTracer::sample_ris (inline_path_tracer.wgsl:258-296) ----
-APD GiRes gi_sample_ris(const DevScene& s, float3 hit, float3 wo, const Frame& fr, const Bsdf& b, float3 T,
-                        float t, bool back_face, uint32_t& rng) {
-  GiRes res;
-  res.M = res.W = res.wsum = res.phat = 0.0f;
-  res.point = f3s(0.0f);
-  res.phat_rng = 0u;
-  float3 wi = f3s(0.0f);
-  float pdf = 0.0f;
-  float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng);
-  float3 refl = disney_sample(b, fr, wo, t, back_face, r0, r1, r2, &wi, &pdf);
-  if (pdf > 1e-6f) {
-    float cos_in = dm::fabs_(dot(wi, fr.n));
-    float3 local = cos_in * refl;
-    float3 tr = T * local;
-    uint32_t phat_rng = rng;
-    float3 point = f3s(0.0f);
-    float3 contribution = inline_trace(s, hit, wi, tr, &point, rng);
-    float phat = luma(contribution);
-    gi_update(res, phat / pdf, rng, point, phat, phat_rng);
-  }
-  if (res.phat > 0.0f && res.M * res.wsum > 0.0f) res.W = (1.0f / res.phat) * (1.0f / res.M * res.wsum);
-  return res;
 }
 
 APD Frame ctx_frame(const uint4 c) {
@@ -289,6 +190,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(DevScene s, FrameBuffers fb, 
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
   const uint32_t* q = fb.queue[c.qin];
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fb.counters[3], count);  // rays traced this frame
   while (true) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(&fb.counters[2], 32u);
@@ -315,13 +217,91 @@ APD float2 velocity_of(const Mats& m, float3 p) {
   return make_float2(cx - px, cy - py);
 }
 
-// trace.wgsl:62-262 after the closest hit (taken from fb.hits).
-__global__ void __launch_bounds__(kBlock) k_shade(DevScene s, FrameBuffers fb, Consts c, Mats mats) {
-  const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
-  const uint32_t* q = fb.queue[c.qin];
+// ---- secondary-ray queues -------------------------------------------------
+
+// Appends one ray per requesting lane with one atomic per warp (ballot + popc).
+APD void push_ray(const FrameBuffers& fb, int q, bool want, float3 o, float tmax, float3 d, uint32_t owner) {
+  const unsigned active = __activemask();
+  const unsigned b = __ballot_sync(active, want);
+  if (!want) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(b) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(&fb.counters[kCounterQueueSize + q], (uint32_t)__popc(b));
+  base = __shfl_sync(b, base, leader);
+  uint32_t slot = base + __popc(b & ((1u << lane) - 1u));
+  fb.rq_o[q][slot] = make_float4(o.x, o.y, o.z, tmax);
+  fb.rq_d[q][slot] = make_float4(d.x, d.y, d.z, __uint_as_float(owner));
+}
+
+// Persistent traversal of one ray queue; each warp takes 32 rays per atomic.
+template <bool kAny>
+__global__ void __launch_bounds__(kBlock) k_trace_queue(DevScene s, FrameBuffers fb, int q, uint4* hits,
+                                                        uint8_t* vis) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t count = fb.counters[kCounterQueueSize + q];
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fb.counters[3], count);
+  const float4* qo = fb.rq_o[q];
+  const float4* qd = fb.rq_d[q];
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&fb.counters[kCounterQueueCursor + q], 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= count) break;
+    uint32_t i = base + lane;
+    if (i < count) {
+      float4 o = qo[i], d = qd[i];
+      uint32_t owner = __float_as_uint(d.w);
+      if (kAny) {
+        vis[owner] = trace_any(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w) ? 0 : 1;
+      } else {
+        Hit h;
+        trace_closest(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, h);
+        hits[owner] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.u), __float_as_uint(h.v), h.tri);
+      }
+    }
+  }
+}
+
+// ---- trace.wgsl:62-262 as four stages around the secondary rays -------------
+//   A: hit attributes, emission, G-buffer, first NEE candidates (area + BSDF);
+//      queues the BSDF candidate ray            (Nee::sample_ris, nee.wgsl:131-197)
+//   B: finishes resampled NEE, queues its shadow ray; Russian roulette; samples
+//      the GI direction and queues the GI candidate ray (inline_path_tracer.wgsl:258-283)
+//   C: sets the DI contribution weight from the shadow ray; shades the GI
+//      candidate's hit and queues its light-sample shadow ray (inline_path_tracer.wgsl:51-256)
+//   D: finishes the GI reservoir
+// The per-path RNG stream is consumed in exactly the reference's order.
+
+constexpr uint32_t F_SHADED = 1u, F_BSDF_RAY = 2u;  // stage A -> B
+constexpr uint32_t F_RIS_SHADOW = 1u, F_GI_RAY = 2u, F_GI_SHADOW = 4u;  // B -> C -> D
+
+APD uint32_t bounce_count(const FrameBuffers& fb, const Consts& c) { return c.bounce == 0 ? c.P : fb.counters[c.qin]; }
+APD uint32_t bounce_path(const FrameBuffers& fb, const Consts& c, uint32_t i) {
+  return c.bounce == 0 ? i : fb.queue[c.qin][i];
+}
+
+// Area light candidate (nee.wgsl:136-155).
+APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& fr, const Bsdf& b, uint32_t& rng,
+                        LightSample* ls, float* pdf, LightEval* ev, float* phat) {
+  float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng), r3 = rnd(rng), r4 = rnd(rng);
+  *ls = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), pdf);
+  *ev = load_eval(s, *ls, hit);
+  *phat = 0.0f;
+  float3 wi = normalize(ev->point - hit);
+  float wdn = dot(wi, fr.n);
+  if (wdn > 0.0f && *pdf > 0.0f) {
+    float sp = 0.0f;
+    float3 refl = disney_eval(b, fr, wo, wi, &sp);
+    if (sp > 0.0f) *phat = luma(refl * wdn * ev->emission);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade_a(DevScene s, FrameBuffers fb, Consts c, Mats mats) {
+  const uint32_t count = bounce_count(fb, c);
   const uint32_t cur = c.frame_idx & 1u;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    uint32_t id = c.bounce == 0 ? i : q[i];
+    uint32_t id = bounce_path(fb, c, i);
     float4 ray = fb.rays[id];
     float3 origin = ray_org(ray), direction = ray_dir(ray);
     uint4 pl = fb.payload[id];
@@ -330,7 +310,6 @@ __global__ void __launch_bounds__(kBlock) k_shade(DevScene s, FrameBuffers fb, C
       pl.y = pcg_hash(id ^ xor_shift(c.seed));
       pl.z = __float_as_uint(0.0f);
     }
-    if (__uint_as_float(pl.z) < 0.0f) continue;
     float3 acc = unpack_rgb9e5(fb.radiance[id]);
     float3 T = unpack_rgb9e5(pl.x);
     uint32_t rng = pl.y;
@@ -340,6 +319,9 @@ __global__ void __launch_bounds__(kBlock) k_shade(DevScene s, FrameBuffers fb, C
     uint4 hr = fb.hits[id];
     Hit h{__uint_as_float(hr.x), __uint_as_float(hr.y), __uint_as_float(hr.z), hr.w};
     float t_out;
+    uint32_t flags = 0;
+    bool want_ray = false;
+    float3 ray_o = f3s(0.0f), wi = f3s(0.0f);
     if (h.tri != kNoHit) {
       float depth_ws = 0.0f + h.t;
       const MaterialDev* m;
@@ -355,11 +337,140 @@ __global__ void __launch_bounds__(kBlock) k_shade(DevScene s, FrameBuffers fb, C
         g_alb = ld3(m->color) + emission;
         vel = velocity_of(mats, sf.hit_point);
       }
-      DiRes dr = sample_ris(s, c.cfg, sf.hit_point, wo, sf.frame, b, h.t, sf.back_face, rng);
-      fb.di_a[id] = di_pack_a(dr);
-      fb.di_b[id] = di_pack_b(dr);
       fb.ctx[id] = make_uint4(sf.material_idx, pack_rgb9e5(T), pack_oct30(sf.n), pack_oct30(sf.frame.cc_t2w.c2));
+      float area_pdf = 0.0f, area_phat = 0.0f, bsdf_pdf = 0.0f;
+      LightSample area_s{make_float2(0.0f, 0.0f), 0u, 0u};
+      if (c.cfg.di_area_samples > 0) {
+        LightEval ev;
+        area_candidate(s, sf.hit_point, wo, sf.frame, b, rng, &area_s, &area_pdf, &ev, &area_phat);
+      }
+      float3 contribution = f3s(0.0f);
+      if (c.cfg.di_bsdf_samples > 0) {
+        float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng);
+        float3 refl = disney_sample(b, sf.frame, wo, h.t, sf.back_face, r0, r1, r2, &wi, &bsdf_pdf);
+        float wdn = dm::fabs_(dot(wi, sf.n));
+        contribution = wdn * refl;
+        if (dot(contribution, contribution) > 0.0f) {
+          want_ray = true;
+          ray_o = sf.hit_point + sf.n * 1e-4f;
+        }
+      }
+      flags = F_SHADED | (want_ray ? F_BSDF_RAY : 0u);
+      fb.st_a[id] = make_uint4(__float_as_uint(area_pdf), __float_as_uint(area_phat), __float_as_uint(bsdf_pdf), flags);
+      fb.st_b[id] = make_uint4(__float_as_uint(area_s.uv.x), __float_as_uint(area_s.uv.y), area_s.inst, area_s.tri);
+      fb.st_c[id] = make_uint4(__float_as_uint(contribution.x), __float_as_uint(contribution.y),
+                               __float_as_uint(contribution.z), 0u);
+      fb.st_d[id] = make_uint4(__float_as_uint(wi.x), __float_as_uint(wi.y), __float_as_uint(wi.z), 0u);
       t_out = depth_ws;
+    } else {
+      g_alb = f3s(1.0f);
+      acc = acc + T * sky_radiance(s, direction, true);
+      t_out = -1.0f;
+      fb.st_a[id] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    push_ray(fb, Q_BSDF_CAND, want_ray, ray_o, 1000.0f, wi, id);
+    fb.radiance[id] = pack_rgb9e5(acc);
+    fb.payload[id] = make_uint4(pack_rgb9e5(T), rng, __float_as_uint(t_out), 0u);
+    if (c.bounce == 0) {
+      fb.gb_a[cur][id] = make_uint4(__float_as_uint(g_pos.x), __float_as_uint(g_pos.y), __float_as_uint(g_pos.z),
+                                    __float_as_uint(g_depth));
+      fb.gb_b[cur][id] = make_uint4(pack_oct30(g_n), pack_rgb9e5(g_alb), __float_as_uint(vel.x), __float_as_uint(vel.y));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade_b(DevScene s, FrameBuffers fb, Consts c) {
+  const uint32_t count = bounce_count(fb, c);
+  const uint32_t NA = c.cfg.di_area_samples, NB = c.cfg.di_bsdf_samples;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t id = bounce_path(fb, c, i);
+    uint4 sa = fb.st_a[id];
+    bool active = (sa.w & F_SHADED) != 0;
+    bool want_shadow = false, want_gi = false;
+    float3 sh_o = f3s(0.0f), sh_d = f3s(0.0f), gi_o = f3s(0.0f), wi = f3s(0.0f);
+    float sh_t = 0.0f;
+    if (active) {
+      uint4 pl = fb.payload[id];
+      float4 ray = fb.rays[id];
+      float3 origin = ray_org(ray), direction = ray_dir(ray);
+      float3 T = unpack_rgb9e5(pl.x);
+      uint32_t rng = pl.y;
+      uint4 hr = fb.hits[id];
+      Hit h{__uint_as_float(hr.x), __uint_as_float(hr.y), __uint_as_float(hr.z), hr.w};
+      const MaterialDev* m;
+      Surface sf = surface(s, h, origin, direction, &m);
+      Bsdf b = load_bsdf(m);
+      float3 wo = -direction;
+      float3 hit = sf.hit_point;
+      float area_pdf = __uint_as_float(sa.x), area_phat = __uint_as_float(sa.y), bsdf_pdf = __uint_as_float(sa.z);
+      uint4 sb = fb.st_b[id];
+      LightSample area_s{make_float2(__uint_as_float(sb.x), __uint_as_float(sb.y)), sb.z, sb.w};
+      LightEval area_e{f3s(0.0f), f3s(0.0f)};
+      if (NA > 0) area_e = load_eval(s, area_s, hit);
+      uint4 sc = fb.st_c[id];
+      float3 contribution = f3(__uint_as_float(sc.x), __uint_as_float(sc.y), __uint_as_float(sc.z));
+      uint4 sd4 = fb.st_d[id];
+      float3 bwi = f3(__uint_as_float(sd4.x), __uint_as_float(sd4.y), __uint_as_float(sd4.z));
+      LightSample bsdf_s = ls_empty();
+      LightEval bsdf_e{f3s(0.0f), f3s(0.0f)};
+      float bsdf_phat = 0.0f;
+      if (sa.w & F_BSDF_RAY) {
+        uint4 h1 = fb.hit_bsdf[id];
+        if (h1.w != kNoHit) {
+          const InstanceDev in = s.instances[s.tri_instance[h1.w]];
+          if (in.emissive_idx != kU32Max)
+            bsdf_s = LightSample{make_float2(__uint_as_float(h1.y), __uint_as_float(h1.z)), in.emissive_idx,
+                                 h1.w - in.first_global_tri};
+        } else {
+          bsdf_s = LightSample{inverse_direction_to_sun(s.sun, bwi), kU32Max - 1, 0u};
+        }
+        if (!ls_is_empty(bsdf_s)) {
+          bsdf_e = load_eval(s, bsdf_s, hit);
+          bsdf_phat = luma(contribution * bsdf_e.emission);
+        }
+      }
+      DiRes res = di_new();
+      LightEval sel{f3s(0.0f), f3s(0.0f)};
+      uint32_t n_iter = NA > NB ? NA : NB;
+      for (uint32_t k = 0; k < n_iter; ++k) {
+        float apdf = 0.0f, aphat = 0.0f, bpdf = 0.0f;
+        LightSample as{make_float2(0.0f, 0.0f), 0u, 0u};
+        LightEval ae{f3s(0.0f), f3s(0.0f)};
+        if (k == 0) {
+          apdf = area_pdf; aphat = area_phat; as = area_s; ae = area_e; bpdf = bsdf_pdf;
+        } else if (k < NA) {
+          area_candidate(s, hit, wo, sf.frame, b, rng, &as, &apdf, &ae, &aphat);
+        }
+        if (k < NA) {
+          float aw = 0.0f;
+          if (apdf > 0.0f) {
+            float mis = apdf / ((float)NA * apdf + (float)NB * bpdf);
+            aw = mis * aphat * (1.0f / dm::fmax(apdf, 1e-8f));
+          }
+          if (di_update(res, aw, rng, as, aphat)) sel = ae;
+        }
+        if (k < NB) {
+          float bw = 0.0f;
+          if (bpdf > 0.0f) {
+            float mis = bpdf / ((float)NB * bpdf + (float)NA * apdf);
+            bw = mis * bsdf_phat * (1.0f / dm::fmax(bpdf, 1e-8f));
+          }
+          if (di_update(res, bw, rng, bsdf_s, bsdf_phat)) sel = bsdf_e;
+        }
+      }
+      if (res.phat > 1e-6f) {
+        sh_d = normalize(sel.point - hit);
+        float dd = dist(sel.point, hit);
+        sh_o = hit + sf.n * 1e-4f;
+        sh_t = dd - 1e-4f * 2.0f;
+        want_shadow = true;
+      }
+      fb.di_a[id] = di_pack_a(res);
+      fb.di_b[id] = di_pack_b(res);
+      float t_out = __uint_as_float(pl.z);
+      float gi_pdf = 0.0f;
+      uint32_t phat_rng = 0;
+      float3 tr = f3s(0.0f);
       if (c.bounce + 1 < c.cfg.max_bounces) {
         bool killed = false;
         if (c.bounce > 1) {
@@ -372,53 +483,190 @@ __global__ void __launch_bounds__(kBlock) k_shade(DevScene s, FrameBuffers fb, C
           }
         }
         if (!killed) {
-          GiRes gr = gi_sample_ris(s, sf.hit_point, wo, sf.frame, b, T, h.t, sf.back_face, rng);
-          fb.gi_a[id] = gi_pack_a(gr);
-          fb.gi_b[id] = gi_pack_b(gr);
+          float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng);
+          float3 refl = disney_sample(b, sf.frame, wo, h.t, sf.back_face, r0, r1, r2, &wi, &gi_pdf);
+          if (gi_pdf > 1e-6f) {
+            float cos_in = dm::fabs_(dot(wi, sf.n));
+            float3 local = cos_in * refl;
+            tr = T * local;
+            phat_rng = rng;
+            gi_o = hit + wi * 1e-4f;
+            want_gi = true;
+          } else {
+            GiRes z = gi_new();
+            fb.gi_a[id] = gi_pack_a(z);
+            fb.gi_b[id] = gi_pack_b(z);
+          }
         }
       }
-    } else {
-      g_alb = f3s(1.0f);
-      acc = acc + T * sky_radiance(s, direction, true);
-      t_out = -1.0f;
+      uint32_t flags = (want_shadow ? F_RIS_SHADOW : 0u) | (want_gi ? F_GI_RAY : 0u);
+      fb.payload[id] = make_uint4(pack_rgb9e5(T), rng, __float_as_uint(t_out), 0u);
+      fb.st_a[id] = make_uint4(__float_as_uint(gi_pdf), phat_rng, 0u, flags);
+      fb.st_c[id] = make_uint4(__float_as_uint(tr.x), __float_as_uint(tr.y), __float_as_uint(tr.z), 0u);
+      fb.st_d[id] = make_uint4(__float_as_uint(wi.x), __float_as_uint(wi.y), __float_as_uint(wi.z), 0u);
     }
-    fb.radiance[id] = pack_rgb9e5(acc);
-    fb.payload[id] = make_uint4(pack_rgb9e5(T), rng, __float_as_uint(t_out), 0u);
-    if (c.bounce == 0) {
-      fb.gb_a[cur][id] = make_uint4(__float_as_uint(g_pos.x), __float_as_uint(g_pos.y), __float_as_uint(g_pos.z),
-                                    __float_as_uint(g_depth));
-      fb.gb_b[cur][id] = make_uint4(pack_oct30(g_n), pack_rgb9e5(g_alb), __float_as_uint(vel.x), __float_as_uint(vel.y));
-    }
+    push_ray(fb, Q_RIS_SHADOW, want_shadow, sh_o, sh_t, sh_d, id);
+    push_ray(fb, Q_GI_CAND, want_gi, gi_o, 1000.0f - 1e-4f * 2.0f, wi, id);
   }
 }
 
-// apply_di.wgsl:48-111
-__global__ void __launch_bounds__(kBlock) k_apply_di(DevScene s, FrameBuffers fb, Consts c) {
-  const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
-  const uint32_t* q = fb.queue[c.qin];
+APD void finish_gi(const FrameBuffers& fb, uint32_t id, float3 contribution, float pdf, float3 point, uint32_t phat_rng,
+                   uint32_t& rng) {
+  GiRes res = gi_new();
+  float phat = luma(contribution);
+  gi_update(res, phat / pdf, rng, point, phat, phat_rng);
+  if (res.phat > 0.0f && res.M * res.wsum > 0.0f) res.W = (1.0f / res.phat) * (1.0f / res.M * res.wsum);
+  fb.gi_a[id] = gi_pack_a(res);
+  fb.gi_b[id] = gi_pack_b(res);
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade_c(DevScene s, FrameBuffers fb, Consts c) {
+  const uint32_t count = bounce_count(fb, c);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    uint32_t id = c.bounce == 0 ? i : q[i];
+    uint32_t id = bounce_path(fb, c, i);
+    uint4 sa = fb.st_a[id];
+    bool want = false;
+    float3 so = f3s(0.0f), sd = f3s(0.0f);
+    float st = 0.0f;
+    if (sa.w & F_RIS_SHADOW) {
+      if (fb.vis[Q_RIS_SHADOW][id]) {
+        uint4 da = fb.di_a[id];
+        float W = (1.0f / __uint_as_float(da.w)) * __uint_as_float(da.z);
+        fb.di_a[id] = make_uint4(da.x, __float_as_uint(W), da.z, da.w);
+      }
+    }
+    if (sa.w & F_GI_RAY) {
+      uint4 pl = fb.payload[id];
+      uint32_t rng = pl.y;
+      float4 ray = fb.rays[id];
+      float3 hit = ray_org(ray) + ray_dir(ray) * __uint_as_float(pl.z);
+      uint4 sc = fb.st_c[id], sdd = fb.st_d[id];
+      float3 tr = f3(__uint_as_float(sc.x), __uint_as_float(sc.y), __uint_as_float(sc.z));
+      float3 wi = f3(__uint_as_float(sdd.x), __uint_as_float(sdd.y), __uint_as_float(sdd.z));
+      float gi_pdf = __uint_as_float(sa.x);
+      uint32_t phat_rng = sa.y;
+      uint4 hr = fb.hit_gi[id];
+      float3 acc = f3s(0.0f), point;
+      if (hr.w != kNoHit) {
+        Hit h{__uint_as_float(hr.x), __uint_as_float(hr.y), __uint_as_float(hr.z), hr.w};
+        const MaterialDev* m;
+        Surface sf = surface(s, h, hit, wi, &m);
+        Bsdf b = load_bsdf(m);
+        float pdf = 0.0f;
+        float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng), r3 = rnd(rng), r4 = rnd(rng);
+        LightSample ls = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), &pdf);
+        float W = 1.0f / pdf;
+        if (W > 0.0f) {
+          LightEval ev = load_eval(s, ls, sf.hit_point);
+          float3 sdir = normalize(ev.point - sf.hit_point);
+          float sdist = dist(ev.point, sf.hit_point);
+          float ndl = dot(sdir, sf.n);
+          if (ndl > 0.0f) {
+            float sp = 0.0f;
+            float3 refl = disney_eval(b, sf.frame, -wi, sdir, &sp);
+            acc = tr * refl * ev.emission * ndl * W;  // added when the shadow ray is unoccluded
+            so = sf.hit_point + sf.n * 1e-4f;
+            sd = sdir;
+            st = sdist - 1e-4f * 2.0f;
+            want = true;
+          }
+        }
+        point = sf.hit_point;
+      } else {
+        point = hit + wi * 1000.0f;
+        acc = acc + tr * sky_radiance(s, wi, true);
+      }
+      if (want) {
+        fb.st_a[id] = make_uint4(sa.x, sa.y, 0u, F_GI_SHADOW);
+        fb.st_b[id] = make_uint4(__float_as_uint(point.x), __float_as_uint(point.y), __float_as_uint(point.z), 0u);
+        fb.st_c[id] = make_uint4(__float_as_uint(acc.x), __float_as_uint(acc.y), __float_as_uint(acc.z), 0u);
+      } else {
+        finish_gi(fb, id, acc, gi_pdf, point, phat_rng, rng);
+        fb.st_a[id] = make_uint4(0u, 0u, 0u, 0u);
+      }
+      pl.y = rng;
+      fb.payload[id] = pl;
+    } else if (sa.w != 0u) {
+      fb.st_a[id] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    push_ray(fb, Q_GI_SHADOW, want, so, st, sd, id);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_shade_d(FrameBuffers fb, Consts c) {
+  const uint32_t count = bounce_count(fb, c);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t id = bounce_path(fb, c, i);
+    uint4 sa = fb.st_a[id];
+    if (!(sa.w & F_GI_SHADOW)) continue;
+    uint4 pl = fb.payload[id];
+    uint32_t rng = pl.y;
+    uint4 sb = fb.st_b[id], sc = fb.st_c[id];
+    float3 point = f3(__uint_as_float(sb.x), __uint_as_float(sb.y), __uint_as_float(sb.z));
+    float3 acc = f3s(0.0f);
+    if (fb.vis[Q_GI_SHADOW][id]) acc = acc + f3(__uint_as_float(sc.x), __uint_as_float(sc.y), __uint_as_float(sc.z));
+    finish_gi(fb, id, acc, __uint_as_float(sa.x), point, sa.y, rng);
+    pl.y = rng;
+    fb.payload[id] = pl;
+  }
+}
+
+// apply_di.wgsl:48-111 in two stages around its shadow ray.
+constexpr uint32_t F_DI_REPACK = 1u, F_DI_SHADOW = 2u;
+__global__ void __launch_bounds__(kBlock) k_apply_di_a(DevScene s, FrameBuffers fb, Consts c) {
+  const uint32_t count = bounce_count(fb, c);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t id = bounce_path(fb, c, i);
     uint4 pl = fb.payload[id];
     float pt = __uint_as_float(pl.z);
-    if (pt < 0.0f) continue;
-    DiRes dr = di_unpack(fb.di_a[id], fb.di_b[id]);
-    if (dr.W == 0.0f) continue;
-    float4 ray = fb.rays[id];
-    float3 origin = ray_org(ray), direction = ray_dir(ray);
-    uint4 cx = fb.ctx[id];
+    uint32_t flags = 0;
+    bool want = false;
+    float3 so = f3s(0.0f), sd = f3s(0.0f);
+    float st = 0.0f;
+    if (pt >= 0.0f) {
+      DiRes dr = di_unpack(fb.di_a[id], fb.di_b[id]);
+      if (dr.W != 0.0f) {
+        flags = F_DI_REPACK;
+        float4 ray = fb.rays[id];
+        float3 origin = ray_org(ray), direction = ray_dir(ray);
+        uint4 cx = fb.ctx[id];
+        float3 T = unpack_rgb9e5(cx.y);
+        Bsdf b = load_bsdf(s.materials + cx.x);
+        float3 hit = origin + direction * pt;
+        Frame fr = ctx_frame(cx);
+        LightEval ev = load_eval(s, dr.s, hit);
+        float3 sdir = normalize(ev.point - hit);
+        float sdist = dist(ev.point, hit);
+        float ndl = dot(sdir, fr.n);
+        if (ndl > 0.0f) {
+          float sp = 0.0f;
+          float3 refl = disney_eval(b, fr, -direction, sdir, &sp);
+          float3 contribution = T * refl * ev.emission * ndl * dr.W;
+          fb.st_c[id] = make_uint4(__float_as_uint(contribution.x), __float_as_uint(contribution.y),
+                                   __float_as_uint(contribution.z), 0u);
+          so = hit + fr.n * 1e-4f;
+          sd = sdir;
+          st = sdist - 1e-4f * 2.0f;
+          want = true;
+          flags |= F_DI_SHADOW;
+        }
+      }
+    }
+    fb.st_a[id] = make_uint4(0u, 0u, 0u, flags);
+    push_ray(fb, Q_DI_SHADOW, want, so, st, sd, id);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_apply_di_b(FrameBuffers fb, Consts c) {
+  const uint32_t count = bounce_count(fb, c);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t id = bounce_path(fb, c, i);
+    uint32_t flags = fb.st_a[id].w;
+    if (!(flags & F_DI_REPACK)) continue;
     float3 acc = unpack_rgb9e5(fb.radiance[id]);
-    float3 T = unpack_rgb9e5(cx.y);
-    Bsdf b = load_bsdf(s.materials + cx.x);
-    float3 hit = origin + direction * pt;
-    Frame fr = ctx_frame(cx);
-    LightEval ev = load_eval(s, dr.s, hit);
-    float3 sdir = normalize(ev.point - hit);
-    float sd = dist(ev.point, hit);
-    float ndl = dot(sdir, fr.n);
-    if (ndl > 0.0f && shadow_ray(s, hit, sdir, sd, fr.n)) {
-      float sp = 0.0f;
-      float3 refl = disney_eval(b, fr, -direction, sdir, &sp);
-      acc = acc + T * refl * ev.emission * ndl * dr.W;
+    if ((flags & F_DI_SHADOW) && fb.vis[Q_DI_SHADOW][id]) {
+      uint4 sc = fb.st_c[id];
+      acc = acc + f3(__uint_as_float(sc.x), __uint_as_float(sc.y), __uint_as_float(sc.z));
     }
     fb.radiance[id] = pack_rgb9e5(acc);
   }
@@ -1075,6 +1323,10 @@ size_t frame_buffer_bytes(uint32_t W, uint32_t H) {
   add(P * 4); add(P * 4);                   // count, hist
   add(P * 4);                               // snapshot
   add(P * 4); add(P * 4);                   // queues
+  for (int i = 0; i < 10; ++i) add(P * 16);  // ray queues (origin, direction) x 5
+  add(P * 16); add(P * 16);                 // hit_bsdf, hit_gi
+  for (int i = 0; i < 5; ++i) add(P);       // visibility
+  for (int i = 0; i < 4; ++i) add(P * 16);  // stage state
   add(64 * 4);                              // counters
   add(P * 12);                              // out rgb
   (void)p;
@@ -1122,12 +1374,44 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
   fb->snapshot = carve<uint32_t>(p, P);
   fb->queue[0] = carve<uint32_t>(p, P);
   fb->queue[1] = carve<uint32_t>(p, P);
+  for (int q = 0; q < 5; ++q) {
+    fb->rq_o[q] = carve<float4>(p, P);
+    fb->rq_d[q] = carve<float4>(p, P);
+  }
+  fb->hit_bsdf = carve<uint4>(p, P);
+  fb->hit_gi = carve<uint4>(p, P);
+  for (int q = 0; q < 5; ++q) fb->vis[q] = carve<uint8_t>(p, P);
+  fb->st_a = carve<uint4>(p, P);
+  fb->st_b = carve<uint4>(p, P);
+  fb->st_c = carve<uint4>(p, P);
+  fb->st_d = carve<uint4>(p, P);
   fb->counters = carve<uint32_t>(p, 64);
   fb->out_rgb = carve<float>(p, 3 * P);
 }
 
-void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
-                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t st) {
+const char* kernel_kind_name(int k) {
+  static const char* names[K_NUM_KINDS] = {"memset", "raygen", "extend", "shade", "di_temporal", "di_spatial",
+                                           "gi_temporal", "gi_spatial", "apply_di", "apply_gi", "demodulate",
+                                           "firefly", "svgf_temporal", "atrous", "taa", "resolve", "copy",
+                                           "trace_closest", "trace_any"};
+  return (k >= 0 && k < K_NUM_KINDS) ? names[k] : "?";
+}
+
+int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
+                 uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t st, FrameProfiler* prof) {
+  int launches = 0;
+  if (prof) {
+    prof->n = 0;
+    cudaEventRecord(prof->ev[0], st);
+  }
+  auto mark = [&](int kind) {
+    if (kind != K_MEMSET && kind != K_COPY) ++launches;
+    if (prof && prof->n < FrameProfiler::kMax) {
+      prof->kind[prof->n] = kind;
+      cudaEventRecord(prof->ev[prof->n + 1], st);
+      prof->n += 1;
+    }
+  };
   const uint32_t P = W * H;
   const uint32_t cur = frame_idx & 1u;
   dim3 b2(16, 16), g2((W + 15) / 16, (H + 15) / 16);
@@ -1140,16 +1424,38 @@ void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConf
   c.frame_idx = frame_idx;
   c.cfg = cfg;
   cudaMemsetAsync(fb.radiance, 0, (size_t)P * 4, st);
+  cudaMemsetAsync(fb.counters + 3, 0, 4, st);
+  mark(K_MEMSET);
   for (uint32_t sample = 0; sample < cfg.sample_count; ++sample) {
     c.seed = frame_idx * cfg.sample_count + sample;
     k_raygen<<<g2, b2, 0, st>>>(fb, W, H, mats);
+    mark(K_RAYGEN);
     for (uint32_t i = 0; i < cfg.max_bounces; ++i) {
       c.bounce = i;
       c.qin = i & 1u;
       c.qout = (i + 1) & 1u;
       cudaMemsetAsync(fb.counters + 2, 0, 4, st);
+      mark(K_MEMSET);
       k_extend<<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
-      k_shade<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c, mats);
+      mark(K_EXTEND);
+      cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+      mark(K_MEMSET);
+      k_shade_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c, mats);
+      mark(K_SHADE);
+      k_trace_queue<false><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_BSDF_CAND, fb.hit_bsdf, nullptr);
+      mark(K_TRACE_CLOSEST);
+      k_shade_b<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
+      mark(K_SHADE);
+      k_trace_queue<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_RIS_SHADOW, nullptr, fb.vis[Q_RIS_SHADOW]);
+      mark(K_TRACE_ANY);
+      k_trace_queue<false><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_GI_CAND, fb.hit_gi, nullptr);
+      mark(K_TRACE_CLOSEST);
+      k_shade_c<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
+      mark(K_SHADE);
+      k_trace_queue<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_GI_SHADOW, nullptr, fb.vis[Q_GI_SHADOW]);
+      mark(K_TRACE_ANY);
+      k_shade_d<<<linear_blocks, kBlock, 0, st>>>(fb, c);
+      mark(K_SHADE);
       if (i == 0) {
         if (cfg.restir_di) {
           uint4* pin_a = fb.di_prev_a[cur];
@@ -1158,6 +1464,7 @@ void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConf
           uint4* pout_b = fb.di_prev_b[cur ^ 1u];
           k_di_temporal<<<g2, b2, 0, st>>>(scene, fb, c, fb.di_a, fb.di_b, fb.di_inter_a, fb.di_inter_b, pin_a, pin_b,
                                            pout_a, pout_b);
+          mark(K_DI_TEMPORAL);
           uint32_t n = cfg.di_spatial_passes;
           for (uint32_t k = 0; k < n; ++k) {
             bool odd = (k % 2) != 0;
@@ -1165,10 +1472,12 @@ void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConf
                                                 odd ? fb.di_a : fb.di_inter_a, odd ? fb.di_b : fb.di_inter_b,
                                                 odd ? fb.di_inter_a : fb.di_a, odd ? fb.di_inter_b : fb.di_b, pout_a,
                                                 pout_b);
+            mark(K_DI_SPATIAL);
           }
           if (n % 2 == 0) {
             cudaMemcpyAsync(fb.di_a, fb.di_inter_a, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
             cudaMemcpyAsync(fb.di_b, fb.di_inter_b, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+            mark(K_COPY);
           }
         }
         if (cfg.restir_gi) {
@@ -1178,10 +1487,12 @@ void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConf
           uint4* pout_b = fb.gi_prev_b[cur ^ 1u];
           k_gi_temporal<<<g2, b2, 0, st>>>(scene, fb, c, fb.gi_a, fb.gi_b, fb.gi_inter_a, fb.gi_inter_b, pin_a, pin_b,
                                            pout_a, pout_b);
+          mark(K_GI_TEMPORAL);
           uint32_t n = cfg.gi_spatial_passes;
           if (n == 0) {
             cudaMemcpyAsync(fb.gi_a, fb.gi_inter_a, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
             cudaMemcpyAsync(fb.gi_b, fb.gi_inter_b, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+            mark(K_COPY);
           }
           for (uint32_t k = 0; k < n; ++k) {
             bool odd = (k % 2) != 0;
@@ -1189,17 +1500,26 @@ void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConf
                                                odd ? fb.gi_a : fb.gi_inter_a, odd ? fb.gi_b : fb.gi_inter_b,
                                                odd ? fb.gi_inter_a : fb.gi_a, odd ? fb.gi_inter_b : fb.gi_b, pout_a,
                                                pout_b);
+            mark(K_GI_SPATIAL);
           }
           if (n > 0 && n % 2 == 0) {
             cudaMemcpyAsync(fb.gi_a, fb.gi_inter_a, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
             cudaMemcpyAsync(fb.gi_b, fb.gi_inter_b, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
+            mark(K_COPY);
           }
         }
       }
-      k_apply_di<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
+      k_apply_di_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
+      mark(K_APPLY_DI);
+      k_trace_queue<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_DI_SHADOW, nullptr, fb.vis[Q_DI_SHADOW]);
+      mark(K_TRACE_ANY);
+      k_apply_di_b<<<linear_blocks, kBlock, 0, st>>>(fb, c);
+      mark(K_APPLY_DI);
       if (i + 1 < cfg.max_bounces) {
         cudaMemsetAsync(fb.counters + c.qout, 0, 4, st);
+        mark(K_MEMSET);
         k_apply_gi<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
+        mark(K_APPLY_GI);
       }
     }
   }
@@ -1208,14 +1528,18 @@ void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConf
   uint32_t* dcur = fb.demod[cur];
   uint32_t* dprev = fb.demod[cur ^ 1u];
   k_demodulate<<<lb, 256, 0, st>>>(fb, P, cur, fb.radiance, dcur, 0);
+  mark(K_DEMODULATE);
   if (cfg.firefly_filter) {
     cudaMemcpyAsync(fb.snapshot, dcur, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
+    mark(K_COPY);
     k_firefly<<<g2, b2, 0, st>>>(fb, W, H, cur, fb.snapshot, dcur);
+    mark(K_FIREFLY);
   }
   if (cfg.svgf) {
     uint32_t f = frame_idx;
     k_svgf_temporal<<<g2, b2, 0, st>>>(fb, c, dcur, fb.svgf_rad[(f + 1) % 2], fb.svgf_mom[f % 2],
                                        fb.svgf_mom[(f + 1) % 2], fb.svgf_var[(f + 1) % 2]);
+    mark(K_SVGF_TEMPORAL);
     for (uint32_t i = 0; i < cfg.svgf_atrous_passes; ++i) {
       const uint32_t* in_rad = fb.svgf_rad[(f + 1 + i) % 2];
       uint32_t* out_rad = fb.svgf_rad[(f + i) % 2];
@@ -1232,16 +1556,24 @@ void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConf
         case 6: k_atrous<64><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
         default: k_atrous<128><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
       }
-      if (i == cfg.svgf_atrous_passes - 1)
+      mark(K_ATROUS);
+      if (i == cfg.svgf_atrous_passes - 1) {
         cudaMemcpyAsync(dcur, out_rad, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
+        mark(K_COPY);
+      }
     }
   }
   if (cfg.taa && frame_idx > 0) {
     cudaMemcpyAsync(fb.snapshot, dcur, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
+    mark(K_COPY);
     k_taa<<<g2, b2, 0, st>>>(fb, c, fb.snapshot, dcur, dprev);
+    mark(K_TAA);
   }
   k_demodulate<<<lb, 256, 0, st>>>(fb, P, cur, dcur, fb.radiance, 1);
+  mark(K_DEMODULATE);
   k_resolve<<<lb, 256, 0, st>>>(fb, P, (float)cfg.sample_count);
+  mark(K_RESOLVE);
+  return launches;
 }
 
 void launch_trace_batch(const DevScene& scene, const float4* origins, const float4* dirs, uint32_t n, int any_hit,

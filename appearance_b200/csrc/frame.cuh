@@ -44,9 +44,23 @@ struct FrameBuffers {
   uint32_t* svgf_hist;
   uint32_t* snapshot;  // pre-filter copy for the firefly filter and TAA
   uint32_t* queue[2];  // active path ids (ping-pong)
-  uint32_t* counters;  // [0..1] queue sizes, [2] work cursor, [3..] statistics
+  // Secondary-ray queues of one bounce (origin.xyz + tmax, direction.xyz + owner
+  // path id): Q_BSDF_CAND closest, Q_RIS_SHADOW any, Q_GI_CAND closest,
+  // Q_GI_SHADOW any, Q_DI_SHADOW any.
+  float4* rq_o[5];
+  float4* rq_d[5];
+  uint4* hit_bsdf;     // closest hit of the NEE BSDF candidate ray, per path
+  uint4* hit_gi;       // closest hit of the GI candidate ray, per path
+  uint8_t* vis[5];     // any-hit queues: 1 = unoccluded, per path
+  uint4 *st_a, *st_b, *st_c, *st_d;  // per-path state between shading stages
+  uint32_t* counters;  // [0..1] path queue sizes, [2] extend cursor, [3] rays traced,
+                       // [4..8] ray queue sizes, [9..13] ray queue cursors
   float* out_rgb;      // linear HDR output, 3 floats per pixel (device)
 };
+
+enum RayQueue { Q_BSDF_CAND = 0, Q_RIS_SHADOW = 1, Q_GI_CAND = 2, Q_GI_SHADOW = 3, Q_DI_SHADOW = 4 };
+constexpr int kCounterQueueSize = 4;
+constexpr int kCounterQueueCursor = 9;
 
 struct Mats {
   float inv_view[16], inv_proj[16], view_proj[16], prev_view_proj[16];
@@ -60,9 +74,30 @@ size_t frame_buffer_bytes(uint32_t W, uint32_t H);
 // Carves `base` (frame_buffer_bytes(W,H) bytes, zeroed by the caller) into buffers.
 void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb);
 
+// Kernel kinds for per-kernel timing (FrameProfiler) and launch counting.
+enum KernelKind : int {
+  K_MEMSET = 0, K_RAYGEN, K_EXTEND, K_SHADE, K_DI_TEMPORAL, K_DI_SPATIAL, K_GI_TEMPORAL, K_GI_SPATIAL,
+  K_APPLY_DI, K_APPLY_GI, K_DEMODULATE, K_FIREFLY, K_SVGF_TEMPORAL, K_ATROUS, K_TAA, K_RESOLVE, K_COPY,
+  K_TRACE_CLOSEST, K_TRACE_ANY, K_NUM_KINDS
+};
+const char* kernel_kind_name(int k);
+
+// Optional instrumentation: when passed to encode_frame, an event is recorded
+// after every launch so that the device time of each kernel kind is the gap
+// between consecutive events on the (in-order) stream.
+struct FrameProfiler {
+  static constexpr int kMax = 512;
+  cudaEvent_t ev[kMax + 1];
+  int kind[kMax];
+  int n = 0;
+  bool created = false;
+};
+
 // Encodes one frame on `stream`.  `frame_idx` selects the ping-pong parity.
-void encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
-                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t stream);
+// Returns the number of kernels launched (memsets and copies excluded).
+int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
+                 uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t stream,
+                 FrameProfiler* prof = nullptr);
 
 // Closest / any hit for a batch of rays (parity tests and traversal bench).
 // rays: origin.xyz + tmax (float4), dirs: float4; out: t, u, v, tri bits.

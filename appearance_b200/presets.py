@@ -19,9 +19,14 @@ FAITHFUL = dict(
 PLAIN = dict(FAITHFUL, max_bounces=5, sample_count=16, restir_di=0, restir_gi=0, firefly_filter=0)
 
 # 1920x1080 real-time frame: depth 8, 1 spp, ReSTIR DI with 32 area candidates,
-# temporal reuse and 5-neighbour spatial reuse, ReSTIR GI (temporal + 5-neighbour
-# spatial), firefly filter, SVGF with 5 a-trous passes, TAA.
+# temporal reuse (M cap 20x) and 5-neighbour spatial reuse, ReSTIR GI with
+# temporal reuse (spatial GI reuse off, as the reference runs it,
+# crates/appearance-path-tracer-gpu/src/lib.rs:441), firefly filter, SVGF with 5
+# a-trous passes, TAA.
 REALTIME = dict(FAITHFUL, max_bounces=8, sample_count=1, svgf=1, taa=1, di_area_samples=32,
-                di_spatial_samples=5, gi_spatial_passes=1, gi_spatial_samples=5)
+                di_spatial_samples=5)
 
-PRESETS = dict(faithful=FAITHFUL, plain=PLAIN, realtime=REALTIME)
+# REALTIME plus one unbiased 5-neighbour ReSTIR GI spatial pass.
+REALTIME_GI_SPATIAL = dict(REALTIME, gi_spatial_passes=1, gi_spatial_samples=5)
+
+PRESETS = dict(faithful=FAITHFUL, plain=PLAIN, realtime=REALTIME, realtime_gi_spatial=REALTIME_GI_SPATIAL)

@@ -154,6 +154,17 @@ class PathTracer:
         self._check(self._lib.ap_read_buffer(self._h, which, _ptr(out), out.nbytes))
         return out
 
+    def profile_frame(self, width: int, height: int) -> dict:
+        """Renders one frame with per-kernel events; returns {kind: (ms, launches)}."""
+        n = 32
+        ms = np.zeros(n, np.float64)
+        cnt = np.zeros(n, np.uint32)
+        names = (ctypes.c_char_p * n)()
+        nk = np.zeros(1, np.uint32)
+        self._check(self._lib.ap_profile_frame(self._h, width, height, _ptr(ms), _ptr(cnt), names, n, _ptr(nk),
+                                               ctypes.byref(self.last_stats)))
+        return {names[i].decode(): (float(ms[i]), int(cnt[i])) for i in range(int(nk[0]))}
+
     def bvh_stats(self) -> dict:
         out = np.zeros(8, np.uint32)
         self._check(self._lib.ap_bvh_stats(self._h, _ptr(out)))

@@ -112,6 +112,7 @@ typedef struct ap_frame_stats {
   uint64_t extension_rays;  /* closest-hit rays of the path-extension stage */
   uint32_t width, height;
   uint32_t frame_idx;
+  uint32_t kernel_launches; /* kernels launched for the frame (copies/memsets excluded) */
 } ap_frame_stats;
 
 /* Fills the reference defaults (PathTracerGpuConfig::default + pass literals). */
@@ -165,6 +166,14 @@ int ap_trace_rays(void* handle, const float* origins_tmax, const float* dirs, ui
  * G-buffer (8), 3 DI reservoirs (8), 4 GI reservoirs (8), 5 light-sample
  * context (4), 7 rays (4). */
 int ap_read_buffer(void* handle, uint32_t which, uint32_t* out, size_t out_bytes);
+
+/* Renders one frame (advancing the frame sequence like ap_render_device) with
+ * an event after every launch, and returns the device milliseconds and the
+ * launch count of each kernel kind: kind_ms and kind_count hold `max_kinds`
+ * entries; names[i] receives a static string naming kind i; *num_kinds the
+ * number of kinds written. */
+int ap_profile_frame(void* handle, uint32_t w, uint32_t h, double* kind_ms, uint32_t* kind_count,
+                     const char** names, uint32_t max_kinds, uint32_t* num_kinds, ap_frame_stats* stats);
 
 /* BVH statistics of the uploaded scene: nodes, triangles, max depth, max
  * traversal stack, build ms (as double bits in out[4..5]). */
