@@ -73,6 +73,6 @@ def load() -> ctypes.CDLL:
     L.ap_trace_rays.argtypes = [P, P, P, U32, ctypes.c_int, P]
     L.ap_read_buffer.argtypes = [P, U32, P, ctypes.c_size_t]
     L.ap_bvh_stats.argtypes = [P, P]
-    L.ap_profile_frame.argtypes = [P, U32, U32, P, P, P, U32, P, ctypes.POINTER(FrameStats)]
+    L.ap_profile_frame.argtypes = [P, U32, U32, P, P, P, U32, P, ctypes.c_int, P, ctypes.POINTER(FrameStats)]
     _lib = L
     return L

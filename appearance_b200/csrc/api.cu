@@ -574,7 +574,8 @@ int ap_read_buffer(void* hp, uint32_t which, uint32_t* out, size_t out_bytes) {
 }
 
 int ap_profile_frame(void* hp, uint32_t w, uint32_t hgt, double* kind_ms, uint32_t* kind_count, const char** names,
-                     uint32_t max_kinds, uint32_t* num_kinds, ap_frame_stats* stats) {
+                     uint32_t max_kinds, uint32_t* num_kinds, int count_visits, uint64_t* visits,
+                     ap_frame_stats* stats) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h || !kind_ms || !kind_count || !num_kinds) return AP_E_INVALID;
   cudaSetDevice(h->device);
@@ -583,9 +584,20 @@ int ap_profile_frame(void* hp, uint32_t w, uint32_t hgt, double* kind_ms, uint32
       if (cudaEventCreate(&h->prof.ev[i]) != cudaSuccess) return fail(h, AP_E_CUDA, "profiler events");
     h->prof.created = true;
   }
+  h->prof.count_visits = count_visits != 0;
   int rc = render_common(h, w, hgt, stats, &h->prof);
+  h->prof.count_visits = false;
   if (rc) return rc;
   uint32_t nk = std::min<uint32_t>(max_kinds, (uint32_t)K_NUM_KINDS);
+  if (visits) {
+    std::vector<unsigned long long> v(3 * K_NUM_KINDS, 0ull);
+    if (count_visits) {
+      rc = check_cuda(h, cudaMemcpy(v.data(), h->fb.visits, v.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+                      "visits");
+      if (rc) return rc;
+    }
+    for (uint32_t k = 0; k < 3 * nk; ++k) visits[k] = v[k];
+  }
   for (uint32_t k = 0; k < nk; ++k) {
     kind_ms[k] = 0.0;
     kind_count[k] = 0;

@@ -186,6 +186,7 @@ __global__ void k_raygen(FrameBuffers fb, uint32_t W, uint32_t H, Mats mats) {
 
 // Persistent closest-hit kernel for the path-extension rays: each warp takes
 // 32 consecutive queue entries per atomic.  Bounce 0 traces every pixel.
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_extend(DevScene s, FrameBuffers fb, Consts c) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
@@ -202,8 +203,14 @@ __global__ void __launch_bounds__(kBlock) k_extend(DevScene s, FrameBuffers fb, 
       float4 r = fb.rays[id];
       float3 o = ray_org(r), d = ray_dir(r);
       Hit h;
-      trace_closest(s, o + d * 1e-4f, d, 1000.0f, h);
+      Visits vc;
+      trace_closest<kCount>(s, o + d * 1e-4f, d, 1000.0f, h, &vc);
       fb.hits[id] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.u), __float_as_uint(h.v), h.tri);
+      if (kCount) {
+        atomicAdd(&fb.visits[3 * K_EXTEND + 0], 1ull);
+        atomicAdd(&fb.visits[3 * K_EXTEND + 1], (unsigned long long)vc.nodes);
+        atomicAdd(&fb.visits[3 * K_EXTEND + 2], (unsigned long long)vc.tris);
+      }
     }
   }
 }
@@ -235,7 +242,7 @@ APD void push_ray(const FrameBuffers& fb, int q, bool want, float3 o, float tmax
 }
 
 // Persistent traversal of one ray queue; each warp takes 32 rays per atomic.
-template <bool kAny>
+template <bool kAny, bool kCount>
 __global__ void __launch_bounds__(kBlock) k_trace_queue(DevScene s, FrameBuffers fb, int q, uint4* hits,
                                                         uint8_t* vis) {
   const uint32_t lane = threadIdx.x & 31;
@@ -252,12 +259,19 @@ __global__ void __launch_bounds__(kBlock) k_trace_queue(DevScene s, FrameBuffers
     if (i < count) {
       float4 o = qo[i], d = qd[i];
       uint32_t owner = __float_as_uint(d.w);
+      Visits vc;
       if (kAny) {
-        vis[owner] = trace_any(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w) ? 0 : 1;
+        vis[owner] = trace_any<kCount>(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, &vc) ? 0 : 1;
       } else {
         Hit h;
-        trace_closest(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, h);
+        trace_closest<kCount>(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, h, &vc);
         hits[owner] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.u), __float_as_uint(h.v), h.tri);
+      }
+      if (kCount) {
+        const int k = kAny ? K_TRACE_ANY : K_TRACE_CLOSEST;
+        atomicAdd(&fb.visits[3 * k + 0], 1ull);
+        atomicAdd(&fb.visits[3 * k + 1], (unsigned long long)vc.nodes);
+        atomicAdd(&fb.visits[3 * k + 2], (unsigned long long)vc.tris);
       }
     }
   }
@@ -1328,6 +1342,7 @@ size_t frame_buffer_bytes(uint32_t W, uint32_t H) {
   for (int i = 0; i < 5; ++i) add(P);       // visibility
   for (int i = 0; i < 4; ++i) add(P * 16);  // stage state
   add(64 * 4);                              // counters
+  add(3 * K_NUM_KINDS * 8);                 // visit counters
   add(P * 12);                              // out rgb
   (void)p;
   return n;
@@ -1386,6 +1401,7 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
   fb->st_c = carve<uint4>(p, P);
   fb->st_d = carve<uint4>(p, P);
   fb->counters = carve<uint32_t>(p, 64);
+  fb->visits = carve<unsigned long long>(p, 3 * K_NUM_KINDS);
   fb->out_rgb = carve<float>(p, 3 * P);
 }
 
@@ -1397,9 +1413,18 @@ const char* kernel_kind_name(int k) {
   return (k >= 0 && k < K_NUM_KINDS) ? names[k] : "?";
 }
 
+template <bool kAny>
+void trace_queue(bool counting, int blocks, cudaStream_t st, const DevScene& scene, const FrameBuffers& fb, int q,
+                 uint4* hits, uint8_t* vis) {
+  if (counting) k_trace_queue<kAny, true><<<blocks, kBlock, 0, st>>>(scene, fb, q, hits, vis);
+  else k_trace_queue<kAny, false><<<blocks, kBlock, 0, st>>>(scene, fb, q, hits, vis);
+}
+
 int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t st, FrameProfiler* prof) {
   int launches = 0;
+  const bool counting = prof && prof->count_visits;
+  if (counting) cudaMemsetAsync(fb.visits, 0, 3 * K_NUM_KINDS * sizeof(unsigned long long), st);
   if (prof) {
     prof->n = 0;
     cudaEventRecord(prof->ev[0], st);
@@ -1436,23 +1461,24 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       c.qout = (i + 1) & 1u;
       cudaMemsetAsync(fb.counters + 2, 0, 4, st);
       mark(K_MEMSET);
-      k_extend<<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
+      if (counting) k_extend<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
+      else k_extend<false><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_EXTEND);
       cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
       mark(K_MEMSET);
       k_shade_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c, mats);
       mark(K_SHADE);
-      k_trace_queue<false><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_BSDF_CAND, fb.hit_bsdf, nullptr);
+      trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_BSDF_CAND, fb.hit_bsdf, nullptr);
       mark(K_TRACE_CLOSEST);
       k_shade_b<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_SHADE);
-      k_trace_queue<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_RIS_SHADOW, nullptr, fb.vis[Q_RIS_SHADOW]);
+      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_RIS_SHADOW, nullptr, fb.vis[Q_RIS_SHADOW]);
       mark(K_TRACE_ANY);
-      k_trace_queue<false><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_GI_CAND, fb.hit_gi, nullptr);
+      trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_GI_CAND, fb.hit_gi, nullptr);
       mark(K_TRACE_CLOSEST);
       k_shade_c<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_SHADE);
-      k_trace_queue<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_GI_SHADOW, nullptr, fb.vis[Q_GI_SHADOW]);
+      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, nullptr, fb.vis[Q_GI_SHADOW]);
       mark(K_TRACE_ANY);
       k_shade_d<<<linear_blocks, kBlock, 0, st>>>(fb, c);
       mark(K_SHADE);
@@ -1511,7 +1537,7 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       }
       k_apply_di_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_APPLY_DI);
-      k_trace_queue<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, Q_DI_SHADOW, nullptr, fb.vis[Q_DI_SHADOW]);
+      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_DI_SHADOW, nullptr, fb.vis[Q_DI_SHADOW]);
       mark(K_TRACE_ANY);
       k_apply_di_b<<<linear_blocks, kBlock, 0, st>>>(fb, c);
       mark(K_APPLY_DI);

@@ -55,6 +55,7 @@ struct FrameBuffers {
   uint4 *st_a, *st_b, *st_c, *st_d;  // per-path state between shading stages
   uint32_t* counters;  // [0..1] path queue sizes, [2] extend cursor, [3] rays traced,
                        // [4..8] ray queue sizes, [9..13] ray queue cursors
+  unsigned long long* visits;  // instrumented traversal: per kernel kind {rays, nodes, tris}
   float* out_rgb;      // linear HDR output, 3 floats per pixel (device)
 };
 
@@ -91,6 +92,7 @@ struct FrameProfiler {
   int kind[kMax];
   int n = 0;
   bool created = false;
+  bool count_visits = false;  // use the visit-counting traversal kernels (fb.visits)
 };
 
 // Encodes one frame on `stream`.  `frame_idx` selects the ping-pong parity.

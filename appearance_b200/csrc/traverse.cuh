@@ -130,9 +130,15 @@ APD uint32_t node_children(const uint4 w0, const uint4 w2, const uint4 w3, const
 
 APD uint32_t meta_of(const uint4 w1, int i) { return ((i < 4 ? w1.z : w1.w) >> (8 * (i & 3))) & 0xffu; }
 
+// Visit counters of one ray (instrumented builds of the traversal kernels).
+struct Visits {
+  uint32_t nodes = 0, tris = 0;
+};
+
 // Closest hit in [0, tmax] (returns false on miss).  Tie rule: smaller t, then
 // smaller global triangle id.
-APD bool trace_closest(const DevScene& s, float3 o, float3 d, float tmax, Hit& hit) {
+template <bool kCount = false>
+APD bool trace_closest(const DevScene& s, float3 o, float3 d, float tmax, Hit& hit, Visits* vc = nullptr) {
   RayPre r = ray_pre(o, d);
   hit.t = tmax;
   hit.u = 0.0f;
@@ -150,6 +156,7 @@ APD bool trace_closest(const DevScene& s, float3 o, float3 d, float tmax, Hit& h
       node = e.x;
     }
     have = false;
+    if (kCount) vc->nodes++;
     const uint4* np = s.nodes + 5 * (size_t)node;
     uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
           w4 = __ldg(np + 4);
@@ -164,6 +171,7 @@ APD bool trace_closest(const DevScene& s, float3 o, float3 d, float tmax, Hit& h
       if ((meta & 0xe0u) == 0) continue;
       uint32_t first = w1.y + (meta & 0x1fu);
       uint32_t cnt = __popc(meta >> 5);
+      if (kCount) vc->tris += cnt;
       for (uint32_t k = 0; k < cnt; ++k) {
         const float4* tp = s.tris + 3 * (size_t)(first + k);
         float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
@@ -209,7 +217,8 @@ APD bool trace_closest(const DevScene& s, float3 o, float3 d, float tmax, Hit& h
 // Any hit in [0, tmax] (shadow rays: terminate on first hit).  Same stack
 // discipline as trace_closest (continue with one inner child, push the rest),
 // so the build-time bound on stack depth (BvhStats::max_stack) covers both.
-APD bool trace_any(const DevScene& s, float3 o, float3 d, float tmax) {
+template <bool kCount = false>
+APD bool trace_any(const DevScene& s, float3 o, float3 d, float tmax, Visits* vc = nullptr) {
   RayPre r = ray_pre(o, d);
   uint32_t stack[kTraversalStack];
   int sp = 0;
@@ -221,6 +230,7 @@ APD bool trace_any(const DevScene& s, float3 o, float3 d, float tmax) {
       node = stack[--sp];
     }
     have = false;
+    if (kCount) vc->nodes++;
     const uint4* np = s.nodes + 5 * (size_t)node;
     uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
           w4 = __ldg(np + 4);
@@ -238,6 +248,7 @@ APD bool trace_any(const DevScene& s, float3 o, float3 d, float tmax) {
           const float4* tp = s.tris + 3 * (size_t)(first + k);
           float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
           float t, u, v;
+          if (kCount) vc->tris++;
           if (intersect_tri(r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), 0.0f, tmax, t, u, v))
             return true;
         }

@@ -154,16 +154,22 @@ class PathTracer:
         self._check(self._lib.ap_read_buffer(self._h, which, _ptr(out), out.nbytes))
         return out
 
-    def profile_frame(self, width: int, height: int) -> dict:
-        """Renders one frame with per-kernel events; returns {kind: (ms, launches)}."""
+    def profile_frame(self, width: int, height: int, count_visits: bool = False) -> dict:
+        """Renders one frame with per-kernel events.  Returns {kind: dict(ms, launches,
+        rays, nodes, tris)}; rays/nodes/tris are filled for the traversal kernels
+        when count_visits (instrumented kernels, times then not representative)."""
         n = 32
         ms = np.zeros(n, np.float64)
         cnt = np.zeros(n, np.uint32)
         names = (ctypes.c_char_p * n)()
         nk = np.zeros(1, np.uint32)
+        visits = np.zeros(3 * n, np.uint64)
         self._check(self._lib.ap_profile_frame(self._h, width, height, _ptr(ms), _ptr(cnt), names, n, _ptr(nk),
+                                               1 if count_visits else 0, _ptr(visits),
                                                ctypes.byref(self.last_stats)))
-        return {names[i].decode(): (float(ms[i]), int(cnt[i])) for i in range(int(nk[0]))}
+        return {names[i].decode(): dict(ms=float(ms[i]), launches=int(cnt[i]), rays=int(visits[3 * i]),
+                                        nodes=int(visits[3 * i + 1]), tris=int(visits[3 * i + 2]))
+                for i in range(int(nk[0]))}
 
     def bvh_stats(self) -> dict:
         out = np.zeros(8, np.uint32)

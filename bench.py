@@ -3,9 +3,9 @@
 Workload (one step = one frame): the seeded 1,310,722-triangle icosphere field
 (1024 icospheres x 1280 triangles + ground quad, 64 emissive spheres, 2048x1024
 procedural sky), 1920x1080, 1 spp, depth 8, ReSTIR DI (32 area candidates,
-temporal M cap 20x, 5-neighbour spatial), ReSTIR GI (temporal + 5-neighbour
-spatial), firefly filter, SVGF (5 a-trous passes), TAA, camera moving along a
-64-frame seeded spline.  Metric: Msamples/s (= pixels x spp / frame time).
+temporal M cap 20x, 5-neighbour spatial), ReSTIR GI (temporal; its spatial pass
+is off as in the reference, lib.rs:441), firefly filter, SVGF (5 a-trous
+passes), TAA, camera moving along a 64-frame seeded spline.  Metric: Msamples/s (= pixels x spp / frame time).
 
   value   device time of the frames (CUDA events on the renderer's stream),
           scene and frame state resident in HBM.
@@ -273,7 +273,9 @@ def main():
             "clocks": clk,
             "gpu_launches": None,
         }
-        line.update(measure_details(pt, scene, path, cfg))
+        details = measure_details(pt, scene, path, cfg)
+        line.update(details)
+        line["gpu_launches"] = int(details["gpu_launches_per_step"]) * args.steps
         if world == 1 and args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(scene, path, cfg)
         print(json.dumps(line), flush=True)

@@ -171,9 +171,13 @@ int ap_read_buffer(void* handle, uint32_t which, uint32_t* out, size_t out_bytes
  * an event after every launch, and returns the device milliseconds and the
  * launch count of each kernel kind: kind_ms and kind_count hold `max_kinds`
  * entries; names[i] receives a static string naming kind i; *num_kinds the
- * number of kinds written. */
+ * number of kinds written.  With count_visits != 0 the traversal kernels run
+ * in their instrumented form (slower; times are then not representative) and
+ * visits[3*i .. 3*i+2] receives {rays, BVH nodes visited, triangles tested}
+ * of kind i. */
 int ap_profile_frame(void* handle, uint32_t w, uint32_t h, double* kind_ms, uint32_t* kind_count,
-                     const char** names, uint32_t max_kinds, uint32_t* num_kinds, ap_frame_stats* stats);
+                     const char** names, uint32_t max_kinds, uint32_t* num_kinds, int count_visits,
+                     uint64_t* visits, ap_frame_stats* stats);
 
 /* BVH statistics of the uploaded scene: nodes, triangles, max depth, max
  * traversal stack, build ms (as double bits in out[4..5]). */

@@ -69,6 +69,7 @@ def lib():
         L.orc_hash_combine.restype = U
         L.orc_hash_combine.argtypes = [U, U]
         L.orc_disney.argtypes = [P] * 7
+        L.orc_detmath.argtypes = [U, P, P, P, U]
         _lib = L
     return _lib
 
@@ -144,3 +145,45 @@ class OracleFrame:
         if getattr(self, "ptr", None):
             lib().orc_frame_free(self.ptr)
             self.ptr = None
+
+
+DETMATH = dict(sin=0, cos=1, exp=2, log=3, pow=4, atan2=5, acos=6)
+
+
+def detmath(fn: str, x, y=None) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float32)
+    yy = None if y is None else np.ascontiguousarray(y, np.float32)
+    out = np.zeros_like(x)
+    lib().orc_detmath(DETMATH[fn], _p(x), _p(yy), _p(out), x.size)
+    return out
+
+
+def rgb9e5_pack(rgb) -> int:
+    a = np.ascontiguousarray(rgb, np.float32)
+    return int(lib().orc_rgb9e5_pack(_p(a)))
+
+
+def rgb9e5_unpack(d: int) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    lib().orc_rgb9e5_unpack(int(d), _p(out))
+    return out
+
+
+def oct30_pack(v) -> int:
+    a = np.ascontiguousarray(v, np.float32)
+    return int(lib().orc_oct30_pack(_p(a)))
+
+
+def oct30_unpack(p: int) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    lib().orc_oct30_unpack(int(p), _p(out))
+    return out
+
+
+def disney(mat, n, wo, wi, r):
+    """Disney evaluate (rgb, pdf) and sample (rgb, pdf, wi) at a point with normal n."""
+    e = np.zeros(4, np.float32)
+    smp = np.zeros(7, np.float32)
+    args = [np.ascontiguousarray(a, np.float32) for a in (mat, n, wo, wi, r)]
+    lib().orc_disney(*[_p(a) for a in args], _p(e), _p(smp))
+    return e, smp

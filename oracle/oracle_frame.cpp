@@ -1257,3 +1257,21 @@ void orc_disney(const float* mat, const float* n3, const float* wo3, const float
 }
 
 }  // extern "C"
+
+// Elementary functions of detmath.h, for the accuracy tests.
+extern "C" void orc_detmath(uint32_t fn, const float* x, const float* y, float* out, uint32_t n) {
+  for (uint32_t i = 0; i < n; ++i) {
+    float a = x[i], b = y ? y[i] : 0.0f, r = 0.0f;
+    switch (fn) {
+      case 0: r = dm::sin_(a); break;
+      case 1: r = dm::cos_(a); break;
+      case 2: r = dm::exp_(a); break;
+      case 3: r = dm::log_(a); break;
+      case 4: r = dm::pow_(a, b); break;
+      case 5: r = dm::atan2_(a, b); break;
+      case 6: r = dm::acos_(a); break;
+      default: r = 0.0f; break;
+    }
+    out[i] = r;
+  }
+}
