@@ -558,6 +558,11 @@ int ap_read_buffer(void* hp, uint32_t which, uint32_t* out, size_t out_bytes) {
     case 4: parts = {{h->fb.gi_a, 16}, {h->fb.gi_b, 16}}; words = 8; break;
     case 5: parts = {{h->fb.ctx, 16}}; words = 4; break;
     case 7: parts = {{h->fb.rays, 16}}; words = 4; break;
+    case 8: parts = {{h->fb.hit_bsdf, 16}}; words = 4; break;
+    case 9: parts = {{h->fb.hit_gi, 16}}; words = 4; break;
+    case 10: parts = {{h->fb.rq_o[Q_GI_CAND], 16}, {h->fb.rq_d[Q_GI_CAND], 16}}; words = 8; break;
+    case 11: parts = {{h->fb.st_a, 16}, {h->fb.st_b, 16}}; words = 8; break;
+    case 12: parts = {{h->fb.st_c, 16}, {h->fb.st_d, 16}}; words = 8; break;
     default: return fail(h, AP_E_INVALID, "unknown buffer");
   }
   if (out_bytes < P * words * 4) return fail(h, AP_E_INVALID, "output buffer too small");

@@ -30,7 +30,8 @@ struct RayPre {
   float3 o, d;
   int kx, ky, kz;
   float sx, sy, sz;
-  float3 inv;  // box-test reciprocal direction (zero components replaced)
+  float3 inv;          // box-test reciprocal direction (0 where the component is 0)
+  uint32_t zero_axes;  // bit k: direction component k is +-0
 };
 
 APD float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
@@ -54,15 +55,14 @@ APD RayPre ray_pre(float3 o, float3 d) {
   r.sx = comp(d, kx) / dz;
   r.sy = comp(d, ky) / dz;
   r.sz = 1.0f / dz;
-  const float tiny = 1e-20f;
-  float dx = dm::fabs_(d.x) < tiny ? copysignf(tiny, d.x) : d.x;
-  float dy = dm::fabs_(d.y) < tiny ? copysignf(tiny, d.y) : d.y;
-  float dzz = dm::fabs_(d.z) < tiny ? copysignf(tiny, d.z) : d.z;
-  r.inv = f3(1.0f / dx, 1.0f / dy, 1.0f / dzz);
+  r.zero_axes = (d.x == 0.0f ? 1u : 0u) | (d.y == 0.0f ? 2u : 0u) | (d.z == 0.0f ? 4u : 0u);
+  r.inv = f3(d.x == 0.0f ? 0.0f : 1.0f / d.x, d.y == 0.0f ? 0.0f : 1.0f / d.y, d.z == 0.0f ? 0.0f : 1.0f / d.z);
   return r;
 }
 
-// Watertight test; same expressions as the oracle (intersect_tri).
+// Watertight inside test and barycentrics in binary32 (Woop, Benthin, Wald,
+// JCGT 2013), distance t in double from the original vertices; same
+// expressions as the oracle (intersect_tri).
 APD bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float tmin, float tmax,
                        float& t, float& u, float& v) {
   float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
@@ -81,11 +81,17 @@ APD bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float t
   if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
   float det = U + V + W;
   if (det == 0.0f) return false;
-  float Az = r.sz * Akz, Bz = r.sz * Bkz, Cz = r.sz * Ckz;
-  float T = U * Az + V * Bz + W * Cz;
+  // distance along the ray in double precision from the original vertices, only
+  // for candidates that passed the inside test (one or two per ray)
+  double e1x = (double)v1.x - v0.x, e1y = (double)v1.y - v0.y, e1z = (double)v1.z - v0.z;
+  double e2x = (double)v2.x - v0.x, e2y = (double)v2.y - v0.y, e2z = (double)v2.z - v0.z;
+  double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+  double wx = (double)v0.x - r.o.x, wy = (double)v0.y - r.o.y, wz = (double)v0.z - r.o.z;
+  double td = (nx * wx + ny * wy + nz * wz) / (nx * r.d.x + ny * r.d.y + nz * r.d.z);
+  if (!(td >= (double)tmin)) return false;
+  float tt = (float)td;
+  if (!(tt <= tmax)) return false;
   float rcp = 1.0f / det;
-  float tt = T * rcp;
-  if (!(tt >= tmin && tt <= tmax)) return false;
   t = tt;
   u = V * rcp;
   v = W * rcp;
@@ -95,9 +101,19 @@ APD bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float t
 APD float byte_f(uint32_t word, int k) { return __uint2float_rn((word >> (8 * k)) & 0xffu); }
 
 // Box tests of the 8 children of one node.  Returns the hit mask; tnear[] gets
-// the entry distance of each hit child.  Bounds are widened by a relative
-// 2^-21 so that no child containing a triangle hit inside [tmin, tmax] is culled
-// by rounding in the slab arithmetic.
+// the entry distance of each hit child.
+//
+// Conservativeness: a slab value is computed as fma(q, s/d, (p - o)/d) with the
+// power-of-two scale s exact.  Its error is at most 3 ulp of |(p - o)/d| (the
+// rounding of p - o, of the product and of the fma, which can cancel against
+// q*s/d) plus a relative error of 1/d itself.  The watertight inside test may
+// accept a hit point outside the exact triangle by a few ulp of the vertex
+// distances from the origin.  Each slab is therefore widened by 2^-19 of
+// (|p - o| + node extent)/|d| and each interval by a relative 2^-21, so no child
+// that holds a triangle accepted inside [tmin, tmax] is culled.  For a zero direction
+// component the slab is all of t when the origin lies inside the child's
+// bounds decoded as p + q*s (rounded to nearest, which never shrinks the
+// conservatively quantised box), and empty otherwise.
 template <bool kClosest>
 APD uint32_t node_children(const uint4 w0, const uint4 w2, const uint4 w3, const uint4 w4,
                            const RayPre& r, float tmin, float tmax, float tnear[8]) {
@@ -107,6 +123,11 @@ APD uint32_t node_children(const uint4 w0, const uint4 w2, const uint4 w3, const
   float szs = __uint_as_float(((w0.w >> 16) & 0xffu) << 23);
   float ax = sxs * r.inv.x, ay = sys * r.inv.y, az = szs * r.inv.z;
   float bx = (px - r.o.x) * r.inv.x, by = (py - r.o.y) * r.inv.y, bz = (pz - r.o.z) * r.inv.z;
+  // slab slack: 2^-19 of the node's distance scale from the origin, |p - o| plus
+  // the node extent (255 quanta), along the axis
+  const float kSlack = 1.9073486e-06f;  // 2^-19
+  float ex = (fabsf(bx) + 255.0f * fabsf(ax)) * kSlack, ey = (fabsf(by) + 255.0f * fabsf(ay)) * kSlack,
+        ez = (fabsf(bz) + 255.0f * fabsf(az)) * kSlack;
   const float grow = 1.0f + 4.8e-7f;
   uint32_t mask = 0;
 #pragma unroll
@@ -118,8 +139,29 @@ APD uint32_t node_children(const uint4 w0, const uint4 w2, const uint4 w3, const
     float x0 = fmaf(byte_f(lox, k), ax, bx), x1 = fmaf(byte_f(hix, k), ax, bx);
     float y0 = fmaf(byte_f(loy, k), ay, by), y1 = fmaf(byte_f(hiy, k), ay, by);
     float z0 = fmaf(byte_f(loz, k), az, bz), z1 = fmaf(byte_f(hiz, k), az, bz);
-    float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-    float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fmaxf(z0, z1));
+    float lx = fminf(x0, x1) - ex, hx = fmaxf(x0, x1) + ex;
+    float ly = fminf(y0, y1) - ey, hy = fmaxf(y0, y1) + ey;
+    float lz = fminf(z0, z1) - ez, hz = fmaxf(z0, z1) + ez;
+    if (r.zero_axes) {
+      const float inf = __uint_as_float(0x7f800000u);
+      if (r.zero_axes & 1u) {
+        bool in = r.o.x >= px + byte_f(lox, k) * sxs && r.o.x <= px + byte_f(hix, k) * sxs;
+        lx = in ? -inf : inf;
+        hx = in ? inf : -inf;
+      }
+      if (r.zero_axes & 2u) {
+        bool in = r.o.y >= py + byte_f(loy, k) * sys && r.o.y <= py + byte_f(hiy, k) * sys;
+        ly = in ? -inf : inf;
+        hy = in ? inf : -inf;
+      }
+      if (r.zero_axes & 4u) {
+        bool in = r.o.z >= pz + byte_f(loz, k) * szs && r.o.z <= pz + byte_f(hiz, k) * szs;
+        lz = in ? -inf : inf;
+        hz = in ? inf : -inf;
+      }
+    }
+    float tn = fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin));
+    float tf = fminf(fminf(hx, hy), hz);
     tf = tf * (tf > 0.0f ? grow : 1.0f / grow);
     tn = tn * (tn > 0.0f ? 1.0f / grow : grow);
     tnear[i] = tn;

@@ -164,7 +164,9 @@ int ap_trace_rays(void* handle, const float* origins_tmax, const float* dirs, ui
 /* Copies a per-pixel state buffer of the last frame to the host, for
  * stage-by-stage comparisons: 0 radiance (1 word), 1 payload (4), 2 current
  * G-buffer (8), 3 DI reservoirs (8), 4 GI reservoirs (8), 5 light-sample
- * context (4), 7 rays (4). */
+ * context (4), 7 rays (4); working buffers of the last bounce that used them:
+ * 8 BSDF-candidate hits (4), 9 GI-candidate hits (4), 10 GI-candidate ray
+ * queue (8: origin+tmax, direction+owner), 11 and 12 shading-stage state (8). */
 int ap_read_buffer(void* handle, uint32_t which, uint32_t* out, size_t out_bytes);
 
 /* Renders one frame (advancing the frame sequence like ap_render_device) with

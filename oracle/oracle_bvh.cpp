@@ -137,8 +137,10 @@ void OracleBvh::build(const Scene& s) {
 }
 
 namespace {
-// Slab test in double with a relative widening, so that every triangle whose
-// binary32 watertight test succeeds inside [tmin, tmax] lies in an accepted box.
+// Slab test in double, widened per slab by 2^-19 of the distance scale of the
+// box from the origin (|lo - o| + |hi - o|) / |d| and by a relative 1e-6, so that
+// every triangle that the watertight test accepts inside [tmin, tmax] (whose
+// inside test rounds at the scale of the vertex distances) lies in an accepted box.
 inline bool box_hit(const float* lo, const float* hi, const double* o, const double* inv,
                     double tmin, double tmax) {
   double t0 = tmin, t1 = tmax;
@@ -147,8 +149,10 @@ inline bool box_hit(const float* lo, const float* hi, const double* o, const dou
     double b = (hi[k] - o[k]) * inv[k];
     if (a > b) std::swap(a, b);
     if (std::isnan(a) || std::isnan(b)) continue;  // ray parallel and on a slab plane
-    a = a - 1e-6 * std::fabs(a) - 1e-12;
-    b = b + 1e-6 * std::fabs(b) + 1e-12;
+    double slack = (std::fabs(a) + std::fabs(b)) * 1.9073486328125e-06 + 1e-12;
+    if (std::isinf(slack)) continue;
+    a = a - 1e-6 * std::fabs(a) - slack;
+    b = b + 1e-6 * std::fabs(b) + slack;
     t0 = std::max(t0, a);
     t1 = std::min(t1, b);
   }

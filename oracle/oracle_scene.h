@@ -74,9 +74,11 @@ struct Hit {
 };
 
 // Watertight ray/triangle intersection (S. Woop, C. Benthin, I. Wald,
-// "Watertight Ray/Triangle Intersection", JCGT 2(1) 2013) in binary32 with the
-// double-precision fallback for zero edge functions.  Returns true and fills
-// t, u (weight of v1), v (weight of v2) when tmin <= t <= tmax.
+// "Watertight Ray/Triangle Intersection", JCGT 2(1) 2013): the inside test and
+// the barycentrics in binary32 with the double-precision fallback for zero
+// edge functions; the distance t in double precision from the original
+// vertices (plane distance), rounded once.  Returns true and fills t, u (weight
+// of v1), v (weight of v2) when tmin <= t <= tmax.
 struct RayPre {
   V3 o, d;
   int kx, ky, kz;
@@ -119,11 +121,17 @@ inline bool intersect_tri(const RayPre& r, V3 v0, V3 v1, V3 v2, float tmin, floa
   if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
   float det = U + V + W;
   if (det == 0.0f) return false;
-  float Az = r.sz * Akz, Bz = r.sz * Bkz, Cz = r.sz * Ckz;
-  float T = U * Az + V * Bz + W * Cz;
+  // distance along the ray in double precision from the original vertices
+  // (accurate where the float sheared form loses sign for hits near t = 0)
+  double e1x = (double)v1.x - v0.x, e1y = (double)v1.y - v0.y, e1z = (double)v1.z - v0.z;
+  double e2x = (double)v2.x - v0.x, e2y = (double)v2.y - v0.y, e2z = (double)v2.z - v0.z;
+  double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+  double wx = (double)v0.x - r.o.x, wy = (double)v0.y - r.o.y, wz = (double)v0.z - r.o.z;
+  double td = (nx * wx + ny * wy + nz * wz) / (nx * r.d.x + ny * r.d.y + nz * r.d.z);
+  if (!(td >= (double)tmin)) return false;
+  float tt = (float)td;
+  if (!(tt <= tmax)) return false;
   float rcp = 1.0f / det;
-  float tt = T * rcp;
-  if (!(tt >= tmin && tt <= tmax)) return false;
   t = tt;
   u = V * rcp;
   v = W * rcp;
