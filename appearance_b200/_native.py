@@ -15,7 +15,8 @@ AP_OK, AP_E_INVALID, AP_E_OOM, AP_E_CUDA, AP_E_TIMEOUT, AP_E_UNSUPPORTED, AP_E_N
 
 EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error", "ap_set_config",
            "ap_world_action", "ap_scene_upload", "ap_set_camera_matrices", "ap_render_hdr", "ap_render_device",
-           "ap_device_framebuffer", "ap_trace_rays", "ap_read_buffer", "ap_profile_frame", "ap_bvh_stats"]
+           "ap_device_framebuffer", "ap_trace_rays", "ap_trace_rays_static", "ap_read_buffer", "ap_profile_frame",
+           "ap_bvh_stats"]
 
 U32, F32, P = ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p
 
@@ -71,6 +72,7 @@ def load() -> ctypes.CDLL:
     L.ap_device_framebuffer.restype = P
     L.ap_device_framebuffer.argtypes = [P]
     L.ap_trace_rays.argtypes = [P, P, P, U32, ctypes.c_int, P]
+    L.ap_trace_rays_static.argtypes = [P, P, P, U32, ctypes.c_int, P]
     L.ap_read_buffer.argtypes = [P, U32, P, ctypes.c_size_t]
     L.ap_bvh_stats.argtypes = [P, P]
     L.ap_profile_frame.argtypes = [P, U32, U32, P, P, P, U32, P, ctypes.c_int, P, ctypes.POINTER(FrameStats)]

@@ -229,6 +229,26 @@ int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats, Fr
 
 }  // namespace
 
+namespace ap {
+// Scene, stream and error slot of a handle, for entry points defined in other
+// translation units (noalloc.cu).  Returns AP_E_NO_SCENE when no scene is loaded.
+int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream, int* num_sms, int* device,
+                         std::string** err) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  *err = &h->err;
+  if (!h->scene.valid) {
+    h->err = "no scene uploaded";
+    return AP_E_NO_SCENE;
+  }
+  *scene = &h->scene.view;
+  *stream = h->stream;
+  *num_sms = h->num_sms;
+  *device = h->device;
+  return AP_OK;
+}
+}  // namespace ap
+
 extern "C" {
 
 void ap_frame_config_default(ap_frame_config* c) {

@@ -161,6 +161,18 @@ const float* ap_device_framebuffer(const void* handle);
 int ap_trace_rays(void* handle, const float* origins_tmax, const float* dirs, uint32_t n, int any_hit,
                   uint32_t* out4);
 
+/* The query of ap_trace_rays for callers that cannot allocate device memory
+ * (a host that owns the whole device-memory budget, or a thread that cannot
+ * take cudaMalloc's device-wide synchronisation).  It has no counterpart in the
+ * reference.  It allocates nothing: its device staging is a fixed static array
+ * of the library, so n is at most 65536 rays per call (AP_E_INVALID above
+ * that).  All calls on a device share that array: calls that overlap on the
+ * GPU race, so serialise them.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Same buffers and results as ap_trace_rays. */
+int ap_trace_rays_static(void* handle, const float* origins_tmax, const float* dirs, uint32_t n, int any_hit,
+                         uint32_t* out4);
+
 /* Copies a per-pixel state buffer of the last frame to the host, for
  * stage-by-stage comparisons: 0 radiance (1 word), 1 payload (4), 2 current
  * G-buffer (8), 3 DI reservoirs (8), 4 GI reservoirs (8), 5 light-sample
