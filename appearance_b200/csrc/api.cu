@@ -10,6 +10,7 @@
 #include "../../include/appearance_cuda.h"
 #include "bvh_build.h"
 #include "dev_common.cuh"
+#include "dev_shade.cuh"
 #include "frame.cuh"
 #include "traverse.cuh"
 
@@ -32,13 +33,16 @@ struct DeviceScene {
   void* materials = nullptr;
   void* emissive_instances = nullptr;
   void* emissive_cdf = nullptr;
+  void* emissive_tris = nullptr;
+  void* emissive_tri_base = nullptr;
   void* env = nullptr;
   DevScene view{};
   BvhStats stats{};
   bool valid = false;
   void release() {
     void** all[] = {&nodes, &tris, &positions, &normals, &indices, &tri_material, &tri_instance,
-                    &instances, &materials, &emissive_instances, &emissive_cdf, &env};
+                    &instances, &materials, &emissive_instances, &emissive_cdf, &emissive_tris,
+                    &emissive_tri_base, &env};
     for (void** p : all) {
       if (*p) cudaFree(*p);
       *p = nullptr;
@@ -92,6 +96,32 @@ int upload(Handle* h, void** dst, const T* src, size_t count) {
   if (rc) return rc;
   if (count) rc = check_cuda(h, cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice), "upload");
   return rc;
+}
+
+// Fills the emissive-triangle table (run once per scene upload).
+__global__ void k_build_emissive_tris(DevScene s, EmissiveTri* out, uint32_t total) {
+  uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  uint32_t lo = 0, hi = s.num_emissive_instances;  // instance whose range holds g
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (s.emissive_tri_base[mid] <= g) lo = mid;
+    else hi = mid;
+  }
+  const InstanceDev in = s.instances[s.emissive_instances[lo]];
+  uint32_t tri = g - s.emissive_tri_base[lo];
+  float3 p0, p1, p2;
+  tri_positions(s, in, tri, &p0, &p1, &p2);
+  float3 cr = cross(p1 - p0, p2 - p0);
+  float3 n = normalize(cr);
+  const MaterialDev* m = s.materials + in.material_idx + s.tri_material[in.first_index / 3 + tri];
+  EmissiveTri e;
+  e.p0[0] = p0.x; e.p0[1] = p0.y; e.p0[2] = p0.z; e.area = len(cr) * 0.5f;
+  e.p1[0] = p1.x; e.p1[1] = p1.y; e.p1[2] = p1.z; e.pad0 = 0.0f;
+  e.p2[0] = p2.x; e.p2[1] = p2.y; e.p2[2] = p2.z; e.pad1 = 0.0f;
+  e.n[0] = n.x; e.n[1] = n.y; e.n[2] = n.z; e.pad2 = 0.0f;
+  e.emission[0] = m->emission[0]; e.emission[1] = m->emission[1]; e.emission[2] = m->emission[2]; e.pad3 = 0.0f;
+  out[g] = e;
 }
 
 __global__ void k_pack_normals(const float* n, uint32_t count, uint32_t* out) {
@@ -423,6 +453,14 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
       }
     }
   }
+  std::vector<uint32_t> tri_base;
+  {
+    uint32_t b = 0;
+    for (uint32_t e : emissive) {
+      tri_base.push_back(b);
+      b += inst[e].num_indices / 3;
+    }
+  }
   std::vector<float> cdf;
   float acc = 0.0f;
   for (uint32_t e : emissive) {
@@ -451,7 +489,10 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
       (rc = upload(h, &s.instances, inst.data(), inst.size())) ||
       (rc = upload(h, &s.materials, reinterpret_cast<const MaterialDev*>(d->materials), d->num_materials)) ||
       (rc = upload(h, &s.emissive_instances, emissive.data(), emissive.size())) ||
-      (rc = upload(h, &s.emissive_cdf, cdf.data(), cdf.size()))) {
+      (rc = upload(h, &s.emissive_cdf, cdf.data(), cdf.size())) ||
+      (rc = upload(h, &s.emissive_tri_base, tri_base.data(), tri_base.size())) ||
+      (rc = check_cuda(h, cudaMalloc(&s.emissive_tris, std::max<size_t>(sizeof(EmissiveTri) * num_emissive_tris, 16)),
+                       "emissive triangles"))) {
     if (nrm_f) cudaFree(nrm_f);
     s.release();
     return rc;
@@ -490,6 +531,17 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
   v.env_h = s.env ? d->env_h : 0;
   std::memcpy(&v.sun, d->sun, sizeof(SunDev));
   v.num_tris = d->num_tris;
+  v.emissive_tri_base = static_cast<const uint32_t*>(s.emissive_tri_base);
+  v.emissive_tris = static_cast<const EmissiveTri*>(s.emissive_tris);
+  if (num_emissive_tris) {
+    k_build_emissive_tris<<<(num_emissive_tris + 255) / 256, 256, 0, h->stream>>>(
+        v, static_cast<EmissiveTri*>(s.emissive_tris), num_emissive_tris);
+    rc = check_cuda(h, cudaStreamSynchronize(h->stream), "emissive triangles");
+    if (rc) {
+      s.release();
+      return rc;
+    }
+  }
   s.stats = bvh.stats;
   s.valid = true;
   return AP_OK;

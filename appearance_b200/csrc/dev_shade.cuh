@@ -567,20 +567,32 @@ APD LightEval load_eval(const DevScene& s, const LightSample& l, float3 hit) {
     return LightEval{sun_intensity(s.sun, dir) * ld3(s.sun.color), dir * 1e6f};
   }
   if (l.inst >= s.num_emissive_instances) return LightEval{f3s(0.0f), f3s(0.0f)};
-  const InstanceDev in = s.instances[s.emissive_instances[l.inst]];
-  uint32_t ntri = in.num_indices / 3;
-  uint32_t tri = l.tri < ntri ? l.tri : ntri - 1;
-  float3 p0, p1, p2;
-  tri_positions(s, in, tri, &p0, &p1, &p2);
+  const uint32_t ntri = s.instances[s.emissive_instances[l.inst]].num_indices / 3;
+  const uint32_t tri = l.tri < ntri ? l.tri : ntri - 1;
+  const EmissiveTri* et = s.emissive_tris + s.emissive_tri_base[l.inst] + tri;
+  const float4* q = reinterpret_cast<const float4*>(et);
+  float4 a = __ldg(q + 0), b = __ldg(q + 1), c = __ldg(q + 2), nn = __ldg(q + 3), em = __ldg(q + 4);
+  float3 p0 = f3(a.x, a.y, a.z), p1 = f3(b.x, b.y, b.z), p2 = f3(c.x, c.y, c.z);
   float bx = 1.0f - l.uv.x - l.uv.y;
   float3 point = p0 * bx + p1 * l.uv.x + p2 * l.uv.y;
   float3 dir = normalize(point - hit);
   float dd = dist(point, hit);
-  float3 tn = normalize(cross(p1 - p0, p2 - p0));
-  const MaterialDev* m = s.materials + in.material_idx + s.tri_material[in.first_index / 3 + tri];
-  float cos_out = dm::fmax(-dot(tn, dir), 0.0f);
+  float cos_out = dm::fmax(-dot(f3(nn.x, nn.y, nn.z), dir), 0.0f);
   float sa = dm::fmin(kTwoPi, cos_out / (sqr(dd) + 0.0001f));
-  return LightEval{ld3(m->emission) * sa * 10.0f, point};
+  return LightEval{f3(em.x, em.y, em.z) * sa * 10.0f, point};
+}
+
+// First emissive instance whose CDF entry is >= r (the reference scans
+// linearly, nee.wgsl:60-61; the CDF is non-decreasing, so the binary search
+// returns the same index), or num_emissive_instances when there is none.
+APD uint32_t cdf_search(const DevScene& s, float r) {
+  uint32_t lo = 0, hi = s.num_emissive_instances;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (r <= __ldg(s.emissive_cdf + mid)) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
 }
 
 APD LightSample sample_uniform(const DevScene& s, float r0, float r1, float r2, float2 r34, float* pdf) {
@@ -589,20 +601,16 @@ APD LightSample sample_uniform(const DevScene& s, float r0, float r1, float r2, 
     *pdf = sun_p;
     return LightSample{r34, kU32Max - 1, 0};
   }
-  for (uint32_t i = 0; i < s.num_emissive_instances; ++i) {
-    if (r1 <= s.emissive_cdf[i]) {
-      const InstanceDev in = s.instances[s.emissive_instances[i]];
-      uint32_t ntri = in.num_indices / 3;
-      uint32_t local = dm::f2u(r2 * (float)ntri);
-      if (local >= ntri) local = ntri - 1;
-      float3 p0, p1, p2;
-      tri_positions(s, in, local, &p0, &p1, &p2);
-      float area = len(cross(p1 - p0, p2 - p0)) * 0.5f;
-      float p = 1.0f / (float)s.num_emissive_tris;
-      p = p / area;
-      *pdf = dm::fmax(1e-6f, p * (1.0f - sun_p));
-      return LightSample{r34, i, local};
-    }
+  uint32_t i = cdf_search(s, r1);
+  if (i < s.num_emissive_instances) {
+    uint32_t ntri = s.instances[s.emissive_instances[i]].num_indices / 3;
+    uint32_t local = dm::f2u(r2 * (float)ntri);
+    if (local >= ntri) local = ntri - 1;
+    float area = __ldg(&s.emissive_tris[s.emissive_tri_base[i] + local].area);
+    float p = 1.0f / (float)s.num_emissive_tris;
+    p = p / area;
+    *pdf = dm::fmax(1e-6f, p * (1.0f - sun_p));
+    return LightSample{r34, i, local};
   }
   *pdf = 0.0f;
   return ls_empty();

@@ -169,6 +169,55 @@ APD void mul4(const float* m, float v0, float v1, float v2, float v3, float out[
   for (int r = 0; r < 4; ++r) out[r] = m[r] * v0 + m[4 + r] * v1 + m[8 + r] * v2 + m[12 + r] * v3;
 }
 
+// Persistent traversal with per-lane refill: a lane that finishes its ray
+// takes the next one through a warp-aggregated atomic on `cursor`, so warps
+// stay full until the batch drains.  Lanes check for a refill every
+// kStepBudget visited nodes.  load(i, o, d, tmax) fetches ray i,
+// store(i, trav, visits) writes its result.  The traversal kernels run with
+// the child tests unrolled and are register-capped for 6 resident blocks of
+// kBlock threads per SM (the best of the measured 1..8 on the benchmark scene).
+constexpr int kStepBudget = 16;
+constexpr int kTraceMinBlocks = 6;
+
+template <bool kAny, bool kCount, class Load, class Store>
+APD void persistent_trace(const DevScene& s, uint32_t count, uint32_t* cursor, Load load, Store store) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint2 stack[kTraversalStack];
+  Trav t;
+  Visits vc;
+  uint32_t cur = 0;
+  bool active = false, exhausted = false;
+  while (true) {
+    if (!exhausted) {
+      const unsigned need = __ballot_sync(0xffffffffu, !active);
+      if (need) {
+        const int leader = __ffs(need) - 1;
+        uint32_t base = 0;
+        if ((int)lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(need));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (base + (uint32_t)__popc(need) >= count) exhausted = true;
+        if (!active) {
+          const uint32_t idx = base + __popc(need & ((1u << lane) - 1u));
+          if (idx < count) {
+            float3 o, d;
+            float tmax;
+            load(idx, o, d, tmax);
+            trav_init(t, o, d, tmax);
+            vc = Visits();
+            cur = idx;
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    if (active && trav_step<kAny, kCount, true>(s, t, stack, kStepBudget, &vc)) {
+      store(cur, t, vc);
+      active = false;
+    }
+  }
+}
+
 // raygen.wgsl:21-39
 __global__ void k_raygen(FrameBuffers fb, uint32_t W, uint32_t H, Mats mats) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -187,32 +236,29 @@ __global__ void k_raygen(FrameBuffers fb, uint32_t W, uint32_t H, Mats mats) {
 // Persistent closest-hit kernel for the path-extension rays: each warp takes
 // 32 consecutive queue entries per atomic.  Bounce 0 traces every pixel.
 template <bool kCount>
-__global__ void __launch_bounds__(kBlock) k_extend(DevScene s, FrameBuffers fb, Consts c) {
-  const uint32_t lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_extend(DevScene s, FrameBuffers fb, Consts c) {
   const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
   const uint32_t* q = fb.queue[c.qin];
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fb.counters[3], count);  // rays traced this frame
-  while (true) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&fb.counters[2], 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= count) break;
-    uint32_t i = base + lane;
-    if (i < count) {
-      uint32_t id = c.bounce == 0 ? i : q[i];
-      float4 r = fb.rays[id];
-      float3 o = ray_org(r), d = ray_dir(r);
-      Hit h;
-      Visits vc;
-      trace_closest<kCount>(s, o + d * 1e-4f, d, 1000.0f, h, &vc);
-      fb.hits[id] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.u), __float_as_uint(h.v), h.tri);
-      if (kCount) {
-        atomicAdd(&fb.visits[3 * K_EXTEND + 0], 1ull);
-        atomicAdd(&fb.visits[3 * K_EXTEND + 1], (unsigned long long)vc.nodes);
-        atomicAdd(&fb.visits[3 * K_EXTEND + 2], (unsigned long long)vc.tris);
-      }
-    }
-  }
+  const bool all = c.bounce == 0;
+  persistent_trace<false, kCount>(
+      s, count, &fb.counters[2],
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        const uint32_t id = all ? i : q[i];
+        const float4 r = fb.rays[id];
+        d = ray_dir(r);
+        o = ray_org(r) + d * 1e-4f;
+        tmax = 1000.0f;
+      },
+      [&](uint32_t i, const Trav& t, const Visits& vc) {
+        const uint32_t id = all ? i : q[i];
+        fb.hits[id] = make_uint4(__float_as_uint(t.hit.t), __float_as_uint(t.hit.u), __float_as_uint(t.hit.v), t.hit.tri);
+        if (kCount) {
+          atomicAdd(&fb.visits[3 * K_EXTEND + 0], 1ull);
+          atomicAdd(&fb.visits[3 * K_EXTEND + 1], (unsigned long long)vc.nodes);
+          atomicAdd(&fb.visits[3 * K_EXTEND + 2], (unsigned long long)vc.tris);
+        }
+      });
 }
 
 APD float2 velocity_of(const Mats& m, float3 p) {
@@ -241,40 +287,36 @@ APD void push_ray(const FrameBuffers& fb, int q, bool want, float3 o, float tmax
   fb.rq_d[q][slot] = make_float4(d.x, d.y, d.z, __uint_as_float(owner));
 }
 
-// Persistent traversal of one ray queue; each warp takes 32 rays per atomic.
+// Persistent traversal of one ray queue (per-lane refill).
 template <bool kAny, bool kCount>
-__global__ void __launch_bounds__(kBlock) k_trace_queue(DevScene s, FrameBuffers fb, int q, uint4* hits,
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_queue(DevScene s, FrameBuffers fb, int q, uint4* hits,
                                                         uint8_t* vis) {
-  const uint32_t lane = threadIdx.x & 31;
   const uint32_t count = fb.counters[kCounterQueueSize + q];
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fb.counters[3], count);
   const float4* qo = fb.rq_o[q];
   const float4* qd = fb.rq_d[q];
-  while (true) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&fb.counters[kCounterQueueCursor + q], 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= count) break;
-    uint32_t i = base + lane;
-    if (i < count) {
-      float4 o = qo[i], d = qd[i];
-      uint32_t owner = __float_as_uint(d.w);
-      Visits vc;
-      if (kAny) {
-        vis[owner] = trace_any<kCount>(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, &vc) ? 0 : 1;
-      } else {
-        Hit h;
-        trace_closest<kCount>(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, h, &vc);
-        hits[owner] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.u), __float_as_uint(h.v), h.tri);
-      }
-      if (kCount) {
-        const int k = kAny ? K_TRACE_ANY : K_TRACE_CLOSEST;
-        atomicAdd(&fb.visits[3 * k + 0], 1ull);
-        atomicAdd(&fb.visits[3 * k + 1], (unsigned long long)vc.nodes);
-        atomicAdd(&fb.visits[3 * k + 2], (unsigned long long)vc.tris);
-      }
-    }
-  }
+  persistent_trace<kAny, kCount>(
+      s, count, &fb.counters[kCounterQueueCursor + q],
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        const float4 a = qo[i], b = qd[i];
+        o = f3(a.x, a.y, a.z);
+        d = f3(b.x, b.y, b.z);
+        tmax = a.w;
+      },
+      [&](uint32_t i, const Trav& t, const Visits& vc) {
+        const uint32_t owner = __float_as_uint(qd[i].w);
+        if (kAny) {
+          vis[owner] = t.hit.tri != kNoHit ? 0 : 1;
+        } else {
+          hits[owner] = make_uint4(__float_as_uint(t.hit.t), __float_as_uint(t.hit.u), __float_as_uint(t.hit.v), t.hit.tri);
+        }
+        if (kCount) {
+          const int k = kAny ? K_TRACE_ANY : K_TRACE_CLOSEST;
+          atomicAdd(&fb.visits[3 * k + 0], 1ull);
+          atomicAdd(&fb.visits[3 * k + 1], (unsigned long long)vc.nodes);
+          atomicAdd(&fb.visits[3 * k + 2], (unsigned long long)vc.tris);
+        }
+      });
 }
 
 // ---- trace.wgsl:62-262 as four stages around the secondary rays -------------
@@ -882,6 +924,17 @@ __global__ void k_gi_temporal(DevScene s, FrameBuffers fb, Consts c, const uint4
   fb.payload[id] = pl;
 }
 
+// Bitwise equality of the inputs a target evaluation depends on.
+APD bool ls_same(const LightSample& a, const LightSample& b) {
+  return __float_as_uint(a.uv.x) == __float_as_uint(b.uv.x) && __float_as_uint(a.uv.y) == __float_as_uint(b.uv.y) &&
+         a.inst == b.inst && a.tri == b.tri;
+}
+APD bool gi_same_key(const GiRes& a, float3 pt, uint32_t prng) {
+  return __float_as_uint(a.point.x) == __float_as_uint(pt.x) && __float_as_uint(a.point.y) == __float_as_uint(pt.y) &&
+         __float_as_uint(a.point.z) == __float_as_uint(pt.z) && a.phat_rng == prng;
+}
+APD bool gi_same(const GiRes& a, const GiRes& b) { return gi_same_key(a, b.point, b.phat_rng); }
+
 APD uint32_t mirror(int x, int mx) {
   int v = ((x + mx) % (2 * mx)) - mx;
   return (uint32_t)(v < 0 ? -v : v);
@@ -932,6 +985,14 @@ __global__ void k_spatial(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_i
   if (GI) rgi = gi_unpack(in_a[id], in_b[id]);
   else rdi = di_unpack(in_a[id], in_b[id]);
   float3 wo = -direction;
+  // Memo of the last target value evaluated at this pixel: the unbiased combine
+  // re-evaluates the combined sample here, and that sample is always either the
+  // neighbour's (evaluated just before) or this pixel's previous one.
+  bool memo = false;
+  LightSample memo_ls = ls_empty();
+  float3 memo_pt = f3s(0.0f);
+  uint32_t memo_rng = 0u;
+  float memo_val = 0.0f;
   for (uint32_t i = 0; i < nsamples; ++i) {
     float angle = (float)i * golden + aoff;
     float cr = dm::pow_((float)i / (float)nsamples, 0.5f) * radius + roff;
@@ -970,7 +1031,14 @@ __global__ void k_spatial(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_i
           di_update(cmb, nr.phat * nr.W * nr.M, rng, nr.s, nr.phat);
           cmb.M = rdi.M + nr.M;
           float z = 0.0f;
-          if (ls_phat(s, cmb.s, cx, hit, wo, true) > 0.0f) z = z + rdi.M;
+          float zc;
+          if (ls_same(cmb.s, nr.s)) zc = nr.phat;
+          else if (memo && ls_same(cmb.s, memo_ls)) zc = memo_val;
+          else zc = ls_phat(s, cmb.s, cx, hit, wo, true);
+          memo = true;
+          memo_ls = cmb.s;
+          memo_val = zc;
+          if (zc > 0.0f) z = z + rdi.M;
           if (ls_phat(s, cmb.s, ncx, npos, nwo, true) > 0.0f) z = z + nr.M;
           if (cmb.phat > 1e-6f && z * cmb.wsum > 1e-6f) cmb.W = (1.0f / cmb.phat) * (1.0f / z * cmb.wsum);
           rdi = cmb;
@@ -990,7 +1058,15 @@ __global__ void k_spatial(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_i
           gi_update(cmb, nr.phat * nr.W * nr.M, rng, nr.point, nr.phat, nr.phat_rng);
           cmb.M = rgi.M + nr.M;
           float z = 0.0f;
-          if (gi_phat(s, cmb, cx, T, hit, wo) > 0.0f) z = z + rgi.M;
+          float zc;
+          if (gi_same(cmb, nr)) zc = nr.phat;
+          else if (memo && gi_same_key(cmb, memo_pt, memo_rng)) zc = memo_val;
+          else zc = gi_phat(s, cmb, cx, T, hit, wo);
+          memo = true;
+          memo_pt = cmb.point;
+          memo_rng = cmb.phat_rng;
+          memo_val = zc;
+          if (zc > 0.0f) z = z + rgi.M;
           if (gi_phat(s, cmb, ncx, nT, npos, nwo) > 0.0f) z = z + nr.M;
           if (cmb.phat > 0.0f && z * cmb.wsum > 0.0f) cmb.W = (1.0f / cmb.phat) * (1.0f / z * cmb.wsum);
           rgi = cmb;
@@ -1279,29 +1355,22 @@ __global__ void k_resolve(FrameBuffers fb, uint32_t P, float inv_count_den) {
   fb.out_rgb[3 * id + 2] = r.z;
 }
 
-// Batch traversal for tests and the traversal benchmark (persistent, warp fetch).
-__global__ void __launch_bounds__(kBlock) k_trace_batch(DevScene s, const float4* origins, const float4* dirs,
-                                                        uint32_t n, int any_hit, uint4* out, uint32_t* cursor) {
-  const uint32_t lane = threadIdx.x & 31;
-  while (true) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(cursor, 32u);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    uint32_t i = base + lane;
-    if (i < n) {
-      float4 o = origins[i], d = dirs[i];
-      float3 oo = f3(o.x, o.y, o.z), dd = f3(d.x, d.y, d.z);
-      if (any_hit) {
-        bool occ = trace_any(s, oo, dd, o.w);
-        out[i] = make_uint4(occ ? 1u : 0u, 0u, 0u, 0u);
-      } else {
-        Hit h;
-        trace_closest(s, oo, dd, o.w, h);
-        out[i] = make_uint4(__float_as_uint(h.t), __float_as_uint(h.u), __float_as_uint(h.v), h.tri);
-      }
-    }
-  }
+// Batch traversal for the ray-query entry points (persistent, per-lane refill).
+template <bool kAny>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_batch(DevScene s, const float4* origins, const float4* dirs,
+                                                        uint32_t n, uint4* out, uint32_t* cursor) {
+  persistent_trace<kAny, false>(
+      s, n, cursor,
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        const float4 a = origins[i], b = dirs[i];
+        o = f3(a.x, a.y, a.z);
+        d = f3(b.x, b.y, b.z);
+        tmax = a.w;
+      },
+      [&](uint32_t i, const Trav& t, const Visits&) {
+        if (kAny) out[i] = make_uint4(t.hit.tri != kNoHit ? 1u : 0u, 0u, 0u, 0u);
+        else out[i] = make_uint4(__float_as_uint(t.hit.t), __float_as_uint(t.hit.u), __float_as_uint(t.hit.v), t.hit.tri);
+      });
 }
 
 template <typename T>
@@ -1409,7 +1478,7 @@ const char* kernel_kind_name(int k) {
   static const char* names[K_NUM_KINDS] = {"memset", "raygen", "extend", "shade", "di_temporal", "di_spatial",
                                            "gi_temporal", "gi_spatial", "apply_di", "apply_gi", "demodulate",
                                            "firefly", "svgf_temporal", "atrous", "taa", "resolve", "copy",
-                                           "trace_closest", "trace_any"};
+                                           "trace_closest", "trace_any", "shade_b", "shade_c", "shade_d"};
   return (k >= 0 && k < K_NUM_KINDS) ? names[k] : "?";
 }
 
@@ -1440,7 +1509,7 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
   const uint32_t P = W * H;
   const uint32_t cur = frame_idx & 1u;
   dim3 b2(16, 16), g2((W + 15) / 16, (H + 15) / 16);
-  const int persistent_blocks = num_sms * 8;  // 8 x 128 threads per SM
+  const int persistent_blocks = num_sms * kTraceMinBlocks;
   const int linear_blocks = (int)std::min<uint32_t>((P + kBlock - 1) / kBlock, (uint32_t)num_sms * 16u);
   Consts c;
   c.W = W;
@@ -1471,17 +1540,17 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_BSDF_CAND, fb.hit_bsdf, nullptr);
       mark(K_TRACE_CLOSEST);
       k_shade_b<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
-      mark(K_SHADE);
+      mark(K_SHADE_B);
       trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_RIS_SHADOW, nullptr, fb.vis[Q_RIS_SHADOW]);
       mark(K_TRACE_ANY);
       trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_GI_CAND, fb.hit_gi, nullptr);
       mark(K_TRACE_CLOSEST);
       k_shade_c<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
-      mark(K_SHADE);
+      mark(K_SHADE_C);
       trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, nullptr, fb.vis[Q_GI_SHADOW]);
       mark(K_TRACE_ANY);
       k_shade_d<<<linear_blocks, kBlock, 0, st>>>(fb, c);
-      mark(K_SHADE);
+      mark(K_SHADE_D);
       if (i == 0) {
         if (cfg.restir_di) {
           uint4* pin_a = fb.di_prev_a[cur];
@@ -1605,7 +1674,8 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
 void launch_trace_batch(const DevScene& scene, const float4* origins, const float4* dirs, uint32_t n, int any_hit,
                         uint4* out, uint32_t* cursor, int num_sms, cudaStream_t st) {
   cudaMemsetAsync(cursor, 0, 4, st);
-  k_trace_batch<<<num_sms * 8, kBlock, 0, st>>>(scene, origins, dirs, n, any_hit, out, cursor);
+  if (any_hit) k_trace_batch<true><<<num_sms * kTraceMinBlocks, kBlock, 0, st>>>(scene, origins, dirs, n, out, cursor);
+  else k_trace_batch<false><<<num_sms * kTraceMinBlocks, kBlock, 0, st>>>(scene, origins, dirs, n, out, cursor);
 }
 
 }  // namespace ap

@@ -62,6 +62,17 @@ struct TriRec {
   float v[12];
 };
 
+// One emissive triangle, precomputed at upload with the same expressions the
+// light sampler would evaluate (80 bytes): vertices, area = |cross(e1, e2)|/2,
+// unit normal = normalize(cross(e1, e2)), emission of its material.
+struct EmissiveTri {
+  float p0[3], area;
+  float p1[3], pad0;
+  float p2[3], pad1;
+  float n[3], pad2;
+  float emission[3], pad3;
+};
+
 struct DevScene {
   const uint4* nodes;       // 5 per WideNode
   const float4* tris;       // 3 per TriRec
@@ -74,6 +85,8 @@ struct DevScene {
   const MaterialDev* materials;
   const uint32_t* emissive_instances;  // emissive index -> instance
   const float* emissive_cdf;
+  const EmissiveTri* emissive_tris;     // all triangles of the emissive instances
+  const uint32_t* emissive_tri_base;    // emissive instance -> first record
   uint32_t num_emissive_instances;
   uint32_t num_emissive_tris;
   const float* env;  // equirect RGB, env_w x env_h, or null

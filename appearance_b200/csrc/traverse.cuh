@@ -98,24 +98,216 @@ APD bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float t
   return true;
 }
 
-APD float byte_f(uint32_t word, int k) { return __uint2float_rn((word >> (8 * k)) & 0xffu); }
-
-// Box tests of the 8 children of one node.  Returns the hit mask; tnear[] gets
-// the entry distance of each hit child.
+// Child boxes of one node: conservativeness.
 //
-// Conservativeness: a slab value is computed as fma(q, s/d, (p - o)/d) with the
-// power-of-two scale s exact.  Its error is at most 3 ulp of |(p - o)/d| (the
-// rounding of p - o, of the product and of the fma, which can cancel against
-// q*s/d) plus a relative error of 1/d itself.  The watertight inside test may
-// accept a hit point outside the exact triangle by a few ulp of the vertex
-// distances from the origin.  Each slab is therefore widened by 2^-19 of
-// (|p - o| + node extent)/|d| and each interval by a relative 2^-21, so no child
-// that holds a triangle accepted inside [tmin, tmax] is culled.  For a zero direction
+// A slab value is computed as fma(q, s/d, (p - o)/d) with the power-of-two
+// scale s exact.  Its error is at most 3 ulp of |(p - o)/d| (the rounding of
+// p - o, of the product and of the fma, which can cancel against q*s/d) plus a
+// relative error of 1/d itself.  The watertight inside test may accept a hit
+// point outside the exact triangle by a few ulp of the vertex distances from
+// the origin.  Each slab is therefore widened by 2^-19 of (|p - o| + node
+// extent)/|d| and each interval by a relative 2^-21, so no child that holds a
+// triangle accepted inside [tmin, tmax] is culled.  For a zero direction
 // component the slab is all of t when the origin lies inside the child's
 // bounds decoded as p + q*s (rounded to nearest, which never shrinks the
 // conservatively quantised box), and empty otherwise.
+struct NodeFrame {
+  float px, py, pz, sxs, sys, szs;  // origin and scales of the quantisation grid
+  float ax, ay, az, bx, by, bz;     // slab = fma(q, a, b) per axis
+  float ex, ey, ez;                 // slab widening
+};
+
+APD NodeFrame node_frame(const uint4 w0, const RayPre& r) {
+  NodeFrame f;
+  f.px = __uint_as_float(w0.x);
+  f.py = __uint_as_float(w0.y);
+  f.pz = __uint_as_float(w0.z);
+  f.sxs = __uint_as_float((w0.w & 0xffu) << 23);
+  f.sys = __uint_as_float(((w0.w >> 8) & 0xffu) << 23);
+  f.szs = __uint_as_float(((w0.w >> 16) & 0xffu) << 23);
+  f.ax = f.sxs * r.inv.x;
+  f.ay = f.sys * r.inv.y;
+  f.az = f.szs * r.inv.z;
+  f.bx = (f.px - r.o.x) * r.inv.x;
+  f.by = (f.py - r.o.y) * r.inv.y;
+  f.bz = (f.pz - r.o.z) * r.inv.z;
+  const float kSlack = 1.9073486e-06f;  // 2^-19
+  f.ex = (fabsf(f.bx) + 255.0f * fabsf(f.ax)) * kSlack;
+  f.ey = (fabsf(f.by) + 255.0f * fabsf(f.ay)) * kSlack;
+  f.ez = (fabsf(f.bz) + 255.0f * fabsf(f.az)) * kSlack;
+  return f;
+}
+
+constexpr float kGrow = 1.0f + 4.8e-7f;  // relative 2^-21
+
+APD float byte_at(uint32_t word, int k) { return __uint2float_rn((word >> (8 * k)) & 0xffu); }
+
+// Entry distance of child i (a compile-time index after unrolling) or +inf
+// when its box is missed inside [tmin, tmax].
+APD float child_entry(const NodeFrame& f, const uint4 w2, const uint4 w3, const uint4 w4, const RayPre& r,
+                      int i, float tmin, float tmax) {
+  const int k = i & 3;
+  const uint32_t lox = i < 4 ? w2.x : w2.y, loy = i < 4 ? w2.z : w2.w;
+  const uint32_t loz = i < 4 ? w3.x : w3.y, hix = i < 4 ? w3.z : w3.w;
+  const uint32_t hiy = i < 4 ? w4.x : w4.y, hiz = i < 4 ? w4.z : w4.w;
+  float x0 = fmaf(byte_at(lox, k), f.ax, f.bx), x1 = fmaf(byte_at(hix, k), f.ax, f.bx);
+  float y0 = fmaf(byte_at(loy, k), f.ay, f.by), y1 = fmaf(byte_at(hiy, k), f.ay, f.by);
+  float z0 = fmaf(byte_at(loz, k), f.az, f.bz), z1 = fmaf(byte_at(hiz, k), f.az, f.bz);
+  float lx = fminf(x0, x1) - f.ex, hx = fmaxf(x0, x1) + f.ex;
+  float ly = fminf(y0, y1) - f.ey, hy = fmaxf(y0, y1) + f.ey;
+  float lz = fminf(z0, z1) - f.ez, hz = fmaxf(z0, z1) + f.ez;
+  if (r.zero_axes) {
+    const float inf = __uint_as_float(0x7f800000u);
+    if (r.zero_axes & 1u) {
+      bool in = r.o.x >= f.px + byte_at(lox, k) * f.sxs && r.o.x <= f.px + byte_at(hix, k) * f.sxs;
+      lx = in ? -inf : inf;
+      hx = in ? inf : -inf;
+    }
+    if (r.zero_axes & 2u) {
+      bool in = r.o.y >= f.py + byte_at(loy, k) * f.sys && r.o.y <= f.py + byte_at(hiy, k) * f.sys;
+      ly = in ? -inf : inf;
+      hy = in ? inf : -inf;
+    }
+    if (r.zero_axes & 4u) {
+      bool in = r.o.z >= f.pz + byte_at(loz, k) * f.szs && r.o.z <= f.pz + byte_at(hiz, k) * f.szs;
+      lz = in ? -inf : inf;
+      hz = in ? inf : -inf;
+    }
+  }
+  float tn = fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin));
+  float tf = fminf(fminf(hx, hy), hz);
+  tf = tf * (tf > 0.0f ? kGrow : 1.0f / kGrow);
+  tn = tn * (tn > 0.0f ? 1.0f / kGrow : kGrow);
+  return (tn <= tf && tn <= tmax * kGrow) ? tn : __uint_as_float(0x7f800000u);
+}
+
+APD uint32_t meta_of(const uint4 w1, int i) { return ((i < 4 ? w1.z : w1.w) >> (8 * (i & 3))) & 0xffu; }
+
+// Visit counters of one ray (instrumented builds of the traversal kernels).
+struct Visits {
+  uint32_t nodes = 0, tris = 0;
+};
+
+// Resumable traversal of one ray.  Closest hit: the nearest hit inner child is
+// visited next and the others are pushed with their entry distance, culled on
+// pop; any hit: stops at the first accepted triangle.  The traversal stack
+// holds at most BvhStats::max_stack entries (checked at build).
+struct Trav {
+  RayPre r;
+  Hit hit;          // closest: best so far (hit.t doubles as tmax); any: hit.tri != kNoHit when occluded
+  float tmax;       // any-hit query range
+  uint32_t node;
+  int sp;
+  bool have;        // `node` is the next node to visit
+};
+
+APD void trav_init(Trav& t, float3 o, float3 d, float tmax) {
+  t.r = ray_pre(o, d);
+  t.hit.t = tmax;
+  t.hit.u = 0.0f;
+  t.hit.v = 0.0f;
+  t.hit.tri = kNoHit;
+  t.tmax = tmax;
+  t.node = 0;
+  t.sp = 0;
+  t.have = true;
+}
+
+// Visits up to `budget` nodes; returns true when the ray is finished.  kUnroll
+// unrolls the 8 child tests (dedicated traversal kernels); the rolled form keeps
+// the code small where traversal is inlined into large shading kernels.
+template <bool kAny, bool kCount, bool kUnroll = false>
+APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits* vc) {
+  for (int step = 0; step < budget; ++step) {
+    if (!t.have) {
+      bool got = false;
+      while (t.sp > 0) {
+        uint2 e = stack[--t.sp];
+        if (kAny || __uint_as_float(e.y) <= t.hit.t * kGrow) {
+          t.node = e.x;
+          got = true;
+          break;
+        }
+      }
+      if (!got) return true;
+    }
+    t.have = false;
+    if (kCount) vc->nodes++;
+    const uint4* np = s.nodes + 5 * (size_t)t.node;
+    const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    const NodeFrame f = node_frame(w0, t.r);
+    const float range = kAny ? t.tmax : t.hit.t;
+    uint32_t leaf_mask = 0;
+    float best_t = __uint_as_float(0x7f800000u);
+    uint32_t best_node = 0;
+#pragma unroll(kUnroll ? 8 : 1)
+    for (int i = 0; i < 8; ++i) {
+      const uint32_t meta = meta_of(w1, i);
+      if (meta == 0u) continue;
+      const float tn = child_entry(f, w2, w3, w4, t.r, i, 0.0f, range);
+      if (!(tn < __uint_as_float(0x7f800000u))) continue;
+      if (meta & 0xe0u) {
+        leaf_mask |= 1u << i;
+      } else {
+        const uint32_t child = w1.x + (meta & 7u);
+        if (kAny) {
+          if (!t.have) {
+            t.node = child;
+            t.have = true;
+          } else if (t.sp < kTraversalStack) {
+            stack[t.sp++] = make_uint2(child, 0u);
+          }
+        } else if (tn < best_t) {
+          if (t.have && t.sp < kTraversalStack) stack[t.sp++] = make_uint2(best_node, __float_as_uint(best_t));
+          best_t = tn;
+          best_node = child;
+          t.have = true;
+        } else if (t.sp < kTraversalStack) {
+          stack[t.sp++] = make_uint2(child, __float_as_uint(tn));
+        }
+      }
+    }
+    if (!kAny) t.node = best_node;
+    while (leaf_mask) {
+      const int i = __ffs(leaf_mask) - 1;
+      leaf_mask &= leaf_mask - 1;
+      const uint32_t meta = meta_of(w1, i);
+      const uint32_t first = w1.y + (meta & 0x1fu);
+      const uint32_t cnt = __popc(meta >> 5);
+      if (kCount) vc->tris += cnt;
+      for (uint32_t k = 0; k < cnt; ++k) {
+        const float4* tp = s.tris + 3 * (size_t)(first + k);
+        const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float th, u, v;
+        const float lim = kAny ? t.tmax : t.hit.t;
+        if (intersect_tri(t.r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), 0.0f, lim, th, u, v)) {
+          const uint32_t gid = __float_as_uint(a.w);
+          if (kAny) {
+            t.hit.tri = gid;
+            return true;
+          }
+          if (th < t.hit.t || gid < t.hit.tri) {  // th <= hit.t here: strictly closer or a tie
+            t.hit.t = th;
+            t.hit.u = u;
+            t.hit.v = v;
+            t.hit.tri = gid;
+          }
+        }
+      }
+    }
+    if (!kAny && t.have && best_t > t.hit.t * kGrow) t.have = false;  // the nearest child is now culled
+  }
+  return false;
+}
+
+// ---- Loop-form traversal for rays traced inline in the large resampling
+// kernels.  Same box test (child_entry's arithmetic, all 8 children in one
+// unrolled pass), same culling and tie rules as trav_step, hence the same
+// results; the loop form has no resumable state, which keeps these kernels'
+// code and local memory small.  Returns the hit mask; tnear[] gets the entry
+// distance of each hit child.
 template <bool kClosest>
-APD uint32_t node_children(const uint4 w0, const uint4 w2, const uint4 w3, const uint4 w4,
+APD uint32_t inline_children(const uint4 w0, const uint4 w2, const uint4 w3, const uint4 w4,
                            const RayPre& r, float tmin, float tmax, float tnear[8]) {
   float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
   float sxs = __uint_as_float((w0.w & 0xffu) << 23);
@@ -136,26 +328,26 @@ APD uint32_t node_children(const uint4 w0, const uint4 w2, const uint4 w3, const
     uint32_t loz = i < 4 ? w3.x : w3.y, hix = i < 4 ? w3.z : w3.w;
     uint32_t hiy = i < 4 ? w4.x : w4.y, hiz = i < 4 ? w4.z : w4.w;
     int k = i & 3;
-    float x0 = fmaf(byte_f(lox, k), ax, bx), x1 = fmaf(byte_f(hix, k), ax, bx);
-    float y0 = fmaf(byte_f(loy, k), ay, by), y1 = fmaf(byte_f(hiy, k), ay, by);
-    float z0 = fmaf(byte_f(loz, k), az, bz), z1 = fmaf(byte_f(hiz, k), az, bz);
+    float x0 = fmaf(byte_at(lox, k), ax, bx), x1 = fmaf(byte_at(hix, k), ax, bx);
+    float y0 = fmaf(byte_at(loy, k), ay, by), y1 = fmaf(byte_at(hiy, k), ay, by);
+    float z0 = fmaf(byte_at(loz, k), az, bz), z1 = fmaf(byte_at(hiz, k), az, bz);
     float lx = fminf(x0, x1) - ex, hx = fmaxf(x0, x1) + ex;
     float ly = fminf(y0, y1) - ey, hy = fmaxf(y0, y1) + ey;
     float lz = fminf(z0, z1) - ez, hz = fmaxf(z0, z1) + ez;
     if (r.zero_axes) {
       const float inf = __uint_as_float(0x7f800000u);
       if (r.zero_axes & 1u) {
-        bool in = r.o.x >= px + byte_f(lox, k) * sxs && r.o.x <= px + byte_f(hix, k) * sxs;
+        bool in = r.o.x >= px + byte_at(lox, k) * sxs && r.o.x <= px + byte_at(hix, k) * sxs;
         lx = in ? -inf : inf;
         hx = in ? inf : -inf;
       }
       if (r.zero_axes & 2u) {
-        bool in = r.o.y >= py + byte_f(loy, k) * sys && r.o.y <= py + byte_f(hiy, k) * sys;
+        bool in = r.o.y >= py + byte_at(loy, k) * sys && r.o.y <= py + byte_at(hiy, k) * sys;
         ly = in ? -inf : inf;
         hy = in ? inf : -inf;
       }
       if (r.zero_axes & 4u) {
-        bool in = r.o.z >= pz + byte_f(loz, k) * szs && r.o.z <= pz + byte_f(hiz, k) * szs;
+        bool in = r.o.z >= pz + byte_at(loz, k) * szs && r.o.z <= pz + byte_at(hiz, k) * szs;
         lz = in ? -inf : inf;
         hz = in ? inf : -inf;
       }
@@ -169,14 +361,6 @@ APD uint32_t node_children(const uint4 w0, const uint4 w2, const uint4 w3, const
   }
   return mask;
 }
-
-APD uint32_t meta_of(const uint4 w1, int i) { return ((i < 4 ? w1.z : w1.w) >> (8 * (i & 3))) & 0xffu; }
-
-// Visit counters of one ray (instrumented builds of the traversal kernels).
-struct Visits {
-  uint32_t nodes = 0, tris = 0;
-};
-
 // Closest hit in [0, tmax] (returns false on miss).  Tie rule: smaller t, then
 // smaller global triangle id.
 template <bool kCount = false>
@@ -203,7 +387,7 @@ APD bool trace_closest(const DevScene& s, float3 o, float3 d, float tmax, Hit& h
     uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
           w4 = __ldg(np + 4);
     float tnear[8];
-    uint32_t mask = node_children<true>(w0, w2, w3, w4, r, 0.0f, hit.t, tnear);
+    uint32_t mask = inline_children<true>(w0, w2, w3, w4, r, 0.0f, hit.t, tnear);
     // leaves first (their hits shrink hit.t before the inner children are ordered)
     uint32_t todo = mask;
     while (todo) {
@@ -277,7 +461,7 @@ APD bool trace_any(const DevScene& s, float3 o, float3 d, float tmax, Visits* vc
     uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3),
           w4 = __ldg(np + 4);
     float tnear[8];
-    uint32_t mask = node_children<false>(w0, w2, w3, w4, r, 0.0f, tmax, tnear);
+    uint32_t mask = inline_children<false>(w0, w2, w3, w4, r, 0.0f, tmax, tnear);
     uint32_t todo = mask;
     while (todo) {
       int i = __ffs(todo) - 1;
