@@ -74,3 +74,46 @@ def frame_roofline(pt, scene, path, cfg, width: int, height: int, peak) -> dict:
     res["kernel_rooflines"] = {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items()}
                                for k, v in roofs.items()}
     return res
+
+
+def _frames_cli(argv=None):
+    """Renders frames of the benchmark workload (seeded 1.31M-triangle
+    icosphere field, seeded camera spline) on cuda:0 and prints each frame's
+    device time; the fixed command that profiler captures run."""
+    import argparse
+
+    from . import PathTracer, presets, scenes
+    ap = argparse.ArgumentParser(prog="python -m appearance_b200.profile")
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--frames", type=int, default=3)
+    ap.add_argument("--preset", default="realtime", choices=sorted(presets.PRESETS))
+    ap.add_argument("--kernels", action="store_true", help="also print per-kernel times of one more frame")
+    a = ap.parse_args(argv)
+    scene = scenes.icosphere_field(seed=0)
+    path = scenes.camera_spline(seed=0, frames=64)
+    pt = PathTracer(presets.PRESETS[a.preset])
+    pt.upload_scene(scene)
+    prev = None
+    f = 0
+    for f in range(a.frames):
+        eye, tgt = path[f % len(path)]
+        mats, prev = scenes.camera_matrices(eye, tgt, 60.0, 0.01, 1000.0, a.width, a.height, prev)
+        pt.set_camera_matrices(mats)
+        ms = pt.render_device(a.width, a.height)
+        print(f"frame {f} {a.width}x{a.height} {ms:.3f} ms launches {pt.last_stats.kernel_launches}", flush=True)
+    if a.kernels:
+        eye, tgt = path[(f + 1) % len(path)]
+        mats, prev = scenes.camera_matrices(eye, tgt, 60.0, 0.01, 1000.0, a.width, a.height, prev)
+        pt.set_camera_matrices(mats)
+        prof = pt.profile_frame(a.width, a.height)
+        tot = sum(v["ms"] for v in prof.values())
+        for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"]):
+            if v["ms"] > 0:
+                print(f"  {k:16s} {v['ms']:9.3f} ms {v['launches']:4d} launches {100 * v['ms'] / tot:5.1f}%")
+        print(f"total {tot:.3f} ms")
+    pt.close()
+
+
+if __name__ == "__main__":
+    _frames_cli()

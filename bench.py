@@ -35,6 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W_FULL, H_FULL = 1920, 1080
+CPU_W, CPU_H = 960, 540  # CPU samples: same scene, preset and camera path, a quarter of the pixels
 METRIC = "Msamples/s (1080p ReSTIR+SVGF+TAA frame, 1.31M-tri scene)"
 
 
@@ -134,16 +135,17 @@ def peaks():
 
 def cpu_baseline(scene, path, cfg) -> dict:
     """The CPU oracle (restatement of the reference frame) on a bounded sample:
-    the same scene, preset and camera at 192x108, 2 frames, all host threads."""
+    the same scene, preset and camera path at 960x540 (a quarter of the
+    pixels), 1 warm + 5 timed frames, all host threads."""
     from oracle.oracle import OracleFrame, OracleScene
-    w, h = 192, 108
+    w, h = CPU_W, CPU_H
     osc = OracleScene(scene)
     fr = OracleFrame(osc, w, h, cfg, threads=os.cpu_count())
     prev = None
     mats, prev = frame_mats(path, 0, prev, w, h)
     fr.render(mats)  # builds nothing new; first frame warms the history
     t0 = time.perf_counter()
-    frames = 2
+    frames = 5
     for f in range(1, 1 + frames):
         mats, prev = frame_mats(path, f, prev, w, h)
         fr.render(mats)
@@ -159,7 +161,7 @@ def run_reference(args, rank, world):
     from appearance_b200 import presets
     scene, path = build_workload()
     from oracle.oracle import OracleFrame, OracleScene
-    w, h = 192, 108
+    w, h = CPU_W, CPU_H
     osc = OracleScene(scene)
     fr = OracleFrame(osc, w, h, presets.REALTIME, threads=os.cpu_count())
     prev = None
