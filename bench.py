@@ -201,7 +201,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    from appearance_b200 import PathTracer, presets
+    from appearance_b200 import PathTracer, presets, replicas
     scene, path = build_workload()
     cfg = dict(presets.REALTIME)
     pt = PathTracer(cfg, device=local)
@@ -216,7 +216,7 @@ def main():
 
     # warm-up
     prev = None
-    f = rank * 7  # each replica starts at its own point of the camera path
+    f = replicas.replica_first_frame(rank)  # each replica renders its own stretch of the camera path
     for _ in range(args.warmup):
         mats, prev = frame_mats(path, f, prev, W_FULL, H_FULL)
         pt.set_camera_matrices(mats)
@@ -251,14 +251,11 @@ def main():
     barrier()
     e2e_s = sum(e2e_t)
     e2e_frames = len(e2e_t)
-    # reduce: max time over ranks
-    t = torch.tensor([dev_s, e2e_s, wall], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_s, e2e_s, wall = t.tolist()
+    # the slowest rank's times; the job's samples over them
+    dev_s, e2e_s, wall = replicas.max_over_ranks([dev_s, e2e_s, wall], world, device="cuda")
     if rank == 0:
-        value = world * P * args.steps / dev_s / 1e6
-        e2e = world * P * e2e_frames / e2e_s / 1e6
+        value = replicas.job_throughput(P * args.steps, world, dev_s) / 1e6
+        e2e = replicas.job_throughput(P * e2e_frames, world, e2e_s) / 1e6
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
