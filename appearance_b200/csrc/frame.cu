@@ -164,6 +164,14 @@ APD GiRes gi_new() {
 
 // ---- kernels ----------------------------------------------------------------
 
+// Lane of the calling thread within its warp, for any block shape (a 2-D
+// block's warps span several rows, so threadIdx.x alone does not give it).
+APD uint32_t lane_id() {
+  uint32_t l;
+  asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
+  return l;
+}
+
 APD void mul4(const float* m, float v0, float v1, float v2, float v3, float out[4]) {
 #pragma unroll
   for (int r = 0; r < 4; ++r) out[r] = m[r] * v0 + m[4 + r] * v1 + m[8 + r] * v2 + m[12 + r] * v3;
@@ -181,7 +189,7 @@ constexpr int kTraceMinBlocks = 6;
 
 template <bool kAny, bool kCount, class Load, class Store>
 APD void persistent_trace(const DevScene& s, uint32_t count, uint32_t* cursor, Load load, Store store) {
-  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t lane = lane_id();
   uint2 stack[kTraversalStack];
   Trav t;
   Visits vc;
@@ -237,7 +245,7 @@ __global__ void k_raygen(FrameBuffers fb, uint32_t W, uint32_t H, Mats mats) {
 // 32 consecutive queue entries per atomic.  Bounce 0 traces every pixel.
 template <bool kCount>
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_extend(DevScene s, FrameBuffers fb, Consts c) {
-  const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
+  const uint32_t count = c.bounce == 0 ? c.P : min(fb.counters[c.qin], c.P);
   const uint32_t* q = fb.queue[c.qin];
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fb.counters[3], count);  // rays traced this frame
   const bool all = c.bounce == 0;
@@ -277,7 +285,7 @@ APD void push_ray(const FrameBuffers& fb, int q, bool want, float3 o, float tmax
   const unsigned active = __activemask();
   const unsigned b = __ballot_sync(active, want);
   if (!want) return;
-  const int lane = threadIdx.x & 31;
+  const int lane = (int)lane_id();
   const int leader = __ffs(b) - 1;
   uint32_t base = 0;
   if (lane == leader) base = atomicAdd(&fb.counters[kCounterQueueSize + q], (uint32_t)__popc(b));
@@ -289,9 +297,10 @@ APD void push_ray(const FrameBuffers& fb, int q, bool want, float3 o, float tmax
 
 // Persistent traversal of one ray queue (per-lane refill).
 template <bool kAny, bool kCount>
-__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_queue(DevScene s, FrameBuffers fb, int q, uint4* hits,
-                                                        uint8_t* vis) {
-  const uint32_t count = fb.counters[kCounterQueueSize + q];
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_queue(DevScene s, FrameBuffers fb, int q, uint32_t cap,
+                                                                         uint4* hits, uint8_t* vis) {
+  // a queue holds at most one ray per pixel
+  const uint32_t count = min(fb.counters[kCounterQueueSize + q], cap);
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fb.counters[3], count);
   const float4* qo = fb.rq_o[q];
   const float4* qd = fb.rq_d[q];
@@ -332,7 +341,7 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_queue(DevScen
 constexpr uint32_t F_SHADED = 1u, F_BSDF_RAY = 2u;  // stage A -> B
 constexpr uint32_t F_RIS_SHADOW = 1u, F_GI_RAY = 2u, F_GI_SHADOW = 4u;  // B -> C -> D
 
-APD uint32_t bounce_count(const FrameBuffers& fb, const Consts& c) { return c.bounce == 0 ? c.P : fb.counters[c.qin]; }
+APD uint32_t bounce_count(const FrameBuffers& fb, const Consts& c) { return c.bounce == 0 ? c.P : min(fb.counters[c.qin], c.P); }
 APD uint32_t bounce_path(const FrameBuffers& fb, const Consts& c, uint32_t i) {
   return c.bounce == 0 ? i : fb.queue[c.qin][i];
 }
@@ -731,10 +740,10 @@ __global__ void __launch_bounds__(kBlock) k_apply_di_b(FrameBuffers fb, Consts c
 // apply_gi.wgsl:44-99, plus re-queueing of the live paths (warp ballot, one
 // atomic per warp) for the next bounce.
 __global__ void __launch_bounds__(kBlock) k_apply_gi(DevScene s, FrameBuffers fb, Consts c) {
-  const uint32_t count = c.bounce == 0 ? c.P : fb.counters[c.qin];
+  const uint32_t count = c.bounce == 0 ? c.P : min(fb.counters[c.qin], c.P);
   const uint32_t* q = fb.queue[c.qin];
   uint32_t* qo = fb.queue[c.qout];
-  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t lane = lane_id();
   const uint32_t stride = gridDim.x * blockDim.x;
   const uint32_t start = blockIdx.x * blockDim.x + threadIdx.x;
   // every lane of a warp runs the same number of iterations (ballot below)
@@ -950,6 +959,67 @@ APD float depth_cs(float d, float zn, float zf) {
   return (zn * zf) / (zf - zl * (zf - zn));
 }
 
+// Per-pixel setup shared by the spatial passes (restir_di_spatial.wgsl:70-100,
+// restir_gi_spatial.wgsl:71-103): the primary hit, its context and the
+// per-pass spiral offsets.
+struct SpatialPixel {
+  uint32_t x, y, id;
+  float3 direction, hit, wo;
+  uint4 cx;
+  float cdepth;
+  float3 cn;
+  float roff, aoff;
+};
+
+template <bool GI>
+APD void spatial_pixel(const FrameBuffers& fb, const Consts& c, uint32_t x, uint32_t y, uint32_t pass_idx,
+                       uint32_t pass_count, float pt, SpatialPixel& sp) {
+  sp.x = x;
+  sp.y = y;
+  sp.id = y * c.W + x;
+  const uint32_t cur = c.frame_idx & 1u;
+  float4 ray = fb.rays[sp.id];
+  sp.direction = ray_dir(ray);
+  sp.hit = ray_org(ray) + sp.direction * pt;
+  sp.wo = -sp.direction;
+  sp.cx = fb.ctx[sp.id];
+  sp.cdepth = depth_cs(__uint_as_float(fb.gb_a[cur][sp.id].w), 0.001f, 10000.0f);
+  sp.cn = unpack_oct30(fb.gb_b[cur][sp.id].x);
+  uint32_t frame_arg = GI ? c.seed * 3u + pass_idx : c.seed * pass_count + pass_idx;
+  sp.roff = ign_animated(x, y, frame_arg);
+  uint32_t psx = pass_idx == 0 ? (x >> 2) : (x >> 1);
+  uint32_t psy = pass_idx == 0 ? (y >> 2) : (y >> 1);
+  uint32_t aseed = hash_combine(psx, hash_combine(psy, frame_arg));
+  sp.aoff = __uint2float_rn(aseed) * (1.0f / 4294967296.0f) * kTwoPi;
+}
+
+APD float spatial_radius0(const Consts& c) { return (float)(c.W + c.H) / 2.0f * 0.05f; }
+
+// Neighbour i on the golden-angle spiral (restir_di_spatial.wgsl:104-113).
+APD uint32_t spatial_neighbour(const Consts& c, const SpatialPixel& sp, uint32_t i, uint32_t nsamples, float radius) {
+  const float golden = 2.39996322972865332f;
+  float angle = (float)i * golden + sp.aoff;
+  float cr = dm::pow_((float)i / (float)nsamples, 0.5f) * radius + sp.roff;
+  float sa, ca;
+  dm::sincos_(angle, &sa, &ca);
+  int ox = dm::f2i(cr * ca), oy = dm::f2i(cr * sa);
+  // mirror_pixel (restir_*_spatial.wgsl:59-68) can return the resolution itself
+  // (one past the edge, an out-of-bounds read in the reference): clamp to the edge
+  uint32_t nx = min(mirror((int)sp.x + ox, (int)c.W), c.W - 1), ny = min(mirror((int)sp.y + oy, (int)c.H), c.H - 1);
+  return ny * c.W + nx;
+}
+
+// Depth (10 %) and normal (25 degrees) similarity of neighbour nid.
+APD bool spatial_similar(const FrameBuffers& fb, const Consts& c, const SpatialPixel& sp, uint32_t nid) {
+  const uint32_t cur = c.frame_idx & 1u;
+  float ndepth = __uint_as_float(fb.gb_a[cur][nid].w);
+  if (ndepth == 0.0f) return false;
+  float nd = depth_cs(ndepth, 0.001f, 10000.0f);
+  bool vd = (dm::fabs_(sp.cdepth - nd) / sp.cdepth) < 0.1f;
+  bool vn = dot(sp.cn, unpack_oct30(fb.gb_b[cur][nid].x)) > 0.906f;
+  return vd && vn;
+}
+
 // restir_di_spatial.wgsl:70-163 (GI = false) and restir_gi_spatial.wgsl:71-166 (GI = true)
 template <bool GI>
 __global__ void k_spatial(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx, uint32_t pass_count,
@@ -961,30 +1031,19 @@ __global__ void k_spatial(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_i
   uint4 pl = fb.payload[id];
   float pt = __uint_as_float(pl.z);
   if (pt < 0.0f) return;
+  SpatialPixel sp;
+  spatial_pixel<GI>(fb, c, x, y, pass_idx, pass_count, pt, sp);
   const uint32_t cur = c.frame_idx & 1u;
   const uint4* ga = fb.gb_a[cur];
-  const uint4* gbb = fb.gb_b[cur];
   uint32_t rng = pl.y;
   float3 T = unpack_rgb9e5(pl.x);
-  float4 ray = fb.rays[id];
-  float3 direction = ray_dir(ray);
-  float3 hit = ray_org(ray) + direction * pt;
-  uint4 cx = fb.ctx[id];
-  float cdepth = depth_cs(__uint_as_float(ga[id].w), 0.001f, 10000.0f);
-  float3 cn = unpack_oct30(gbb[id].x);
-  float radius = (float)(c.W + c.H) / 2.0f * 0.05f;
-  uint32_t frame_arg = GI ? c.seed * 3u + pass_idx : c.seed * pass_count + pass_idx;
-  float roff = ign_animated(x, y, frame_arg);
-  uint32_t psx = pass_idx == 0 ? (x >> 2) : (x >> 1);
-  uint32_t psy = pass_idx == 0 ? (y >> 2) : (y >> 1);
-  uint32_t aseed = hash_combine(psx, hash_combine(psy, frame_arg));
-  float aoff = __uint2float_rn(aseed) * (1.0f / 4294967296.0f) * kTwoPi;
-  const float golden = 2.39996322972865332f;
+  const float3 hit = sp.hit, wo = sp.wo;
+  const uint4 cx = sp.cx;
+  float radius = spatial_radius0(c);
   DiRes rdi;
   GiRes rgi;
   if (GI) rgi = gi_unpack(in_a[id], in_b[id]);
   else rdi = di_unpack(in_a[id], in_b[id]);
-  float3 wo = -direction;
   // Memo of the last target value evaluated at this pixel: the unbiased combine
   // re-evaluates the combined sample here, and that sample is always either the
   // neighbour's (evaluated just before) or this pixel's previous one.
@@ -994,27 +1053,10 @@ __global__ void k_spatial(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_i
   uint32_t memo_rng = 0u;
   float memo_val = 0.0f;
   for (uint32_t i = 0; i < nsamples; ++i) {
-    float angle = (float)i * golden + aoff;
-    float cr = dm::pow_((float)i / (float)nsamples, 0.5f) * radius + roff;
-    float sa, ca;
-    dm::sincos_(angle, &sa, &ca);
-    int ox = dm::f2i(cr * ca), oy = dm::f2i(cr * sa);
-    // mirror_pixel (restir_*_spatial.wgsl:59-68) can return the resolution itself
-    // (one past the edge, an out-of-bounds read in the reference): clamp to the edge
-    uint32_t nx = min(mirror((int)x + ox, (int)c.W), c.W - 1), ny = min(mirror((int)y + oy, (int)c.H), c.H - 1);
-    uint32_t nid = ny * c.W + nx;
+    uint32_t nid = spatial_neighbour(c, sp, i, nsamples, radius);
     if (nid == id) continue;
-    bool valid = true;
+    bool valid = spatial_similar(fb, c, sp, nid);
     uint4 nga = ga[nid];
-    float ndepth = __uint_as_float(nga.w);
-    if (ndepth == 0.0f) {
-      valid = false;
-    } else {
-      float nd = depth_cs(ndepth, 0.001f, 10000.0f);
-      bool vd = (dm::fabs_(cdepth - nd) / cdepth) < 0.1f;
-      bool vn = dot(cn, unpack_oct30(gbb[nid].x)) > 0.906f;
-      valid = vd && vn;
-    }
     if (valid) {
       float3 npos = f3(__uint_as_float(nga.x), __uint_as_float(nga.y), __uint_as_float(nga.z));
       if (!GI) {
@@ -1092,6 +1134,204 @@ __global__ void k_spatial(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_i
   }
   pl.y = rng;
   fb.payload[id] = pl;
+}
+
+// ---- unbiased ReSTIR DI spatial pass as wavefront stages ---------------------
+//
+// The same pass as k_spatial<false> with unbiased = 1, split at its visibility
+// tests so that every shadow ray goes through the persistent any-hit queue
+// kernel instead of being traversed inline.  Per neighbour i:
+//   k_dsp_ca(i)  finishes neighbour i-1 (its Z, hence W), picks neighbour i,
+//                queues the visibility ray of the neighbour's sample here;
+//   any-hit queue Q_DI_SHADOW;
+//   k_dsp_b(i)   combines; queues the visibility ray of the combined sample
+//                here (unless its target is already known) on Q_RIS_SHADOW
+//                and at the neighbour on Q_GI_SHADOW;
+//   any-hit queues.
+// k_dsp_ca(nsamples) finishes the last neighbour and writes the history and
+// the payload's RNG.  The reservoir being built lives in out_a/out_b; the loop
+// state in the stage buffers:
+//   st_a {radius, rng, neighbour id, flags}   st_b memoised light sample
+//   st_c {memo target, target of the neighbour's sample here, of the combined
+//         sample here, of the combined sample at the neighbour}
+//   st_d {M of the pixel's reservoir, M of the neighbour's, known target here}
+// Targets are the unshadowed values of LightSample::phat
+// (di_reservoir.wgsl:58-97); a target counts only when its ray is unoccluded.
+enum : uint32_t {
+  SP_ACTIVE = 1u,    // neighbour passed the depth/normal test this iteration
+  SP_RAY_N = 2u,     // visibility ray of the neighbour's sample here queued
+  SP_RAY_C = 4u,     // visibility ray of the combined sample here queued
+  SP_RAY_CN = 8u,    // visibility ray of the combined sample at the neighbour queued
+  SP_ZC_KNOWN = 16u, // target of the combined sample here known without a ray
+  SP_MEMO = 32u,     // st_b/st_c.x hold a memoised target
+};
+
+// LightSample::phat split at its visibility test: the unshadowed target and the
+// shadow ray (helpers/trace.wgsl:7-18 offsets) that decides whether it counts.
+struct PhatSplit {
+  float value;
+  bool ray;
+  float3 o, d;
+  float tmax;
+};
+APD PhatSplit ls_phat_split(const DevScene& s, const LightSample& l, const uint4 c, float3 hit, float3 wo) {
+  LightEval ev = load_eval(s, l, hit);
+  Bsdf b = load_bsdf(s.materials + c.x);
+  Frame fr = ctx_frame(c);
+  float3 wi = normalize(ev.point - hit);
+  float wdn = dot(wi, fr.n);
+  PhatSplit r;
+  r.value = 0.0f;
+  r.ray = false;
+  r.o = f3s(0.0f);
+  r.d = f3s(0.0f);
+  r.tmax = 0.0f;
+  if (wdn > 0.0f) {
+    float sp = 0.0f;
+    float3 refl = disney_eval(b, fr, wo, wi, &sp);
+    r.value = luma(refl * wdn * ev.emission);
+    r.ray = __float_as_uint(r.value) != 0u;  // a +0 target is +0 whether or not the ray is occluded
+    r.o = hit + fr.n * 1e-4f;
+    r.d = wi;
+    r.tmax = dist(ev.point, hit) - 1e-4f * 2.0f;
+  }
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_dsp_ca(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
+                                                uint32_t pass_count, uint32_t nsamples, uint32_t i,
+                                                const uint4* in_a, const uint4* in_b, uint4* out_a, uint4* out_b,
+                                                uint4* prev_a, uint4* prev_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  const uint32_t id = y * c.W + x;
+  uint4 pl = fb.payload[id];
+  const float pt = __uint_as_float(pl.z);
+  if (pt < 0.0f) return;
+  uint4 sa, sb, sc;
+  if (i == 0) {
+    sa = make_uint4(__float_as_uint(spatial_radius0(c)), pl.y, 0u, 0u);
+    sb = make_uint4(0u, 0u, 0u, 0u);
+    sc = make_uint4(0u, 0u, 0u, 0u);
+    out_a[id] = in_a[id];
+    out_b[id] = in_b[id];
+  } else {
+    sa = fb.st_a[id];
+    sb = fb.st_b[id];
+    sc = fb.st_c[id];
+    if (sa.w & SP_ACTIVE) {
+      // finish neighbour i-1: Z of the combined sample, then W
+      const uint4 sd = fb.st_d[id];
+      float zc;
+      if (sa.w & SP_ZC_KNOWN) zc = __uint_as_float(sd.z);
+      else zc = ((sa.w & SP_RAY_C) && fb.vis[Q_RIS_SHADOW][id]) ? __uint_as_float(sc.z) : 0.0f;
+      DiRes cmb = di_unpack(out_a[id], out_b[id]);
+      sb = di_pack_b(cmb);  // memo: the combined sample and its target here
+      sc.x = __float_as_uint(zc);
+      sa.w |= SP_MEMO;
+      float z = 0.0f;
+      if (zc > 0.0f) z = z + __uint_as_float(sd.x);
+      const bool nbr = (sa.w & SP_RAY_CN) && fb.vis[Q_GI_SHADOW][id] && __uint_as_float(sc.w) > 0.0f;
+      if (nbr) z = z + __uint_as_float(sd.y);
+      if (cmb.phat > 1e-6f && z * cmb.wsum > 1e-6f) {
+        cmb.W = (1.0f / cmb.phat) * (1.0f / z * cmb.wsum);
+        out_a[id] = di_pack_a(cmb);
+      }
+    }
+  }
+  sa.w &= SP_MEMO;
+  if (i == nsamples) {
+    if (pass_idx == pass_count - 1) {
+      prev_a[id] = out_a[id];
+      prev_b[id] = out_b[id];
+    }
+    pl.y = sa.y;
+    fb.payload[id] = pl;
+    return;
+  }
+  SpatialPixel sp;
+  spatial_pixel<false>(fb, c, x, y, pass_idx, pass_count, pt, sp);
+  float radius = __uint_as_float(sa.x);
+  const uint32_t nid = spatial_neighbour(c, sp, i, nsamples, radius);
+  PhatSplit ph;
+  ph.ray = false;
+  ph.value = 0.0f;
+  if (nid != id) {
+    if (spatial_similar(fb, c, sp, nid)) {
+      const DiRes nr = di_unpack(in_a[nid], in_b[nid]);
+      ph = ls_phat_split(s, nr.s, sp.cx, sp.hit, sp.wo);
+      sa.w |= SP_ACTIVE | (ph.ray ? SP_RAY_N : 0u);
+      sc.y = __float_as_uint(ph.value);
+    } else {
+      radius = dm::fmax(radius * 0.5f, 3.0f);
+    }
+  }
+  sa.x = __float_as_uint(radius);
+  sa.z = nid;
+  fb.st_a[id] = sa;
+  fb.st_b[id] = sb;
+  fb.st_c[id] = sc;
+  push_ray(fb, Q_DI_SHADOW, ph.ray, ph.o, ph.tmax, ph.d, id);
+}
+
+__global__ void __launch_bounds__(256) k_dsp_b(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
+                                               uint32_t pass_count, const uint4* in_a, const uint4* in_b,
+                                               uint4* out_a, uint4* out_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  const uint32_t id = y * c.W + x;
+  const float pt = __uint_as_float(fb.payload[id].z);
+  if (pt < 0.0f) return;
+  uint4 sa = fb.st_a[id];
+  if (!(sa.w & SP_ACTIVE)) return;
+  uint4 sc = fb.st_c[id];
+  const uint4 sb = fb.st_b[id];
+  const uint32_t nid = sa.z;
+  uint32_t rng = sa.y;
+  DiRes rdi = di_unpack(out_a[id], out_b[id]);
+  DiRes nr = di_unpack(in_a[nid], in_b[nid]);
+  nr.phat = ((sa.w & SP_RAY_N) && fb.vis[Q_DI_SHADOW][id]) ? __uint_as_float(sc.y) : 0.0f;
+  const bool valid = nr.phat > 0.0f;
+  DiRes cmb = di_new();
+  di_update(cmb, rdi.phat * rdi.W * rdi.M, rng, rdi.s, rdi.phat);
+  di_update(cmb, nr.phat * nr.W * nr.M, rng, nr.s, nr.phat);
+  cmb.M = rdi.M + nr.M;
+  SpatialPixel sp;
+  spatial_pixel<false>(fb, c, x, y, pass_idx, pass_count, pt, sp);
+  const LightSample memo_ls{make_float2(__uint_as_float(sb.x), __uint_as_float(sb.y)), sb.z, sb.w};
+  float zc = 0.0f;
+  PhatSplit here;
+  here.ray = false;
+  here.value = 0.0f;
+  if (ls_same(cmb.s, nr.s)) {
+    zc = nr.phat;
+    sa.w |= SP_ZC_KNOWN;
+  } else if ((sa.w & SP_MEMO) && ls_same(cmb.s, memo_ls)) {
+    zc = __uint_as_float(sc.x);
+    sa.w |= SP_ZC_KNOWN;
+  } else {
+    here = ls_phat_split(s, cmb.s, sp.cx, sp.hit, sp.wo);
+    if (here.ray) sa.w |= SP_RAY_C;
+    else sa.w |= SP_ZC_KNOWN;  // target 0 without a ray
+    sc.z = __float_as_uint(here.value);
+  }
+  const uint4 nga = fb.gb_a[c.frame_idx & 1u][nid];
+  const float3 npos = f3(__uint_as_float(nga.x), __uint_as_float(nga.y), __uint_as_float(nga.z));
+  const float3 nwo = -ray_dir(fb.rays[nid]);
+  const PhatSplit there = ls_phat_split(s, cmb.s, fb.ctx[nid], npos, nwo);
+  if (there.ray) sa.w |= SP_RAY_CN;
+  sc.w = __float_as_uint(there.value);
+  float radius = __uint_as_float(sa.x);
+  if (!valid) radius = dm::fmax(radius * 0.5f, 3.0f);
+  sa.x = __float_as_uint(radius);
+  sa.y = rng;
+  out_a[id] = di_pack_a(cmb);
+  out_b[id] = di_pack_b(cmb);
+  fb.st_a[id] = sa;
+  fb.st_c[id] = sc;
+  fb.st_d[id] = make_uint4(__float_as_uint(rdi.M), __float_as_uint(nr.M), __float_as_uint(zc), 0u);
+  push_ray(fb, Q_RIS_SHADOW, here.ray, here.o, here.tmax, here.d, id);
+  push_ray(fb, Q_GI_SHADOW, there.ray, there.o, there.tmax, there.d, id);
 }
 
 // ---- denoising -------------------------------------------------------------
@@ -1484,9 +1724,9 @@ const char* kernel_kind_name(int k) {
 
 template <bool kAny>
 void trace_queue(bool counting, int blocks, cudaStream_t st, const DevScene& scene, const FrameBuffers& fb, int q,
-                 uint4* hits, uint8_t* vis) {
-  if (counting) k_trace_queue<kAny, true><<<blocks, kBlock, 0, st>>>(scene, fb, q, hits, vis);
-  else k_trace_queue<kAny, false><<<blocks, kBlock, 0, st>>>(scene, fb, q, hits, vis);
+                 uint32_t cap, uint4* hits, uint8_t* vis) {
+  if (counting) k_trace_queue<kAny, true><<<blocks, kBlock, 0, st>>>(scene, fb, q, cap, hits, vis);
+  else k_trace_queue<kAny, false><<<blocks, kBlock, 0, st>>>(scene, fb, q, cap, hits, vis);
 }
 
 int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
@@ -1537,17 +1777,17 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       mark(K_MEMSET);
       k_shade_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c, mats);
       mark(K_SHADE);
-      trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_BSDF_CAND, fb.hit_bsdf, nullptr);
+      trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_BSDF_CAND, P, fb.hit_bsdf, nullptr);
       mark(K_TRACE_CLOSEST);
       k_shade_b<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_SHADE_B);
-      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_RIS_SHADOW, nullptr, fb.vis[Q_RIS_SHADOW]);
+      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_RIS_SHADOW, P, nullptr, fb.vis[Q_RIS_SHADOW]);
       mark(K_TRACE_ANY);
-      trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_GI_CAND, fb.hit_gi, nullptr);
+      trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_GI_CAND, P, fb.hit_gi, nullptr);
       mark(K_TRACE_CLOSEST);
       k_shade_c<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_SHADE_C);
-      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, nullptr, fb.vis[Q_GI_SHADOW]);
+      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, P, nullptr, fb.vis[Q_GI_SHADOW]);
       mark(K_TRACE_ANY);
       k_shade_d<<<linear_blocks, kBlock, 0, st>>>(fb, c);
       mark(K_SHADE_D);
@@ -1563,11 +1803,34 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
           uint32_t n = cfg.di_spatial_passes;
           for (uint32_t k = 0; k < n; ++k) {
             bool odd = (k % 2) != 0;
-            k_spatial<false><<<g2, b2, 0, st>>>(scene, fb, c, k, n, cfg.di_spatial_samples, cfg.di_unbiased,
-                                                odd ? fb.di_a : fb.di_inter_a, odd ? fb.di_b : fb.di_inter_b,
-                                                odd ? fb.di_inter_a : fb.di_a, odd ? fb.di_inter_b : fb.di_b, pout_a,
-                                                pout_b);
-            mark(K_DI_SPATIAL);
+            const uint4* in_a = odd ? fb.di_a : fb.di_inter_a;
+            const uint4* in_b = odd ? fb.di_b : fb.di_inter_b;
+            uint4* out_a = odd ? fb.di_inter_a : fb.di_a;
+            uint4* out_b = odd ? fb.di_inter_b : fb.di_b;
+            if (!cfg.di_unbiased) {
+              k_spatial<false><<<g2, b2, 0, st>>>(scene, fb, c, k, n, cfg.di_spatial_samples, 0u, in_a, in_b, out_a,
+                                                  out_b, pout_a, pout_b);
+              mark(K_DI_SPATIAL);
+              continue;
+            }
+            // unbiased: wavefront stages, shadow rays through the any-hit queues
+            const uint32_t ns = cfg.di_spatial_samples;
+            for (uint32_t j = 0; j <= ns; ++j) {
+              cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+              mark(K_MEMSET);
+              k_dsp_ca<<<g2, b2, 0, st>>>(scene, fb, c, k, n, ns, j, in_a, in_b, out_a, out_b, pout_a, pout_b);
+              mark(K_DI_SPATIAL);
+              if (j == ns) break;
+              trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_DI_SHADOW, P, nullptr, fb.vis[Q_DI_SHADOW]);
+              mark(K_TRACE_ANY);
+              k_dsp_b<<<g2, b2, 0, st>>>(scene, fb, c, k, n, in_a, in_b, out_a, out_b);
+              mark(K_DI_SPATIAL);
+              trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_RIS_SHADOW, P, nullptr,
+                                fb.vis[Q_RIS_SHADOW]);
+              mark(K_TRACE_ANY);
+              trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, P, nullptr, fb.vis[Q_GI_SHADOW]);
+              mark(K_TRACE_ANY);
+            }
           }
           if (n % 2 == 0) {
             cudaMemcpyAsync(fb.di_a, fb.di_inter_a, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);
@@ -1606,7 +1869,7 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       }
       k_apply_di_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_APPLY_DI);
-      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_DI_SHADOW, nullptr, fb.vis[Q_DI_SHADOW]);
+      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_DI_SHADOW, P, nullptr, fb.vis[Q_DI_SHADOW]);
       mark(K_TRACE_ANY);
       k_apply_di_b<<<linear_blocks, kBlock, 0, st>>>(fb, c);
       mark(K_APPLY_DI);
