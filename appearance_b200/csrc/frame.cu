@@ -180,11 +180,12 @@ APD void mul4(const float* m, float v0, float v1, float v2, float v3, float out[
 // Persistent traversal with per-lane refill: a lane that finishes its ray
 // takes the next one through a warp-aggregated atomic on `cursor`, so warps
 // stay full until the batch drains.  Lanes check for a refill every
-// kStepBudget visited nodes.  load(i, o, d, tmax) fetches ray i,
+// kStepBudget steps (the best of 8, 16, 32 measured on the benchmark
+// scene).  load(i, o, d, tmax) fetches ray i,
 // store(i, trav, visits) writes its result.  The traversal kernels run with
 // the child tests unrolled and are register-capped for 6 resident blocks of
 // kBlock threads per SM (the best of the measured 1..8 on the benchmark scene).
-constexpr int kStepBudget = 16;
+constexpr int kStepBudget = 8;
 constexpr int kTraceMinBlocks = 6;
 
 template <bool kAny, bool kCount, class Load, class Store>
@@ -338,7 +339,8 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_queue(DevScen
 //   D: finishes the GI reservoir
 // The per-path RNG stream is consumed in exactly the reference's order.
 
-constexpr uint32_t F_SHADED = 1u, F_BSDF_RAY = 2u;  // stage A -> B
+constexpr uint32_t F_SHADED = 1u, F_BSDF_RAY = 2u;  // stage A -> B1
+constexpr uint32_t F_B_SHADOW = 4u;                  // stage B1 -> B2
 constexpr uint32_t F_RIS_SHADOW = 1u, F_GI_RAY = 2u, F_GI_SHADOW = 4u;  // B -> C -> D
 
 APD uint32_t bounce_count(const FrameBuffers& fb, const Consts& c) { return c.bounce == 0 ? c.P : min(fb.counters[c.qin], c.P); }
@@ -444,15 +446,17 @@ __global__ void __launch_bounds__(kBlock) k_shade_a(DevScene s, FrameBuffers fb,
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade_b(DevScene s, FrameBuffers fb, Consts c) {
+// Stage B1: resampled importance sampling of the direct light (Nee::sample_ris,
+// nee.wgsl:122-237) and its shadow ray.
+__global__ void __launch_bounds__(kBlock, 4) k_shade_b(DevScene s, FrameBuffers fb, Consts c) {
   const uint32_t count = bounce_count(fb, c);
   const uint32_t NA = c.cfg.di_area_samples, NB = c.cfg.di_bsdf_samples;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     uint32_t id = bounce_path(fb, c, i);
     uint4 sa = fb.st_a[id];
     bool active = (sa.w & F_SHADED) != 0;
-    bool want_shadow = false, want_gi = false;
-    float3 sh_o = f3s(0.0f), sh_d = f3s(0.0f), gi_o = f3s(0.0f), wi = f3s(0.0f);
+    bool want_shadow = false;
+    float3 sh_o = f3s(0.0f), sh_d = f3s(0.0f);
     float sh_t = 0.0f;
     if (active) {
       uint4 pl = fb.payload[id];
@@ -532,6 +536,37 @@ __global__ void __launch_bounds__(kBlock) k_shade_b(DevScene s, FrameBuffers fb,
       }
       fb.di_a[id] = di_pack_a(res);
       fb.di_b[id] = di_pack_b(res);
+      fb.payload[id] = make_uint4(pl.x, rng, pl.z, pl.w);
+      fb.st_a[id] = make_uint4(0u, 0u, 0u, F_SHADED | (want_shadow ? F_B_SHADOW : 0u));
+    }
+    push_ray(fb, Q_RIS_SHADOW, want_shadow, sh_o, sh_t, sh_d, id);
+  }
+}
+
+// Stage B2: Russian roulette (trace.wgsl:220-230) and the BSDF-sampled GI
+// candidate direction (InlinePathTracer::sample_ris, inline_path_tracer.wgsl:258-296),
+// continuing the path's RNG stream after stage B1.
+__global__ void __launch_bounds__(kBlock) k_shade_b2(DevScene s, FrameBuffers fb, Consts c) {
+  const uint32_t count = bounce_count(fb, c);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t id = bounce_path(fb, c, i);
+    uint4 sa = fb.st_a[id];
+    bool active = (sa.w & F_SHADED) != 0;
+    bool want_gi = false;
+    float3 gi_o = f3s(0.0f), wi = f3s(0.0f);
+    if (active) {
+      uint4 pl = fb.payload[id];
+      float4 ray = fb.rays[id];
+      float3 origin = ray_org(ray), direction = ray_dir(ray);
+      float3 T = unpack_rgb9e5(pl.x);
+      uint32_t rng = pl.y;
+      uint4 hr = fb.hits[id];
+      Hit h{__uint_as_float(hr.x), __uint_as_float(hr.y), __uint_as_float(hr.z), hr.w};
+      const MaterialDev* m;
+      Surface sf = surface(s, h, origin, direction, &m);
+      Bsdf b = load_bsdf(m);
+      float3 wo = -direction;
+      float3 hit = sf.hit_point;
       float t_out = __uint_as_float(pl.z);
       float gi_pdf = 0.0f;
       uint32_t phat_rng = 0;
@@ -564,13 +599,12 @@ __global__ void __launch_bounds__(kBlock) k_shade_b(DevScene s, FrameBuffers fb,
           }
         }
       }
-      uint32_t flags = (want_shadow ? F_RIS_SHADOW : 0u) | (want_gi ? F_GI_RAY : 0u);
+      uint32_t flags = ((sa.w & F_B_SHADOW) ? F_RIS_SHADOW : 0u) | (want_gi ? F_GI_RAY : 0u);
       fb.payload[id] = make_uint4(pack_rgb9e5(T), rng, __float_as_uint(t_out), 0u);
       fb.st_a[id] = make_uint4(__float_as_uint(gi_pdf), phat_rng, 0u, flags);
       fb.st_c[id] = make_uint4(__float_as_uint(tr.x), __float_as_uint(tr.y), __float_as_uint(tr.z), 0u);
       fb.st_d[id] = make_uint4(__float_as_uint(wi.x), __float_as_uint(wi.y), __float_as_uint(wi.z), 0u);
     }
-    push_ray(fb, Q_RIS_SHADOW, want_shadow, sh_o, sh_t, sh_d, id);
     push_ray(fb, Q_GI_CAND, want_gi, gi_o, 1000.0f - 1e-4f * 2.0f, wi, id);
   }
 }
@@ -852,10 +886,58 @@ APD GiRes gi_combine(const GiRes& r1, const GiRes& r2, uint32_t& rng) {
   return c;
 }
 
-// restir_di_temporal.wgsl:68-176 (BILINEAR = false)
-__global__ void k_di_temporal(DevScene s, FrameBuffers fb, Consts c, const uint4* in_a, const uint4* in_b,
-                              uint4* out_a, uint4* out_b, const uint4* prev_a, const uint4* prev_b,
-                              uint4* pout_a, uint4* pout_b) {
+
+
+// LightSample::phat split at its visibility test: the unshadowed target and the
+// shadow ray (helpers/trace.wgsl:7-18 offsets) that decides whether it counts.
+struct PhatSplit {
+  float value;
+  bool ray;
+  float3 o, d;
+  float tmax;
+};
+APD PhatSplit ls_phat_split(const DevScene& s, const LightSample& l, const uint4 c, float3 hit, float3 wo) {
+  LightEval ev = load_eval(s, l, hit);
+  Bsdf b = load_bsdf(s.materials + c.x);
+  Frame fr = ctx_frame(c);
+  float3 wi = normalize(ev.point - hit);
+  float wdn = dot(wi, fr.n);
+  PhatSplit r;
+  r.value = 0.0f;
+  r.ray = false;
+  r.o = f3s(0.0f);
+  r.d = f3s(0.0f);
+  r.tmax = 0.0f;
+  if (wdn > 0.0f) {
+    float sp = 0.0f;
+    float3 refl = disney_eval(b, fr, wo, wi, &sp);
+    r.value = luma(refl * wdn * ev.emission);
+    r.ray = __float_as_uint(r.value) != 0u;  // a +0 target is +0 whether or not the ray is occluded
+    r.o = hit + fr.n * 1e-4f;
+    r.d = wi;
+    r.tmax = dist(ev.point, hit) - 1e-4f * 2.0f;
+  }
+  return r;
+}
+
+// ---- temporal passes as wavefront stages -------------------------------------
+//
+// The temporal resampling passes (restir_di_temporal.wgsl:68-176,
+// restir_gi_temporal.wgsl:67-116), split at their rays so that the rays go
+// through the persistent traversal queues.  Loop state in
+// the stage buffers: st_a {pixel rng, previous-frame pixel, flags, -},
+// st_c {throughput or light contribution}, st_b {the target's value (DI)}.
+enum : uint32_t {
+  TP_HIST = 1u,    // history reprojected and valid: combine with the previous reservoir
+  TP_RAY = 2u,     // the target's visibility ray was queued (DI)
+  TP_SHADOW = 4u,  // GI re-trace: the NEE shadow ray was queued
+  TP_DONE = 8u,    // GI re-trace: radiance known without a shadow ray (sky)
+};
+
+// DI temporal, stage 1 (restir_di_temporal.wgsl:68-158): reprojection, the
+// previous reservoir and its target here, whose visibility ray is queued.
+__global__ void __launch_bounds__(256) k_dt_a(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
+                                              const uint4* prev_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
   uint32_t id = y * c.W + x;
@@ -864,23 +946,52 @@ __global__ void k_di_temporal(DevScene s, FrameBuffers fb, Consts c, const uint4
   if (pt < 0.0f) return;
   const uint32_t cur = c.frame_idx & 1u;
   uint32_t rng = pl.y;
-  float4 ray = fb.rays[id];
-  float3 direction = ray_dir(ray);
-  float3 hit = ray_org(ray) + direction * pt;
-  uint4 cx = fb.ctx[id];
-  DiRes r = di_unpack(in_a[id], in_b[id]);
+  uint32_t flags = 0, pid = 0;
+  PhatSplit ph;
+  ph.ray = false;
+  ph.value = 0.0f;
   float2 pp;
   if (prev_point(fb, cur, x, y, c.W, c.H, &pp)) {
     GT g = gt_load(fb.gb_a[cur], fb.gb_b[cur], id);
     GT pg = sample_prev_gbuffer(fb.gb_a[cur ^ 1u], fb.gb_b[cur ^ 1u], c.W, c.H, pp);
     if (history_valid(g, pg)) {
       float r0 = rnd(rng), r1 = rnd(rng);
-      uint32_t pid = stochastic_prev_id(pp, r0, r1, c.W, c.H);
-      DiRes pr = di_unpack(prev_a[pid], prev_b[pid]);
-      pr.M = dm::fmin(pr.M, c.cfg.di_temporal_m_factor * r.M);
-      pr.phat = ls_phat(s, pr.s, cx, hit, -direction, c.cfg.di_unbiased > 0);
-      r = di_combine(r, pr, rng);
+      pid = stochastic_prev_id(pp, r0, r1, c.W, c.H);
+      const DiRes pr = di_unpack(prev_a[pid], prev_b[pid]);
+      float4 ray = fb.rays[id];
+      float3 direction = ray_dir(ray);
+      float3 hit = ray_org(ray) + direction * pt;
+      ph = ls_phat_split(s, pr.s, fb.ctx[id], hit, -direction);
+      flags = TP_HIST;
+      if (c.cfg.di_unbiased) {
+        if (ph.ray) flags |= TP_RAY;
+      } else {
+        ph.ray = false;
+      }
     }
+  }
+  fb.st_a[id] = make_uint4(rng, pid, flags, __float_as_uint(ph.value));
+  push_ray(fb, Q_DI_SHADOW, ph.ray, ph.o, ph.tmax, ph.d, id);
+}
+
+// DI temporal, stage 2 (restir_di_temporal.wgsl:159-176): M cap and combine.
+__global__ void __launch_bounds__(256) k_dt_b(FrameBuffers fb, Consts c, const uint4* in_a, const uint4* in_b,
+                                              uint4* out_a, uint4* out_b, const uint4* prev_a, const uint4* prev_b,
+                                              uint4* pout_a, uint4* pout_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  uint32_t id = y * c.W + x;
+  uint4 pl = fb.payload[id];
+  if (__uint_as_float(pl.z) < 0.0f) return;
+  const uint4 sa = fb.st_a[id];
+  uint32_t rng = sa.x;
+  DiRes r = di_unpack(in_a[id], in_b[id]);
+  if (sa.z & TP_HIST) {
+    DiRes pr = di_unpack(prev_a[sa.y], prev_b[sa.y]);
+    pr.M = dm::fmin(pr.M, c.cfg.di_temporal_m_factor * r.M);
+    if (!c.cfg.di_unbiased) pr.phat = __uint_as_float(sa.w);  // target without visibility
+    else pr.phat = ((sa.z & TP_RAY) && fb.vis[Q_DI_SHADOW][id]) ? __uint_as_float(sa.w) : 0.0f;
+    r = di_combine(r, pr, rng);
   }
   out_a[id] = di_pack_a(r);
   out_b[id] = di_pack_b(r);
@@ -892,10 +1003,11 @@ __global__ void k_di_temporal(DevScene s, FrameBuffers fb, Consts c, const uint4
   fb.payload[id] = pl;
 }
 
-// restir_gi_temporal.wgsl:67-116
-__global__ void k_gi_temporal(DevScene s, FrameBuffers fb, Consts c, const uint4* in_a, const uint4* in_b,
-                              uint4* out_a, uint4* out_b, const uint4* prev_a, const uint4* prev_b,
-                              uint4* pout_a, uint4* pout_b) {
+// GI temporal, stage 1 (restir_gi_temporal.wgsl:67-96): reprojection, the
+// previous reservoir, and the first ray of its target's re-trace
+// (GiReservoir::phat, inline_path_tracer.wgsl:299-331).
+__global__ void __launch_bounds__(256) k_gt_a(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
+                                              const uint4* prev_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
   uint32_t id = y * c.W + x;
@@ -904,24 +1016,120 @@ __global__ void k_gi_temporal(DevScene s, FrameBuffers fb, Consts c, const uint4
   if (pt < 0.0f) return;
   const uint32_t cur = c.frame_idx & 1u;
   uint32_t rng = pl.y;
-  float3 T = unpack_rgb9e5(pl.x);
-  float4 ray = fb.rays[id];
-  float3 direction = ray_dir(ray);
-  float3 hit = ray_org(ray) + direction * pt;
-  uint4 cx = fb.ctx[id];
-  GiRes r = gi_unpack(in_a[id], in_b[id]);
+  uint32_t flags = 0, pid = 0;
+  bool want = false;
+  float3 o = f3s(0.0f), wi = f3s(0.0f), tr = f3s(0.0f);
   float2 pp;
   if (prev_point(fb, cur, x, y, c.W, c.H, &pp)) {
     float r0 = rnd(rng), r1 = rnd(rng);
-    uint32_t pid = stochastic_prev_id(pp, r0, r1, c.W, c.H);
+    pid = stochastic_prev_id(pp, r0, r1, c.W, c.H);
     GT g = gt_load(fb.gb_a[cur], fb.gb_b[cur], id);
     GT pg = sample_prev_gbuffer(fb.gb_a[cur ^ 1u], fb.gb_b[cur ^ 1u], c.W, c.H, pp);
     if (history_valid(g, pg)) {
-      GiRes pr = gi_unpack(prev_a[pid], prev_b[pid]);
-      pr.M = dm::fmin(pr.M, c.cfg.gi_temporal_m_cap);
-      pr.phat = gi_phat(s, pr, cx, T, hit, -direction);
-      r = gi_combine(r, pr, rng);
+      const GiRes pr = gi_unpack(prev_a[pid], prev_b[pid]);
+      float4 ray = fb.rays[id];
+      float3 direction = ray_dir(ray);
+      float3 hit = ray_org(ray) + direction * pt;
+      const uint4 cx = fb.ctx[id];
+      Bsdf b = load_bsdf(s.materials + cx.x);
+      Frame fr = ctx_frame(cx);
+      wi = normalize(pr.point - hit);
+      float sp = 0.0f;
+      float3 refl = disney_eval(b, fr, -direction, wi, &sp);
+      float cos_in = dm::fabs_(dot(wi, fr.n));
+      float3 local = cos_in * refl;
+      float3 gi_origin = hit + wi * 0.0001f;
+      tr = unpack_rgb9e5(pl.x) * local;
+      o = gi_origin + wi * 1e-4f;
+      want = true;
+      flags = TP_HIST;
     }
+  }
+  fb.st_a[id] = make_uint4(rng, pid, flags, 0u);
+  fb.st_c[id] = make_uint4(__float_as_uint(tr.x), __float_as_uint(tr.y), __float_as_uint(tr.z), 0u);
+  push_ray(fb, Q_GI_CAND, want, o, 1000.0f - 1e-4f * 2.0f, wi, id);
+}
+
+// GI temporal, stage 2: the re-trace's hit (InlinePathTracer::trace with the
+// approx() config, inline_path_tracer.wgsl:51-256): uniform light sample and its
+// shadow ray, or the sky on a miss.
+__global__ void __launch_bounds__(256) k_gt_b(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
+                                              const uint4* prev_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  uint32_t id = y * c.W + x;
+  float pt = __uint_as_float(fb.payload[id].z);
+  if (pt < 0.0f) return;
+  uint4 sa = fb.st_a[id];
+  if (!(sa.z & TP_HIST)) return;
+  const uint4 sc = fb.st_c[id];
+  const float3 throughput = f3(__uint_as_float(sc.x), __uint_as_float(sc.y), __uint_as_float(sc.z));
+  const GiRes pr = gi_unpack(prev_a[sa.y], prev_b[sa.y]);
+  float4 ray = fb.rays[id];
+  float3 hit = ray_org(ray) + ray_dir(ray) * pt;
+  const float3 wi = normalize(pr.point - hit);
+  const float3 gi_origin = hit + wi * 0.0001f;
+  const uint4 hr = fb.hit_gi[id];
+  bool want = false;
+  float3 so = f3s(0.0f), sd = f3s(0.0f), val = f3s(0.0f);
+  float st = 0.0f;
+  if (hr.w != kNoHit) {
+    Hit h{__uint_as_float(hr.x), __uint_as_float(hr.y), __uint_as_float(hr.z), hr.w};
+    const MaterialDev* m;
+    Surface sf = surface(s, h, gi_origin, wi, &m);
+    Bsdf b = load_bsdf(m);
+    uint32_t prng = pr.phat_rng;
+    float pdf = 0.0f;
+    float r0 = rnd(prng), r1 = rnd(prng), r2 = rnd(prng), r3 = rnd(prng), r4 = rnd(prng);
+    LightSample ls = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), &pdf);
+    float W = 1.0f / pdf;
+    if (W > 0.0f) {
+      LightEval ev = load_eval(s, ls, sf.hit_point);
+      float3 sdir = normalize(ev.point - sf.hit_point);
+      float sdist = dist(ev.point, sf.hit_point);
+      float ndl = dot(sdir, sf.n);
+      if (ndl > 0.0f) {
+        float sp = 0.0f;
+        float3 refl = disney_eval(b, sf.frame, -wi, sdir, &sp);
+        val = throughput * refl * ev.emission * ndl * W;
+        so = sf.hit_point + sf.n * 1e-4f;
+        sd = sdir;
+        st = sdist - 1e-4f * 2.0f;
+        want = true;
+        sa.z |= TP_SHADOW;
+      }
+    }
+  } else {
+    val = f3s(0.0f) + throughput * sky_radiance(s, wi, true);
+    sa.z |= TP_DONE;
+  }
+  fb.st_a[id] = sa;
+  fb.st_c[id] = make_uint4(__float_as_uint(val.x), __float_as_uint(val.y), __float_as_uint(val.z), 0u);
+  push_ray(fb, Q_GI_SHADOW, want, so, st, sd, id);
+}
+
+// GI temporal, stage 3 (restir_gi_temporal.wgsl:97-116): the target, M cap and combine.
+__global__ void __launch_bounds__(256) k_gt_c(FrameBuffers fb, Consts c, const uint4* in_a, const uint4* in_b,
+                                              uint4* out_a, uint4* out_b, const uint4* prev_a, const uint4* prev_b,
+                                              uint4* pout_a, uint4* pout_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  uint32_t id = y * c.W + x;
+  uint4 pl = fb.payload[id];
+  if (__uint_as_float(pl.z) < 0.0f) return;
+  const uint4 sa = fb.st_a[id];
+  uint32_t rng = sa.x;
+  GiRes r = gi_unpack(in_a[id], in_b[id]);
+  if (sa.z & TP_HIST) {
+    GiRes pr = gi_unpack(prev_a[sa.y], prev_b[sa.y]);
+    pr.M = dm::fmin(pr.M, c.cfg.gi_temporal_m_cap);
+    const uint4 sc = fb.st_c[id];
+    const float3 val = f3(__uint_as_float(sc.x), __uint_as_float(sc.y), __uint_as_float(sc.z));
+    float3 acc = f3s(0.0f);
+    if (sa.z & TP_DONE) acc = val;
+    else if ((sa.z & TP_SHADOW) && fb.vis[Q_GI_SHADOW][id]) acc = acc + val;
+    pr.phat = luma(acc);
+    r = gi_combine(r, pr, rng);
   }
   out_a[id] = gi_pack_a(r);
   out_b[id] = gi_pack_b(r);
@@ -1165,38 +1373,6 @@ enum : uint32_t {
   SP_ZC_KNOWN = 16u, // target of the combined sample here known without a ray
   SP_MEMO = 32u,     // st_b/st_c.x hold a memoised target
 };
-
-// LightSample::phat split at its visibility test: the unshadowed target and the
-// shadow ray (helpers/trace.wgsl:7-18 offsets) that decides whether it counts.
-struct PhatSplit {
-  float value;
-  bool ray;
-  float3 o, d;
-  float tmax;
-};
-APD PhatSplit ls_phat_split(const DevScene& s, const LightSample& l, const uint4 c, float3 hit, float3 wo) {
-  LightEval ev = load_eval(s, l, hit);
-  Bsdf b = load_bsdf(s.materials + c.x);
-  Frame fr = ctx_frame(c);
-  float3 wi = normalize(ev.point - hit);
-  float wdn = dot(wi, fr.n);
-  PhatSplit r;
-  r.value = 0.0f;
-  r.ray = false;
-  r.o = f3s(0.0f);
-  r.d = f3s(0.0f);
-  r.tmax = 0.0f;
-  if (wdn > 0.0f) {
-    float sp = 0.0f;
-    float3 refl = disney_eval(b, fr, wo, wi, &sp);
-    r.value = luma(refl * wdn * ev.emission);
-    r.ray = __float_as_uint(r.value) != 0u;  // a +0 target is +0 whether or not the ray is occluded
-    r.o = hit + fr.n * 1e-4f;
-    r.d = wi;
-    r.tmax = dist(ev.point, hit) - 1e-4f * 2.0f;
-  }
-  return r;
-}
 
 __global__ void __launch_bounds__(256) k_dsp_ca(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
                                                 uint32_t pass_count, uint32_t nsamples, uint32_t i,
@@ -1718,7 +1894,7 @@ const char* kernel_kind_name(int k) {
   static const char* names[K_NUM_KINDS] = {"memset", "raygen", "extend", "shade", "di_temporal", "di_spatial",
                                            "gi_temporal", "gi_spatial", "apply_di", "apply_gi", "demodulate",
                                            "firefly", "svgf_temporal", "atrous", "taa", "resolve", "copy",
-                                           "trace_closest", "trace_any", "shade_b", "shade_c", "shade_d"};
+                                           "trace_closest", "trace_any", "shade_b", "shade_c", "shade_d", "shade_b2"};
   return (k >= 0 && k < K_NUM_KINDS) ? names[k] : "?";
 }
 
@@ -1781,6 +1957,8 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       mark(K_TRACE_CLOSEST);
       k_shade_b<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_SHADE_B);
+      k_shade_b2<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
+      mark(K_SHADE_B2);
       trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_RIS_SHADOW, P, nullptr, fb.vis[Q_RIS_SHADOW]);
       mark(K_TRACE_ANY);
       trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_GI_CAND, P, fb.hit_gi, nullptr);
@@ -1797,8 +1975,14 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
           uint4* pin_b = fb.di_prev_b[cur];
           uint4* pout_a = fb.di_prev_a[cur ^ 1u];
           uint4* pout_b = fb.di_prev_b[cur ^ 1u];
-          k_di_temporal<<<g2, b2, 0, st>>>(scene, fb, c, fb.di_a, fb.di_b, fb.di_inter_a, fb.di_inter_b, pin_a, pin_b,
-                                           pout_a, pout_b);
+          cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+          mark(K_MEMSET);
+          k_dt_a<<<g2, b2, 0, st>>>(scene, fb, c, pin_a, pin_b);
+          mark(K_DI_TEMPORAL);
+          trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_DI_SHADOW, P, nullptr, fb.vis[Q_DI_SHADOW]);
+          mark(K_TRACE_ANY);
+          k_dt_b<<<g2, b2, 0, st>>>(fb, c, fb.di_a, fb.di_b, fb.di_inter_a, fb.di_inter_b, pin_a, pin_b, pout_a,
+                                    pout_b);
           mark(K_DI_TEMPORAL);
           uint32_t n = cfg.di_spatial_passes;
           for (uint32_t k = 0; k < n; ++k) {
@@ -1843,8 +2027,18 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
           uint4* pin_b = fb.gi_prev_b[cur];
           uint4* pout_a = fb.gi_prev_a[cur ^ 1u];
           uint4* pout_b = fb.gi_prev_b[cur ^ 1u];
-          k_gi_temporal<<<g2, b2, 0, st>>>(scene, fb, c, fb.gi_a, fb.gi_b, fb.gi_inter_a, fb.gi_inter_b, pin_a, pin_b,
-                                           pout_a, pout_b);
+          cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+          mark(K_MEMSET);
+          k_gt_a<<<g2, b2, 0, st>>>(scene, fb, c, pin_a, pin_b);
+          mark(K_GI_TEMPORAL);
+          trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_GI_CAND, P, fb.hit_gi, nullptr);
+          mark(K_TRACE_CLOSEST);
+          k_gt_b<<<g2, b2, 0, st>>>(scene, fb, c, pin_a, pin_b);
+          mark(K_GI_TEMPORAL);
+          trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, P, nullptr, fb.vis[Q_GI_SHADOW]);
+          mark(K_TRACE_ANY);
+          k_gt_c<<<g2, b2, 0, st>>>(fb, c, fb.gi_a, fb.gi_b, fb.gi_inter_a, fb.gi_inter_b, pin_a, pin_b, pout_a,
+                                    pout_b);
           mark(K_GI_TEMPORAL);
           uint32_t n = cfg.gi_spatial_passes;
           if (n == 0) {
@@ -1866,6 +2060,11 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
             mark(K_COPY);
           }
         }
+      }
+      if (i == 0 && (cfg.restir_di || cfg.restir_gi)) {
+        // the resampling passes used the ray queues: start the DI shadow queue empty
+        cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+        mark(K_MEMSET);
       }
       k_apply_di_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_APPLY_DI);

@@ -79,7 +79,7 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb);
 enum KernelKind : int {
   K_MEMSET = 0, K_RAYGEN, K_EXTEND, K_SHADE, K_DI_TEMPORAL, K_DI_SPATIAL, K_GI_TEMPORAL, K_GI_SPATIAL,
   K_APPLY_DI, K_APPLY_GI, K_DEMODULATE, K_FIREFLY, K_SVGF_TEMPORAL, K_ATROUS, K_TAA, K_RESOLVE, K_COPY,
-  K_TRACE_CLOSEST, K_TRACE_ANY, K_SHADE_B, K_SHADE_C, K_SHADE_D, K_NUM_KINDS
+  K_TRACE_CLOSEST, K_TRACE_ANY, K_SHADE_B, K_SHADE_C, K_SHADE_D, K_SHADE_B2, K_NUM_KINDS
 };
 const char* kernel_kind_name(int k);
 

@@ -140,7 +140,12 @@ APD NodeFrame node_frame(const uint4 w0, const RayPre& r) {
 
 constexpr float kGrow = 1.0f + 4.8e-7f;  // relative 2^-21
 
-APD float byte_at(uint32_t word, int k) { return __uint2float_rn((word >> (8 * k)) & 0xffu); }
+// Byte k of `word` as a float.  Exact: the byte is placed under the exponent
+// of 2^23 (0x4B000000) with one byte permute, and 2^23 + b - 2^23 = b exactly;
+// this keeps the 48 conversions of a node off the conversion pipe.
+APD float byte_at(uint32_t word, int k) {
+  return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
+}
 
 // Entry distance of child i (a compile-time index after unrolling) or +inf
 // when its box is missed inside [tmin, tmax].
@@ -192,11 +197,20 @@ struct Visits {
 // visited next and the others are pushed with their entry distance, culled on
 // pop; any hit: stops at the first accepted triangle.  The traversal stack
 // holds at most BvhStats::max_stack entries (checked at build).
+//
+// One step is either one node (8 child boxes) or one triangle: the triangles
+// of a node's leaf children (at most 24, stored contiguously from the node's
+// triangle base) become a pending bit mask that the following steps test one
+// at a time, before the next node.  Short, uniform steps keep the lanes of a
+// warp on the same path more of the time than testing all of a node's
+// triangles at once.
 struct Trav {
   RayPre r;
   Hit hit;          // closest: best so far (hit.t doubles as tmax); any: hit.tri != kNoHit when occluded
   float tmax;       // any-hit query range
   uint32_t node;
+  float node_t;     // entry distance of `node` (closest hit)
+  uint32_t tri_base, tri_mask;  // pending triangles: tri_base + bit index
   int sp;
   bool have;        // `node` is the next node to visit
 };
@@ -209,16 +223,42 @@ APD void trav_init(Trav& t, float3 o, float3 d, float tmax) {
   t.hit.tri = kNoHit;
   t.tmax = tmax;
   t.node = 0;
+  t.node_t = 0.0f;
+  t.tri_base = 0;
+  t.tri_mask = 0;
   t.sp = 0;
   t.have = true;
 }
 
-// Visits up to `budget` nodes; returns true when the ray is finished.  kUnroll
-// unrolls the 8 child tests (dedicated traversal kernels); the rolled form keeps
-// the code small where traversal is inlined into large shading kernels.
+// Runs up to `budget` steps; returns true when the ray is finished.  kUnroll
+// unrolls the 8 child tests.
 template <bool kAny, bool kCount, bool kUnroll = false>
 APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits* vc) {
   for (int step = 0; step < budget; ++step) {
+    if (t.tri_mask) {
+      const int j = __ffs(t.tri_mask) - 1;
+      t.tri_mask &= t.tri_mask - 1;
+      if (kCount) vc->tris++;
+      const float4* tp = s.tris + 3 * (size_t)(t.tri_base + j);
+      const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+      float th, u, v;
+      const float lim = kAny ? t.tmax : t.hit.t;
+      if (intersect_tri(t.r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), 0.0f, lim, th, u, v)) {
+        const uint32_t gid = __float_as_uint(a.w);
+        if (kAny) {
+          t.hit.tri = gid;
+          return true;
+        }
+        if (th < t.hit.t || gid < t.hit.tri) {  // th <= hit.t here: strictly closer or a tie
+          t.hit.t = th;
+          t.hit.u = u;
+          t.hit.v = v;
+          t.hit.tri = gid;
+        }
+      }
+      continue;
+    }
+    if (t.have && !kAny && t.node_t > t.hit.t * kGrow) t.have = false;  // culled by a hit found since
     if (!t.have) {
       bool got = false;
       while (t.sp > 0) {
@@ -237,7 +277,7 @@ APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits*
     const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
     const NodeFrame f = node_frame(w0, t.r);
     const float range = kAny ? t.tmax : t.hit.t;
-    uint32_t leaf_mask = 0;
+    uint32_t tri_mask = 0;
     float best_t = __uint_as_float(0x7f800000u);
     uint32_t best_node = 0;
 #pragma unroll(kUnroll ? 8 : 1)
@@ -247,7 +287,7 @@ APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits*
       const float tn = child_entry(f, w2, w3, w4, t.r, i, 0.0f, range);
       if (!(tn < __uint_as_float(0x7f800000u))) continue;
       if (meta & 0xe0u) {
-        leaf_mask |= 1u << i;
+        tri_mask |= (meta >> 5) << (meta & 0x1fu);  // unary count at the leaf's offset
       } else {
         const uint32_t child = w1.x + (meta & 7u);
         if (kAny) {
@@ -267,35 +307,12 @@ APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits*
         }
       }
     }
-    if (!kAny) t.node = best_node;
-    while (leaf_mask) {
-      const int i = __ffs(leaf_mask) - 1;
-      leaf_mask &= leaf_mask - 1;
-      const uint32_t meta = meta_of(w1, i);
-      const uint32_t first = w1.y + (meta & 0x1fu);
-      const uint32_t cnt = __popc(meta >> 5);
-      if (kCount) vc->tris += cnt;
-      for (uint32_t k = 0; k < cnt; ++k) {
-        const float4* tp = s.tris + 3 * (size_t)(first + k);
-        const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
-        float th, u, v;
-        const float lim = kAny ? t.tmax : t.hit.t;
-        if (intersect_tri(t.r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), 0.0f, lim, th, u, v)) {
-          const uint32_t gid = __float_as_uint(a.w);
-          if (kAny) {
-            t.hit.tri = gid;
-            return true;
-          }
-          if (th < t.hit.t || gid < t.hit.tri) {  // th <= hit.t here: strictly closer or a tie
-            t.hit.t = th;
-            t.hit.u = u;
-            t.hit.v = v;
-            t.hit.tri = gid;
-          }
-        }
-      }
+    if (!kAny) {
+      t.node = best_node;
+      t.node_t = best_t;
     }
-    if (!kAny && t.have && best_t > t.hit.t * kGrow) t.have = false;  // the nearest child is now culled
+    t.tri_base = w1.y;
+    t.tri_mask = tri_mask;
   }
   return false;
 }
