@@ -16,7 +16,8 @@ AP_OK, AP_E_INVALID, AP_E_OOM, AP_E_CUDA, AP_E_TIMEOUT, AP_E_UNSUPPORTED, AP_E_N
 EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error", "ap_set_config",
            "ap_world_action", "ap_scene_upload", "ap_set_camera_matrices", "ap_render_hdr", "ap_render_device",
            "ap_device_framebuffer", "ap_trace_rays", "ap_trace_rays_static", "ap_read_buffer", "ap_profile_frame",
-           "ap_bvh_stats"]
+           "ap_bvh_stats", "ap_server_create", "ap_server_destroy", "ap_server_last_error", "ap_server_add_scene",
+           "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_stats"]
 
 U32, F32, P = ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p
 
@@ -44,6 +45,16 @@ class SceneDesc(ctypes.Structure):
 class FrameStats(ctypes.Structure):
     _fields_ = [("gpu_ms", ctypes.c_double), ("extension_rays", ctypes.c_uint64), ("width", U32),
                 ("height", U32), ("frame_idx", U32), ("kernel_launches", U32)]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("scene", U32), ("width", U32), ("height", U32), ("spp", U32), ("max_depth", U32), ("seed", U32),
+                ("mats", F32 * 64)]
+
+
+class JobResult(ctypes.Structure):
+    _fields_ = [("queued_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("gpu_ms", ctypes.c_double),
+                ("device_bytes", ctypes.c_uint64), ("graph_mode", U32), ("slot", U32)]
 
 
 _lib = None
@@ -76,5 +87,18 @@ def load() -> ctypes.CDLL:
     L.ap_read_buffer.argtypes = [P, U32, P, ctypes.c_size_t]
     L.ap_bvh_stats.argtypes = [P, P]
     L.ap_profile_frame.argtypes = [P, U32, U32, P, P, P, U32, P, ctypes.c_int, P, ctypes.POINTER(FrameStats)]
+    L.ap_server_create.restype = P
+    L.ap_server_create.argtypes = [ctypes.POINTER(FrameConfig), ctypes.c_int, ctypes.c_uint64, U32, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_int)]
+    L.ap_server_destroy.argtypes = [P]
+    L.ap_server_last_error.restype = ctypes.c_char_p
+    L.ap_server_last_error.argtypes = [P]
+    L.ap_server_add_scene.argtypes = [P, ctypes.POINTER(SceneDesc), ctypes.POINTER(U32)]
+    L.ap_server_job_bytes.restype = ctypes.c_uint64
+    L.ap_server_job_bytes.argtypes = [U32, U32]
+    L.ap_server_submit.argtypes = [P, ctypes.POINTER(Job), P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]
+    L.ap_server_query.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]
+    L.ap_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(JobResult)]
+    L.ap_server_stats.argtypes = [P, P]
     _lib = L
     return L

@@ -38,6 +38,7 @@ struct DeviceScene {
   void* env = nullptr;
   DevScene view{};
   BvhStats stats{};
+  size_t bytes = 0;  // device memory held
   bool valid = false;
   void release() {
     void** all[] = {&nodes, &tris, &positions, &normals, &indices, &tri_material, &tri_instance,
@@ -47,6 +48,7 @@ struct DeviceScene {
       if (*p) cudaFree(*p);
       *p = nullptr;
     }
+    bytes = 0;
     valid = false;
   }
 };
@@ -94,6 +96,7 @@ int upload(Handle* h, void** dst, const T* src, size_t count) {
   size_t bytes = std::max<size_t>(count * sizeof(T), 16);
   int rc = check_cuda(h, cudaMalloc(dst, bytes), "cudaMalloc");
   if (rc) return rc;
+  h->scene.bytes += bytes;
   if (count) rc = check_cuda(h, cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice), "upload");
   return rc;
 }
@@ -276,6 +279,12 @@ int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream,
   *num_sms = h->num_sms;
   *device = h->device;
   return AP_OK;
+}
+
+// Device bytes held by a handle's scene (0 without one).
+size_t handle_scene_bytes(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  return (h && h->scene.valid) ? h->scene.bytes : 0;
 }
 }  // namespace ap
 
@@ -543,6 +552,7 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
     }
   }
   s.stats = bvh.stats;
+  s.bytes += std::max<size_t>(4 * (size_t)d->num_vertices, 16) + std::max<size_t>(sizeof(EmissiveTri) * num_emissive_tris, 16);
   s.valid = true;
   return AP_OK;
 }

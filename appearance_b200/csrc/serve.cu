@@ -1,0 +1,484 @@
+// Render-serving loop (include/appearance_cuda.h, "serving"): resident scenes,
+// jobs of mixed resolution / samples / scene admitted as device memory and
+// execution slots free up, and run concurrently, each on its own stream.
+//
+// The reference serves frames through a synchronous frame farm (Host/Node,
+// crates/appearance-render-loop/src/host.rs:250-505, node.rs:27-147): one
+// resident renderer per node renders the rows it is asked for, one request at
+// a time.  Here one process owns the GPU and keeps every scene's BVH and
+// tables resident; a dispatcher thread admits queued jobs in arrival order
+// while their frame state fits the device-memory budget and a slot is free,
+// allocates that state from the stream-ordered pool (cudaMallocAsync, no
+// device-wide synchronisation), and launches the job's frame (the same
+// encode_frame as ap_render_*) on the slot's stream, optionally as a CUDA graph
+// captured once per job shape and updated in place for later jobs.  Jobs in
+// flight overlap on the device; a host callback on each stream wakes the
+// dispatcher when a job's result has reached host memory.  A job's result is
+// a function of its own inputs only (its seed, camera, scene and sizes), so it
+// is the same alone and in any mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/appearance_cuda.h"
+#include "frame.cuh"
+
+namespace ap {
+int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream, int* num_sms, int* device,
+                         std::string** err);
+size_t handle_scene_bytes(void* hp);
+}  // namespace ap
+
+namespace {
+
+using namespace ap;
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct Job {
+  uint64_t ticket = 0;
+  ap_job desc{};
+  float* out = nullptr;
+  bool out_pinned = false;
+  Clock::time_point t_submit, t_admit, t_done;
+  int slot = -1;
+  void* dev = nullptr;
+  size_t bytes = 0;
+  bool done = false;
+  int rc = AP_OK;
+  std::string err;
+  double gpu_ms = 0.0;
+  int graph_mode = 0;  // 0 direct launches, 1 graph instantiated, 2 graph updated in place
+};
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float* staging = nullptr;  // pinned, for callers whose output buffer is pageable
+  size_t staging_bytes = 0;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t exec_key = 0;
+  Job* job = nullptr;
+  bool finished = false;  // set by the stream callback
+};
+
+struct Server {
+  int device = 0;
+  int num_sms = 148;
+  uint64_t budget = 0;
+  int use_graphs = 0;
+  FrameConfig base{};
+  std::vector<void*> scenes;
+  size_t scene_bytes = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Job*> pending;
+  std::map<uint64_t, Job*> jobs;
+  std::vector<Slot> slots;
+  size_t in_use = 0, peak = 0;
+  uint64_t next_ticket = 1, completed = 0;
+  std::atomic<uint64_t> graph_updates{0}, graph_instantiations{0};  // written by the dispatcher
+  bool stop = false;
+  std::thread worker;
+  std::string err;
+};
+
+struct CallbackArg {
+  Server* srv;
+  int slot;
+};
+
+void CUDART_CB on_slot_done(void* p) {  // runs on a CUDA callback thread: no CUDA calls here
+  CallbackArg* a = static_cast<CallbackArg*>(p);
+  {
+    std::lock_guard<std::mutex> lk(a->srv->mu);
+    a->srv->slots[a->slot].finished = true;
+  }
+  a->srv->cv_work.notify_one();
+  delete a;
+}
+
+uint64_t shape_key(const ap_job& j, const FrameConfig& cfg) {
+  uint64_t k = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) { k = (k ^ v) * 1099511628211ull; };
+  mix(j.width);
+  mix(j.height);
+  mix(cfg.sample_count);
+  mix(cfg.max_bounces);
+  mix(j.scene);
+  return k;
+}
+
+// Enqueues one admitted job on its slot's stream (dispatcher thread, no lock
+// held).  Returns false when nothing was enqueued (the job failed up front).
+bool launch_job(Server* s, Job* j, Slot& sl) {
+  const ap_job& d = j->desc;
+  const DevScene* scene = nullptr;
+  cudaStream_t unused_stream;
+  int sms = 0, dev = 0;
+  std::string* err = nullptr;
+  ap::handle_trace_context(s->scenes[d.scene], &scene, &unused_stream, &sms, &dev, &err);
+  FrameConfig cfg = s->base;
+  cfg.sample_count = d.spp;
+  cfg.max_bounces = d.max_depth;
+  const size_t out_bytes = (size_t)d.width * d.height * 12;
+  cudaError_t e = cudaMallocAsync(&j->dev, j->bytes, sl.stream);
+  if (e != cudaSuccess) {
+    j->rc = e == cudaErrorMemoryAllocation ? AP_E_OOM : AP_E_CUDA;
+    j->err = std::string("job frame state: ") + cudaGetErrorString(e);
+    j->dev = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  cudaMemsetAsync(j->dev, 0, j->bytes, sl.stream);  // a job starts from a fresh frame sequence
+  FrameBuffers fb{};
+  frame_buffers_carve(j->dev, d.width, d.height, &fb);
+  Mats mats;
+  std::memcpy(&mats, d.mats, sizeof(Mats));
+  float* dst = j->out_pinned ? j->out : sl.staging;
+  cudaEventRecord(sl.ev0, sl.stream);
+  if (s->use_graphs) {
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      encode_frame(*scene, fb, cfg, mats, d.width, d.height, d.seed, s->num_sms, sl.stream, nullptr);
+      cudaMemcpyAsync(dst, fb.out_rgb, out_bytes, cudaMemcpyDeviceToHost, sl.stream);
+      e = cudaStreamEndCapture(sl.stream, &g);
+    }
+    if (e == cudaSuccess) {
+      const uint64_t key = shape_key(d, cfg);
+      cudaGraphExecUpdateResultInfo info;
+      if (sl.exec && sl.exec_key == key && cudaGraphExecUpdate(sl.exec, g, &info) == cudaSuccess) {
+        j->graph_mode = 2;
+        s->graph_updates++;
+      } else {
+        cudaGetLastError();  // a failed update leaves a recoverable error
+        if (sl.exec) cudaGraphExecDestroy(sl.exec);
+        sl.exec = nullptr;
+        e = cudaGraphInstantiate(&sl.exec, g, 0);
+        sl.exec_key = key;
+        j->graph_mode = 1;
+        s->graph_instantiations++;
+      }
+      cudaGraphDestroy(g);
+      if (e == cudaSuccess) e = cudaGraphLaunch(sl.exec, sl.stream);
+    }
+  } else {
+    encode_frame(*scene, fb, cfg, mats, d.width, d.height, d.seed, s->num_sms, sl.stream, nullptr);
+    cudaMemcpyAsync(dst, fb.out_rgb, out_bytes, cudaMemcpyDeviceToHost, sl.stream);
+    e = cudaGetLastError();
+  }
+  cudaEventRecord(sl.ev1, sl.stream);
+  if (e != cudaSuccess) {
+    j->rc = AP_E_CUDA;
+    j->err = std::string("job launch: ") + cudaGetErrorString(e);
+  }
+  cudaLaunchHostFunc(sl.stream, on_slot_done, new CallbackArg{s, j->slot});
+  return true;
+}
+
+void dispatcher(Server* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    // completions
+    for (size_t i = 0; i < s->slots.size(); ++i) {
+      Slot& sl = s->slots[i];
+      if (!sl.job || !sl.finished) continue;
+      Job* j = sl.job;
+      cudaError_t e = cudaEventSynchronize(sl.ev1);  // already complete: returns at once
+      float ms = 0.0f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
+      if (e != cudaSuccess && j->rc == AP_OK) {
+        j->rc = AP_E_CUDA;
+        j->err = std::string("job: ") + cudaGetErrorString(e);
+      }
+      if (j->rc == AP_OK && !j->out_pinned)
+        std::memcpy(j->out, sl.staging, (size_t)j->desc.width * j->desc.height * 12);
+      if (j->dev) cudaFreeAsync(j->dev, sl.stream);
+      j->dev = nullptr;
+      s->in_use -= j->bytes;
+      j->gpu_ms = ms;
+      j->t_done = Clock::now();
+      j->done = true;
+      s->completed++;
+      sl.job = nullptr;
+      sl.finished = false;
+      s->cv_done.notify_all();
+    }
+    // admissions, in arrival order
+    while (!s->pending.empty()) {
+      int free_slot = -1;
+      for (size_t i = 0; i < s->slots.size(); ++i)
+        if (!s->slots[i].job) {
+          free_slot = (int)i;
+          break;
+        }
+      if (free_slot < 0) break;
+      Job* j = s->pending.front();
+      if (s->scene_bytes + s->in_use + j->bytes > s->budget) {
+        if (s->in_use == 0) {  // cannot fit even alone
+          s->pending.pop_front();
+          j->rc = AP_E_OOM;
+          j->err = "job frame state exceeds the device-memory budget";
+          j->t_admit = j->t_done = Clock::now();
+          j->done = true;
+          s->completed++;
+          s->cv_done.notify_all();
+          continue;
+        }
+        break;  // wait for memory to free up
+      }
+      s->pending.pop_front();
+      Slot& sl = s->slots[free_slot];
+      const size_t out_bytes = (size_t)j->desc.width * j->desc.height * 12;
+      if (!j->out_pinned && sl.staging_bytes < out_bytes) {
+        lk.unlock();
+        if (sl.staging) cudaFreeHost(sl.staging);
+        sl.staging = nullptr;
+        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&sl.staging), out_bytes, cudaHostAllocDefault);
+        lk.lock();
+        sl.staging_bytes = e == cudaSuccess ? out_bytes : 0;
+        if (e != cudaSuccess) {
+          sl.staging = nullptr;
+          j->rc = AP_E_OOM;
+          j->err = "pinned staging buffer";
+          j->t_admit = j->t_done = Clock::now();
+          j->done = true;
+          s->completed++;
+          s->cv_done.notify_all();
+          continue;
+        }
+      }
+      j->slot = free_slot;
+      j->t_admit = Clock::now();
+      s->in_use += j->bytes;
+      s->peak = std::max(s->peak, s->scene_bytes + s->in_use);
+      sl.job = j;
+      sl.finished = false;
+      lk.unlock();
+      const bool enqueued = launch_job(s, j, sl);
+      lk.lock();
+      if (!enqueued) {
+        s->in_use -= j->bytes;
+        j->t_done = Clock::now();
+        j->done = true;
+        s->completed++;
+        sl.job = nullptr;
+        s->cv_done.notify_all();
+      }
+    }
+    bool inflight = false;
+    for (const Slot& sl : s->slots) inflight = inflight || sl.job;
+    if (s->stop && s->pending.empty() && !inflight) break;
+    bool ready = false;
+    for (const Slot& sl : s->slots) ready = ready || (sl.job && sl.finished);
+    if (!ready) s->cv_work.wait(lk);
+  }
+}
+
+int srv_fail(Server* s, int code, const std::string& msg) {
+  if (s) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->err = msg;
+  }
+  return code;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* ap_server_create(const ap_frame_config* cfg, int device, uint64_t hbm_budget, uint32_t max_inflight,
+                       int use_graphs, int* err) {
+  if (err) *err = AP_OK;
+  if (!cfg || max_inflight == 0 || max_inflight > 64 || hbm_budget == 0) {
+    if (err) *err = AP_E_INVALID;
+    return nullptr;
+  }
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    if (err) *err = AP_E_CUDA;
+    return nullptr;
+  }
+  cudaSetDevice(device);
+  Server* s = new Server;
+  s->device = device;
+  s->budget = hbm_budget;
+  s->use_graphs = use_graphs;
+  std::memcpy(&s->base, cfg, sizeof(FrameConfig));
+  cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
+  // keep freed job state in the pool (no release back to the driver between jobs)
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  s->slots.resize(max_inflight);
+  for (Slot& sl : s->slots) {
+    if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&sl.ev0) != cudaSuccess || cudaEventCreate(&sl.ev1) != cudaSuccess) {
+      if (err) *err = AP_E_CUDA;
+      for (Slot& t : s->slots) {
+        if (t.stream) cudaStreamDestroy(t.stream);
+        if (t.ev0) cudaEventDestroy(t.ev0);
+        if (t.ev1) cudaEventDestroy(t.ev1);
+      }
+      delete s;
+      return nullptr;
+    }
+  }
+  s->worker = std::thread(dispatcher, s);
+  return s;
+}
+
+void ap_server_destroy(void* sp) {
+  Server* s = static_cast<Server*>(sp);
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();  // drains queued and in-flight jobs
+  cudaSetDevice(s->device);
+  for (Slot& sl : s->slots) {
+    if (sl.stream) cudaStreamSynchronize(sl.stream);
+    if (sl.exec) cudaGraphExecDestroy(sl.exec);
+    if (sl.staging) cudaFreeHost(sl.staging);
+    if (sl.ev0) cudaEventDestroy(sl.ev0);
+    if (sl.ev1) cudaEventDestroy(sl.ev1);
+    if (sl.stream) cudaStreamDestroy(sl.stream);
+  }
+  for (auto& kv : s->jobs) delete kv.second;
+  for (void* h : s->scenes) ap_destroy(h);
+  delete s;
+}
+
+const char* ap_server_last_error(const void* sp) {
+  const Server* s = static_cast<const Server*>(sp);
+  return s ? s->err.c_str() : "null server";
+}
+
+int ap_server_add_scene(void* sp, const ap_scene_desc* desc, uint32_t* scene_id) {
+  Server* s = static_cast<Server*>(sp);
+  if (!s || !desc || !scene_id) return AP_E_INVALID;
+  int e = 0;
+  void* h = ap_create(reinterpret_cast<const ap_frame_config*>(&s->base), s->device, &e);
+  if (!h) return srv_fail(s, e ? e : AP_E_CUDA, "scene handle");
+  int rc = ap_scene_upload(h, desc);
+  if (rc != AP_OK) {
+    std::string msg = ap_last_error(h);
+    ap_destroy(h);
+    return srv_fail(s, rc, "scene upload: " + msg);
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->scenes.push_back(h);
+  s->scene_bytes += ap::handle_scene_bytes(h);
+  *scene_id = (uint32_t)(s->scenes.size() - 1);
+  return AP_OK;
+}
+
+uint64_t ap_server_job_bytes(uint32_t width, uint32_t height) { return frame_buffer_bytes(width, height); }
+
+int ap_server_submit(void* sp, const ap_job* job, float* out_rgb, size_t out_bytes, uint64_t* ticket) {
+  Server* s = static_cast<Server*>(sp);
+  if (!s || !job || !out_rgb || !ticket) return AP_E_INVALID;
+  if (job->width == 0 || job->height == 0 || (uint64_t)job->width * job->height > (1ull << 26))
+    return srv_fail(s, AP_E_INVALID, "job: bad resolution");
+  if (job->spp == 0 || job->spp > 4096 || job->max_depth == 0 || job->max_depth > 64)
+    return srv_fail(s, AP_E_INVALID, "job: spp or depth out of range");
+  if (out_bytes < (size_t)job->width * job->height * 12) return srv_fail(s, AP_E_INVALID, "job: output buffer too small");
+  cudaPointerAttributes attr;
+  bool pinned = cudaPointerGetAttributes(&attr, out_rgb) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  Job* j = new Job;
+  j->desc = *job;
+  j->out = out_rgb;
+  j->out_pinned = pinned;
+  j->bytes = frame_buffer_bytes(job->width, job->height);
+  j->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (job->scene >= s->scenes.size()) {
+      delete j;
+      s->err = "job: unknown scene";
+      return AP_E_INVALID;
+    }
+    j->ticket = s->next_ticket++;
+    s->jobs[j->ticket] = j;
+    s->pending.push_back(j);
+    *ticket = j->ticket;
+  }
+  s->cv_work.notify_one();
+  return AP_OK;
+}
+
+int ap_server_query(void* sp, uint64_t ticket, int* done) {
+  Server* s = static_cast<Server*>(sp);
+  if (!s || !done) return AP_E_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return AP_E_INVALID;
+  *done = it->second->done ? 1 : 0;
+  return AP_OK;
+}
+
+int ap_server_wait(void* sp, uint64_t ticket, ap_job_result* res) {
+  Server* s = static_cast<Server*>(sp);
+  if (!s) return AP_E_INVALID;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) {
+    s->err = "unknown ticket";
+    return AP_E_INVALID;
+  }
+  Job* j = it->second;
+  s->cv_done.wait(lk, [&] { return j->done; });
+  if (res) {
+    res->queued_ms = ms_between(j->t_submit, j->t_admit);
+    res->total_ms = ms_between(j->t_submit, j->t_done);
+    res->gpu_ms = j->gpu_ms;
+    res->device_bytes = j->bytes;
+    res->graph_mode = (uint32_t)j->graph_mode;
+    res->slot = (uint32_t)j->slot;
+  }
+  int rc = j->rc;
+  if (rc != AP_OK) s->err = j->err;
+  s->jobs.erase(it);
+  delete j;
+  return rc;
+}
+
+int ap_server_stats(void* sp, uint64_t* out8) {
+  Server* s = static_cast<Server*>(sp);
+  if (!s || !out8) return AP_E_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  uint64_t inflight = 0;
+  for (const Slot& sl : s->slots) inflight += sl.job ? 1 : 0;
+  out8[0] = s->completed;
+  out8[1] = inflight;
+  out8[2] = s->pending.size();
+  out8[3] = s->scene_bytes + s->in_use;
+  out8[4] = s->peak;
+  out8[5] = s->scene_bytes;
+  out8[6] = s->graph_instantiations.load();
+  out8[7] = s->graph_updates.load();
+  return AP_OK;
+}
+
+}  // extern "C"

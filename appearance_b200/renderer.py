@@ -40,6 +40,30 @@ def config_struct(cfg: dict | None) -> _native.FrameConfig:
     return c
 
 
+def scene_desc(scene: Scene):
+    """ap_scene_desc for a Scene, and the arrays it points into (keep them alive
+    until the upload returns)."""
+    keep = dict(pos=np.ascontiguousarray(scene.positions, np.float32),
+                nrm=np.ascontiguousarray(scene.normals, np.float32),
+                idx=np.ascontiguousarray(scene.indices, np.uint32),
+                tm=np.ascontiguousarray(scene.tri_material, np.uint32),
+                mesh=np.ascontiguousarray(scene.meshes, np.uint32),
+                mat=np.ascontiguousarray(scene.materials, np.float32),
+                env=None if scene.env is None else np.ascontiguousarray(scene.env, np.float32))
+    d = _native.SceneDesc()
+    d.positions, d.normals = _ptr(keep["pos"]), _ptr(keep["nrm"])
+    d.num_vertices = keep["pos"].shape[0]
+    d.indices, d.tri_material = _ptr(keep["idx"]), _ptr(keep["tm"])
+    d.num_tris = keep["idx"].shape[0]
+    d.meshes, d.num_meshes = _ptr(keep["mesh"]), keep["mesh"].shape[0]
+    d.materials, d.num_materials = _ptr(keep["mat"]), keep["mat"].shape[0]
+    if keep["env"] is not None:
+        d.env, d.env_h, d.env_w = _ptr(keep["env"]), keep["env"].shape[0], keep["env"].shape[1]
+    for i in range(8):
+        d.sun[i] = float(scene.sun[i])
+    return d, keep
+
+
 class PathTracer:
     """One renderer instance (one CUDA stream, persistent temporal state)."""
 
@@ -85,24 +109,7 @@ class PathTracer:
         return m.tobytes() + struct.pack("<fffI", fov_deg, near, far, 0)
 
     def upload_scene(self, scene: Scene):
-        keep = dict(pos=np.ascontiguousarray(scene.positions, np.float32),
-                    nrm=np.ascontiguousarray(scene.normals, np.float32),
-                    idx=np.ascontiguousarray(scene.indices, np.uint32),
-                    tm=np.ascontiguousarray(scene.tri_material, np.uint32),
-                    mesh=np.ascontiguousarray(scene.meshes, np.uint32),
-                    mat=np.ascontiguousarray(scene.materials, np.float32),
-                    env=None if scene.env is None else np.ascontiguousarray(scene.env, np.float32))
-        d = _native.SceneDesc()
-        d.positions, d.normals = _ptr(keep["pos"]), _ptr(keep["nrm"])
-        d.num_vertices = keep["pos"].shape[0]
-        d.indices, d.tri_material = _ptr(keep["idx"]), _ptr(keep["tm"])
-        d.num_tris = keep["idx"].shape[0]
-        d.meshes, d.num_meshes = _ptr(keep["mesh"]), keep["mesh"].shape[0]
-        d.materials, d.num_materials = _ptr(keep["mat"]), keep["mat"].shape[0]
-        if keep["env"] is not None:
-            d.env, d.env_h, d.env_w = _ptr(keep["env"]), keep["env"].shape[0], keep["env"].shape[1]
-        for i in range(8):
-            d.sun[i] = float(scene.sun[i])
+        d, self._scene_keep = scene_desc(scene)
         self._check(self._lib.ap_scene_upload(self._h, ctypes.byref(d)))
 
     def set_camera_matrices(self, mats: np.ndarray):

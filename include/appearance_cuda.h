@@ -197,6 +197,57 @@ int ap_profile_frame(void* handle, uint32_t w, uint32_t h, double* kind_ms, uint
  * traversal stack, build ms (as double bits in out[4..5]). */
 int ap_bvh_stats(void* handle, uint32_t* out8);
 
+/* ---- render-serving loop ------------------------------------------------
+ * No reference counterpart as an API: it takes the role of the reference's
+ * frame farm (Host/Node, crates/appearance-render-loop/src/host.rs:250-505,
+ * node.rs:27-147), where each node renders one request at a time.  Here one
+ * server owns the GPU: scenes stay resident, submitted jobs are admitted in
+ * arrival order while their frame state fits `hbm_budget` (scene bytes
+ * included) and one of `max_inflight` slots is free, and jobs in flight run
+ * concurrently, one stream each.  A job renders `spp` samples per pixel with
+ * `max_depth` bounces using the server's frame configuration otherwise, from
+ * a fresh frame sequence with PCG frame index `seed`; its result is the same
+ * alone and in any mix of jobs.  use_graphs != 0 launches each job as a CUDA
+ * graph (captured per job, updated in place when a slot's previous job had
+ * the same shape).  The server's dispatcher thread and CUDA callbacks do the
+ * work; all entry points are thread-safe. */
+typedef struct ap_job {
+  uint32_t scene;           /* id from ap_server_add_scene */
+  uint32_t width, height;
+  uint32_t spp;             /* 1..4096 */
+  uint32_t max_depth;       /* bounces, 1..64 */
+  uint32_t seed;            /* frame index of the per-pixel PCG streams */
+  float mats[64];           /* inv_view, inv_proj, view_proj, prev_view_proj (column-major) */
+} ap_job;
+
+typedef struct ap_job_result {
+  double queued_ms;         /* submit -> admitted */
+  double total_ms;          /* submit -> result in the caller's buffer */
+  double gpu_ms;            /* the job's span on its stream (CUDA events) */
+  uint64_t device_bytes;    /* frame state held while it ran */
+  uint32_t graph_mode;      /* 0 direct launches, 1 graph instantiated, 2 graph updated in place */
+  uint32_t slot;
+} ap_job_result;
+
+void* ap_server_create(const ap_frame_config* cfg, int device, uint64_t hbm_budget, uint32_t max_inflight,
+                       int use_graphs, int* err);
+/* Finishes queued and in-flight jobs, then frees everything. */
+void ap_server_destroy(void* server);
+const char* ap_server_last_error(const void* server);
+int ap_server_add_scene(void* server, const ap_scene_desc* desc, uint32_t* scene_id);
+/* Device bytes of one job's frame state at width x height. */
+uint64_t ap_server_job_bytes(uint32_t width, uint32_t height);
+/* Queues a job; returns at once.  The linear HDR RGB f32 result (w*h*3 floats,
+ * row-major) is written to out_rgb, which must stay valid until the job is
+ * waited for; page-locked memory (cudaHostAlloc) receives it directly. */
+int ap_server_submit(void* server, const ap_job* job, float* out_rgb, size_t out_bytes, uint64_t* ticket);
+int ap_server_query(void* server, uint64_t ticket, int* done);
+/* Blocks until the job is done; returns its status and releases the ticket. */
+int ap_server_wait(void* server, uint64_t ticket, ap_job_result* result);
+/* completed, in flight, queued, device bytes in use, peak device bytes, scene
+ * bytes, graphs instantiated, graphs updated in place */
+int ap_server_stats(void* server, uint64_t* out8);
+
 #ifdef __cplusplus
 }
 #endif
