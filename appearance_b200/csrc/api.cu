@@ -78,6 +78,7 @@ struct Handle {
   size_t trace_bytes = 0;
   uint64_t ext_rays = 0;
   FrameProfiler prof;
+  uint32_t accum_count = 0;  // frames in the display accumulation (resolve.wgsl accum_frame_count)
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -223,6 +224,7 @@ int ensure_frame(Handle* h, uint32_t w, uint32_t hgt) {
   h->W = w;
   h->H = hgt;
   h->frame_idx = 0;  // SizedResources::new restarts the temporal state
+  h->accum_count = 0;
   return AP_OK;
 }
 
@@ -576,6 +578,31 @@ int ap_render_hdr(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32
   int rc = render_common(h, w, hgt, stats);
   if (rc) return rc;
   rc = check_cuda(h, cudaMemcpyAsync(out, h->fb.out_rgb + (size_t)row_start * w * 3, need, cudaMemcpyDeviceToHost, h->stream),
+                  "readback");
+  if (rc) return rc;
+  return check_cuda(h, cudaStreamSynchronize(h->stream), "readback");
+}
+
+int ap_render_rgba8(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32_t row_end, int accumulate,
+                    uint8_t* out, size_t out_bytes, ap_frame_stats* stats) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  if (row_start >= row_end || row_end > hgt) return fail(h, AP_E_INVALID, "bad row range");
+  size_t need = (size_t)(row_end - row_start) * w * 4;
+  if (!out || out_bytes < need) return fail(h, AP_E_INVALID, "output buffer too small");
+  cudaSetDevice(h->device);
+  int rc = render_common(h, w, hgt, stats);
+  if (rc) return rc;
+  // lib.rs:349-352: a moved camera or accumulation off restarts the average
+  if (!accumulate || std::memcmp(h->mats.view_proj, h->mats.prev_view_proj, sizeof(h->mats.view_proj)) != 0) {
+    cudaMemsetAsync(h->fb.accum, 0, (size_t)w * hgt * sizeof(float4), h->stream);
+    h->accum_count = 0;
+  }
+  encode_resolve_rgba8(h->fb, w, hgt, h->cfg.sample_count, h->accum_count, h->stream);
+  h->accum_count += 1;  // SizedResources::end_frame (lib.rs:209-216)
+  rc = check_cuda(h, cudaGetLastError(), "resolve");
+  if (rc) return rc;
+  rc = check_cuda(h, cudaMemcpyAsync(out, h->fb.rgba + (size_t)row_start * w, need, cudaMemcpyDeviceToHost, h->stream),
                   "readback");
   if (rc) return rc;
   return check_cuda(h, cudaStreamSynchronize(h->stream), "readback");

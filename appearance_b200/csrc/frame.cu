@@ -1771,6 +1771,42 @@ __global__ void k_resolve(FrameBuffers fb, uint32_t P, float inv_count_den) {
   fb.out_rgb[3 * id + 2] = r.z;
 }
 
+// resolve.wgsl:29-38 (hdr_to_sdr, the ACES fit)
+APD float3 hdr_to_sdr(float3 hdr) {
+  const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+  float3 sdr = (hdr * (a * hdr + f3s(b))) / (hdr * (c * hdr + f3s(d)) + f3s(e));
+  return f3(dm::fmin(dm::fmax(sdr.x, 0.0f), 1.0f), dm::fmin(dm::fmax(sdr.y, 0.0f), 1.0f),
+            dm::fmin(dm::fmax(sdr.z, 0.0f), 1.0f));
+}
+
+// block.wgsl:3-16: texture position of pixel (x, y) in 64x64 blocks.
+APD uint2 linear_to_block_pixel(uint32_t x, uint32_t y, uint32_t width) {
+  const uint32_t B = 64;
+  uint32_t blocks_per_row = (width + B - 1) / B;
+  uint32_t block_index = (y / B) * blocks_per_row + x / B;
+  uint32_t pixel_index = block_index * (B * B) + (y % B) * B + x % B;
+  return make_uint2(pixel_index % width, pixel_index / width);
+}
+
+APD uint32_t unorm8(float v) { return __float2uint_rn(v * 255.0f); }  // v in [0, 1]
+
+// resolve.wgsl:40-59
+__global__ void k_resolve_rgba8(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t spp, uint32_t accum_count) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= W || y >= H) return;
+  uint32_t i = y * W + x;
+  float3 r = unpack_rgb9e5(fb.radiance[i]);
+  r = r / (float)spp;
+  r = hdr_to_sdr(r);
+  float4 acc = fb.accum[i];
+  float3 a = f3(acc.x, acc.y, acc.z) + r;
+  fb.accum[i] = make_float4(a.x, a.y, a.z, 0.0f);
+  uint2 p = linear_to_block_pixel(x, y, W);
+  if (p.x >= W || p.y >= H) return;  // outside the texture: the store is dropped
+  float3 o = a / (float)(accum_count + 1);
+  fb.rgba[p.y * W + p.x] = unorm8(o.x) | (unorm8(o.y) << 8) | (unorm8(o.z) << 16) | (255u << 24);
+}
+
 // Batch traversal for the ray-query entry points (persistent, per-lane refill).
 template <bool kAny>
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_batch(DevScene s, const float4* origins, const float4* dirs,
@@ -1829,6 +1865,8 @@ size_t frame_buffer_bytes(uint32_t W, uint32_t H) {
   add(64 * 4);                              // counters
   add(3 * K_NUM_KINDS * 8);                 // visit counters
   add(P * 12);                              // out rgb
+  add(P * 16);                              // display accumulation
+  add(P * 4);                               // RGBA8 texture
   (void)p;
   return n;
 }
@@ -1888,6 +1926,8 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
   fb->counters = carve<uint32_t>(p, 64);
   fb->visits = carve<unsigned long long>(p, 3 * K_NUM_KINDS);
   fb->out_rgb = carve<float>(p, 3 * P);
+  fb->accum = carve<float4>(p, P);
+  fb->rgba = carve<uint32_t>(p, P);
 }
 
 const char* kernel_kind_name(int k) {
@@ -2131,6 +2171,12 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
   k_resolve<<<lb, 256, 0, st>>>(fb, P, (float)cfg.sample_count);
   mark(K_RESOLVE);
   return launches;
+}
+
+void encode_resolve_rgba8(const FrameBuffers& fb, uint32_t W, uint32_t H, uint32_t spp, uint32_t accum_count,
+                          cudaStream_t st) {
+  dim3 b2(16, 16), g2((W + 15) / 16, (H + 15) / 16);
+  k_resolve_rgba8<<<g2, b2, 0, st>>>(fb, W, H, spp, accum_count);
 }
 
 void launch_trace_batch(const DevScene& scene, const float4* origins, const float4* dirs, uint32_t n, int any_hit,

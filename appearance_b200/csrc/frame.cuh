@@ -57,6 +57,8 @@ struct FrameBuffers {
                        // [4..8] ray queue sizes, [9..13] ray queue cursors
   unsigned long long* visits;  // instrumented traversal: per kernel kind {rays, nodes, tris}
   float* out_rgb;      // linear HDR output, 3 floats per pixel (device)
+  float4* accum;       // display accumulation (resolve.wgsl accum_radiance)
+  uint32_t* rgba;      // RGBA8 display texture, 64x64-block swizzled
 };
 
 enum RayQueue { Q_BSDF_CAND = 0, Q_RIS_SHADOW = 1, Q_GI_CAND = 2, Q_GI_SHADOW = 3, Q_DI_SHADOW = 4 };
@@ -103,6 +105,12 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
 
 // Closest / any hit for a batch of rays (parity tests and traversal bench).
 // rays: origin.xyz + tmax (float4), dirs: float4; out: t, u, v, tri bits.
+// The display resolve (resolve.wgsl:40-59): ACES-fit tonemap of radiance /
+// spp, accumulated over `accum_count` earlier frames, stored as RGBA8 at the
+// 64x64-block-swizzled position (block.wgsl:3-16).
+void encode_resolve_rgba8(const FrameBuffers& fb, uint32_t W, uint32_t H, uint32_t spp, uint32_t accum_count,
+                          cudaStream_t st);
+
 void launch_trace_batch(const DevScene& scene, const float4* origins, const float4* dirs, uint32_t n,
                         int any_hit, uint4* out, uint32_t* cursor, int num_sms, cudaStream_t stream);
 

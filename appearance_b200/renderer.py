@@ -136,6 +136,19 @@ class PathTracer:
             result_callback(out.tobytes())
         return out
 
+    def render_rgba8(self, resolution, start_row: int = 0, end_row: int | None = None, accumulate: bool = False,
+                     result_callback=None) -> np.ndarray:
+        """The reference's byte output: ACES-tonemapped RGBA8 at 64x64-block-swizzled
+        positions (rows [start_row, end_row) of the texture)."""
+        w, h = int(resolution[0]), int(resolution[1])
+        end_row = h if end_row is None else end_row
+        out = np.zeros((end_row - start_row, w, 4), np.uint8)
+        self._check(self._lib.ap_render_rgba8(self._h, w, h, start_row, end_row, 1 if accumulate else 0, _ptr(out),
+                                              out.nbytes, ctypes.byref(self.last_stats)))
+        if result_callback is not None:
+            result_callback(out.tobytes())
+        return out
+
     def render_device(self, width: int, height: int) -> float:
         """Renders into the device framebuffer only; returns the frame's GPU ms."""
         self._check(self._lib.ap_render_device(self._h, width, height, ctypes.byref(self.last_stats)))

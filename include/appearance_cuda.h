@@ -149,6 +149,17 @@ int ap_set_camera_matrices(void* handle, const float* mats16x4);
 int ap_render_hdr(void* handle, uint32_t w, uint32_t h, uint32_t row_start, uint32_t row_end, float* out_rgb,
                   size_t out_bytes, ap_frame_stats* stats);
 
+/* The byte output of NodeRenderer::render / PathTracerGpu::render
+ * (lib.rs:556-609): the same frame, then the display resolve (resolve.wgsl:
+ * 29-59): radiance / sample count through the ACES fit, averaged over the
+ * frames rendered by this call since the camera last moved when `accumulate`
+ * != 0 (PathTracerGpuConfig::accum_frames, lib.rs:223,349-352), stored as RGBA8
+ * at the 64x64-block-swizzled position of block.wgsl:3-16 (the texture the
+ * reference reads back).  Rows [row_start, row_end) of the w x h texture
+ * (4 bytes per pixel, row-major) go to `out_rgba`. */
+int ap_render_rgba8(void* handle, uint32_t w, uint32_t h, uint32_t row_start, uint32_t row_end, int accumulate,
+                    uint8_t* out_rgba, size_t out_bytes, ap_frame_stats* stats);
+
 /* Renders one frame into the device-resident framebuffer only (no copy to
  * the host); ap_device_framebuffer() returns its device address. */
 int ap_render_device(void* handle, uint32_t w, uint32_t h, ap_frame_stats* stats);

@@ -70,6 +70,7 @@ def lib():
         L.orc_hash_combine.argtypes = [U, U]
         L.orc_disney.argtypes = [P] * 7
         L.orc_detmath.argtypes = [U, P, P, P, U]
+        L.orc_resolve_rgba8.argtypes = [P, U, U, U, P, U, P]
         _lib = L
     return _lib
 
@@ -145,6 +146,29 @@ class OracleFrame:
         if getattr(self, "ptr", None):
             lib().orc_frame_free(self.ptr)
             self.ptr = None
+
+
+class OracleDisplay:
+    """Display resolve state (resolve.wgsl accum_radiance / accum_frame_count):
+    `resolve` takes a frame's RGB9E5 radiance words and its camera matrices and
+    returns the h x w x 4 RGBA8 texture, accumulating while the camera is still
+    (view_proj == prev_view_proj) and `accumulate` is set (lib.rs:349-352)."""
+
+    def __init__(self, width: int, height: int):
+        self.w, self.h = width, height
+        self.accum = np.zeros((height * width, 4), np.float32)
+        self.count = 0
+
+    def resolve(self, radiance_words: np.ndarray, mats: np.ndarray, spp: int, accumulate: bool) -> np.ndarray:
+        m = np.asarray(mats, np.float32).reshape(4, 16)
+        if not accumulate or not np.array_equal(m[2].view(np.uint32), m[3].view(np.uint32)):
+            self.accum[:] = 0.0
+            self.count = 0
+        out = np.zeros((self.h, self.w, 4), np.uint8)
+        lib().orc_resolve_rgba8(_p(np.ascontiguousarray(radiance_words, np.uint32)), self.w, self.h, spp,
+                                _p(self.accum), self.count, _p(out))
+        self.count += 1
+        return out
 
 
 DETMATH = dict(sin=0, cos=1, exp=2, log=3, pow=4, atan2=5, acos=6)

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <thread>
 #include <vector>
@@ -1215,6 +1216,37 @@ void orc_frame_buffer(void* fp, uint32_t which, uint32_t* out) {
     case 7: for (size_t i = 0; i < P; ++i) memcpy(out + 4 * i, &f->rays[i], 16); break;
     default: break;
   }
+}
+
+// Display resolve (resolve.wgsl:29-59 with block.wgsl:3-16): radiance / spp
+// through the ACES fit (hdr_to_sdr, resolve.wgsl:29-38), added to the
+// accumulation, written as RGBA8 (round to nearest) at the 64x64-block-
+// swizzled texture position; positions outside the texture are dropped.
+void orc_resolve_rgba8(const uint32_t* radiance, uint32_t w, uint32_t h, uint32_t spp, float* accum4,
+                       uint32_t accum_count, uint8_t* texture) {
+  const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+  const uint32_t B = 64, blocks_per_row = (w + B - 1) / B;
+  for (uint32_t y = 0; y < h; ++y)
+    for (uint32_t x = 0; x < w; ++x) {
+      uint32_t i = y * w + x;
+      V3 r = rgb9e5_unpack(radiance[i]);
+      float hdr[3] = {r.x / (float)spp, r.y / (float)spp, r.z / (float)spp};
+      float acc[3];
+      for (int k = 0; k < 3; ++k) {
+        float sdr = (hdr[k] * (a * hdr[k] + b)) / (hdr[k] * (c * hdr[k] + d) + e);
+        sdr = dm::fmin(dm::fmax(sdr, 0.0f), 1.0f);
+        acc[k] = accum4[4 * i + k] + sdr;
+        accum4[4 * i + k] = acc[k];
+      }
+      accum4[4 * i + 3] = 0.0f;
+      uint32_t block_index = (y / B) * blocks_per_row + x / B;
+      uint32_t pixel_index = block_index * (B * B) + (y % B) * B + x % B;
+      uint32_t px = pixel_index % w, py = pixel_index / w;
+      if (px >= w || py >= h) continue;
+      uint8_t* o = texture + 4 * ((size_t)py * w + px);
+      for (int k = 0; k < 3; ++k) o[k] = (uint8_t)std::nearbyint(acc[k] / (float)(accum_count + 1) * 255.0f);
+      o[3] = 255;
+    }
 }
 
 // Packing / RNG / Disney entry points for the golden-vector tests.

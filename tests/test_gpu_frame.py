@@ -115,3 +115,32 @@ def test_row_range_is_a_crop():
     b.upload_scene(sc)
     b.set_camera_matrices(mats)
     assert_bits(b.render((48, 40), 7, 29), full[7:29], "row range")
+
+
+@pytest.mark.parametrize("accumulate", [False, True])
+def test_rgba8_display_output_matches_oracle(accumulate):
+    """ap_render_rgba8 (the reference's byte output): ACES fit, accumulation
+    while the camera is still, 64x64-block-swizzled RGBA8, bit-exact."""
+    from oracle.oracle import OracleDisplay
+    sc = scenes.cornell_box()
+    cfg = dict(presets.PRESETS["faithful"])
+    w, h = 128, 96  # one full and one partial block row: swizzled positions past the texture are dropped
+    cam = scenes.cornell_camera()
+    eye, tgt = np.array(cam["eye"]), np.array(cam["target"])
+    args = (cam["fov"], cam["near"], cam["far"], w, h)
+    m0, vp0 = scenes.camera_matrices(eye, tgt, *args, None)  # prev == current: a still camera
+    moved, vp1 = scenes.camera_matrices(eye + np.array([0.01, 0.0, 0.0]), tgt, *args, vp0)
+    still, _ = scenes.camera_matrices(eye + np.array([0.01, 0.0, 0.0]), tgt, *args, vp1)
+    pt = PathTracer(cfg)
+    pt.upload_scene(sc)
+    of = OracleFrame(OracleScene(sc), w, h, cfg)
+    disp = OracleDisplay(w, h)
+    for m in (m0, m0, m0, moved, still, still):
+        m = np.array(m, np.float32)
+        pt.set_camera_matrices(m)
+        img = pt.render_rgba8((w, h), accumulate=accumulate)
+        of.render(m)
+        ref = disp.resolve(of.buffer(0, 1)[:, 0], m, cfg["sample_count"], accumulate)
+        assert np.array_equal(img, ref)
+    part = pt.render_rgba8((w, h), start_row=32, end_row=80, accumulate=accumulate)
+    assert part.shape == (48, w, 4)
