@@ -277,10 +277,48 @@ def main():
         line["gpu_launches"] = int(details["gpu_launches_per_step"]) * args.steps
         if world == 1 and args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(scene, path, cfg)
+        line["configs"] = {"cornell_512_16spp_depth5": cornell_config(world == 1 and bool(args.cpu_baseline))}
         print(json.dumps(line), flush=True)
     pt.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def cornell_config(cpu: bool) -> dict:
+    """The plain CPU-comparable configuration: the seeded Cornell box at
+    512x512, 16 spp, depth 5, RIS next-event estimation without reuse or
+    denoising.  Device time of 5 frames after 2 warm-up frames; the CPU oracle
+    of the same estimator on a 256x256 render (same scene, spp and depth,
+    all host threads) beside it."""
+    from appearance_b200 import PathTracer, presets, scenes
+    cfg = dict(presets.PLAIN)
+    w = h = 512
+    sc = scenes.cornell_box()
+    cam = scenes.cornell_camera()
+    mats, _ = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], cam["near"], cam["far"], w, h, None)
+    pt = PathTracer(cfg)
+    pt.upload_scene(sc)
+    pt.set_camera_matrices(mats)
+    for _ in range(2):
+        pt.render_device(w, h)
+    ms = [pt.render_device(w, h) for _ in range(5)]
+    pt.close()
+    samples = w * h * cfg["sample_count"]
+    out = {"workload": "cornell box 512x512, 16 spp, depth 5, plain estimator", "triangles": int(sc.num_tris),
+           "frame_ms": statistics.median(ms), "value": samples / (statistics.median(ms) * 1e-3) / 1e6,
+           "unit": "Msamples/s"}
+    if cpu:
+        from oracle.oracle import OracleFrame, OracleScene
+        cw = ch = 256
+        cm, _ = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], cam["near"], cam["far"], cw, ch, None)
+        fr = OracleFrame(OracleScene(sc), cw, ch, cfg, threads=os.cpu_count())
+        t0 = time.perf_counter()
+        fr.render(cm)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": cw * ch * cfg["sample_count"] / dt / 1e6, "unit": "Msamples/s",
+                               "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"oracle, same scene and estimator at {cw}x{ch}, 16 spp, depth 5, 1 frame"}
+    return out
 
 
 def measure_details(pt, scene, path, cfg) -> dict:
