@@ -35,6 +35,7 @@ struct DeviceScene {
   void* emissive_cdf = nullptr;
   void* emissive_tris = nullptr;
   void* emissive_tri_base = nullptr;
+  void* emissive_info = nullptr;
   void* env = nullptr;
   DevScene view{};
   BvhStats stats{};
@@ -43,7 +44,7 @@ struct DeviceScene {
   void release() {
     void** all[] = {&nodes, &tris, &positions, &normals, &indices, &tri_material, &tri_instance,
                     &instances, &materials, &emissive_instances, &emissive_cdf, &emissive_tris,
-                    &emissive_tri_base, &env};
+                    &emissive_tri_base, &emissive_info, &env};
     for (void** p : all) {
       if (*p) cudaFree(*p);
       *p = nullptr;
@@ -479,6 +480,12 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
     acc = acc + pdf;
     cdf.push_back(acc);
   }
+  std::vector<uint4> info(emissive.size());
+  for (size_t e = 0; e < emissive.size(); ++e) {
+    uint32_t cb;
+    std::memcpy(&cb, &cdf[e], 4);
+    info[e] = make_uint4(cb, tri_base[e], inst[emissive[e]].num_indices / 3, 0u);
+  }
   WideBvh bvh;
   std::string berr;
   if (!build_wide_bvh(tv.data(), d->num_tris, (uint32_t)kTraversalStack, &bvh, &berr))
@@ -502,6 +509,7 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
       (rc = upload(h, &s.emissive_instances, emissive.data(), emissive.size())) ||
       (rc = upload(h, &s.emissive_cdf, cdf.data(), cdf.size())) ||
       (rc = upload(h, &s.emissive_tri_base, tri_base.data(), tri_base.size())) ||
+      (rc = upload(h, &s.emissive_info, info.data(), info.size())) ||
       (rc = check_cuda(h, cudaMalloc(&s.emissive_tris, std::max<size_t>(sizeof(EmissiveTri) * num_emissive_tris, 16)),
                        "emissive triangles"))) {
     if (nrm_f) cudaFree(nrm_f);
@@ -543,6 +551,7 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
   std::memcpy(&v.sun, d->sun, sizeof(SunDev));
   v.num_tris = d->num_tris;
   v.emissive_tri_base = static_cast<const uint32_t*>(s.emissive_tri_base);
+  v.emissive_info = static_cast<const uint4*>(s.emissive_info);
   v.emissive_tris = static_cast<const EmissiveTri*>(s.emissive_tris);
   if (num_emissive_tris) {
     k_build_emissive_tris<<<(num_emissive_tris + 255) / 256, 256, 0, h->stream>>>(

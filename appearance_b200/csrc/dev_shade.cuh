@@ -561,15 +561,18 @@ APD void tri_positions(const DevScene& s, const InstanceDev& in, uint32_t tri, f
   *p2 = f3(c.x, c.y, c.z);
 }
 
-APD LightEval load_eval(const DevScene& s, const LightSample& l, float3 hit) {
+// `lights` is the scene's emissive_info table, or a copy of it in shared
+// memory (the candidate-heavy kernels stage it once per block).
+APD LightEval load_eval(const DevScene& s, const LightSample& l, float3 hit, const uint4* lights) {
   if (ls_is_sun(l)) {
     float3 dir = direction_to_sun(s.sun, l.uv);
     return LightEval{sun_intensity(s.sun, dir) * ld3(s.sun.color), dir * 1e6f};
   }
   if (l.inst >= s.num_emissive_instances) return LightEval{f3s(0.0f), f3s(0.0f)};
-  const uint32_t ntri = s.instances[s.emissive_instances[l.inst]].num_indices / 3;
+  const uint4 li = lights[l.inst];
+  const uint32_t ntri = li.z;
   const uint32_t tri = l.tri < ntri ? l.tri : ntri - 1;
-  const EmissiveTri* et = s.emissive_tris + s.emissive_tri_base[l.inst] + tri;
+  const EmissiveTri* et = s.emissive_tris + li.y + tri;
   const float4* q = reinterpret_cast<const float4*>(et);
   float4 a = __ldg(q + 0), b = __ldg(q + 1), c = __ldg(q + 2), nn = __ldg(q + 3), em = __ldg(q + 4);
   float3 p0 = f3(a.x, a.y, a.z), p1 = f3(b.x, b.y, b.z), p2 = f3(c.x, c.y, c.z);
@@ -581,32 +584,37 @@ APD LightEval load_eval(const DevScene& s, const LightSample& l, float3 hit) {
   float sa = dm::fmin(kTwoPi, cos_out / (sqr(dd) + 0.0001f));
   return LightEval{f3(em.x, em.y, em.z) * sa * 10.0f, point};
 }
+APD LightEval load_eval(const DevScene& s, const LightSample& l, float3 hit) {
+  return load_eval(s, l, hit, s.emissive_info);
+}
 
 // First emissive instance whose CDF entry is >= r (the reference scans
 // linearly, nee.wgsl:60-61; the CDF is non-decreasing, so the binary search
 // returns the same index), or num_emissive_instances when there is none.
-APD uint32_t cdf_search(const DevScene& s, float r) {
-  uint32_t lo = 0, hi = s.num_emissive_instances;
+APD uint32_t cdf_search(const uint4* lights, uint32_t n, float r) {
+  uint32_t lo = 0, hi = n;
   while (lo < hi) {
     uint32_t mid = (lo + hi) >> 1;
-    if (r <= __ldg(s.emissive_cdf + mid)) hi = mid;
+    if (r <= __uint_as_float(lights[mid].x)) hi = mid;
     else lo = mid + 1;
   }
   return lo;
 }
 
-APD LightSample sample_uniform(const DevScene& s, float r0, float r1, float r2, float2 r34, float* pdf) {
+APD LightSample sample_uniform(const DevScene& s, float r0, float r1, float r2, float2 r34, float* pdf,
+                               const uint4* lights) {
   float sun_p = s.num_emissive_tris > 0 ? 0.5f : 1.0f;
   if (r0 < sun_p) {
     *pdf = sun_p;
     return LightSample{r34, kU32Max - 1, 0};
   }
-  uint32_t i = cdf_search(s, r1);
+  uint32_t i = cdf_search(lights, s.num_emissive_instances, r1);
   if (i < s.num_emissive_instances) {
-    uint32_t ntri = s.instances[s.emissive_instances[i]].num_indices / 3;
+    const uint4 li = lights[i];
+    uint32_t ntri = li.z;
     uint32_t local = dm::f2u(r2 * (float)ntri);
     if (local >= ntri) local = ntri - 1;
-    float area = __ldg(&s.emissive_tris[s.emissive_tri_base[i] + local].area);
+    float area = __ldg(&s.emissive_tris[li.y + local].area);
     float p = 1.0f / (float)s.num_emissive_tris;
     p = p / area;
     *pdf = dm::fmax(1e-6f, p * (1.0f - sun_p));
@@ -614,6 +622,9 @@ APD LightSample sample_uniform(const DevScene& s, float r0, float r1, float r2, 
   }
   *pdf = 0.0f;
   return ls_empty();
+}
+APD LightSample sample_uniform(const DevScene& s, float r0, float r1, float r2, float2 r34, float* pdf) {
+  return sample_uniform(s, r0, r1, r2, r34, pdf, s.emissive_info);
 }
 
 // ---- reservoirs (di_reservoir.wgsl:6-56, gi_reservoir.wgsl:6-74) ----

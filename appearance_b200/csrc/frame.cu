@@ -349,11 +349,23 @@ APD uint32_t bounce_path(const FrameBuffers& fb, const Consts& c, uint32_t i) {
 }
 
 // Area light candidate (nee.wgsl:136-155).
+// Shared-memory copy of the light table (emissive_info) for the kernels that
+// sample many light candidates per path; scenes with more emissive instances
+// than fit read the table from global memory.
+constexpr uint32_t kSmemLights = 512;
+// All threads of the block must call this (it synchronises the block when it stages).
+APD const uint4* stage_lights(const DevScene& s, uint4* sm) {
+  if (s.num_emissive_instances > kSmemLights) return s.emissive_info;
+  for (uint32_t i = threadIdx.x; i < s.num_emissive_instances; i += blockDim.x) sm[i] = s.emissive_info[i];
+  __syncthreads();
+  return sm;
+}
+
 APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& fr, const Bsdf& b, uint32_t& rng,
-                        LightSample* ls, float* pdf, LightEval* ev, float* phat) {
+                        LightSample* ls, float* pdf, LightEval* ev, float* phat, const uint4* lights) {
   float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng), r3 = rnd(rng), r4 = rnd(rng);
-  *ls = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), pdf);
-  *ev = load_eval(s, *ls, hit);
+  *ls = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), pdf, lights);
+  *ev = load_eval(s, *ls, hit, lights);
   *phat = 0.0f;
   float3 wi = normalize(ev->point - hit);
   float wdn = dot(wi, fr.n);
@@ -365,6 +377,8 @@ APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& f
 }
 
 __global__ void __launch_bounds__(kBlock) k_shade_a(DevScene s, FrameBuffers fb, Consts c, Mats mats) {
+  __shared__ uint4 s_lights[kSmemLights];
+  const uint4* lights = stage_lights(s, s_lights);
   const uint32_t count = bounce_count(fb, c);
   const uint32_t cur = c.frame_idx & 1u;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -409,7 +423,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_a(DevScene s, FrameBuffers fb,
       LightSample area_s{make_float2(0.0f, 0.0f), 0u, 0u};
       if (c.cfg.di_area_samples > 0) {
         LightEval ev;
-        area_candidate(s, sf.hit_point, wo, sf.frame, b, rng, &area_s, &area_pdf, &ev, &area_phat);
+        area_candidate(s, sf.hit_point, wo, sf.frame, b, rng, &area_s, &area_pdf, &ev, &area_phat, lights);
       }
       float3 contribution = f3s(0.0f);
       if (c.cfg.di_bsdf_samples > 0) {
@@ -449,6 +463,8 @@ __global__ void __launch_bounds__(kBlock) k_shade_a(DevScene s, FrameBuffers fb,
 // Stage B1: resampled importance sampling of the direct light (Nee::sample_ris,
 // nee.wgsl:122-237) and its shadow ray.
 __global__ void __launch_bounds__(kBlock, 4) k_shade_b(DevScene s, FrameBuffers fb, Consts c) {
+  __shared__ uint4 s_lights[kSmemLights];
+  const uint4* lights = stage_lights(s, s_lights);
   const uint32_t count = bounce_count(fb, c);
   const uint32_t NA = c.cfg.di_area_samples, NB = c.cfg.di_bsdf_samples;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -475,7 +491,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_shade_b(DevScene s, FrameBuffers 
       uint4 sb = fb.st_b[id];
       LightSample area_s{make_float2(__uint_as_float(sb.x), __uint_as_float(sb.y)), sb.z, sb.w};
       LightEval area_e{f3s(0.0f), f3s(0.0f)};
-      if (NA > 0) area_e = load_eval(s, area_s, hit);
+      if (NA > 0) area_e = load_eval(s, area_s, hit, lights);
       uint4 sc = fb.st_c[id];
       float3 contribution = f3(__uint_as_float(sc.x), __uint_as_float(sc.y), __uint_as_float(sc.z));
       uint4 sd4 = fb.st_d[id];
@@ -494,7 +510,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_shade_b(DevScene s, FrameBuffers 
           bsdf_s = LightSample{inverse_direction_to_sun(s.sun, bwi), kU32Max - 1, 0u};
         }
         if (!ls_is_empty(bsdf_s)) {
-          bsdf_e = load_eval(s, bsdf_s, hit);
+          bsdf_e = load_eval(s, bsdf_s, hit, lights);
           bsdf_phat = luma(contribution * bsdf_e.emission);
         }
       }
@@ -508,7 +524,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_shade_b(DevScene s, FrameBuffers 
         if (k == 0) {
           apdf = area_pdf; aphat = area_phat; as = area_s; ae = area_e; bpdf = bsdf_pdf;
         } else if (k < NA) {
-          area_candidate(s, hit, wo, sf.frame, b, rng, &as, &apdf, &ae, &aphat);
+          area_candidate(s, hit, wo, sf.frame, b, rng, &as, &apdf, &ae, &aphat, lights);
         }
         if (k < NA) {
           float aw = 0.0f;

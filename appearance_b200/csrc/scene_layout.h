@@ -87,6 +87,9 @@ struct DevScene {
   const float* emissive_cdf;
   const EmissiveTri* emissive_tris;     // all triangles of the emissive instances
   const uint32_t* emissive_tri_base;    // emissive instance -> first record
+  // per emissive instance: {CDF entry (float bits), first emissive-triangle
+  // record, triangle count, 0}: what light sampling needs in one 16-byte load
+  const uint4* emissive_info;
   uint32_t num_emissive_instances;
   uint32_t num_emissive_tris;
   const float* env;  // equirect RGB, env_w x env_h, or null

@@ -12,6 +12,12 @@ Algorithmic bytes (what `achieved` is computed from):
 from __future__ import annotations
 
 TRAVERSAL = ("extend", "trace_closest", "trace_any")
+
+# DRAM bytes (read + write) per ray of the queue traversal kernels, from one
+# ncu capture of every traversal launch of a 960x540 benchmark frame divided by
+# that frame's ray count (`python -m appearance_b200.profile --visits`); used
+# as the measured `traffic` of a full frame, scaled by its ray count.
+NCU_DRAM_BYTES_PER_RAY = {"trace_any": 136.4, "trace_closest": 152.7}
 PER_PIXEL_BYTES = {"atrous": 40.0, "svgf_temporal": 88.0, "taa": 52.0}
 
 
@@ -64,8 +70,13 @@ def frame_roofline(pt, scene, path, cfg, width: int, height: int, peak) -> dict:
     }
     if best:
         r = roofs[best]
+        traffic = None
+        if best in NCU_DRAM_BYTES_PER_RAY and "rays" in r:
+            traffic = NCU_DRAM_BYTES_PER_RAY[best] * r["rays"]
         res["roofline"] = {"kernel": best, "bound": "hbm", "achieved": round(r["achieved_gbs"], 2),
-                           "peak": peak_gbs, "unit": "GB/s", "frac": round(r["frac"], 4), "traffic": None,
+                           "peak": peak_gbs, "unit": "GB/s", "frac": round(r["frac"], 4), "traffic": traffic,
+                           "traffic_note": "DRAM bytes per frame of this kernel kind: ncu bytes/ray of a 960x540 "
+                                           "frame x this frame's rays" if traffic else None,
                            "peak_source": peak_kind,
                            "algorithmic_bytes_per_frame": r["bytes"]}
         if "bytes_per_ray" in r:
@@ -89,6 +100,8 @@ def _frames_cli(argv=None):
     ap.add_argument("--frames", type=int, default=3)
     ap.add_argument("--preset", default="realtime", choices=sorted(presets.PRESETS))
     ap.add_argument("--kernels", action="store_true", help="also print per-kernel times of one more frame")
+    ap.add_argument("--visits", action="store_true",
+                    help="also print rays, BVH nodes and triangles per traversal kind of one more (instrumented) frame")
     a = ap.parse_args(argv)
     scene = scenes.icosphere_field(seed=0)
     path = scenes.camera_spline(seed=0, frames=64)
@@ -112,6 +125,17 @@ def _frames_cli(argv=None):
             if v["ms"] > 0:
                 print(f"  {k:16s} {v['ms']:9.3f} ms {v['launches']:4d} launches {100 * v['ms'] / tot:5.1f}%")
         print(f"total {tot:.3f} ms")
+        f += 1
+    if a.visits:
+        eye, tgt = path[(f + 1) % len(path)]
+        mats, prev = scenes.camera_matrices(eye, tgt, 60.0, 0.01, 1000.0, a.width, a.height, prev)
+        pt.set_camera_matrices(mats)
+        prof = pt.profile_frame(a.width, a.height, count_visits=True)
+        for k in TRAVERSAL:
+            v = prof.get(k, {})
+            if v.get("rays"):
+                print(f"  visits {k:14s} rays {v['rays']} nodes {v['nodes']} tris {v['tris']} "
+                      f"bytes/ray {traversal_bytes(v['rays'], v['nodes'], v['tris']) / v['rays']:.1f}")
     pt.close()
 
 
