@@ -17,7 +17,9 @@ EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error"
            "ap_world_action", "ap_scene_upload", "ap_set_camera_matrices", "ap_render_hdr", "ap_render_rgba8", "ap_render_device",
            "ap_device_framebuffer", "ap_trace_rays", "ap_trace_rays_static", "ap_read_buffer", "ap_profile_frame",
            "ap_bvh_stats", "ap_server_create", "ap_server_destroy", "ap_server_last_error", "ap_server_add_scene",
-           "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_stats"]
+           "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_stats",
+           "ap_rc_create", "ap_rc_destroy", "ap_rc_last_error", "ap_rc_set_params", "ap_rc_get_params", "ap_rc_infer",
+           "ap_rc_train"]
 
 U32, F32, P = ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p
 
@@ -101,5 +103,14 @@ def load() -> ctypes.CDLL:
     L.ap_server_query.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]
     L.ap_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(JobResult)]
     L.ap_server_stats.argtypes = [P, P]
+    L.ap_rc_create.restype = P
+    L.ap_rc_create.argtypes = [ctypes.c_int, P, P, U32, ctypes.POINTER(ctypes.c_int)]
+    L.ap_rc_destroy.argtypes = [P]
+    L.ap_rc_last_error.restype = ctypes.c_char_p
+    L.ap_rc_last_error.argtypes = [P]
+    L.ap_rc_set_params.argtypes = [P, P, U32]
+    L.ap_rc_get_params.argtypes = [P, P, U32]
+    L.ap_rc_infer.argtypes = [P, P, U32, P]
+    L.ap_rc_train.argtypes = [P, P, P, U32, F32, ctypes.c_int, P, P]
     _lib = L
     return L

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libappearance_cuda.so")
-SOURCES = ["frame.cu", "api.cu", "noalloc.cu", "serve.cu", "bvh_build.cpp"]
+SOURCES = ["frame.cu", "api.cu", "noalloc.cu", "serve.cu", "mlp.cu", "bvh_build.cpp"]
 HEADERS = ["detmath.h", "dev_common.cuh", "dev_shade.cuh", "traverse.cuh", "frame.cuh", "scene_layout.h",
            "bvh_build.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",

@@ -259,6 +259,32 @@ int ap_server_wait(void* server, uint64_t ticket, ap_job_result* result);
  * bytes, graphs instantiated, graphs updated in place */
 int ap_server_stats(void* server, uint64_t* out8);
 
+/* ---- radiance cache -------------------------------------------------------
+ * No reference counterpart (the reference traces every path to full depth).
+ * A small MLP (144 encoded inputs, 4 hidden layers of 64 with ReLU, 3 outputs
+ * with exp; FP16 weights and activations, FP32 accumulation and master
+ * weights) predicting the outgoing radiance of a path vertex, trained online
+ * with Adam on a relative L2 loss.  A query is 16 floats: position (3),
+ * roughness, outgoing direction (3, unit), 0, diffuse albedo (3), specular
+ * albedo (3), 0, 0.  Positions are normalised to the box [scene_lo, scene_hi].
+ * Parameters: AP_RC_NUM_PARAMS floats, W0 (64 x 144), W1, W2, W3 (64 x 64),
+ * W4 (3 x 64), each row-major [out][in]. */
+#define AP_RC_NUM_PARAMS 21696
+void* ap_rc_create(int device, const float* scene_lo, const float* scene_hi, uint32_t seed, int* err);
+void ap_rc_destroy(void* cache);
+const char* ap_rc_last_error(const void* cache);
+/* Replaces the master weights and restarts Adam. */
+int ap_rc_set_params(void* cache, const float* params, uint32_t count);
+int ap_rc_get_params(void* cache, float* params, uint32_t count);
+/* Predicted RGB radiance of n queries (tensor-core inference); host buffers. */
+int ap_rc_infer(void* cache, const float* queries, uint32_t n, float* out_rgb);
+/* One training step on n (query, target RGB) pairs: loss and gradients, then
+ * an Adam update (lr; beta1 0.9, beta2 0.999, eps 1e-8) when update != 0.
+ * Writes the batch loss to *loss and, when grad_out is not NULL, the
+ * gradient of the loss (AP_RC_NUM_PARAMS floats). */
+int ap_rc_train(void* cache, const float* queries, const float* targets, uint32_t n, float lr, int update,
+                float* loss, float* grad_out);
+
 #ifdef __cplusplus
 }
 #endif
