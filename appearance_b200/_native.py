@@ -19,7 +19,7 @@ EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error"
            "ap_bvh_stats", "ap_server_create", "ap_server_destroy", "ap_server_last_error", "ap_server_add_scene",
            "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_stats",
            "ap_rc_create", "ap_rc_destroy", "ap_rc_last_error", "ap_rc_set_params", "ap_rc_get_params", "ap_rc_infer",
-           "ap_rc_train"]
+           "ap_rc_train", "ap_rc_attach"]
 
 U32, F32, P = ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p
 
@@ -112,5 +112,6 @@ def load() -> ctypes.CDLL:
     L.ap_rc_get_params.argtypes = [P, P, U32]
     L.ap_rc_infer.argtypes = [P, P, U32, P]
     L.ap_rc_train.argtypes = [P, P, P, U32, F32, ctypes.c_int, P, P]
+    L.ap_rc_attach.argtypes = [P, P, U32, U32, U32, F32, ctypes.c_int]
     _lib = L
     return L

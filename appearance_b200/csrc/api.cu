@@ -80,6 +80,10 @@ struct Handle {
   uint64_t ext_rays = 0;
   FrameProfiler prof;
   uint32_t accum_count = 0;  // frames in the display accumulation (resolve.wgsl accum_frame_count)
+  // radiance cache mode (ap_rc_attach)
+  RcFrame rc{};
+  void* rc_mem = nullptr;
+  uint32_t rc_w = 0, rc_h = 0;
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -239,9 +243,20 @@ int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats, Fr
     return fail(h, AP_E_INVALID, "frame config out of range");
   int rc = ensure_frame(h, w, hgt);
   if (rc) return rc;
+  if (h->rc.cache && (h->rc_w != w || h->rc_h != hgt)) {
+    if (h->rc_mem) cudaFree(h->rc_mem);
+    h->rc_mem = nullptr;
+    h->rc_w = h->rc_h = 0;
+    rc = check_cuda(h, cudaMalloc(&h->rc_mem, rc_frame_bytes(w, hgt, h->rc.stride, h->rc.batch)), "radiance cache buffers");
+    if (rc) return rc;
+    rc_frame_carve(h->rc_mem, w, hgt, h->rc.stride, h->rc.batch, &h->rc);
+    h->rc_w = w;
+    h->rc_h = hgt;
+  }
   compute_mats(h, w, hgt);
   cudaEventRecord(h->ev0, h->stream);
-  int launches = encode_frame(h->scene.view, h->fb, h->cfg, h->mats, w, hgt, h->frame_idx, h->num_sms, h->stream, prof);
+  int launches = encode_frame(h->scene.view, h->fb, h->cfg, h->mats, w, hgt, h->frame_idx, h->num_sms, h->stream, prof,
+                              h->rc.cache ? &h->rc : nullptr);
   cudaEventRecord(h->ev1, h->stream);
   uint32_t rays = 0;
   cudaMemcpyAsync(&rays, h->fb.counters + 3, 4, cudaMemcpyDeviceToHost, h->stream);
@@ -348,6 +363,7 @@ void ap_destroy(void* hp) {
   h->scene.release();
   if (h->frame_mem) cudaFree(h->frame_mem);
   if (h->trace_mem) cudaFree(h->trace_mem);
+  if (h->rc_mem) cudaFree(h->rc_mem);
   if (h->prof.created)
     for (int i = 0; i <= FrameProfiler::kMax; ++i) cudaEventDestroy(h->prof.ev[i]);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -592,6 +608,30 @@ int ap_render_hdr(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32
   return check_cuda(h, cudaStreamSynchronize(h->stream), "readback");
 }
 
+int ap_rc_attach(void* hp, void* cache, uint32_t prefix_bounces, uint32_t train_stride, uint32_t train_batch, float lr,
+                 int train) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  if (cache && (prefix_bounces == 0 || prefix_bounces >= kRcMaxBounces || train_stride == 0 || train_batch == 0 ||
+                train_batch > (1u << 22) || !(lr >= 0.0f)))
+    return fail(h, AP_E_INVALID, "radiance cache: parameters out of range");
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  if (h->rc_mem) cudaFree(h->rc_mem);
+  h->rc_mem = nullptr;
+  h->rc_w = h->rc_h = 0;
+  h->rc = RcFrame{};
+  if (cache) {
+    h->rc.cache = cache;
+    h->rc.prefix = prefix_bounces;
+    h->rc.stride = train_stride;
+    h->rc.batch = train_batch;
+    h->rc.lr = lr;
+    h->rc.train = train;
+  }
+  return AP_OK;
+}
+
 int ap_render_rgba8(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32_t row_end, int accumulate,
                     uint8_t* out, size_t out_bytes, ap_frame_stats* stats) {
   Handle* h = static_cast<Handle*>(hp);
@@ -639,6 +679,7 @@ int ap_trace_rays(void* hp, const float* origins_tmax, const float* dirs, uint32
   size_t need = (size_t)n * 48 + 256;
   if (h->trace_bytes < need) {
     if (h->trace_mem) cudaFree(h->trace_mem);
+  if (h->rc_mem) cudaFree(h->rc_mem);
     h->trace_mem = nullptr;
     int rc = check_cuda(h, cudaMalloc(&h->trace_mem, need), "trace scratch");
     if (rc) return rc;

@@ -26,6 +26,7 @@ constexpr int kBlock = 128;
 struct Consts {
   uint32_t W, H, P;
   uint32_t bounce, seed, frame_idx, qin, qout;
+  uint32_t sample;
   FrameConfig cfg;
 };
 
@@ -403,7 +404,10 @@ __global__ void __launch_bounds__(kBlock) k_shade_a(DevScene s, FrameBuffers fb,
     uint32_t flags = 0;
     bool want_ray = false;
     float3 ray_o = f3s(0.0f), wi = f3s(0.0f);
-    if (h.tri != kNoHit) {
+    if (h.tri == kRcRetired) {  // ended in the radiance cache at this vertex
+      t_out = -1.0f;
+      fb.st_a[id] = make_uint4(0u, 0u, 0u, 0u);
+    } else if (h.tri != kNoHit) {
       float depth_ws = 0.0f + h.t;
       const MaterialDev* m;
       Surface sf = surface(s, h, origin, direction, &m);
@@ -1526,6 +1530,107 @@ __global__ void __launch_bounds__(256) k_dsp_b(DevScene s, FrameBuffers fb, Cons
   push_ray(fb, Q_GI_SHADOW, there.ray, there.o, there.tmax, there.d, id);
 }
 
+// ---- radiance cache mode ------------------------------------------------------
+
+// Query of the cache at a path vertex: position, roughness, outgoing direction,
+// diffuse albedo color (1 - metallic)(1 - transmission), specular albedo
+// mix(0.08 specular, color, metallic).
+APD void rc_query(const Surface& sf, const MaterialDev* m, float3 wo, float4* q) {
+  const float3 col = ld3(m->color);
+  const float kd = (1.0f - m->metallic) * (1.0f - m->transmission);
+  const float3 spec = f3s(0.08f * m->specular) * (1.0f - m->metallic) + col * m->metallic;
+  q[0] = make_float4(sf.hit_point.x, sf.hit_point.y, sf.hit_point.z, m->roughness);
+  q[1] = make_float4(wo.x, wo.y, wo.z, 0.0f);
+  q[2] = make_float4(col.x * kd, col.y * kd, col.z * kd, spec.x);
+  q[3] = make_float4(spec.y, spec.z, 0.0f, 0.0f);
+}
+
+APD bool rc_training_pixel(uint32_t id, uint32_t frame_idx, uint32_t stride) {
+  return id % stride == (frame_idx * 7u + 3u) % stride;
+}
+
+// After the extension rays of a bounce: training pixels record each suffix
+// vertex (query, throughput, radiance so far); other pixels retire their path
+// at the prefix-th hit into the cache.
+__global__ void __launch_bounds__(kBlock) k_rc_vertex(DevScene s, FrameBuffers fb, Consts c, RcFrame rc) {
+  const uint32_t count = bounce_count(fb, c);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t id = bounce_path(fb, c, i);
+    const uint4 hr = fb.hits[id];
+    if (hr.w == kNoHit) continue;
+    const bool tp = rc_training_pixel(id, c.frame_idx, rc.stride);
+    if (!tp && c.bounce != rc.prefix) continue;
+    if (tp && (c.bounce == 0 || c.bounce >= kRcMaxBounces)) continue;
+    const float4 ray = fb.rays[id];
+    const float3 origin = ray_org(ray), direction = ray_dir(ray);
+    Hit h{__uint_as_float(hr.x), __uint_as_float(hr.y), __uint_as_float(hr.z), hr.w};
+    const MaterialDev* m;
+    const Surface sf = surface(s, h, origin, direction, &m);
+    float4 q[4];
+    rc_query(sf, m, -direction, q);
+    const float3 T = unpack_rgb9e5(fb.payload[id].x);
+    if (tp) {
+      float4* r = rc.rec + ((size_t)(id / rc.stride) * kRcMaxBounces + c.bounce) * 6;
+      const float3 acc = unpack_rgb9e5(fb.radiance[id]);
+      r[0] = q[0]; r[1] = q[1]; r[2] = q[2]; r[3] = q[3];
+      r[4] = make_float4(T.x, T.y, T.z, 0.0f);
+      r[5] = make_float4(acc.x, acc.y, acc.z, (float)(c.sample + 1));  // tag: the sample that wrote it
+    } else {
+      float4* dst = rc.q + 4 * (size_t)id;
+      dst[0] = q[0]; dst[1] = q[1]; dst[2] = q[2]; dst[3] = q[3];
+      rc.T[id] = make_float4(T.x, T.y, T.z, 1.0f);
+      fb.hits[id].w = kRcRetired;
+    }
+  }
+}
+
+APD float3 rc_target(const float4* r, float3 acc_end) {
+  const float3 T = f3(r[4].x, r[4].y, r[4].z), a = f3(r[5].x, r[5].y, r[5].z);
+  const float3 d = acc_end - a;
+  return f3(T.x > 0.0f ? dm::fmax(d.x, 0.0f) / T.x : 0.0f, T.y > 0.0f ? dm::fmax(d.y, 0.0f) / T.y : 0.0f,
+            T.z > 0.0f ? dm::fmax(d.z, 0.0f) / T.z : 0.0f);
+}
+
+// Pass 1: count the valid records.  Pass 2: keep each with probability
+// batch / count (a hash of the record slot and frame), up to `batch`.
+// Only records of the frame's last sample pair with its final radiance.
+__global__ void k_rc_count(RcFrame rc, uint32_t slots, float last_tag) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  bool v = k < slots && rc.rec[6 * (size_t)k + 5].w == last_tag;
+  unsigned b = __ballot_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(&rc.counts[0], (uint32_t)__popc(b));
+}
+
+__global__ void k_rc_batch(FrameBuffers fb, RcFrame rc, uint32_t slots, uint32_t frame_idx, float last_tag) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= slots) return;
+  const float4* r = rc.rec + 6 * (size_t)k;
+  if (r[5].w != last_tag) return;
+  const uint32_t cand = rc.counts[0];
+  const float keep = cand <= rc.batch ? 1.0f : (float)rc.batch / (float)cand;
+  const float u = (float)(pcg_hash(k ^ xor_shift(frame_idx * 0x9E3779B9u)) >> 8) * (1.0f / 16777216.0f);
+  if (u >= keep) return;
+  const uint32_t slot = atomicAdd(&rc.counts[1], 1u);
+  if (slot >= rc.batch) return;
+  const uint32_t pixel = (k / kRcMaxBounces) * rc.stride + (frame_idx * 7u + 3u) % rc.stride;
+  const float3 t = rc_target(r, unpack_rgb9e5(fb.radiance[pixel]));
+  float4* q = rc.bq + 4 * (size_t)slot;
+  q[0] = r[0]; q[1] = r[1]; q[2] = r[2]; q[3] = r[3];
+  rc.bt[3 * slot + 0] = t.x;
+  rc.bt[3 * slot + 1] = t.y;
+  rc.bt[3 * slot + 2] = t.z;
+}
+
+// Adds throughput x predicted radiance to every retired path's pixel.
+__global__ void k_rc_apply(FrameBuffers fb, RcFrame rc, uint32_t P) {
+  uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= P) return;
+  const float4 T = rc.T[id];
+  if (T.w == 0.0f) return;
+  const float3 L = f3(rc.out[3 * id], rc.out[3 * id + 1], rc.out[3 * id + 2]);
+  fb.radiance[id] = pack_rgb9e5(unpack_rgb9e5(fb.radiance[id]) + f3(T.x, T.y, T.z) * L);
+}
+
 // ---- denoising -------------------------------------------------------------
 
 // demodulate_radiance.wgsl:24-42
@@ -1946,11 +2051,30 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
   fb->rgba = carve<uint32_t>(p, P);
 }
 
+size_t rc_frame_bytes(uint32_t W, uint32_t H, uint32_t stride, uint32_t batch) {
+  const size_t P = (size_t)W * H, slots = ((P + stride - 1) / stride) * kRcMaxBounces;
+  auto a = [](size_t b) { return ((b + 255) / 256) * 256; };
+  return a(P * 64) + a(P * 16) + a(P * 12) + a(slots * 96) + a((size_t)batch * 64) + a((size_t)batch * 12) + a(8);
+}
+
+void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_t batch, RcFrame* rc) {
+  char* p = static_cast<char*>(base);
+  const size_t P = (size_t)W * H, slots = ((P + stride - 1) / stride) * kRcMaxBounces;
+  rc->q = carve<float4>(p, 4 * P);
+  rc->T = carve<float4>(p, P);
+  rc->out = carve<float>(p, 3 * P);
+  rc->rec = carve<float4>(p, 6 * slots);
+  rc->bq = carve<float4>(p, 4 * (size_t)batch);
+  rc->bt = carve<float>(p, 3 * (size_t)batch);
+  rc->counts = carve<uint32_t>(p, 2);
+}
+
 const char* kernel_kind_name(int k) {
   static const char* names[K_NUM_KINDS] = {"memset", "raygen", "extend", "shade", "di_temporal", "di_spatial",
                                            "gi_temporal", "gi_spatial", "apply_di", "apply_gi", "demodulate",
                                            "firefly", "svgf_temporal", "atrous", "taa", "resolve", "copy",
-                                           "trace_closest", "trace_any", "shade_b", "shade_c", "shade_d", "shade_b2"};
+                                           "trace_closest", "trace_any", "shade_b", "shade_c", "shade_d", "shade_b2", "rc",
+                                           "rc_infer", "rc_train"};
   return (k >= 0 && k < K_NUM_KINDS) ? names[k] : "?";
 }
 
@@ -1962,7 +2086,8 @@ void trace_queue(bool counting, int blocks, cudaStream_t st, const DevScene& sce
 }
 
 int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
-                 uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t st, FrameProfiler* prof) {
+                 uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t st, FrameProfiler* prof,
+                 const RcFrame* rc) {
   int launches = 0;
   const bool counting = prof && prof->count_visits;
   if (counting) cudaMemsetAsync(fb.visits, 0, 3 * K_NUM_KINDS * sizeof(unsigned long long), st);
@@ -1988,12 +2113,26 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
   c.H = H;
   c.P = P;
   c.frame_idx = frame_idx;
+  c.sample = 0;
   c.cfg = cfg;
   cudaMemsetAsync(fb.radiance, 0, (size_t)P * 4, st);
   cudaMemsetAsync(fb.counters + 3, 0, 4, st);
   mark(K_MEMSET);
+  const bool cache = rc && rc->cache && cfg.max_bounces > rc->prefix;
+  const uint32_t rc_slots = cache ? ((P + rc->stride - 1) / rc->stride) * kRcMaxBounces : 0;
+  if (cache) {
+    cudaMemsetAsync(rc->T, 0, (size_t)P * sizeof(float4), st);
+    cudaMemsetAsync(rc->rec, 0, (size_t)rc_slots * 6 * sizeof(float4), st);
+    cudaMemsetAsync(rc->counts, 0, 2 * sizeof(uint32_t), st);
+    mark(K_MEMSET);
+  }
   for (uint32_t sample = 0; sample < cfg.sample_count; ++sample) {
     c.seed = frame_idx * cfg.sample_count + sample;
+    c.sample = sample;
+    if (cache) {
+      cudaMemsetAsync(rc->T, 0, (size_t)P * sizeof(float4), st);  // retired-path flags of this sample
+      mark(K_MEMSET);
+    }
     k_raygen<<<g2, b2, 0, st>>>(fb, W, H, mats);
     mark(K_RAYGEN);
     for (uint32_t i = 0; i < cfg.max_bounces; ++i) {
@@ -2005,6 +2144,10 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       if (counting) k_extend<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
       else k_extend<false><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_EXTEND);
+      if (cache) {
+        k_rc_vertex<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c, *rc);
+        mark(K_RC);
+      }
       cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
       mark(K_MEMSET);
       k_shade_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c, mats);
@@ -2134,6 +2277,24 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
         k_apply_gi<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
         mark(K_APPLY_GI);
       }
+    }
+    if (cache) {  // this sample's retired paths: predicted radiance on the tensor cores
+      rc_infer_device(rc->cache, rc->q, P, rc->out, st);
+      mark(K_RC_INFER);
+      k_rc_apply<<<(P + 255) / 256, 256, 0, st>>>(fb, *rc, P);
+      mark(K_RC);
+    }
+  }
+  if (cache && rc->train) {
+    // training targets of the last sample's suffix vertices (the radiance of
+    // the training pixels is final here), one Adam step
+    const float last_tag = (float)cfg.sample_count;
+    k_rc_count<<<(rc_slots + 255) / 256, 256, 0, st>>>(*rc, rc_slots, last_tag);
+    k_rc_batch<<<(rc_slots + 255) / 256, 256, 0, st>>>(fb, *rc, rc_slots, frame_idx, last_tag);
+    mark(K_RC);
+    {
+      rc_train_device(rc->cache, rc->bq, rc->bt, rc->counts + 1, rc->batch, rc->lr, 1, st);
+      mark(K_RC_TRAIN);
     }
   }
   // demodulate -> firefly -> SVGF -> TAA -> remodulate -> resolve (lib.rs:492-576)

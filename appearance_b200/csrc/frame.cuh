@@ -81,7 +81,7 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb);
 enum KernelKind : int {
   K_MEMSET = 0, K_RAYGEN, K_EXTEND, K_SHADE, K_DI_TEMPORAL, K_DI_SPATIAL, K_GI_TEMPORAL, K_GI_SPATIAL,
   K_APPLY_DI, K_APPLY_GI, K_DEMODULATE, K_FIREFLY, K_SVGF_TEMPORAL, K_ATROUS, K_TAA, K_RESOLVE, K_COPY,
-  K_TRACE_CLOSEST, K_TRACE_ANY, K_SHADE_B, K_SHADE_C, K_SHADE_D, K_SHADE_B2, K_NUM_KINDS
+  K_TRACE_CLOSEST, K_TRACE_ANY, K_SHADE_B, K_SHADE_C, K_SHADE_D, K_SHADE_B2, K_RC, K_RC_INFER, K_RC_TRAIN, K_NUM_KINDS
 };
 const char* kernel_kind_name(int k);
 
@@ -99,9 +99,36 @@ struct FrameProfiler {
 
 // Encodes one frame on `stream`.  `frame_idx` selects the ping-pong parity.
 // Returns the number of kernels launched (memsets and copies excluded).
+// Radiance-cache mode of a frame (a cache attached with ap_rc_attach): paths of
+// most pixels end at their `prefix`-th hit with the cache's prediction; the
+// paths of one pixel in `stride` (a different subset each frame) go to full
+// depth and give the training targets of their suffix vertices.
+struct RcFrame {
+  void* cache = nullptr;  // radiance cache (mlp.cu)
+  uint32_t prefix = 2, stride = 16, batch = 65536;
+  float lr = 1e-3f;
+  int train = 1;
+  float4* q = nullptr;       // per pixel: query of the retired path (4 float4)
+  float4* T = nullptr;       // per pixel: throughput at the retired vertex; w = 1 when retired
+  float* out = nullptr;      // per pixel: predicted RGB
+  float4* rec = nullptr;     // per training pixel and bounce: query (4), throughput (1), radiance so far (1; w = valid)
+  float4* bq = nullptr;      // training batch queries (batch x 4)
+  float* bt = nullptr;       // training batch targets (batch x 3)
+  uint32_t* counts = nullptr;  // [0] candidate records, [1] batch entries
+};
+constexpr uint32_t kRcMaxBounces = 8;        // record slots per training pixel
+constexpr uint32_t kRcRetired = 0xFFFFFFFEu;  // hit id of a path retired into the cache
+size_t rc_frame_bytes(uint32_t W, uint32_t H, uint32_t stride, uint32_t batch);
+void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_t batch, RcFrame* rc);
+
+// mlp.cu: inference over n queries, and one training step on a device-assembled batch
+int rc_infer_device(void* cache, const float4* queries, uint32_t n, float* out, cudaStream_t st);
+int rc_train_device(void* cache, const float4* queries, const float* targets, const uint32_t* n_dev, uint32_t cap,
+                    float lr, int update, cudaStream_t st);
+
 int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t stream,
-                 FrameProfiler* prof = nullptr);
+                 FrameProfiler* prof = nullptr, const RcFrame* rc = nullptr);
 
 // Closest / any hit for a batch of rays (parity tests and traversal bench).
 // rays: origin.xyz + tmax (float4), dirs: float4; out: t, u, v, tri bits.

@@ -282,10 +282,12 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__
 // Backward: d4 = dL/dy, d_l = (W_{l+1}^T d_{l+1}) * [h_{l+1} > 0].  Stores
 // h_l and d_l for the weight gradients dW_l = sum_s d_l h_l^T.
 __global__ void __launch_bounds__(128) k_rc_forward_backward(const float* __restrict__ wf, const float4* __restrict__ queries,
-                                                             const float* __restrict__ targets, uint32_t n, RcBounds bounds,
-                                                             float* __restrict__ h, float* __restrict__ d,
-                                                             float* __restrict__ loss_sum) {
+                                                             const float* __restrict__ targets, const uint32_t* __restrict__ n_dev,
+                                                             uint32_t cap, RcBounds bounds, float* __restrict__ h,
+                                                             float* __restrict__ d, float* __restrict__ loss_sum) {
   extern __shared__ float sw[];
+  const uint32_t n = min(*n_dev, cap);
+  if (blockIdx.x * blockDim.x >= n) return;
   for (int i = threadIdx.x; i < kNumParams; i += blockDim.x) sw[i] = wf[i];
   __syncthreads();
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -356,9 +358,12 @@ __global__ void __launch_bounds__(128) k_rc_forward_backward(const float* __rest
 
 // dW_l[o][i] += sum over a chunk of samples of d_l[s][o] * h_l[s][i].
 __global__ void __launch_bounds__(256) k_rc_weight_grad(const float* __restrict__ h, const float* __restrict__ d,
-                                                        uint32_t n, int layer, uint32_t chunk, float* __restrict__ grad) {
+                                                        const uint32_t* __restrict__ n_dev, uint32_t cap, int layer,
+                                                        uint32_t chunk, float* __restrict__ grad) {
   __shared__ float sd[32][kHid];
   __shared__ float sh[32][kIn];
+  const uint32_t n = min(*n_dev, cap);
+  if (blockIdx.x * chunk >= n) return;
   const int K = layer == 0 ? kIn : kHid, O = layer == 4 ? kOut : kHid;
   const int hoff = layer == 0 ? 0 : kIn + (layer - 1) * kHid;
   const int doff = layer == 4 ? 4 * kHid : layer * kHid;
@@ -427,6 +432,7 @@ struct Cache {
   cudaStream_t stream = nullptr;
   RcBounds bounds{};
   float *master = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr, *wf = nullptr, *loss = nullptr;
+  uint32_t* count = nullptr;  // sample count of host-submitted batches
   __half* packed = nullptr;
   uint32_t* err = nullptr;
   int step = 0;
@@ -483,19 +489,21 @@ int rc_infer_device(void* cp, const float4* queries, uint32_t n, float* out, cud
   return cuda_ok(c, cudaGetLastError(), "radiance cache inference");
 }
 
-int rc_train_device(void* cp, const float4* queries, const float* targets, uint32_t n, float lr, int update,
-                    cudaStream_t st) {
+// Training step on at most `cap` samples; the sample count is read from device
+// memory (n_dev), so a batch assembled on the device needs no host round trip.
+int rc_train_device(void* cp, const float4* queries, const float* targets, const uint32_t* n_dev, uint32_t cap, float lr,
+                    int update, cudaStream_t st) {
   Cache* c = static_cast<Cache*>(cp);
-  if (n == 0) return AP_OK;
-  int rc = ensure_batch(c, n);
+  if (cap == 0) return AP_OK;
+  int rc = ensure_batch(c, cap);
   if (rc) return rc;
   cudaMemsetAsync(c->grad, 0, kNumParams * 4, st);
   cudaMemsetAsync(c->loss, 0, 4, st);
-  k_rc_forward_backward<<<(n + 127) / 128, 128, kNumParams * 4, st>>>(c->wf, queries, targets, n, c->bounds, c->h, c->d,
-                                                                     c->loss);
+  k_rc_forward_backward<<<(cap + 127) / 128, 128, kNumParams * 4, st>>>(c->wf, queries, targets, n_dev, cap, c->bounds,
+                                                                       c->h, c->d, c->loss);
   const uint32_t chunk = 1024;
   for (int l = 0; l < 5; ++l)
-    k_rc_weight_grad<<<(n + chunk - 1) / chunk, 256, 0, st>>>(c->h, c->d, n, l, chunk, c->grad);
+    k_rc_weight_grad<<<(cap + chunk - 1) / chunk, 256, 0, st>>>(c->h, c->d, n_dev, cap, l, chunk, c->grad);
   if (update) {
     c->step += 1;
     const float b1 = 0.9f, b2 = 0.999f;
@@ -538,6 +546,7 @@ void* ap_rc_create(int device, const float* scene_lo, const float* scene_hi, uin
       (rc = ap::cuda_ok(c, cudaMalloc(&c->wf, ap::kNumParams * 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->loss, 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->err, 4), "params")) ||
+      (rc = ap::cuda_ok(c, cudaMalloc(&c->count, 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->packed, ap::kPackHalves * 2), "params")) ||
       (rc = ap::cuda_ok(c, cudaFuncSetAttribute(ap::k_rc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 ap::kSmemInfer), "smem")) ||
@@ -570,8 +579,8 @@ void ap_rc_destroy(void* cp) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->wf, c->loss, c->err, c->packed, c->h, c->d, c->targets, c->queries,
-                  c->out};
+  void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->wf, c->loss, c->err, c->count, c->packed, c->h, c->d, c->targets,
+                  c->queries, c->out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -633,7 +642,8 @@ int ap_rc_train(void* cp, const float* queries, const float* targets, uint32_t n
   if (rc) return rc;
   cudaMemcpyAsync(c->queries, queries, (size_t)n * 64, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(c->targets, targets, (size_t)n * 12, cudaMemcpyHostToDevice, c->stream);
-  if ((rc = ap::rc_train_device(c, c->queries, c->targets, n, lr, update, c->stream))) return rc;
+  cudaMemcpyAsync(c->count, &n, 4, cudaMemcpyHostToDevice, c->stream);
+  if ((rc = ap::rc_train_device(c, c->queries, c->targets, c->count, n, lr, update, c->stream))) return rc;
   float l = 0.0f;
   cudaMemcpyAsync(&l, c->loss, 4, cudaMemcpyDeviceToHost, c->stream);
   if (grad_out) cudaMemcpyAsync(grad_out, c->grad, ap::kNumParams * 4, cudaMemcpyDeviceToHost, c->stream);

@@ -136,6 +136,13 @@ class PathTracer:
             result_callback(out.tobytes())
         return out
 
+    def attach_radiance_cache(self, cache, prefix_bounces: int = 2, train_stride: int = 16, train_batch: int = 65536,
+                              lr: float = 1e-3, train: bool = True):
+        """Radiance-cache mode (ap_rc_attach); `cache` None detaches."""
+        self._rc = cache
+        self._check(self._lib.ap_rc_attach(self._h, None if cache is None else cache._c, prefix_bounces, train_stride,
+                                           train_batch, lr, 1 if train else 0))
+
     def render_rgba8(self, resolution, start_row: int = 0, end_row: int | None = None, accumulate: bool = False,
                      result_callback=None) -> np.ndarray:
         """The reference's byte output: ACES-tonemapped RGBA8 at 64x64-block-swizzled

@@ -284,6 +284,16 @@ int ap_rc_infer(void* cache, const float* queries, uint32_t n, float* out_rgb);
  * gradient of the loss (AP_RC_NUM_PARAMS floats). */
 int ap_rc_train(void* cache, const float* queries, const float* targets, uint32_t n, float lr, int update,
                 float* loss, float* grad_out);
+/* Radiance-cache mode of a renderer (cache NULL detaches): in every frame the
+ * paths of most pixels end at their `prefix_bounces`-th hit with T x the
+ * cache's prediction (the frame's max_bounces must exceed prefix_bounces);
+ * one pixel in `train_stride`, a different subset each frame, traces to
+ * max_bounces and its suffix vertices (bounces 1..7) give training targets
+ * (the radiance measured after the vertex divided by the throughput at it),
+ * of which `train_batch` are drawn at random for one Adam step (learning rate
+ * `lr`) per frame when `train` != 0.  The cache must outlive the attachment. */
+int ap_rc_attach(void* handle, void* cache, uint32_t prefix_bounces, uint32_t train_stride, uint32_t train_batch,
+                 float lr, int train);
 
 #ifdef __cplusplus
 }
