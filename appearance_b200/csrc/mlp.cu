@@ -16,9 +16,10 @@
 // thread issues tcgen05.mma (M=128, N=64 or 16, K=16 per instruction) with the
 // FP32 accumulator in tensor memory; every warp reads its 32 rows back with
 // tcgen05.ld, applies ReLU, rounds to FP16 and writes the next layer's
-// operand.  Training (k_rc_forward_backward, k_rc_weight_grad, k_rc_adam) runs
-// on the CUDA cores in FP32 on the same FP16-rounded weights and activations:
-// 2^16 samples per step is a few GFLOP, small beside the frame.
+// operand.  Training (k_rc_encode_batch, k_sgemm, k_rc_loss, k_rc_adam) runs
+// on the CUDA cores in FP32 on the same FP16-rounded weights and activations,
+// layer by layer as tiled GEMMs over the batch: 2^16 samples per step is about
+// 7 GFLOP, small beside the frame.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -66,39 +67,52 @@ struct RcBounds {
 };
 
 // Query record (16 floats): position, roughness, direction (unit, outgoing),
-// 0, diffuse albedo, specular albedo, 0, 0.
-APD void rc_encode(const float* q, const RcBounds& b, float* f) {
+// 0, diffuse albedo, specular albedo, 0, 0.  The 144 features go to
+// sink(k, value).  Octave o of each position axis is sin/cos(2^o pi x), by the
+// double-angle recurrence from o = 0.  Each one-blob bin i holds
+// exp(-0.5 c_i^2), c_i = (v - (i + 0.5)/32) * 32; only the 13 bins around the
+// peak are evaluated (written after zeroing all 32): farther bins are below
+// half the smallest FP16 subnormal, so their FP16 value is 0 either way.
+template <class Sink>
+APD void rc_encode(const float* q, const RcBounds& b, Sink sink) {
   const float kPi = 3.14159265358979323846f;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    float x = (q[a] - b.lo[a]) * b.inv[a];
-    float scale = kPi;
+    const float x = (q[a] - b.lo[a]) * b.inv[a];
+    float s, c;
+    dm::sincos_(x * kPi, &s, &c);
 #pragma unroll
     for (int o = 0; o < 12; ++o) {
-      float s, c;
-      dm::sincos_(x * scale, &s, &c);
-      f[a * 24 + 2 * o] = s;
-      f[a * 24 + 2 * o + 1] = c;
-      scale = scale * 2.0f;
+      sink(a * 24 + 2 * o, s);
+      sink(a * 24 + 2 * o + 1, c);
+      const float s2 = 2.0f * s * c, c2 = 1.0f - 2.0f * s * s;
+      s = s2;
+      c = c2;
     }
   }
-  float th = dm::acos_(dm::clamp(q[6], -1.0f, 1.0f)) * (1.0f / kPi);
-  float ph = dm::atan2_(q[5], q[4]) * (0.5f / kPi) + 0.5f;
+  const float v[2] = {dm::acos_(dm::clamp(q[6], -1.0f, 1.0f)) * (1.0f / kPi),
+                      dm::atan2_(q[5], q[4]) * (0.5f / kPi) + 0.5f};
 #pragma unroll
-  for (int i = 0; i < 32; ++i) {
-    float cth = (th - ((float)i + 0.5f) * (1.0f / 32.0f)) * 32.0f;
-    float cph = (ph - ((float)i + 0.5f) * (1.0f / 32.0f)) * 32.0f;
-    f[72 + i] = dm::exp_(-0.5f * cth * cth);
-    f[104 + i] = dm::exp_(-0.5f * cph * cph);
+  for (int j = 0; j < 2; ++j) {
+#pragma unroll
+    for (int i = 0; i < 32; ++i) sink(72 + 32 * j + i, 0.0f);
+    const int b0 = min(max((int)floorf(v[j] * 32.0f), 0), 31);
+#pragma unroll
+    for (int w = -6; w <= 6; ++w) {
+      const int i = b0 + w;
+      if (i < 0 || i > 31) continue;
+      const float ci = (v[j] - ((float)i + 0.5f) * (1.0f / 32.0f)) * 32.0f;
+      sink(72 + 32 * j + i, dm::exp_(-0.5f * ci * ci));
+    }
   }
-  f[136] = q[3];
-  f[137] = q[8];
-  f[138] = q[9];
-  f[139] = q[10];
-  f[140] = q[11];
-  f[141] = q[12];
-  f[142] = q[13];
-  f[143] = 0.0f;
+  sink(136, q[3]);
+  sink(137, q[8]);
+  sink(138, q[9]);
+  sink(139, q[10]);
+  sink(140, q[11]);
+  sink(141, q[12]);
+  sink(142, q[13]);
+  sink(143, 0.0f);
 }
 
 APD float h16(float x) { return __half2float(__float2half_rn(x)); }
@@ -244,20 +258,18 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__
   for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
     const uint32_t row = tile * kTile + t;
     {  // encode this thread's query into row t of A0 (128 x 144)
-      float q[kQueryFloats], f[kIn];
+      float q[kQueryFloats];
       if (row < n) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           float4 v = queries[4 * (size_t)row + i];
           q[4 * i] = v.x; q[4 * i + 1] = v.y; q[4 * i + 2] = v.z; q[4 * i + 3] = v.w;
         }
-        rc_encode(q, bounds, f);
+        rc_encode(q, bounds, [&](int k, float x) { act[core_offset(t, k, kIn)] = __float2half_rn(x); });
       } else {
 #pragma unroll
-        for (int i = 0; i < kIn; ++i) f[i] = 0.0f;
+        for (int k = 0; k < kIn; k += 8) *reinterpret_cast<uint4*>(act + core_offset(t, k, kIn)) = make_uint4(0, 0, 0, 0);
       }
-#pragma unroll
-      for (int k = 0; k < kIn; k += 8) store_row8(act, t, k, kIn, f + k);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -274,130 +286,143 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__
 }
 
 // ---- training (CUDA cores, FP32 on FP16-rounded weights and activations) ----
-
+//
 // Per sample: h0 = encode (FP16-rounded), h_{l+1} = fp16(relu(W_l h_l)) for
 // l = 0..3, y = W4 h4, prediction exp(y).  Relative L2 loss (the prediction in
 // the denominator held constant), averaged over samples and channels:
 //   L = mean (exp(y) - t)^2 / (exp(y)^2 + 0.01).
-// Backward: d4 = dL/dy, d_l = (W_{l+1}^T d_{l+1}) * [h_{l+1} > 0].  Stores
-// h_l and d_l for the weight gradients dW_l = sum_s d_l h_l^T.
-__global__ void __launch_bounds__(128) k_rc_forward_backward(const float* __restrict__ wf, const float4* __restrict__ queries,
-                                                             const float* __restrict__ targets, const uint32_t* __restrict__ n_dev,
-                                                             uint32_t cap, RcBounds bounds, float* __restrict__ h,
-                                                             float* __restrict__ d, float* __restrict__ loss_sum) {
-  extern __shared__ float sw[];
+// Backward: d4 = dL/dy, d_l = (W_{l+1}^T d_{l+1}) * [h_{l+1} > 0], and the
+// weight gradients dW_l = sum_s d_l h_l^T.  The batch is processed layer by
+// layer as tiled GEMMs over all samples (activations H_l and gradients D_l
+// stored row-major per sample); the sample count comes from device memory.
+
+// Encodes the batch: H0[s] = fp16-rounded features.
+__global__ void k_rc_encode_batch(const float4* __restrict__ queries, const uint32_t* __restrict__ n_dev, uint32_t cap,
+                                  RcBounds bounds, float* __restrict__ h0) {
   const uint32_t n = min(*n_dev, cap);
-  if (blockIdx.x * blockDim.x >= n) return;
-  for (int i = threadIdx.x; i < kNumParams; i += blockDim.x) sw[i] = wf[i];
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  float q[kQueryFloats];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    float4 v = queries[4 * (size_t)s + i];
+    q[4 * i] = v.x; q[4 * i + 1] = v.y; q[4 * i + 2] = v.z; q[4 * i + 3] = v.w;
+  }
+  float* row = h0 + (size_t)s * kIn;
+  rc_encode(q, bounds, [&](int k, float x) { row[k] = h16(x); });
+}
+
+enum { EPI_RELU_H16 = 0, EPI_MASK = 1, EPI_ATOMIC = 2 };
+
+// C(m, n) = sum_k A(m, k) B(k, n) over 64 x 64 tiles, 256 threads of 4 x 4
+// outputs, K staged 16 at a time in shared memory.  A(m, k) is A[m*lda + k]
+// (kAT false) or A[k*lda + m]; B(k, n) is B[k*ldb + n] (kBT false) or
+// B[n*ldb + k].  Rows m of sample-indexed operands stop at the device count
+// (kRowsAreSamples); for the weight gradients K runs over samples, split into
+// chunks along gridDim.z and summed with atomics (EPI_ATOMIC).  Epilogues:
+// fp16(relu) for hidden layers, the ReLU mask `aux` > 0 for backward
+// gradients, atomic accumulation for weight gradients.
+template <bool kAT, bool kBT, int kEpi>
+__global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, const float* __restrict__ A, int lda,
+                                               const float* __restrict__ B, int ldb, float* __restrict__ C, int ldc,
+                                               const float* __restrict__ aux, int ldaux, const uint32_t* __restrict__ n_dev,
+                                               uint32_t cap, int kchunk) {
+  __shared__ float As[16][64 + 4];
+  __shared__ float Bs[16][64 + 4];
+  const uint32_t n = min(*n_dev, cap);
+  if (kEpi != EPI_ATOMIC) M = min(M, (int)n);  // rows are samples
+  else K = min(K, (int)n);                      // the reduction runs over samples
+  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+  const int kb = kEpi == EPI_ATOMIC ? blockIdx.z * kchunk : 0;
+  const int ke = kEpi == EPI_ATOMIC ? min(K, kb + kchunk) : K;
+  if (m0 >= M || kb >= ke) return;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+  float acc[4][4] = {};
+  for (int k0 = kb; k0 < ke; k0 += 16) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int e = t * 4 + j;  // 1024 elements of each tile
+      const int kk = e >> 6, mm = e & 63;  // A tile as [k][m]
+      const int gk = k0 + kk, gm = m0 + mm, gn = n0 + mm;
+      float av = 0.0f, bv = 0.0f;
+      if (gk < ke && gm < M) av = kAT ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
+      if (gk < ke && gn < N) bv = kBT ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
+      As[kk][mm] = av;
+      Bs[kk][mm] = bv;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        a[i] = As[kk][ty * 4 + i];
+        b[i] = Bs[kk][tx * 4 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + ty * 4 + i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gn = n0 + tx * 4 + j;
+      if (gn >= N) continue;
+      float* c = C + (size_t)gm * ldc + gn;
+      if (kEpi == EPI_RELU_H16) *c = h16(fmaxf(acc[i][j], 0.0f));
+      else if (kEpi == EPI_MASK) *c = aux[(size_t)gm * ldaux + gn] > 0.0f ? acc[i][j] : 0.0f;
+      else atomicAdd(c, acc[i][j]);
+    }
+  }
+}
+
+// Output layer, loss and the first two gradients per sample: y = W4 h4,
+// d4 = dL/dy (through exp), d3 = (W4^T d4) * [h4 > 0].
+__global__ void __launch_bounds__(128) k_rc_loss(const float* __restrict__ wf, const float* __restrict__ h4,
+                                                 const float* __restrict__ targets, const uint32_t* __restrict__ n_dev,
+                                                 uint32_t cap, float* __restrict__ d4, float* __restrict__ d3,
+                                                 float* __restrict__ loss_sum) {
+  __shared__ float w4[kOut * kHid];
+  for (int i = threadIdx.x; i < kOut * kHid; i += blockDim.x) w4[i] = wf[kOffW4 + i];
   __syncthreads();
+  const uint32_t n = min(*n_dev, cap);
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   float loss = 0.0f;
   if (s < n) {
-    float* hs = h + (size_t)s * (kIn + 4 * kHid);  // h0 (144) then h1..h4 (64 each)
-    float* ds = d + (size_t)s * (4 * kHid + kOut);  // d0..d3 (64 each) then d4 (3)
-    float q[kQueryFloats], f[kIn];
-    for (int i = 0; i < 4; ++i) {
-      float4 v = queries[4 * (size_t)s + i];
-      q[4 * i] = v.x; q[4 * i + 1] = v.y; q[4 * i + 2] = v.z; q[4 * i + 3] = v.w;
-    }
-    rc_encode(q, bounds, f);
-    for (int i = 0; i < kIn; ++i) hs[i] = h16(f[i]);
-    const float* prev = hs;
-    int K = kIn;
-    const int woff[4] = {kOffW0, kOffW1, kOffW2, kOffW3};
-    for (int l = 0; l < 4; ++l) {
-      float* cur = hs + kIn + l * kHid;
-      for (int o = 0; o < kHid; ++o) {
-        const float* wr = sw + woff[l] + o * K;
-        float z = 0.0f;
-        for (int i = 0; i < K; ++i) z = fmaf(wr[i], prev[i], z);
-        cur[o] = h16(fmaxf(z, 0.0f));
-      }
-      prev = cur;
-      K = kHid;
-    }
-    float y[kOut], dy[kOut];
+    const float* h = h4 + (size_t)s * kHid;
+    float hv[kHid];
+#pragma unroll
+    for (int i = 0; i < kHid; ++i) hv[i] = h[i];
+    float dy[kOut];
     const float inv_count = 1.0f / (3.0f * (float)n);
+#pragma unroll
     for (int c = 0; c < kOut; ++c) {
-      const float* wr = sw + kOffW4 + c * kHid;
       float z = 0.0f;
-      for (int i = 0; i < kHid; ++i) z = fmaf(wr[i], prev[i], z);
-      y[c] = z;
-      float p = dm::exp_(z), tg = targets[3 * (size_t)s + c];
-      float den = p * p + 0.01f;
+#pragma unroll
+      for (int i = 0; i < kHid; ++i) z = fmaf(w4[c * kHid + i], hv[i], z);
+      const float p = dm::exp_(z), tg = targets[3 * (size_t)s + c];
+      const float den = p * p + 0.01f;
       loss += (p - tg) * (p - tg) / den;
-      dy[c] = 2.0f * (p - tg) / den * p * inv_count;  // through exp
-      ds[4 * kHid + c] = dy[c];
+      dy[c] = 2.0f * (p - tg) / den * p * inv_count;
+      d4[4 * (size_t)s + c] = dy[c];
     }
-    // d3 = (W4^T dy) * [h4 > 0]
-    float g[kHid];
-    const float* h4 = hs + kIn + 3 * kHid;
+    d4[4 * (size_t)s + 3] = 0.0f;
+#pragma unroll
     for (int i = 0; i < kHid; ++i) {
       float a = 0.0f;
-      for (int c = 0; c < kOut; ++c) a = fmaf(sw[kOffW4 + c * kHid + i], dy[c], a);
-      g[i] = h4[i] > 0.0f ? a : 0.0f;
-      ds[3 * kHid + i] = g[i];
+#pragma unroll
+      for (int c = 0; c < kOut; ++c) a = fmaf(w4[c * kHid + i], dy[c], a);
+      d3[(size_t)s * kHid + i] = hv[i] > 0.0f ? a : 0.0f;
     }
-    const int wnext[3] = {kOffW3, kOffW2, kOffW1};
-    for (int l = 2; l >= 0; --l) {  // d_l = (W_{l+1}^T d_{l+1}) * [h_{l+1} > 0]
-      const float* hl1 = hs + kIn + l * kHid;
-      const float* dn = ds + (l + 1) * kHid;
-      const float* W = sw + wnext[2 - l];
-      for (int i = 0; i < kHid; ++i) {
-        float a = 0.0f;
-        for (int o = 0; o < kHid; ++o) a = fmaf(W[o * kHid + i], dn[o], a);
-        ds[l * kHid + i] = hl1[i] > 0.0f ? a : 0.0f;
-      }
-    }
-    (void)y;
   }
-  // block sum of the loss
   for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(loss_sum, loss);
-}
-
-// dW_l[o][i] += sum over a chunk of samples of d_l[s][o] * h_l[s][i].
-__global__ void __launch_bounds__(256) k_rc_weight_grad(const float* __restrict__ h, const float* __restrict__ d,
-                                                        const uint32_t* __restrict__ n_dev, uint32_t cap, int layer,
-                                                        uint32_t chunk, float* __restrict__ grad) {
-  __shared__ float sd[32][kHid];
-  __shared__ float sh[32][kIn];
-  const uint32_t n = min(*n_dev, cap);
-  if (blockIdx.x * chunk >= n) return;
-  const int K = layer == 0 ? kIn : kHid, O = layer == 4 ? kOut : kHid;
-  const int hoff = layer == 0 ? 0 : kIn + (layer - 1) * kHid;
-  const int doff = layer == 4 ? 4 * kHid : layer * kHid;
-  const int goff = layer == 0 ? kOffW0 : (layer == 1 ? kOffW1 : (layer == 2 ? kOffW2 : (layer == 3 ? kOffW3 : kOffW4)));
-  const uint32_t s0 = blockIdx.x * chunk, s1 = min(n, s0 + chunk);
-  constexpr int kPer = (kHid * kIn + 255) / 256;
-  float acc[kPer];
-  for (int e = 0; e < kPer; ++e) acc[e] = 0.0f;
-  for (uint32_t sb = s0; sb < s1; sb += 32) {
-    const uint32_t m = min(32u, s1 - sb);
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < 32 * K; idx += 256) {
-      int r = idx / K, c = idx % K;
-      sh[r][c] = (uint32_t)r < m ? h[(size_t)(sb + r) * (kIn + 4 * kHid) + hoff + c] : 0.0f;
-    }
-    for (int idx = threadIdx.x; idx < 32 * O; idx += 256) {
-      int r = idx / O, c = idx % O;
-      sd[r][c] = (uint32_t)r < m ? d[(size_t)(sb + r) * (4 * kHid + kOut) + doff + c] : 0.0f;
-    }
-    __syncthreads();
-    for (int e = 0; e < kPer; ++e) {
-      int idx = threadIdx.x + e * 256;
-      if (idx >= O * K) break;
-      int o = idx / K, i = idx % K;
-      float a = acc[e];
-      for (int r = 0; r < 32; ++r) a = fmaf(sd[r][o], sh[r][i], a);
-      acc[e] = a;
-    }
-  }
-  for (int e = 0; e < kPer; ++e) {
-    int idx = threadIdx.x + e * 256;
-    if (idx >= O * K) break;
-    atomicAdd(&grad[goff + idx], acc[e]);
-  }
 }
 
 // Adam on the FP32 master weights, then the FP16-rounded FP32 copy used by
@@ -462,7 +487,7 @@ int ensure_batch(Cache* c, uint32_t n) {
   c->cap = 0;
   int rc;
   if ((rc = cuda_ok(c, cudaMalloc(&c->h, (size_t)n * (kIn + 4 * kHid) * 4), "batch")) ||
-      (rc = cuda_ok(c, cudaMalloc(&c->d, (size_t)n * (4 * kHid + kOut) * 4), "batch")) ||
+      (rc = cuda_ok(c, cudaMalloc(&c->d, (size_t)n * (4 * kHid + 4) * 4), "batch")) ||
       (rc = cuda_ok(c, cudaMalloc(&c->targets, (size_t)n * 12), "batch")) ||
       (rc = cuda_ok(c, cudaMalloc(&c->queries, (size_t)n * 64), "batch")) ||
       (rc = cuda_ok(c, cudaMalloc(&c->out, (size_t)n * 12), "batch")))
@@ -499,11 +524,28 @@ int rc_train_device(void* cp, const float4* queries, const float* targets, const
   if (rc) return rc;
   cudaMemsetAsync(c->grad, 0, kNumParams * 4, st);
   cudaMemsetAsync(c->loss, 0, 4, st);
-  k_rc_forward_backward<<<(cap + 127) / 128, 128, kNumParams * 4, st>>>(c->wf, queries, targets, n_dev, cap, c->bounds,
-                                                                       c->h, c->d, c->loss);
-  const uint32_t chunk = 1024;
-  for (int l = 0; l < 5; ++l)
-    k_rc_weight_grad<<<(cap + chunk - 1) / chunk, 256, 0, st>>>(c->h, c->d, n_dev, cap, l, chunk, c->grad);
+  const size_t S = cap;
+  float* H[5] = {c->h, c->h + S * kIn, c->h + S * (kIn + kHid), c->h + S * (kIn + 2 * kHid), c->h + S * (kIn + 3 * kHid)};
+  float* D[5] = {c->d, c->d + S * kHid, c->d + S * 2 * kHid, c->d + S * 3 * kHid, c->d + S * 4 * kHid};
+  const int woff[5] = {kOffW0, kOffW1, kOffW2, kOffW3, kOffW4};
+  const int width[5] = {kIn, kHid, kHid, kHid, kHid};
+  const int mt = (int)((cap + 63) / 64);
+  k_rc_encode_batch<<<(cap + 127) / 128, 128, 0, st>>>(queries, n_dev, cap, c->bounds, H[0]);
+  for (int l = 0; l < 4; ++l)  // H_{l+1} = fp16(relu(H_l W_l^T))
+    k_sgemm<false, true, EPI_RELU_H16><<<dim3(1, mt, 1), 256, 0, st>>>((int)cap, kHid, width[l], H[l], width[l],
+                                                                      c->wf + woff[l], width[l], H[l + 1], kHid, nullptr, 0,
+                                                                      n_dev, cap, 0);
+  k_rc_loss<<<(cap + 127) / 128, 128, 0, st>>>(c->wf, H[4], targets, n_dev, cap, D[4], D[3], c->loss);
+  for (int l = 2; l >= 0; --l)  // D_l = (D_{l+1} W_{l+1}) * [H_{l+1} > 0]
+    k_sgemm<false, false, EPI_MASK><<<dim3(1, mt, 1), 256, 0, st>>>((int)cap, kHid, kHid, D[l + 1], kHid,
+                                                                   c->wf + woff[l + 1], kHid, D[l], kHid, H[l + 1], kHid,
+                                                                   n_dev, cap, 0);
+  const int kchunk = 512, splits = (int)((cap + kchunk - 1) / kchunk);
+  for (int l = 0; l < 5; ++l) {  // dW_l = D_l^T H_l (sum over samples)
+    const int M = l == 4 ? kOut : kHid, N = width[l], lda = l == 4 ? 4 : kHid;
+    k_sgemm<true, false, EPI_ATOMIC><<<dim3((N + 63) / 64, 1, splits), 256, 0, st>>>(
+        M, N, (int)cap, D[l], lda, H[l], N, c->grad + woff[l], N, nullptr, 0, n_dev, cap, kchunk);
+  }
   if (update) {
     c->step += 1;
     const float b1 = 0.9f, b2 = 0.999f;
@@ -549,9 +591,7 @@ void* ap_rc_create(int device, const float* scene_lo, const float* scene_hi, uin
       (rc = ap::cuda_ok(c, cudaMalloc(&c->count, 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->packed, ap::kPackHalves * 2), "params")) ||
       (rc = ap::cuda_ok(c, cudaFuncSetAttribute(ap::k_rc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                ap::kSmemInfer), "smem")) ||
-      (rc = ap::cuda_ok(c, cudaFuncSetAttribute(ap::k_rc_forward_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                ap::kNumParams * 4), "smem"))) {
+                                                ap::kSmemInfer), "smem"))) {
     if (err) *err = rc;
     ap_rc_destroy(c);
     return nullptr;

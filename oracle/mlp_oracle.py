@@ -36,21 +36,24 @@ def encode(q, lo, hi):
     pi = f32(3.14159265358979323846)
     for a in range(3):
         x = ((q[:, a] - lo[a]) * inv[a]).astype(f32)
-        scale = pi
-        for o in range(12):
-            ang = (x * scale).astype(f32)
-            f[:, a * 24 + 2 * o] = detmath("sin", ang)
-            f[:, a * 24 + 2 * o + 1] = detmath("cos", ang)
-            scale = f32(scale * f32(2.0))
+        ang = (x * pi).astype(f32)
+        s, c = detmath("sin", ang), detmath("cos", ang)
+        for o in range(12):  # double-angle recurrence, float32 in the device's order
+            f[:, a * 24 + 2 * o] = s
+            f[:, a * 24 + 2 * o + 1] = c
+            s, c = ((f32(2.0) * s) * c).astype(f32), (f32(1.0) - (f32(2.0) * s) * s).astype(f32)
     z = np.clip(q[:, 6], f32(-1.0), f32(1.0)).astype(f32)
     th = (detmath("acos", z) * f32(1.0 / np.float32(pi))).astype(f32)
     ph = (detmath("atan2", q[:, 5], q[:, 4]) * f32(f32(0.5) / pi) + f32(0.5)).astype(f32)
-    for i in range(32):
-        c = f32((f32(i) + f32(0.5)) * f32(1.0 / 32.0))
-        cth = ((th - c) * f32(32.0)).astype(f32)
-        cph = ((ph - c) * f32(32.0)).astype(f32)
-        f[:, 72 + i] = detmath("exp", ((f32(-0.5) * cth) * cth).astype(f32))
-        f[:, 104 + i] = detmath("exp", ((f32(-0.5) * cph) * cph).astype(f32))
+    # the device evaluates the 13 bins around each peak; the rest are far below
+    # the FP16 subnormal range and round to 0 with the features
+    for j, v in enumerate((th, ph)):
+        b0 = np.clip(np.floor(v * f32(32.0)).astype(np.int64), 0, 31)
+        for i in range(32):
+            c = f32((f32(i) + f32(0.5)) * f32(1.0 / 32.0))
+            ci = ((v - c) * f32(32.0)).astype(f32)
+            val = detmath("exp", ((f32(-0.5) * ci) * ci).astype(f32))
+            f[:, 72 + 32 * j + i] = np.where(np.abs(i - b0) <= 6, val, f32(0.0))
     f[:, 136] = q[:, 3]
     f[:, 137:140] = q[:, 8:11]
     f[:, 140:143] = q[:, 11:14]

@@ -19,7 +19,13 @@ def test_encoding_ranges():
     rng = np.random.default_rng(0)
     f = mo.encode(rand_queries(500, rng), [-1, -1, -1], [11, 11, 11])
     assert f.shape == (500, 144) and f.dtype == np.float32
-    assert np.all(np.abs(f[:, :72]) <= 1.0 + 1e-6)
+    # octaves by the double-angle recurrence: within 1e-2 of sin/cos(2^o pi x)
+    qq = rand_queries(500, np.random.default_rng(0))
+    x = (qq[:, 0:3].astype(np.float64) + 1.0) / 12.0
+    for a in range(3):
+        for o in range(12):
+            assert np.abs(f[:, a * 24 + 2 * o] - np.sin(2 ** o * np.pi * x[:, a])).max() < 1e-2
+            assert np.abs(f[:, a * 24 + 2 * o + 1] - np.cos(2 ** o * np.pi * x[:, a])).max() < 1e-2
     assert np.all((f[:, 72:136] >= 0.0) & (f[:, 72:136] <= 1.0))
     # each one-blob peaks at the bin nearest the angle
     assert np.all(f[:, 72:104].max(1) > 0.88) and np.all(f[:, 104:136].max(1) > 0.88)
