@@ -12,6 +12,8 @@
 #include "dev_common.cuh"
 #include "dev_shade.cuh"
 #include "frame.cuh"
+#include "spectral.cuh"
+#include "spectral_fit.h"
 #include "traverse.cuh"
 
 namespace {
@@ -38,6 +40,9 @@ struct DeviceScene {
   void* emissive_info = nullptr;
   void* env = nullptr;
   DevScene view{};
+  // host copies for the spectral tables (ap_spectral_setup)
+  std::vector<float> host_materials;  // 26 floats per material
+  std::vector<float> host_env;        // RGB per texel
   BvhStats stats{};
   size_t bytes = 0;  // device memory held
   bool valid = false;
@@ -84,6 +89,19 @@ struct Handle {
   RcFrame rc{};
   void* rc_mem = nullptr;
   uint32_t rc_w = 0, rc_h = 0;
+  // spectral mode (ap_spectral_setup / ap_render_spectral)
+  void* spec_mats = nullptr;
+  void* spec_env = nullptr;
+  void* spec_out = nullptr;
+  size_t spec_out_bytes = 0;
+  SpectralView spec{};
+  bool spec_ready = false;
+  void spec_release() {
+    if (spec_mats) cudaFree(spec_mats);
+    if (spec_env) cudaFree(spec_env);
+    spec_mats = spec_env = nullptr;
+    spec_ready = false;
+  }
 };
 
 int fail(Handle* h, int code, const std::string& msg) {
@@ -364,6 +382,8 @@ void ap_destroy(void* hp) {
   if (h->frame_mem) cudaFree(h->frame_mem);
   if (h->trace_mem) cudaFree(h->trace_mem);
   if (h->rc_mem) cudaFree(h->rc_mem);
+  h->spec_release();
+  if (h->spec_out) cudaFree(h->spec_out);
   if (h->prof.created)
     for (int i = 0; i <= FrameProfiler::kMax; ++i) cudaEventDestroy(h->prof.ev[i]);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -449,6 +469,7 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
   h->scene.release();
+  h->spec_release();
   // flattened world triangles, instances, emissive list and CDF (vertex_pool.rs:307-348)
   std::vector<float> tv(9 * (size_t)d->num_tris);
   std::vector<InstanceDev> inst(d->num_meshes);
@@ -578,6 +599,12 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
       return rc;
     }
   }
+  {
+    const float* mf = reinterpret_cast<const float*>(d->materials);
+    s.host_materials.assign(mf, mf + 26 * (size_t)d->num_materials);
+  }
+  if (s.env) s.host_env.assign(d->env, d->env + 3 * (size_t)d->env_w * d->env_h);
+  else s.host_env.clear();
   s.stats = bvh.stats;
   s.bytes += std::max<size_t>(4 * (size_t)d->num_vertices, 16) + std::max<size_t>(sizeof(EmissiveTri) * num_emissive_tris, 16);
   s.valid = true;
@@ -777,6 +804,102 @@ int ap_profile_frame(void* hp, uint32_t w, uint32_t hgt, double* kind_ms, uint32
     }
   }
   *num_kinds = nk;
+  return AP_OK;
+}
+
+int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, float sun_scale, float scene_radius,
+                      float env_scale) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !sun_dir3 || !sun_rgb3) return AP_E_INVALID;
+  if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  if (!(scene_radius > 0.0f) || !(sun_scale >= 0.0f) || !(env_scale >= 0.0f) ||
+      !(sun_dir3[0] * sun_dir3[0] + sun_dir3[1] * sun_dir3[1] + sun_dir3[2] * sun_dir3[2] > 0.0f))
+    return fail(h, AP_E_INVALID, "spectral setup: bad light parameters");
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  h->spec_release();
+  const DeviceScene& sc = h->scene;
+  const uint32_t nm = (uint32_t)(sc.host_materials.size() / 26);
+  std::vector<spec::Material> mats(nm);
+  spec::upsample_materials(sc.host_materials.data(), nm, mats.data());
+  const size_t texels = sc.host_env.size() / 3;
+  std::vector<float> env4(4 * texels);
+  if (texels) spec::upsample_env(sc.host_env.data(), texels, env4.data());
+  int rc = check_cuda(h, cudaMalloc(&h->spec_mats, sizeof(spec::Material) * std::max<uint32_t>(nm, 1)), "spectral materials");
+  if (!rc) rc = check_cuda(h, cudaMalloc(&h->spec_env, std::max<size_t>(sizeof(float) * env4.size(), 16)), "spectral env");
+  if (!rc) rc = check_cuda(h, cudaMemcpy(h->spec_mats, mats.data(), sizeof(spec::Material) * nm, cudaMemcpyHostToDevice),
+                           "spectral materials");
+  if (!rc && texels)
+    rc = check_cuda(h, cudaMemcpy(h->spec_env, env4.data(), sizeof(float) * env4.size(), cudaMemcpyHostToDevice),
+                    "spectral env");
+  if (rc) {
+    h->spec_release();
+    return rc;
+  }
+  h->spec.mats = static_cast<const spec::Material*>(h->spec_mats);
+  h->spec.env = static_cast<const float4*>(h->spec_env);
+  h->spec.env_w = texels ? sc.view.env_w : 0;
+  h->spec.env_h = texels ? sc.view.env_h : 0;
+  h->spec.env_scale = env_scale;
+  h->spec.sun = spec::make_sun(sun_dir3, sun_rgb3, sun_scale, scene_radius);
+  h->spec_ready = true;
+  return AP_OK;
+}
+
+int ap_render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32_t row_end, uint32_t spp,
+                       uint32_t max_depth, uint32_t seed, float* out_rgb, size_t out_bytes, ap_frame_stats* stats) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  if (!h->spec_ready) return fail(h, AP_E_INVALID, "spectral mode not set up (ap_spectral_setup)");
+  if (w == 0 || hgt == 0 || w > 65536 || row_start >= row_end || row_end > hgt || spp == 0 || max_depth == 0 ||
+      max_depth > 1000)
+    return fail(h, AP_E_INVALID, "spectral render: bad arguments");
+  const size_t need = (size_t)(row_end - row_start) * w * 3 * sizeof(float);
+  if (out_rgb && out_bytes < need) return fail(h, AP_E_INVALID, "output buffer too small");
+  cudaSetDevice(h->device);
+  // the image, then the 64-bit ray counter (need is a multiple of 4 bytes: pad to 8)
+  const size_t need8 = (need + 7) & ~(size_t)7;
+  if (h->spec_out_bytes < need8 + 8) {
+    if (h->spec_out) cudaFree(h->spec_out);
+    h->spec_out = nullptr;
+    h->spec_out_bytes = 0;
+    int rc = check_cuda(h, cudaMalloc(&h->spec_out, need8 + 8), "spectral output");
+    if (rc) return rc;
+    h->spec_out_bytes = need8 + 8;
+  }
+  compute_mats(h, w, hgt);
+  SpectralCamera cam;
+  std::memcpy(cam.inv_view, h->mats.inv_view, sizeof(cam.inv_view));
+  std::memcpy(cam.inv_proj, h->mats.inv_proj, sizeof(cam.inv_proj));
+  unsigned long long* counter = reinterpret_cast<unsigned long long*>(static_cast<char*>(h->spec_out) + need8);
+  cudaMemsetAsync(counter, 0, sizeof(unsigned long long), h->stream);
+  cudaEventRecord(h->ev0, h->stream);
+  launch_spectral(h->scene.view, h->spec, cam, w, hgt, row_start, row_end, spp, (int)max_depth, seed,
+                  static_cast<float*>(h->spec_out), counter, h->stream);
+  cudaEventRecord(h->ev1, h->stream);
+  int rc = check_cuda(h, cudaGetLastError(), "spectral launch");
+  if (rc) return rc;
+  unsigned long long rays = 0;
+  rc = check_cuda(h, cudaMemcpyAsync(&rays, counter, sizeof(rays), cudaMemcpyDeviceToHost, h->stream), "ray count");
+  if (rc) return rc;
+  if (out_rgb) {
+    rc = check_cuda(h, cudaMemcpyAsync(out_rgb, h->spec_out, need, cudaMemcpyDeviceToHost, h->stream), "spectral readback");
+    if (rc) return rc;
+  }
+  rc = check_cuda(h, cudaStreamSynchronize(h->stream), "spectral render");
+  if (rc) return rc;
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->gpu_ms = ms;
+    stats->extension_rays = rays;
+    stats->kernel_launches = 1;
+    stats->width = w;
+    stats->height = hgt;
+    stats->frame_idx = h->frame_idx;
+  }
   return AP_OK;
 }
 

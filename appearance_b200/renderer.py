@@ -198,6 +198,30 @@ class PathTracer:
                                         nodes=int(visits[3 * i + 1]), tris=int(visits[3 * i + 2]))
                 for i in range(int(nk[0]))}
 
+    # -- spectral mode (the CPU tracer's estimator, crates/appearance-path-tracer)
+    SUN_DIR = (0.0, -1.0, 0.2)  # DistantLight::new in GeometryResources::new (geometry_resources.rs:52-64)
+    SUN_RGB = (1.0, 1.0, 0.95)
+
+    def spectral_setup(self, sun_dir=SUN_DIR, sun_rgb=SUN_RGB, sun_scale: float = 100.0, scene_radius: float = 1000.0,
+                       env_scale: float = 1.0):
+        """Builds the spectral tables of the uploaded scene (ap_spectral_setup)."""
+        d = np.asarray(sun_dir, np.float32).reshape(3)
+        c = np.asarray(sun_rgb, np.float32).reshape(3)
+        self._check(self._lib.ap_spectral_setup(self._h, _ptr(d), _ptr(c), sun_scale, scene_radius, env_scale))
+
+    def render_spectral(self, resolution, spp: int = 1, max_depth: int = 4, seed: int = 0, start_row: int = 0,
+                        end_row: int | None = None, to_host: bool = True):
+        """Hero-wavelength render: linear sRGB f32 rows [start_row, end_row), mean
+        of `spp` paths per pixel (to_host False keeps it on the device and
+        returns None; last_stats.gpu_ms holds the kernel time)."""
+        w, h = int(resolution[0]), int(resolution[1])
+        end_row = h if end_row is None else end_row
+        out = np.empty((end_row - start_row, w, 3), np.float32) if to_host else None
+        self._check(self._lib.ap_render_spectral(self._h, w, h, start_row, end_row, spp, max_depth, seed,
+                                                 _ptr(out) if to_host else None, out.nbytes if to_host else 0,
+                                                 ctypes.byref(self.last_stats)))
+        return out
+
     def bvh_stats(self) -> dict:
         out = np.zeros(8, np.uint32)
         self._check(self._lib.ap_bvh_stats(self._h, _ptr(out)))

@@ -251,6 +251,104 @@ def icosphere_field(seed: int = 0, num_spheres: int = 1024, num_emissive: int = 
     return b.finish(env, sun)
 
 
+def city(seed: int = 0, lots: int = 64, extent: float = 2000.0, cols: int = 16, rows: int = 19,
+         num_emissive_tris: int = 10000, env_size=(2048, 1024)) -> Scene:
+    """Procedural city: a lots x lots grid of box buildings over extent x extent
+    metres (64 x 64 on 2 km by default), footprint U[0.4, 0.85] of the lot per
+    side, height log-uniform in [5, 200] m, facade colour U[0.2, 0.8]^3 (diffuse).
+    Every facade carries a cols x rows grid of window quads 5 cm in front of it
+    (cell fill U[0.5, 0.8] per building; mirror-like metallic grey), so a
+    building has 12 + 8 cols rows triangles (2444 by default; 10.0M triangles
+    over 4096 buildings).  num_emissive_tris / 2 windows drawn uniformly over the
+    city are emitters of radiance U[1, 20] x (1, 0.8, 0.55), grouped per building
+    into emissive meshes; a 1.1 x extent ground quad and the sky_env
+    environment complete the scene.  Each building is its own mesh (flattened
+    at upload like every instance)."""
+    rng = np.random.default_rng(seed)
+    nb = lots * lots
+    lot = extent / lots
+    gx, gz = np.meshgrid(np.arange(lots), np.arange(lots), indexing="ij")
+    cx = (gx.reshape(-1) + 0.5) * lot - extent / 2
+    cz = (gz.reshape(-1) + 0.5) * lot - extent / 2
+    sx = rng.uniform(0.4, 0.85, nb) * lot
+    sz = rng.uniform(0.4, 0.85, nb) * lot
+    cx = cx + rng.uniform(-0.5, 0.5, nb) * (lot - sx) * 0.9
+    cz = cz + rng.uniform(-0.5, 0.5, nb) * (lot - sz) * 0.9
+    height = np.exp(rng.uniform(math.log(5.0), math.log(200.0), nb))
+    facade = rng.uniform(0.2, 0.8, (nb, 3))
+    fill = rng.uniform(0.5, 0.8, (nb, 2))
+    nwin = 4 * cols * rows
+    emit_flat = rng.choice(nb * nwin, size=num_emissive_tris // 2, replace=False)
+    emissive = np.zeros(nb * nwin, bool)
+    emissive[emit_flat] = True
+    emissive = emissive.reshape(nb, nwin)
+    radiance = rng.uniform(1.0, 20.0, nb * nwin).reshape(nb, nwin)
+
+    # window corners of all buildings: facade f spans corner a -> b at the base,
+    # outward normal n; window (c, r) covers the middle fill fraction of its cell
+    hx, hz = sx / 2, sz / 2
+    fac = [  # (start xz, end xz, normal xz) in units of the half extents
+        ((-1, 1), (1, 1), (0, 1)), ((1, -1), (-1, -1), (0, -1)), ((1, 1), (1, -1), (1, 0)), ((-1, -1), (-1, 1), (-1, 0))]
+    c_idx, r_idx = np.meshgrid(np.arange(cols), np.arange(rows), indexing="ij")
+    c_idx, r_idx = c_idx.reshape(-1), r_idx.reshape(-1)
+    win_p = np.zeros((nb, 4, cols * rows, 4, 3), np.float64)
+    win_n = np.zeros((nb, 4, 3), np.float64)
+    for f, ((ax, az), (bx, bz), (nx, nz)) in enumerate(fac):
+        a = np.stack([cx + ax * hx, np.zeros(nb), cz + az * hz], -1)
+        b_ = np.stack([cx + bx * hx, np.zeros(nb), cz + bz * hz], -1)
+        n = np.array([nx, 0.0, nz])
+        win_n[:, f] = n
+        u0 = (c_idx[None] + 0.5 - fill[:, :1] / 2) / cols
+        u1 = (c_idx[None] + 0.5 + fill[:, :1] / 2) / cols
+        v0 = (r_idx[None] + 0.5 - fill[:, 1:] / 2) / rows * height[:, None]
+        v1 = (r_idx[None] + 0.5 + fill[:, 1:] / 2) / rows * height[:, None]
+        along = (b_ - a)[:, None, :]
+        base = a[:, None, :] + 0.05 * n
+        up = np.array([0.0, 1.0, 0.0])
+        for k, (uu, vv) in enumerate(((u0, v0), (u1, v0), (u1, v1), (u0, v1))):
+            win_p[:, f, :, k] = base + uu[..., None] * along + vv[..., None] * up
+    win_p = win_p.reshape(nb, nwin, 4, 3).astype(np.float32)
+    quad_i = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+
+    b = _Builder()
+    glass = material(color=(0.55, 0.6, 0.65), metallic=1.0, roughness=0.1)
+    for i in range(nb):
+        box_p, box_n, box_i = _box((cx[i], cz[i]), (sx[i], height[i], sz[i]), 0.0)
+        keep = ~emissive[i]
+        wp = win_p[i, keep].reshape(-1, 3)
+        wn = np.repeat(np.repeat(win_n[i], cols * rows, 0)[keep], 4, 0)
+        nk = int(keep.sum())
+        wi = (quad_i[None] + 4 * np.arange(nk, dtype=np.uint32)[:, None, None]).reshape(-1, 3) + box_p.shape[0]
+        m = b.add_material(material(color=facade[i], roughness=0.9))
+        b.add_material(glass)
+        tm = np.concatenate([np.zeros(12, np.uint32), np.ones(2 * nk, np.uint32)])
+        b.add_mesh(np.concatenate([box_p, wp]), np.concatenate([box_n, wn]), np.concatenate([box_i, wi]), tm, m,
+                   False)
+        ne = int(emissive[i].sum())
+        if ne:
+            ep = win_p[i, emissive[i]].reshape(-1, 3)
+            en = np.repeat(np.repeat(win_n[i], cols * rows, 0)[emissive[i]], 4, 0)
+            ei = (quad_i[None] + 4 * np.arange(ne, dtype=np.uint32)[:, None, None]).reshape(-1, 3)
+            first = None
+            for r in radiance[i, emissive[i]]:
+                k = b.add_material(material(color=(0.8, 0.8, 0.8), roughness=1.0,
+                                            emission=(r, 0.8 * r, 0.55 * r)))
+                first = k if first is None else first
+            b.add_mesh(ep, en, ei, np.repeat(np.arange(ne, dtype=np.uint32), 2), first, True)
+    g = b.add_material(material(color=(0.3, 0.3, 0.3), roughness=0.9))
+    e = 0.55 * extent
+    gp, gn, gi = _quad((-e, 0.0, e), (e, 0.0, e), (e, 0.0, -e), (-e, 0.0, -e))
+    b.add_mesh(gp, gn, gi, np.zeros(2, np.uint32), g, False)
+    env = sky_env(*env_size) if env_size else None
+    sun = np.array([0.3, -1.0, 0.2, 0.5, 1.0, 1.0, 0.95, 0.0], np.float32)
+    return b.finish(env, sun)
+
+
+def city_camera(extent: float = 2000.0):
+    """Elevated view over the city towards its centre."""
+    return dict(eye=(-0.42 * extent, 0.12 * extent, -0.42 * extent), target=(0.0, 20.0, 0.0), fov=50.0)
+
+
 def camera_spline(seed: int = 0, frames: int = 64, box: float = 40.0):
     """Closed Catmull-Rom spline through 8 seeded control points circling the
     field; returns `frames` (eye, target) pairs."""

@@ -1,0 +1,124 @@
+"""Spectral-mode benchmark on the procedural city (10.0M triangles, 4096
+buildings on a 2 km grid, 10k emissive window triangles, sky environment):
+hero-wavelength paths of depth 16 at 4096 x 4096 and 64 spp, rendered in row
+bands, timed on the device.  Reports Msamples/s, Mrays/s and rays per sample;
+with --quality also the relMSE of the 64-spp image on the centre 1024 x 1024
+crop against a high-spp reference of that crop accumulated in float64.
+
+The CPU figure (--cpu-rows > 0) is the oracle's restatement of the same
+integrator on all host threads over a band of rows of the crop at 1 spp,
+extrapolated to Msamples/s.
+
+    python -m appearance_b200.spectral_bench [--lots 64] [--size 4096] [--spp 64]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import PathTracer, presets, scenes
+
+SUN = dict(sun_dir=(0.0, -1.0, 0.2), sun_rgb=(1.0, 1.0, 0.95), sun_scale=100.0)
+
+
+def setup(lots: int, size: int):
+    t0 = time.perf_counter()
+    sc = scenes.city(lots=lots, extent=2000.0 * lots / 64)
+    gen_s = time.perf_counter() - t0
+    cam = scenes.city_camera(2000.0 * lots / 64)
+    mats, _ = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], 0.5, 5000.0, size, size, None)
+    return sc, mats, gen_s
+
+
+def rel_mse(x, ref):
+    return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def render_bands(pt, size, spp, depth, seed, band, to_host=False):
+    """The image in row bands; returns (image or None, device ms, rays)."""
+    img = np.empty((size, size, 3), np.float32) if to_host else None
+    ms, rays = 0.0, 0
+    for r0 in range(0, size, band):
+        r1 = min(size, r0 + band)
+        out = pt.render_spectral((size, size), spp=spp, max_depth=depth, seed=seed, start_row=r0, end_row=r1,
+                                 to_host=to_host)
+        if to_host:
+            img[r0:r1] = out
+        ms += pt.last_stats.gpu_ms
+        rays += int(pt.last_stats.extension_rays)
+    return img, ms, rays
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m appearance_b200.spectral_bench")
+    ap.add_argument("--lots", type=int, default=64)
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--depth", type=int, default=16)
+    ap.add_argument("--band", type=int, default=512, help="rows per launch")
+    ap.add_argument("--repeats", type=int, default=1)
+    ap.add_argument("--quality", action="store_true", help="relMSE of the crop against a high-spp reference")
+    ap.add_argument("--ref-spp", type=int, default=4096)
+    ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the crop rendered by the CPU oracle")
+    a = ap.parse_args(argv)
+    sc, mats, gen_s = setup(a.lots, a.size)
+    pt = PathTracer(presets.PLAIN)
+    t0 = time.perf_counter()
+    pt.upload_scene(sc)
+    upload_s = time.perf_counter() - t0
+    pt.set_camera_matrices(mats)
+    radius = 0.75 * 2000.0 * a.lots / 64
+    pt.spectral_setup(scene_radius=radius, **SUN)
+    # warm-up: one band at a few samples
+    render_bands(pt, a.size, min(a.spp, 4), a.depth, 1, a.band)
+    runs = []
+    for rep in range(a.repeats):
+        _, ms, rays = render_bands(pt, a.size, a.spp, a.depth, 100 + rep, a.band)
+        runs.append((ms, rays))
+    ms = float(np.median([r[0] for r in runs]))
+    rays = runs[0][1]
+    samples = a.size * a.size * a.spp
+    res = {"metric": "spectral Msamples/s", "value": samples / (ms * 1e3), "unit": "Msamples/s",
+           "frame_ms": ms, "rays": rays, "rays_per_sample": rays / samples, "mrays_per_s": rays / (ms * 1e3),
+           "config": {"workload": f"city {a.lots}x{a.lots} buildings, {sc.num_tris} tris, "
+                                  f"{a.size}x{a.size} x {a.spp} spp, depth {a.depth}, 4 wavelengths",
+                      "band_rows": a.band, "scene_gen_s": gen_s, "upload_and_bvh_s": upload_s},
+           "bvh": pt.bvh_stats()}
+    c0, c1 = a.size // 2 - a.size // 8, a.size // 2 + a.size // 8  # centre crop rows/cols (1024 of 4096)
+    if a.quality:
+        img, _, _ = render_bands(pt, a.size, a.spp, a.depth, 100, a.band, to_host=True)
+        ref = np.zeros((c1 - c0, c1 - c0, 3), np.float64)
+        chunk, done, seed = 256, 0, 10_000
+        while done < a.ref_spp:
+            k = min(chunk, a.ref_spp - done)
+            out = pt.render_spectral((a.size, a.size), spp=k, max_depth=a.depth, seed=seed, start_row=c0, end_row=c1)
+            ref += out[:, c0:c1].astype(np.float64) * k
+            done += k
+            seed += 1
+        ref /= a.ref_spp
+        res["quality"] = {"crop": [c0, c1], "ref_spp": a.ref_spp,
+                          "relmse_crop": rel_mse(img[c0:c1, c0:c1].astype(np.float64), ref),
+                          "mean_crop": ref.mean(axis=(0, 1)).tolist()}
+    if a.cpu_rows > 0:
+        from oracle.oracle import OracleScene, OracleSpectral  # the CPU baseline only
+        osp = OracleSpectral(OracleScene(sc), scene_radius=radius, **SUN)
+        r0 = a.size // 2 - a.cpu_rows // 2
+        threads = os.cpu_count()
+        t0 = time.perf_counter()
+        osp.render(mats, a.size, a.size, spp=1, max_depth=a.depth, seed=100, row0=r0, row1=r0 + a.cpu_rows,
+                   threads=threads)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": a.cpu_rows * a.size / dt / 1e6, "unit": "Msamples/s", "cores": threads,
+                               "kind": "port", "sample": f"rows {r0}..{r0 + a.cpu_rows} of the {a.size}^2 image "
+                                                         f"(full width) at 1 spp, {dt:.1f} s"}
+    pt.close()
+    print(json.dumps(res), flush=True)
+    return res
+
+
+if __name__ == "__main__":
+    main()

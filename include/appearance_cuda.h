@@ -208,6 +208,33 @@ int ap_profile_frame(void* handle, uint32_t w, uint32_t h, double* kind_ms, uint
  * traversal stack, build ms (as double bits in out[4..5]). */
 int ap_bvh_stats(void* handle, uint32_t* out8);
 
+/* ---- spectral mode: the CPU tracer's estimator (appearance-path-tracer) ----
+ *
+ * Replaces the render of crates/appearance-path-tracer/src/lib.rs:79-195
+ * (PathTracer::render -> path_tracer::render_pixels, path_tracer.rs:28-67 ->
+ * PathIntegrator::li, path_integrator.rs:103-307): four hero wavelengths per
+ * path, RGB albedos and emitters upsampled to spectra, diffuse / conductor /
+ * dielectric BxDFs, the distant light by next-event estimation and the
+ * environment on escape.
+ *
+ * ap_spectral_setup builds the spectral tables of the uploaded scene (call
+ * again after every ap_scene_upload): the distant light travels along
+ * sun_dir3 with radiance sun_scale x the illuminant spectrum of sun_rgb3, its
+ * shadow rays end 2 x scene_radius away (DistantLight::new(dir, spectrum,
+ * scale, scene_radius), geometry_resources.rs:52-64: (0,-1,0.2), (1,1,0.95),
+ * 100, 1000); the environment's texels are scaled by env_scale. */
+int ap_spectral_setup(void* handle, const float* sun_dir3, const float* sun_rgb3, float sun_scale, float scene_radius,
+                      float env_scale);
+/* Renders rows [row_start, row_end) of a w x h image with `spp` paths per
+ * pixel through the pixel centre (the reference renders 1 per frame), paths of
+ * at most max_depth surface interactions (the reference uses 4), random
+ * numbers from (pixel, sample, seed).  out_rgb receives linear sRGB, 3 floats
+ * per pixel, the mean over the samples; with out_rgb NULL the image stays on
+ * the device (timing).  Synchronous; stats->gpu_ms is the kernel's device time
+ * and stats->extension_rays the rays it traced (closest and shadow). */
+int ap_render_spectral(void* handle, uint32_t w, uint32_t h, uint32_t row_start, uint32_t row_end, uint32_t spp,
+                       uint32_t max_depth, uint32_t seed, float* out_rgb, size_t out_bytes, ap_frame_stats* stats);
+
 /* ---- render-serving loop ------------------------------------------------
  * No reference counterpart as an API: it takes the role of the reference's
  * frame farm (Host/Node, crates/appearance-render-loop/src/host.rs:250-505,

@@ -71,6 +71,16 @@ def lib():
         L.orc_disney.argtypes = [P] * 7
         L.orc_detmath.argtypes = [U, P, P, P, U]
         L.orc_resolve_rgba8.argtypes = [P, U, U, U, P, U, P]
+        L.orc_spectral_new.restype = P
+        L.orc_spectral_new.argtypes = [P, P, P, F, F, F]
+        L.orc_spectral_free.argtypes = [P]
+        L.orc_spectral_render.argtypes = [P, P, P, U, U, U, U, U, ctypes.c_int, U, U, P]
+        L.orc_spectral_tables.argtypes = [P, P, P]
+        L.orc_spectral_cmf.argtypes = [F, P]
+        L.orc_spectral_fit.argtypes = [P, P]
+        L.orc_spectral_sigmoid.argtypes = [P, F, P]
+        L.orc_spectral_wavelength.argtypes = [F, P]
+        L.orc_spectral_illuminant_norm.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -169,6 +179,68 @@ class OracleDisplay:
                                 _p(self.accum), self.count, _p(out))
         self.count += 1
         return out
+
+
+class OracleSpectral:
+    """The spectral mode on the CPU (oracle_spectral.cpp) for one scene; the
+    arguments mean what they mean in PathTracer.spectral_setup / render_spectral."""
+
+    def __init__(self, oscene: OracleScene, sun_dir=(0.0, -1.0, 0.2), sun_rgb=(1.0, 1.0, 0.95), sun_scale=100.0,
+                 scene_radius=1000.0, env_scale=1.0):
+        self.scene = oscene
+        self.n_mats = oscene._keep["mat"].shape[0]
+        env = oscene._keep["env"]
+        self.env_texels = 0 if env is None else env.shape[0] * env.shape[1]
+        self.ptr = lib().orc_spectral_new(oscene.ptr, _p(np.asarray(sun_dir, np.float32)),
+                                          _p(np.asarray(sun_rgb, np.float32)), sun_scale, scene_radius, env_scale)
+
+    def render(self, mats: np.ndarray, width: int, height: int, spp: int = 1, max_depth: int = 4, seed: int = 0,
+               row0: int = 0, row1: int | None = None, threads: int = 0) -> np.ndarray:
+        row1 = height if row1 is None else row1
+        m = np.ascontiguousarray(np.asarray(mats, np.float32).reshape(4, 16))
+        out = np.zeros((row1 - row0, width, 3), np.float32)
+        lib().orc_spectral_render(self.ptr, _p(m[0]), _p(m[1]), width, height, row0, row1, spp, max_depth, seed,
+                                  threads or os.cpu_count(), _p(out))
+        return out
+
+    def tables(self):
+        mats = np.zeros((self.n_mats, 12), np.float32)
+        env = np.zeros((self.env_texels, 4), np.float32)
+        lib().orc_spectral_tables(self.ptr, _p(mats), _p(env))
+        return mats, env
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().orc_spectral_free(self.ptr)
+            self.ptr = None
+
+
+def spectral_cmf(lam: float) -> np.ndarray:
+    out = np.zeros(4, np.float32)
+    lib().orc_spectral_cmf(lam, _p(out))
+    return out
+
+
+def spectral_fit(rgb) -> np.ndarray:
+    c = np.zeros(3, np.float32)
+    lib().orc_spectral_fit(_p(np.asarray(rgb, np.float32)), _p(c))
+    return c
+
+
+def spectral_sigmoid(coef, lam: float) -> float:
+    out = np.zeros(1, np.float32)
+    lib().orc_spectral_sigmoid(_p(np.asarray(coef, np.float32)), lam, _p(out))
+    return float(out[0])
+
+
+def spectral_wavelength(u: float):
+    out = np.zeros(2, np.float32)
+    lib().orc_spectral_wavelength(u, _p(out))
+    return float(out[0]), float(out[1])
+
+
+def spectral_illuminant_norm() -> float:
+    return float(lib().orc_spectral_illuminant_norm())
 
 
 DETMATH = dict(sin=0, cos=1, exp=2, log=3, pow=4, atan2=5, acos=6)

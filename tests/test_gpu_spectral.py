@@ -1,0 +1,83 @@
+"""Spectral mode on the GPU vs the oracle: both run the same hero-wavelength
+integrator (spectral.h) under the same per-(pixel, sample) PCG streams, the
+GPU through the compressed 8-wide BVH and the oracle through its binary BVH,
+so the images must be identical bit for bit."""
+import numpy as np
+import pytest
+
+from appearance_b200 import PathTracer, presets, scenes
+from appearance_b200.renderer import RendererError
+from oracle.oracle import OracleScene, OracleSpectral
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_bits(a, b, what):
+    a, b = np.ascontiguousarray(a, np.float32), np.ascontiguousarray(b, np.float32)
+    same = a.view(np.uint32) == b.view(np.uint32)
+    assert same.all(), f"{what}: {(~same).sum()} of {same.size} words differ"
+
+
+def field_scene():
+    sc = scenes.icosphere_field(seed=2, num_spheres=48, num_emissive=6, subdiv=2, box=10.0, env_size=(128, 64))
+    sc.materials[:10, 8] = 1.0  # dielectrics
+    sc.materials[:10, 3] = 0.0
+    return sc
+
+
+CASES = {
+    "cornell": (scenes.cornell_box, lambda w, h: scenes.camera_matrices(
+        scenes.cornell_camera()["eye"], scenes.cornell_camera()["target"], scenes.cornell_camera()["fov"],
+        0.01, 100.0, w, h, None)[0], dict(sun_scale=0.0, scene_radius=10.0)),
+    "field": (field_scene, lambda w, h: scenes.camera_matrices((5.0, 6.0, -14.0), (5.0, 3.0, 5.0), 60.0, 0.01,
+                                                                1000.0, w, h, None)[0],
+              dict(sun_scale=20.0, scene_radius=100.0, env_scale=0.5)),
+}
+
+
+@pytest.mark.parametrize("case,spp,depth,seed", [("cornell", 2, 4, 0), ("cornell", 1, 16, 5), ("field", 2, 8, 3),
+                                                 ("field", 1, 16, 11)])
+def test_spectral_matches_oracle_bit_exact(case, spp, depth, seed):
+    make, cam, light = CASES[case]
+    sc = make()
+    w, h = 64, 48
+    mats = cam(w, h)
+    pt = PathTracer(presets.PLAIN)
+    pt.upload_scene(sc)
+    pt.set_camera_matrices(mats)
+    pt.spectral_setup(**light)
+    img = pt.render_spectral((w, h), spp=spp, max_depth=depth, seed=seed)
+    ref = OracleSpectral(OracleScene(sc), **light).render(mats, w, h, spp=spp, max_depth=depth, seed=seed)
+    assert img.mean() > 0.0
+    assert_bits(img, ref, f"{case} spp={spp} depth={depth}")
+    # a row range renders the same rows
+    part = pt.render_spectral((w, h), spp=spp, max_depth=depth, seed=seed, start_row=7, end_row=30)
+    assert_bits(part, img[7:30], "rows 7..30")
+    pt.close()
+
+
+def test_spectral_device_only_and_errors():
+    sc = scenes.cornell_box()
+    pt = PathTracer(presets.PLAIN)
+    pt.upload_scene(sc)
+    cam = scenes.cornell_camera()
+    pt.set_camera(cam["eye"], cam["target"], cam["fov"], 0.01, 100.0, 32, 32)
+    with pytest.raises(RendererError):
+        pt.render_spectral((32, 32))  # not set up
+    pt.spectral_setup(sun_scale=0.0, scene_radius=10.0)
+    assert pt.render_spectral((32, 32), spp=4, to_host=False) is None
+    assert pt.last_stats.gpu_ms > 0.0
+    a = pt.render_spectral((32, 32), spp=4, seed=1)
+    b = pt.render_spectral((32, 32), spp=4, seed=1)
+    assert_bits(a, b, "repeat")
+    with pytest.raises(RendererError):
+        pt.render_spectral((32, 32), spp=0)
+    with pytest.raises(RendererError):
+        pt.render_spectral((32, 32), start_row=10, end_row=5)
+    with pytest.raises(RendererError):
+        pt.spectral_setup(sun_dir=(0.0, 0.0, 0.0))
+    # re-uploading the scene drops the tables
+    pt.upload_scene(sc)
+    with pytest.raises(RendererError):
+        pt.render_spectral((32, 32))
+    pt.close()
