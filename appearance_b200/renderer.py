@@ -216,7 +216,7 @@ class PathTracer:
         returns None; last_stats.gpu_ms holds the kernel time)."""
         w, h = int(resolution[0]), int(resolution[1])
         end_row = h if end_row is None else end_row
-        out = np.empty((end_row - start_row, w, 3), np.float32) if to_host else None
+        out = np.empty((max(0, end_row - start_row), w, 3), np.float32) if to_host else None
         self._check(self._lib.ap_render_spectral(self._h, w, h, start_row, end_row, spp, max_depth, seed,
                                                  _ptr(out) if to_host else None, out.nbytes if to_host else 0,
                                                  ctypes.byref(self.last_stats)))
