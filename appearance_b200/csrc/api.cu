@@ -853,30 +853,32 @@ int ap_render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, u
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
   if (!h->spec_ready) return fail(h, AP_E_INVALID, "spectral mode not set up (ap_spectral_setup)");
   if (w == 0 || hgt == 0 || w > 65536 || row_start >= row_end || row_end > hgt || spp == 0 || max_depth == 0 ||
-      max_depth > 1000)
+      max_depth > (uint32_t)kSpectralMaxDepth || (uint64_t)w * (row_end - row_start) > (1ull << 26))
     return fail(h, AP_E_INVALID, "spectral render: bad arguments");
   const size_t need = (size_t)(row_end - row_start) * w * 3 * sizeof(float);
   if (out_rgb && out_bytes < need) return fail(h, AP_E_INVALID, "output buffer too small");
   cudaSetDevice(h->device);
-  // the image, then the 64-bit ray counter (need is a multiple of 4 bytes: pad to 8)
-  const size_t need8 = (need + 7) & ~(size_t)7;
-  if (h->spec_out_bytes < need8 + 8) {
+  // the image, then the wavefront's work area
+  const uint32_t P = w * (row_end - row_start);
+  const size_t need_a = (need + 255) & ~(size_t)255;
+  const size_t total = need_a + spectral_work_bytes(P);
+  if (h->spec_out_bytes < total) {
     if (h->spec_out) cudaFree(h->spec_out);
     h->spec_out = nullptr;
     h->spec_out_bytes = 0;
-    int rc = check_cuda(h, cudaMalloc(&h->spec_out, need8 + 8), "spectral output");
+    int rc = check_cuda(h, cudaMalloc(&h->spec_out, total), "spectral buffers");
     if (rc) return rc;
-    h->spec_out_bytes = need8 + 8;
+    h->spec_out_bytes = total;
   }
   compute_mats(h, w, hgt);
   SpectralCamera cam;
   std::memcpy(cam.inv_view, h->mats.inv_view, sizeof(cam.inv_view));
   std::memcpy(cam.inv_proj, h->mats.inv_proj, sizeof(cam.inv_proj));
-  unsigned long long* counter = reinterpret_cast<unsigned long long*>(static_cast<char*>(h->spec_out) + need8);
-  cudaMemsetAsync(counter, 0, sizeof(unsigned long long), h->stream);
+  void* work = static_cast<char*>(h->spec_out) + need_a;
+  const unsigned long long* counter = spectral_ray_counter(work, P);
   cudaEventRecord(h->ev0, h->stream);
-  launch_spectral(h->scene.view, h->spec, cam, w, hgt, row_start, row_end, spp, (int)max_depth, seed,
-                  static_cast<float*>(h->spec_out), counter, h->stream);
+  const int launches = launch_spectral(h->scene.view, h->spec, cam, w, hgt, row_start, row_end, spp, (int)max_depth,
+                                       seed, static_cast<float*>(h->spec_out), work, h->num_sms, h->stream);
   cudaEventRecord(h->ev1, h->stream);
   int rc = check_cuda(h, cudaGetLastError(), "spectral launch");
   if (rc) return rc;
@@ -895,7 +897,7 @@ int ap_render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, u
     std::memset(stats, 0, sizeof(*stats));
     stats->gpu_ms = ms;
     stats->extension_rays = rays;
-    stats->kernel_launches = 1;
+    stats->kernel_launches = (uint32_t)launches;
     stats->width = w;
     stats->height = hgt;
     stats->frame_idx = h->frame_idx;

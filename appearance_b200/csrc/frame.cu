@@ -15,6 +15,7 @@
 
 #include "dev_shade.cuh"
 #include "frame.cuh"
+#include "persistent.cuh"
 #include "traverse.cuh"
 
 namespace ap {
@@ -167,65 +168,9 @@ APD GiRes gi_new() {
 
 // Lane of the calling thread within its warp, for any block shape (a 2-D
 // block's warps span several rows, so threadIdx.x alone does not give it).
-APD uint32_t lane_id() {
-  uint32_t l;
-  asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
-  return l;
-}
-
 APD void mul4(const float* m, float v0, float v1, float v2, float v3, float out[4]) {
 #pragma unroll
   for (int r = 0; r < 4; ++r) out[r] = m[r] * v0 + m[4 + r] * v1 + m[8 + r] * v2 + m[12 + r] * v3;
-}
-
-// Persistent traversal with per-lane refill: a lane that finishes its ray
-// takes the next one through a warp-aggregated atomic on `cursor`, so warps
-// stay full until the batch drains.  Lanes check for a refill every
-// kStepBudget steps (the best of 8, 16, 32 measured on the benchmark
-// scene).  load(i, o, d, tmax) fetches ray i,
-// store(i, trav, visits) writes its result.  The traversal kernels run with
-// the child tests unrolled and are register-capped for 6 resident blocks of
-// kBlock threads per SM (the best of the measured 1..8 on the benchmark scene).
-constexpr int kStepBudget = 8;
-constexpr int kTraceMinBlocks = 6;
-
-template <bool kAny, bool kCount, class Load, class Store>
-APD void persistent_trace(const DevScene& s, uint32_t count, uint32_t* cursor, Load load, Store store) {
-  const uint32_t lane = lane_id();
-  uint2 stack[kTraversalStack];
-  Trav t;
-  Visits vc;
-  uint32_t cur = 0;
-  bool active = false, exhausted = false;
-  while (true) {
-    if (!exhausted) {
-      const unsigned need = __ballot_sync(0xffffffffu, !active);
-      if (need) {
-        const int leader = __ffs(need) - 1;
-        uint32_t base = 0;
-        if ((int)lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(need));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (base + (uint32_t)__popc(need) >= count) exhausted = true;
-        if (!active) {
-          const uint32_t idx = base + __popc(need & ((1u << lane) - 1u));
-          if (idx < count) {
-            float3 o, d;
-            float tmax;
-            load(idx, o, d, tmax);
-            trav_init(t, o, d, tmax);
-            vc = Visits();
-            cur = idx;
-            active = true;
-          }
-        }
-      }
-    }
-    if (!__any_sync(0xffffffffu, active)) break;
-    if (active && trav_step<kAny, kCount, true>(s, t, stack, kStepBudget, &vc)) {
-      store(cur, t, vc);
-      active = false;
-    }
-  }
 }
 
 // raygen.wgsl:21-39

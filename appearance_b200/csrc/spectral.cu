@@ -1,14 +1,27 @@
-// Spectral (hero-wavelength) rendering on sm_100a: one thread per pixel runs
-// spec::pixel_sample (spectral.h) for each of its samples, tracing through the
-// compressed 8-wide BVH with the shared closest-hit and any-hit traversals
-// (traverse.cuh).  Output is linear sRGB, the mean over the pixel's samples.
-// Rays traced are summed per warp and added to a 64-bit counter.
+// Spectral (hero-wavelength) rendering on sm_100a as a wavefront.
+//
+// One pass per sample index renders that sample for every pixel of the rows:
+// the camera rays of all pixels, then up to max_depth + 1 rounds of
+//   extend: persistent closest-hit traversal of the compacted ray queue;
+//   shade:  spec::path_vertex (spectral.h) per live path -- emission or the
+//           environment, the light sample's shadow ray, BSDF sampling and
+//           Russian roulette -- pushing surviving paths and shadow rays into
+//           the next queues (warp ballot + one atomic per warp);
+//   shadow: persistent any-hit traversal of the shadow queue, adding the
+//           light sample's contribution of unoccluded rays;
+// then the pass's radiance goes through the XYZ sensor into the pixel sums.
+// Each path runs exactly the vertex sequence of spec::li, so the image equals
+// the per-pixel loop of the CPU restatement bit for bit.
+#include <algorithm>
+
+#include "persistent.cuh"
 #include "spectral.cuh"
-#include "traverse.cuh"
 
 namespace ap {
 
 namespace {
+
+constexpr int kBlock = 128;
 
 struct GpuGeo {
   const DevScene& s;
@@ -17,20 +30,7 @@ struct GpuGeo {
   uint32_t env_w, env_h;
   float env_scale;
   spec::Sun sun;
-  uint32_t* rays;  // rays traced by this thread
 
-  APD bool closest(spec::V3 o, spec::V3 d, float tmax, spec::Hit& h) const {
-    *rays += 1;
-    Hit r;
-    bool hit = trace_closest(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), tmax, r);
-    h.t = r.t;
-    h.tri = r.tri;
-    return hit;
-  }
-  APD bool occluded(spec::V3 o, spec::V3 d, float tmax) const {
-    *rays += 1;
-    return trace_any(s, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), tmax);
-  }
   APD void tri(uint32_t g, spec::V3* p0, spec::V3* p1, spec::V3* p2) const {
     const InstanceDev& in = s.instances[s.tri_instance[g]];
     uint32_t fi = in.first_index + (g - in.first_global_tri) * 3;
@@ -54,38 +54,212 @@ struct GpuGeo {
   }
 };
 
-__global__ void __launch_bounds__(128) k_spectral(DevScene s, SpectralView v, SpectralCamera cam, uint32_t W,
-                                                  uint32_t H, uint32_t row0, uint32_t row1, uint32_t spp,
-                                                  int max_depth, uint32_t seed, float* out,
-                                                  unsigned long long* ray_count) {
-  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t y = row0 + blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= W || y >= row1) return;
-  uint32_t rays = 0;
-  GpuGeo g{s, v.mats, v.env, v.env_w, v.env_h, v.env_scale, v.sun, &rays};
-  spec::V3 acc = spec::v3(0.0f, 0.0f, 0.0f);
-  for (uint32_t k = 0; k < spp; ++k)
-    acc = acc + spec::pixel_sample(g, cam.inv_view, cam.inv_proj, x, y, W, H, k, seed, max_depth);
-  const float inv = 1.0f / (float)spp;
-  float* o = out + 3 * ((size_t)(y - row0) * W + x);
-  o[0] = acc.x * inv;
-  o[1] = acc.y * inv;
-  o[2] = acc.z * inv;
-  const uint32_t mask = __activemask();
-  const uint32_t warp_rays = __reduce_add_sync(mask, rays);
-  uint32_t lane;
-  asm("mov.u32 %0, %%laneid;" : "=r"(lane));
-  if (ray_count && __ffs(mask) - 1 == (int)lane) atomicAdd(ray_count, (unsigned long long)warp_rays);
+// Per-path state and queues of P paths (one per pixel of the rows).
+struct SpecBuffers {
+  float4* rq_o[2];  // extension ray queue (by bounce parity): origin
+  float4* rq_d[2];  //   direction, w = owning path (bits)
+  uint2* hits;      // per extension queue slot: t (bits), triangle
+  float4* sq_o;     // shadow ray queue: origin, w = tmax
+  float4* sq_d;     //   direction, w = owning path (bits)
+  float4* L;        // spectral radiance of the path (4 wavelengths)
+  float4* beta;     // path throughput
+  float4* lambda;   // the path's wavelengths
+  float4* shc;      // contribution of the pending shadow ray
+  float4* acc;      // linear sRGB sum over the samples so far (xyz)
+  uint4* misc;      // rng state, depth, eta_scale (bits), 0
+  uint32_t* counters;  // per round: extension size, cursor, shadow size, cursor
+  unsigned long long* rays;
+};
+
+constexpr size_t kAlign = 256;
+
+size_t carve(void* base, uint32_t P, SpecBuffers* b) {
+  char* p = static_cast<char*>(base);
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> void* {
+    void* r = p ? p + off : nullptr;
+    off += (bytes + kAlign - 1) & ~(kAlign - 1);
+    return r;
+  };
+  const size_t f4 = sizeof(float4) * (size_t)P;
+  for (int q = 0; q < 2; ++q) {
+    b->rq_o[q] = static_cast<float4*>(take(f4));
+    b->rq_d[q] = static_cast<float4*>(take(f4));
+  }
+  b->hits = static_cast<uint2*>(take(sizeof(uint2) * (size_t)P));
+  b->sq_o = static_cast<float4*>(take(f4));
+  b->sq_d = static_cast<float4*>(take(f4));
+  b->L = static_cast<float4*>(take(f4));
+  b->beta = static_cast<float4*>(take(f4));
+  b->lambda = static_cast<float4*>(take(f4));
+  b->shc = static_cast<float4*>(take(f4));
+  b->acc = static_cast<float4*>(take(f4));
+  b->misc = static_cast<uint4*>(take(sizeof(uint4) * (size_t)P));
+  b->counters = static_cast<uint32_t*>(take(sizeof(uint32_t) * 4 * (kSpectralMaxDepth + 2)));
+  b->rays = static_cast<unsigned long long*>(take(sizeof(unsigned long long)));
+  return off;
+}
+
+APD float4 f4(spec::S4 a) { return make_float4(a.v[0], a.v[1], a.v[2], a.v[3]); }
+APD spec::S4 s4of(float4 a) { return spec::S4{{a.x, a.y, a.z, a.w}}; }
+
+// Appends (o, w0), (d, owner) to a queue with one atomic per warp.
+APD void push(bool want, uint32_t* size, float4* qo, float4* qd, spec::V3 o, float w0, spec::V3 d, uint32_t owner) {
+  const unsigned active = __activemask();
+  const unsigned bal = __ballot_sync(active, want);
+  if (!want) return;
+  const int lane = (int)lane_id();
+  const int leader = __ffs(bal) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(size, (uint32_t)__popc(bal));
+  base = __shfl_sync(bal, base, leader);
+  const uint32_t slot = base + __popc(bal & ((1u << lane) - 1u));
+  qo[slot] = make_float4(o.x, o.y, o.z, w0);
+  qd[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(owner));
+}
+
+__global__ void __launch_bounds__(kBlock) k_sgen(SpecBuffers b, SpectralCamera cam, uint32_t W, uint32_t H,
+                                                 uint32_t row0, uint32_t P, uint32_t sample, uint32_t seed) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const uint32_t x = p % W, y = row0 + p / W;
+  spec::V3 o, d;
+  spec::camera_ray(cam.inv_view, cam.inv_proj, x, y, W, H, &o, &d);
+  spec::Rng rng = spec::rng_for(y * W + x, sample, seed);
+  const spec::Wavelengths w = spec::sample_visible(rng.next());
+  b.rq_o[0][p] = make_float4(o.x, o.y, o.z, 0.0f);
+  b.rq_d[0][p] = make_float4(d.x, d.y, d.z, __uint_as_float(p));
+  b.lambda[p] = f4(w.lambda);
+  b.L[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  b.beta[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+  b.misc[p] = make_uint4(rng.s, 0u, __float_as_uint(1.0f), 0u);
+  if (sample == 0) b.acc[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s, SpecBuffers b, uint32_t round,
+                                                                     uint32_t P) {
+  const uint32_t count = round == 0 ? P : min(b.counters[4 * round], P);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && count) atomicAdd(b.rays, (unsigned long long)count);
+  const float4* qo = b.rq_o[round & 1];
+  const float4* qd = b.rq_d[round & 1];
+  persistent_trace<false, false>(
+      s, count, &b.counters[4 * round + 1],
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        const float4 a = qo[i], c = qd[i];
+        o = f3(a.x, a.y, a.z);
+        d = f3(c.x, c.y, c.z);
+        tmax = 1e30f;
+      },
+      [&](uint32_t i, const Trav& t, const Visits&) { b.hits[i] = make_uint2(__float_as_uint(t.hit.t), t.hit.tri); });
+}
+
+__global__ void __launch_bounds__(kBlock) k_sshade(DevScene s, SpectralView v, SpecBuffers b, uint32_t round,
+                                                   uint32_t P, int max_depth) {
+  const uint32_t count = round == 0 ? P : min(b.counters[4 * round], P);
+  const float4* qo = b.rq_o[round & 1];
+  const float4* qd = b.rq_d[round & 1];
+  float4* no = b.rq_o[(round + 1) & 1];
+  float4* nd = b.rq_d[(round + 1) & 1];
+  const GpuGeo g{s, v.mats, v.env, v.env_w, v.env_h, v.env_scale, v.sun};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const float4 ro = qo[i], rd = qd[i];
+    const uint32_t owner = __float_as_uint(rd.w);
+    const uint2 hh = b.hits[i];
+    spec::V3 o = spec::v3(ro.x, ro.y, ro.z), d = spec::v3(rd.x, rd.y, rd.z);
+    const spec::Hit h{__uint_as_float(hh.x), hh.y};
+    const uint4 m = b.misc[owner];
+    spec::PathState ps{s4of(b.L[owner]), s4of(b.beta[owner]), __uint_as_float(m.z), (int)m.y, spec::Rng{m.x}};
+    const spec::S4 lam = s4of(b.lambda[owner]);
+    bool shadow;
+    spec::ShadowRay sh = {};
+    const bool more = spec::path_vertex(g, o, d, hh.y != kNoHit ? &h : nullptr, lam, ps, max_depth, &shadow, &sh);
+    b.L[owner] = f4(ps.L);
+    if (more) {
+      b.beta[owner] = f4(ps.beta);
+      b.misc[owner] = make_uint4(ps.rng.s, (uint32_t)ps.depth, __float_as_uint(ps.eta_scale), 0u);
+    }
+    if (shadow) b.shc[owner] = f4(sh.c);
+    push(shadow, &b.counters[4 * round + 2], b.sq_o, b.sq_d, sh.o, sh.tmax, sh.d, owner);
+    push(more, &b.counters[4 * (round + 1)], no, nd, o, 0.0f, d, owner);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sshadow(DevScene s, SpecBuffers b, uint32_t round,
+                                                                     uint32_t P) {
+  const uint32_t count = min(b.counters[4 * round + 2], P);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && count) atomicAdd(b.rays, (unsigned long long)count);
+  persistent_trace<true, false>(
+      s, count, &b.counters[4 * round + 3],
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        const float4 a = b.sq_o[i], c = b.sq_d[i];
+        o = f3(a.x, a.y, a.z);
+        d = f3(c.x, c.y, c.z);
+        tmax = a.w;
+      },
+      [&](uint32_t i, const Trav& t, const Visits&) {
+        if (t.hit.tri != kNoHit) return;  // occluded
+        const uint32_t owner = __float_as_uint(b.sq_d[i].w);
+        b.L[owner] = f4(s4of(b.L[owner]) + s4of(b.shc[owner]));
+      });
+}
+
+__global__ void __launch_bounds__(kBlock) k_saccum(SpecBuffers b, uint32_t P, bool last, float inv, float* out) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  spec::Wavelengths w;
+  w.lambda = s4of(b.lambda[p]);
+  for (int k = 0; k < 4; ++k) w.pdf.v[k] = spec::visible_wavelength_pdf(w.lambda.v[k]);
+  const spec::V3 rgb = spec::xyz_to_srgb(spec::to_xyz(s4of(b.L[p]), w));
+  const float4 a = b.acc[p];
+  const spec::V3 acc = spec::v3(a.x, a.y, a.z) + rgb;
+  if (last) {
+    out[3 * (size_t)p + 0] = acc.x * inv;
+    out[3 * (size_t)p + 1] = acc.y * inv;
+    out[3 * (size_t)p + 2] = acc.z * inv;
+  } else {
+    b.acc[p] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+  }
 }
 
 }  // namespace
 
-void launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCamera& cam, uint32_t W, uint32_t H,
-                     uint32_t row0, uint32_t row1, uint32_t spp, int max_depth, uint32_t seed, float* out,
-                     unsigned long long* ray_count, cudaStream_t st) {
-  dim3 block(16, 8);
-  dim3 grid((W + block.x - 1) / block.x, (row1 - row0 + block.y - 1) / block.y);
-  k_spectral<<<grid, block, 0, st>>>(s, v, cam, W, H, row0, row1, spp, max_depth, seed, out, ray_count);
+size_t spectral_work_bytes(uint32_t P) {
+  SpecBuffers b;
+  return carve(nullptr, P, &b);
+}
+
+const unsigned long long* spectral_ray_counter(void* work, uint32_t P) {
+  SpecBuffers b;
+  carve(work, P, &b);
+  return b.rays;
+}
+
+int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCamera& cam, uint32_t W, uint32_t H,
+                    uint32_t row0, uint32_t row1, uint32_t spp, int max_depth, uint32_t seed, float* out, void* work,
+                    int num_sms, cudaStream_t st) {
+  const uint32_t P = W * (row1 - row0);
+  SpecBuffers b;
+  carve(work, P, &b);
+  const uint32_t rounds = (uint32_t)max_depth + 1;
+  const int linear = (int)((P + kBlock - 1) / kBlock);
+  const int persistent = num_sms * kTraceMinBlocks;
+  const int shade = std::min(linear, num_sms * 16);
+  int launches = 0;
+  cudaMemsetAsync(b.rays, 0, sizeof(unsigned long long), st);
+  for (uint32_t k = 0; k < spp; ++k) {
+    cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * 4 * (rounds + 1), st);
+    k_sgen<<<linear, kBlock, 0, st>>>(b, cam, W, H, row0, P, k, seed);
+    ++launches;
+    for (uint32_t r = 0; r < rounds; ++r) {
+      k_sextend<<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      k_sshade<<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth);
+      k_sshadow<<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      launches += 3;
+    }
+    k_saccum<<<linear, kBlock, 0, st>>>(b, P, k + 1 == spp, 1.0f / (float)spp, out);
+    ++launches;
+  }
+  return launches;
 }
 
 }  // namespace ap

@@ -146,14 +146,14 @@ SPHD float illuminant(float l) {
 
 // Albedo (RgbAlbedoSpectrum) and emission (RgbIlluminantSpectrum: scale x
 // sigmoid x illuminant) samples at the four wavelengths.
-SPHD S4 albedo4(const float* c, const Wavelengths& w) {
+SPHD S4 albedo4(const float* c, const S4& lambda) {
   S4 r;
-  for (int i = 0; i < 4; ++i) r.v[i] = sigmoid_poly(c, w.lambda.v[i]);
+  for (int i = 0; i < 4; ++i) r.v[i] = sigmoid_poly(c, lambda.v[i]);
   return r;
 }
-SPHD S4 emission4(const float* c, float scale, const Wavelengths& w) {
+SPHD S4 emission4(const float* c, float scale, const S4& lambda) {
   S4 r;
-  for (int i = 0; i < 4; ++i) r.v[i] = scale * sigmoid_poly(c, w.lambda.v[i]) * illuminant(w.lambda.v[i]);
+  for (int i = 0; i < 4; ++i) r.v[i] = scale * sigmoid_poly(c, lambda.v[i]) * illuminant(lambda.v[i]);
   return r;
 }
 
@@ -381,7 +381,7 @@ struct Hit {
 // (sampling/mod.rs:65-70); the spectra of the four nearest texel centres are
 // interpolated bilinearly (clamped).
 template <class Geo>
-SPHD S4 env_le(const Geo& g, V3 d, const Wavelengths& w) {
+SPHD S4 env_le(const Geo& g, V3 d, const S4& lambda) {
   if (g.env_w == 0) return s4(0.0f);
   float u = (dm::atan2_(d.z, d.x) + kPi) * (1.0f / (2.0f * kPi));
   float v = dm::acos_(dm::clamp(d.y, -1.0f, 1.0f)) * (1.0f / kPi);
@@ -397,67 +397,105 @@ SPHD S4 env_le(const Geo& g, V3 d, const Wavelengths& w) {
     float wgt = ((k & 1) ? ax : 1.0f - ax) * ((k >> 1) ? ay : 1.0f - ay);
     float c[4];
     g.env_texel((uint32_t)yi * g.env_w + (uint32_t)xi, c);
-    acc = acc + emission4(c, c[3], w) * wgt;
+    acc = acc + emission4(c, c[3], lambda) * wgt;
   }
   return acc * g.env_scale;
 }
 
-// PathIntegrator::li (path_integrator.rs:103-307) for one camera ray; returns
-// the spectral radiance at the four wavelengths.
+// State of one path of PathIntegrator::li between vertices.
+struct PathState {
+  S4 L, beta;
+  float eta_scale;
+  int depth;
+  Rng rng;
+};
+SPHD PathState path_start(Rng rng) { return PathState{s4(0.0f), s4(1.0f), 1.0f, 0, rng}; }
+
+// Shadow ray of the distant light: its contribution c is added to L unless
+// the segment (o, d, [0, tmax]) is occluded.
+struct ShadowRay {
+  V3 o, d;
+  float tmax;
+  S4 c;
+};
+
+// One vertex of PathIntegrator::li (path_integrator.rs:103-307): `hit` is the
+// closest hit of the ray (o, d), or null when it escaped.  Adds emission (or
+// the environment on escape), sets *shadow and fills sh for the light sample,
+// samples the BSDF and applies Russian roulette.  Returns true when the path
+// goes on along the updated (o, d).  li below runs it in a loop; the GPU runs
+// it as one stage of a wavefront.
 template <class Geo>
-SPHD S4 li(const Geo& g, V3 o, V3 d, const Wavelengths& w, Rng& rng, int max_depth) {
-  S4 L = s4(0.0f), beta = s4(1.0f);
-  float eta_scale = 1.0f;
-  int depth = 0;
-  for (int guard = 0; guard < 1024; ++guard) {
-    Hit h;
-    if (!g.closest(o, d, 1e30f, h)) {  // escaped: the environment (not in the light sampler: weight 1)
-      L = L + beta * env_le(g, d, w);
-      break;
-    }
-    V3 p0, p1, p2;
-    g.tri(h.tri, &p0, &p1, &p2);
-    const Material& m = g.material(h.tri);
-    V3 hit = o + d * h.t;
-    V3 ng = normalize(cross(p1 - p0, p2 - p0));
-    V3 wo = -d;
-    if (m.emit_scale > 0.0f && dot(ng, wo) > 0.0f) L = L + beta * emission4(m.emit, m.emit_scale, w);
-    depth += 1;
-    if (depth > max_depth) break;
-    Bsdf b;
-    if (m.metallic > 0.9f) b.kind = BX_CONDUCTOR;
-    else if (m.transmission > 0.0f) b.kind = BX_DIELECTRIC;
-    else b.kind = BX_DIFFUSE;
-    b.albedo = albedo4(m.albedo, w);
-    V3 n = (b.kind != BX_DIELECTRIC && dot(ng, wo) < 0.0f) ? -ng : ng;
-    b.fr = frame_of(n);
-    if (b.kind != BX_DIELECTRIC && g.sun.scale > 0.0f) {  // sample_ld: the distant light (delta: no MIS)
-      V3 wi = v3(-g.sun.dir[0], -g.sun.dir[1], -g.sun.dir[2]);
-      S4 f = bsdf_f(b, wo, wi) * dm::fabs_(dot(wi, n));
-      if (nonzero(f)) {
-        V3 lp = hit + wi * (2.0f * g.sun.radius);
-        if (!g.occluded(hit + wi * 0.0001f, wi, dist(hit, lp)))
-          L = L + beta * (f * emission4(g.sun.coef, g.sun.scale, w));
-      }
-    }
-    // three draws in a fixed order (argument evaluation order is unspecified)
-    const float uc = rng.next();
-    const float u0 = rng.next();
-    const float u1 = rng.next();
-    BsdfSample s = bsdf_sample(b, wo, uc, u0, u1);
-    if (!s.ok) break;
-    beta = beta * (s.f * (dm::fabs_(dot(s.wi, n)) / s.pdf));
-    if (s.transmission) eta_scale = eta_scale * (s.eta * s.eta);
-    o = hit + s.wi * 0.0001f;
-    d = s.wi;
-    S4 rr = beta * eta_scale;
-    if (max4(rr) < 1.0f && depth > 1) {
-      float q = dm::fmax(1.0f - max4(rr), 0.0f);
-      if (rng.next() < q) break;
-      beta = beta * (1.0f / (1.0f - q));
+SPHD bool path_vertex(const Geo& g, V3& o, V3& d, const Hit* h, const S4& lambda, PathState& ps, int max_depth,
+                      bool* shadow, ShadowRay* sh) {
+  *shadow = false;
+  if (!h) {  // escaped: the environment (not in the light sampler: weight 1)
+    ps.L = ps.L + ps.beta * env_le(g, d, lambda);
+    return false;
+  }
+  V3 p0, p1, p2;
+  g.tri(h->tri, &p0, &p1, &p2);
+  const Material& m = g.material(h->tri);
+  V3 hit = o + d * h->t;
+  V3 ng = normalize(cross(p1 - p0, p2 - p0));
+  V3 wo = -d;
+  if (m.emit_scale > 0.0f && dot(ng, wo) > 0.0f) ps.L = ps.L + ps.beta * emission4(m.emit, m.emit_scale, lambda);
+  ps.depth += 1;
+  if (ps.depth > max_depth) return false;
+  Bsdf b;
+  if (m.metallic > 0.9f) b.kind = BX_CONDUCTOR;
+  else if (m.transmission > 0.0f) b.kind = BX_DIELECTRIC;
+  else b.kind = BX_DIFFUSE;
+  b.albedo = albedo4(m.albedo, lambda);
+  V3 n = (b.kind != BX_DIELECTRIC && dot(ng, wo) < 0.0f) ? -ng : ng;
+  b.fr = frame_of(n);
+  if (b.kind != BX_DIELECTRIC && g.sun.scale > 0.0f) {  // sample_ld: the distant light (delta: no MIS)
+    V3 wi = v3(-g.sun.dir[0], -g.sun.dir[1], -g.sun.dir[2]);
+    S4 f = bsdf_f(b, wo, wi) * dm::fabs_(dot(wi, n));
+    if (nonzero(f)) {
+      V3 lp = hit + wi * (2.0f * g.sun.radius);
+      sh->o = hit + wi * 0.0001f;
+      sh->d = wi;
+      sh->tmax = dist(hit, lp);
+      sh->c = ps.beta * (f * emission4(g.sun.coef, g.sun.scale, lambda));
+      *shadow = true;
     }
   }
-  return L;
+  // three draws in a fixed order (argument evaluation order is unspecified)
+  const float uc = ps.rng.next();
+  const float u0 = ps.rng.next();
+  const float u1 = ps.rng.next();
+  BsdfSample s = bsdf_sample(b, wo, uc, u0, u1);
+  if (!s.ok) return false;
+  ps.beta = ps.beta * (s.f * (dm::fabs_(dot(s.wi, n)) / s.pdf));
+  if (s.transmission) ps.eta_scale = ps.eta_scale * (s.eta * s.eta);
+  o = hit + s.wi * 0.0001f;
+  d = s.wi;
+  S4 rr = ps.beta * ps.eta_scale;
+  if (max4(rr) < 1.0f && ps.depth > 1) {
+    float q = dm::fmax(1.0f - max4(rr), 0.0f);
+    if (ps.rng.next() < q) return false;
+    ps.beta = ps.beta * (1.0f / (1.0f - q));
+  }
+  return true;
+}
+
+// PathIntegrator::li for one camera ray: at most max_depth + 1 closest-hit
+// rays, each followed by its vertex and the vertex's shadow ray.
+template <class Geo>
+SPHD S4 li(const Geo& g, V3 o, V3 d, const S4& lambda, Rng& rng, int max_depth) {
+  PathState ps = path_start(rng);
+  for (int k = 0; k <= max_depth; ++k) {
+    Hit h;
+    const bool hit = g.closest(o, d, 1e30f, h);
+    bool shadow;
+    ShadowRay sh = {};
+    const bool more = path_vertex(g, o, d, hit ? &h : nullptr, lambda, ps, max_depth, &shadow, &sh);
+    if (shadow && !g.occluded(sh.o, sh.d, sh.tmax)) ps.L = ps.L + sh.c;
+    if (!more) break;
+  }
+  rng = ps.rng;
+  return ps.L;
 }
 
 // Column-major 4x4 matrix times (x, y, z, w), summed in a fixed order.
@@ -465,24 +503,33 @@ SPHD void mul4(const float* m, float x, float y, float z, float w, float* o) {
   for (int r = 0; r < 4; ++r) o[r] = m[r] * x + m[4 + r] * y + m[8 + r] * z + m[12 + r] * w;
 }
 
-// Linear sRGB of one sample of pixel (x, y): the ray through the pixel centre
-// (uv of lib.rs:138-142, camera of path_tracer.rs:42-45), the wavelengths
+// Camera ray through the centre of pixel (x, y): the uv of lib.rs:138-142 and
+// the camera of path_tracer.rs:42-45 (direction normalised).
+SPHD void camera_ray(const float* inv_view, const float* inv_proj, uint32_t x, uint32_t y, uint32_t W, uint32_t H,
+                     V3* o, V3* d) {
+  float ux = (((float)x + 0.5f) / (float)W) * 2.0f - 1.0f;
+  float uy = (((float)y + 0.5f) / (float)H) * 2.0f - 1.0f;
+  uy = -uy;
+  float oo[4], t[4], dd[4];
+  mul4(inv_view, 0.0f, 0.0f, 0.0f, 1.0f, oo);
+  mul4(inv_proj, ux, uy, 1.0f, 1.0f, t);
+  V3 tn = normalize(v3(t[0], t[1], t[2]));
+  mul4(inv_view, tn.x, tn.y, tn.z, 0.0f, dd);
+  *o = v3(oo[0], oo[1], oo[2]);
+  *d = normalize(v3(dd[0], dd[1], dd[2]));
+}
+
+// Linear sRGB of one sample of pixel (x, y): the camera ray, the wavelengths
 // from the sample's first random number (path_tracer.rs:59), li, the XYZ
 // sensor and the sRGB matrix.
 template <class Geo>
 SPHD V3 pixel_sample(const Geo& g, const float* inv_view, const float* inv_proj, uint32_t x, uint32_t y, uint32_t W,
                      uint32_t H, uint32_t sample, uint32_t seed, int max_depth) {
-  float ux = (((float)x + 0.5f) / (float)W) * 2.0f - 1.0f;
-  float uy = (((float)y + 0.5f) / (float)H) * 2.0f - 1.0f;
-  uy = -uy;
-  float o[4], t[4], d[4];
-  mul4(inv_view, 0.0f, 0.0f, 0.0f, 1.0f, o);
-  mul4(inv_proj, ux, uy, 1.0f, 1.0f, t);
-  V3 tn = normalize(v3(t[0], t[1], t[2]));
-  mul4(inv_view, tn.x, tn.y, tn.z, 0.0f, d);
+  V3 o, d;
+  camera_ray(inv_view, inv_proj, x, y, W, H, &o, &d);
   Rng rng = rng_for(y * W + x, sample, seed);
   Wavelengths w = sample_visible(rng.next());
-  S4 L = li(g, v3(o[0], o[1], o[2]), normalize(v3(d[0], d[1], d[2])), w, rng, max_depth);
+  S4 L = li(g, o, d, w.lambda, rng, max_depth);
   return xyz_to_srgb(to_xyz(L, w));
 }
 
