@@ -53,69 +53,74 @@ def render_bands(pt, size, spp, depth, seed, band, to_host=False):
     return img, ms, rays
 
 
+def measure(lots=64, size=4096, spp=64, depth=16, band=4096, repeats=1, quality=False, ref_spp=4096,
+            cpu_rows=0) -> dict:
+    sc, mats, gen_s = setup(lots, size)
+    pt = PathTracer(presets.PLAIN)
+    t0 = time.perf_counter()
+    pt.upload_scene(sc)
+    upload_s = time.perf_counter() - t0
+    pt.set_camera_matrices(mats)
+    radius = 0.75 * 2000.0 * lots / 64
+    pt.spectral_setup(scene_radius=radius, **SUN)
+    render_bands(pt, size, min(spp, 4), depth, 1, band)  # warm-up at a few samples
+    runs = []
+    for rep in range(repeats):
+        _, ms, rays = render_bands(pt, size, spp, depth, 100 + rep, band)
+        runs.append((ms, rays, pt.last_stats.kernel_launches))
+    ms = float(np.median([r[0] for r in runs]))
+    rays = runs[0][1]
+    samples = size * size * spp
+    res = {"metric": "spectral Msamples/s", "value": samples / (ms * 1e3), "unit": "Msamples/s",
+           "frame_ms": ms, "rays": rays, "rays_per_sample": rays / samples, "mrays_per_s": rays / (ms * 1e3),
+           "workload": f"city {lots}x{lots} buildings, {sc.num_tris} tris, {size}x{size} x {spp} spp, "
+                       f"depth {depth}, 4 wavelengths, wavefront in bands of {band} rows",
+           "kernel_launches_per_band": runs[0][2], "scene_gen_s": gen_s, "upload_and_bvh_s": upload_s,
+           "bvh": pt.bvh_stats()}
+    c0, c1 = size // 2 - size // 8, size // 2 + size // 8  # centre crop rows/cols (1024 of 4096)
+    if quality:
+        img, _, _ = render_bands(pt, size, spp, depth, 100, band, to_host=True)
+        ref = np.zeros((c1 - c0, c1 - c0, 3), np.float64)
+        chunk, done, seed = 256, 0, 10_000
+        while done < ref_spp:
+            k = min(chunk, ref_spp - done)
+            out = pt.render_spectral((size, size), spp=k, max_depth=depth, seed=seed, start_row=c0, end_row=c1)
+            ref += out[:, c0:c1].astype(np.float64) * k
+            done += k
+            seed += 1
+        ref /= ref_spp
+        res["quality"] = {"crop": [c0, c1], "ref_spp": ref_spp,
+                          "relmse_crop": rel_mse(img[c0:c1, c0:c1].astype(np.float64), ref),
+                          "mean_crop": ref.mean(axis=(0, 1)).tolist()}
+    pt.close()
+    if cpu_rows > 0:
+        from oracle.oracle import OracleScene, OracleSpectral  # the CPU baseline only
+        osp = OracleSpectral(OracleScene(sc), scene_radius=radius, **SUN)
+        r0 = size // 2 - cpu_rows // 2
+        threads = os.cpu_count()
+        t0 = time.perf_counter()
+        osp.render(mats, size, size, spp=1, max_depth=depth, seed=100, row0=r0, row1=r0 + cpu_rows,
+                   threads=threads)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": cpu_rows * size / dt / 1e6, "unit": "Msamples/s", "cores": threads,
+                               "kind": "port", "sample": f"oracle, rows {r0}..{r0 + cpu_rows} of the {size}^2 "
+                                                         f"image (full width) at 1 spp, {dt:.1f} s"}
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m appearance_b200.spectral_bench")
     ap.add_argument("--lots", type=int, default=64)
     ap.add_argument("--size", type=int, default=4096)
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--depth", type=int, default=16)
-    ap.add_argument("--band", type=int, default=512, help="rows per launch")
+    ap.add_argument("--band", type=int, default=4096, help="rows per launch sequence")
     ap.add_argument("--repeats", type=int, default=1)
     ap.add_argument("--quality", action="store_true", help="relMSE of the crop against a high-spp reference")
     ap.add_argument("--ref-spp", type=int, default=4096)
     ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the crop rendered by the CPU oracle")
     a = ap.parse_args(argv)
-    sc, mats, gen_s = setup(a.lots, a.size)
-    pt = PathTracer(presets.PLAIN)
-    t0 = time.perf_counter()
-    pt.upload_scene(sc)
-    upload_s = time.perf_counter() - t0
-    pt.set_camera_matrices(mats)
-    radius = 0.75 * 2000.0 * a.lots / 64
-    pt.spectral_setup(scene_radius=radius, **SUN)
-    # warm-up: one band at a few samples
-    render_bands(pt, a.size, min(a.spp, 4), a.depth, 1, a.band)
-    runs = []
-    for rep in range(a.repeats):
-        _, ms, rays = render_bands(pt, a.size, a.spp, a.depth, 100 + rep, a.band)
-        runs.append((ms, rays))
-    ms = float(np.median([r[0] for r in runs]))
-    rays = runs[0][1]
-    samples = a.size * a.size * a.spp
-    res = {"metric": "spectral Msamples/s", "value": samples / (ms * 1e3), "unit": "Msamples/s",
-           "frame_ms": ms, "rays": rays, "rays_per_sample": rays / samples, "mrays_per_s": rays / (ms * 1e3),
-           "config": {"workload": f"city {a.lots}x{a.lots} buildings, {sc.num_tris} tris, "
-                                  f"{a.size}x{a.size} x {a.spp} spp, depth {a.depth}, 4 wavelengths",
-                      "band_rows": a.band, "scene_gen_s": gen_s, "upload_and_bvh_s": upload_s},
-           "bvh": pt.bvh_stats()}
-    c0, c1 = a.size // 2 - a.size // 8, a.size // 2 + a.size // 8  # centre crop rows/cols (1024 of 4096)
-    if a.quality:
-        img, _, _ = render_bands(pt, a.size, a.spp, a.depth, 100, a.band, to_host=True)
-        ref = np.zeros((c1 - c0, c1 - c0, 3), np.float64)
-        chunk, done, seed = 256, 0, 10_000
-        while done < a.ref_spp:
-            k = min(chunk, a.ref_spp - done)
-            out = pt.render_spectral((a.size, a.size), spp=k, max_depth=a.depth, seed=seed, start_row=c0, end_row=c1)
-            ref += out[:, c0:c1].astype(np.float64) * k
-            done += k
-            seed += 1
-        ref /= a.ref_spp
-        res["quality"] = {"crop": [c0, c1], "ref_spp": a.ref_spp,
-                          "relmse_crop": rel_mse(img[c0:c1, c0:c1].astype(np.float64), ref),
-                          "mean_crop": ref.mean(axis=(0, 1)).tolist()}
-    if a.cpu_rows > 0:
-        from oracle.oracle import OracleScene, OracleSpectral  # the CPU baseline only
-        osp = OracleSpectral(OracleScene(sc), scene_radius=radius, **SUN)
-        r0 = a.size // 2 - a.cpu_rows // 2
-        threads = os.cpu_count()
-        t0 = time.perf_counter()
-        osp.render(mats, a.size, a.size, spp=1, max_depth=a.depth, seed=100, row0=r0, row1=r0 + a.cpu_rows,
-                   threads=threads)
-        dt = time.perf_counter() - t0
-        res["cpu_baseline"] = {"value": a.cpu_rows * a.size / dt / 1e6, "unit": "Msamples/s", "cores": threads,
-                               "kind": "port", "sample": f"rows {r0}..{r0 + a.cpu_rows} of the {a.size}^2 image "
-                                                         f"(full width) at 1 spp, {dt:.1f} s"}
-    pt.close()
+    res = measure(a.lots, a.size, a.spp, a.depth, a.band, a.repeats, a.quality, a.ref_spp, a.cpu_rows)
     print(json.dumps(res), flush=True)
     return res
 

@@ -277,7 +277,9 @@ def main():
         line["gpu_launches"] = int(details["gpu_launches_per_step"]) * args.steps
         if world == 1 and args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(scene, path, cfg)
-        line["configs"] = {"cornell_512_16spp_depth5": cornell_config(world == 1 and bool(args.cpu_baseline))}
+        cpu = world == 1 and bool(args.cpu_baseline)
+        line["configs"] = {"cornell_512_16spp_depth5": cornell_config(cpu),
+                           "city_spectral_4096_64spp_depth16": city_spectral_config(cpu)}
         print(json.dumps(line), flush=True)
     pt.close()
     if world > 1:
@@ -319,6 +321,17 @@ def cornell_config(cpu: bool) -> dict:
                                "cores": os.cpu_count(), "kind": "port",
                                "sample": f"oracle, same scene and estimator at {cw}x{ch}, 16 spp, depth 5, 1 frame"}
     return out
+
+
+def city_spectral_config(cpu: bool) -> dict:
+    """The large spectral configuration: the seeded 10.0M-triangle city (4096
+    buildings on a 2 km grid, 10k emissive window triangles, sky environment),
+    hero-wavelength paths (4 wavelengths in 360-830 nm, RGB-to-spectrum
+    albedos and emitters), depth 16, 4096x4096 at 64 spp: one warm-up image at
+    4 spp, then one timed image (device time).  The CPU oracle of the same
+    integrator renders 64 full-width rows at 1 spp beside it."""
+    from appearance_b200 import spectral_bench
+    return spectral_bench.measure(cpu_rows=64 if cpu else 0)
 
 
 def measure_details(pt, scene, path, cfg) -> dict:
