@@ -846,8 +846,10 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
   return AP_OK;
 }
 
-int ap_render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32_t row_end, uint32_t spp,
-                       uint32_t max_depth, uint32_t seed, float* out_rgb, size_t out_bytes, ap_frame_stats* stats) {
+namespace {
+int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32_t row_end, uint32_t spp,
+                    uint32_t max_depth, uint32_t seed, float* out_rgb, size_t out_bytes, ap_frame_stats* stats,
+                    uint64_t* visits6) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return AP_E_INVALID;
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
@@ -875,15 +877,16 @@ int ap_render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, u
   std::memcpy(cam.inv_view, h->mats.inv_view, sizeof(cam.inv_view));
   std::memcpy(cam.inv_proj, h->mats.inv_proj, sizeof(cam.inv_proj));
   void* work = static_cast<char*>(h->spec_out) + need_a;
-  const unsigned long long* counter = spectral_ray_counter(work, P);
+  const unsigned long long* counter = spectral_stats(work, P);
   cudaEventRecord(h->ev0, h->stream);
   const int launches = launch_spectral(h->scene.view, h->spec, cam, w, hgt, row_start, row_end, spp, (int)max_depth,
-                                       seed, static_cast<float*>(h->spec_out), work, h->num_sms, h->stream);
+                                       seed, static_cast<float*>(h->spec_out), work, h->num_sms, visits6 != nullptr,
+                                       h->stream);
   cudaEventRecord(h->ev1, h->stream);
   int rc = check_cuda(h, cudaGetLastError(), "spectral launch");
   if (rc) return rc;
-  unsigned long long rays = 0;
-  rc = check_cuda(h, cudaMemcpyAsync(&rays, counter, sizeof(rays), cudaMemcpyDeviceToHost, h->stream), "ray count");
+  unsigned long long cnt[6] = {0, 0, 0, 0, 0, 0};
+  rc = check_cuda(h, cudaMemcpyAsync(cnt, counter, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream), "ray count");
   if (rc) return rc;
   if (out_rgb) {
     rc = check_cuda(h, cudaMemcpyAsync(out_rgb, h->spec_out, need, cudaMemcpyDeviceToHost, h->stream), "spectral readback");
@@ -896,13 +899,27 @@ int ap_render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, u
   if (stats) {
     std::memset(stats, 0, sizeof(*stats));
     stats->gpu_ms = ms;
-    stats->extension_rays = rays;
+    stats->extension_rays = cnt[0] + cnt[3];
     stats->kernel_launches = (uint32_t)launches;
     stats->width = w;
     stats->height = hgt;
     stats->frame_idx = h->frame_idx;
   }
+  if (visits6)
+    for (int i = 0; i < 6; ++i) visits6[i] = cnt[i];
   return AP_OK;
+}
+}  // namespace
+
+int ap_render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32_t row_end, uint32_t spp,
+                       uint32_t max_depth, uint32_t seed, float* out_rgb, size_t out_bytes, ap_frame_stats* stats) {
+  return render_spectral(hp, w, hgt, row_start, row_end, spp, max_depth, seed, out_rgb, out_bytes, stats, nullptr);
+}
+
+int ap_profile_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32_t row_end, uint32_t spp,
+                        uint32_t max_depth, uint32_t seed, uint64_t* visits6, ap_frame_stats* stats) {
+  if (!visits6) return AP_E_INVALID;
+  return render_spectral(hp, w, hgt, row_start, row_end, spp, max_depth, seed, nullptr, 0, stats, visits6);
 }
 
 int ap_bvh_stats(void* hp, uint32_t* out8) {

@@ -68,7 +68,9 @@ struct SpecBuffers {
   float4* acc;      // linear sRGB sum over the samples so far (xyz)
   uint4* misc;      // rng state, depth, eta_scale (bits), 0
   uint32_t* counters;  // per round: extension size, cursor, shadow size, cursor
-  unsigned long long* rays;
+  // closest-hit rays, nodes, triangles; any-hit rays, nodes, triangles (nodes
+  // and triangles only in the counting form)
+  unsigned long long* stats;
 };
 
 constexpr size_t kAlign = 256;
@@ -96,7 +98,7 @@ size_t carve(void* base, uint32_t P, SpecBuffers* b) {
   b->acc = static_cast<float4*>(take(f4));
   b->misc = static_cast<uint4*>(take(sizeof(uint4) * (size_t)P));
   b->counters = static_cast<uint32_t*>(take(sizeof(uint32_t) * 4 * (kSpectralMaxDepth + 2)));
-  b->rays = static_cast<unsigned long long*>(take(sizeof(unsigned long long)));
+  b->stats = static_cast<unsigned long long*>(take(6 * sizeof(unsigned long long)));
   return off;
 }
 
@@ -136,13 +138,14 @@ __global__ void __launch_bounds__(kBlock) k_sgen(SpecBuffers b, SpectralCamera c
   if (sample == 0) b.acc[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s, SpecBuffers b, uint32_t round,
                                                                      uint32_t P) {
   const uint32_t count = round == 0 ? P : min(b.counters[4 * round], P);
-  if (blockIdx.x == 0 && threadIdx.x == 0 && count) atomicAdd(b.rays, (unsigned long long)count);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && count) atomicAdd(&b.stats[0], (unsigned long long)count);
   const float4* qo = b.rq_o[round & 1];
   const float4* qd = b.rq_d[round & 1];
-  persistent_trace<false, false>(
+  persistent_trace<false, kCount>(
       s, count, &b.counters[4 * round + 1],
       [&](uint32_t i, float3& o, float3& d, float& tmax) {
         const float4 a = qo[i], c = qd[i];
@@ -150,7 +153,13 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s,
         d = f3(c.x, c.y, c.z);
         tmax = 1e30f;
       },
-      [&](uint32_t i, const Trav& t, const Visits&) { b.hits[i] = make_uint2(__float_as_uint(t.hit.t), t.hit.tri); });
+      [&](uint32_t i, const Trav& t, const Visits& vc) {
+        b.hits[i] = make_uint2(__float_as_uint(t.hit.t), t.hit.tri);
+        if (kCount) {
+          atomicAdd(&b.stats[1], (unsigned long long)vc.nodes);
+          atomicAdd(&b.stats[2], (unsigned long long)vc.tris);
+        }
+      });
 }
 
 __global__ void __launch_bounds__(kBlock) k_sshade(DevScene s, SpectralView v, SpecBuffers b, uint32_t round,
@@ -184,11 +193,12 @@ __global__ void __launch_bounds__(kBlock) k_sshade(DevScene s, SpectralView v, S
   }
 }
 
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sshadow(DevScene s, SpecBuffers b, uint32_t round,
                                                                      uint32_t P) {
   const uint32_t count = min(b.counters[4 * round + 2], P);
-  if (blockIdx.x == 0 && threadIdx.x == 0 && count) atomicAdd(b.rays, (unsigned long long)count);
-  persistent_trace<true, false>(
+  if (blockIdx.x == 0 && threadIdx.x == 0 && count) atomicAdd(&b.stats[3], (unsigned long long)count);
+  persistent_trace<true, kCount>(
       s, count, &b.counters[4 * round + 3],
       [&](uint32_t i, float3& o, float3& d, float& tmax) {
         const float4 a = b.sq_o[i], c = b.sq_d[i];
@@ -196,7 +206,11 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sshadow(DevScene s,
         d = f3(c.x, c.y, c.z);
         tmax = a.w;
       },
-      [&](uint32_t i, const Trav& t, const Visits&) {
+      [&](uint32_t i, const Trav& t, const Visits& vc) {
+        if (kCount) {
+          atomicAdd(&b.stats[4], (unsigned long long)vc.nodes);
+          atomicAdd(&b.stats[5], (unsigned long long)vc.tris);
+        }
         if (t.hit.tri != kNoHit) return;  // occluded
         const uint32_t owner = __float_as_uint(b.sq_d[i].w);
         b.L[owner] = f4(s4of(b.L[owner]) + s4of(b.shc[owner]));
@@ -228,15 +242,15 @@ size_t spectral_work_bytes(uint32_t P) {
   return carve(nullptr, P, &b);
 }
 
-const unsigned long long* spectral_ray_counter(void* work, uint32_t P) {
+const unsigned long long* spectral_stats(void* work, uint32_t P) {
   SpecBuffers b;
   carve(work, P, &b);
-  return b.rays;
+  return b.stats;
 }
 
 int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCamera& cam, uint32_t W, uint32_t H,
                     uint32_t row0, uint32_t row1, uint32_t spp, int max_depth, uint32_t seed, float* out, void* work,
-                    int num_sms, cudaStream_t st) {
+                    int num_sms, bool count_visits, cudaStream_t st) {
   const uint32_t P = W * (row1 - row0);
   SpecBuffers b;
   carve(work, P, &b);
@@ -245,15 +259,17 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
   const int persistent = num_sms * kTraceMinBlocks;
   const int shade = std::min(linear, num_sms * 16);
   int launches = 0;
-  cudaMemsetAsync(b.rays, 0, sizeof(unsigned long long), st);
+  cudaMemsetAsync(b.stats, 0, 6 * sizeof(unsigned long long), st);
   for (uint32_t k = 0; k < spp; ++k) {
     cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * 4 * (rounds + 1), st);
     k_sgen<<<linear, kBlock, 0, st>>>(b, cam, W, H, row0, P, k, seed);
     ++launches;
     for (uint32_t r = 0; r < rounds; ++r) {
-      k_sextend<<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      if (count_visits) k_sextend<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      else k_sextend<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
       k_sshade<<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth);
-      k_sshadow<<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      if (count_visits) k_sshadow<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      else k_sshadow<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
       launches += 3;
     }
     k_saccum<<<linear, kBlock, 0, st>>>(b, P, k + 1 == spp, 1.0f / (float)spp, out);

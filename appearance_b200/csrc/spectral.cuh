@@ -26,15 +26,18 @@ constexpr int kSpectralMaxDepth = 1000;
 
 // Device bytes of the work area for P = W x rows paths.
 size_t spectral_work_bytes(uint32_t P);
-// The 64-bit count of rays traced by the last launch_spectral on `work`.
-const unsigned long long* spectral_ray_counter(void* work, uint32_t P);
+// Counters of the last launch_spectral on `work` (device): closest-hit rays,
+// nodes, triangles; any-hit rays, nodes, triangles (nodes and triangles only
+// when it ran with count_visits).
+const unsigned long long* spectral_stats(void* work, uint32_t P);
 
 // Renders rows [row0, row1) of a W x H image at `spp` samples per pixel into
 // out (3 floats per pixel, row row0 first), with `work` of
 // spectral_work_bytes(W * (row1 - row0)) bytes; asynchronous on `st`.
-// Returns the number of kernels launched.
+// With count_visits the traversal kernels run in their instrumented form
+// (slower).  Returns the number of kernels launched.
 int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCamera& cam, uint32_t W, uint32_t H,
                     uint32_t row0, uint32_t row1, uint32_t spp, int max_depth, uint32_t seed, float* out, void* work,
-                    int num_sms, cudaStream_t st);
+                    int num_sms, bool count_visits, cudaStream_t st);
 
 }  // namespace ap

@@ -32,6 +32,7 @@ struct RayPre {
   float sx, sy, sz;
   float3 inv;          // box-test reciprocal direction (0 where the component is 0)
   uint32_t zero_axes;  // bit k: direction component k is +-0
+  uint32_t neg_axes;   // bit k: direction component k is negative (the far plane is entered first)
 };
 
 APD float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
@@ -57,6 +58,7 @@ APD RayPre ray_pre(float3 o, float3 d) {
   r.sz = 1.0f / dz;
   r.zero_axes = (d.x == 0.0f ? 1u : 0u) | (d.y == 0.0f ? 2u : 0u) | (d.z == 0.0f ? 4u : 0u);
   r.inv = f3(d.x == 0.0f ? 0.0f : 1.0f / d.x, d.y == 0.0f ? 0.0f : 1.0f / d.y, d.z == 0.0f ? 0.0f : 1.0f / d.z);
+  r.neg_axes = (r.inv.x < 0.0f ? 1u : 0u) | (r.inv.y < 0.0f ? 2u : 0u) | (r.inv.z < 0.0f ? 4u : 0u);
   return r;
 }
 
@@ -147,43 +149,69 @@ APD float byte_at(uint32_t word, int k) {
   return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
 }
 
+// A node's quantised child planes ordered by the ray's octant: per axis the
+// words (children 0-3, 4-7) of the plane the ray enters first (near) and the
+// one it leaves by (far).  With a negative direction component the larger
+// coordinate is reached first, so lo and hi swap; then near <= far holds per
+// child without a min/max (fma(q, a, b) is monotonic in q), and the values
+// are the ones min/max would pick.  Zero components (inv = 0) keep lo/hi.
+struct NodePlanes {
+  uint32_t nx[2], fx[2], ny[2], fy[2], nz[2], fz[2];
+};
+
+APD NodePlanes node_planes(const uint4 w2, const uint4 w3, const uint4 w4, uint32_t neg) {
+  NodePlanes p;
+  const bool sx = neg & 1u, sy = neg & 2u, sz = neg & 4u;
+  p.nx[0] = sx ? w3.z : w2.x;
+  p.nx[1] = sx ? w3.w : w2.y;
+  p.fx[0] = sx ? w2.x : w3.z;
+  p.fx[1] = sx ? w2.y : w3.w;
+  p.ny[0] = sy ? w4.x : w2.z;
+  p.ny[1] = sy ? w4.y : w2.w;
+  p.fy[0] = sy ? w2.z : w4.x;
+  p.fy[1] = sy ? w2.w : w4.y;
+  p.nz[0] = sz ? w4.z : w3.x;
+  p.nz[1] = sz ? w4.w : w3.y;
+  p.fz[0] = sz ? w3.x : w4.z;
+  p.fz[1] = sz ? w3.y : w4.w;
+  return p;
+}
+
+// Interval widening by a relative 2^-21 toward +-inf: x + |x| 2^-21 equals
+// x * (1 + 2^-21) for x >= 0 and x * (1 - 2^-21) for x < 0, in one fma.
+constexpr float kRelGrow = 4.76837158e-07f;  // 2^-21
+APD float grow_up(float x) { return fmaf(fabsf(x), kRelGrow, x); }
+APD float grow_down(float x) { return fmaf(-fabsf(x), kRelGrow, x); }
+
 // Entry distance of child i (a compile-time index after unrolling) or +inf
-// when its box is missed inside [tmin, tmax].
-APD float child_entry(const NodeFrame& f, const uint4 w2, const uint4 w3, const uint4 w4, const RayPre& r,
-                      int i, float tmin, float tmax) {
-  const int k = i & 3;
-  const uint32_t lox = i < 4 ? w2.x : w2.y, loy = i < 4 ? w2.z : w2.w;
-  const uint32_t loz = i < 4 ? w3.x : w3.y, hix = i < 4 ? w3.z : w3.w;
-  const uint32_t hiy = i < 4 ? w4.x : w4.y, hiz = i < 4 ? w4.z : w4.w;
-  float x0 = fmaf(byte_at(lox, k), f.ax, f.bx), x1 = fmaf(byte_at(hix, k), f.ax, f.bx);
-  float y0 = fmaf(byte_at(loy, k), f.ay, f.by), y1 = fmaf(byte_at(hiy, k), f.ay, f.by);
-  float z0 = fmaf(byte_at(loz, k), f.az, f.bz), z1 = fmaf(byte_at(hiz, k), f.az, f.bz);
-  float lx = fminf(x0, x1) - f.ex, hx = fmaxf(x0, x1) + f.ex;
-  float ly = fminf(y0, y1) - f.ey, hy = fmaxf(y0, y1) + f.ey;
-  float lz = fminf(z0, z1) - f.ez, hz = fmaxf(z0, z1) + f.ez;
+// when its box is missed inside [tmin, tmax]; tmax_grown = tmax * kGrow.
+APD float child_entry(const NodeFrame& f, const NodePlanes& pl, const RayPre& r, int i, float tmin,
+                      float tmax_grown) {
+  const int k = i & 3, h = i >> 2;
+  float lx = fmaf(byte_at(pl.nx[h], k), f.ax, f.bx) - f.ex, hx = fmaf(byte_at(pl.fx[h], k), f.ax, f.bx) + f.ex;
+  float ly = fmaf(byte_at(pl.ny[h], k), f.ay, f.by) - f.ey, hy = fmaf(byte_at(pl.fy[h], k), f.ay, f.by) + f.ey;
+  float lz = fmaf(byte_at(pl.nz[h], k), f.az, f.bz) - f.ez, hz = fmaf(byte_at(pl.fz[h], k), f.az, f.bz) + f.ez;
   if (r.zero_axes) {
     const float inf = __uint_as_float(0x7f800000u);
     if (r.zero_axes & 1u) {
-      bool in = r.o.x >= f.px + byte_at(lox, k) * f.sxs && r.o.x <= f.px + byte_at(hix, k) * f.sxs;
+      bool in = r.o.x >= f.px + byte_at(pl.nx[h], k) * f.sxs && r.o.x <= f.px + byte_at(pl.fx[h], k) * f.sxs;
       lx = in ? -inf : inf;
       hx = in ? inf : -inf;
     }
     if (r.zero_axes & 2u) {
-      bool in = r.o.y >= f.py + byte_at(loy, k) * f.sys && r.o.y <= f.py + byte_at(hiy, k) * f.sys;
+      bool in = r.o.y >= f.py + byte_at(pl.ny[h], k) * f.sys && r.o.y <= f.py + byte_at(pl.fy[h], k) * f.sys;
       ly = in ? -inf : inf;
       hy = in ? inf : -inf;
     }
     if (r.zero_axes & 4u) {
-      bool in = r.o.z >= f.pz + byte_at(loz, k) * f.szs && r.o.z <= f.pz + byte_at(hiz, k) * f.szs;
+      bool in = r.o.z >= f.pz + byte_at(pl.nz[h], k) * f.szs && r.o.z <= f.pz + byte_at(pl.fz[h], k) * f.szs;
       lz = in ? -inf : inf;
       hz = in ? inf : -inf;
     }
   }
-  float tn = fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin));
-  float tf = fminf(fminf(hx, hy), hz);
-  tf = tf * (tf > 0.0f ? kGrow : 1.0f / kGrow);
-  tn = tn * (tn > 0.0f ? 1.0f / kGrow : kGrow);
-  return (tn <= tf && tn <= tmax * kGrow) ? tn : __uint_as_float(0x7f800000u);
+  const float tn = grow_down(fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin)));
+  const float tf = grow_up(fminf(fminf(hx, hy), hz));
+  return (tn <= tf && tn <= tmax_grown) ? tn : __uint_as_float(0x7f800000u);
 }
 
 APD uint32_t meta_of(const uint4 w1, int i) { return ((i < 4 ? w1.z : w1.w) >> (8 * (i & 3))) & 0xffu; }
@@ -276,7 +304,8 @@ APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits*
     const uint4* np = s.nodes + 5 * (size_t)t.node;
     const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
     const NodeFrame f = node_frame(w0, t.r);
-    const float range = kAny ? t.tmax : t.hit.t;
+    const NodePlanes pl = node_planes(w2, w3, w4, t.r.neg_axes);
+    const float range_grown = (kAny ? t.tmax : t.hit.t) * kGrow;
     uint32_t tri_mask = 0;
     float best_t = __uint_as_float(0x7f800000u);
     uint32_t best_node = 0;
@@ -284,7 +313,7 @@ APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits*
     for (int i = 0; i < 8; ++i) {
       const uint32_t meta = meta_of(w1, i);
       if (meta == 0u) continue;
-      const float tn = child_entry(f, w2, w3, w4, t.r, i, 0.0f, range);
+      const float tn = child_entry(f, pl, t.r, i, 0.0f, range_grown);
       if (!(tn < __uint_as_float(0x7f800000u))) continue;
       if (meta & 0xe0u) {
         tri_mask |= (meta >> 5) << (meta & 0x1fu);  // unary count at the leaf's offset
@@ -337,44 +366,37 @@ APD uint32_t inline_children(const uint4 w0, const uint4 w2, const uint4 w3, con
   const float kSlack = 1.9073486e-06f;  // 2^-19
   float ex = (fabsf(bx) + 255.0f * fabsf(ax)) * kSlack, ey = (fabsf(by) + 255.0f * fabsf(ay)) * kSlack,
         ez = (fabsf(bz) + 255.0f * fabsf(az)) * kSlack;
-  const float grow = 1.0f + 4.8e-7f;
+  const NodePlanes pl = node_planes(w2, w3, w4, r.neg_axes);
+  const float tmax_grown = tmax * kGrow;
   uint32_t mask = 0;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    uint32_t lox = i < 4 ? w2.x : w2.y, loy = i < 4 ? w2.z : w2.w;
-    uint32_t loz = i < 4 ? w3.x : w3.y, hix = i < 4 ? w3.z : w3.w;
-    uint32_t hiy = i < 4 ? w4.x : w4.y, hiz = i < 4 ? w4.z : w4.w;
-    int k = i & 3;
-    float x0 = fmaf(byte_at(lox, k), ax, bx), x1 = fmaf(byte_at(hix, k), ax, bx);
-    float y0 = fmaf(byte_at(loy, k), ay, by), y1 = fmaf(byte_at(hiy, k), ay, by);
-    float z0 = fmaf(byte_at(loz, k), az, bz), z1 = fmaf(byte_at(hiz, k), az, bz);
-    float lx = fminf(x0, x1) - ex, hx = fmaxf(x0, x1) + ex;
-    float ly = fminf(y0, y1) - ey, hy = fmaxf(y0, y1) + ey;
-    float lz = fminf(z0, z1) - ez, hz = fmaxf(z0, z1) + ez;
+    const int k = i & 3, h = i >> 2;
+    float lx = fmaf(byte_at(pl.nx[h], k), ax, bx) - ex, hx = fmaf(byte_at(pl.fx[h], k), ax, bx) + ex;
+    float ly = fmaf(byte_at(pl.ny[h], k), ay, by) - ey, hy = fmaf(byte_at(pl.fy[h], k), ay, by) + ey;
+    float lz = fmaf(byte_at(pl.nz[h], k), az, bz) - ez, hz = fmaf(byte_at(pl.fz[h], k), az, bz) + ez;
     if (r.zero_axes) {
       const float inf = __uint_as_float(0x7f800000u);
       if (r.zero_axes & 1u) {
-        bool in = r.o.x >= px + byte_at(lox, k) * sxs && r.o.x <= px + byte_at(hix, k) * sxs;
+        bool in = r.o.x >= px + byte_at(pl.nx[h], k) * sxs && r.o.x <= px + byte_at(pl.fx[h], k) * sxs;
         lx = in ? -inf : inf;
         hx = in ? inf : -inf;
       }
       if (r.zero_axes & 2u) {
-        bool in = r.o.y >= py + byte_at(loy, k) * sys && r.o.y <= py + byte_at(hiy, k) * sys;
+        bool in = r.o.y >= py + byte_at(pl.ny[h], k) * sys && r.o.y <= py + byte_at(pl.fy[h], k) * sys;
         ly = in ? -inf : inf;
         hy = in ? inf : -inf;
       }
       if (r.zero_axes & 4u) {
-        bool in = r.o.z >= pz + byte_at(loz, k) * szs && r.o.z <= pz + byte_at(hiz, k) * szs;
+        bool in = r.o.z >= pz + byte_at(pl.nz[h], k) * szs && r.o.z <= pz + byte_at(pl.fz[h], k) * szs;
         lz = in ? -inf : inf;
         hz = in ? inf : -inf;
       }
     }
-    float tn = fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin));
-    float tf = fminf(fminf(hx, hy), hz);
-    tf = tf * (tf > 0.0f ? grow : 1.0f / grow);
-    tn = tn * (tn > 0.0f ? 1.0f / grow : grow);
+    const float tn = grow_down(fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin)));
+    const float tf = grow_up(fminf(fminf(hx, hy), hz));
     tnear[i] = tn;
-    if (tn <= tf && tn <= tmax * grow) mask |= 1u << i;
+    if (tn <= tf && tn <= tmax_grown) mask |= 1u << i;
   }
   return mask;
 }

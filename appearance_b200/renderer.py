@@ -222,6 +222,18 @@ class PathTracer:
                                                  ctypes.byref(self.last_stats)))
         return out
 
+    def profile_spectral(self, resolution, spp: int = 1, max_depth: int = 4, seed: int = 0, start_row: int = 0,
+                         end_row: int | None = None) -> dict:
+        """render_spectral with instrumented traversal: rays, nodes and triangles
+        of the closest-hit and the shadow rays (times not representative)."""
+        w, h = int(resolution[0]), int(resolution[1])
+        end_row = h if end_row is None else end_row
+        v = np.zeros(6, np.uint64)
+        self._check(self._lib.ap_profile_spectral(self._h, w, h, start_row, end_row, spp, max_depth, seed, _ptr(v),
+                                                  ctypes.byref(self.last_stats)))
+        return {"closest": dict(rays=int(v[0]), nodes=int(v[1]), tris=int(v[2])),
+                "any": dict(rays=int(v[3]), nodes=int(v[4]), tris=int(v[5]))}
+
     def bvh_stats(self) -> dict:
         out = np.zeros(8, np.uint32)
         self._check(self._lib.ap_bvh_stats(self._h, _ptr(out)))

@@ -77,6 +77,19 @@ def measure(lots=64, size=4096, spp=64, depth=16, band=4096, repeats=1, quality=
                        f"depth {depth}, 4 wavelengths, wavefront in bands of {band} rows",
            "kernel_launches_per_band": runs[0][2], "scene_gen_s": gen_s, "upload_and_bvh_s": upload_s,
            "bvh": pt.bvh_stats()}
+    # traversal work per ray from the instrumented kernels on one sample per pixel
+    v = pt.profile_spectral((size, size), spp=1, max_depth=depth, seed=100)
+    trav = {}
+    total_bytes = 0.0
+    for kind in ("closest", "any"):
+        r = max(v[kind]["rays"], 1)
+        n, t = v[kind]["nodes"] / r, v[kind]["tris"] / r
+        b = 48.0 + 80.0 * n + 36.0 * t  # ray 32 + hit 16, 80 B per node, 36 B per triangle
+        trav[kind] = {"nodes_per_ray": n, "tris_per_ray": t, "bytes_per_ray": b,
+                      "ray_share": v[kind]["rays"] / max(v["closest"]["rays"] + v["any"]["rays"], 1)}
+        total_bytes += b * trav[kind]["ray_share"]
+    trav["algorithmic_gbs_over_image_time"] = total_bytes * rays / (ms * 1e-3) / 1e9
+    res["traversal"] = trav
     c0, c1 = size // 2 - size // 8, size // 2 + size // 8  # centre crop rows/cols (1024 of 4096)
     if quality:
         img, _, _ = render_bands(pt, size, spp, depth, 100, band, to_host=True)

@@ -234,6 +234,12 @@ int ap_spectral_setup(void* handle, const float* sun_dir3, const float* sun_rgb3
  * and stats->extension_rays the rays it traced (closest and shadow). */
 int ap_render_spectral(void* handle, uint32_t w, uint32_t h, uint32_t row_start, uint32_t row_end, uint32_t spp,
                        uint32_t max_depth, uint32_t seed, float* out_rgb, size_t out_bytes, ap_frame_stats* stats);
+/* ap_render_spectral (image kept on the device) with the traversal kernels in
+ * their instrumented form: visits6 receives closest-hit rays, nodes visited,
+ * triangles tested, then the same for the any-hit (shadow) rays.  Times are
+ * not representative.  It has no counterpart in the reference. */
+int ap_profile_spectral(void* handle, uint32_t w, uint32_t h, uint32_t row_start, uint32_t row_end, uint32_t spp,
+                        uint32_t max_depth, uint32_t seed, uint64_t* visits6, ap_frame_stats* stats);
 
 /* ---- render-serving loop ------------------------------------------------
  * No reference counterpart as an API: it takes the role of the reference's

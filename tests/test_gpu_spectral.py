@@ -68,8 +68,14 @@ def test_spectral_device_only_and_errors():
     assert pt.render_spectral((32, 32), spp=4, to_host=False) is None
     assert pt.last_stats.gpu_ms > 0.0
     a = pt.render_spectral((32, 32), spp=4, seed=1)
+    rays = pt.last_stats.extension_rays
     b = pt.render_spectral((32, 32), spp=4, seed=1)
     assert_bits(a, b, "repeat")
+    # the instrumented kernels trace the same rays
+    v = pt.profile_spectral((32, 32), spp=4, seed=1)
+    assert v["closest"]["rays"] + v["any"]["rays"] == rays
+    assert v["closest"]["rays"] >= 32 * 32 * 4 and v["closest"]["nodes"] >= v["closest"]["rays"]
+    assert v["closest"]["tris"] > 0
     with pytest.raises(RendererError):
         pt.render_spectral((32, 32), spp=0)
     with pytest.raises(RendererError):
