@@ -181,6 +181,18 @@ DM_HD float pow_(float x, float y) {
   return exp_(y * log_(x));
 }
 
+// x^128 for x >= 0 as seven squarings: the a-trous normal weight's exponent
+// (PHI_NORMAL = 128, svgf_atrous.wgsl) is a power of two.
+DM_HD float pow128(float x) {
+  x = x * x;
+  x = x * x;
+  x = x * x;
+  x = x * x;
+  x = x * x;
+  x = x * x;
+  return x * x;
+}
+
 // ---- atan2 -----------------------------------------------------------------
 DM_HD float atan_unit(float t) {  // t in [0, 1]
   const float TAN_PI_8 = 0.414213562373095048802f;

@@ -1670,72 +1670,102 @@ __global__ void k_svgf_temporal(FrameBuffers fb, Consts c, const uint32_t* demod
   fb.svgf_count[id] = count;
 }
 
-// svgf_atrous.wgsl:48-117.  A 16x16 block stages radiance, variance, normal
-// and depth of its tile plus a halo of 2*step pixels in shared memory when the
-// halo is small (steps 1, 2, 4); larger steps read through L1/L2.
+// The a-trous passes' per-pixel inputs, unpacked once per frame: normal and
+// depth (constant over the passes) and the first pass's radiance with its luma.
+__global__ void k_atrous_prep(FrameBuffers fb, uint32_t P, uint32_t cur, const uint32_t* in_rad) {
+  const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= P) return;
+  const float3 n = unpack_oct30(fb.gb_b[cur][id].x);
+  fb.atr_nd[id] = make_float4(n.x, n.y, n.z, __uint_as_float(fb.gb_a[cur][id].w));
+  const float3 r = unpack_rgb9e5(in_rad[id]);
+  fb.atr_rad[0][id] = make_float4(r.x, r.y, r.z, luma(r));
+}
+
+// svgf_atrous.wgsl:48-117.  Inputs come unpacked (k_atrous_prep and the
+// previous pass): radiance + luma and normal + depth as float4, variance.  A
+// 16x16 block stages its tile plus a halo of 2*step pixels in shared memory
+// when the halo is small (steps 1, 2, 4); larger steps read through L1/L2.
+// The two exponential weights are one exp of the summed exponents with the
+// divisions as products by reciprocals, and pow(., 128) is seven squarings
+// (the oracle evaluates the same expressions).  Each pass writes its packed
+// radiance (RGB9E5, as the reference stores it) and, for the next pass, the
+// unpacked value of that packed radiance with its luma.
 constexpr int kAtrousTile = 16;
 template <int STEP>
-__global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t cur,
-                                                uint32_t pass_idx, const uint32_t* in_rad, uint32_t* out_rad,
+__global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t pass_idx,
+                                                const float4* in_rad4, float4* out_rad4, uint32_t* out_rad,
                                                 const float* in_var, float* out_var) {
   constexpr int HALO = 2 * STEP;
   constexpr int SW = kAtrousTile + 2 * HALO;
   constexpr bool kShared = STEP <= 4;
-  __shared__ uint4 s_px[kShared ? SW * SW : 1];  // radiance, variance bits, normal, depth bits
+  __shared__ float4 s_rad[kShared ? SW * SW : 1];
+  __shared__ float4 s_nd[kShared ? SW * SW : 1];
+  __shared__ float s_var[kShared ? SW * SW : 1];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int x0 = blockIdx.x * kAtrousTile, y0 = blockIdx.y * kAtrousTile;
-  const uint4* ga = fb.gb_a[cur];
-  const uint4* gbb = fb.gb_b[cur];
+  const float4* nd = fb.atr_nd;
   if (kShared) {
     for (int k = ty * kAtrousTile + tx; k < SW * SW; k += kAtrousTile * kAtrousTile) {
       int sx = x0 - HALO + (k % SW), sy = y0 - HALO + (k / SW);
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f), n = r;
+      float v = 0.0f;
       if (sx >= 0 && sy >= 0 && sx < (int)W && sy < (int)H) {
         uint32_t sid = (uint32_t)sy * W + (uint32_t)sx;
-        v = make_uint4(in_rad[sid], __float_as_uint(in_var[sid]), gbb[sid].x, ga[sid].w);
+        r = in_rad4[sid];
+        n = nd[sid];
+        v = in_var[sid];
       }
-      s_px[k] = v;
+      s_rad[k] = r;
+      s_nd[k] = n;
+      s_var[k] = v;
     }
     __syncthreads();
   }
   int x = x0 + tx, y = y0 + ty;
   if (x >= (int)W || y >= (int)H) return;
   uint32_t id = (uint32_t)y * W + (uint32_t)x;
-  auto fetch = [&](int px, int py) -> uint4 {
-    if (kShared) return s_px[(py - y0 + HALO) * SW + (px - x0 + HALO)];
-    uint32_t sid = (uint32_t)py * W + (uint32_t)px;
-    return make_uint4(in_rad[sid], __float_as_uint(in_var[sid]), gbb[sid].x, ga[sid].w);
-  };
-  uint4 cpx = fetch(x, y);
-  float cdepth = __uint_as_float(cpx.w);
+  auto slot = [&](int px, int py) { return (py - y0 + HALO) * SW + (px - x0 + HALO); };
+  const float4 cnd = kShared ? s_nd[slot(x, y)] : nd[id];
+  const float cdepth = cnd.w;
   if (cdepth == 0.0f) return;
-  float3 cn = unpack_oct30(cpx.z);
+  const float3 cn = f3(cnd.x, cnd.y, cnd.z);
+  const float4 crad = kShared ? s_rad[slot(x, y)] : in_rad4[id];
   const float KW[3] = {3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
-  float3 rsum = unpack_rgb9e5(cpx.x);
-  float vsum = __uint_as_float(cpx.y);
+  float3 rsum = f3(crad.x, crad.y, crad.z);
+  float vsum = kShared ? s_var[slot(x, y)] : in_var[id];
   float wsum = 1.0f;
-  float cl = luma(rsum);
-  float cv = vsum;
-  float lum_den = dm::fmax(4.0f * dm::sqrt_(cv), 1e-8f);
+  const float cl = crad.w;
+  const float cv = vsum;
+  const float inv_lum = 1.0f / dm::fmax(4.0f * dm::sqrt_(cv), 1e-8f);
+  const float depth_k = 1.0f / (2.0f * sqr(0.1f));
+#pragma unroll
   for (int dy = -2; dy <= 2; ++dy)
+#pragma unroll
     for (int dx = -2; dx <= 2; ++dx) {
       if (dy == 0 && dx == 0) continue;
       int sx = x + dx * STEP, sy = y + dy * STEP;
       if (sx < 0 || sy < 0 || sx >= (int)W || sy >= (int)H) continue;
-      uint4 spx = fetch(sx, sy);
-      float sdepth = __uint_as_float(spx.w);
-      if (sdepth == 0.0f) continue;
-      float3 srad = unpack_rgb9e5(spx.x);
-      float sl = luma(srad);
-      float nw = dm::pow_(dm::fmax(dot(cn, unpack_oct30(spx.z)), 0.0f), 128.0f);
-      float dd = dm::fabs_(cdepth - sdepth);
-      float dw = dm::exp_(-sqr(dd) / (2.0f * sqr(0.1f)));
-      float ld = dm::fabs_(cl - sl);
-      float lw = dm::exp_(-ld / lum_den);
-      float w = nw * dw * lw;
+      float4 snd, srad;
+      float svar;
+      if (kShared) {
+        const int k = slot(sx, sy);
+        snd = s_nd[k];
+        srad = s_rad[k];
+        svar = s_var[k];
+      } else {
+        const uint32_t sid = (uint32_t)sy * W + (uint32_t)sx;
+        snd = nd[sid];
+        srad = in_rad4[sid];
+        svar = in_var[sid];
+      }
+      if (snd.w == 0.0f) continue;
+      float nw = dm::pow128(dm::fmax(dot(cn, f3(snd.x, snd.y, snd.z)), 0.0f));
+      float dd = dm::fabs_(cdepth - snd.w);
+      float ld = dm::fabs_(cl - srad.w);
+      float w = nw * dm::exp_(-(sqr(dd) * depth_k) - ld * inv_lum);
       w = w * (KW[dx < 0 ? -dx : dx] * KW[dy < 0 ? -dy : dy]);
-      rsum = rsum + srad * w;
-      vsum = vsum + __uint_as_float(spx.y) * sqr(w);
+      rsum = rsum + f3(srad.x, srad.y, srad.z) * w;
+      vsum = vsum + svar * sqr(w);
       wsum = wsum + w;
     }
   rsum = rsum / wsum;
@@ -1743,6 +1773,8 @@ __global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uin
   uint32_t packed = pack_rgb9e5(rsum);
   out_rad[id] = packed;
   out_var[id] = vsum;
+  const float3 q = unpack_rgb9e5(packed);
+  out_rad4[id] = make_float4(q.x, q.y, q.z, luma(q));
   if (pass_idx == 0) fb.svgf_hist[id] = packed;
 }
 
@@ -1991,6 +2023,9 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
   fb->st_d = carve<uint4>(p, P);
   fb->counters = carve<uint32_t>(p, 64);
   fb->visits = carve<unsigned long long>(p, 3 * K_NUM_KINDS);
+  fb->atr_nd = fb->rq_o[0];
+  fb->atr_rad[0] = fb->rq_d[0];
+  fb->atr_rad[1] = fb->rq_o[1];
   fb->out_rgb = carve<float>(p, 3 * P);
   fb->accum = carve<float4>(p, P);
   fb->rgba = carve<uint32_t>(p, P);
@@ -2019,7 +2054,7 @@ const char* kernel_kind_name(int k) {
                                            "gi_temporal", "gi_spatial", "apply_di", "apply_gi", "demodulate",
                                            "firefly", "svgf_temporal", "atrous", "taa", "resolve", "copy",
                                            "trace_closest", "trace_any", "shade_b", "shade_c", "shade_d", "shade_b2", "rc",
-                                           "rc_infer", "rc_train"};
+                                           "rc_infer", "rc_train", "atrous_prep"};
   return (k >= 0 && k < K_NUM_KINDS) ? names[k] : "?";
 }
 
@@ -2259,21 +2294,26 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
     k_svgf_temporal<<<g2, b2, 0, st>>>(fb, c, dcur, fb.svgf_rad[(f + 1) % 2], fb.svgf_mom[f % 2],
                                        fb.svgf_mom[(f + 1) % 2], fb.svgf_var[(f + 1) % 2]);
     mark(K_SVGF_TEMPORAL);
+    if (cfg.svgf_atrous_passes > 0) {
+      k_atrous_prep<<<lb, 256, 0, st>>>(fb, P, cur, fb.svgf_rad[(f + 1) % 2]);
+      mark(K_ATROUS_PREP);
+    }
     for (uint32_t i = 0; i < cfg.svgf_atrous_passes; ++i) {
-      const uint32_t* in_rad = fb.svgf_rad[(f + 1 + i) % 2];
+      const float4* in4 = fb.atr_rad[i & 1u];
+      float4* out4 = fb.atr_rad[(i + 1) & 1u];
       uint32_t* out_rad = fb.svgf_rad[(f + i) % 2];
       const float* in_var = fb.svgf_var[(f + 1 + i) % 2];
       float* out_var = fb.svgf_var[(f + i) % 2];
       dim3 bt(kAtrousTile, kAtrousTile), gt((W + kAtrousTile - 1) / kAtrousTile, (H + kAtrousTile - 1) / kAtrousTile);
       switch (i) {
-        case 0: k_atrous<1><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
-        case 1: k_atrous<2><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
-        case 2: k_atrous<4><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
-        case 3: k_atrous<8><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
-        case 4: k_atrous<16><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
-        case 5: k_atrous<32><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
-        case 6: k_atrous<64><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
-        default: k_atrous<128><<<gt, bt, 0, st>>>(fb, W, H, cur, i, in_rad, out_rad, in_var, out_var); break;
+        case 0: k_atrous<1><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
+        case 1: k_atrous<2><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
+        case 2: k_atrous<4><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
+        case 3: k_atrous<8><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
+        case 4: k_atrous<16><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
+        case 5: k_atrous<32><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
+        case 6: k_atrous<64><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
+        default: k_atrous<128><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
       }
       mark(K_ATROUS);
       if (i == cfg.svgf_atrous_passes - 1) {

@@ -56,6 +56,10 @@ struct FrameBuffers {
   uint32_t* counters;  // [0..1] path queue sizes, [2] extend cursor, [3] rays traced,
                        // [4..8] ray queue sizes, [9..13] ray queue cursors
   unsigned long long* visits;  // instrumented traversal: per kernel kind {rays, nodes, tris}
+  // a-trous inputs unpacked once: normal + depth per pixel, radiance + luma
+  // (ping-pong); aliases of ray-queue storage, idle after the bounce loop
+  float4* atr_nd;
+  float4* atr_rad[2];
   float* out_rgb;      // linear HDR output, 3 floats per pixel (device)
   float4* accum;       // display accumulation (resolve.wgsl accum_radiance)
   uint32_t* rgba;      // RGBA8 display texture, 64x64-block swizzled
@@ -81,7 +85,7 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb);
 enum KernelKind : int {
   K_MEMSET = 0, K_RAYGEN, K_EXTEND, K_SHADE, K_DI_TEMPORAL, K_DI_SPATIAL, K_GI_TEMPORAL, K_GI_SPATIAL,
   K_APPLY_DI, K_APPLY_GI, K_DEMODULATE, K_FIREFLY, K_SVGF_TEMPORAL, K_ATROUS, K_TAA, K_RESOLVE, K_COPY,
-  K_TRACE_CLOSEST, K_TRACE_ANY, K_SHADE_B, K_SHADE_C, K_SHADE_D, K_SHADE_B2, K_RC, K_RC_INFER, K_RC_TRAIN, K_NUM_KINDS
+  K_TRACE_CLOSEST, K_TRACE_ANY, K_SHADE_B, K_SHADE_C, K_SHADE_D, K_SHADE_B2, K_RC, K_RC_INFER, K_RC_TRAIN, K_ATROUS_PREP, K_NUM_KINDS
 };
 const char* kernel_kind_name(int k);
 

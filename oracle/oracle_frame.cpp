@@ -915,6 +915,11 @@ struct Frame {
         float wsum = 1.0f;
         float cl = luma(rsum);
         float cv = vsum;
+        // exp(-dd^2 / (2 phi_d^2)) * exp(-ld / max(phi_l sqrt(var), 1e-8)) as one
+        // exp of the summed exponents, each division as a product with its
+        // reciprocal; pow(., 128) as seven squarings
+        const float inv_lum = 1.0f / dm::fmax(4.0f * dm::sqrt_(cv), 1e-8f);
+        const float depth_k = 1.0f / (2.0f * sqr(0.1f));
         for (int dy = -2; dy <= 2; ++dy)
           for (int dx = -2; dx <= 2; ++dx) {
             if (dy == 0 && dx == 0) continue;
@@ -925,12 +930,10 @@ struct Frame {
             if (gt_is_sky(sg.depth)) continue;
             V3 srad = rgb9e5_unpack(in_rad[sid]);
             float sl = luma(srad);
-            float nw = dm::pow_(dm::fmax(dot(cur.n, sg.n), 0.0f), 128.0f);
+            float nw = dm::pow128(dm::fmax(dot(cur.n, sg.n), 0.0f));
             float dd = dm::fabs_(cur.depth - sg.depth);
-            float dw = dm::exp_(-sqr(dd) / (2.0f * sqr(0.1f)));
             float ld = dm::fabs_(cl - sl);
-            float lw = dm::exp_(-ld / (dm::fmax(4.0f * dm::sqrt_(cv), 1e-8f)));
-            float w = nw * dw * lw;
+            float w = nw * dm::exp_(-(sqr(dd) * depth_k) - ld * inv_lum);
             w = w * (KW[dx < 0 ? -dx : dx] * KW[dy < 0 ? -dy : dy]);
             rsum = rsum + srad * w;
             vsum = vsum + in_var[sid] * sqr(w);
