@@ -319,14 +319,7 @@ APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits*
         tri_mask |= (meta >> 5) << (meta & 0x1fu);  // unary count at the leaf's offset
       } else {
         const uint32_t child = w1.x + (meta & 7u);
-        if (kAny) {
-          if (!t.have) {
-            t.node = child;
-            t.have = true;
-          } else if (t.sp < kTraversalStack) {
-            stack[t.sp++] = make_uint2(child, 0u);
-          }
-        } else if (tn < best_t) {
+        if (tn < best_t) {  // nearest child next (any hit too: occluders near the origin are found sooner)
           if (t.have && t.sp < kTraversalStack) stack[t.sp++] = make_uint2(best_node, __float_as_uint(best_t));
           best_t = tn;
           best_node = child;
@@ -336,10 +329,8 @@ APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits*
         }
       }
     }
-    if (!kAny) {
-      t.node = best_node;
-      t.node_t = best_t;
-    }
+    t.node = best_node;
+    t.node_t = best_t;
     t.tri_base = w1.y;
     t.tri_mask = tri_mask;
   }

@@ -26,6 +26,25 @@ def test_icosphere_field_counts():
     assert np.array_equal(sc.positions, again.positions)
 
 
+def test_city_counts_and_layout():
+    sc = scenes.city(seed=0, lots=8, extent=250.0, num_emissive_tris=200, env_size=(64, 32))
+    per_building = 12 + 2 * 4 * 16 * 19  # box + two triangles per window, 16 x 19 windows per facade
+    assert per_building == 2444
+    assert sc.num_tris == 64 * per_building + 2
+    emissive = sc.meshes[sc.meshes[:, 5] == 1]
+    assert int(emissive[:, 3].sum()) // 3 == 200
+    for m in emissive:  # emitters: radiance U[1, 20] x (1, 0.8, 0.55)
+        r = sc.materials[m[4]][5:8]
+        assert 1.0 <= r[0] <= 20.0 and np.isclose(r[1], 0.8 * r[0]) and np.isclose(r[2], 0.55 * r[0])
+    # buildings stay inside their lots and under 200 m
+    lo, hi = sc.positions.min(0), sc.positions.max(0)
+    assert hi[1] <= 200.0 + 1e-3 and lo[1] >= -1e-3
+    assert np.all(np.abs(sc.positions[:, [0, 2]]) <= 0.55 * 250.0 + 1e-3)
+    assert np.allclose(np.linalg.norm(sc.normals, axis=1), 1.0, atol=1e-5)
+    again = scenes.city(seed=0, lots=8, extent=250.0, num_emissive_tris=200, env_size=(64, 32))
+    assert np.array_equal(sc.positions, again.positions)
+
+
 def test_sky_env_peak():
     env = scenes.sky_env(256, 128, sun_sigma=0.05)
     assert env.shape == (128, 256, 3)
