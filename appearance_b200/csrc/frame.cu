@@ -322,7 +322,10 @@ APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& f
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade_a(DevScene s, FrameBuffers fb, Consts c, Mats mats) {
+#ifndef AP_SHADE_A_MIN_BLOCKS
+#define AP_SHADE_A_MIN_BLOCKS 8  // resident blocks per SM the kernel is register-capped for (measured)
+#endif
+__global__ void __launch_bounds__(kBlock, AP_SHADE_A_MIN_BLOCKS) k_shade_a(DevScene s, FrameBuffers fb, Consts c, Mats mats) {
   __shared__ uint4 s_lights[kSmemLights];
   const uint4* lights = stage_lights(s, s_lights);
   const uint32_t count = bounce_count(fb, c);
@@ -411,7 +414,10 @@ __global__ void __launch_bounds__(kBlock) k_shade_a(DevScene s, FrameBuffers fb,
 
 // Stage B1: resampled importance sampling of the direct light (Nee::sample_ris,
 // nee.wgsl:122-237) and its shadow ray.
-__global__ void __launch_bounds__(kBlock, 4) k_shade_b(DevScene s, FrameBuffers fb, Consts c) {
+#ifndef AP_SHADE_B_MIN_BLOCKS
+#define AP_SHADE_B_MIN_BLOCKS 8  // resident blocks per SM the RIS stage is register-capped for (measured)
+#endif
+__global__ void __launch_bounds__(kBlock, AP_SHADE_B_MIN_BLOCKS) k_shade_b(DevScene s, FrameBuffers fb, Consts c) {
   __shared__ uint4 s_lights[kSmemLights];
   const uint4* lights = stage_lights(s, s_lights);
   const uint32_t count = bounce_count(fb, c);
@@ -584,7 +590,10 @@ APD void finish_gi(const FrameBuffers& fb, uint32_t id, float3 contribution, flo
   fb.gi_b[id] = gi_pack_b(res);
 }
 
-__global__ void __launch_bounds__(kBlock) k_shade_c(DevScene s, FrameBuffers fb, Consts c) {
+#ifndef AP_SHADE_C_MIN_BLOCKS
+#define AP_SHADE_C_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(kBlock, AP_SHADE_C_MIN_BLOCKS) k_shade_c(DevScene s, FrameBuffers fb, Consts c) {
   const uint32_t count = bounce_count(fb, c);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     uint32_t id = bounce_path(fb, c, i);
@@ -1339,7 +1348,10 @@ enum : uint32_t {
   SP_MEMO = 32u,     // st_b/st_c.x hold a memoised target
 };
 
-__global__ void __launch_bounds__(256) k_dsp_ca(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
+#ifndef AP_DSP_MIN_BLOCKS
+#define AP_DSP_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_dsp_ca(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
                                                 uint32_t pass_count, uint32_t nsamples, uint32_t i,
                                                 const uint4* in_a, const uint4* in_b, uint4* out_a, uint4* out_b,
                                                 uint4* prev_a, uint4* prev_b) {
@@ -1415,7 +1427,7 @@ __global__ void __launch_bounds__(256) k_dsp_ca(DevScene s, FrameBuffers fb, Con
   push_ray(fb, Q_DI_SHADOW, ph.ray, ph.o, ph.tmax, ph.d, id);
 }
 
-__global__ void __launch_bounds__(256) k_dsp_b(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
+__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_dsp_b(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
                                                uint32_t pass_count, const uint4* in_a, const uint4* in_b,
                                                uint4* out_a, uint4* out_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;

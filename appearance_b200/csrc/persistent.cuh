@@ -20,8 +20,14 @@ APD uint32_t lane_id() {
 // store(i, trav, visits) writes its result.  The traversal kernels run with
 // the child tests unrolled and are register-capped for 6 resident blocks of
 // kBlock threads per SM (the best of the measured 1..8 on the benchmark scene).
-constexpr int kStepBudget = 8;
-constexpr int kTraceMinBlocks = 6;
+#ifndef AP_TRACE_MIN_BLOCKS
+#define AP_TRACE_MIN_BLOCKS 6
+#endif
+#ifndef AP_STEP_BUDGET
+#define AP_STEP_BUDGET 8
+#endif
+constexpr int kStepBudget = AP_STEP_BUDGET;
+constexpr int kTraceMinBlocks = AP_TRACE_MIN_BLOCKS;
 
 template <bool kAny, bool kCount, class Load, class Store>
 APD void persistent_trace(const DevScene& s, uint32_t count, uint32_t* cursor, Load load, Store store) {
