@@ -123,13 +123,20 @@ class PathTracer:
         return vp
 
     # -- rendering
-    def render(self, resolution, start_row: int = 0, end_row: int | None = None, result_callback=None) -> np.ndarray:
+    def render(self, resolution, start_row: int = 0, end_row: int | None = None, result_callback=None,
+               out: np.ndarray | None = None) -> np.ndarray:
         """NodeRenderer::render: linear HDR RGB f32 rows [start_row, end_row) of a
         resolution=(width, height) frame.  The callback, when given, receives the
-        rows as bytes (the reference passes &[u8]) and the array is returned."""
+        rows as bytes (the reference passes &[u8]) and the array is returned.
+        `out` (C-contiguous float32 of shape (rows, width, 3)) is filled instead
+        of a new array; a page-locked one (e.g. from torch's pin_memory) makes
+        the device-to-host copy run at full PCIe/C2C speed."""
         w, h = int(resolution[0]), int(resolution[1])
         end_row = h if end_row is None else end_row
-        out = np.empty((end_row - start_row, w, 3), np.float32)
+        if out is None:
+            out = np.empty((max(0, end_row - start_row), w, 3), np.float32)
+        elif out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"] or out.shape != (end_row - start_row, w, 3):
+            raise ValueError("out must be C-contiguous float32 of shape (rows, width, 3)")
         self._check(self._lib.ap_render_hdr(self._h, w, h, start_row, end_row, _ptr(out), out.nbytes,
                                             ctypes.byref(self.last_stats)))
         if result_callback is not None:

@@ -144,3 +144,28 @@ def test_rgba8_display_output_matches_oracle(accumulate):
         assert np.array_equal(img, ref)
     part = pt.render_rgba8((w, h), start_row=32, end_row=80, accumulate=accumulate)
     assert part.shape == (48, w, 4)
+
+
+def test_render_into_caller_buffer():
+    sc = scenes.cornell_box()
+    cam = scenes.cornell_camera()
+    w, h = 40, 24
+    mats, _ = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], cam["near"], cam["far"], w, h)
+    a = PathTracer(presets.PLAIN)
+    a.upload_scene(sc)
+    a.set_camera_matrices(mats)
+    b = PathTracer(presets.PLAIN)
+    b.upload_scene(sc)
+    b.set_camera_matrices(mats)
+    import torch
+    out = torch.empty((h, w, 3), dtype=torch.float32, pin_memory=True).numpy()
+    ref = a.render((w, h))
+    got = b.render((w, h), out=out)
+    assert got is out
+    assert_bits(out, ref, "pinned caller buffer")
+    part = np.zeros((7, w, 3), np.float32)
+    b.set_camera_matrices(mats)
+    with pytest.raises(ValueError):
+        b.render((w, h), 3, 12, out=part)
+    a.close()
+    b.close()
