@@ -125,6 +125,24 @@ int upload(Handle* h, void** dst, const T* src, size_t count) {
   return rc;
 }
 
+__global__ void k_sun_derive(SunDev* s) { sun_derive(*s); }
+
+// The sun's derived fields, computed on the device like every other use of
+// the sun functions' arithmetic (run once per scene upload).
+int derive_sun(Handle* h, SunDev* sun) {
+  void* d = nullptr;
+  int rc = check_cuda(h, cudaMalloc(&d, sizeof(SunDev)), "sun");
+  if (rc) return rc;
+  rc = check_cuda(h, cudaMemcpy(d, sun, sizeof(SunDev), cudaMemcpyHostToDevice), "sun");
+  if (!rc) {
+    k_sun_derive<<<1, 1, 0, h->stream>>>(static_cast<SunDev*>(d));
+    rc = check_cuda(h, cudaStreamSynchronize(h->stream), "sun derive");
+  }
+  if (!rc) rc = check_cuda(h, cudaMemcpy(sun, d, sizeof(SunDev), cudaMemcpyDeviceToHost), "sun");
+  cudaFree(d);
+  return rc;
+}
+
 // Fills the emissive-triangle table (run once per scene upload).
 __global__ void k_build_emissive_tris(DevScene s, EmissiveTri* out, uint32_t total) {
   uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -585,7 +603,12 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
   v.env = static_cast<const float*>(s.env);
   v.env_w = s.env ? d->env_w : 0;
   v.env_h = s.env ? d->env_h : 0;
-  std::memcpy(&v.sun, d->sun, sizeof(SunDev));
+  std::memset(&v.sun, 0, sizeof(SunDev));
+  std::memcpy(&v.sun, d->sun, 8 * sizeof(float));  // direction, size, color, intensity
+  if ((rc = derive_sun(h, &v.sun))) {
+    s.release();
+    return rc;
+  }
   v.num_tris = d->num_tris;
   v.emissive_tri_base = static_cast<const uint32_t*>(s.emissive_tri_base);
   v.emissive_info = static_cast<const uint4*>(s.emissive_info);

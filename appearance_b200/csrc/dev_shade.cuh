@@ -479,37 +479,41 @@ APD float3 perpendicular(float3 u) {
   return cross(u, f3((float)xm, (float)ym, (float)zm));
 }
 APD float3 sun_dir(const SunDev& s) { return ld3(s.direction); }
-APD float sun_intensity(const SunDev& s, float3 direction) {
+// The per-scene part of the sun functions, evaluated once (k_sun_derive).
+APD void sun_derive(SunDev& s) {
   const float cutoff = kPi / 1.95f;
   float3 l = -sun_dir(s);
   float zc = dot(l, f3(0.0f, 1.0f, 0.0f));
-  float it = s.intensity * dm::fmax(0.0f, 1.0f - dm::exp_(-((cutoff - dm::acos_(zc)) / 1.4f)));
-  float ct = dot(direction, l);
-  float dc = dm::cos_(s.size * 0.1f);
-  return it * (ct > dc ? 1.0f : 0.0f);
+  s.it = s.intensity * dm::fmax(0.0f, 1.0f - dm::exp_(-((cutoff - dm::acos_(zc)) / 1.4f)));
+  s.cos_size = dm::cos_(s.size * 0.1f);
+  float3 bt = perpendicular(l);
+  float3 tg = cross(bt, l);
+  s.l[0] = l.x; s.l[1] = l.y; s.l[2] = l.z;
+  s.bt[0] = bt.x; s.bt[1] = bt.y; s.bt[2] = bt.z;
+  s.tg[0] = tg.x; s.tg[1] = tg.y; s.tg[2] = tg.z;
+}
+APD float sun_intensity(const SunDev& s, float3 direction) {
+  float ct = dot(direction, ld3(s.l));
+  return s.it * (ct > s.cos_size ? 1.0f : 0.0f);
 }
 APD float3 direction_to_sun(const SunDev& s, float2 uv) {
-  float3 dir = -sun_dir(s);
-  float h = dm::cos_(s.size * 0.1f);
+  float3 dir = ld3(s.l);
+  float h = s.cos_size;
   float phi = 2.0f * kPi * uv.x;
   float z = h + (1.0f - h) * uv.y;
   float st = dm::sqrt_(1.0f - z * z);
   float sp, cp;
   dm::sincos_(phi, &sp, &cp);
   float x = cp * st, y = sp * st;
-  float3 bt = perpendicular(dir);
-  float3 tg = cross(bt, dir);
-  return normalize(bt * x + tg * y + dir * z);
+  return normalize(ld3(s.bt) * x + ld3(s.tg) * y + dir * z);
 }
 APD float2 inverse_direction_to_sun(const SunDev& s, float3 d) {
-  float3 sd = -sun_dir(s);
-  float3 bt = perpendicular(sd);
-  float3 tg = cross(bt, sd);
-  float z = dot(d, sd), x = dot(d, bt), y = dot(d, tg);
+  float3 sd = ld3(s.l);
+  float z = dot(d, sd), x = dot(d, ld3(s.bt)), y = dot(d, ld3(s.tg));
   float phi = dm::atan2_(y, x);
   float q = phi / (2.0f * kPi);
   float ux = q - truncf(q / 1.0f) * 1.0f;
-  float c = dm::cos_(s.size * 0.1f);
+  float c = s.cos_size;
   return make_float2(ux, (z - c) / (1.0f - c));
 }
 // Sky::sky: bilinear, repeat-addressed equirect lookup plus the optional sun disk.

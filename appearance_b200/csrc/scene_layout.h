@@ -41,6 +41,12 @@ struct SunDev {
   float size;
   float color[3];
   float intensity;
+  // Derived once per scene upload on the device (k_sun_derive), with the
+  // arithmetic the sun functions would otherwise repeat on every call:
+  float it;         // intensity x horizon falloff (Sky::sun_intensity)
+  float cos_size;   // cos(size * 0.1): the sun disk's angular radius
+  float l[3];       // -direction: toward the sun
+  float bt[3], tg[3];  // tangent frame around l (perpendicular(l), cross(bt, l))
 };
 
 // Compressed 8-wide BVH node, 80 bytes = 5 x uint4:
