@@ -383,6 +383,139 @@ APD float3 disney_sample(const Bsdf& b, const Frame& f, float3 wow, float distan
   return value;
 }
 
+// The parts of DisneyBsdf::evaluate that depend only on the material and the
+// outgoing direction, computed once per shading point with the same
+// expressions the per-direction evaluation would repeat: lobe weights, GGX
+// and clearcoat roughness, wo in both tangent frames, the Smith lambda of wo,
+// the GTR1 normalisation and the specular Fresnel base.
+struct DisneyCtx {
+  float w0, w1, w2, w3;  // normalised lobe weights; all 0 when their sum is 0
+  float ax, ay, one_lam_wo, g1_wo;  // GGX: alphas, 1 + lambda(wo), 1 / (1 + lambda(wo))
+  float3 wol, spec_f0;              // wo in the specular frame, spec_fresnel's base colour
+  float cca, cc_a2, cc_da, cc_log_a2, cc_one_lam_wo;  // clearcoat (GTR1)
+  float3 wol_cc;
+  bool zero;
+};
+
+APD float gtr1_lambda_c(float a2, float log_a2, float3 v) {  // gtr1_lambda with a2 and log(a2) given
+  if (v.z == 0.0f) return 0.0f;
+  float c2 = sqr(v.z);
+  float st = dm::sqrt_(dm::fmax(0.0f, 1.0f - c2));
+  if (st == 0.0f) return 0.0f;
+  float cot2 = c2 / sqr(st);
+  float cot = dm::sqrt_(cot2);
+  float a = dm::sqrt_(cot2 + a2);
+  float b = dm::sqrt_(cot2 + 1.0f);
+  float c = dm::log_(cot + b);
+  float d = dm::log_(cot + a);
+  return (a - b + cot * (c - d)) / (cot * log_a2);
+}
+
+APD DisneyCtx disney_ctx(const Bsdf& b, const Frame& f, float3 wow) {
+  DisneyCtx c;
+  float w0 = mixf(b.luminance, 0.0f, b.metallic), w1 = mixf(b.sheen, 0.0f, b.metallic);
+  float w2 = mixf(b.specular, 1.0f, b.metallic), w3 = b.clearcoat * 0.25f;
+  float ws = w0 + w1 + w2 + w3;
+  c.zero = ws == 0.0f;
+  if (c.zero) {
+    c.w0 = c.w1 = c.w2 = c.w3 = 0.0f;
+  } else {
+    float inv = 1.0f / ws;
+    c.w0 = w0 * inv; c.w1 = w1 * inv; c.w2 = w2 * inv; c.w3 = w3 * inv;
+  }
+  if (c.w2 > 0.0f) {
+    c.wol = mul_t(f.t2w, wow);
+    float2 al = alpha_from_roughness(b.roughness, b.anisotropic);
+    c.ax = al.x;
+    c.ay = al.y;
+    c.one_lam_wo = 1.0f + ggx_lambda(c.ax, c.ay, c.wol);
+    c.g1_wo = 1.0f / c.one_lam_wo;
+    float3 v = b.spec_tint;
+    v = v * (b.specular * 0.08f);
+    c.spec_f0 = (1.0f - b.metallic) * v + b.metallic * b.color;
+  }
+  if (c.w3 > 0.0f) {
+    c.wol_cc = mul_t(f.cc_t2w, wow);
+    c.cca = clearcoat_alpha(b);
+    c.cc_a2 = sqr(dm::clamp(c.cca, 0.001f, 0.999f));
+    c.cc_log_a2 = dm::log_(c.cc_a2);
+    c.cc_da = (c.cc_a2 - 1.0f) / (kPi * c.cc_log_a2);
+    c.cc_one_lam_wo = 1.0f + gtr1_lambda_c(c.cc_a2, c.cc_log_a2, c.wol_cc);
+  }
+  return c;
+}
+
+// DisneyBsdf::evaluate (disney_bsdf.wgsl:567-682) for the reflective lobes,
+// with the shading point's DisneyCtx; same arithmetic as eval_diffuse,
+// eval_sheen and eval_mf.
+APD float3 disney_eval_ctx(const Bsdf& b, const DisneyCtx& c, const Frame& f, float3 wow, float3 wiw, float* pdf) {
+  if (c.zero) {
+    *pdf = 0.0f;
+    return f3s(0.0f);
+  }
+  *pdf = 0.0f;
+  float3 value = f3s(0.0f);
+  if (c.w0 + c.w1 > 0.0f) {
+    float3 m = normalize(wiw + wow);
+    if (c.w0 > 0.0f) {
+      float3 o;
+      *pdf = *pdf + c.w0 * eval_diffuse(b, f.n, wow, wiw, m, &o);
+      value = value + o;
+    }
+    if (c.w1 > 0.0f) {
+      float3 o;
+      *pdf = *pdf + c.w1 * eval_sheen(b, wiw, m, &o);
+      value = value + o;
+    }
+  }
+  if (c.w2 + c.w3 > 0.0f) {
+    if (c.w2 > 0.0f) {
+      const float3 wol = c.wol, wil = mul_t(f.t2w, wiw);
+      const float3 m = normalize(wol + wil);
+      float sp = 0.0f;
+      float3 o = f3s(0.0f);
+      if (wol.z != 0.0f && wil.z != 0.0f) {
+        const float coh = dot(wol, m);
+        if (coh != 0.0f) {
+          const float d = ggx_d(c.ax, c.ay, m);
+          const float g = 1.0f / (c.one_lam_wo + ggx_lambda(c.ax, c.ay, wil));
+          const float sf = schlick(dm::fabs_(dot(wol, m)));
+          o = (1.0f - sf) * c.spec_f0 + f3s(sf);
+          o = o * (d * g / dm::fabs_(4.0f * wol.z * wil.z));
+          sp = (c.g1_wo * dm::fabs_(dot(wol, m)) * d / dm::fabs_(wol.z)) / dm::fabs_(4.0f * coh);
+        }
+      }
+      sp = c.w2 * sp;
+      if (sp > 0.0f) {
+        *pdf = *pdf + c.w2 * sp;
+        value = value + o;
+      }
+    }
+    if (c.w3 > 0.0f) {
+      const float3 wol = c.wol_cc, wil = mul_t(f.cc_t2w, wiw);
+      const float3 m = normalize(wol + wil);
+      float cp = 0.0f;
+      float3 o = f3s(0.0f);
+      if (wol.z != 0.0f && wil.z != 0.0f) {
+        const float coh = dot(wol, m);
+        if (coh != 0.0f) {
+          const float d = c.cc_da * (1.0f / (1.0f + (c.cc_a2 - 1.0f) * sqr(m.z)));
+          const float g = 1.0f / (c.cc_one_lam_wo + gtr1_lambda_c(c.cc_a2, c.cc_log_a2, wil));
+          o = cc_fresnel(b, wol, m);
+          o = o * (d * g / dm::fabs_(4.0f * wol.z * wil.z));
+          cp = d * dm::fabs_(m.z) / dm::fabs_(4.0f * coh);
+        }
+      }
+      cp = c.w3 * cp;
+      if (cp > 0.0f) {
+        *pdf = *pdf + c.w3 * cp;
+        value = value + o;
+      }
+    }
+  }
+  return value;
+}
+
 // DisneyBsdf::evaluate (disney_bsdf.wgsl:567-682).
 APD float3 disney_eval(const Bsdf& b, const Frame& f, float3 wow, float3 wiw, float* pdf) {
   if (b.transmission > 0.5f) {
@@ -419,55 +552,7 @@ APD float3 disney_eval(const Bsdf& b, const Frame& f, float3 wow, float3 wiw, fl
     *pdf = *pdf * (jac * ggx_pdf(al.x, al.y, wol, m));
     return ret;
   }
-  float w0 = mixf(b.luminance, 0.0f, b.metallic), w1 = mixf(b.sheen, 0.0f, b.metallic);
-  float w2 = mixf(b.specular, 1.0f, b.metallic), w3 = b.clearcoat * 0.25f;
-  float ws = w0 + w1 + w2 + w3;
-  if (ws == 0.0f) {
-    *pdf = 0.0f;
-    return f3s(0.0f);
-  }
-  float inv = 1.0f / ws;
-  w0 = w0 * inv; w1 = w1 * inv; w2 = w2 * inv; w3 = w3 * inv;
-  *pdf = 0.0f;
-  float3 value = f3s(0.0f);
-  if (w0 + w1 > 0.0f) {
-    float3 m = normalize(wiw + wow);
-    if (w0 > 0.0f) {
-      float3 c;
-      *pdf = *pdf + w0 * eval_diffuse(b, f.n, wow, wiw, m, &c);
-      value = value + c;
-    }
-    if (w1 > 0.0f) {
-      float3 c;
-      *pdf = *pdf + w1 * eval_sheen(b, wiw, m, &c);
-      value = value + c;
-    }
-  }
-  if (w2 + w3 > 0.0f) {
-    if (w2 > 0.0f) {
-      float3 wol = mul_t(f.t2w, wow), wil = mul_t(f.t2w, wiw);
-      float3 m = normalize(wol + wil);
-      float2 al = alpha_from_roughness(b.roughness, b.anisotropic);
-      float3 c = f3s(0.0f);
-      float sp = w2 * eval_mf(b, al.x, al.y, wol, wil, m, false, &c);
-      if (sp > 0.0f) {
-        *pdf = *pdf + w2 * sp;
-        value = value + c;
-      }
-    }
-    if (w3 > 0.0f) {
-      float3 wol = mul_t(f.cc_t2w, wow), wil = mul_t(f.cc_t2w, wiw);
-      float3 m = normalize(wol + wil);
-      float a = clearcoat_alpha(b);
-      float3 c = f3s(0.0f);
-      float cp = w3 * eval_mf(b, a, a, wol, wil, m, true, &c);
-      if (cp > 0.0f) {
-        *pdf = *pdf + w3 * cp;
-        value = value + c;
-      }
-    }
-  }
-  return value;
+  return disney_eval_ctx(b, disney_ctx(b, f, wow), f, wow, wiw, pdf);
 }
 
 // ---- sky and sun (sky_bindings.wgsl:4-78, sampling.wgsl:57-73, math.wgsl:88-106) ----

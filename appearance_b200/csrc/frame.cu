@@ -307,8 +307,11 @@ APD const uint4* stage_lights(const DevScene& s, uint4* sm) {
   return sm;
 }
 
+// `ctx` (the shading point's DisneyCtx, or null) saves the per-candidate
+// evaluation its wo-only terms; transmissive materials evaluate in full.
 APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& fr, const Bsdf& b, uint32_t& rng,
-                        LightSample* ls, float* pdf, LightEval* ev, float* phat, const uint4* lights) {
+                        LightSample* ls, float* pdf, LightEval* ev, float* phat, const uint4* lights,
+                        const DisneyCtx* ctx = nullptr) {
   float r0 = rnd(rng), r1 = rnd(rng), r2 = rnd(rng), r3 = rnd(rng), r4 = rnd(rng);
   *ls = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), pdf, lights);
   *ev = load_eval(s, *ls, hit, lights);
@@ -317,7 +320,8 @@ APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& f
   float wdn = dot(wi, fr.n);
   if (wdn > 0.0f && *pdf > 0.0f) {
     float sp = 0.0f;
-    float3 refl = disney_eval(b, fr, wo, wi, &sp);
+    float3 refl = (ctx && b.transmission <= 0.5f) ? disney_eval_ctx(b, *ctx, fr, wo, wi, &sp)
+                                                  : disney_eval(b, fr, wo, wi, &sp);
     if (sp > 0.0f) *phat = luma(refl * wdn * ev->emission);
   }
 }
@@ -472,6 +476,7 @@ __global__ void __launch_bounds__(kBlock, AP_SHADE_B_MIN_BLOCKS) k_shade_b(DevSc
       DiRes res = di_new();
       LightEval sel{f3s(0.0f), f3s(0.0f)};
       uint32_t n_iter = NA > NB ? NA : NB;
+      const DisneyCtx dctx = disney_ctx(b, sf.frame, wo);
       for (uint32_t k = 0; k < n_iter; ++k) {
         float apdf = 0.0f, aphat = 0.0f, bpdf = 0.0f;
         LightSample as{make_float2(0.0f, 0.0f), 0u, 0u};
@@ -479,7 +484,7 @@ __global__ void __launch_bounds__(kBlock, AP_SHADE_B_MIN_BLOCKS) k_shade_b(DevSc
         if (k == 0) {
           apdf = area_pdf; aphat = area_phat; as = area_s; ae = area_e; bpdf = bsdf_pdf;
         } else if (k < NA) {
-          area_candidate(s, hit, wo, sf.frame, b, rng, &as, &apdf, &ae, &aphat, lights);
+          area_candidate(s, hit, wo, sf.frame, b, rng, &as, &apdf, &ae, &aphat, lights, &dctx);
         }
         if (k < NA) {
           float aw = 0.0f;
