@@ -37,3 +37,26 @@ def test_full_frame_deterministic_and_finite(bench_scene):
     rays, launches = sa[-1]
     assert rays > 1920 * 1080  # extension rays of every bounce plus queued secondary rays
     assert launches > 50
+
+
+def test_full_size_frames_match_oracle(bench_scene):
+    """The benchmark workload itself (1920x1080, 1.31M triangles, 2048x1024 sky,
+    realtime preset: ReSTIR DI+GI, SVGF, TAA), two frames along the camera
+    path, against the oracle: identical bits."""
+    import os
+    from oracle.oracle import OracleFrame, OracleScene
+    sc, path = bench_scene
+    w, h = 1920, 1080
+    cfg = dict(presets.REALTIME)
+    pt = PathTracer(cfg)
+    pt.upload_scene(sc)
+    of = OracleFrame(OracleScene(sc), w, h, cfg, threads=os.cpu_count())
+    prev = None
+    for f in range(2):
+        mats, prev = scenes.camera_matrices(path[f][0], path[f][1], 60.0, 0.01, 1000.0, w, h, prev)
+        pt.set_camera_matrices(mats)
+        got = pt.render((w, h))
+        ref = of.render(mats)
+        same = got.view(np.uint32) == ref.view(np.uint32)
+        assert same.all(), f"frame {f}: {(~same).sum()} of {same.size} words differ"
+    pt.close()

@@ -87,3 +87,24 @@ def test_spectral_device_only_and_errors():
     with pytest.raises(RendererError):
         pt.render_spectral((32, 32))
     pt.close()
+
+
+def test_spectral_full_city_matches_oracle():
+    """The large spectral configuration's scene (10.0M-triangle city, sky,
+    depth 16) at a reduced image size: identical bits."""
+    import os
+    sc = scenes.city()
+    w = h = 96
+    cam = scenes.city_camera()
+    mats = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], 0.5, 5000.0, w, h, None)[0]
+    light = dict(sun_dir=(0.0, -1.0, 0.2), sun_rgb=(1.0, 1.0, 0.95), sun_scale=100.0, scene_radius=1500.0)
+    pt = PathTracer(presets.PLAIN)
+    pt.upload_scene(sc)
+    pt.set_camera_matrices(mats)
+    pt.spectral_setup(**light)
+    img = pt.render_spectral((w, h), spp=2, max_depth=16, seed=3)
+    pt.close()
+    ref = OracleSpectral(OracleScene(sc), **light).render(mats, w, h, spp=2, max_depth=16, seed=3,
+                                                        threads=os.cpu_count())
+    assert img.mean() > 0.0
+    assert_bits(img, ref, "city 96x96 spp=2 depth=16")
