@@ -522,7 +522,10 @@ __global__ void __launch_bounds__(kBlock, AP_SHADE_B_MIN_BLOCKS) k_shade_b(DevSc
 // Stage B2: Russian roulette (trace.wgsl:220-230) and the BSDF-sampled GI
 // candidate direction (InlinePathTracer::sample_ris, inline_path_tracer.wgsl:258-296),
 // continuing the path's RNG stream after stage B1.
-__global__ void __launch_bounds__(kBlock) k_shade_b2(DevScene s, FrameBuffers fb, Consts c) {
+#ifndef AP_SHADE_B2_MIN_BLOCKS
+#define AP_SHADE_B2_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(kBlock, AP_SHADE_B2_MIN_BLOCKS) k_shade_b2(DevScene s, FrameBuffers fb, Consts c) {
   const uint32_t count = bounce_count(fb, c);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     uint32_t id = bounce_path(fb, c, i);
@@ -691,7 +694,10 @@ __global__ void __launch_bounds__(kBlock) k_shade_d(FrameBuffers fb, Consts c) {
 
 // apply_di.wgsl:48-111 in two stages around its shadow ray.
 constexpr uint32_t F_DI_REPACK = 1u, F_DI_SHADOW = 2u;
-__global__ void __launch_bounds__(kBlock) k_apply_di_a(DevScene s, FrameBuffers fb, Consts c) {
+#ifndef AP_APPLY_MIN_BLOCKS
+#define AP_APPLY_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(kBlock, AP_APPLY_MIN_BLOCKS) k_apply_di_a(DevScene s, FrameBuffers fb, Consts c) {
   const uint32_t count = bounce_count(fb, c);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     uint32_t id = bounce_path(fb, c, i);
@@ -752,7 +758,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_di_b(FrameBuffers fb, Consts c
 
 // apply_gi.wgsl:44-99, plus re-queueing of the live paths (warp ballot, one
 // atomic per warp) for the next bounce.
-__global__ void __launch_bounds__(kBlock) k_apply_gi(DevScene s, FrameBuffers fb, Consts c) {
+__global__ void __launch_bounds__(kBlock, AP_APPLY_MIN_BLOCKS) k_apply_gi(DevScene s, FrameBuffers fb, Consts c) {
   const uint32_t count = c.bounce == 0 ? c.P : min(fb.counters[c.qin], c.P);
   const uint32_t* q = fb.queue[c.qin];
   uint32_t* qo = fb.queue[c.qout];
@@ -915,7 +921,10 @@ enum : uint32_t {
 
 // DI temporal, stage 1 (restir_di_temporal.wgsl:68-158): reprojection, the
 // previous reservoir and its target here, whose visibility ray is queued.
-__global__ void __launch_bounds__(256) k_dt_a(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
+#ifndef AP_TEMPORAL_MIN_BLOCKS
+#define AP_TEMPORAL_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, AP_TEMPORAL_MIN_BLOCKS) k_dt_a(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
                                               const uint4* prev_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
@@ -985,7 +994,7 @@ __global__ void __launch_bounds__(256) k_dt_b(FrameBuffers fb, Consts c, const u
 // GI temporal, stage 1 (restir_gi_temporal.wgsl:67-96): reprojection, the
 // previous reservoir, and the first ray of its target's re-trace
 // (GiReservoir::phat, inline_path_tracer.wgsl:299-331).
-__global__ void __launch_bounds__(256) k_gt_a(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
+__global__ void __launch_bounds__(256, AP_TEMPORAL_MIN_BLOCKS) k_gt_a(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
                                               const uint4* prev_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
@@ -1032,7 +1041,7 @@ __global__ void __launch_bounds__(256) k_gt_a(DevScene s, FrameBuffers fb, Const
 // GI temporal, stage 2: the re-trace's hit (InlinePathTracer::trace with the
 // approx() config, inline_path_tracer.wgsl:51-256): uniform light sample and its
 // shadow ray, or the sky on a miss.
-__global__ void __launch_bounds__(256) k_gt_b(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
+__global__ void __launch_bounds__(256, AP_TEMPORAL_MIN_BLOCKS) k_gt_b(DevScene s, FrameBuffers fb, Consts c, const uint4* prev_a,
                                               const uint4* prev_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
