@@ -92,6 +92,7 @@ struct Handle {
   // spectral mode (ap_spectral_setup / ap_render_spectral)
   void* spec_mats = nullptr;
   void* spec_env = nullptr;
+  void* spec_tab = nullptr;  // illuminant upsampling table (cache mode's predictions)
   void* spec_out = nullptr;
   size_t spec_out_bytes = 0;
   SpectralView spec{};
@@ -99,7 +100,8 @@ struct Handle {
   void spec_release() {
     if (spec_mats) cudaFree(spec_mats);
     if (spec_env) cudaFree(spec_env);
-    spec_mats = spec_env = nullptr;
+    if (spec_tab) cudaFree(spec_tab);
+    spec_mats = spec_env = spec_tab = nullptr;
     spec_ready = false;
   }
 };
@@ -855,6 +857,11 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
   if (!rc && texels)
     rc = check_cuda(h, cudaMemcpy(h->spec_env, env4.data(), sizeof(float) * env4.size(), cudaMemcpyHostToDevice),
                     "spectral env");
+  const spec::IlluminantTable& tab = spec::illuminant_table();
+  if (!rc) rc = check_cuda(h, cudaMalloc(&h->spec_tab, sizeof(float) * tab.coef.size()), "spectral table");
+  if (!rc)
+    rc = check_cuda(h, cudaMemcpy(h->spec_tab, tab.coef.data(), sizeof(float) * tab.coef.size(), cudaMemcpyHostToDevice),
+                    "spectral table");
   if (rc) {
     h->spec_release();
     return rc;
@@ -865,6 +872,8 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
   h->spec.env_h = texels ? sc.view.env_h : 0;
   h->spec.env_scale = env_scale;
   h->spec.sun = spec::make_sun(sun_dir3, sun_rgb3, sun_scale, scene_radius);
+  h->spec.illum_tab = static_cast<const float*>(h->spec_tab);
+  h->spec.illum_norm = (float)spec::illuminant_norm();
   h->spec_ready = true;
   return AP_OK;
 }
@@ -885,8 +894,14 @@ int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
   cudaSetDevice(h->device);
   // the image, then the wavefront's work area
   const uint32_t P = w * (row_end - row_start);
+  SpectralCache cache_mode{};
+  const SpectralCache* rcp = nullptr;
+  if (h->rc.cache) {  // radiance-cache mode (ap_rc_attach)
+    cache_mode = SpectralCache{h->rc.cache, h->rc.prefix, h->rc.stride, h->rc.batch, h->rc.lr, h->rc.train};
+    rcp = &cache_mode;
+  }
   const size_t need_a = (need + 255) & ~(size_t)255;
-  const size_t total = need_a + spectral_work_bytes(P);
+  const size_t total = need_a + spectral_work_bytes(P, rcp);
   if (h->spec_out_bytes < total) {
     if (h->spec_out) cudaFree(h->spec_out);
     h->spec_out = nullptr;
@@ -900,11 +915,11 @@ int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
   std::memcpy(cam.inv_view, h->mats.inv_view, sizeof(cam.inv_view));
   std::memcpy(cam.inv_proj, h->mats.inv_proj, sizeof(cam.inv_proj));
   void* work = static_cast<char*>(h->spec_out) + need_a;
-  const unsigned long long* counter = spectral_stats(work, P);
+  const unsigned long long* counter = spectral_stats(work, P, rcp);
   cudaEventRecord(h->ev0, h->stream);
   const int launches = launch_spectral(h->scene.view, h->spec, cam, w, hgt, row_start, row_end, spp, (int)max_depth,
                                        seed, static_cast<float*>(h->spec_out), work, h->num_sms, visits6 != nullptr,
-                                       h->stream);
+                                       rcp, h->stream);
   cudaEventRecord(h->ev1, h->stream);
   int rc = check_cuda(h, cudaGetLastError(), "spectral launch");
   if (rc) return rc;

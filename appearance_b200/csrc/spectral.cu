@@ -12,8 +12,17 @@
 // then the pass's radiance goes through the XYZ sensor into the pixel sums.
 // Each path runs exactly the vertex sequence of spec::li, so the image equals
 // the per-pixel loop of the CPU restatement bit for bit.
+//
+// Radiance-cache mode (SpectralCache): after each extension round, k_svertex
+// retires the paths reaching their prefix-th hit (query stored, path ended)
+// and records the suffix vertices of a rotating 1/stride of the pixels; after
+// the rounds the cache infers the retired queries (tensor-core MLP, mlp.cu),
+// k_sapply adds throughput x the prediction upsampled to the path's
+// wavelengths, and a batch of recorded vertices, with RGB targets from their
+// spectral suffix radiance, trains it.
 #include <algorithm>
 
+#include "frame.cuh"
 #include "persistent.cuh"
 #include "spectral.cuh"
 
@@ -71,11 +80,21 @@ struct SpecBuffers {
   // closest-hit rays, nodes, triangles; any-hit rays, nodes, triangles (nodes
   // and triangles only in the counting form)
   unsigned long long* stats;
+  // cache mode only
+  float4* cq;       // per path: query of the retired vertex (4 float4)
+  float4* cT;       // per path: throughput at the retired vertex
+  float* cout;      // per path: predicted RGB
+  float4* rec;      // per training pixel and round: query (4), throughput, radiance so far, tag
+  float4* bq;       // training batch queries
+  float* bt;        // training batch targets (RGB)
+  uint32_t* ccount; // [0] candidate records, [1] batch entries
 };
+
+constexpr uint32_t kSpecRecord = 7;  // float4 per recorded vertex
 
 constexpr size_t kAlign = 256;
 
-size_t carve(void* base, uint32_t P, SpecBuffers* b) {
+size_t carve(void* base, uint32_t P, const SpectralCache* rc, SpecBuffers* b) {
   char* p = static_cast<char*>(base);
   size_t off = 0;
   auto take = [&](size_t bytes) -> void* {
@@ -99,6 +118,19 @@ size_t carve(void* base, uint32_t P, SpecBuffers* b) {
   b->misc = static_cast<uint4*>(take(sizeof(uint4) * (size_t)P));
   b->counters = static_cast<uint32_t*>(take(sizeof(uint32_t) * 4 * (kSpectralMaxDepth + 2)));
   b->stats = static_cast<unsigned long long*>(take(6 * sizeof(unsigned long long)));
+  b->cq = b->cT = b->rec = b->bq = nullptr;
+  b->cout = b->bt = nullptr;
+  b->ccount = nullptr;
+  if (rc) {
+    const size_t slots = ((size_t)P / rc->stride + 1) * kRcMaxBounces;
+    b->cq = static_cast<float4*>(take(4 * f4));
+    b->cT = static_cast<float4*>(take(f4));
+    b->cout = static_cast<float*>(take(3 * sizeof(float) * (size_t)P));
+    b->rec = static_cast<float4*>(take(sizeof(float4) * kSpecRecord * slots));
+    b->bq = static_cast<float4*>(take(sizeof(float4) * 4 * (size_t)rc->batch));
+    b->bt = static_cast<float*>(take(sizeof(float) * 3 * (size_t)rc->batch));
+    b->ccount = static_cast<uint32_t*>(take(2 * sizeof(uint32_t)));
+  }
   return off;
 }
 
@@ -174,6 +206,7 @@ __global__ void __launch_bounds__(kBlock) k_sshade(DevScene s, SpectralView v, S
     const float4 ro = qo[i], rd = qd[i];
     const uint32_t owner = __float_as_uint(rd.w);
     const uint2 hh = b.hits[i];
+    if (hh.y == kRcRetired) continue;  // ended in the radiance cache at this vertex
     spec::V3 o = spec::v3(ro.x, ro.y, ro.z), d = spec::v3(rd.x, rd.y, rd.z);
     const spec::Hit h{__uint_as_float(hh.x), hh.y};
     const uint4 m = b.misc[owner];
@@ -217,6 +250,110 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sshadow(DevScene s,
       });
 }
 
+// ---- radiance-cache mode ----
+
+APD bool training_path(uint32_t p, uint32_t pass, uint32_t seed, uint32_t stride) {
+  return p % stride == (pass * 7u + 3u + seed) % stride;
+}
+
+// The cache's query at a hit (position, roughness, outgoing direction, diffuse
+// albedo, specular albedo) from the scene's RGB material, as the RGB frame
+// builds it.
+APD void spec_query(const DevScene& s, uint32_t tri, spec::V3 p, spec::V3 wo, float4* q) {
+  const InstanceDev& in = s.instances[s.tri_instance[tri]];
+  const MaterialDev* m = s.materials + in.material_idx + s.tri_material[in.first_index / 3 + (tri - in.first_global_tri)];
+  const float3 col = f3(m->color[0], m->color[1], m->color[2]);
+  const float kd = (1.0f - m->metallic) * (1.0f - m->transmission);
+  const float3 spec = f3s(0.08f * m->specular) * (1.0f - m->metallic) + col * m->metallic;
+  q[0] = make_float4(p.x, p.y, p.z, m->roughness);
+  q[1] = make_float4(wo.x, wo.y, wo.z, 0.0f);
+  q[2] = make_float4(col.x * kd, col.y * kd, col.z * kd, spec.x);
+  q[3] = make_float4(spec.y, spec.z, 0.0f, 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock) k_svertex(DevScene s, SpecBuffers b, SpectralCache rc, uint32_t round,
+                                                    uint32_t P, uint32_t pass, uint32_t seed) {
+  const uint32_t count = round == 0 ? P : min(b.counters[4 * round], P);
+  const float4* qo = b.rq_o[round & 1];
+  const float4* qd = b.rq_d[round & 1];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint2 hh = b.hits[i];
+    if (hh.y == kNoHit) continue;
+    const float4 rd = qd[i];
+    const uint32_t p = __float_as_uint(rd.w);
+    const bool tp = training_path(p, pass, seed, rc.stride);
+    if (!tp && round != rc.prefix) continue;
+    if (tp && (round == 0 || round >= kRcMaxBounces)) continue;
+    const float4 ro = qo[i];
+    const float t = __uint_as_float(hh.x);
+    const spec::V3 o = spec::v3(ro.x, ro.y, ro.z), d = spec::v3(rd.x, rd.y, rd.z);
+    float4 q[4];
+    spec_query(s, hh.y, o + d * t, -d, q);
+    if (tp) {
+      float4* r = b.rec + ((size_t)(p / rc.stride) * kRcMaxBounces + round) * kSpecRecord;
+      r[0] = q[0]; r[1] = q[1]; r[2] = q[2]; r[3] = q[3];
+      r[4] = b.beta[p];
+      r[5] = b.L[p];
+      r[6] = make_float4((float)(pass + 1), 0.0f, 0.0f, 0.0f);  // tag: the pass that wrote it
+    } else {
+      float4* dst = b.cq + 4 * (size_t)p;
+      dst[0] = q[0]; dst[1] = q[1]; dst[2] = q[2]; dst[3] = q[3];
+      b.cT[p] = b.beta[p];
+      b.misc[p].w = 1u;  // retired
+      b.hits[i].y = kRcRetired;
+    }
+  }
+}
+
+// L += throughput x the prediction, upsampled to the path's wavelengths.
+__global__ void __launch_bounds__(kBlock) k_sapply(SpectralView v, SpecBuffers b, uint32_t P) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P || b.misc[p].w == 0u) return;
+  float rgb[3] = {b.cout[3 * (size_t)p], b.cout[3 * (size_t)p + 1], b.cout[3 * (size_t)p + 2]};
+  float c[4];
+  spec::illum_lookup(v.illum_tab, v.illum_norm, rgb, c);
+  const spec::S4 Lc = spec::emission4(c, c[3], s4of(b.lambda[p]));
+  b.L[p] = f4(s4of(b.L[p]) + s4of(b.cT[p]) * Lc);
+}
+
+__global__ void k_scount(SpecBuffers b, SpectralCache rc, uint32_t slots, float tag) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = k < slots && b.rec[(size_t)k * kSpecRecord + 6].x == tag;
+  const unsigned bal = __ballot_sync(0xffffffffu, ok);
+  if ((threadIdx.x & 31) == 0 && bal) atomicAdd(&b.ccount[0], (uint32_t)__popc(bal));
+}
+
+// Keeps each of this pass's records with probability batch / count; its
+// target is the RGB of the path's radiance after the vertex divided by the
+// throughput at the vertex, per wavelength (clamped at 0).
+__global__ void k_sbatch(SpecBuffers b, SpectralCache rc, uint32_t slots, float tag, uint32_t pass, uint32_t seed,
+                         uint32_t P) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= slots) return;
+  const float4* r = b.rec + (size_t)k * kSpecRecord;
+  if (r[6].x != tag) return;
+  const uint32_t cand = b.ccount[0];
+  const float keep = cand <= rc.batch ? 1.0f : (float)rc.batch / (float)cand;
+  const float u = (float)(spec::pcg(k * 2654435761u ^ spec::pcg(pass + seed * 7919u)) >> 8) * (1.0f / 16777216.0f);
+  if (u >= keep) return;
+  const uint32_t p = (k / kRcMaxBounces) * rc.stride + (pass * 7u + 3u + seed) % rc.stride;
+  if (p >= P) return;
+  const uint32_t slot = atomicAdd(&b.ccount[1], 1u);
+  if (slot >= rc.batch) return;
+  const spec::S4 Lend = s4of(b.L[p]), Lv = s4of(r[5]), T = s4of(r[4]);
+  spec::S4 dl;
+  for (int j = 0; j < 4; ++j) dl.v[j] = T.v[j] > 0.0f ? dm::fmax(Lend.v[j] - Lv.v[j], 0.0f) / T.v[j] : 0.0f;
+  spec::Wavelengths w;
+  w.lambda = s4of(b.lambda[p]);
+  for (int j = 0; j < 4; ++j) w.pdf.v[j] = spec::visible_wavelength_pdf(w.lambda.v[j]);
+  const spec::V3 rgb = spec::xyz_to_srgb(spec::to_xyz(dl, w));
+  float4* q = b.bq + 4 * (size_t)slot;
+  q[0] = r[0]; q[1] = r[1]; q[2] = r[2]; q[3] = r[3];
+  b.bt[3 * (size_t)slot + 0] = dm::fmax(rgb.x, 0.0f);
+  b.bt[3 * (size_t)slot + 1] = dm::fmax(rgb.y, 0.0f);
+  b.bt[3 * (size_t)slot + 2] = dm::fmax(rgb.z, 0.0f);
+}
+
 __global__ void __launch_bounds__(kBlock) k_saccum(SpecBuffers b, uint32_t P, bool last, float inv, float* out) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
@@ -237,23 +374,25 @@ __global__ void __launch_bounds__(kBlock) k_saccum(SpecBuffers b, uint32_t P, bo
 
 }  // namespace
 
-size_t spectral_work_bytes(uint32_t P) {
+size_t spectral_work_bytes(uint32_t P, const SpectralCache* rc) {
   SpecBuffers b;
-  return carve(nullptr, P, &b);
+  return carve(nullptr, P, rc, &b);
 }
 
-const unsigned long long* spectral_stats(void* work, uint32_t P) {
+const unsigned long long* spectral_stats(void* work, uint32_t P, const SpectralCache* rc) {
   SpecBuffers b;
-  carve(work, P, &b);
+  carve(work, P, rc, &b);
   return b.stats;
 }
 
 int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCamera& cam, uint32_t W, uint32_t H,
                     uint32_t row0, uint32_t row1, uint32_t spp, int max_depth, uint32_t seed, float* out, void* work,
-                    int num_sms, bool count_visits, cudaStream_t st) {
+                    int num_sms, bool count_visits, const SpectralCache* rc, cudaStream_t st) {
   const uint32_t P = W * (row1 - row0);
   SpecBuffers b;
-  carve(work, P, &b);
+  carve(work, P, rc, &b);
+  const uint32_t slots = rc ? (P / rc->stride + 1) * kRcMaxBounces : 0u;
+  if (rc) cudaMemsetAsync(b.rec, 0, sizeof(float4) * kSpecRecord * slots, st);  // no tags from an earlier call
   const uint32_t rounds = (uint32_t)max_depth + 1;
   const int linear = (int)((P + kBlock - 1) / kBlock);
   const int persistent = num_sms * kTraceMinBlocks;
@@ -267,10 +406,28 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
     for (uint32_t r = 0; r < rounds; ++r) {
       if (count_visits) k_sextend<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
       else k_sextend<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      if (rc) {
+        k_svertex<<<shade, kBlock, 0, st>>>(s, b, *rc, r, P, k, seed);
+        ++launches;
+      }
       k_sshade<<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth);
       if (count_visits) k_sshadow<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
       else k_sshadow<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
       launches += 3;
+    }
+    if (rc) {
+      rc_infer_device(rc->cache, b.cq, P, b.cout, st);
+      k_sapply<<<linear, kBlock, 0, st>>>(v, b, P);
+      launches += 2;
+      if (rc->train) {
+        const float tag = (float)(k + 1);
+        const int sb = (int)((slots + 255) / 256);
+        cudaMemsetAsync(b.ccount, 0, 2 * sizeof(uint32_t), st);
+        k_scount<<<sb, 256, 0, st>>>(b, *rc, slots, tag);
+        k_sbatch<<<sb, 256, 0, st>>>(b, *rc, slots, tag, k, seed, P);
+        rc_train_device(rc->cache, b.bq, b.bt, b.ccount + 1, rc->batch, rc->lr, 1, st);
+        launches += 3;
+      }
     }
     k_saccum<<<linear, kBlock, 0, st>>>(b, P, k + 1 == spp, 1.0f / (float)spp, out);
     ++launches;

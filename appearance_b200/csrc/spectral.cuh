@@ -16,6 +16,20 @@ struct SpectralView {
   uint32_t env_w, env_h;
   float env_scale;
   spec::Sun sun;
+  const float* illum_tab;  // 33^3 x 3 illuminant upsampling coefficients (spec::illum_lookup)
+  float illum_norm;
+};
+
+// Radiance-cache mode of the spectral render (the cache of ap_rc_attach):
+// paths are retired at their prefix-th hit into the cache's RGB prediction,
+// upsampled to the path's wavelengths; a rotating 1/stride of the pixels trace
+// full paths and, per sample pass, a batch of their suffix vertices trains
+// the cache (RGB targets from the spectral estimates).
+struct SpectralCache {
+  void* cache;
+  uint32_t prefix, stride, batch;
+  float lr;
+  int train;
 };
 
 struct SpectralCamera {
@@ -24,12 +38,13 @@ struct SpectralCamera {
 
 constexpr int kSpectralMaxDepth = 1000;
 
-// Device bytes of the work area for P = W x rows paths.
-size_t spectral_work_bytes(uint32_t P);
+// Device bytes of the work area for P = W x rows paths (and the cache mode's
+// buffers when rc is non-null).
+size_t spectral_work_bytes(uint32_t P, const SpectralCache* rc);
 // Counters of the last launch_spectral on `work` (device): closest-hit rays,
 // nodes, triangles; any-hit rays, nodes, triangles (nodes and triangles only
 // when it ran with count_visits).
-const unsigned long long* spectral_stats(void* work, uint32_t P);
+const unsigned long long* spectral_stats(void* work, uint32_t P, const SpectralCache* rc);
 
 // Renders rows [row0, row1) of a W x H image at `spp` samples per pixel into
 // out (3 floats per pixel, row row0 first), with `work` of
@@ -38,6 +53,6 @@ const unsigned long long* spectral_stats(void* work, uint32_t P);
 // (slower).  Returns the number of kernels launched.
 int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCamera& cam, uint32_t W, uint32_t H,
                     uint32_t row0, uint32_t row1, uint32_t spp, int max_depth, uint32_t seed, float* out, void* work,
-                    int num_sms, bool count_visits, cudaStream_t st);
+                    int num_sms, bool count_visits, const SpectralCache* rc, cudaStream_t st);
 
 }  // namespace ap

@@ -157,6 +157,39 @@ SPHD S4 emission4(const float* c, float scale, const S4& lambda) {
   return r;
 }
 
+// Unbounded RGB (an emitter's radiance, an environment texel, a predicted
+// radiance) as an illuminant spectrum: the sigmoid coefficients of
+// rgb / (2 max) interpolated trilinearly in a 33^3 table over rgb / max
+// (`tab`, 3 floats per entry, built by spectral_fit.cpp), and the scale
+// 2 max(rgb) x norm (RgbIlluminantSpectrum).  out: 3 coefficients, scale.
+SPHD void illum_lookup(const float* tab, float norm, const float rgb[3], float out[4]) {
+  const float m = dm::fmax(rgb[0], dm::fmax(rgb[1], rgb[2]));
+  if (!(m > 0.0f)) {
+    out[0] = 0.0f;
+    out[1] = 0.0f;
+    out[2] = -1e4f;  // sigmoid -> 0
+    out[3] = 0.0f;
+    return;
+  }
+  float f[3];
+  int i0[3];
+  for (int k = 0; k < 3; ++k) {
+    const float x = dm::clamp(rgb[k] / m, 0.0f, 1.0f) * 32.0f;
+    i0[k] = (int)x < 31 ? (int)x : 31;
+    f[k] = x - (float)i0[k];
+  }
+  for (int c = 0; c < 3; ++c) {
+    float v = 0.0f;
+    for (int corner = 0; corner < 8; ++corner) {
+      const int dr = corner & 1, dg = (corner >> 1) & 1, db = corner >> 2;
+      const float w = (dr ? f[0] : 1.0f - f[0]) * (dg ? f[1] : 1.0f - f[1]) * (db ? f[2] : 1.0f - f[2]);
+      v = v + w * tab[3 * (((i0[2] + db) * 33 + (i0[1] + dg)) * 33 + (i0[0] + dr)) + c];
+    }
+    out[c] = v;
+  }
+  out[3] = 2.0f * m * norm;
+}
+
 // XYZ of one path's spectral radiance (to_xyz) and linear sRGB.
 SPHD V3 to_xyz(S4 L, const Wavelengths& w) {
   float x = 0.0f, y = 0.0f, z = 0.0f;

@@ -153,32 +153,7 @@ IlluminantTable::IlluminantTable() : coef(33 * 33 * 33 * 3) {
 }
 
 void IlluminantTable::lookup(const float rgb[3], float out[4]) const {
-  float m = std::fmax(rgb[0], std::fmax(rgb[1], rgb[2]));
-  if (!(m > 0.0f)) {
-    out[0] = 0.0f;
-    out[1] = 0.0f;
-    out[2] = -1e4f;  // sigmoid -> 0
-    out[3] = 0.0f;
-    return;
-  }
-  float x[3];
-  int i0[3];
-  float f[3];
-  for (int k = 0; k < 3; ++k) {
-    x[k] = std::fmin(std::fmax(rgb[k] / m, 0.0f), 1.0f) * 32.0f;
-    i0[k] = std::min((int)x[k], 31);
-    f[k] = x[k] - (float)i0[k];
-  }
-  for (int c = 0; c < 3; ++c) {
-    float v = 0.0f;
-    for (int corner = 0; corner < 8; ++corner) {
-      int dr = corner & 1, dg = (corner >> 1) & 1, db = corner >> 2;
-      float w = (dr ? f[0] : 1.0f - f[0]) * (dg ? f[1] : 1.0f - f[1]) * (db ? f[2] : 1.0f - f[2]);
-      v += w * coef[3 * (((i0[2] + db) * 33 + (i0[1] + dg)) * 33 + (i0[0] + dr)) + c];
-    }
-    out[c] = v;
-  }
-  out[3] = 2.0f * m * (float)illuminant_norm();  // RgbIlluminantSpectrum scale = 2 max(rgb)
+  illum_lookup(coef.data(), (float)illuminant_norm(), rgb, out);
 }
 
 const IlluminantTable& illuminant_table() {

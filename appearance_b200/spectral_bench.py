@@ -3,7 +3,9 @@ buildings on a 2 km grid, 10k emissive window triangles, sky environment):
 hero-wavelength paths of depth 16 at 4096 x 4096 and 64 spp, rendered in row
 bands, timed on the device.  Reports Msamples/s, Mrays/s and rays per sample;
 with --quality also the relMSE of the 64-spp image on the centre 1024 x 1024
-crop against a high-spp reference of that crop accumulated in float64.
+crop against a high-spp reference of that crop accumulated in float64; with
+--cache the same for the radiance-cache mode (paths ended at their first
+bounce's hit in the online-trained cache).
 
 The CPU figure (--cpu-rows > 0) is the oracle's restatement of the same
 integrator on all host threads over a band of rows of the crop at 1 spp,
@@ -54,7 +56,7 @@ def render_bands(pt, size, spp, depth, seed, band, to_host=False):
 
 
 def measure(lots=64, size=4096, spp=64, depth=16, band=4096, repeats=1, quality=False, ref_spp=4096,
-            cpu_rows=0) -> dict:
+            cpu_rows=0, cache=False, cache_prefix=1) -> dict:
     sc, mats, gen_s = setup(lots, size)
     pt = PathTracer(presets.PLAIN)
     t0 = time.perf_counter()
@@ -105,6 +107,23 @@ def measure(lots=64, size=4096, spp=64, depth=16, band=4096, repeats=1, quality=
         res["quality"] = {"crop": [c0, c1], "ref_spp": ref_spp,
                           "relmse_crop": rel_mse(img[c0:c1, c0:c1].astype(np.float64), ref),
                           "mean_crop": ref.mean(axis=(0, 1)).tolist()}
+    if cache:
+        # radiance-cache mode: paths end at their prefix-th hit in the online-trained
+        # cache; 1/16 of the pixels per pass trace full paths and train it
+        from .radiance_cache import RadianceCache
+        ext = sc.positions.max(0) - sc.positions.min(0)
+        rc = RadianceCache(sc.positions.min(0) - 0.02 * ext, sc.positions.max(0) + 0.02 * ext, seed=1)
+        pt.attach_radiance_cache(rc, prefix_bounces=cache_prefix, train_stride=16, train_batch=65536, lr=1e-3)
+        warm_ms = render_bands(pt, size, 8, depth, 7, band)[1]  # 8 passes of online training first
+        _, ms_c, rays_c = render_bands(pt, size, spp, depth, 100, band)
+        res["cache"] = {"value": samples / (ms_c * 1e3), "unit": "Msamples/s", "frame_ms": ms_c,
+                        "rays_per_sample": rays_c / samples, "prefix": cache_prefix, "warmup_ms": warm_ms,
+                        "training": "65536 suffix vertices per sample pass from 1/16 of the pixels, Adam lr 1e-3"}
+        if quality:
+            img_c, _, _ = render_bands(pt, size, spp, depth, 100, band, to_host=True)
+            res["cache"]["relmse_crop"] = rel_mse(img_c[c0:c1, c0:c1].astype(np.float64), ref)
+        pt.attach_radiance_cache(None)
+        rc.close()
     pt.close()
     if cpu_rows > 0:
         from oracle.oracle import OracleScene, OracleSpectral  # the CPU baseline only
@@ -132,8 +151,11 @@ def main(argv=None):
     ap.add_argument("--quality", action="store_true", help="relMSE of the crop against a high-spp reference")
     ap.add_argument("--ref-spp", type=int, default=4096)
     ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the crop rendered by the CPU oracle")
+    ap.add_argument("--cache", action="store_true", help="also run the radiance-cache mode")
+    ap.add_argument("--cache-prefix", type=int, default=1)
     a = ap.parse_args(argv)
-    res = measure(a.lots, a.size, a.spp, a.depth, a.band, a.repeats, a.quality, a.ref_spp, a.cpu_rows)
+    res = measure(a.lots, a.size, a.spp, a.depth, a.band, a.repeats, a.quality, a.ref_spp, a.cpu_rows, a.cache,
+                  a.cache_prefix)
     print(json.dumps(res), flush=True)
     return res
 

@@ -331,10 +331,12 @@ def city_spectral_config(cpu: bool) -> dict:
     buildings on a 2 km grid, 10k emissive window triangles, sky environment),
     hero-wavelength paths (4 wavelengths in 360-830 nm, RGB-to-spectrum
     albedos and emitters), depth 16, 4096x4096 at 64 spp: one warm-up image at
-    4 spp, then one timed image (device time).  The CPU oracle of the same
-    integrator renders 64 full-width rows at 1 spp beside it."""
+    4 spp, then one timed image (device time); then the same in radiance-cache
+    mode (`cache`: paths ended at their first bounce's hit in the online-trained
+    cache, after 8 training passes).  The CPU oracle of the same integrator
+    renders 64 full-width rows at 1 spp beside it."""
     from appearance_b200 import spectral_bench
-    return spectral_bench.measure(cpu_rows=64 if cpu else 0)
+    return spectral_bench.measure(cpu_rows=64 if cpu else 0, cache=True)
 
 
 def measure_details(pt, scene, path, cfg) -> dict:

@@ -324,7 +324,10 @@ int ap_rc_train(void* cache, const float* queries, const float* targets, uint32_
  * max_bounces and its suffix vertices (bounces 1..7) give training targets
  * (the radiance measured after the vertex divided by the throughput at it),
  * of which `train_batch` are drawn at random for one Adam step (learning rate
- * `lr`) per frame when `train` != 0.  The cache must outlive the attachment. */
+ * `lr`) per frame when `train` != 0.  The cache must outlive the attachment.
+ * ap_render_spectral uses the attachment too: each sample pass is a frame,
+ * the prediction (RGB) is upsampled to each path's wavelengths, and training
+ * targets are the RGB of the spectral suffix estimates. */
 int ap_rc_attach(void* handle, void* cache, uint32_t prefix_bounces, uint32_t train_stride, uint32_t train_batch,
                  float lr, int train);
 

@@ -108,3 +108,47 @@ def test_spectral_full_city_matches_oracle():
                                                         threads=os.cpu_count())
     assert img.mean() > 0.0
     assert_bits(img, ref, "city 96x96 spp=2 depth=16")
+
+
+def test_spectral_cache_mode():
+    """Radiance-cache mode of the spectral render (ap_rc_attach): deterministic
+    with a frozen cache, and after online training a 1-bounce prefix ended in
+    the cache recovers the light that truncating the paths there loses."""
+    from appearance_b200.radiance_cache import RadianceCache
+
+    def rel_mse(x, ref):
+        return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    sc = scenes.cornell_box()
+    w, h = 64, 48
+    cam = scenes.cornell_camera()
+    mats = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], 0.01, 100.0, w, h, None)[0]
+    light = dict(sun_scale=0.0, scene_radius=10.0)
+    pt = PathTracer(presets.PLAIN)
+    pt.upload_scene(sc)
+    pt.set_camera_matrices(mats)
+    pt.spectral_setup(**light)
+    ref = pt.render_spectral((w, h), spp=4096, max_depth=16, seed=1).astype(np.float64)
+    cut = pt.render_spectral((w, h), spp=512, max_depth=1, seed=2).astype(np.float64)
+
+    rc = RadianceCache([-0.05, -0.05, -0.05], [1.05, 1.05, 1.05], seed=1)
+    pt.attach_radiance_cache(rc, prefix_bounces=1, train_stride=4, train_batch=16384, lr=5e-3, train=False)
+    a = pt.render_spectral((w, h), spp=4, max_depth=16, seed=3)
+    b = pt.render_spectral((w, h), spp=4, max_depth=16, seed=3)
+    assert_bits(a, b, "frozen cache")
+    assert np.isfinite(a).all()
+
+    pt.attach_radiance_cache(rc, prefix_bounces=1, train_stride=4, train_batch=16384, lr=5e-3, train=True)
+    for k in range(3):  # 192 training steps (one per sample pass)
+        pt.render_spectral((w, h), spp=64, max_depth=16, seed=10 + k, to_host=False)
+    cached = pt.render_spectral((w, h), spp=512, max_depth=16, seed=2).astype(np.float64)
+    pt.attach_radiance_cache(None)
+    pt.close()
+    rc.close()
+    e_cut, e_cached = rel_mse(cut, ref), rel_mse(cached, ref)
+    print(f"spectral relMSE truncated {e_cut:.5f} cached {e_cached:.5f}; mean ref {ref.mean():.4f} "
+          f"cut {cut.mean():.4f} cached {cached.mean():.4f}")
+    assert np.isfinite(cached).all()
+    assert cut.mean() < 0.9 * ref.mean()
+    assert abs(cached.mean() - ref.mean()) < 0.5 * abs(cut.mean() - ref.mean())
+    assert e_cached < 0.6 * e_cut
