@@ -280,9 +280,10 @@ def main():
         line["gpu_launches"] = int(details["gpu_launches_per_step"]) * args.steps
         if world == 1 and args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(scene, path, cfg)
-        cpu = world == 1 and bool(args.cpu_baseline)
-        line["configs"] = {"cornell_512_16spp_depth5": cornell_config(cpu),
-                           "city_spectral_4096_64spp_depth16": city_spectral_config(cpu)}
+        if world == 1:  # the other configurations are single-GPU cases, measured on one GPU only
+            cpu = bool(args.cpu_baseline)
+            line["configs"] = {"cornell_512_16spp_depth5": cornell_config(cpu),
+                               "city_spectral_4096_64spp_depth16": city_spectral_config(cpu)}
         print(json.dumps(line), flush=True)
     pt.close()
     if world > 1:
