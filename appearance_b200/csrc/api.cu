@@ -302,6 +302,10 @@ int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats, Fr
   if (rc) return rc;
   rc = check_cuda(h, cudaEventSynchronize(h->ev1), "frame");
   if (rc) return rc;
+  if (h->rc.cache) {
+    std::string msg;
+    if ((rc = rc_take_status(h->rc.cache, &msg))) return fail(h, rc, "radiance cache: " + msg);
+  }
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, h->ev0, h->ev1);
   if (stats) {
@@ -932,6 +936,10 @@ int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
   }
   rc = check_cuda(h, cudaStreamSynchronize(h->stream), "spectral render");
   if (rc) return rc;
+  if (rcp) {
+    std::string msg;
+    if ((rc = rc_take_status(rcp->cache, &msg))) return fail(h, rc, "radiance cache: " + msg);
+  }
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, h->ev0, h->ev1);
   if (stats) {

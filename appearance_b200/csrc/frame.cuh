@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "scene_layout.h"
 
 namespace ap {
@@ -129,6 +131,9 @@ void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_
 int rc_infer_device(void* cache, const float4* queries, uint32_t n, float* out, cudaStream_t st);
 int rc_train_device(void* cache, const float4* queries, const float* targets, const uint32_t* n_dev, uint32_t cap,
                     float lr, int update, cudaStream_t st);
+// After the stream drained: the first error of those calls since the last
+// check, or AP_E_TIMEOUT for an inference wait that ran out; clears it.
+int rc_take_status(void* cache, std::string* msg);
 
 int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t stream,

@@ -467,6 +467,7 @@ struct Cache {
   float* out = nullptr;
   uint32_t cap = 0;
   std::string msg;
+  int pending = 0;  // first error of a frame-driven call (rc_infer_device / rc_train_device)
 };
 
 int cfail(Cache* c, int code, const std::string& m) {
@@ -511,7 +512,24 @@ int rc_infer_device(void* cp, const float4* queries, uint32_t n, float* out, cud
   const int tiles = (int)((n + kTile - 1) / kTile);
   const int grid = tiles < 2 * c->num_sms ? tiles : 2 * c->num_sms;
   k_rc_infer<<<grid, kTile, kSmemInfer, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, n, c->bounds, out, c->err);
-  return cuda_ok(c, cudaGetLastError(), "radiance cache inference");
+  const int rc = cuda_ok(c, cudaGetLastError(), "radiance cache inference");
+  if (rc && !c->pending) c->pending = rc;
+  return rc;
+}
+
+// After the caller's stream has drained: the first error of the frame-driven
+// calls since the last check, or AP_E_TIMEOUT when an inference tile's
+// tensor-core wait ran out of its bound; clears both.
+int rc_take_status(void* cp, std::string* msg) {
+  Cache* c = static_cast<Cache*>(cp);
+  uint32_t e = 0;
+  cudaMemcpy(&e, c->err, 4, cudaMemcpyDeviceToHost);
+  int rc = c->pending;
+  if (!rc && e) rc = cfail(c, AP_E_TIMEOUT, "inference: tensor-core wait timed out");
+  if (rc && msg) *msg = c->msg;
+  if (e) cudaMemset(c->err, 0, 4);
+  c->pending = 0;
+  return rc;
 }
 
 // Training step on at most `cap` samples; the sample count is read from device
@@ -521,7 +539,10 @@ int rc_train_device(void* cp, const float4* queries, const float* targets, const
   Cache* c = static_cast<Cache*>(cp);
   if (cap == 0) return AP_OK;
   int rc = ensure_batch(c, cap);
-  if (rc) return rc;
+  if (rc) {
+    if (!c->pending) c->pending = rc;
+    return rc;
+  }
   cudaMemsetAsync(c->grad, 0, kNumParams * 4, st);
   cudaMemsetAsync(c->loss, 0, 4, st);
   const size_t S = cap;
@@ -553,7 +574,9 @@ int rc_train_device(void* cp, const float4* queries, const float* targets, const
     k_rc_adam<<<(kNumParams + 255) / 256, 256, 0, st>>>(c->master, c->m1, c->m2, c->grad, lr, b1, b2, 1e-8f, c1, c2, 1,
                                                         c->wf, c->packed);
   }
-  return cuda_ok(c, cudaGetLastError(), "radiance cache training");
+  rc = cuda_ok(c, cudaGetLastError(), "radiance cache training");
+  if (rc && !c->pending) c->pending = rc;
+  return rc;
 }
 
 }  // namespace ap
