@@ -19,7 +19,7 @@ EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error"
            "ap_bvh_stats", "ap_server_create", "ap_server_destroy", "ap_server_last_error", "ap_server_add_scene",
            "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_stats",
            "ap_rc_create", "ap_rc_destroy", "ap_rc_last_error", "ap_rc_set_params", "ap_rc_get_params", "ap_rc_infer",
-           "ap_rc_train", "ap_rc_attach", "ap_spectral_setup", "ap_render_spectral", "ap_profile_spectral"]
+           "ap_rc_train", "ap_rc_attach", "ap_rc_wait_selftest", "ap_spectral_setup", "ap_render_spectral", "ap_profile_spectral"]
 
 U32, F32, P = ctypes.c_uint32, ctypes.c_float, ctypes.c_void_p
 
@@ -89,6 +89,7 @@ def load() -> ctypes.CDLL:
     L.ap_trace_rays_static.argtypes = [P, P, P, U32, ctypes.c_int, P]
     L.ap_read_buffer.argtypes = [P, U32, P, ctypes.c_size_t]
     L.ap_bvh_stats.argtypes = [P, P]
+    L.ap_rc_wait_selftest.argtypes = [ctypes.c_int, ctypes.c_int, P]
     L.ap_spectral_setup.argtypes = [P, P, P, F32, F32, F32]
     L.ap_render_spectral.argtypes = [P, U32, U32, U32, U32, U32, U32, U32, P, ctypes.c_size_t,
                                      ctypes.POINTER(FrameStats)]

@@ -146,8 +146,8 @@ APD void mma_commit(uint32_t bar) {
 }
 
 // Waits for phase `parity` of the mbarrier with an iteration limit; returns false on timeout.
-APD bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); ++it) {
+APD bool mbar_wait(uint32_t bar, uint32_t parity, int limit = 1 << 22) {
+  for (int it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -158,6 +158,21 @@ APD bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (done) return true;
   }
   return false;
+}
+
+// Self-test of the bounded wait, with no tensor-core work: a barrier that
+// nothing arrives on must give up after `limit` tries and say so (out[0] = 0);
+// one that the thread itself arrived on must complete (out[1] = 1).
+__global__ void k_wait_selftest(int limit, uint32_t* out) {
+  __shared__ __align__(8) uint64_t bar[2];
+  if (threadIdx.x != 0) return;
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])));
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])));
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  out[0] = mbar_wait(smem_u32(&bar[0]), 0u, limit) ? 1u : 0u;
+  uint64_t state;
+  asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(state) : "r"(smem_u32(&bar[1])) : "memory");
+  out[1] = mbar_wait(smem_u32(&bar[1]), 0u, limit) ? 1u : 0u;
 }
 
 APD void tmem_ld16(uint32_t taddr, float* v) {
@@ -653,6 +668,19 @@ void ap_rc_destroy(void* cp) {
 const char* ap_rc_last_error(const void* cp) {
   const Cache* c = static_cast<const Cache*>(cp);
   return c ? c->msg.c_str() : "null cache";
+}
+
+int ap_rc_wait_selftest(int device, int limit, uint32_t* out2) {
+  if (!out2 || limit <= 0 || limit > (1 << 22)) return AP_E_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return AP_E_CUDA;
+  uint32_t* d = nullptr;
+  if (cudaMalloc(&d, 8) != cudaSuccess) return AP_E_OOM;
+  cudaMemset(d, 0xff, 8);
+  ap::k_wait_selftest<<<1, 32>>>(limit, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(out2, d, 8, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? AP_OK : AP_E_CUDA;
 }
 
 int ap_rc_set_params(void* cp, const float* params, uint32_t count) {

@@ -317,6 +317,13 @@ int ap_rc_infer(void* cache, const float* queries, uint32_t n, float* out_rgb);
  * gradient of the loss (AP_RC_NUM_PARAMS floats). */
 int ap_rc_train(void* cache, const float* queries, const float* targets, uint32_t n, float lr, int update,
                 float* loss, float* grad_out);
+/* Self-test of the bounded tensor-core completion wait used by ap_rc_infer
+ * (no counterpart in the reference): on `device`, a barrier that nothing
+ * arrives on must give up after `limit` tries (1..2^22) and report it,
+ * out2[0] = 0; one that has completed must report success, out2[1] = 1.
+ * The error path it exercises is the one that turns a stalled tensor-core
+ * wait into AP_E_TIMEOUT instead of a hung kernel. */
+int ap_rc_wait_selftest(int device, int limit, uint32_t* out2);
 /* Radiance-cache mode of a renderer (cache NULL detaches): in every frame the
  * paths of most pixels end at their `prefix_bounces`-th hit with T x the
  * cache's prediction (the frame's max_bounces must exceed prefix_bounces);

@@ -1,6 +1,8 @@
 """Radiance cache on the GPU against the numpy oracle (oracle/mlp_oracle.py):
 tensor-core inference, training gradients and the Adam step; and that training
 fits a smooth radiance field."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -89,3 +91,17 @@ def test_training_fits_a_smooth_radiance_field():
     assert np.mean(losses[-20:]) < 0.1 * np.mean(losses[:5])
     assert after < 0.05 * before
     rc.close()
+
+
+def test_bounded_wait_reports_timeout():
+    """The tensor-core completion wait gives up after its iteration limit and
+    reports it (the path that turns a stalled wait into AP_E_TIMEOUT), without
+    faulting or hanging the GPU: a barrier that nothing arrives on times out,
+    one that has completed does not."""
+    import numpy as np
+    from appearance_b200 import _native
+    lib = _native.load()
+    out = np.full(2, 7, np.uint32)
+    assert lib.ap_rc_wait_selftest(0, 1024, out.ctypes.data_as(ctypes.c_void_p)) == _native.AP_OK
+    assert out.tolist() == [0, 1]
+    assert lib.ap_rc_wait_selftest(0, 0, out.ctypes.data_as(ctypes.c_void_p)) == _native.AP_E_INVALID
