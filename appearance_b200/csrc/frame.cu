@@ -318,7 +318,10 @@ APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& f
   *phat = 0.0f;
   float3 wi = normalize(ev->point - hit);
   float wdn = dot(wi, fr.n);
-  if (wdn > 0.0f && *pdf > 0.0f) {
+  // a light sample without emission (a sun of intensity 0) has target +0 whatever
+  // the BSDF value: skip its evaluation (the oracle skips it too)
+  const bool lit = ev->emission.x != 0.0f || ev->emission.y != 0.0f || ev->emission.z != 0.0f;
+  if (wdn > 0.0f && *pdf > 0.0f && lit) {
     float sp = 0.0f;
     float3 refl = (ctx && b.transmission <= 0.5f) ? disney_eval_ctx(b, *ctx, fr, wo, wi, &sp)
                                                   : disney_eval(b, fr, wo, wi, &sp);

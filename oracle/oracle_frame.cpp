@@ -173,7 +173,9 @@ struct Frame {
         area_eval = load_eval_data(*scene, area_sample, hit);
         V3 wi = normalize(area_eval.point - hit);
         float wdn = dot(wi, fr.n);
-        if (wdn > 0.0f && area_pdf > 0.0f) {
+        const bool lit = area_eval.emission.x != 0.0f || area_eval.emission.y != 0.0f ||
+                         area_eval.emission.z != 0.0f;
+        if (wdn > 0.0f && area_pdf > 0.0f && lit) {  // no emission: target +0, no BSDF evaluation
           float spdf = 0.0f;
           V3 refl = disney_evaluate(b, fr, wo, wi, &spdf);
           if (spdf > 0.0f) area_phat = luma(refl * wdn * area_eval.emission);
