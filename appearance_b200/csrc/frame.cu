@@ -652,7 +652,10 @@ __global__ void __launch_bounds__(kBlock, AP_SHADE_C_MIN_BLOCKS) k_shade_c(DevSc
             so = sf.hit_point + sf.n * 1e-4f;
             sd = sdir;
             st = sdist - 1e-4f * 2.0f;
-            want = true;
+            // a zero contribution (a light sample without emission) leaves +0 whether or not
+            // the ray is occluded (k_shade_d adds it to +0): finish here without the ray
+            want = acc.x != 0.0f || acc.y != 0.0f || acc.z != 0.0f;
+            if (!want) acc = f3s(0.0f);
           }
         }
         point = sf.hit_point;
