@@ -128,7 +128,9 @@ size_t rc_frame_bytes(uint32_t W, uint32_t H, uint32_t stride, uint32_t batch);
 void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_t batch, RcFrame* rc);
 
 // mlp.cu: inference over n queries, and one training step on a device-assembled batch
-int rc_infer_device(void* cache, const float4* queries, uint32_t n, float* out, cudaStream_t st);
+// (n_dev, when given: the number of queries, read on the device, at most n)
+int rc_infer_device(void* cache, const float4* queries, uint32_t n, float* out, cudaStream_t st,
+                    const uint32_t* n_dev = nullptr);
 int rc_train_device(void* cache, const float4* queries, const float* targets, const uint32_t* n_dev, uint32_t cap,
                     float lr, int update, cudaStream_t st);
 // After the stream drained: the first error of those calls since the last

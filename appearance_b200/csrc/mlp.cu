@@ -241,7 +241,8 @@ APD bool rc_layer(uint32_t tmem, uint32_t bar, uint32_t& phase, uint32_t a_base,
 
 __global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__ packed, const float4* __restrict__ queries,
                                                        uint32_t n, RcBounds bounds, float* __restrict__ out,
-                                                       uint32_t* __restrict__ err) {
+                                                       uint32_t* __restrict__ err, const uint32_t* __restrict__ n_dev) {
+  if (n_dev) n = min(n, *n_dev);  // a query count produced on the device (at most n)
   extern __shared__ __align__(1024) unsigned char smem[];
   __half* w = reinterpret_cast<__half*>(smem);
   __half* act = reinterpret_cast<__half*>(smem + kSmemWeights);
@@ -521,12 +522,13 @@ void repack(Cache* c) {
 }  // namespace
 
 // Entry points used by the frame (device pointers, the caller's stream).
-int rc_infer_device(void* cp, const float4* queries, uint32_t n, float* out, cudaStream_t st) {
+int rc_infer_device(void* cp, const float4* queries, uint32_t n, float* out, cudaStream_t st, const uint32_t* n_dev) {
   Cache* c = static_cast<Cache*>(cp);
   if (n == 0) return AP_OK;
   const int tiles = (int)((n + kTile - 1) / kTile);
   const int grid = tiles < 2 * c->num_sms ? tiles : 2 * c->num_sms;
-  k_rc_infer<<<grid, kTile, kSmemInfer, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, n, c->bounds, out, c->err);
+  k_rc_infer<<<grid, kTile, kSmemInfer, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, n, c->bounds, out, c->err,
+                                               n_dev);
   const int rc = cuda_ok(c, cudaGetLastError(), "radiance cache inference");
   if (rc && !c->pending) c->pending = rc;
   return rc;
@@ -714,7 +716,7 @@ int ap_rc_infer(void* cp, const float* queries, uint32_t n, float* out_rgb) {
   int rc = ap::ensure_batch(c, n);
   if (rc) return rc;
   cudaMemcpyAsync(c->queries, queries, (size_t)n * 64, cudaMemcpyHostToDevice, c->stream);
-  if ((rc = ap::rc_infer_device(c, c->queries, n, c->out, c->stream))) return rc;
+  if ((rc = ap::rc_infer_device(c, c->queries, n, c->out, c->stream, nullptr))) return rc;
   cudaMemcpyAsync(out_rgb, c->out, (size_t)n * 12, cudaMemcpyDeviceToHost, c->stream);
   uint32_t e = 0;
   cudaMemcpyAsync(&e, c->err, 4, cudaMemcpyDeviceToHost, c->stream);

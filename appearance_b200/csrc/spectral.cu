@@ -81,13 +81,14 @@ struct SpecBuffers {
   // and triangles only in the counting form)
   unsigned long long* stats;
   // cache mode only
-  float4* cq;       // per path: query of the retired vertex (4 float4)
-  float4* cT;       // per path: throughput at the retired vertex
-  float* cout;      // per path: predicted RGB
+  float4* cq;       // per retired path (compacted): query of its last vertex (4 float4)
+  float4* cT;       //   throughput at that vertex
+  uint32_t* cown;   //   the path
+  float* cout;      //   predicted RGB
   float4* rec;      // per training pixel and round: query (4), throughput, radiance so far, tag
   float4* bq;       // training batch queries
   float* bt;        // training batch targets (RGB)
-  uint32_t* ccount; // [0] candidate records, [1] batch entries
+  uint32_t* ccount; // [0] candidate records, [1] batch entries, [2] retired paths of the pass
 };
 
 constexpr uint32_t kSpecRecord = 7;  // float4 per recorded vertex
@@ -120,16 +121,17 @@ size_t carve(void* base, uint32_t P, const SpectralCache* rc, SpecBuffers* b) {
   b->stats = static_cast<unsigned long long*>(take(6 * sizeof(unsigned long long)));
   b->cq = b->cT = b->rec = b->bq = nullptr;
   b->cout = b->bt = nullptr;
-  b->ccount = nullptr;
+  b->ccount = b->cown = nullptr;
   if (rc) {
     const size_t slots = ((size_t)P / rc->stride + 1) * kRcMaxBounces;
     b->cq = static_cast<float4*>(take(4 * f4));
     b->cT = static_cast<float4*>(take(f4));
+    b->cown = static_cast<uint32_t*>(take(sizeof(uint32_t) * (size_t)P));
     b->cout = static_cast<float*>(take(3 * sizeof(float) * (size_t)P));
     b->rec = static_cast<float4*>(take(sizeof(float4) * kSpecRecord * slots));
     b->bq = static_cast<float4*>(take(sizeof(float4) * 4 * (size_t)rc->batch));
     b->bt = static_cast<float*>(take(sizeof(float) * 3 * (size_t)rc->batch));
-    b->ccount = static_cast<uint32_t*>(take(2 * sizeof(uint32_t)));
+    b->ccount = static_cast<uint32_t*>(take(3 * sizeof(uint32_t)));
   }
   return off;
 }
@@ -295,25 +297,32 @@ __global__ void __launch_bounds__(kBlock) k_svertex(DevScene s, SpecBuffers b, S
       r[4] = b.beta[p];
       r[5] = b.L[p];
       r[6] = make_float4((float)(pass + 1), 0.0f, 0.0f, 0.0f);  // tag: the pass that wrote it
-    } else {
-      float4* dst = b.cq + 4 * (size_t)p;
+    } else {  // retired: its query goes to the next compact slot (one atomic per warp)
+      const unsigned m = __activemask();
+      const int lane = (int)lane_id(), leader = __ffs(m) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(&b.ccount[2], (uint32_t)__popc(m));
+      const uint32_t j = __shfl_sync(m, base, leader) + __popc(m & ((1u << lane) - 1u));
+      float4* dst = b.cq + 4 * (size_t)j;
       dst[0] = q[0]; dst[1] = q[1]; dst[2] = q[2]; dst[3] = q[3];
-      b.cT[p] = b.beta[p];
-      b.misc[p].w = 1u;  // retired
+      b.cT[j] = b.beta[p];
+      b.cown[j] = p;
       b.hits[i].y = kRcRetired;
     }
   }
 }
 
-// L += throughput x the prediction, upsampled to the path's wavelengths.
+// For each retired path: L += throughput x the prediction, upsampled to the
+// path's wavelengths.
 __global__ void __launch_bounds__(kBlock) k_sapply(SpectralView v, SpecBuffers b, uint32_t P) {
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P || b.misc[p].w == 0u) return;
-  float rgb[3] = {b.cout[3 * (size_t)p], b.cout[3 * (size_t)p + 1], b.cout[3 * (size_t)p + 2]};
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= min(b.ccount[2], P)) return;
+  const uint32_t p = b.cown[j];
+  float rgb[3] = {b.cout[3 * (size_t)j], b.cout[3 * (size_t)j + 1], b.cout[3 * (size_t)j + 2]};
   float c[4];
   spec::illum_lookup(v.illum_tab, v.illum_norm, rgb, c);
   const spec::S4 Lc = spec::emission4(c, c[3], s4of(b.lambda[p]));
-  b.L[p] = f4(s4of(b.L[p]) + s4of(b.cT[p]) * Lc);
+  b.L[p] = f4(s4of(b.L[p]) + s4of(b.cT[j]) * Lc);
 }
 
 __global__ void k_scount(SpecBuffers b, SpectralCache rc, uint32_t slots, float tag) {
@@ -401,6 +410,7 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
   cudaMemsetAsync(b.stats, 0, 6 * sizeof(unsigned long long), st);
   for (uint32_t k = 0; k < spp; ++k) {
     cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * 4 * (rounds + 1), st);
+    if (rc) cudaMemsetAsync(b.ccount + 2, 0, sizeof(uint32_t), st);
     k_sgen<<<linear, kBlock, 0, st>>>(b, cam, W, H, row0, P, k, seed);
     ++launches;
     for (uint32_t r = 0; r < rounds; ++r) {
@@ -416,7 +426,7 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
       launches += 3;
     }
     if (rc) {
-      rc_infer_device(rc->cache, b.cq, P, b.cout, st);
+      rc_infer_device(rc->cache, b.cq, P, b.cout, st, b.ccount + 2);  // the retired queries only
       k_sapply<<<linear, kBlock, 0, st>>>(v, b, P);
       launches += 2;
       if (rc->train) {
