@@ -1552,10 +1552,16 @@ __global__ void __launch_bounds__(kBlock) k_rc_vertex(DevScene s, FrameBuffers f
       r[0] = q[0]; r[1] = q[1]; r[2] = q[2]; r[3] = q[3];
       r[4] = make_float4(T.x, T.y, T.z, 0.0f);
       r[5] = make_float4(acc.x, acc.y, acc.z, (float)(c.sample + 1));  // tag: the sample that wrote it
-    } else {
-      float4* dst = rc.q + 4 * (size_t)id;
+    } else {  // retired: its query goes to the next compact slot (one atomic per warp)
+      const unsigned am = __activemask();
+      const int lane = (int)lane_id(), leader = __ffs(am) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(&rc.counts[2], (uint32_t)__popc(am));
+      const uint32_t j = __shfl_sync(am, base, leader) + __popc(am & ((1u << lane) - 1u));
+      float4* dst = rc.q + 4 * (size_t)j;
       dst[0] = q[0]; dst[1] = q[1]; dst[2] = q[2]; dst[3] = q[3];
-      rc.T[id] = make_float4(T.x, T.y, T.z, 1.0f);
+      rc.T[j] = make_float4(T.x, T.y, T.z, 1.0f);
+      rc.own[j] = id;
       fb.hits[id].w = kRcRetired;
     }
   }
@@ -1600,11 +1606,11 @@ __global__ void k_rc_batch(FrameBuffers fb, RcFrame rc, uint32_t slots, uint32_t
 
 // Adds throughput x predicted radiance to every retired path's pixel.
 __global__ void k_rc_apply(FrameBuffers fb, RcFrame rc, uint32_t P) {
-  uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= P) return;
-  const float4 T = rc.T[id];
-  if (T.w == 0.0f) return;
-  const float3 L = f3(rc.out[3 * id], rc.out[3 * id + 1], rc.out[3 * id + 2]);
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= min(rc.counts[2], P)) return;
+  const uint32_t id = rc.own[j];
+  const float4 T = rc.T[j];
+  const float3 L = f3(rc.out[3 * (size_t)j], rc.out[3 * (size_t)j + 1], rc.out[3 * (size_t)j + 2]);
   fb.radiance[id] = pack_rgb9e5(unpack_rgb9e5(fb.radiance[id]) + f3(T.x, T.y, T.z) * L);
 }
 
@@ -2066,7 +2072,8 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
 size_t rc_frame_bytes(uint32_t W, uint32_t H, uint32_t stride, uint32_t batch) {
   const size_t P = (size_t)W * H, slots = ((P + stride - 1) / stride) * kRcMaxBounces;
   auto a = [](size_t b) { return ((b + 255) / 256) * 256; };
-  return a(P * 64) + a(P * 16) + a(P * 12) + a(slots * 96) + a((size_t)batch * 64) + a((size_t)batch * 12) + a(8);
+  return a(P * 64) + a(P * 16) + a(P * 4) + a(P * 12) + a(slots * 96) + a((size_t)batch * 64) + a((size_t)batch * 12) +
+         a(12);
 }
 
 void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_t batch, RcFrame* rc) {
@@ -2074,11 +2081,12 @@ void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_
   const size_t P = (size_t)W * H, slots = ((P + stride - 1) / stride) * kRcMaxBounces;
   rc->q = carve<float4>(p, 4 * P);
   rc->T = carve<float4>(p, P);
+  rc->own = carve<uint32_t>(p, P);
   rc->out = carve<float>(p, 3 * P);
   rc->rec = carve<float4>(p, 6 * slots);
   rc->bq = carve<float4>(p, 4 * (size_t)batch);
   rc->bt = carve<float>(p, 3 * (size_t)batch);
-  rc->counts = carve<uint32_t>(p, 2);
+  rc->counts = carve<uint32_t>(p, 3);
 }
 
 const char* kernel_kind_name(int k) {
@@ -2133,16 +2141,15 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
   const bool cache = rc && rc->cache && cfg.max_bounces > rc->prefix;
   const uint32_t rc_slots = cache ? ((P + rc->stride - 1) / rc->stride) * kRcMaxBounces : 0;
   if (cache) {
-    cudaMemsetAsync(rc->T, 0, (size_t)P * sizeof(float4), st);
     cudaMemsetAsync(rc->rec, 0, (size_t)rc_slots * 6 * sizeof(float4), st);
-    cudaMemsetAsync(rc->counts, 0, 2 * sizeof(uint32_t), st);
+    cudaMemsetAsync(rc->counts, 0, 3 * sizeof(uint32_t), st);
     mark(K_MEMSET);
   }
   for (uint32_t sample = 0; sample < cfg.sample_count; ++sample) {
     c.seed = frame_idx * cfg.sample_count + sample;
     c.sample = sample;
     if (cache) {
-      cudaMemsetAsync(rc->T, 0, (size_t)P * sizeof(float4), st);  // retired-path flags of this sample
+      cudaMemsetAsync(rc->counts + 2, 0, sizeof(uint32_t), st);  // retired paths of this sample
       mark(K_MEMSET);
     }
     k_raygen<<<g2, b2, 0, st>>>(fb, W, H, mats);
@@ -2291,7 +2298,7 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       }
     }
     if (cache) {  // this sample's retired paths: predicted radiance on the tensor cores
-      rc_infer_device(rc->cache, rc->q, P, rc->out, st);
+      rc_infer_device(rc->cache, rc->q, P, rc->out, st, rc->counts + 2);  // the retired queries only
       mark(K_RC_INFER);
       k_rc_apply<<<(P + 255) / 256, 256, 0, st>>>(fb, *rc, P);
       mark(K_RC);

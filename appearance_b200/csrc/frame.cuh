@@ -114,13 +114,14 @@ struct RcFrame {
   uint32_t prefix = 2, stride = 16, batch = 65536;
   float lr = 1e-3f;
   int train = 1;
-  float4* q = nullptr;       // per pixel: query of the retired path (4 float4)
-  float4* T = nullptr;       // per pixel: throughput at the retired vertex; w = 1 when retired
-  float* out = nullptr;      // per pixel: predicted RGB
+  float4* q = nullptr;       // per retired path (compacted): query of its last vertex (4 float4)
+  float4* T = nullptr;       //   throughput at that vertex
+  uint32_t* own = nullptr;   //   its pixel
+  float* out = nullptr;      //   predicted RGB
   float4* rec = nullptr;     // per training pixel and bounce: query (4), throughput (1), radiance so far (1; w = valid)
   float4* bq = nullptr;      // training batch queries (batch x 4)
   float* bt = nullptr;       // training batch targets (batch x 3)
-  uint32_t* counts = nullptr;  // [0] candidate records, [1] batch entries
+  uint32_t* counts = nullptr;  // [0] candidate records, [1] batch entries, [2] retired paths of the sample
 };
 constexpr uint32_t kRcMaxBounces = 8;        // record slots per training pixel
 constexpr uint32_t kRcRetired = 0xFFFFFFFEu;  // hit id of a path retired into the cache
