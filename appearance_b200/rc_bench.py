@@ -9,7 +9,7 @@ fixed camera, and their relMSE = mean((x - ref)^2 / (ref^2 + 0.01)) against a
 against accumulated device time.  Reported: relMSE at equal time, and the time
 the plain tracer needs to reach the cache's relMSE.
 
-    python -m appearance_b200.rc_bench [--scenes cornell,field] [--budget-ms 400]
+    python -m appearance_b200.rc_bench [--scenes cornell,field] [--budget-ms 400] [--study-size 480x270]
 """
 from __future__ import annotations
 
@@ -84,8 +84,7 @@ def time_to(curve, target):
     return None
 
 
-def study(name, budget_ms, warm_frames):
-    w, h = 480, 270
+def study(name, budget_ms, warm_frames, w=480, h=270):
     sc, mats, lo, hi = scene_setup(name, w, h)
     pt = tracer(sc, mats, dict(PLAIN, sample_count=16))
     ref = np.zeros((h, w, 3))
@@ -129,18 +128,23 @@ def main(argv=None):
     ap.add_argument("--scenes", default="cornell,field")
     ap.add_argument("--budget-ms", type=float, default=400.0)
     ap.add_argument("--warm-frames", type=int, default=200)
+    ap.add_argument("--study-size", default="480x270", help="resolution of the equal-time study, WxH")
+    ap.add_argument("--skip-frame-ms", action="store_true", help="only the equal-time study")
     a = ap.parse_args(argv)
+    sw, sh = (int(v) for v in a.study_size.split("x"))
     result = {"metric": "radiance cache vs plain full-depth tracer", "config": {
         "mlp": "144 -> 4x64 ReLU -> 3 exp, FP16 weights/activations, FP32 accumulation (tcgen05)",
         "training": "2^16 suffix vertices per frame from 1/16 of the pixels, Adam lr 1e-3, relative L2",
         "plain": "1 spp, depth 8, RIS next-event estimation, no reuse or denoising"}}
     for name in a.scenes.split(","):
         w, h = 1920, 1080
-        sc, mats, lo, hi = scene_setup(name, w, h)
-        r = {"frame_ms_1080p": {"plain": frame_ms(sc, mats, w, h),
-                                "cache_prefix2": frame_ms(sc, mats, w, h, 2, lo, hi),
-                                "cache_prefix1": frame_ms(sc, mats, w, h, 1, lo, hi)}}
-        r["equal_time_480x270"] = study(name, a.budget_ms, a.warm_frames)
+        r = {}
+        if not a.skip_frame_ms:
+            sc, mats, lo, hi = scene_setup(name, w, h)
+            r["frame_ms_1080p"] = {"plain": frame_ms(sc, mats, w, h),
+                                   "cache_prefix2": frame_ms(sc, mats, w, h, 2, lo, hi),
+                                   "cache_prefix1": frame_ms(sc, mats, w, h, 1, lo, hi)}
+        r[f"equal_time_{sw}x{sh}"] = study(name, a.budget_ms, a.warm_frames, sw, sh)
         result[name] = r
         print(json.dumps({name: r}), flush=True)
     print(json.dumps(result), flush=True)
