@@ -9,8 +9,9 @@ passes), TAA, camera moving along a 64-frame seeded spline.  Metric: Msamples/s 
 
   value   device time of the frames (CUDA events on the renderer's stream),
           scene and frame state resident in HBM.
-  e2e     the same frames through the public C ABI call ap_render_hdr with a
-          host output buffer (page-locked, allocated once): per frame the
+  e2e     the same camera frames again through the public C ABI call
+          ap_render_hdr with a host output buffer (page-locked, allocated
+          once): per frame the
           camera goes host->device and the 1920x1080 RGB f32 framebuffer comes
           back device->host.
 
@@ -226,6 +227,7 @@ def main():
     # timed device-resident frames; the output (24.9 MB) exceeds nothing in L2 reuse terms:
     # every frame rewrites ~1 GB of per-pixel state, far beyond the 126 MB L2.
     clocks = ClockSampler(local)
+    f0, prev0 = f, prev  # the e2e pass below renders the same camera frames
     barrier()
     clocks.start()
     gpu_ms = []
@@ -244,7 +246,8 @@ def main():
     # the caller's output buffer: page-locked host memory, allocated once
     out = torch.empty((H_FULL, W_FULL, 3), dtype=torch.float32, pin_memory=True).numpy()
     e2e_t = []
-    for _ in range(max(2, args.steps // 2)):
+    f, prev = f0, prev0
+    for _ in range(args.steps):
         mats, prev = frame_mats(path, f, prev, W_FULL, H_FULL)
         t1 = time.perf_counter()
         pt.set_camera_matrices(mats)
