@@ -11,9 +11,8 @@ passes), TAA, camera moving along a 64-frame seeded spline.  Metric: Msamples/s 
           scene and frame state resident in HBM.
   e2e     the same camera frames again through the public C ABI call
           ap_render_hdr with a host output buffer (page-locked, allocated
-          once): per frame the
-          camera goes host->device and the 1920x1080 RGB f32 framebuffer comes
-          back device->host.
+          once): per frame the camera goes host->device and the 1920x1080 RGB
+          f32 framebuffer comes back device->host.
 
 Run with torchrun for N>1: every rank renders its own independent replica of
 the job (the frame does not shard), so scaling is weak and value sums ranks.
