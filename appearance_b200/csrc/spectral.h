@@ -151,10 +151,21 @@ SPHD S4 albedo4(const float* c, const S4& lambda) {
   for (int i = 0; i < 4; ++i) r.v[i] = sigmoid_poly(c, lambda.v[i]);
   return r;
 }
-SPHD S4 emission4(const float* c, float scale, const S4& lambda) {
+SPHD S4 illuminant4(const S4& lambda) {
   S4 r;
-  for (int i = 0; i < 4; ++i) r.v[i] = scale * sigmoid_poly(c, lambda.v[i]) * illuminant(lambda.v[i]);
+  for (int i = 0; i < 4; ++i) r.v[i] = illuminant(lambda.v[i]);
   return r;
+}
+// emission4 with the illuminant at the four wavelengths given (illuminant4):
+// the same products in the same order, for callers evaluating several spectra
+// at one set of wavelengths.
+SPHD S4 emission4_ill(const float* c, float scale, const S4& lambda, const S4& ill) {
+  S4 r;
+  for (int i = 0; i < 4; ++i) r.v[i] = scale * sigmoid_poly(c, lambda.v[i]) * ill.v[i];
+  return r;
+}
+SPHD S4 emission4(const float* c, float scale, const S4& lambda) {
+  return emission4_ill(c, scale, lambda, illuminant4(lambda));
 }
 
 // Unbounded RGB (an emitter's radiance, an environment texel, a predicted
@@ -422,6 +433,7 @@ SPHD S4 env_le(const Geo& g, V3 d, const S4& lambda) {
   float fx = dm::floor_(x), fy = dm::floor_(y);
   float ax = x - fx, ay = y - fy;
   int x0 = (int)fx, y0 = (int)fy;
+  const S4 ill = illuminant4(lambda);
   S4 acc = s4(0.0f);
   for (int k = 0; k < 4; ++k) {
     int xi = x0 + (k & 1), yi = y0 + (k >> 1);
@@ -430,7 +442,7 @@ SPHD S4 env_le(const Geo& g, V3 d, const S4& lambda) {
     float wgt = ((k & 1) ? ax : 1.0f - ax) * ((k >> 1) ? ay : 1.0f - ay);
     float c[4];
     g.env_texel((uint32_t)yi * g.env_w + (uint32_t)xi, c);
-    acc = acc + emission4(c, c[3], lambda) * wgt;
+    acc = acc + emission4_ill(c, c[3], lambda, ill) * wgt;
   }
   return acc * g.env_scale;
 }
