@@ -7,9 +7,8 @@ crop against a high-spp reference of that crop accumulated in float64; with
 --cache the same for the radiance-cache mode (paths ended at their first
 bounce's hit in the online-trained cache).
 
-The CPU figure (--cpu-rows > 0) is the oracle's restatement of the same
-integrator on all host threads over a band of rows of the crop at 1 spp,
-extrapolated to Msamples/s.
+The CPU figure beside it (the oracle's restatement of the same integrator on
+all host threads over a band of rows at 1 spp) is taken by bench.py.
 
     python -m appearance_b200.spectral_bench [--lots 64] [--size 4096] [--spp 64]
 """
@@ -17,7 +16,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import os
 import time
 
 import numpy as np
@@ -56,7 +54,10 @@ def render_bands(pt, size, spp, depth, seed, band, to_host=False):
 
 
 def measure(lots=64, size=4096, spp=64, depth=16, band=4096, repeats=1, quality=False, ref_spp=4096,
-            cpu_rows=0, cache=False, cache_prefix=1) -> dict:
+            cache=False, cache_prefix=1, keep_scene=None) -> dict:
+    """The measurements above as a dict; `keep_scene` (a dict), when given,
+    receives the scene, camera matrices and light parameters for a caller's
+    own comparison run."""
     sc, mats, gen_s = setup(lots, size)
     pt = PathTracer(presets.PLAIN)
     t0 = time.perf_counter()
@@ -125,18 +126,8 @@ def measure(lots=64, size=4096, spp=64, depth=16, band=4096, repeats=1, quality=
         pt.attach_radiance_cache(None)
         rc.close()
     pt.close()
-    if cpu_rows > 0:
-        from oracle.oracle import OracleScene, OracleSpectral  # the CPU baseline only
-        osp = OracleSpectral(OracleScene(sc), scene_radius=radius, **SUN)
-        r0 = size // 2 - cpu_rows // 2
-        threads = os.cpu_count()
-        t0 = time.perf_counter()
-        osp.render(mats, size, size, spp=1, max_depth=depth, seed=100, row0=r0, row1=r0 + cpu_rows,
-                   threads=threads)
-        dt = time.perf_counter() - t0
-        res["cpu_baseline"] = {"value": cpu_rows * size / dt / 1e6, "unit": "Msamples/s", "cores": threads,
-                               "kind": "port", "sample": f"oracle, rows {r0}..{r0 + cpu_rows} of the {size}^2 "
-                                                         f"image (full width) at 1 spp, {dt:.1f} s"}
+    if keep_scene is not None:
+        keep_scene.update(scene=sc, mats=mats, light=dict(scene_radius=radius, **SUN), size=size, depth=depth)
     return res
 
 
@@ -150,12 +141,10 @@ def main(argv=None):
     ap.add_argument("--repeats", type=int, default=1)
     ap.add_argument("--quality", action="store_true", help="relMSE of the crop against a high-spp reference")
     ap.add_argument("--ref-spp", type=int, default=4096)
-    ap.add_argument("--cpu-rows", type=int, default=0, help="rows of the crop rendered by the CPU oracle")
     ap.add_argument("--cache", action="store_true", help="also run the radiance-cache mode")
     ap.add_argument("--cache-prefix", type=int, default=1)
     a = ap.parse_args(argv)
-    res = measure(a.lots, a.size, a.spp, a.depth, a.band, a.repeats, a.quality, a.ref_spp, a.cpu_rows, a.cache,
-                  a.cache_prefix)
+    res = measure(a.lots, a.size, a.spp, a.depth, a.band, a.repeats, a.quality, a.ref_spp, a.cache, a.cache_prefix)
     print(json.dumps(res), flush=True)
     return res
 

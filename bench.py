@@ -339,7 +339,21 @@ def city_spectral_config(cpu: bool) -> dict:
     cache, after 8 training passes).  The CPU oracle of the same integrator
     renders 64 full-width rows at 1 spp beside it."""
     from appearance_b200 import spectral_bench
-    return spectral_bench.measure(cpu_rows=64 if cpu else 0, cache=True)
+    kept = {}
+    res = spectral_bench.measure(cache=True, keep_scene=kept if cpu else None)
+    if cpu:
+        from oracle.oracle import OracleScene, OracleSpectral
+        rows, size, threads = 64, kept["size"], os.cpu_count()
+        osp = OracleSpectral(OracleScene(kept["scene"]), **kept["light"])
+        r0 = size // 2 - rows // 2
+        t0 = time.perf_counter()
+        osp.render(kept["mats"], size, size, spp=1, max_depth=kept["depth"], seed=100, row0=r0, row1=r0 + rows,
+                   threads=threads)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": rows * size / dt / 1e6, "unit": "Msamples/s", "cores": threads, "kind": "port",
+                               "sample": f"oracle, rows {r0}..{r0 + rows} of the {size}^2 image (full width) at 1 spp, "
+                                         f"{dt:.1f} s"}
+    return res
 
 
 def measure_details(pt, scene, path, cfg) -> dict:
