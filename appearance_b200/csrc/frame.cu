@@ -330,7 +330,7 @@ APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& f
 }
 
 #ifndef AP_SHADE_A_MIN_BLOCKS
-#define AP_SHADE_A_MIN_BLOCKS 8  // resident blocks per SM the kernel is register-capped for (measured)
+#define AP_SHADE_A_MIN_BLOCKS 10  // resident blocks per SM the kernel is register-capped for (measured)
 #endif
 __global__ void __launch_bounds__(kBlock, AP_SHADE_A_MIN_BLOCKS) k_shade_a(DevScene s, FrameBuffers fb, Consts c, Mats mats) {
   __shared__ uint4 s_lights[kSmemLights];
