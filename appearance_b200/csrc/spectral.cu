@@ -196,7 +196,11 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s,
       });
 }
 
-__global__ void __launch_bounds__(kBlock) k_sshade(DevScene s, SpectralView v, SpecBuffers b, uint32_t round,
+#ifndef AP_SSHADE_MIN_BLOCKS
+#define AP_SSHADE_MIN_BLOCKS 8  // resident blocks per SM the shading kernel is register-capped for (measured)
+#endif
+__global__ void __launch_bounds__(kBlock, AP_SSHADE_MIN_BLOCKS) k_sshade(DevScene s, SpectralView v, SpecBuffers b,
+                                                                     uint32_t round,
                                                    uint32_t P, int max_depth) {
   const uint32_t count = round == 0 ? P : min(b.counters[4 * round], P);
   const float4* qo = b.rq_o[round & 1];
