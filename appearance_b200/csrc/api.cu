@@ -65,6 +65,7 @@ struct Handle {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  FrameStreams fs;  // second stream of the frame (DI shadow rays beside the next extension)
   std::string err;
   DeviceScene scene;
   void* frame_mem = nullptr;
@@ -294,7 +295,7 @@ int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats, Fr
   compute_mats(h, w, hgt);
   cudaEventRecord(h->ev0, h->stream);
   int launches = encode_frame(h->scene.view, h->fb, h->cfg, h->mats, w, hgt, h->frame_idx, h->num_sms, h->stream, prof,
-                              h->rc.cache ? &h->rc : nullptr);
+                              h->rc.cache ? &h->rc : nullptr, &h->fs);
   cudaEventRecord(h->ev1, h->stream);
   uint32_t rays = 0;
   cudaMemcpyAsync(&rays, h->fb.counters + 3, 4, cudaMemcpyDeviceToHost, h->stream);
@@ -388,8 +389,12 @@ void* ap_create(const ap_frame_config* cfg, int device, int* err) {
   if (cfg) std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
   else ap_frame_config_default(reinterpret_cast<ap_frame_config*>(&h->cfg));
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
+      frame_streams_create(&h->fs) != 0) {
     *err = AP_E_CUDA;
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return nullptr;
   }
@@ -410,6 +415,7 @@ void ap_destroy(void* hp) {
   if (h->spec_out) cudaFree(h->spec_out);
   if (h->prof.created)
     for (int i = 0; i <= FrameProfiler::kMax; ++i) cudaEventDestroy(h->prof.ev[i]);
+  frame_streams_destroy(&h->fs);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -275,6 +275,40 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_queue(DevScen
       });
 }
 
+// Persistent any-hit traversal of two ray queues in one launch: rays [0, n0)
+// of the combined range come from queue Q0, the rest from Q1, each result
+// going to its own queue's visibility array.  One launch instead of two
+// saves a launch and the second drain tail; every ray's result is the same.
+template <int Q0, int Q1, bool kCount>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_pair(DevScene s, FrameBuffers fb, uint32_t cap) {
+  const uint32_t n0 = min(fb.counters[kCounterQueueSize + Q0], cap);
+  const uint32_t count = n0 + min(fb.counters[kCounterQueueSize + Q1], cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fb.counters[3], count);
+  const float4 *o0 = fb.rq_o[Q0], *d0 = fb.rq_d[Q0], *o1 = fb.rq_o[Q1], *d1 = fb.rq_d[Q1];
+  uint8_t *v0 = fb.vis[Q0], *v1 = fb.vis[Q1];
+  persistent_trace<true, kCount>(
+      s, count, &fb.counters[kCounterQueueCursor + Q0],
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        const bool first = i < n0;
+        const uint32_t j = first ? i : i - n0;
+        const float4 a = (first ? o0 : o1)[j], b = (first ? d0 : d1)[j];
+        o = f3(a.x, a.y, a.z);
+        d = f3(b.x, b.y, b.z);
+        tmax = a.w;
+      },
+      [&](uint32_t i, const Trav& t, const Visits& vc) {
+        const bool first = i < n0;
+        const uint32_t j = first ? i : i - n0;
+        const uint32_t owner = __float_as_uint((first ? d0 : d1)[j].w);
+        (first ? v0 : v1)[owner] = t.hit.tri != kNoHit ? 0 : 1;
+        if (kCount) {
+          atomicAdd(&fb.visits[3 * K_TRACE_ANY + 0], 1ull);
+          atomicAdd(&fb.visits[3 * K_TRACE_ANY + 1], (unsigned long long)vc.nodes);
+          atomicAdd(&fb.visits[3 * K_TRACE_ANY + 2], (unsigned long long)vc.tris);
+        }
+      });
+}
+
 // ---- trace.wgsl:62-262 as four stages around the secondary rays -------------
 //   A: hit attributes, emission, G-buffer, first NEE candidates (area + BSDF);
 //      queues the BSDF candidate ray            (Nee::sample_ris, nee.wgsl:131-197)
@@ -612,13 +646,8 @@ __global__ void __launch_bounds__(kBlock, AP_SHADE_C_MIN_BLOCKS) k_shade_c(DevSc
     bool want = false;
     float3 so = f3s(0.0f), sd = f3s(0.0f);
     float st = 0.0f;
-    if (sa.w & F_RIS_SHADOW) {
-      if (fb.vis[Q_RIS_SHADOW][id]) {
-        uint4 da = fb.di_a[id];
-        float W = (1.0f / __uint_as_float(da.w)) * __uint_as_float(da.z);
-        fb.di_a[id] = make_uint4(da.x, __float_as_uint(W), da.z, da.w);
-      }
-    }
+    // the RIS shadow ray is traced after this stage; k_shade_d applies it
+    const uint32_t ris = sa.w & F_RIS_SHADOW;
     if (sa.w & F_GI_RAY) {
       uint4 pl = fb.payload[id];
       uint32_t rng = pl.y;
@@ -664,17 +693,17 @@ __global__ void __launch_bounds__(kBlock, AP_SHADE_C_MIN_BLOCKS) k_shade_c(DevSc
         acc = acc + tr * sky_radiance(s, wi, true);
       }
       if (want) {
-        fb.st_a[id] = make_uint4(sa.x, sa.y, 0u, F_GI_SHADOW);
+        fb.st_a[id] = make_uint4(sa.x, sa.y, 0u, F_GI_SHADOW | ris);
         fb.st_b[id] = make_uint4(__float_as_uint(point.x), __float_as_uint(point.y), __float_as_uint(point.z), 0u);
         fb.st_c[id] = make_uint4(__float_as_uint(acc.x), __float_as_uint(acc.y), __float_as_uint(acc.z), 0u);
       } else {
         finish_gi(fb, id, acc, gi_pdf, point, phat_rng, rng);
-        fb.st_a[id] = make_uint4(0u, 0u, 0u, 0u);
+        fb.st_a[id] = make_uint4(0u, 0u, 0u, ris);
       }
       pl.y = rng;
       fb.payload[id] = pl;
     } else if (sa.w != 0u) {
-      fb.st_a[id] = make_uint4(0u, 0u, 0u, 0u);
+      fb.st_a[id] = make_uint4(0u, 0u, 0u, ris);
     }
     push_ray(fb, Q_GI_SHADOW, want, so, st, sd, id);
   }
@@ -685,6 +714,16 @@ __global__ void __launch_bounds__(kBlock) k_shade_d(FrameBuffers fb, Consts c) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     uint32_t id = bounce_path(fb, c, i);
     uint4 sa = fb.st_a[id];
+    if (sa.w & F_RIS_SHADOW) {
+      // the resampled light sample is visible: its contribution weight (nee.wgsl)
+      if (fb.vis[Q_RIS_SHADOW][id]) {
+        uint4 da = fb.di_a[id];
+        float W = (1.0f / __uint_as_float(da.w)) * __uint_as_float(da.z);
+        fb.di_a[id] = make_uint4(da.x, __float_as_uint(W), da.z, da.w);
+      }
+      sa.w &= ~F_RIS_SHADOW;
+      fb.st_a[id] = sa;
+    }
     if (!(sa.w & F_GI_SHADOW)) continue;
     uint4 pl = fb.payload[id];
     uint32_t rng = pl.y;
@@ -2105,10 +2144,36 @@ void trace_queue(bool counting, int blocks, cudaStream_t st, const DevScene& sce
   else k_trace_queue<kAny, false><<<blocks, kBlock, 0, st>>>(scene, fb, q, cap, hits, vis);
 }
 
+// The RIS shadow queue and the GI shadow queue, traced by one any-hit launch.
+void trace_shadow_pair(bool counting, int blocks, cudaStream_t st, const DevScene& scene, const FrameBuffers& fb,
+                       uint32_t cap) {
+  if (counting) k_trace_pair<Q_RIS_SHADOW, Q_GI_SHADOW, true><<<blocks, kBlock, 0, st>>>(scene, fb, cap);
+  else k_trace_pair<Q_RIS_SHADOW, Q_GI_SHADOW, false><<<blocks, kBlock, 0, st>>>(scene, fb, cap);
+}
+
+int frame_streams_create(FrameStreams* fs) {
+  cudaError_t e = cudaStreamCreateWithFlags(&fs->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fs->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fs->join, cudaEventDisableTiming);
+  if (e != cudaSuccess) frame_streams_destroy(fs);
+  return (int)e;
+}
+
+void frame_streams_destroy(FrameStreams* fs) {
+  if (fs->side) cudaStreamSynchronize(fs->side);
+  if (fs->fork) cudaEventDestroy(fs->fork);
+  if (fs->join) cudaEventDestroy(fs->join);
+  if (fs->side) cudaStreamDestroy(fs->side);
+  *fs = FrameStreams();
+}
+
 int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t st, FrameProfiler* prof,
-                 const RcFrame* rc) {
+                 const RcFrame* rc, const FrameStreams* fs) {
   int launches = 0;
+  const bool overlap = fs && fs->side && fs->fork && fs->join && !prof;
+  bool di_pending = false;  // a DI shadow pass in flight on fs->side; k_apply_di_b waits for it
+  Consts di_c{};
   const bool counting = prof && prof->count_visits;
   if (counting) cudaMemsetAsync(fb.visits, 0, 3 * K_NUM_KINDS * sizeof(unsigned long long), st);
   if (prof) {
@@ -2163,6 +2228,13 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       if (counting) k_extend<true><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
       else k_extend<false><<<persistent_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_EXTEND);
+      if (di_pending) {  // the previous bounce's DI shadow rays, traced beside this extension
+        cudaEventRecord(fs->join, fs->side);
+        cudaStreamWaitEvent(st, fs->join, 0);
+        k_apply_di_b<<<linear_blocks, kBlock, 0, st>>>(fb, di_c);
+        mark(K_APPLY_DI);
+        di_pending = false;
+      }
       if (cache) {
         k_rc_vertex<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c, *rc);
         mark(K_RC);
@@ -2177,13 +2249,12 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       mark(K_SHADE_B);
       k_shade_b2<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_SHADE_B2);
-      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_RIS_SHADOW, P, nullptr, fb.vis[Q_RIS_SHADOW]);
-      mark(K_TRACE_ANY);
       trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_GI_CAND, P, fb.hit_gi, nullptr);
       mark(K_TRACE_CLOSEST);
       k_shade_c<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_SHADE_C);
-      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, P, nullptr, fb.vis[Q_GI_SHADOW]);
+      // the RIS shadow rays (queued by k_shade_b, read by k_shade_d) with the GI shadow rays
+      trace_shadow_pair(counting, persistent_blocks, st, scene, fb, P);
       mark(K_TRACE_ANY);
       k_shade_d<<<linear_blocks, kBlock, 0, st>>>(fb, c);
       mark(K_SHADE_D);
@@ -2227,10 +2298,7 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
               mark(K_TRACE_ANY);
               k_dsp_b<<<g2, b2, 0, st>>>(scene, fb, c, k, n, in_a, in_b, out_a, out_b);
               mark(K_DI_SPATIAL);
-              trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_RIS_SHADOW, P, nullptr,
-                                fb.vis[Q_RIS_SHADOW]);
-              mark(K_TRACE_ANY);
-              trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, P, nullptr, fb.vis[Q_GI_SHADOW]);
+              trace_shadow_pair(counting, persistent_blocks, st, scene, fb, P);
               mark(K_TRACE_ANY);
             }
           }
@@ -2286,10 +2354,22 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
       }
       k_apply_di_a<<<linear_blocks, kBlock, 0, st>>>(scene, fb, c);
       mark(K_APPLY_DI);
-      trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_DI_SHADOW, P, nullptr, fb.vis[Q_DI_SHADOW]);
-      mark(K_TRACE_ANY);
-      k_apply_di_b<<<linear_blocks, kBlock, 0, st>>>(fb, c);
-      mark(K_APPLY_DI);
+      if (overlap && i + 1 < cfg.max_bounces) {
+        // nothing before the next extension reads these rays' results (k_apply_di_b
+        // follows it, still before the next bounce adds to the radiance)
+        cudaEventRecord(fs->fork, st);
+        cudaStreamWaitEvent(fs->side, fs->fork, 0);
+        trace_queue<true>(false, persistent_blocks, fs->side, scene, fb, Q_DI_SHADOW, P, nullptr,
+                          fb.vis[Q_DI_SHADOW]);
+        mark(K_TRACE_ANY);
+        di_pending = true;
+        di_c = c;
+      } else {
+        trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_DI_SHADOW, P, nullptr, fb.vis[Q_DI_SHADOW]);
+        mark(K_TRACE_ANY);
+        k_apply_di_b<<<linear_blocks, kBlock, 0, st>>>(fb, c);
+        mark(K_APPLY_DI);
+      }
       if (i + 1 < cfg.max_bounces) {
         cudaMemsetAsync(fb.counters + c.qout, 0, 4, st);
         mark(K_MEMSET);

@@ -138,9 +138,21 @@ int rc_train_device(void* cache, const float4* queries, const float* targets, co
 // check, or AP_E_TIMEOUT for an inference wait that ran out; clears it.
 int rc_take_status(void* cache, std::string* msg);
 
+// Optional second stream for encode_frame: the DI shadow rays of every bounce
+// but the last are traced on `side` beside the next bounce's path extension
+// (apply_gi -> extend), which reads none of their results, so one persistent
+// launch's drain tail overlaps the other's work; `fork` and `join` order the
+// two streams.  Ignored while profiling (per-kernel times need one stream).
+struct FrameStreams {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+int frame_streams_create(FrameStreams* fs);  // cudaError_t of the first failing call
+void frame_streams_destroy(FrameStreams* fs);
+
 int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfig& cfg, const Mats& mats,
                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t stream,
-                 FrameProfiler* prof = nullptr, const RcFrame* rc = nullptr);
+                 FrameProfiler* prof = nullptr, const RcFrame* rc = nullptr, const FrameStreams* fs = nullptr);
 
 // Closest / any hit for a batch of rays (parity tests and traversal bench).
 // rays: origin.xyz + tmax (float4), dirs: float4; out: t, u, v, tri bits.
