@@ -118,7 +118,10 @@ typedef struct ap_frame_stats {
 /* Fills the reference defaults (PathTracerGpuConfig::default + pass literals). */
 void ap_frame_config_default(ap_frame_config* cfg);
 
-/* PathTracerGpu::new (lib.rs:260-281).  Returns NULL and sets *err on failure. */
+/* PathTracerGpu::new (lib.rs:260-281).  Returns NULL and sets *err on failure.
+ * The handle owns two non-blocking CUDA streams on `device` (the frame's, and
+ * a second one for traversal that overlaps the next bounce); both are idle
+ * when a render call returns. */
 void* ap_create(const ap_frame_config* cfg, int device, int* err);
 void ap_destroy(void* handle);
 const char* ap_last_error(const void* handle);
