@@ -169,3 +169,28 @@ def test_render_into_caller_buffer():
         b.render((w, h), 3, 12, out=part)
     a.close()
     b.close()
+
+
+def test_second_stream_frames_equal_one_stream_frames():
+    """A render traces the DI shadow rays of every bounce but the last on the
+    handle's second stream, beside the next bounce's extension; a profiled frame
+    runs every launch on one stream.  Both orders leave every per-path state
+    buffer bit-identical, frame after frame (320x180, the benchmark scene and
+    preset)."""
+    sc = scenes.icosphere_field(seed=0, env_size=(512, 256))
+    w, h = 320, 180
+    path = scenes.camera_spline(seed=0, frames=64)
+    a = PathTracer(dict(presets.REALTIME))
+    b = PathTracer(dict(presets.REALTIME))
+    a.upload_scene(sc)
+    b.upload_scene(sc)
+    prev = None
+    for f in range(3):
+        mats, prev = scenes.camera_matrices(path[f][0], path[f][1], 60.0, 0.01, 1000.0, w, h, prev)
+        a.set_camera_matrices(mats)
+        b.set_camera_matrices(mats)
+        a.render_device(w, h)
+        b.profile_frame(w, h)
+        for which, (name, gw, _) in BUFFERS.items():
+            assert_bits(a.read_buffer(which, gw, w * h), b.read_buffer(which, gw, w * h), f"{name} frame {f}")
+    assert a.last_stats.extension_rays == b.last_stats.extension_rays
