@@ -929,7 +929,7 @@ int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
   cudaEventRecord(h->ev0, h->stream);
   const int launches = launch_spectral(h->scene.view, h->spec, cam, w, hgt, row_start, row_end, spp, (int)max_depth,
                                        seed, static_cast<float*>(h->spec_out), work, h->num_sms, visits6 != nullptr,
-                                       rcp, h->stream);
+                                       rcp, h->stream, &h->fs);
   cudaEventRecord(h->ev1, h->stream);
   int rc = check_cuda(h, cudaGetLastError(), "spectral launch");
   if (rc) return rc;

@@ -400,8 +400,11 @@ const unsigned long long* spectral_stats(void* work, uint32_t P, const SpectralC
 
 int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCamera& cam, uint32_t W, uint32_t H,
                     uint32_t row0, uint32_t row1, uint32_t spp, int max_depth, uint32_t seed, float* out, void* work,
-                    int num_sms, bool count_visits, const SpectralCache* rc, cudaStream_t st) {
+                    int num_sms, bool count_visits, const SpectralCache* rc, cudaStream_t st,
+                    const FrameStreams* fs) {
   const uint32_t P = W * (row1 - row0);
+  const bool overlap = fs && fs->side && fs->fork && fs->join && !count_visits;
+  bool shadow_pending = false;  // a shadow pass in flight on fs->side
   SpecBuffers b;
   carve(work, P, rc, &b);
   const uint32_t slots = rc ? (P / rc->stride + 1) * kRcMaxBounces : 0u;
@@ -420,13 +423,27 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
     for (uint32_t r = 0; r < rounds; ++r) {
       if (count_visits) k_sextend<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
       else k_sextend<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      if (shadow_pending) {  // the previous round's shadow rays, traced beside this extension
+        cudaEventRecord(fs->join, fs->side);
+        cudaStreamWaitEvent(st, fs->join, 0);
+        shadow_pending = false;
+      }
       if (rc) {
         k_svertex<<<shade, kBlock, 0, st>>>(s, b, *rc, r, P, k, seed);
         ++launches;
       }
       k_sshade<<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth);
-      if (count_visits) k_sshadow<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
-      else k_sshadow<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      if (overlap && r + 1 < rounds) {
+        // only the next shading pass reads what these rays add to L
+        cudaEventRecord(fs->fork, st);
+        cudaStreamWaitEvent(fs->side, fs->fork, 0);
+        k_sshadow<false><<<persistent, kBlock, 0, fs->side>>>(s, b, r, P);
+        shadow_pending = true;
+      } else if (count_visits) {
+        k_sshadow<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      } else {
+        k_sshadow<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      }
       launches += 3;
     }
     if (rc) {
