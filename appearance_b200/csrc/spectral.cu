@@ -387,9 +387,12 @@ __global__ void __launch_bounds__(kBlock) k_saccum(SpecBuffers b, uint32_t P, bo
 
 }  // namespace
 
+// Without the cache the work area holds a second set of path state, so that
+// two sample passes can be in flight (launch_spectral).
 size_t spectral_work_bytes(uint32_t P, const SpectralCache* rc) {
   SpecBuffers b;
-  return carve(nullptr, P, rc, &b);
+  const size_t one = carve(nullptr, P, rc, &b);
+  return rc ? one : 2 * one;
 }
 
 const unsigned long long* spectral_stats(void* work, uint32_t P, const SpectralCache* rc) {
@@ -404,9 +407,20 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
                     const FrameStreams* fs) {
   const uint32_t P = W * (row1 - row0);
   const bool overlap = fs && fs->side && fs->fork && fs->join && !count_visits;
+  // Two sample passes in flight: even samples on `st`, odd ones on fs->side,
+  // each with its own path state; the accumulator and the counters are
+  // shared, and every pass adds to the accumulator after the previous pass
+  // did (an event between the streams), so the sum's order is unchanged.
+  const bool pipe = overlap && !rc && spp > 1;
   bool shadow_pending = false;  // a shadow pass in flight on fs->side
-  SpecBuffers b;
-  carve(work, P, rc, &b);
+  SpecBuffers bufs[2];
+  const size_t set_bytes = carve(work, P, rc, &bufs[0]);
+  if (pipe) {
+    carve(static_cast<char*>(work) + set_bytes, P, nullptr, &bufs[1]);
+    bufs[1].acc = bufs[0].acc;
+    bufs[1].stats = bufs[0].stats;
+  }
+  SpecBuffers& b = bufs[0];
   const uint32_t slots = rc ? (P / rc->stride + 1) * kRcMaxBounces : 0u;
   if (rc) cudaMemsetAsync(b.rec, 0, sizeof(float4) * kSpecRecord * slots, st);  // no tags from an earlier call
   const uint32_t rounds = (uint32_t)max_depth + 1;
@@ -415,6 +429,31 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
   const int shade = std::min(linear, num_sms * 16);
   int launches = 0;
   cudaMemsetAsync(b.stats, 0, 6 * sizeof(unsigned long long), st);
+  if (pipe) {
+    cudaEventRecord(fs->fork, st);
+    cudaStreamWaitEvent(fs->side, fs->fork, 0);
+    for (uint32_t k = 0; k < spp; ++k) {
+      const int h = (int)(k & 1u);
+      const cudaStream_t sk = h ? fs->side : st;
+      const SpecBuffers& bk = bufs[h];
+      cudaMemsetAsync(bk.counters, 0, sizeof(uint32_t) * 4 * (rounds + 1), sk);
+      k_sgen<<<linear, kBlock, 0, sk>>>(bk, cam, W, H, row0, P, k, seed);
+      ++launches;
+      for (uint32_t r = 0; r < rounds; ++r) {
+        k_sextend<false><<<persistent, kBlock, 0, sk>>>(s, bk, r, P);
+        k_sshade<<<shade, kBlock, 0, sk>>>(s, v, bk, r, P, max_depth);
+        k_sshadow<false><<<persistent, kBlock, 0, sk>>>(s, bk, r, P);
+        launches += 3;
+      }
+      if (k > 0) cudaStreamWaitEvent(sk, fs->join, 0);  // the previous pass's accumulation
+      k_saccum<<<linear, kBlock, 0, sk>>>(bk, P, k + 1 == spp, 1.0f / (float)spp, out);
+      cudaEventRecord(fs->join, sk);
+      ++launches;
+    }
+    // the last pass recorded fs->join after its accumulation, which followed every other pass's
+    cudaStreamWaitEvent(st, fs->join, 0);
+    return launches;
+  }
   for (uint32_t k = 0; k < spp; ++k) {
     cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * 4 * (rounds + 1), st);
     if (rc) cudaMemsetAsync(b.ccount + 2, 0, sizeof(uint32_t), st);
