@@ -145,6 +145,7 @@ int rc_take_status(void* cache, std::string* msg);
 // two streams.  Ignored while profiling (per-kernel times need one stream).
 struct FrameStreams {
   cudaStream_t side = nullptr;
+  cudaStream_t side2 = nullptr;  // a third stream (the spectral mode's third sample pass)
   cudaEvent_t fork = nullptr, join = nullptr;
 };
 int frame_streams_create(FrameStreams* fs);  // cudaError_t of the first failing call

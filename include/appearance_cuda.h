@@ -119,9 +119,10 @@ typedef struct ap_frame_stats {
 void ap_frame_config_default(ap_frame_config* cfg);
 
 /* PathTracerGpu::new (lib.rs:260-281).  Returns NULL and sets *err on failure.
- * The handle owns two non-blocking CUDA streams on `device` (the frame's, and
- * a second one for traversal that overlaps the next bounce); both are idle
- * when a render call returns. */
+ * The handle owns three non-blocking CUDA streams on `device`: the frame's,
+ * one for traversal that overlaps the next bounce, and (with the second) the
+ * spectral mode's concurrent sample passes; all are idle when a render call
+ * returns. */
 void* ap_create(const ap_frame_config* cfg, int device, int* err);
 void ap_destroy(void* handle);
 const char* ap_last_error(const void* handle);
