@@ -2154,6 +2154,7 @@ void trace_shadow_pair(bool counting, int blocks, cudaStream_t st, const DevScen
 int frame_streams_create(FrameStreams* fs) {
   cudaError_t e = cudaStreamCreateWithFlags(&fs->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&fs->side2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&fs->side3, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fs->fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fs->join, cudaEventDisableTiming);
   if (e != cudaSuccess) frame_streams_destroy(fs);
@@ -2163,10 +2164,12 @@ int frame_streams_create(FrameStreams* fs) {
 void frame_streams_destroy(FrameStreams* fs) {
   if (fs->side) cudaStreamSynchronize(fs->side);
   if (fs->side2) cudaStreamSynchronize(fs->side2);
+  if (fs->side3) cudaStreamSynchronize(fs->side3);
   if (fs->fork) cudaEventDestroy(fs->fork);
   if (fs->join) cudaEventDestroy(fs->join);
   if (fs->side) cudaStreamDestroy(fs->side);
   if (fs->side2) cudaStreamDestroy(fs->side2);
+  if (fs->side3) cudaStreamDestroy(fs->side3);
   *fs = FrameStreams();
 }
 

@@ -138,14 +138,14 @@ int rc_train_device(void* cache, const float4* queries, const float* targets, co
 // check, or AP_E_TIMEOUT for an inference wait that ran out; clears it.
 int rc_take_status(void* cache, std::string* msg);
 
-// Optional second stream for encode_frame: the DI shadow rays of every bounce
+// Optional second stream for encode_frame (side2 and side3 serve the spectral mode): the DI shadow rays of every bounce
 // but the last are traced on `side` beside the next bounce's path extension
 // (apply_gi -> extend), which reads none of their results, so one persistent
 // launch's drain tail overlaps the other's work; `fork` and `join` order the
 // two streams.  Ignored while profiling (per-kernel times need one stream).
 struct FrameStreams {
   cudaStream_t side = nullptr;
-  cudaStream_t side2 = nullptr;  // a third stream (the spectral mode's third sample pass)
+  cudaStream_t side2 = nullptr, side3 = nullptr;  // the spectral mode's third and fourth sample passes
   cudaEvent_t fork = nullptr, join = nullptr;
 };
 int frame_streams_create(FrameStreams* fs);  // cudaError_t of the first failing call

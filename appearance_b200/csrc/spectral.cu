@@ -387,14 +387,14 @@ __global__ void __launch_bounds__(kBlock) k_saccum(SpecBuffers b, uint32_t P, bo
 
 }  // namespace
 
-// Sample passes in flight at once without the cache (launch_spectral); three
-// measured 3 % faster than two on a 2048^2 x 16 spp city image (two: 8 % faster
-// than one pass with its shadow rays beside the next extension).
+// Sample passes in flight at once without the cache (launch_spectral).  On a
+// 2048^2 x 16 spp city image (Msamples/s): one pass with its shadow rays beside
+// the next extension 448, two passes 476, three 490, four 503.
 #ifndef AP_SPEC_PASSES
-#define AP_SPEC_PASSES 3
+#define AP_SPEC_PASSES 4
 #endif
 constexpr int kSpecPasses = AP_SPEC_PASSES;
-static_assert(kSpecPasses >= 2 && kSpecPasses <= 3, "two or three sample passes in flight");
+static_assert(kSpecPasses >= 2 && kSpecPasses <= 4, "two to four sample passes in flight");
 
 // Without the cache the work area holds kSpecPasses sets of path state.
 size_t spectral_work_bytes(uint32_t P, const SpectralCache* rc) {
@@ -416,11 +416,11 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
   const uint32_t P = W * (row1 - row0);
   const bool overlap = fs && fs->side && fs->fork && fs->join && !count_visits;
   // kSpecPasses sample passes in flight: sample k on stream k % kSpecPasses
-  // (`st`, fs->side, fs->side2), each with its own path state; the
+  // (`st`, fs->side, fs->side2, fs->side3), each with its own path state; the
   // accumulator and the counters are shared, and every pass adds to the
   // accumulator after the previous pass did (an event between the streams), so
   // the sum's order is unchanged.
-  const bool pipe = overlap && !rc && spp > 1 && (kSpecPasses < 3 || fs->side2);
+  const bool pipe = overlap && !rc && spp > 1 && (kSpecPasses < 3 || fs->side2) && (kSpecPasses < 4 || fs->side3);
   bool shadow_pending = false;  // a shadow pass in flight on fs->side
   SpecBuffers bufs[kSpecPasses];
   const size_t set_bytes = carve(work, P, rc, &bufs[0]);
@@ -441,7 +441,7 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
   int launches = 0;
   cudaMemsetAsync(b.stats, 0, 6 * sizeof(unsigned long long), st);
   if (pipe) {
-    const cudaStream_t streams[3] = {st, fs->side, fs->side2};
+    const cudaStream_t streams[4] = {st, fs->side, fs->side2, fs->side3};
     cudaEventRecord(fs->fork, st);
     for (int h = 1; h < kSpecPasses; ++h) cudaStreamWaitEvent(streams[h], fs->fork, 0);
     for (uint32_t k = 0; k < spp; ++k) {

@@ -51,8 +51,8 @@ const unsigned long long* spectral_stats(void* work, uint32_t P, const SpectralC
 // spectral_work_bytes(W * (row1 - row0)) bytes; asynchronous on `st`.
 // With count_visits the traversal kernels run in their instrumented form
 // (slower).  With `fs` (more streams, not used with count_visits): without
-// the cache and with spp > 1, three sample passes are in flight, sample k on
-// the k % 3-th of `st`, fs->side, fs->side2, each with its own path state in
+// the cache and with spp > 1, four sample passes are in flight, sample k on
+// the k % 4-th of `st`, fs->side, fs->side2, fs->side3, each with its own path state in
 // `work`, adding to the shared accumulator in sample order; otherwise each round's
 // shadow rays are traced on fs->side beside the next round's extension, which
 // reads none of their results.  The streams have joined into `st` when the

@@ -119,8 +119,8 @@ typedef struct ap_frame_stats {
 void ap_frame_config_default(ap_frame_config* cfg);
 
 /* PathTracerGpu::new (lib.rs:260-281).  Returns NULL and sets *err on failure.
- * The handle owns three non-blocking CUDA streams on `device`: the frame's,
- * one for traversal that overlaps the next bounce, and (with the second) the
+ * The handle owns four non-blocking CUDA streams on `device`: the frame's,
+ * one for traversal that overlaps the next bounce, and (with those two) the
  * spectral mode's concurrent sample passes; all are idle when a render call
  * returns. */
 void* ap_create(const ap_frame_config* cfg, int device, int* err);

@@ -35,8 +35,8 @@ CASES = {
 }
 
 
-# spp > 1 runs three sample passes in flight on three streams (sample k on
-# the k % 3-th); spp 5 ends on the second stream, 2 leaves the third idle
+# spp > 1 runs four sample passes in flight on four streams (sample k on the
+# k % 4-th); spp 5 wraps around to the first stream, spp 2 leaves two idle
 @pytest.mark.parametrize("case,spp,depth,seed", [("cornell", 2, 4, 0), ("cornell", 1, 16, 5), ("field", 2, 8, 3),
                                                  ("field", 1, 16, 11), ("cornell", 5, 6, 7)])
 def test_spectral_matches_oracle_bit_exact(case, spp, depth, seed):
