@@ -9,13 +9,14 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libappearance_cuda.so")
 SOURCES = ["frame.cu", "api.cu", "noalloc.cu", "serve.cu", "mlp.cu", "spectral.cu", "bvh_build.cpp", "spectral_fit.cpp"]
 HEADERS = ["detmath.h", "dev_common.cuh", "dev_shade.cuh", "traverse.cuh", "frame.cuh", "scene_layout.h",
-           "bvh_build.h", "spectral.h", "spectral.cuh", "spectral_fit.h", "persistent.cuh"]
+           "bvh_build.h", "spectral.h", "spectral.cuh", "spectral_fit.h", "persistent.cuh", "device_scope.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-Xptxas", "-v"]
 
@@ -32,14 +33,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
-    logs = []
-    for s in srcs:
+    def compile_one(s):
         o = os.path.join(objdir, os.path.basename(s) + ".o")
         cmd = ["nvcc", *NVCC_FLAGS, "-c", s, "-o", o]
         if s.endswith(".cpp"):
             cmd = ["nvcc", "-x", "cu", *NVCC_FLAGS, "-c", s, "-o", o]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        return o, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as pool:
+        results = list(pool.map(compile_one, srcs))
+    objs, logs = [], []
+    for s, (o, r) in zip(srcs, results):
         logs.append(r.stdout + r.stderr)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

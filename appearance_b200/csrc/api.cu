@@ -10,6 +10,7 @@
 #include "../../include/appearance_cuda.h"
 #include "bvh_build.h"
 #include "dev_common.cuh"
+#include "device_scope.h"
 #include "dev_shade.cuh"
 #include "frame.cuh"
 #include "spectral.cuh"
@@ -388,7 +389,8 @@ void* ap_create(const ap_frame_config* cfg, int device, int* err) {
   h->device = device;
   if (cfg) std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
   else ap_frame_config_default(reinterpret_cast<ap_frame_config*>(&h->cfg));
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+  ap::DeviceScope device_scope(device);
+  if (device_scope.status() != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
       frame_streams_create(&h->fs) != 0) {
     *err = AP_E_CUDA;
@@ -405,7 +407,7 @@ void* ap_create(const ap_frame_config* cfg, int device, int* err) {
 void ap_destroy(void* hp) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return;
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   h->scene.release();
   if (h->frame_mem) cudaFree(h->frame_mem);
@@ -432,7 +434,7 @@ int ap_set_config(void* hp, const ap_frame_config* cfg) {
   if (!h || !cfg) return AP_E_INVALID;
   std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
   // a new configuration starts a new frame sequence: drop the temporal state
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   cudaStreamSynchronize(h->stream);
   if (h->frame_mem) cudaFree(h->frame_mem);
   h->frame_mem = nullptr;
@@ -456,12 +458,13 @@ int ap_world_action(void* hp, uint32_t ty, const void* bytes, size_t len) {
       h->explicit_mats = false;
       return AP_OK;
     }
-    case 4:  // Clear
+    case 4: {  // Clear
       if (!bytes || len != 4) return fail(h, AP_E_INVALID, "Clear expects 4 bytes");
-      cudaSetDevice(h->device);
+      ap::DeviceScope device_scope(h->device);
       cudaStreamSynchronize(h->stream);
       h->scene.release();
       return AP_OK;
+    }
     case 1:
     case 2:
     case 3:
@@ -496,7 +499,7 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
       if (me.material_idx + d->tri_material[me.first_index / 3 + t] >= d->num_materials)
         return fail(h, AP_E_INVALID, "scene: triangle material out of range");
   }
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   cudaStreamSynchronize(h->stream);
   h->scene.release();
   h->spec_release();
@@ -661,7 +664,7 @@ int ap_render_hdr(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint32
   if (row_start >= row_end || row_end > hgt) return fail(h, AP_E_INVALID, "bad row range");
   size_t need = (size_t)(row_end - row_start) * w * 3 * sizeof(float);
   if (!out || out_bytes < need) return fail(h, AP_E_INVALID, "output buffer too small");
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   int rc = render_common(h, w, hgt, stats);
   if (rc) return rc;
   rc = check_cuda(h, cudaMemcpyAsync(out, h->fb.out_rgb + (size_t)row_start * w * 3, need, cudaMemcpyDeviceToHost, h->stream),
@@ -677,7 +680,7 @@ int ap_rc_attach(void* hp, void* cache, uint32_t prefix_bounces, uint32_t train_
   if (cache && (prefix_bounces == 0 || prefix_bounces >= kRcMaxBounces || train_stride == 0 || train_batch == 0 ||
                 train_batch > (1u << 22) || !(lr >= 0.0f)))
     return fail(h, AP_E_INVALID, "radiance cache: parameters out of range");
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   cudaStreamSynchronize(h->stream);
   if (h->rc_mem) cudaFree(h->rc_mem);
   h->rc_mem = nullptr;
@@ -701,7 +704,7 @@ int ap_render_rgba8(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
   if (row_start >= row_end || row_end > hgt) return fail(h, AP_E_INVALID, "bad row range");
   size_t need = (size_t)(row_end - row_start) * w * 4;
   if (!out || out_bytes < need) return fail(h, AP_E_INVALID, "output buffer too small");
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   int rc = render_common(h, w, hgt, stats);
   if (rc) return rc;
   // lib.rs:349-352: a moved camera or accumulation off restarts the average
@@ -722,7 +725,7 @@ int ap_render_rgba8(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
 int ap_render_device(void* hp, uint32_t w, uint32_t hgt, ap_frame_stats* stats) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return AP_E_INVALID;
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   return render_common(h, w, hgt, stats);
 }
 
@@ -737,11 +740,10 @@ int ap_trace_rays(void* hp, const float* origins_tmax, const float* dirs, uint32
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
   if (!origins_tmax || !dirs || !out4) return fail(h, AP_E_INVALID, "null buffer");
   if (n == 0) return AP_OK;
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   size_t need = (size_t)n * 48 + 256;
   if (h->trace_bytes < need) {
     if (h->trace_mem) cudaFree(h->trace_mem);
-  if (h->rc_mem) cudaFree(h->rc_mem);
     h->trace_mem = nullptr;
     int rc = check_cuda(h, cudaMalloc(&h->trace_mem, need), "trace scratch");
     if (rc) return rc;
@@ -767,7 +769,7 @@ int ap_read_buffer(void* hp, uint32_t which, uint32_t* out, size_t out_bytes) {
   if (!h->frame_mem) return fail(h, AP_E_INVALID, "no frame rendered");
   size_t P = (size_t)h->W * h->H;
   uint32_t cur = (h->frame_idx + 1) & 1u;  // parity of the last rendered frame
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   struct Part { const void* ptr; size_t stride; };
   std::vector<Part> parts;
   size_t words = 0;
@@ -804,7 +806,7 @@ int ap_profile_frame(void* hp, uint32_t w, uint32_t hgt, double* kind_ms, uint32
                      ap_frame_stats* stats) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h || !kind_ms || !kind_count || !num_kinds) return AP_E_INVALID;
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   if (!h->prof.created) {
     for (int i = 0; i <= FrameProfiler::kMax; ++i)
       if (cudaEventCreate(&h->prof.ev[i]) != cudaSuccess) return fail(h, AP_E_CUDA, "profiler events");
@@ -850,7 +852,7 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
   if (!(scene_radius > 0.0f) || !(sun_scale >= 0.0f) || !(env_scale >= 0.0f) ||
       !(sun_dir3[0] * sun_dir3[0] + sun_dir3[1] * sun_dir3[1] + sun_dir3[2] * sun_dir3[2] > 0.0f))
     return fail(h, AP_E_INVALID, "spectral setup: bad light parameters");
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   cudaStreamSynchronize(h->stream);
   h->spec_release();
   const DeviceScene& sc = h->scene;
@@ -901,7 +903,7 @@ int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
     return fail(h, AP_E_INVALID, "spectral render: bad arguments");
   const size_t need = (size_t)(row_end - row_start) * w * 3 * sizeof(float);
   if (out_rgb && out_bytes < need) return fail(h, AP_E_INVALID, "output buffer too small");
-  cudaSetDevice(h->device);
+  ap::DeviceScope device_scope(h->device);
   // the image, then the wavefront's work area
   const uint32_t P = w * (row_end - row_start);
   SpectralCache cache_mode{};

@@ -30,6 +30,7 @@
 
 #include "../../include/appearance_cuda.h"
 #include "dev_common.cuh"
+#include "device_scope.h"
 
 namespace ap {
 namespace {
@@ -610,7 +611,7 @@ void* ap_rc_create(int device, const float* scene_lo, const float* scene_hi, uin
     if (err) *err = scene_lo && scene_hi ? AP_E_CUDA : AP_E_INVALID;
     return nullptr;
   }
-  cudaSetDevice(device);
+  ap::DeviceScope device_scope(device);
   Cache* c = new Cache;
   c->device = device;
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -657,7 +658,7 @@ void* ap_rc_create(int device, const float* scene_lo, const float* scene_hi, uin
 void ap_rc_destroy(void* cp) {
   Cache* c = static_cast<Cache*>(cp);
   if (!c) return;
-  cudaSetDevice(c->device);
+  ap::DeviceScope device_scope(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->wf, c->loss, c->err, c->count, c->packed, c->h, c->d, c->targets,
                   c->queries, c->out};
@@ -674,7 +675,8 @@ const char* ap_rc_last_error(const void* cp) {
 
 int ap_rc_wait_selftest(int device, int limit, uint32_t* out2) {
   if (!out2 || limit <= 0 || limit > (1 << 22)) return AP_E_INVALID;
-  if (cudaSetDevice(device) != cudaSuccess) return AP_E_CUDA;
+  ap::DeviceScope device_scope(device);
+  if (device_scope.status() != cudaSuccess) return AP_E_CUDA;
   uint32_t* d = nullptr;
   if (cudaMalloc(&d, 8) != cudaSuccess) return AP_E_OOM;
   cudaMemset(d, 0xff, 8);
@@ -688,7 +690,7 @@ int ap_rc_wait_selftest(int device, int limit, uint32_t* out2) {
 int ap_rc_set_params(void* cp, const float* params, uint32_t count) {
   Cache* c = static_cast<Cache*>(cp);
   if (!c || !params || count != ap::kNumParams) return ap::cfail(c, AP_E_INVALID, "parameter count");
-  cudaSetDevice(c->device);
+  ap::DeviceScope device_scope(c->device);
   int rc;
   if ((rc = ap::cuda_ok(c, cudaMemcpy(c->master, params, ap::kNumParams * 4, cudaMemcpyHostToDevice), "params")))
     return rc;
@@ -703,7 +705,7 @@ int ap_rc_set_params(void* cp, const float* params, uint32_t count) {
 int ap_rc_get_params(void* cp, float* params, uint32_t count) {
   Cache* c = static_cast<Cache*>(cp);
   if (!c || !params || count != ap::kNumParams) return ap::cfail(c, AP_E_INVALID, "parameter count");
-  cudaSetDevice(c->device);
+  ap::DeviceScope device_scope(c->device);
   cudaStreamSynchronize(c->stream);
   return ap::cuda_ok(c, cudaMemcpy(params, c->master, ap::kNumParams * 4, cudaMemcpyDeviceToHost), "params");
 }
@@ -712,7 +714,7 @@ int ap_rc_infer(void* cp, const float* queries, uint32_t n, float* out_rgb) {
   Cache* c = static_cast<Cache*>(cp);
   if (!c || (n && (!queries || !out_rgb))) return ap::cfail(c, AP_E_INVALID, "null buffer");
   if (n == 0) return AP_OK;
-  cudaSetDevice(c->device);
+  ap::DeviceScope device_scope(c->device);
   int rc = ap::ensure_batch(c, n);
   if (rc) return rc;
   cudaMemcpyAsync(c->queries, queries, (size_t)n * 64, cudaMemcpyHostToDevice, c->stream);
@@ -730,7 +732,7 @@ int ap_rc_train(void* cp, const float* queries, const float* targets, uint32_t n
   Cache* c = static_cast<Cache*>(cp);
   if (!c || (n && (!queries || !targets))) return ap::cfail(c, AP_E_INVALID, "null buffer");
   if (n == 0) return AP_OK;
-  cudaSetDevice(c->device);
+  ap::DeviceScope device_scope(c->device);
   int rc = ap::ensure_batch(c, n);
   if (rc) return rc;
   cudaMemcpyAsync(c->queries, queries, (size_t)n * 64, cudaMemcpyHostToDevice, c->stream);

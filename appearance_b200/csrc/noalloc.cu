@@ -19,13 +19,22 @@
 // Set-up: the first call on a device, with that device current, looks up the
 // array's device address with cudaGetSymbolAddress (the array's name is only a
 // host-side stand-in, not a device address) and caches it; that first call
-// should therefore come before any stream capture.
+// should therefore come before any stream capture.  The cached address belongs
+// to the device's context of that moment: after cudaDeviceReset (or any
+// teardown of the primary context) in the same process it is stale, so this
+// entry point must not be used across a device reset.
+//
+// The call makes the handle's device current for its duration and gives the
+// calling thread its previous current device back before it returns; on every
+// path that returns after the first copy was queued it waits for the stream,
+// so no copy or kernel on the shared array outlives the call.
 #include <cuda_runtime.h>
 
 #include <mutex>
 #include <string>
 
 #include "../../include/appearance_cuda.h"
+#include "device_scope.h"
 #include "frame.cuh"
 
 namespace ap {
@@ -91,7 +100,8 @@ extern "C" int ap_trace_rays_static(void* handle, const float* origins_tmax, con
     *err = "device index out of range";
     return AP_E_INVALID;
   }
-  cudaError_t e = cudaSetDevice(device);
+  ap::DeviceScope device_scope(device);
+  cudaError_t e = device_scope.status();
   if (e != cudaSuccess) return cuda_fail(err, e, "cudaSetDevice");
   char* base = nullptr;
   e = scratch_address(device, &base);
@@ -100,13 +110,19 @@ extern "C" int ap_trace_rays_static(void* handle, const float* origins_tmax, con
   float4* d = reinterpret_cast<float4*>(base + kDirOff);
   uint4* hits = reinterpret_cast<uint4*>(base + kHitOff);
   uint32_t* cursor = reinterpret_cast<uint32_t*>(base + kCursorOff);
+  // From the first queued copy on, every return waits for the stream first.
+  auto fail_after_queue = [&](cudaError_t code, const char* what) {
+    cudaStreamSynchronize(stream);
+    cudaGetLastError();
+    return cuda_fail(err, code, what);
+  };
   if ((e = cudaMemcpyAsync(o, origins_tmax, (size_t)n * 16, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
       (e = cudaMemcpyAsync(d, dirs, (size_t)n * 16, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-    return cuda_fail(err, e, "ray upload");
+    return fail_after_queue(e, "ray upload");
   ap::launch_trace_batch(*scene, o, d, n, any_hit, hits, cursor, num_sms, stream);  // zeroes the cursor first
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(err, e, "trace launch");
+  if ((e = cudaGetLastError()) != cudaSuccess) return fail_after_queue(e, "trace launch");
   if ((e = cudaMemcpyAsync(out4, hits, (size_t)n * 16, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
-    return cuda_fail(err, e, "hit readback");
+    return fail_after_queue(e, "hit readback");
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(err, e, "trace");
   return AP_OK;
 }

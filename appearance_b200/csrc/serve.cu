@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "../../include/appearance_cuda.h"
+#include "device_scope.h"
 #include "frame.cuh"
 
 namespace ap {
@@ -94,6 +95,7 @@ struct Server {
   bool stop = false;
   std::thread worker;
   std::string err;
+  cudaMemPool_t pool = nullptr;  // the server's own stream-ordered pool
 };
 
 struct CallbackArg {
@@ -135,7 +137,7 @@ bool launch_job(Server* s, Job* j, Slot& sl) {
   cfg.sample_count = d.spp;
   cfg.max_bounces = d.max_depth;
   const size_t out_bytes = (size_t)d.width * d.height * 12;
-  cudaError_t e = cudaMallocAsync(&j->dev, j->bytes, sl.stream);
+  cudaError_t e = cudaMallocFromPoolAsync(&j->dev, j->bytes, s->pool, sl.stream);
   if (e != cudaSuccess) {
     j->rc = e == cudaErrorMemoryAllocation ? AP_E_OOM : AP_E_CUDA;
     j->err = std::string("job frame state: ") + cudaGetErrorString(e);
@@ -315,32 +317,42 @@ void* ap_server_create(const ap_frame_config* cfg, int device, uint64_t hbm_budg
     if (err) *err = AP_E_CUDA;
     return nullptr;
   }
-  cudaSetDevice(device);
+  ap::DeviceScope device_scope(device);
   Server* s = new Server;
   s->device = device;
   s->budget = hbm_budget;
   s->use_graphs = use_graphs;
   std::memcpy(&s->base, cfg, sizeof(FrameConfig));
   cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
-  // keep freed job state in the pool (no release back to the driver between jobs)
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+  // The server's own pool, so that job state freed between jobs stays mapped
+  // for the next job (no release back to the driver) without changing the
+  // device's default pool, which belongs to the whole process.
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  bool ok = cudaMemPoolCreate(&s->pool, &props) == cudaSuccess;
+  if (ok) {
     uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    ok = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &thr) == cudaSuccess;
   }
   s->slots.resize(max_inflight);
   for (Slot& sl : s->slots) {
-    if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&sl.ev0) != cudaSuccess || cudaEventCreate(&sl.ev1) != cudaSuccess) {
-      if (err) *err = AP_E_CUDA;
-      for (Slot& t : s->slots) {
-        if (t.stream) cudaStreamDestroy(t.stream);
-        if (t.ev0) cudaEventDestroy(t.ev0);
-        if (t.ev1) cudaEventDestroy(t.ev1);
-      }
-      delete s;
-      return nullptr;
+    if (!ok) break;
+    ok = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreate(&sl.ev0) == cudaSuccess && cudaEventCreate(&sl.ev1) == cudaSuccess;
+  }
+  if (!ok) {
+    cudaGetLastError();
+    if (err) *err = AP_E_CUDA;
+    for (Slot& t : s->slots) {
+      if (t.stream) cudaStreamDestroy(t.stream);
+      if (t.ev0) cudaEventDestroy(t.ev0);
+      if (t.ev1) cudaEventDestroy(t.ev1);
     }
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    delete s;
+    return nullptr;
   }
   s->worker = std::thread(dispatcher, s);
   return s;
@@ -355,7 +367,7 @@ void ap_server_destroy(void* sp) {
   }
   s->cv_work.notify_all();
   if (s->worker.joinable()) s->worker.join();  // drains queued and in-flight jobs
-  cudaSetDevice(s->device);
+  ap::DeviceScope device_scope(s->device);
   for (Slot& sl : s->slots) {
     if (sl.stream) cudaStreamSynchronize(sl.stream);
     if (sl.exec) cudaGraphExecDestroy(sl.exec);
@@ -366,6 +378,7 @@ void ap_server_destroy(void* sp) {
   }
   for (auto& kv : s->jobs) delete kv.second;
   for (void* h : s->scenes) ap_destroy(h);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
 }
 

@@ -61,3 +61,38 @@ def test_trained_cache_beats_truncation():
     assert cut.mean() < 0.9 * ref.mean()  # truncation loses light here
     assert abs(cached.mean() - ref.mean()) < 0.5 * abs(cut.mean() - ref.mean())
     assert e_cached < 0.6 * e_cut
+
+
+def test_ray_queries_between_cached_frames_leave_the_cache_state_intact():
+    """A batch ray query that grows the handle's query scratch must not touch
+    the radiance cache's frame state: the frames after it equal the frames of
+    the same sequence without the query."""
+    sc = scenes.cornell_box()
+    cam = scenes.cornell_camera()
+    mats, _ = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], cam["near"], cam["far"], W, H, None)
+    cfg = dict(presets.PLAIN, max_bounces=4, sample_count=2)
+    rng = np.random.default_rng(3)
+    o = rng.uniform(0.1, 0.9, (4096, 3)).astype(np.float32)
+    d = rng.normal(size=(4096, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+
+    def run(with_query):
+        rc = RadianceCache([-0.05, -0.05, -0.05], [1.05, 1.05, 1.05], seed=2)
+        pt = PathTracer(cfg)
+        pt.upload_scene(sc)
+        pt.set_camera_matrices(mats)
+        # lr 0: the weights stay put (the split-K gradient sums are not
+        # bit-reproducible), while every frame-side cache buffer is still used
+        pt.attach_radiance_cache(rc, prefix_bounces=1, train_stride=4, train_batch=4096, lr=0.0)
+        frames = [pt.render((W, H))]
+        if with_query:
+            pt.trace_rays(o[:16], d[:16], 100.0)
+            pt.trace_rays(o, d, 100.0)  # larger than before: the query scratch grows
+        frames += [pt.render((W, H)) for _ in range(3)]
+        pt.close()
+        rc.close()
+        return frames
+
+    a, b = run(False), run(True)
+    for i, (x, y) in enumerate(zip(a, b)):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), f"frame {i} differs"

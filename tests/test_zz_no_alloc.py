@@ -38,19 +38,32 @@ def _call(lib, fn, h, o, d, any_hit):
     return out
 
 
+def _free_device_bytes():
+    # the CUDA runtime the library itself loaded (already mapped in this process)
+    rt = ctypes.CDLL("libcudart.so.12")
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert rt.cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+    return free.value
+
+
 def test_static_scratch_query_matches_allocating_query():
     lib = _native.load()
     sc = scenes.icosphere_field(seed=4, num_spheres=64, num_emissive=4, subdiv=2, box=12.0, env_size=None)
     pt = PathTracer(presets.FAITHFUL)
     pt.upload_scene(sc)
     h = pt._h
-    for call, (n, any_hit) in enumerate([(STATIC_MAX_RAYS, 0), (40000, 1)]):  # two calls in a row
-        o, d = _rays(n, 100 + call, -2.0, 14.0)
-        ref = _call(lib, "ap_trace_rays", h, o, d, any_hit)
+    batches = [(STATIC_MAX_RAYS, 0), (40000, 1)]
+    rays = [_rays(n, 100 + call, -2.0, 14.0) for call, (n, _) in enumerate(batches)]
+    refs = [_call(lib, "ap_trace_rays", h, o, d, any_hit) for (o, d), (_, any_hit) in zip(rays, batches)]
+    for call, ((o, d), (n, any_hit), ref) in enumerate(zip(rays, batches, refs)):  # two calls in a row
+        free_before = _free_device_bytes()
         got = _call(lib, "ap_trace_rays_static", h, o, d, any_hit)
+        free_after = _free_device_bytes()
         assert np.array_equal(got, ref), f"call {call}: {(got != ref).any(1).sum()} rays differ"
         if not any_hit:
             assert (got[:, 3] != 0xFFFFFFFF).mean() > 0.05
+        if call > 0:  # the first call may load the library's device code; later calls change nothing
+            assert free_after == free_before, f"call {call}: device memory changed by {free_before - free_after} B"
 
 
 def test_static_scratch_query_rejects_oversized_batches():
