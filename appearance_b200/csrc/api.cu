@@ -29,6 +29,7 @@ struct DeviceScene {
   void* tris = nullptr;
   void* positions = nullptr;
   void* normals = nullptr;
+  void* normals_f = nullptr;  // float vertex normals (the spectral mode's shading normals)
   void* indices = nullptr;
   void* tri_material = nullptr;
   void* tri_instance = nullptr;
@@ -48,7 +49,7 @@ struct DeviceScene {
   size_t bytes = 0;  // device memory held
   bool valid = false;
   void release() {
-    void** all[] = {&nodes, &tris, &positions, &normals, &indices, &tri_material, &tri_instance,
+    void** all[] = {&nodes, &tris, &positions, &normals, &normals_f, &indices, &tri_material, &tri_instance,
                     &instances, &materials, &emissive_instances, &emissive_cdf, &emissive_tris,
                     &emissive_tri_base, &emissive_info, &env};
     for (void** p : all) {
@@ -93,7 +94,7 @@ struct Handle {
   uint32_t rc_w = 0, rc_h = 0;
   // spectral mode (ap_spectral_setup / ap_render_spectral)
   void* spec_mats = nullptr;
-  void* spec_env = nullptr;
+  void* spec_env = nullptr;  // the environment's compensated sampling distribution
   void* spec_tab = nullptr;  // illuminant upsampling table (cache mode's predictions)
   void* spec_out = nullptr;
   size_t spec_out_bytes = 0;
@@ -565,11 +566,10 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
     pos4[i] = make_float4(d->positions[3 * i], d->positions[3 * i + 1], d->positions[3 * i + 2], 0.0f);
   DeviceScene& s = h->scene;
   int rc = 0;
-  void* nrm_f = nullptr;
   if ((rc = upload(h, &s.nodes, bvh.nodes.data(), bvh.nodes.size())) ||
       (rc = upload(h, &s.tris, bvh.tris.data(), bvh.tris.size())) ||
       (rc = upload(h, &s.positions, pos4.data(), pos4.size())) ||
-      (rc = upload(h, &nrm_f, d->normals, 3 * (size_t)d->num_vertices)) ||
+      (rc = upload(h, &s.normals_f, d->normals, 3 * (size_t)d->num_vertices)) ||
       (rc = check_cuda(h, cudaMalloc(&s.normals, std::max<size_t>(4 * (size_t)d->num_vertices, 16)), "normals")) ||
       (rc = upload(h, &s.indices, d->indices, 3 * (size_t)d->num_tris)) ||
       (rc = upload(h, &s.tri_material, d->tri_material, d->num_tris)) ||
@@ -582,15 +582,14 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
       (rc = upload(h, &s.emissive_info, info.data(), info.size())) ||
       (rc = check_cuda(h, cudaMalloc(&s.emissive_tris, std::max<size_t>(sizeof(EmissiveTri) * num_emissive_tris, 16)),
                        "emissive triangles"))) {
-    if (nrm_f) cudaFree(nrm_f);
     s.release();
     return rc;
   }
   if (d->num_vertices)
-    k_pack_normals<<<(d->num_vertices + 255) / 256, 256, 0, h->stream>>>(static_cast<const float*>(nrm_f), d->num_vertices,
+    k_pack_normals<<<(d->num_vertices + 255) / 256, 256, 0, h->stream>>>(static_cast<const float*>(s.normals_f),
+                                                                           d->num_vertices,
                                                                            static_cast<uint32_t*>(s.normals));
   rc = check_cuda(h, cudaStreamSynchronize(h->stream), "pack normals");
-  cudaFree(nrm_f);
   if (rc) {
     s.release();
     return rc;
@@ -606,6 +605,7 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
   v.tris = static_cast<const float4*>(s.tris);
   v.positions = static_cast<const float4*>(s.positions);
   v.normals = static_cast<const uint32_t*>(s.normals);
+  v.normals_f = static_cast<const float*>(s.normals_f);
   v.indices = static_cast<const uint32_t*>(s.indices);
   v.tri_material = static_cast<const uint32_t*>(s.tri_material);
   v.tri_instance = static_cast<const uint32_t*>(s.tri_instance);
@@ -860,14 +860,15 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
   std::vector<spec::Material> mats(nm);
   spec::upsample_materials(sc.host_materials.data(), nm, mats.data());
   const size_t texels = sc.host_env.size() / 3;
-  std::vector<float> env4(4 * texels);
-  if (texels) spec::upsample_env(sc.host_env.data(), texels, env4.data());
+  std::vector<float> env_pdf(texels);
+  float env_integral = 0.0f;
+  if (texels) spectral_env_distribution(sc.host_env.data(), sc.view.env_w, sc.view.env_h, env_pdf.data(), &env_integral);
   int rc = check_cuda(h, cudaMalloc(&h->spec_mats, sizeof(spec::Material) * std::max<uint32_t>(nm, 1)), "spectral materials");
-  if (!rc) rc = check_cuda(h, cudaMalloc(&h->spec_env, std::max<size_t>(sizeof(float) * env4.size(), 16)), "spectral env");
+  if (!rc) rc = check_cuda(h, cudaMalloc(&h->spec_env, std::max<size_t>(sizeof(float) * texels, 16)), "spectral env");
   if (!rc) rc = check_cuda(h, cudaMemcpy(h->spec_mats, mats.data(), sizeof(spec::Material) * nm, cudaMemcpyHostToDevice),
                            "spectral materials");
   if (!rc && texels)
-    rc = check_cuda(h, cudaMemcpy(h->spec_env, env4.data(), sizeof(float) * env4.size(), cudaMemcpyHostToDevice),
+    rc = check_cuda(h, cudaMemcpy(h->spec_env, env_pdf.data(), sizeof(float) * texels, cudaMemcpyHostToDevice),
                     "spectral env");
   const spec::IlluminantTable& tab = spec::illuminant_table();
   if (!rc) rc = check_cuda(h, cudaMalloc(&h->spec_tab, sizeof(float) * tab.coef.size()), "spectral table");
@@ -879,7 +880,8 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
     return rc;
   }
   h->spec.mats = static_cast<const spec::Material*>(h->spec_mats);
-  h->spec.env = static_cast<const float4*>(h->spec_env);
+  h->spec.env_pdf = static_cast<const float*>(h->spec_env);
+  h->spec.env_pdf_integral = env_integral;
   h->spec.env_w = texels ? sc.view.env_w : 0;
   h->spec.env_h = texels ? sc.view.env_h : 0;
   h->spec.env_scale = env_scale;

@@ -1700,15 +1700,21 @@ __global__ void k_firefly(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t cur,
   dst[id] = pack_rgb9e5(rec);
 }
 
-// svgf_temporal.wgsl:87-139
+// svgf_temporal.wgsl:87-139.  Besides the packed temporal radiance (kept for
+// the reference's buffer ping-pong, which the sky pixels of later frames read)
+// it writes the a-trous passes' records: oct30 normal + depth, and packed
+// radiance + variance.
 __global__ void k_svgf_temporal(FrameBuffers fb, Consts c, const uint32_t* demod, uint32_t* out_rad,
-                                const float2* in_mom, float2* out_mom, float* out_var) {
+                                const float2* in_mom, float2* out_mom, int write_records) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
   uint32_t id = y * c.W + x;
   const uint32_t cur = c.frame_idx & 1u;
-  GT g = gt_load(fb.gb_a[cur], fb.gb_b[cur], id);
+  const uint4 ga = fb.gb_a[cur][id], gbv = fb.gb_b[cur][id];
+  GT g = GT{f3(__uint_as_float(ga.x), __uint_as_float(ga.y), __uint_as_float(ga.z)), __uint_as_float(ga.w),
+            unpack_oct30(gbv.x), unpack_rgb9e5(gbv.y)};
   float3 rad = unpack_rgb9e5(demod[id]);
+  if (write_records) fb.atr_nd[id] = make_uint2(gbv.x, ga.w);
   if (g.depth == 0.0f) {
     out_rad[id] = pack_rgb9e5(rad);
     return;
@@ -1741,121 +1747,132 @@ __global__ void k_svgf_temporal(FrameBuffers fb, Consts c, const uint32_t* demod
   tmx = mixf(tmx, mx, alpha);
   tmy = mixf(tmy, my, alpha);
   trad = mix3(trad, rad, alpha);
-  out_var[id] = dm::fmax(tmy - sqr(tmx), 0.0f);
-  out_rad[id] = pack_rgb9e5(trad);
+  const float var = dm::fmax(tmy - sqr(tmx), 0.0f);
+  const uint32_t packed = pack_rgb9e5(trad);
+  out_rad[id] = packed;
+  if (write_records) fb.atr_rv[0][id] = make_uint2(packed, __float_as_uint(var));
   out_mom[id] = make_float2(tmx, tmy);
   fb.svgf_count[id] = count;
 }
 
-// The a-trous passes' per-pixel inputs, unpacked once per frame: normal and
-// depth (constant over the passes) and the first pass's radiance with its luma.
-__global__ void k_atrous_prep(FrameBuffers fb, uint32_t P, uint32_t cur, const uint32_t* in_rad) {
-  const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= P) return;
-  const float3 n = unpack_oct30(fb.gb_b[cur][id].x);
-  fb.atr_nd[id] = make_float4(n.x, n.y, n.z, __uint_as_float(fb.gb_a[cur][id].w));
-  const float3 r = unpack_rgb9e5(in_rad[id]);
-  fb.atr_rad[0][id] = make_float4(r.x, r.y, r.z, luma(r));
-}
-
-// svgf_atrous.wgsl:48-117.  Inputs come unpacked (k_atrous_prep and the
-// previous pass): radiance + luma and normal + depth as float4, variance.  A
-// 16x16 block stages its tile plus a halo of 2*step pixels in shared memory
-// when the halo is small (steps 1, 2, 4); larger steps read through L1/L2.
-// The two exponential weights are one exp of the summed exponents with the
-// divisions as products by reciprocals, and pow(., 128) is seven squarings
-// (the oracle evaluates the same expressions).  Each pass writes its packed
-// radiance (RGB9E5, as the reference stores it) and, for the next pass, the
-// unpacked value of that packed radiance with its luma.
+// svgf_atrous.wgsl:48-117, one pass of step STEP.
+//
+// A block filters a 16x16 lattice of pixels STEP apart (one residue class of a
+// (16 STEP)^2 pixel tile), so that every tap of every pixel, at offsets of
+// +-STEP and +-2 STEP, falls on the same lattice: the block stages a 20x20
+// lattice tile in shared memory, decoding each record once (normal, depth,
+// radiance, luma, variance), and the 24 taps read shared memory only, for
+// every step.  Pixels outside the image are staged as sky (depth 0), which
+// the taps skip as the reference skips both.
+//
+// Arithmetic: the two exponential weights are one hardware exp of the summed
+// exponents and pow(., 128) is seven squarings; sums use fused multiply-adds.
+// The result therefore differs from the reference's literal expressions in
+// the last bits of the weights; after RGB9E5 packing (9-bit mantissas) most
+// pixels are bit-identical and the rest differ by a rounding step.
+//
+// Stores: the next pass's record (packed radiance, variance); pass 0 the
+// history radiance of the next frame's temporal pass (svgf_hist); the last
+// pass whose output lands in svgf_rad[(frame + 1) % 2] in the reference's
+// ping-pong stores it there (sky pixels of the next frame read it); the final
+// pass writes the filtered frame, and for sky pixels, which no pass writes in
+// the reference, the value the reference's final buffer still holds.
 constexpr int kAtrousTile = 16;
+constexpr int kAtrousSpan = kAtrousTile + 4;
+enum : uint32_t { ATR_HIST = 1u, ATR_STATE = 2u, ATR_FINAL = 4u, ATR_NEXT = 8u };
 template <int STEP>
-__global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t pass_idx,
-                                                const float4* in_rad4, float4* out_rad4, uint32_t* out_rad,
-                                                const float* in_var, float* out_var) {
-  constexpr int HALO = 2 * STEP;
-  constexpr int SW = kAtrousTile + 2 * HALO;
-  constexpr bool kShared = STEP <= 4;
-  __shared__ float4 s_rad[kShared ? SW * SW : 1];
-  __shared__ float4 s_nd[kShared ? SW * SW : 1];
-  __shared__ float s_var[kShared ? SW * SW : 1];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int x0 = blockIdx.x * kAtrousTile, y0 = blockIdx.y * kAtrousTile;
-  const float4* nd = fb.atr_nd;
-  if (kShared) {
-    for (int k = ty * kAtrousTile + tx; k < SW * SW; k += kAtrousTile * kAtrousTile) {
-      int sx = x0 - HALO + (k % SW), sy = y0 - HALO + (k / SW);
-      float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f), n = r;
-      float v = 0.0f;
-      if (sx >= 0 && sy >= 0 && sx < (int)W && sy < (int)H) {
-        uint32_t sid = (uint32_t)sy * W + (uint32_t)sx;
-        r = in_rad4[sid];
-        n = nd[sid];
-        v = in_var[sid];
+__global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t flags,
+                                                const uint2* in_rv, uint2* out_rv, uint32_t* state_rad,
+                                                const uint32_t* final_src, uint32_t* final_dst) {
+  __shared__ float4 s_rad[kAtrousSpan * kAtrousSpan];  // radiance, luma
+  __shared__ float4 s_nd[kAtrousSpan * kAtrousSpan];   // normal, depth (0: sky or outside)
+  __shared__ float s_var[kAtrousSpan * kAtrousSpan];
+  const int tiles_x = (int)((W + kAtrousTile * STEP - 1) / (kAtrousTile * STEP));
+  (void)tiles_x;
+  const int bx = (int)blockIdx.x / STEP, rx = (int)blockIdx.x % STEP;
+  const int by = (int)blockIdx.y / STEP, ry = (int)blockIdx.y % STEP;
+  const int base_x = bx * kAtrousTile * STEP + rx, base_y = by * kAtrousTile * STEP + ry;
+  if (base_x >= (int)W || base_y >= (int)H) return;  // the whole lattice lies outside
+  const int tid = threadIdx.y * kAtrousTile + threadIdx.x;
+  for (int k = tid; k < kAtrousSpan * kAtrousSpan; k += kAtrousTile * kAtrousTile) {
+    const int px = base_x + STEP * (k % kAtrousSpan - 2), py = base_y + STEP * (k / kAtrousSpan - 2);
+    float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f), n = r;
+    float v = 0.0f;
+    if (px >= 0 && py >= 0 && px < (int)W && py < (int)H) {
+      const uint32_t sid = (uint32_t)py * W + (uint32_t)px;
+      const uint2 nd = fb.atr_nd[sid];
+      n.w = __uint_as_float(nd.y);
+      if (n.w != 0.0f) {
+        const float3 nn = unpack_oct30(nd.x);
+        n.x = nn.x;
+        n.y = nn.y;
+        n.z = nn.z;
+        const uint2 rv = in_rv[sid];
+        const float3 rr = unpack_rgb9e5(rv.x);
+        r = make_float4(rr.x, rr.y, rr.z, luma(rr));
+        v = __uint_as_float(rv.y);
       }
-      s_rad[k] = r;
-      s_nd[k] = n;
-      s_var[k] = v;
     }
-    __syncthreads();
+    s_rad[k] = r;
+    s_nd[k] = n;
+    s_var[k] = v;
   }
-  int x = x0 + tx, y = y0 + ty;
+  __syncthreads();
+  const int x = base_x + STEP * (int)threadIdx.x, y = base_y + STEP * (int)threadIdx.y;
   if (x >= (int)W || y >= (int)H) return;
-  uint32_t id = (uint32_t)y * W + (uint32_t)x;
-  auto slot = [&](int px, int py) { return (py - y0 + HALO) * SW + (px - x0 + HALO); };
-  const float4 cnd = kShared ? s_nd[slot(x, y)] : nd[id];
-  const float cdepth = cnd.w;
-  if (cdepth == 0.0f) return;
-  const float3 cn = f3(cnd.x, cnd.y, cnd.z);
-  const float4 crad = kShared ? s_rad[slot(x, y)] : in_rad4[id];
-  const float KW[3] = {3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
+  const uint32_t id = (uint32_t)y * W + (uint32_t)x;
+  const int c = ((int)threadIdx.y + 2) * kAtrousSpan + (int)threadIdx.x + 2;
+  const float4 cnd = s_nd[c];
+  if (cnd.w == 0.0f) {  // sky: the reference writes nothing for this pixel
+    if (flags & ATR_FINAL) final_dst[id] = final_src[id];
+    return;
+  }
+  const float4 crad = s_rad[c];
+  float vsum = s_var[c];
   float3 rsum = f3(crad.x, crad.y, crad.z);
-  float vsum = kShared ? s_var[slot(x, y)] : in_var[id];
   float wsum = 1.0f;
-  const float cl = crad.w;
-  const float cv = vsum;
-  const float inv_lum = 1.0f / dm::fmax(4.0f * dm::sqrt_(cv), 1e-8f);
-  const float depth_k = 1.0f / (2.0f * sqr(0.1f));
+  // exp(-dd^2 / (2 PHI_DEPTH^2)) * exp(-ld / max(PHI_LUMA sqrt(var), 1e-8)),
+  // PHI_DEPTH 0.1, PHI_LUMA 4, PHI_NORMAL 128 (svgf_atrous.wgsl:7-9)
+  const float inv_lum = 1.0f / fmaxf(4.0f * sqrtf(vsum), 1e-8f);
+  const float depth_k = 1.0f / (2.0f * 0.1f * 0.1f);
+  const float KW[3] = {3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
 #pragma unroll
   for (int dy = -2; dy <= 2; ++dy)
 #pragma unroll
     for (int dx = -2; dx <= 2; ++dx) {
       if (dy == 0 && dx == 0) continue;
-      int sx = x + dx * STEP, sy = y + dy * STEP;
-      if (sx < 0 || sy < 0 || sx >= (int)W || sy >= (int)H) continue;
-      float4 snd, srad;
-      float svar;
-      if (kShared) {
-        const int k = slot(sx, sy);
-        snd = s_nd[k];
-        srad = s_rad[k];
-        svar = s_var[k];
-      } else {
-        const uint32_t sid = (uint32_t)sy * W + (uint32_t)sx;
-        snd = nd[sid];
-        srad = in_rad4[sid];
-        svar = in_var[sid];
-      }
-      if (snd.w == 0.0f) continue;
-      float nw = dm::pow128(dm::fmax(dot(cn, f3(snd.x, snd.y, snd.z)), 0.0f));
-      float dd = dm::fabs_(cdepth - snd.w);
-      float ld = dm::fabs_(cl - srad.w);
-      float w = nw * dm::exp_(-(sqr(dd) * depth_k) - ld * inv_lum);
-      w = w * (KW[dx < 0 ? -dx : dx] * KW[dy < 0 ? -dy : dy]);
-      rsum = rsum + f3(srad.x, srad.y, srad.z) * w;
-      vsum = vsum + svar * sqr(w);
-      wsum = wsum + w;
+      const int k = c + dy * kAtrousSpan + dx;
+      const float4 snd = s_nd[k];
+      const float4 srad = s_rad[k];
+      const float svar = s_var[k];
+      float d = __fmaf_rn(cnd.x, snd.x, __fmaf_rn(cnd.y, snd.y, __fmul_rn(cnd.z, snd.z)));
+      d = fmaxf(d, 0.0f);
+      d = d * d; d = d * d; d = d * d; d = d * d; d = d * d; d = d * d; d = d * d;  // ^128
+      const float dd = cnd.w - snd.w;
+      const float e = __fmaf_rn(-fabsf(crad.w - srad.w), inv_lum, -(dd * dd) * depth_k);
+      float w = d * __expf(e) * (KW[dx < 0 ? -dx : dx] * KW[dy < 0 ? -dy : dy]);
+      w = snd.w == 0.0f ? 0.0f : w;  // sky neighbour or outside the image: skipped
+      rsum.x = __fmaf_rn(srad.x, w, rsum.x);
+      rsum.y = __fmaf_rn(srad.y, w, rsum.y);
+      rsum.z = __fmaf_rn(srad.z, w, rsum.z);
+      vsum = __fmaf_rn(svar, w * w, vsum);
+      wsum += w;
     }
-  rsum = rsum / wsum;
-  vsum = vsum / sqr(wsum);
-  uint32_t packed = pack_rgb9e5(rsum);
-  out_rad[id] = packed;
-  out_var[id] = vsum;
-  const float3 q = unpack_rgb9e5(packed);
-  out_rad4[id] = make_float4(q.x, q.y, q.z, luma(q));
-  if (pass_idx == 0) fb.svgf_hist[id] = packed;
+  const float inv_w = 1.0f / wsum;
+  rsum = rsum * inv_w;
+  vsum = vsum * (inv_w * inv_w);
+  const uint32_t packed = pack_rgb9e5(rsum);
+  if (flags & ATR_NEXT) out_rv[id] = make_uint2(packed, __float_as_uint(vsum));
+  if (flags & ATR_HIST) fb.svgf_hist[id] = packed;
+  if (flags & ATR_STATE) state_rad[id] = packed;
+  if (flags & ATR_FINAL) final_dst[id] = packed;
 }
 
-// taa.wgsl:67-171; neighbours come from the pre-TAA copy `src`.
+// taa.wgsl:67-171.  A 16x16 block stages the 18x18 neighbourhood of the
+// pre-TAA frame `src` in shared memory (unpacked once, clamped at zero, with
+// its luma); the 3x3 filter and the colour-box statistics read it from there.
+// Weights and the history clip use hardware division and square root.  Sky
+// pixels keep `src`'s value (the reference leaves them untouched).
 APD float mitchell(float x_, float B, float C) {
   float x = dm::fabs_(2.0f * x_);
   float ods = 1.0f / 6.0f;
@@ -1865,34 +1882,56 @@ APD float mitchell(float x_, float B, float C) {
   return ((12.0f - 9.0f * B - 6.0f * C) * x * x * x + (-18.0f + 12.0f * B + 6.0f * C) * x * x + (6.0f - 2.0f * B)) *
          ods;
 }
-__global__ void k_taa(FrameBuffers fb, Consts c, const uint32_t* src, uint32_t* dst, const uint32_t* prevb) {
-  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+constexpr int kTaaTile = 16;
+constexpr int kTaaSpan = kTaaTile + 2;
+__global__ void __launch_bounds__(256) k_taa(FrameBuffers fb, Consts c, const uint32_t* src, uint32_t* dst,
+                                             const uint32_t* prevb) {
+  __shared__ float4 s_c[kTaaSpan * kTaaSpan];  // max(colour, 0), luma; w < 0 outside the image
+  const int x0 = blockIdx.x * kTaaTile, y0 = blockIdx.y * kTaaTile;
+  const int tid = threadIdx.y * kTaaTile + threadIdx.x;
+  for (int k = tid; k < kTaaSpan * kTaaSpan; k += kTaaTile * kTaaTile) {
+    const int px = x0 + k % kTaaSpan - 1, py = y0 + k / kTaaSpan - 1;
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+    if (px >= 0 && py >= 0 && px < (int)c.W && py < (int)c.H) {
+      const float3 sc = vmax(unpack_rgb9e5(src[(uint32_t)py * c.W + (uint32_t)px]), f3s(0.0f));
+      v = make_float4(sc.x, sc.y, sc.z, luma(sc));
+    }
+    s_c[k] = v;
+  }
+  __syncthreads();
+  const uint32_t x = x0 + threadIdx.x, y = y0 + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
-  uint32_t id = y * c.W + x;
+  const uint32_t id = y * c.W + x;
   const uint32_t cur = c.frame_idx & 1u;
-  float cdepth = __uint_as_float(fb.gb_a[cur][id].w);
-  if (cdepth == 0.0f) return;
-  float3 curc = unpack_rgb9e5(src[id]);
+  const float cdepth = __uint_as_float(fb.gb_a[cur][id].w);
+  const uint32_t csrc = src[id];
+  if (cdepth == 0.0f) {
+    dst[id] = csrc;
+    return;
+  }
+  const float3 curc = unpack_rgb9e5(csrc);
   float wsum = sqr(mitchell(0.0f, 0.33f, 0.33f));
   float3 rec = curc * wsum;
   float3 m1 = curc, m2 = curc * curc;
   float cnt = 1.0f;
+  const int cs = ((int)threadIdx.y + 1) * kTaaSpan + (int)threadIdx.x + 1;
+#pragma unroll
   for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
     for (int dy = -1; dy <= 1; ++dy) {
       if (dx == 0 && dy == 0) continue;
-      int sx = (int)x + dx, sy = (int)y + dy;
-      if (sx < 0 || sy < 0 || sx >= (int)c.W || sy >= (int)c.H) continue;
-      uint32_t sid = (uint32_t)sy * c.W + (uint32_t)sx;
-      float3 sc = vmax(unpack_rgb9e5(src[sid]), f3s(0.0f));
-      float w = mitchell((float)dx, 0.33f, 0.33f) * mitchell((float)dy, 0.33f, 0.33f);
-      w = w * (1.0f / (1.0f + luma(sc)));
+      const float4 v = s_c[cs + dy * kTaaSpan + dx];
+      if (v.w < 0.0f) continue;
+      const float3 sc = f3(v.x, v.y, v.z);
+      const float w = (mitchell((float)dx, 0.33f, 0.33f) * mitchell((float)dy, 0.33f, 0.33f)) *
+                      __frcp_rn(1.0f + v.w);
       rec = rec + sc * w;
       wsum = wsum + w;
       m1 = m1 + sc;
       m2 = m2 + sc * sc;
       cnt = cnt + 1.0f;
     }
-  rec = rec / dm::fmax(wsum, 1e-5f);
+  rec = rec * __frcp_rn(fmaxf(wsum, 1e-5f));
   float3 hist;
   uint32_t pid;
   float2 pp;
@@ -1917,21 +1956,22 @@ __global__ void k_taa(FrameBuffers fb, Consts c, const uint32_t* src, uint32_t* 
   float pdepth = __uint_as_float(fb.gb_a[cur ^ 1u][pid].w);
   float cdcs = depth_cs(cdepth, 0.001f, 10000.0f), pdcs = depth_cs(pdepth, 0.001f, 10000.0f);
   bool vdd = (dm::fabs_(cdcs - pdcs) / cdcs) < 0.1f;
-  float3 mean = m1 / cnt;
-  float3 sd = vabs(m2 - (m1 * m1) / cnt);
-  sd = sd / (cnt - 1.0f);
-  sd = vsqrt(sd);
+  const float inv_cnt = __frcp_rn(cnt);
+  float3 mean = m1 * inv_cnt;
+  float3 sd = vabs(m2 - (m1 * m1) * inv_cnt);
+  sd = sd * __frcp_rn(cnt - 1.0f);
+  sd = f3(sqrtf(sd.x), sqrtf(sd.y), sqrtf(sd.z));
   float3 lo = mean - sd, hi = mean + sd;
   float3 center = 0.5f * (hi + lo);
   float3 ext = 0.5f * (hi - lo);
   float3 rtc = hist - center;
-  float3 rtcu = vabs(rtc / ext);
+  float3 rtcu = vabs(f3(__fdividef(rtc.x, ext.x), __fdividef(rtc.y, ext.y), __fdividef(rtc.z, ext.z)));
   float mxv = dm::fmax(rtcu.x, dm::fmax(rtcu.y, rtcu.z));
-  float3 clipped = mxv > 1.0f ? center + rtc / mxv : hist;
+  float3 clipped = mxv > 1.0f ? center + rtc * __frcp_rn(mxv) : hist;
   float blend = 1.0f - (c.cfg.taa_history_influence * (vdd ? 1.0f : 0.0f));
-  float cw = dm::saturate(blend * (1.0f / (1.0f + luma(rec))));
-  float hw = dm::saturate((1.0f - blend) * (1.0f / (1.0f + luma(clipped))));
-  rec = (cw * rec + hw * clipped) / (cw + hw);
+  float cw = dm::saturate(blend * __frcp_rn(1.0f + luma(rec)));
+  float hw = dm::saturate((1.0f - blend) * __frcp_rn(1.0f + luma(clipped)));
+  rec = (cw * rec + hw * clipped) * __frcp_rn(cw + hw);
   dst[id] = pack_rgb9e5(rec);
 }
 
@@ -2029,7 +2069,6 @@ size_t frame_buffer_bytes(uint32_t W, uint32_t H) {
   add(P * 4); add(P * 4);                   // demod
   add(P * 4); add(P * 4);                   // svgf rad
   add(P * 8); add(P * 8);                   // moments
-  add(P * 4); add(P * 4);                   // variance
   add(P * 4); add(P * 4);                   // count, hist
   add(P * 4);                               // snapshot
   add(P * 4); add(P * 4);                   // queues
@@ -2080,8 +2119,6 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
   fb->svgf_rad[1] = carve<uint32_t>(p, P);
   fb->svgf_mom[0] = carve<float2>(p, P);
   fb->svgf_mom[1] = carve<float2>(p, P);
-  fb->svgf_var[0] = carve<float>(p, P);
-  fb->svgf_var[1] = carve<float>(p, P);
   fb->svgf_count = carve<uint32_t>(p, P);
   fb->svgf_hist = carve<uint32_t>(p, P);
   fb->snapshot = carve<uint32_t>(p, P);
@@ -2100,9 +2137,9 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
   fb->st_d = carve<uint4>(p, P);
   fb->counters = carve<uint32_t>(p, 64);
   fb->visits = carve<unsigned long long>(p, 3 * K_NUM_KINDS);
-  fb->atr_nd = fb->rq_o[0];
-  fb->atr_rad[0] = fb->rq_d[0];
-  fb->atr_rad[1] = fb->rq_o[1];
+  fb->atr_nd = reinterpret_cast<uint2*>(fb->rq_o[0]);
+  fb->atr_rv[0] = reinterpret_cast<uint2*>(fb->rq_d[0]);
+  fb->atr_rv[1] = reinterpret_cast<uint2*>(fb->rq_o[1]);
   fb->out_rgb = carve<float>(p, 3 * P);
   fb->accum = carve<float4>(p, P);
   fb->rgba = carve<uint32_t>(p, P);
@@ -2414,42 +2451,48 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
     k_firefly<<<g2, b2, 0, st>>>(fb, W, H, cur, fb.snapshot, dcur);
     mark(K_FIREFLY);
   }
+  // With a-trous passes the last pass writes the pre-TAA frame straight into
+  // the TAA's neighbourhood copy; otherwise the copy is made here.
+  const bool atrous = cfg.svgf && cfg.svgf_atrous_passes > 0;
+  const bool taa = cfg.taa && frame_idx > 0;
   if (cfg.svgf) {
-    uint32_t f = frame_idx;
+    const uint32_t f = frame_idx, passes = cfg.svgf_atrous_passes;
     k_svgf_temporal<<<g2, b2, 0, st>>>(fb, c, dcur, fb.svgf_rad[(f + 1) % 2], fb.svgf_mom[f % 2],
-                                       fb.svgf_mom[(f + 1) % 2], fb.svgf_var[(f + 1) % 2]);
+                                       fb.svgf_mom[(f + 1) % 2], atrous ? 1 : 0);
     mark(K_SVGF_TEMPORAL);
-    if (cfg.svgf_atrous_passes > 0) {
-      k_atrous_prep<<<lb, 256, 0, st>>>(fb, P, cur, fb.svgf_rad[(f + 1) % 2]);
-      mark(K_ATROUS_PREP);
-    }
-    for (uint32_t i = 0; i < cfg.svgf_atrous_passes; ++i) {
-      const float4* in4 = fb.atr_rad[i & 1u];
-      float4* out4 = fb.atr_rad[(i + 1) & 1u];
-      uint32_t* out_rad = fb.svgf_rad[(f + i) % 2];
-      const float* in_var = fb.svgf_var[(f + 1 + i) % 2];
-      float* out_var = fb.svgf_var[(f + i) % 2];
-      dim3 bt(kAtrousTile, kAtrousTile), gt((W + kAtrousTile - 1) / kAtrousTile, (H + kAtrousTile - 1) / kAtrousTile);
-      switch (i) {
-        case 0: k_atrous<1><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
-        case 1: k_atrous<2><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
-        case 2: k_atrous<4><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
-        case 3: k_atrous<8><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
-        case 4: k_atrous<16><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
-        case 5: k_atrous<32><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
-        case 6: k_atrous<64><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
-        default: k_atrous<128><<<gt, bt, 0, st>>>(fb, W, H, i, in4, out4, out_rad, in_var, out_var); break;
+    // the reference ping-pongs pass i's output into svgf_rad[(f + i) % 2]; of
+    // those stores only the last odd pass's survive into the next frame
+    const int last_odd = passes >= 2 ? (int)(((passes - 1) & 1u) ? passes - 1 : passes - 2) : -1;
+    uint32_t* final_dst = taa ? fb.snapshot : dcur;
+    for (uint32_t i = 0; i < passes; ++i) {
+      const bool last = i == passes - 1;
+      const uint32_t flags = (i == 0 ? ATR_HIST : 0u) | ((int)i == last_odd ? ATR_STATE : 0u) |
+                             (last ? ATR_FINAL : ATR_NEXT);
+      const uint2* in_rv = fb.atr_rv[i & 1u];
+      uint2* out_rv = fb.atr_rv[(i + 1) & 1u];
+      uint32_t* state_rad = fb.svgf_rad[(f + 1) % 2];
+      const uint32_t* final_src = fb.svgf_rad[(f + passes - 1) % 2];
+      const uint32_t step = i < 8 ? (1u << i) : 128u;
+      const uint32_t span = kAtrousTile * step;
+      dim3 bt(kAtrousTile, kAtrousTile), gt(((W + span - 1) / span) * step, ((H + span - 1) / span) * step);
+      switch (step) {
+        case 1: k_atrous<1><<<gt, bt, 0, st>>>(fb, W, H, flags, in_rv, out_rv, state_rad, final_src, final_dst); break;
+        case 2: k_atrous<2><<<gt, bt, 0, st>>>(fb, W, H, flags, in_rv, out_rv, state_rad, final_src, final_dst); break;
+        case 4: k_atrous<4><<<gt, bt, 0, st>>>(fb, W, H, flags, in_rv, out_rv, state_rad, final_src, final_dst); break;
+        case 8: k_atrous<8><<<gt, bt, 0, st>>>(fb, W, H, flags, in_rv, out_rv, state_rad, final_src, final_dst); break;
+        case 16: k_atrous<16><<<gt, bt, 0, st>>>(fb, W, H, flags, in_rv, out_rv, state_rad, final_src, final_dst); break;
+        case 32: k_atrous<32><<<gt, bt, 0, st>>>(fb, W, H, flags, in_rv, out_rv, state_rad, final_src, final_dst); break;
+        case 64: k_atrous<64><<<gt, bt, 0, st>>>(fb, W, H, flags, in_rv, out_rv, state_rad, final_src, final_dst); break;
+        default: k_atrous<128><<<gt, bt, 0, st>>>(fb, W, H, flags, in_rv, out_rv, state_rad, final_src, final_dst); break;
       }
       mark(K_ATROUS);
-      if (i == cfg.svgf_atrous_passes - 1) {
-        cudaMemcpyAsync(dcur, out_rad, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
-        mark(K_COPY);
-      }
     }
   }
-  if (cfg.taa && frame_idx > 0) {
-    cudaMemcpyAsync(fb.snapshot, dcur, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
-    mark(K_COPY);
+  if (taa) {
+    if (!atrous) {
+      cudaMemcpyAsync(fb.snapshot, dcur, (size_t)P * 4, cudaMemcpyDeviceToDevice, st);
+      mark(K_COPY);
+    }
     k_taa<<<g2, b2, 0, st>>>(fb, c, fb.snapshot, dcur, dprev);
     mark(K_TAA);
   }

@@ -41,7 +41,6 @@ struct FrameBuffers {
   uint32_t* demod[2];
   uint32_t* svgf_rad[2];
   float2* svgf_mom[2];
-  float* svgf_var[2];
   uint32_t* svgf_count;
   uint32_t* svgf_hist;
   uint32_t* snapshot;  // pre-filter copy for the firefly filter and TAA
@@ -58,10 +57,11 @@ struct FrameBuffers {
   uint32_t* counters;  // [0..1] path queue sizes, [2] extend cursor, [3] rays traced,
                        // [4..8] ray queue sizes, [9..13] ray queue cursors
   unsigned long long* visits;  // instrumented traversal: per kernel kind {rays, nodes, tris}
-  // a-trous inputs unpacked once: normal + depth per pixel, radiance + luma
-  // (ping-pong); aliases of ray-queue storage, idle after the bounce loop
-  float4* atr_nd;
-  float4* atr_rad[2];
+  // a-trous records: oct30 normal + depth per pixel, and (ping-pong) packed
+  // RGB9E5 radiance + variance; aliases of ray-queue storage, idle after the
+  // bounce loop
+  uint2* atr_nd;
+  uint2* atr_rv[2];
   float* out_rgb;      // linear HDR output, 3 floats per pixel (device)
   float4* accum;       // display accumulation (resolve.wgsl accum_radiance)
   uint32_t* rgba;      // RGBA8 display texture, 64x64-block swizzled

@@ -84,6 +84,7 @@ struct DevScene {
   const float4* tris;       // 3 per TriRec
   const float4* positions;  // world position per vertex (w = 0)
   const uint32_t* normals;  // oct30 per vertex
+  const float* normals_f;   // the same normals as floats, 3 per vertex
   const uint32_t* indices;  // mesh-local vertex index, 3 per triangle
   const uint32_t* tri_material;
   const uint32_t* tri_instance;  // flattened triangle -> instance

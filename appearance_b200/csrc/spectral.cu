@@ -25,6 +25,7 @@
 #include "frame.cuh"
 #include "persistent.cuh"
 #include "spectral.cuh"
+#include "spectral_data.h"
 
 namespace ap {
 
@@ -32,42 +33,83 @@ namespace {
 
 constexpr int kBlock = 128;
 
+// The gold tables (spectral_data.h) in device memory, read through the
+// read-only cache.
+__device__ const float g_au_lambda[spec::kAuSamples] = {SPEC_AU_LAMBDA};
+__device__ const float g_au_eta[spec::kAuSamples] = {SPEC_AU_ETA};
+__device__ const float g_au_k[spec::kAuSamples] = {SPEC_AU_K};
+
+// PiecewiseLinearSpectrum::reflectance over a gold table (spectrum.rs:552-566,
+// find_interval_fast, math/mod.rs:97-113).
+APD float au_sample(const float* vals, float l) {
+  constexpr int n = spec::kAuSamples;
+  if (l < __ldg(&g_au_lambda[0]) || l > __ldg(&g_au_lambda[n - 1])) return 0.0f;
+  int size = n - 2, first = 1;
+  while (size > 0) {
+    const int half = size >> 1, middle = first + half;
+    const bool pred = __ldg(&g_au_lambda[middle]) <= l;
+    first = pred ? middle + 1 : first;
+    size = pred ? size - (half + 1) : half;
+  }
+  const int o = min(max(first - 1, 0), n - 2);
+  const float l0 = __ldg(&g_au_lambda[o]), l1 = __ldg(&g_au_lambda[o + 1]);
+  const float a = __ldg(&vals[o]), b = __ldg(&vals[o + 1]);
+  return a + (b - a) * ((l - l0) / (l1 - l0));
+}
+
 struct GpuGeo {
   const DevScene& s;
-  const spec::Material* mats;
-  const float4* env;
+  const SpectralView& v;
   uint32_t env_w, env_h;
-  float env_scale;
+  float env_scale, env_pdf_integral;
   spec::Sun sun;
 
-  APD void tri(uint32_t g, spec::V3* p0, spec::V3* p1, spec::V3* p2) const {
+  APD void tri_index(uint32_t g, uint32_t* i0, uint32_t* i1, uint32_t* i2) const {
     const InstanceDev& in = s.instances[s.tri_instance[g]];
-    uint32_t fi = in.first_index + (g - in.first_global_tri) * 3;
-    float4 a = s.positions[in.first_vertex + s.indices[fi + 0]];
-    float4 b = s.positions[in.first_vertex + s.indices[fi + 1]];
-    float4 c = s.positions[in.first_vertex + s.indices[fi + 2]];
+    const uint32_t fi = in.first_index + (g - in.first_global_tri) * 3;
+    *i0 = in.first_vertex + s.indices[fi + 0];
+    *i1 = in.first_vertex + s.indices[fi + 1];
+    *i2 = in.first_vertex + s.indices[fi + 2];
+  }
+  APD void tri(uint32_t g, spec::V3* p0, spec::V3* p1, spec::V3* p2) const {
+    uint32_t i0, i1, i2;
+    tri_index(g, &i0, &i1, &i2);
+    const float4 a = s.positions[i0], b = s.positions[i1], c = s.positions[i2];
     *p0 = spec::v3(a.x, a.y, a.z);
     *p1 = spec::v3(b.x, b.y, b.z);
     *p2 = spec::v3(c.x, c.y, c.z);
   }
+  APD void tri_normals(uint32_t g, spec::V3* n0, spec::V3* n1, spec::V3* n2) const {
+    uint32_t i0, i1, i2;
+    tri_index(g, &i0, &i1, &i2);
+    const float* n = s.normals_f;
+    *n0 = spec::v3(n[3 * (size_t)i0], n[3 * (size_t)i0 + 1], n[3 * (size_t)i0 + 2]);
+    *n1 = spec::v3(n[3 * (size_t)i1], n[3 * (size_t)i1 + 1], n[3 * (size_t)i1 + 2]);
+    *n2 = spec::v3(n[3 * (size_t)i2], n[3 * (size_t)i2 + 1], n[3 * (size_t)i2 + 2]);
+  }
   APD const spec::Material& material(uint32_t g) const {
     const InstanceDev& in = s.instances[s.tri_instance[g]];
-    return mats[in.material_idx + s.tri_material[in.first_index / 3 + (g - in.first_global_tri)]];
+    return v.mats[in.material_idx + s.tri_material[in.first_index / 3 + (g - in.first_global_tri)]];
   }
-  APD void env_texel(uint32_t idx, float c[4]) const {
-    float4 v = __ldg(env + idx);
-    c[0] = v.x;
-    c[1] = v.y;
-    c[2] = v.z;
-    c[3] = v.w;
+  APD void env_rgb(uint32_t x, uint32_t y, float c[3]) const {
+    const float* p = s.env + 3 * ((size_t)y * env_w + x);
+    c[0] = __ldg(p);
+    c[1] = __ldg(p + 1);
+    c[2] = __ldg(p + 2);
   }
+  APD void illum_coef(const float rgb[3], float out[4]) const {
+    spec::illum_lookup(v.illum_tab, v.illum_norm, rgb, out);
+  }
+  APD float env_pdf_func(size_t i) const { return __ldg(v.env_pdf + i); }
+  APD float au_eta(float l) const { return au_sample(g_au_eta, l); }
+  APD float au_k(float l) const { return au_sample(g_au_k, l); }
 };
 
 // Per-path state and queues of P paths (one per pixel of the rows).
 struct SpecBuffers {
   float4* rq_o[2];  // extension ray queue (by bounce parity): origin
   float4* rq_d[2];  //   direction, w = owning path (bits)
-  uint2* hits;      // per extension queue slot: t (bits), triangle
+  uint4* hits;      // per extension queue slot: t, u, v (bits), triangle
   float4* sq_o;     // shadow ray queue: origin, w = tmax
   float4* sq_d;     //   direction, w = owning path (bits)
   float4* L;        // spectral radiance of the path (4 wavelengths)
@@ -75,7 +117,8 @@ struct SpecBuffers {
   float4* lambda;   // the path's wavelengths
   float4* shc;      // contribution of the pending shadow ray
   float4* acc;      // linear sRGB sum over the samples so far (xyz)
-  uint4* misc;      // rng state, depth, eta_scale (bits), 0
+  uint4* misc;      // sampler dimension, depth | specular << 16, eta_scale, p_b (bits)
+  uint32_t* morton; // Morton index of the path's sampler pixel
   uint32_t* counters;  // per round: extension size, cursor, shadow size, cursor
   // closest-hit rays, nodes, triangles; any-hit rays, nodes, triangles (nodes
   // and triangles only in the counting form)
@@ -108,7 +151,7 @@ size_t carve(void* base, uint32_t P, const SpectralCache* rc, SpecBuffers* b) {
     b->rq_o[q] = static_cast<float4*>(take(f4));
     b->rq_d[q] = static_cast<float4*>(take(f4));
   }
-  b->hits = static_cast<uint2*>(take(sizeof(uint2) * (size_t)P));
+  b->hits = static_cast<uint4*>(take(sizeof(uint4) * (size_t)P));
   b->sq_o = static_cast<float4*>(take(f4));
   b->sq_d = static_cast<float4*>(take(f4));
   b->L = static_cast<float4*>(take(f4));
@@ -117,6 +160,7 @@ size_t carve(void* base, uint32_t P, const SpectralCache* rc, SpecBuffers* b) {
   b->shc = static_cast<float4*>(take(f4));
   b->acc = static_cast<float4*>(take(f4));
   b->misc = static_cast<uint4*>(take(sizeof(uint4) * (size_t)P));
+  b->morton = static_cast<uint32_t*>(take(sizeof(uint32_t) * (size_t)P));
   b->counters = static_cast<uint32_t*>(take(sizeof(uint32_t) * 4 * (kSpectralMaxDepth + 2)));
   b->stats = static_cast<unsigned long long*>(take(6 * sizeof(unsigned long long)));
   b->cq = b->cT = b->rec = b->bq = nullptr;
@@ -154,21 +198,28 @@ APD void push(bool want, uint32_t* size, float4* qo, float4* qd, spec::V3 o, flo
   qd[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(owner));
 }
 
+// Camera rays of one sample pass: the sample is the reference's 1-spp frame
+// with seed `frame_seed`; the sampler starts at dimension 0 of the path's
+// sampler pixel and gives the wavelengths their first draw.
 __global__ void __launch_bounds__(kBlock) k_sgen(SpecBuffers b, SpectralCamera cam, uint32_t W, uint32_t H,
-                                                 uint32_t row0, uint32_t P, uint32_t sample, uint32_t seed) {
+                                                 uint32_t row0, uint32_t P, uint32_t sample, uint32_t digits,
+                                                 uint64_t frame_seed) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const uint32_t x = p % W, y = row0 + p / W;
   spec::V3 o, d;
   spec::camera_ray(cam.inv_view, cam.inv_proj, x, y, W, H, &o, &d);
-  spec::Rng rng = spec::rng_for(y * W + x, sample, seed);
-  const spec::Wavelengths w = spec::sample_visible(rng.next());
+  uint32_t px, py;
+  spec::sampler_pixel(x, y, W, H, &px, &py);
+  spec::ZSobol z{spec::morton2(px, py), digits, frame_seed, 0u};
+  const spec::Wavelengths w = spec::sample_visible(z.get1d());
   b.rq_o[0][p] = make_float4(o.x, o.y, o.z, 0.0f);
   b.rq_d[0][p] = make_float4(d.x, d.y, d.z, __uint_as_float(p));
   b.lambda[p] = f4(w.lambda);
   b.L[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   b.beta[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-  b.misc[p] = make_uint4(rng.s, 0u, __float_as_uint(1.0f), 0u);
+  b.misc[p] = make_uint4(z.dim, 0u, __float_as_uint(1.0f), __float_as_uint(1.0f));
+  b.morton[p] = z.morton;
   if (sample == 0) b.acc[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
@@ -188,7 +239,8 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s,
         tmax = 1e30f;
       },
       [&](uint32_t i, const Trav& t, const Visits& vc) {
-        b.hits[i] = make_uint2(__float_as_uint(t.hit.t), t.hit.tri);
+        b.hits[i] = make_uint4(__float_as_uint(t.hit.t), __float_as_uint(t.hit.u), __float_as_uint(t.hit.v),
+                               t.hit.tri);
         if (kCount) {
           atomicAdd(&b.stats[1], (unsigned long long)vc.nodes);
           atomicAdd(&b.stats[2], (unsigned long long)vc.tris);
@@ -200,31 +252,34 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s,
 #define AP_SSHADE_MIN_BLOCKS 8  // resident blocks per SM the shading kernel is register-capped for (measured)
 #endif
 __global__ void __launch_bounds__(kBlock, AP_SSHADE_MIN_BLOCKS) k_sshade(DevScene s, SpectralView v, SpecBuffers b,
-                                                                     uint32_t round,
-                                                   uint32_t P, int max_depth) {
+                                                                     uint32_t round, uint32_t P, int max_depth,
+                                                                     uint32_t digits, uint64_t frame_seed) {
   const uint32_t count = round == 0 ? P : min(b.counters[4 * round], P);
   const float4* qo = b.rq_o[round & 1];
   const float4* qd = b.rq_d[round & 1];
   float4* no = b.rq_o[(round + 1) & 1];
   float4* nd = b.rq_d[(round + 1) & 1];
-  const GpuGeo g{s, v.mats, v.env, v.env_w, v.env_h, v.env_scale, v.sun};
+  const GpuGeo g{s, v, v.env_w, v.env_h, v.env_scale, v.env_pdf_integral, v.sun};
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const float4 ro = qo[i], rd = qd[i];
     const uint32_t owner = __float_as_uint(rd.w);
-    const uint2 hh = b.hits[i];
-    if (hh.y == kRcRetired) continue;  // ended in the radiance cache at this vertex
+    const uint4 hh = b.hits[i];
+    if (hh.w == kRcRetired) continue;  // ended in the radiance cache at this vertex
     spec::V3 o = spec::v3(ro.x, ro.y, ro.z), d = spec::v3(rd.x, rd.y, rd.z);
-    const spec::Hit h{__uint_as_float(hh.x), hh.y};
+    const spec::Hit h{__uint_as_float(hh.x), __uint_as_float(hh.y), __uint_as_float(hh.z), hh.w};
     const uint4 m = b.misc[owner];
-    spec::PathState ps{s4of(b.L[owner]), s4of(b.beta[owner]), __uint_as_float(m.z), (int)m.y, spec::Rng{m.x}};
+    spec::PathState ps{s4of(b.L[owner]), s4of(b.beta[owner]), __uint_as_float(m.z), __uint_as_float(m.w),
+                       (m.y >> 16) != 0u, (int)(m.y & 0xffffu),
+                       spec::ZSobol{b.morton[owner], digits, frame_seed, m.x}};
     const spec::S4 lam = s4of(b.lambda[owner]);
     bool shadow;
     spec::ShadowRay sh = {};
-    const bool more = spec::path_vertex(g, o, d, hh.y != kNoHit ? &h : nullptr, lam, ps, max_depth, &shadow, &sh);
+    const bool more = spec::path_vertex(g, o, d, hh.w != kNoHit ? &h : nullptr, lam, ps, max_depth, &shadow, &sh);
     b.L[owner] = f4(ps.L);
     if (more) {
       b.beta[owner] = f4(ps.beta);
-      b.misc[owner] = make_uint4(ps.rng.s, (uint32_t)ps.depth, __float_as_uint(ps.eta_scale), 0u);
+      b.misc[owner] = make_uint4(ps.smp.dim, (uint32_t)ps.depth | (ps.specular ? 1u << 16 : 0u),
+                                 __float_as_uint(ps.eta_scale), __float_as_uint(ps.p_b));
     }
     if (shadow) b.shc[owner] = f4(sh.c);
     push(shadow, &b.counters[4 * round + 2], b.sq_o, b.sq_d, sh.o, sh.tmax, sh.d, owner);
@@ -283,8 +338,8 @@ __global__ void __launch_bounds__(kBlock) k_svertex(DevScene s, SpecBuffers b, S
   const float4* qo = b.rq_o[round & 1];
   const float4* qd = b.rq_d[round & 1];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const uint2 hh = b.hits[i];
-    if (hh.y == kNoHit) continue;
+    const uint4 hh = b.hits[i];
+    if (hh.w == kNoHit) continue;
     const float4 rd = qd[i];
     const uint32_t p = __float_as_uint(rd.w);
     const bool tp = training_path(p, pass, seed, rc.stride);
@@ -294,7 +349,7 @@ __global__ void __launch_bounds__(kBlock) k_svertex(DevScene s, SpecBuffers b, S
     const float t = __uint_as_float(hh.x);
     const spec::V3 o = spec::v3(ro.x, ro.y, ro.z), d = spec::v3(rd.x, rd.y, rd.z);
     float4 q[4];
-    spec_query(s, hh.y, o + d * t, -d, q);
+    spec_query(s, hh.w, o + d * t, -d, q);
     if (tp) {
       float4* r = b.rec + ((size_t)(p / rc.stride) * kRcMaxBounces + round) * kSpecRecord;
       r[0] = q[0]; r[1] = q[1]; r[2] = q[2]; r[3] = q[3];
@@ -311,7 +366,7 @@ __global__ void __launch_bounds__(kBlock) k_svertex(DevScene s, SpecBuffers b, S
       dst[0] = q[0]; dst[1] = q[1]; dst[2] = q[2]; dst[3] = q[3];
       b.cT[j] = b.beta[p];
       b.cown[j] = p;
-      b.hits[i].y = kRcRetired;
+      b.hits[i].w = kRcRetired;
     }
   }
 }
@@ -325,7 +380,9 @@ __global__ void __launch_bounds__(kBlock) k_sapply(SpectralView v, SpecBuffers b
   float rgb[3] = {b.cout[3 * (size_t)j], b.cout[3 * (size_t)j + 1], b.cout[3 * (size_t)j + 2]};
   float c[4];
   spec::illum_lookup(v.illum_tab, v.illum_norm, rgb, c);
-  const spec::S4 Lc = spec::emission4(c, c[3], s4of(b.lambda[p]));
+  const spec::S4 lam = s4of(b.lambda[p]);
+  spec::S4 Lc;
+  for (int i = 0; i < 4; ++i) Lc.v[i] = spec::illum_at(c, lam.v[i]);
   b.L[p] = f4(s4of(b.L[p]) + s4of(b.cT[j]) * Lc);
 }
 
@@ -387,6 +444,31 @@ __global__ void __launch_bounds__(kBlock) k_saccum(SpecBuffers b, uint32_t P, bo
 
 }  // namespace
 
+void spectral_env_distribution(const float* rgb, uint32_t W, uint32_t H, float* func, float* integral) {
+  // Texture::get_sampling_distribution (appearance-texture lib.rs:193-205):
+  // the texel's channel mean, stored x-major
+  const size_t n = (size_t)W * H;
+  for (uint32_t y = 0; y < H; ++y)
+    for (uint32_t x = 0; x < W; ++x) {
+      const float* p = rgb + 3 * ((size_t)y * W + x);
+      func[(size_t)x * H + y] = (p[0] + p[1] + p[2]) / 3.0f;
+    }
+  // InfiniteLight::new (infinite_light.rs:41-54): minus the mean, clamped at 0
+  float average = 0.0f;
+  for (size_t i = 0; i < n; ++i) average += func[i];
+  average /= (float)n;
+  for (size_t i = 0; i < n; ++i) func[i] = spec::fmax_nan(func[i] - average, 0.0f);
+  // PiecewiseConstant2D::new (piecewise_constant.rs:101-125) over rows of W
+  // of that x-major array, and PiecewiseConstant1D's integrals (:21-49)
+  float marginal = 0.0f;
+  for (uint32_t v = 0; v < H; ++v) {
+    float row = 0.0f;
+    for (uint32_t u = 0; u < W; ++u) row = row + func[(size_t)v * W + u] * 1.0f / (float)W;
+    marginal = marginal + row * 1.0f / (float)H;
+  }
+  *integral = marginal;
+}
+
 // Sample passes in flight at once without the cache (launch_spectral).  On a
 // 2048^2 x 16 spp city image (Msamples/s): one pass with its shadow rays beside
 // the next extension 448, two passes 476, three 490, four 503.
@@ -435,6 +517,7 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
   const uint32_t slots = rc ? (P / rc->stride + 1) * kRcMaxBounces : 0u;
   if (rc) cudaMemsetAsync(b.rec, 0, sizeof(float4) * kSpecRecord * slots, st);  // no tags from an earlier call
   const uint32_t rounds = (uint32_t)max_depth + 1;
+  const uint32_t digits = spec::zsobol_digits(W, H);
   const int linear = (int)((P + kBlock - 1) / kBlock);
   const int persistent = num_sms * kTraceMinBlocks;
   const int shade = std::min(linear, num_sms * 16);
@@ -449,11 +532,11 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
       const cudaStream_t sk = streams[h];
       const SpecBuffers& bk = bufs[h];
       cudaMemsetAsync(bk.counters, 0, sizeof(uint32_t) * 4 * (rounds + 1), sk);
-      k_sgen<<<linear, kBlock, 0, sk>>>(bk, cam, W, H, row0, P, k, seed);
+      k_sgen<<<linear, kBlock, 0, sk>>>(bk, cam, W, H, row0, P, k, digits, (uint64_t)seed + k);
       ++launches;
       for (uint32_t r = 0; r < rounds; ++r) {
         k_sextend<false><<<persistent, kBlock, 0, sk>>>(s, bk, r, P);
-        k_sshade<<<shade, kBlock, 0, sk>>>(s, v, bk, r, P, max_depth);
+        k_sshade<<<shade, kBlock, 0, sk>>>(s, v, bk, r, P, max_depth, digits, (uint64_t)seed + k);
         k_sshadow<false><<<persistent, kBlock, 0, sk>>>(s, bk, r, P);
         launches += 3;
       }
@@ -469,7 +552,7 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
   for (uint32_t k = 0; k < spp; ++k) {
     cudaMemsetAsync(b.counters, 0, sizeof(uint32_t) * 4 * (rounds + 1), st);
     if (rc) cudaMemsetAsync(b.ccount + 2, 0, sizeof(uint32_t), st);
-    k_sgen<<<linear, kBlock, 0, st>>>(b, cam, W, H, row0, P, k, seed);
+    k_sgen<<<linear, kBlock, 0, st>>>(b, cam, W, H, row0, P, k, digits, (uint64_t)seed + k);
     ++launches;
     for (uint32_t r = 0; r < rounds; ++r) {
       if (count_visits) k_sextend<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
@@ -483,7 +566,7 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
         k_svertex<<<shade, kBlock, 0, st>>>(s, b, *rc, r, P, k, seed);
         ++launches;
       }
-      k_sshade<<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth);
+      k_sshade<<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth, digits, (uint64_t)seed + k);
       if (overlap && r + 1 < rounds) {
         // only the next shading pass reads what these rays add to L
         cudaEventRecord(fs->fork, st);

@@ -9,16 +9,28 @@
 namespace ap {
 
 // Device tables of the spectral mode: the upsampled material table (one per
-// scene material) and environment texels {sigmoid coefficients, scale}.
+// scene material), the environment's scale and compensated sampling
+// distribution (InfiniteLight, infinite_light.rs:30-67: the function values
+// in the reference's x-major flattening, rows of env_w, and its integral; the
+// environment's RGB texels are the scene's), the distant light, and the
+// illuminant upsampling table.
 struct SpectralView {
   const spec::Material* mats;
-  const float4* env;  // env_w x env_h, or null with env_w = 0
+  const float* env_pdf;  // env_w x env_h, or null with env_w = 0
+  float env_pdf_integral;
   uint32_t env_w, env_h;
   float env_scale;
   spec::Sun sun;
   const float* illum_tab;  // 33^3 x 3 illuminant upsampling coefficients (spec::illum_lookup)
   float illum_norm;
 };
+
+// The compensated environment distribution of the reference's InfiniteLight
+// (texture.get_sampling_distribution, then minus its average, clamped at
+// zero), flattened x-major and cut into rows of env_w as PiecewiseConstant2D
+// reads it, with the integral of that distribution (float sums in the
+// reference's order).  rgb: env_w x env_h texels, row-major.
+void spectral_env_distribution(const float* rgb, uint32_t env_w, uint32_t env_h, float* func, float* integral);
 
 // Radiance-cache mode of the spectral render (the cache of ap_rc_attach):
 // paths are retired at their prefix-th hit into the cache's RGB prediction,

@@ -179,24 +179,16 @@ void upsample_materials(const float* mats26, uint32_t n, Material* out) {
   }
 }
 
-void upsample_env(const float* rgb, size_t texels, float* out4) {
-  const IlluminantTable& tab = illuminant_table();
-  for (size_t i = 0; i < texels; ++i) tab.lookup(rgb + 3 * i, out4 + 4 * i);
-}
-
 Sun make_sun(const float dir[3], const float rgb[3], float scale, float radius) {
   Sun s;
   V3 d = normalize(v3(dir[0], dir[1], dir[2]));
   s.dir[0] = d.x;
   s.dir[1] = d.y;
   s.dir[2] = d.z;
-  float e[4];
-  illuminant_table().lookup(rgb, e);
-  s.coef[0] = e[0];
-  s.coef[1] = e[1];
-  s.coef[2] = e[2];
-  s.scale = scale * e[3];
+  s.scale = scale;
+  illuminant_table().lookup(rgb, s.coef);
   s.radius = radius;
+  s.pad0 = s.pad1 = s.pad2 = 0.0f;
   return s;
 }
 

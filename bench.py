@@ -3,9 +3,9 @@
 Workload (one step = one frame): the seeded 1,310,722-triangle icosphere field
 (1024 icospheres x 1280 triangles + ground quad, 64 emissive spheres, 2048x1024
 procedural sky), 1920x1080, 1 spp, depth 8, ReSTIR DI (32 area candidates,
-temporal M cap 20x, 5-neighbour spatial), ReSTIR GI (temporal; its spatial pass
-is off as in the reference, lib.rs:441), firefly filter, SVGF (5 a-trous
-passes), TAA, camera moving along a 64-frame seeded spline.  Metric: Msamples/s (= pixels x spp / frame time).
+temporal M cap 20x, 5-neighbour spatial), ReSTIR GI (temporal and one unbiased
+5-neighbour spatial pass), firefly filter, SVGF (5 a-trous passes), TAA,
+camera moving along a 64-frame seeded spline.  Metric: Msamples/s (= pixels x spp / frame time).
 
   value   device time of the frames (CUDA events on the renderer's stream),
           scene and frame state resident in HBM.
@@ -17,7 +17,8 @@ passes), TAA, camera moving along a 64-frame seeded spline.  Metric: Msamples/s 
 Run with torchrun for N>1: every rank renders its own independent replica of
 the job (the frame does not shard), so scaling is weak and value sums ranks.
 `--impl reference` times the CPU restatement of the reference frame (the
-reference itself is Rust/WGSL on wgpu and cannot run here) on all host cores.
+reference itself is Rust/WGSL on wgpu and cannot run here) on all host cores,
+on the same 1920x1080 frames of the same workload.
 """
 from __future__ import annotations
 
@@ -36,7 +37,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W_FULL, H_FULL = 1920, 1080
-CPU_W, CPU_H = 960, 540  # CPU samples: same scene, preset and camera path, a quarter of the pixels
+CPU_W, CPU_H = W_FULL, H_FULL  # CPU samples: the same frames of the same workload
+CPU_TIMED_FRAMES = 2
+PRESET = "realtime_gi_spatial"
 METRIC = "Msamples/s (1080p ReSTIR+SVGF+TAA frame, 1.31M-tri scene)"
 
 
@@ -136,8 +139,8 @@ def peaks():
 
 def cpu_baseline(scene, path, cfg) -> dict:
     """The CPU oracle (restatement of the reference frame) on a bounded sample:
-    the same scene, preset and camera path at 960x540 (a quarter of the
-    pixels), 1 warm + 5 timed frames, all host threads."""
+    the same scene, preset, camera path and resolution, 1 warm + 2 timed
+    frames, all host threads."""
     from oracle.oracle import OracleFrame, OracleScene
     w, h = CPU_W, CPU_H
     osc = OracleScene(scene)
@@ -146,7 +149,7 @@ def cpu_baseline(scene, path, cfg) -> dict:
     mats, prev = frame_mats(path, 0, prev, w, h)
     fr.render(mats)  # builds nothing new; first frame warms the history
     t0 = time.perf_counter()
-    frames = 5
+    frames = CPU_TIMED_FRAMES
     for f in range(1, 1 + frames):
         mats, prev = frame_mats(path, f, prev, w, h)
         fr.render(mats)
@@ -164,7 +167,7 @@ def run_reference(args, rank, world):
     from oracle.oracle import OracleFrame, OracleScene
     w, h = CPU_W, CPU_H
     osc = OracleScene(scene)
-    fr = OracleFrame(osc, w, h, presets.REALTIME, threads=os.cpu_count())
+    fr = OracleFrame(osc, w, h, presets.PRESETS[PRESET], threads=os.cpu_count())
     prev = None
     for f in range(args.warmup):
         mats, prev = frame_mats(path, f, prev, w, h)
@@ -181,8 +184,8 @@ def run_reference(args, rank, world):
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                       "data": "synthetic (seeded icosphere field)",
-                      "config": {"workload": "icosphere-field-1.31M-tris realtime frame (CPU sample)", "width": w,
-                                 "height": h},
+                      "config": {"workload": "icosphere-field-1.31M-tris 1920x1080 realtime frame", "width": w,
+                                 "height": h, "spp": 1, "preset": PRESET},
                       "cpu_baseline": {"value": v, "unit": "Msamples/s", "cores": os.cpu_count(), "kind": "port",
                                        "sample": sample},
                       "e2e": {"value": v, "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
@@ -204,7 +207,7 @@ def main():
                                 device_id=torch.device("cuda", local))
     from appearance_b200 import PathTracer, presets, replicas
     scene, path = build_workload()
-    cfg = dict(presets.REALTIME)
+    cfg = dict(presets.PRESETS[PRESET])
     pt = PathTracer(cfg, device=local)
     pt.upload_scene(scene)
     bvh = pt.bvh_stats()
@@ -267,7 +270,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded icosphere field, procedural sky, seeded camera spline)",
             "config": {"workload": "icosphere-field-1.31M-tris 1920x1080 realtime frame", "width": W_FULL,
-                       "height": H_FULL, "spp": 1, "depth": cfg["max_bounces"], "preset": "realtime",
+                       "height": H_FULL, "spp": 1, "depth": cfg["max_bounces"], "preset": PRESET,
+                       "gi_spatial_passes": cfg["gi_spatial_passes"],
                        "parallelism": f"replicas x{world}", "l2": "inputs+state ~1 GB/frame > 126 MB L2",
                        "bvh": bvh},
             "frame_ms": {"median": statistics.median(gpu_ms), "min": min(gpu_ms), "max": max(gpu_ms)},

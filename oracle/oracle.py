@@ -72,10 +72,11 @@ def lib():
         L.orc_detmath.argtypes = [U, P, P, P, U]
         L.orc_resolve_rgba8.argtypes = [P, U, U, U, P, U, P]
         L.orc_spectral_new.restype = P
-        L.orc_spectral_new.argtypes = [P, P, P, F, F, F]
+        L.orc_spectral_new.argtypes = [P, P, P, P, F, F, F]
         L.orc_spectral_free.argtypes = [P]
         L.orc_spectral_render.argtypes = [P, P, P, U, U, U, U, U, ctypes.c_int, U, U, P]
-        L.orc_spectral_tables.argtypes = [P, P, P]
+        L.orc_murmur3_x64_128.argtypes = [P, ctypes.c_size_t, ctypes.c_uint64, P]
+        L.orc_zsobol.argtypes = [U, U, U, ctypes.c_uint64, U, U, U, P, U, P]
         L.orc_spectral_cmf.argtypes = [F, P]
         L.orc_spectral_fit.argtypes = [P, P]
         L.orc_spectral_sigmoid.argtypes = [P, F, P]
@@ -191,7 +192,7 @@ class OracleSpectral:
         self.n_mats = oscene._keep["mat"].shape[0]
         env = oscene._keep["env"]
         self.env_texels = 0 if env is None else env.shape[0] * env.shape[1]
-        self.ptr = lib().orc_spectral_new(oscene.ptr, _p(np.asarray(sun_dir, np.float32)),
+        self.ptr = lib().orc_spectral_new(oscene.ptr, _p(oscene._keep["nrm"]), _p(np.asarray(sun_dir, np.float32)),
                                           _p(np.asarray(sun_rgb, np.float32)), sun_scale, scene_radius, env_scale)
 
     def render(self, mats: np.ndarray, width: int, height: int, spp: int = 1, max_depth: int = 4, seed: int = 0,
@@ -203,16 +204,26 @@ class OracleSpectral:
                                   threads or os.cpu_count(), _p(out))
         return out
 
-    def tables(self):
-        mats = np.zeros((self.n_mats, 12), np.float32)
-        env = np.zeros((self.env_texels, 4), np.float32)
-        lib().orc_spectral_tables(self.ptr, _p(mats), _p(env))
-        return mats, env
-
     def __del__(self):
         if getattr(self, "ptr", None):
             lib().orc_spectral_free(self.ptr)
             self.ptr = None
+
+
+def murmur3_x64_128(data: bytes, seed: int = 0) -> tuple:
+    """MurmurHash3 x64_128 of `data` as (h1, h2)."""
+    buf = np.frombuffer(data, np.uint8) if data else np.zeros(1, np.uint8)
+    out = np.zeros(2, np.uint64)
+    lib().orc_murmur3_x64_128(_p(buf), len(data), seed, _p(out))
+    return int(out[0]), int(out[1])
+
+
+def zsobol(res, spp, seed, pixel, sample_idx, kinds) -> np.ndarray:
+    """The draws of one ZSobol sample stream (1 = get_1d, 2 = get_2d)."""
+    k = np.asarray(kinds, np.uint8)
+    out = np.zeros(int(k.astype(np.int64).sum()), np.float32)
+    lib().orc_zsobol(res[0], res[1], spp, seed, pixel[0], pixel[1], sample_idx, _p(k), len(k), _p(out))
+    return out
 
 
 def spectral_cmf(lam: float) -> np.ndarray:

@@ -173,9 +173,7 @@ struct Frame {
         area_eval = load_eval_data(*scene, area_sample, hit);
         V3 wi = normalize(area_eval.point - hit);
         float wdn = dot(wi, fr.n);
-        const bool lit = area_eval.emission.x != 0.0f || area_eval.emission.y != 0.0f ||
-                         area_eval.emission.z != 0.0f;
-        if (wdn > 0.0f && area_pdf > 0.0f && lit) {  // no emission: target +0, no BSDF evaluation
+        if (wdn > 0.0f && area_pdf > 0.0f) {
           float spdf = 0.0f;
           V3 refl = disney_evaluate(b, fr, wo, wi, &spdf);
           if (spdf > 0.0f) area_phat = luma(refl * wdn * area_eval.emission);
@@ -917,11 +915,6 @@ struct Frame {
         float wsum = 1.0f;
         float cl = luma(rsum);
         float cv = vsum;
-        // exp(-dd^2 / (2 phi_d^2)) * exp(-ld / max(phi_l sqrt(var), 1e-8)) as one
-        // exp of the summed exponents, each division as a product with its
-        // reciprocal; pow(., 128) as seven squarings
-        const float inv_lum = 1.0f / dm::fmax(4.0f * dm::sqrt_(cv), 1e-8f);
-        const float depth_k = 1.0f / (2.0f * sqr(0.1f));
         for (int dy = -2; dy <= 2; ++dy)
           for (int dx = -2; dx <= 2; ++dx) {
             if (dy == 0 && dx == 0) continue;
@@ -932,10 +925,13 @@ struct Frame {
             if (gt_is_sky(sg.depth)) continue;
             V3 srad = rgb9e5_unpack(in_rad[sid]);
             float sl = luma(srad);
-            float nw = dm::pow128(dm::fmax(dot(cur.n, sg.n), 0.0f));
+            // PHI_NORMAL 128, PHI_DEPTH 0.1, PHI_LUMA 4 (svgf_atrous.wgsl:24-26)
+            float nw = dm::pow_(dm::fmax(dot(cur.n, sg.n), 0.0f), 128.0f);
             float dd = dm::fabs_(cur.depth - sg.depth);
+            float dw = dm::exp_(-sqr(dd) / (2.0f * sqr(0.1f)));
             float ld = dm::fabs_(cl - sl);
-            float w = nw * dm::exp_(-(sqr(dd) * depth_k) - ld * inv_lum);
+            float lw = dm::exp_(-ld / (dm::fmax(4.0f * dm::sqrt_(cv), 1e-8f)));
+            float w = nw * dw * lw;
             w = w * (KW[dx < 0 ? -dx : dx] * KW[dy < 0 ? -dy : dy]);
             rsum = rsum + srad * w;
             vsum = vsum + in_var[sid] * sqr(w);

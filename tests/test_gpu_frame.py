@@ -1,10 +1,13 @@
 """CUDA frame vs the oracle under identical PCG streams.
 
-The arithmetic contract (no contraction, IEEE division and square root,
-detmath.h elementary functions, same evaluation order) makes the CUDA frame a
-bit-exact function of its inputs, so renders and every per-pixel state buffer
-(radiance, path payload, G-buffer, DI/GI reservoirs, light-sample context, rays)
-must be identical to the oracle's, frame after frame."""
+The arithmetic contract of the path-tracing stages (no contraction, IEEE
+division and square root, detmath.h elementary functions, same evaluation
+order) makes them a bit-exact function of their inputs: every per-pixel state
+buffer (path payload, G-buffer, DI/GI reservoirs, light-sample context, rays)
+must be identical to the oracle's, frame after frame, and so must frames
+without the SVGF a-trous passes and TAA.  Frames through those passes, whose
+kernels use hardware exp and fused multiply-adds, are held to the tolerance
+stated in tests/parity.py."""
 import os
 
 import numpy as np
@@ -12,6 +15,7 @@ import pytest
 
 from appearance_b200 import PathTracer, presets, scenes
 from oracle.oracle import OracleFrame, OracleScene
+from parity import assert_bits, assert_frame, assert_post_close, rgb9e5_to_rgb, uses_post_tolerance
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -27,16 +31,13 @@ def load_golden_module():
     return mg
 
 
-def assert_bits(a, b, what):
-    a, b = np.asarray(a), np.asarray(b)
-    same = a.view(np.uint32) == b.view(np.uint32)
-    assert same.all(), f"{what}: {(~same).sum()} of {same.size} words differ"
-
-
-def compare_state(pt, of, w, h):
+def compare_state(pt, of, w, h, cfg):
     for which, (name, gw, ow) in BUFFERS.items():
         g = pt.read_buffer(which, gw, w * h)[:, :ow]
-        assert_bits(g, of.buffer(which, ow), name)
+        if name == "radiance" and uses_post_tolerance(cfg):  # remodulated output of the denoise chain
+            assert_post_close(rgb9e5_to_rgb(g), rgb9e5_to_rgb(of.buffer(which, ow)), name)
+        else:
+            assert_bits(g, of.buffer(which, ow), name)
 
 
 @pytest.mark.parametrize("name", ["cornell_plain_32", "spheres_realtime_48x32"])
@@ -47,7 +48,7 @@ def test_golden_fixture(name):
     pt.upload_scene(sc)
     for f in range(len(mats)):
         pt.set_camera_matrices(mats[f])
-        assert_bits(pt.render((w, h)), images[f], f"{name} frame {f}")
+        assert_frame(pt.render((w, h)), images[f], cfg, f"{name} frame {f}")
 
 
 @pytest.mark.parametrize("preset,override", [
@@ -55,7 +56,7 @@ def test_golden_fixture(name):
     ("faithful", dict(di_unbiased=0, gi_unbiased=0)), ("faithful", dict(di_spatial_passes=2)),
     ("realtime", dict(max_bounces=3)), ("realtime_gi_spatial", dict(max_bounces=4, gi_spatial_passes=2)),
 ])
-def test_cornell_sequences_bit_exact(preset, override):
+def test_cornell_sequences_match_oracle(preset, override):
     sc = scenes.cornell_box()
     cfg = dict(presets.PRESETS[preset], **override)
     pt = PathTracer(cfg)
@@ -67,8 +68,8 @@ def test_cornell_sequences_bit_exact(preset, override):
         eye = np.asarray(cam["eye"]) + np.array([0.01 * f, -0.005 * f, 0.0])
         mats, prev = scenes.camera_matrices(eye, cam["target"], cam["fov"], cam["near"], cam["far"], 40, 36, prev)
         pt.set_camera_matrices(mats)
-        assert_bits(pt.render((40, 36)), of.render(mats), f"{preset} frame {f}")
-    compare_state(pt, of, 40, 36)
+        assert_frame(pt.render((40, 36)), of.render(mats), cfg, f"{preset} frame {f}")
+    compare_state(pt, of, 40, 36, cfg)
 
 
 @pytest.mark.parametrize("w,h", [(1, 1), (17, 9), (64, 3), (3, 70), (129, 65)])
@@ -83,8 +84,8 @@ def test_ragged_resolutions(w, h):
     for f in range(2):
         mats, prev = scenes.camera_matrices(path[f][0], path[f][1], 60.0, 0.01, 500.0, w, h, prev)
         pt.set_camera_matrices(mats)
-        assert_bits(pt.render((w, h)), of.render(mats), f"{w}x{h} frame {f}")
-    compare_state(pt, of, w, h)
+        assert_frame(pt.render((w, h)), of.render(mats), cfg, f"{w}x{h} frame {f}")
+    compare_state(pt, of, w, h, cfg)
 
 
 def test_benchmark_scene_small_view():
@@ -99,8 +100,8 @@ def test_benchmark_scene_small_view():
     for f in range(3):
         mats, prev = scenes.camera_matrices(path[f][0], path[f][1], 60.0, 0.01, 1000.0, 96, 54, prev)
         pt.set_camera_matrices(mats)
-        assert_bits(pt.render((96, 54)), of.render(mats), f"benchmark scene frame {f}")
-    compare_state(pt, of, 96, 54)
+        assert_frame(pt.render((96, 54)), of.render(mats), cfg, f"benchmark scene frame {f}")
+    compare_state(pt, of, 96, 54, cfg)
 
 
 def test_row_range_is_a_crop():

@@ -15,7 +15,7 @@ def bench_scene():
 
 
 def render_seq(sc, path, frames, w=1920, h=1080):
-    pt = PathTracer(presets.REALTIME)
+    pt = PathTracer(presets.REALTIME_GI_SPATIAL)
     pt.upload_scene(sc)
     prev, out = None, None
     stats = []
@@ -39,15 +39,18 @@ def test_full_frame_deterministic_and_finite(bench_scene):
     assert launches > 50
 
 
-def test_full_size_frames_match_oracle(bench_scene):
+@pytest.mark.parametrize("preset", ["realtime_gi_spatial", "realtime"])
+def test_full_size_frames_match_oracle(bench_scene, preset):
     """The benchmark workload itself (1920x1080, 1.31M triangles, 2048x1024 sky,
-    realtime preset: ReSTIR DI+GI, SVGF, TAA), two frames along the camera
-    path, against the oracle: identical bits."""
+    ReSTIR DI+GI with and without GI spatial reuse, SVGF, TAA), two frames
+    along the camera path, against the oracle: every path-tracing state buffer
+    bit-identical, the denoised frame within the tolerance of tests/parity.py."""
     import os
     from oracle.oracle import OracleFrame, OracleScene
+    from parity import assert_bits, assert_frame, assert_post_close, rgb9e5_to_rgb
     sc, path = bench_scene
     w, h = 1920, 1080
-    cfg = dict(presets.REALTIME)
+    cfg = dict(presets.PRESETS[preset])
     pt = PathTracer(cfg)
     pt.upload_scene(sc)
     of = OracleFrame(OracleScene(sc), w, h, cfg, threads=os.cpu_count())
@@ -57,6 +60,9 @@ def test_full_size_frames_match_oracle(bench_scene):
         pt.set_camera_matrices(mats)
         got = pt.render((w, h))
         ref = of.render(mats)
-        same = got.view(np.uint32) == ref.view(np.uint32)
-        assert same.all(), f"frame {f}: {(~same).sum()} of {same.size} words differ"
+        assert_frame(got, ref, cfg, f"{preset} frame {f}")
+    for which, ow, name in ((1, 3, "payload"), (2, 6, "gbuffer"), (3, 8, "di"), (4, 8, "gi"), (5, 4, "ctx")):
+        gw = {1: 4, 2: 8, 3: 8, 4: 8, 5: 4}[which]
+        assert_bits(pt.read_buffer(which, gw, w * h)[:, :ow], of.buffer(which, ow), name)
+    assert_post_close(rgb9e5_to_rgb(pt.read_buffer(0, 1, w * h)), rgb9e5_to_rgb(of.buffer(0, 1)), "radiance")
     pt.close()

@@ -1,13 +1,17 @@
-"""Spectral mode on the GPU vs the oracle: both run the same hero-wavelength
-integrator (spectral.h) under the same per-(pixel, sample) PCG streams, the
-GPU through the compressed 8-wide BVH and the oracle through its binary BVH,
-so the images must be identical bit for bit."""
+"""Spectral mode on the GPU vs the oracle.  The GPU runs the library's
+restatement of the reference's CPU spectral tracer (spectral.h, in a
+wavefront), the oracle its own restatement (oracle_spectral.cpp), both from
+the same ZSobol draws, the GPU through the compressed 8-wide BVH and the oracle
+through its binary BVH.  Images agree within the tolerance stated in
+tests/parity.py; images of the GPU path itself (repeats, row ranges, four
+passes in flight) agree bit for bit."""
 import numpy as np
 import pytest
 
 from appearance_b200 import PathTracer, presets, scenes
 from appearance_b200.renderer import RendererError
 from oracle.oracle import OracleScene, OracleSpectral
+from parity import assert_spectral_close
 
 pytestmark = pytest.mark.gpu
 
@@ -39,7 +43,7 @@ CASES = {
 # k % 4-th); spp 5 wraps around to the first stream, spp 2 leaves two idle
 @pytest.mark.parametrize("case,spp,depth,seed", [("cornell", 2, 4, 0), ("cornell", 1, 16, 5), ("field", 2, 8, 3),
                                                  ("field", 1, 16, 11), ("cornell", 5, 6, 7)])
-def test_spectral_matches_oracle_bit_exact(case, spp, depth, seed):
+def test_spectral_matches_oracle(case, spp, depth, seed):
     make, cam, light = CASES[case]
     sc = make()
     w, h = 64, 48
@@ -51,7 +55,7 @@ def test_spectral_matches_oracle_bit_exact(case, spp, depth, seed):
     img = pt.render_spectral((w, h), spp=spp, max_depth=depth, seed=seed)
     ref = OracleSpectral(OracleScene(sc), **light).render(mats, w, h, spp=spp, max_depth=depth, seed=seed)
     assert img.mean() > 0.0
-    assert_bits(img, ref, f"{case} spp={spp} depth={depth}")
+    assert_spectral_close(img, ref, f"{case} spp={spp} depth={depth}")
     # a row range renders the same rows
     part = pt.render_spectral((w, h), spp=spp, max_depth=depth, seed=seed, start_row=7, end_row=30)
     assert_bits(part, img[7:30], "rows 7..30")
@@ -93,7 +97,7 @@ def test_spectral_device_only_and_errors():
 
 def test_spectral_full_city_matches_oracle():
     """The large spectral configuration's scene (10.0M-triangle city, sky,
-    depth 16) at a reduced image size: identical bits."""
+    gold windows, depth 16) at a reduced image size."""
     import os
     sc = scenes.city()
     w = h = 96
@@ -109,7 +113,7 @@ def test_spectral_full_city_matches_oracle():
     ref = OracleSpectral(OracleScene(sc), **light).render(mats, w, h, spp=2, max_depth=16, seed=3,
                                                         threads=os.cpu_count())
     assert img.mean() > 0.0
-    assert_bits(img, ref, "city 96x96 spp=2 depth=16")
+    assert_spectral_close(img, ref, "city 96x96 spp=2 depth=16")
 
 
 def test_spectral_cache_mode():

@@ -1,5 +1,6 @@
-"""Spectral-mode building blocks on the CPU (oracle_spectral.cpp over spectral.h):
-matching functions, wavelength sampling, RGB upsampling, and the CPU render's
+"""Spectral-mode building blocks on the CPU (the oracle's restatement of the
+reference's CPU tracer, oracle_spectral.cpp): matching functions, wavelength
+sampling, RGB upsampling, the ZSobol sampler and its hash, and the CPU render's
 basic properties."""
 import math
 import os
@@ -92,22 +93,50 @@ def _small_scene():
     return sc
 
 
-def test_spectral_tables_of_a_scene():
-    sc = _small_scene()
-    os_ = oracle.OracleScene(sc)
-    spec = oracle.OracleSpectral(os_, env_scale=1.0)
-    mats, env = spec.tables()
-    assert mats.shape == (sc.materials.shape[0], 12)
-    np.testing.assert_array_equal(mats[:, 3], sc.materials[:, 3])   # metallic
-    np.testing.assert_array_equal(mats[:, 8], sc.materials[:, 8])   # transmission
-    emissive = np.any(sc.materials[:, 5:8] > 0, axis=1)
-    assert np.all(mats[emissive, 7] > 0) and np.all(mats[~emissive, 7] == 0)
-    assert env.shape == (64 * 32, 4) and np.all(env[:, 3] >= 0)
-    # emission scale = 2 max(rgb) x the illuminant normaliser
-    norm = oracle.spectral_illuminant_norm()
-    assert 0.9 < norm < 1.1
-    i = int(np.argmax(emissive))
-    assert mats[i, 7] == pytest.approx(2.0 * sc.materials[i, 5:8].max() * norm, rel=1e-6)
+def test_illuminant_normaliser_is_near_one():
+    assert 0.9 < oracle.spectral_illuminant_norm() < 1.1
+
+
+def test_murmur3_x64_128_matches_its_published_verification_value():
+    """MurmurHash3 x64_128, which the ZSobol sampler hashes (dimension, seed)
+    with (the murmurhash3 crate): SMHasher's verification test hashes the keys
+    [0..i) with seed 256 - i for i = 0..255, hashes the concatenated results
+    with seed 0 and reads the first four bytes little-endian."""
+    hashes = b""
+    for i in range(256):
+        h1, h2 = oracle.murmur3_x64_128(bytes(range(i)), 256 - i)
+        hashes += h1.to_bytes(8, "little") + h2.to_bytes(8, "little")
+    h1, _ = oracle.murmur3_x64_128(hashes, 0)
+    assert h1 & 0xFFFFFFFF == 0x6384BA69
+    assert oracle.murmur3_x64_128(b"", 0) == (0, 0)
+
+
+def _block_draws(x0, y0, n, seed, kinds, res=(64, 64)):
+    return np.array([oracle.zsobol(res, 1, seed, (x0 + x, y0 + y), 0, kinds) for y in range(n) for x in range(n)])
+
+
+@pytest.mark.parametrize("seed", [0, 7])
+def test_zsobol_pixels_of_an_aligned_block_stratify_every_draw(seed):
+    """At one sample per pixel the 4^k pixels of an aligned 2^k x 2^k block
+    take 4^k consecutive (permuted) Sobol indices, so each draw over the block
+    is a stratified set: every 1-D draw puts one value in each of 256 equal
+    intervals, every 2-D draw one point in each cell of a 16 x 16 grid."""
+    kinds = [1, 2, 1, 2, 1]  # wavelength, light sample, light pick, BSDF, roulette order
+    d = _block_draws(16, 32, 16, seed, kinds)
+    assert d.shape == (256, 7) and np.all((d >= 0.0) & (d <= 1.0))
+    for col in (0, 3, 6):
+        assert sorted(np.floor(d[:, col] * 256).astype(int).tolist()) == list(range(256))
+    for cx, cy in ((1, 2), (4, 5)):
+        cells = np.floor(d[:, cx] * 16).astype(int) * 16 + np.floor(d[:, cy] * 16).astype(int)
+        assert sorted(cells.tolist()) == list(range(256))
+
+
+def test_zsobol_streams_depend_on_pixel_seed_and_dimension():
+    a = oracle.zsobol((64, 64), 1, 0, (3, 5), 0, [1, 1, 1, 1])
+    assert len(set(a.tolist())) == 4                      # successive dimensions differ
+    assert not np.array_equal(a, oracle.zsobol((64, 64), 1, 1, (3, 5), 0, [1, 1, 1, 1]))  # frame seed
+    assert not np.array_equal(a, oracle.zsobol((64, 64), 1, 0, (4, 5), 0, [1, 1, 1, 1]))  # pixel
+    np.testing.assert_array_equal(a, oracle.zsobol((64, 64), 1, 0, (3, 5), 0, [1, 1, 1, 1]))
 
 
 def test_spectral_render_is_deterministic_and_threads_agree():
