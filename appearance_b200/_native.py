@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libappearance_cuda.so")
 AP_OK, AP_E_INVALID, AP_E_OOM, AP_E_CUDA, AP_E_TIMEOUT, AP_E_UNSUPPORTED, AP_E_NO_SCENE = range(7)
 
 EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error", "ap_set_config",
-           "ap_world_action", "ap_scene_upload", "ap_set_camera_matrices", "ap_render_hdr", "ap_render_rgba8", "ap_render_device",
+           "ap_world_action", "ap_scene_upload", "ap_model_register", "ap_set_camera_matrices", "ap_render_hdr", "ap_render_rgba8", "ap_render_device",
            "ap_device_framebuffer", "ap_trace_rays", "ap_trace_rays_static", "ap_read_buffer", "ap_profile_frame",
            "ap_bvh_stats", "ap_server_create", "ap_server_destroy", "ap_server_last_error", "ap_server_add_scene",
            "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_stats",
@@ -79,6 +79,7 @@ def load() -> ctypes.CDLL:
     L.ap_set_config.argtypes = [P, ctypes.POINTER(FrameConfig)]
     L.ap_world_action.argtypes = [P, U32, P, ctypes.c_size_t]
     L.ap_scene_upload.argtypes = [P, ctypes.POINTER(SceneDesc)]
+    L.ap_model_register.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(SceneDesc)]
     L.ap_set_camera_matrices.argtypes = [P, P]
     L.ap_render_hdr.argtypes = [P, U32, U32, U32, U32, P, ctypes.c_size_t, ctypes.POINTER(FrameStats)]
     L.ap_render_rgba8.argtypes = [P, U32, U32, U32, U32, ctypes.c_int, P, ctypes.c_size_t, ctypes.POINTER(FrameStats)]

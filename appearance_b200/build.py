@@ -14,9 +14,11 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libappearance_cuda.so")
-SOURCES = ["frame.cu", "api.cu", "noalloc.cu", "serve.cu", "mlp.cu", "spectral.cu", "bvh_build.cpp", "spectral_fit.cpp"]
+SOURCES = ["frame.cu", "api.cu", "noalloc.cu", "serve.cu", "mlp.cu", "spectral.cu", "bvh_build.cpp", "spectral_fit.cpp",
+           "world.cpp"]
 HEADERS = ["detmath.h", "dev_common.cuh", "dev_shade.cuh", "traverse.cuh", "frame.cuh", "scene_layout.h",
-           "bvh_build.h", "spectral.h", "spectral.cuh", "spectral_fit.h", "persistent.cuh", "device_scope.h"]
+           "bvh_build.h", "spectral.h", "spectral.cuh", "spectral_fit.h", "persistent.cuh", "device_scope.h",
+           "spectral_tables.h", "spectral_data.h", "world.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-Xptxas", "-v"]
 

@@ -16,6 +16,7 @@
 #include "spectral.cuh"
 #include "spectral_fit.h"
 #include "traverse.cuh"
+#include "world.h"
 
 namespace {
 
@@ -100,6 +101,8 @@ struct Handle {
   size_t spec_out_bytes = 0;
   SpectralView spec{};
   bool spec_ready = false;
+  // base scene, registered models and spawned instances (world actions)
+  World world;
   void spec_release() {
     if (spec_mats) cudaFree(spec_mats);
     if (spec_env) cudaFree(spec_env);
@@ -274,8 +277,11 @@ int ensure_frame(Handle* h, uint32_t w, uint32_t hgt) {
   return AP_OK;
 }
 
+int world_sync(Handle* h);
+
 int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats, FrameProfiler* prof = nullptr) {
   if (w == 0 || hgt == 0 || (uint64_t)w * hgt > (1ull << 28)) return fail(h, AP_E_INVALID, "bad resolution");
+  if (int wrc = world_sync(h)) return wrc;
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
   const FrameConfig& c = h->cfg;
   if (c.sample_count == 0 || c.max_bounces == 0 || c.max_bounces > 64 || c.di_area_samples > 1024 ||
@@ -323,161 +329,7 @@ int render_common(Handle* h, uint32_t w, uint32_t hgt, ap_frame_stats* stats, Fr
   return AP_OK;
 }
 
-}  // namespace
-
-namespace ap {
-// Scene, stream and error slot of a handle, for entry points defined in other
-// translation units (noalloc.cu).  Returns AP_E_NO_SCENE when no scene is loaded.
-int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream, int* num_sms, int* device,
-                         std::string** err) {
-  Handle* h = static_cast<Handle*>(hp);
-  if (!h) return AP_E_INVALID;
-  *err = &h->err;
-  if (!h->scene.valid) {
-    h->err = "no scene uploaded";
-    return AP_E_NO_SCENE;
-  }
-  *scene = &h->scene.view;
-  *stream = h->stream;
-  *num_sms = h->num_sms;
-  *device = h->device;
-  return AP_OK;
-}
-
-// Device bytes held by a handle's scene (0 without one).
-size_t handle_scene_bytes(void* hp) {
-  Handle* h = static_cast<Handle*>(hp);
-  return (h && h->scene.valid) ? h->scene.bytes : 0;
-}
-}  // namespace ap
-
-extern "C" {
-
-void ap_frame_config_default(ap_frame_config* c) {
-  if (!c) return;
-  c->max_bounces = 2;
-  c->sample_count = 1;
-  c->restir_di = 1;
-  c->restir_gi = 1;
-  c->svgf = 0;
-  c->firefly_filter = 1;
-  c->taa = 0;
-  c->di_area_samples = 4;
-  c->di_bsdf_samples = 1;
-  c->di_temporal_m_factor = 20.0f;
-  c->di_spatial_passes = 1;
-  c->di_spatial_samples = 3;
-  c->di_unbiased = 1;
-  c->gi_temporal_m_cap = 30.0f;
-  c->gi_spatial_passes = 0;
-  c->gi_spatial_samples = 5;
-  c->gi_unbiased = 1;
-  c->svgf_max_history = 24;
-  c->svgf_atrous_passes = 5;
-  c->taa_history_influence = 0.8f;
-}
-
-void* ap_create(const ap_frame_config* cfg, int device, int* err) {
-  int dummy;
-  if (!err) err = &dummy;
-  *err = AP_OK;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
-    *err = AP_E_CUDA;
-    return nullptr;
-  }
-  Handle* h = new Handle();
-  h->device = device;
-  if (cfg) std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
-  else ap_frame_config_default(reinterpret_cast<ap_frame_config*>(&h->cfg));
-  ap::DeviceScope device_scope(device);
-  if (device_scope.status() != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
-      frame_streams_create(&h->fs) != 0) {
-    *err = AP_E_CUDA;
-    if (h->ev0) cudaEventDestroy(h->ev0);
-    if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->stream) cudaStreamDestroy(h->stream);
-    delete h;
-    return nullptr;
-  }
-  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
-  return h;
-}
-
-void ap_destroy(void* hp) {
-  Handle* h = static_cast<Handle*>(hp);
-  if (!h) return;
-  ap::DeviceScope device_scope(h->device);
-  if (h->stream) cudaStreamSynchronize(h->stream);
-  h->scene.release();
-  if (h->frame_mem) cudaFree(h->frame_mem);
-  if (h->trace_mem) cudaFree(h->trace_mem);
-  if (h->rc_mem) cudaFree(h->rc_mem);
-  h->spec_release();
-  if (h->spec_out) cudaFree(h->spec_out);
-  if (h->prof.created)
-    for (int i = 0; i <= FrameProfiler::kMax; ++i) cudaEventDestroy(h->prof.ev[i]);
-  frame_streams_destroy(&h->fs);
-  if (h->ev0) cudaEventDestroy(h->ev0);
-  if (h->ev1) cudaEventDestroy(h->ev1);
-  if (h->stream) cudaStreamDestroy(h->stream);
-  delete h;
-}
-
-const char* ap_last_error(const void* hp) {
-  const Handle* h = static_cast<const Handle*>(hp);
-  return h ? h->err.c_str() : "null handle";
-}
-
-int ap_set_config(void* hp, const ap_frame_config* cfg) {
-  Handle* h = static_cast<Handle*>(hp);
-  if (!h || !cfg) return AP_E_INVALID;
-  std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
-  // a new configuration starts a new frame sequence: drop the temporal state
-  ap::DeviceScope device_scope(h->device);
-  cudaStreamSynchronize(h->stream);
-  if (h->frame_mem) cudaFree(h->frame_mem);
-  h->frame_mem = nullptr;
-  h->W = h->H = 0;
-  h->frame_idx = 0;
-  h->have_prev = false;
-  return AP_OK;
-}
-
-int ap_world_action(void* hp, uint32_t ty, const void* bytes, size_t len) {
-  Handle* h = static_cast<Handle*>(hp);
-  if (!h) return AP_E_INVALID;
-  switch (ty) {
-    case 0: {  // CameraUpdateData {Mat4, fov, near, far, pad}
-      if (!bytes || len != 80) return fail(h, AP_E_INVALID, "CameraUpdate expects 80 bytes");
-      const float* f = static_cast<const float*>(bytes);
-      for (int i = 0; i < 16; ++i) h->cam_transform[i] = f[i];
-      h->fov = f[16];
-      h->znear = f[17];
-      h->zfar = f[18];
-      h->explicit_mats = false;
-      return AP_OK;
-    }
-    case 4: {  // Clear
-      if (!bytes || len != 4) return fail(h, AP_E_INVALID, "Clear expects 4 bytes");
-      ap::DeviceScope device_scope(h->device);
-      cudaStreamSynchronize(h->stream);
-      h->scene.release();
-      return AP_OK;
-    }
-    case 1:
-    case 2:
-    case 3:
-      return fail(h, AP_E_UNSUPPORTED, "SpawnModel/TransformModel/DestroyModel name glTF assets; upload meshes with ap_scene_upload");
-    default:
-      return fail(h, AP_E_INVALID, "unknown world action type");
-  }
-}
-
-int ap_scene_upload(void* hp, const ap_scene_desc* d) {
-  Handle* h = static_cast<Handle*>(hp);
-  if (!h || !d) return AP_E_INVALID;
+int validate_scene(Handle* h, const ap_scene_desc* d) {
   if (!d->positions || !d->normals || !d->indices || !d->tri_material || !d->meshes || !d->materials)
     return fail(h, AP_E_INVALID, "scene: null array");
   if (d->num_meshes == 0 || d->num_materials == 0) return fail(h, AP_E_INVALID, "scene: no meshes or materials");
@@ -500,6 +352,11 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
       if (me.material_idx + d->tri_material[me.first_index / 3 + t] >= d->num_materials)
         return fail(h, AP_E_INVALID, "scene: triangle material out of range");
   }
+  return AP_OK;
+}
+
+// Replaces the device scene with `d` (validated) and builds its BVH.
+int upload_scene(Handle* h, const ap_scene_desc* d) {
   ap::DeviceScope device_scope(h->device);
   cudaStreamSynchronize(h->stream);
   h->scene.release();
@@ -649,6 +506,207 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
   return AP_OK;
 }
 
+// Re-uploads the world after world actions changed it (the reference rebuilds
+// its TLAS before every frame, scene_resources/mod.rs:218-276).
+int world_sync(Handle* h) {
+  if (!h->world.dirty) return AP_OK;
+  h->world.dirty = false;
+  HostScene flat;
+  h->world.flatten(&flat);
+  if (flat.meshes.empty()) {
+    ap::DeviceScope device_scope(h->device);
+    cudaStreamSynchronize(h->stream);
+    h->scene.release();
+    h->spec_release();
+    return AP_OK;
+  }
+  const ap_scene_desc d = flat.desc();
+  int rc = validate_scene(h, &d);
+  if (rc) return rc;
+  return upload_scene(h, &d);
+}
+
+}  // namespace
+
+namespace ap {
+// Scene, stream and error slot of a handle, for entry points defined in other
+// translation units (noalloc.cu).  Returns AP_E_NO_SCENE when no scene is loaded.
+int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream, int* num_sms, int* device,
+                         std::string** err) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  *err = &h->err;
+  if (int rc = world_sync(h)) return rc;
+  if (!h->scene.valid) {
+    h->err = "no scene uploaded";
+    return AP_E_NO_SCENE;
+  }
+  *scene = &h->scene.view;
+  *stream = h->stream;
+  *num_sms = h->num_sms;
+  *device = h->device;
+  return AP_OK;
+}
+
+// Device bytes held by a handle's scene (0 without one).
+size_t handle_scene_bytes(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  return (h && h->scene.valid) ? h->scene.bytes : 0;
+}
+}  // namespace ap
+
+extern "C" {
+
+void ap_frame_config_default(ap_frame_config* c) {
+  if (!c) return;
+  c->max_bounces = 2;
+  c->sample_count = 1;
+  c->restir_di = 1;
+  c->restir_gi = 1;
+  c->svgf = 0;
+  c->firefly_filter = 1;
+  c->taa = 0;
+  c->di_area_samples = 4;
+  c->di_bsdf_samples = 1;
+  c->di_temporal_m_factor = 20.0f;
+  c->di_spatial_passes = 1;
+  c->di_spatial_samples = 3;
+  c->di_unbiased = 1;
+  c->gi_temporal_m_cap = 30.0f;
+  c->gi_spatial_passes = 0;
+  c->gi_spatial_samples = 5;
+  c->gi_unbiased = 1;
+  c->svgf_max_history = 24;
+  c->svgf_atrous_passes = 5;
+  c->taa_history_influence = 0.8f;
+}
+
+void* ap_create(const ap_frame_config* cfg, int device, int* err) {
+  int dummy;
+  if (!err) err = &dummy;
+  *err = AP_OK;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    *err = AP_E_CUDA;
+    return nullptr;
+  }
+  Handle* h = new Handle();
+  h->device = device;
+  if (cfg) std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
+  else ap_frame_config_default(reinterpret_cast<ap_frame_config*>(&h->cfg));
+  ap::DeviceScope device_scope(device);
+  if (device_scope.status() != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess ||
+      frame_streams_create(&h->fs) != 0) {
+    *err = AP_E_CUDA;
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return nullptr;
+  }
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+  return h;
+}
+
+void ap_destroy(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return;
+  ap::DeviceScope device_scope(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  h->scene.release();
+  if (h->frame_mem) cudaFree(h->frame_mem);
+  if (h->trace_mem) cudaFree(h->trace_mem);
+  if (h->rc_mem) cudaFree(h->rc_mem);
+  h->spec_release();
+  if (h->spec_out) cudaFree(h->spec_out);
+  if (h->prof.created)
+    for (int i = 0; i <= FrameProfiler::kMax; ++i) cudaEventDestroy(h->prof.ev[i]);
+  frame_streams_destroy(&h->fs);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+const char* ap_last_error(const void* hp) {
+  const Handle* h = static_cast<const Handle*>(hp);
+  return h ? h->err.c_str() : "null handle";
+}
+
+int ap_set_config(void* hp, const ap_frame_config* cfg) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !cfg) return AP_E_INVALID;
+  std::memcpy(&h->cfg, cfg, sizeof(FrameConfig));
+  // a new configuration starts a new frame sequence: drop the temporal state
+  ap::DeviceScope device_scope(h->device);
+  cudaStreamSynchronize(h->stream);
+  if (h->frame_mem) cudaFree(h->frame_mem);
+  h->frame_mem = nullptr;
+  h->W = h->H = 0;
+  h->frame_idx = 0;
+  h->have_prev = false;
+  return AP_OK;
+}
+
+int ap_world_action(void* hp, uint32_t ty, const void* bytes, size_t len) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h) return AP_E_INVALID;
+  switch (ty) {
+    case 0: {  // CameraUpdateData {Mat4, fov, near, far, pad}
+      if (!bytes || len != 80) return fail(h, AP_E_INVALID, "CameraUpdate expects 80 bytes");
+      const float* f = static_cast<const float*>(bytes);
+      for (int i = 0; i < 16; ++i) h->cam_transform[i] = f[i];
+      h->fov = f[16];
+      h->znear = f[17];
+      h->zfar = f[18];
+      h->explicit_mats = false;
+      return AP_OK;
+    }
+    case 4: {  // Clear
+      if (!bytes || len != 4) return fail(h, AP_E_INVALID, "Clear expects 4 bytes");
+      h->world.clear();
+      return world_sync(h);
+    }
+    case 1:
+    case 2:
+    case 3: {
+      const uint8_t* b = static_cast<const uint8_t*>(bytes);
+      std::string msg;
+      const int rc = ty == 1 ? h->world.spawn(b, len, &msg)
+                             : (ty == 2 ? h->world.transform(b, len, &msg) : h->world.destroy(b, len, &msg));
+      return rc ? fail(h, rc, msg) : AP_OK;
+    }
+    default:
+      return fail(h, AP_E_INVALID, "unknown world action type");
+  }
+}
+
+int ap_scene_upload(void* hp, const ap_scene_desc* d) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !d) return AP_E_INVALID;
+  int rc = validate_scene(h, d);
+  if (rc) return rc;
+  h->world.base.assign(*d);
+  h->world.instances.clear();
+  h->world.dirty = false;
+  return upload_scene(h, d);
+}
+
+int ap_model_register(void* hp, const char* asset_path, const ap_scene_desc* d) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (!h || !d || !asset_path) return AP_E_INVALID;
+  const std::string path(asset_path);
+  if (path.empty() || path.size() >= 256) return fail(h, AP_E_INVALID, "model: asset path must have 1..255 bytes");
+  int rc = validate_scene(h, d);
+  if (rc) return rc;
+  h->world.models[path].assign(*d);
+  for (const World::Instance& in : h->world.instances)
+    if (in.path == path) h->world.dirty = true;
+  return AP_OK;
+}
+
+
 int ap_set_camera_matrices(void* hp, const float* m) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h || !m) return AP_E_INVALID;
@@ -737,6 +795,7 @@ const float* ap_device_framebuffer(const void* hp) {
 int ap_trace_rays(void* hp, const float* origins_tmax, const float* dirs, uint32_t n, int any_hit, uint32_t* out4) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return AP_E_INVALID;
+  if (int wrc = world_sync(h)) return wrc;
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
   if (!origins_tmax || !dirs || !out4) return fail(h, AP_E_INVALID, "null buffer");
   if (n == 0) return AP_OK;
@@ -848,6 +907,7 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
                       float env_scale) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h || !sun_dir3 || !sun_rgb3) return AP_E_INVALID;
+  if (int wrc = world_sync(h)) return wrc;
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
   if (!(scene_radius > 0.0f) || !(sun_scale >= 0.0f) || !(env_scale >= 0.0f) ||
       !(sun_dir3[0] * sun_dir3[0] + sun_dir3[1] * sun_dir3[1] + sun_dir3[2] * sun_dir3[2] > 0.0f))
@@ -898,6 +958,7 @@ int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
                     uint64_t* visits6) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return AP_E_INVALID;
+  if (int wrc = world_sync(h)) return wrc;
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
   if (!h->spec_ready) return fail(h, AP_E_INVALID, "spectral mode not set up (ap_spectral_setup)");
   if (w == 0 || hgt == 0 || w > 65536 || row_start >= row_end || row_end > hgt || spp == 0 || max_depth == 0 ||
@@ -981,6 +1042,7 @@ int ap_profile_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, 
 int ap_bvh_stats(void* hp, uint32_t* out8) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h || !out8) return AP_E_INVALID;
+  if (int wrc = world_sync(h)) return wrc;
   if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
   const BvhStats& s = h->scene.stats;
   out8[0] = s.num_nodes;

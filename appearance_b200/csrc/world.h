@@ -1,0 +1,66 @@
+// The world of a renderer handle as the reference's world actions build it
+// (VisibleWorldActionType, crates/appearance-world/src/visible_world_action.rs:
+// 9-125; handled by PathTracerGpu's SceneResources::handle_visible_world_action,
+// crates/appearance-path-tracer-gpu/src/scene_resources/mod.rs:107-156):
+// models registered under an asset path (the reference loads them from its
+// asset database by that path), instances spawned from them with a 4x4
+// transform and an entity uuid, moved, destroyed, cleared.  The device scene
+// of a handle is the uploaded base scene plus every live instance, flattened
+// to world space in spawn order (the reference rebuilds its TLAS before every
+// frame); a change marks the world dirty and the next render re-uploads it.
+#pragma once
+
+#include <stdint.h>
+
+#include <array>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/appearance_cuda.h"
+
+namespace ap {
+
+// An owned copy of an ap_scene_desc.
+struct HostScene {
+  std::vector<float> positions, normals, env;
+  std::vector<uint32_t> indices, tri_material;
+  std::vector<ap_mesh> meshes;
+  std::vector<ap_material> materials;
+  uint32_t env_w = 0, env_h = 0;
+  float sun[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  void assign(const ap_scene_desc& d);
+  ap_scene_desc desc() const;
+  uint32_t num_tris() const { return (uint32_t)(indices.size() / 3); }
+};
+
+// Wire sizes of the world actions (bytemuck layouts, visible_world_action.rs).
+constexpr size_t kSpawnModelBytes = 64 + 16 + 256;  // Mat4, Uuid, asset path
+constexpr size_t kTransformModelBytes = 64 + 16;    // Mat4, Uuid
+constexpr size_t kDestroyModelBytes = 16;           // Uuid
+
+struct World {
+  struct Instance {
+    std::array<uint8_t, 16> uuid;
+    std::string path;
+    float m[16];  // column-major (glam Mat4)
+  };
+  HostScene base;
+  std::map<std::string, HostScene> models;
+  std::vector<Instance> instances;  // spawn order
+  bool dirty = false;
+
+  // Each returns AP_OK or an AP_E_* status with `err` set.
+  int spawn(const uint8_t* bytes, size_t len, std::string* err);
+  int transform(const uint8_t* bytes, size_t len, std::string* err);
+  int destroy(const uint8_t* bytes, size_t len, std::string* err);
+  // Clear: drops the base scene and every instance (the registered models
+  // stay, as the reference's asset database does).
+  void clear();
+  // base + instances, in world space: positions by the instance transform,
+  // normals by its inverse transpose (renormalised); a model's materials are
+  // appended once, the first time one of its instances is.
+  void flatten(HostScene* out) const;
+};
+
+}  // namespace ap

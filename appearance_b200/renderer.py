@@ -112,6 +112,41 @@ class PathTracer:
         d, self._scene_keep = scene_desc(scene)
         self._check(self._lib.ap_scene_upload(self._h, ctypes.byref(d)))
 
+    def register_model(self, asset_path: str, model: Scene):
+        """ap_model_register: the geometry SpawnModel instantiates by `asset_path`
+        (model space; a glTF file read by appearance_b200.gltf, for example)."""
+        d, keep = scene_desc(model)
+        self._check(self._lib.ap_model_register(self._h, asset_path.encode(), ctypes.byref(d)))
+        del keep
+
+    @staticmethod
+    def spawn_model_bytes(transform_col_major, entity_uuid: bytes, asset_path: str) -> bytes:
+        """SpawnModelData {Mat4, Uuid, [u8; 256]} (visible_world_action.rs:17-48)."""
+        p = asset_path.encode()
+        if len(p) > 255 or len(entity_uuid) != 16:
+            raise ValueError("asset path of at most 255 bytes and a 16-byte uuid")
+        m = np.asarray(transform_col_major, np.float32).reshape(16)
+        return m.tobytes() + bytes(entity_uuid) + p + bytes(256 - len(p))
+
+    @staticmethod
+    def transform_model_bytes(transform_col_major, entity_uuid: bytes) -> bytes:
+        """TransformModelData {Mat4, Uuid} (visible_world_action.rs:50-55)."""
+        if len(entity_uuid) != 16:
+            raise ValueError("16-byte uuid")
+        return np.asarray(transform_col_major, np.float32).reshape(16).tobytes() + bytes(entity_uuid)
+
+    def spawn_model(self, entity_uuid: bytes, asset_path: str, transform_col_major):
+        self.handle_visible_world_action(1, self.spawn_model_bytes(transform_col_major, entity_uuid, asset_path))
+
+    def transform_model(self, entity_uuid: bytes, transform_col_major):
+        self.handle_visible_world_action(2, self.transform_model_bytes(transform_col_major, entity_uuid))
+
+    def destroy_model(self, entity_uuid: bytes):
+        self.handle_visible_world_action(3, bytes(entity_uuid))
+
+    def clear(self):
+        self.handle_visible_world_action(4, struct.pack("<I", 0))
+
     def set_camera_matrices(self, mats: np.ndarray):
         m = np.ascontiguousarray(mats, np.float32).reshape(64)
         self._check(self._lib.ap_set_camera_matrices(self._h, _ptr(m)))

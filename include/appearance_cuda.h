@@ -131,15 +131,37 @@ const char* ap_last_error(const void* handle);
 int ap_set_config(void* handle, const ap_frame_config* cfg);
 
 /* NodeRenderer::visible_world_action (node.rs:16): `ty` and `bytes` exactly as
- * VisibleWorldActionType::from_ty_and_bytes (visible_world_action.rs:87-96).
- * 0 CameraUpdate {Mat4 transform, fov deg, near, far, pad} is applied;
- * 4 Clear drops the scene; 1 SpawnModel / 2 TransformModel / 3 DestroyModel
- * name glTF assets and entity uuids, which this library does not load:
- * they return AP_E_UNSUPPORTED (use ap_scene_upload). */
+ * VisibleWorldActionType::from_ty_and_bytes (visible_world_action.rs:87-96),
+ * handled as PathTracerGpu's SceneResources does
+ * (crates/appearance-path-tracer-gpu/src/scene_resources/mod.rs:107-156):
+ *   0 CameraUpdate {Mat4 transform, fov deg, near, far, pad}, 80 bytes;
+ *   1 SpawnModel {Mat4 transform, Uuid entity, [u8; 256] asset path}, 336
+ *     bytes: an instance of the model registered under that path
+ *     (ap_model_register; AP_E_INVALID when none is), keyed by the uuid;
+ *   2 TransformModel {Mat4 transform, Uuid entity}, 80 bytes: moves the
+ *     instance (AP_E_INVALID for an unknown uuid, which the reference only
+ *     logs);
+ *   3 DestroyModel {Uuid entity}, 16 bytes: removes it;
+ *   4 Clear (u32), 4 bytes: drops the base scene and all instances.
+ * Matrices are glam Mat4, column-major.  The scene the renders see is the
+ * uploaded base scene plus every instance, flattened to world space; a world
+ * action that changes it takes effect at the next render (which rebuilds
+ * the BVH, as the reference rebuilds its TLAS before every frame) and drops
+ * the spectral tables (call ap_spectral_setup again). */
 int ap_world_action(void* handle, uint32_t ty, const void* bytes, size_t len);
 
-/* Uploads (replaces) the scene and builds its wide BVH. */
+/* Uploads (replaces) the base scene, removes every spawned instance, and
+ * builds the wide BVH. */
 int ap_scene_upload(void* handle, const ap_scene_desc* desc);
+
+/* Registers (or replaces) the model SpawnModel names by `asset_path` (1..255
+ * bytes): its meshes, materials and vertex pool in model space, as an
+ * ap_scene_desc whose environment and sun are ignored.  The reference loads a
+ * model from its asset database by that path (a glTF file,
+ * AssetDatabase<Model>::get, scene_resources/mod.rs:121); a host loads the
+ * file itself (appearance_b200/gltf.py reads glTF 2.0) and registers its
+ * geometry here. */
+int ap_model_register(void* handle, const char* asset_path, const ap_scene_desc* model);
 
 /* Explicit camera: inv_view, inv_proj, view_proj, prev_view_proj as 4
  * column-major float[16], used for the next render (overrides CameraUpdate). */
@@ -217,9 +239,10 @@ int ap_bvh_stats(void* handle, uint32_t* out8);
  * Replaces the render of crates/appearance-path-tracer/src/lib.rs:79-195
  * (PathTracer::render -> path_tracer::render_pixels, path_tracer.rs:28-67 ->
  * PathIntegrator::li, path_integrator.rs:103-307): four hero wavelengths per
- * path, RGB albedos and emitters upsampled to spectra, diffuse / conductor /
- * dielectric BxDFs, the distant light by next-event estimation and the
- * environment on escape.
+ * path, RGB albedos and emitters upsampled to spectra, diffuse / gold
+ * conductor / dielectric BxDFs, interpolated vertex normals, the distant light
+ * by next-event estimation and the environment on escape, weighted by the
+ * power heuristic against its compensated sampling density.
  *
  * ap_spectral_setup builds the spectral tables of the uploaded scene (call
  * again after every ap_scene_upload): the distant light travels along
@@ -230,12 +253,15 @@ int ap_bvh_stats(void* handle, uint32_t* out8);
 int ap_spectral_setup(void* handle, const float* sun_dir3, const float* sun_rgb3, float sun_scale, float scene_radius,
                       float env_scale);
 /* Renders rows [row_start, row_end) of a w x h image with `spp` paths per
- * pixel through the pixel centre (the reference renders 1 per frame), paths of
- * at most max_depth surface interactions (the reference uses 4), random
- * numbers from (pixel, sample, seed).  out_rgb receives linear sRGB, 3 floats
- * per pixel, the mean over the samples; with out_rgb NULL the image stays on
- * the device (timing).  Synchronous; stats->gpu_ms is the kernel's device time
- * and stats->extension_rays the rays it traced (closest and shadow). */
+ * pixel through the pixel centre, paths of at most max_depth surface
+ * interactions (the reference uses 4).  Sample k of every pixel is the
+ * reference's 1-sample frame with frame index seed + k: the same ZSobol
+ * sampler (zsobol_sampler.rs, seeded with the frame index) at the pixel the
+ * reference derives from the flipped uv (path_tracer.rs:52-56).  out_rgb
+ * receives linear sRGB, 3 floats per pixel, the mean over the samples; with
+ * out_rgb NULL the image stays on the device (timing).  Synchronous;
+ * stats->gpu_ms is the kernel's device time and stats->extension_rays the rays
+ * it traced (closest and shadow). */
 int ap_render_spectral(void* handle, uint32_t w, uint32_t h, uint32_t row_start, uint32_t row_end, uint32_t spp,
                        uint32_t max_depth, uint32_t seed, float* out_rgb, size_t out_bytes, ap_frame_stats* stats);
 /* ap_render_spectral (image kept on the device) with the traversal kernels in
