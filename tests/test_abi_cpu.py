@@ -56,3 +56,36 @@ def test_camera_update_wire_format():
     b = PathTracer.camera_update_bytes(m, 60.0, 0.1, 300.0)
     assert len(b) == 80  # CameraUpdateData: Mat4 + fov + near + far + pad
     assert struct.unpack_from("<fff", b, 64) == (60.0, np.float32(0.1), 300.0)
+
+
+def _c_params(src, name):
+    m = re.search(r"\b" + name + r"\s*\(([^)]*)\)", src, re.S)
+    args = m.group(1).strip()
+    return 0 if args in ("", "void") else len(args.split(","))
+
+
+def test_rust_ffi_crate_declares_the_header():
+    """ffi/appearance-path-tracer-cuda/src/ffi.rs (no Rust toolchain here to
+    compile it) declares every entry point of the header with as many
+    parameters, and its #[repr(C)] structs list the header's fields in order."""
+    hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "appearance_cuda.h")).read(), flags=re.S)
+    rs = open(os.path.join(ROOT, "ffi", "appearance-path-tracer-cuda", "src", "ffi.rs")).read()
+    rs_fns = dict(re.findall(r"pub fn (ap_[a-z0-9_]+)\(([^)]*)\)", rs, re.S))
+    assert sorted(rs_fns) == declared_symbols()
+    for name, args in rs_fns.items():
+        n_rs = 0 if not args.strip() else len([a for a in args.split(",") if a.strip()])
+        assert n_rs == _c_params(hdr, name), name
+    for c_name, rs_name in (("ap_frame_config", "ApFrameConfig"), ("ap_material", "ApMaterial"),
+                            ("ap_mesh", "ApMesh"), ("ap_frame_stats", "ApFrameStats"), ("ap_job", "ApJob"),
+                            ("ap_job_result", "ApJobResult")):
+        body = re.search(r"typedef struct " + c_name + r" \{(.*?)\} " + c_name, hdr, re.S).group(1)
+        c_fields = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            names = decl.split(None, 1)[1] if decl.split()[0] not in ("const",) else decl.split(None, 2)[2]
+            c_fields += [n.strip().lstrip("*").split("[")[0] for n in names.split(",")]
+        rs_body = re.search(r"pub struct " + rs_name + r" \{(.*?)\n\}", rs, re.S).group(1)
+        rs_fields = re.findall(r"pub ([a-z0-9_]+):", rs_body)
+        assert rs_fields == c_fields, rs_name
