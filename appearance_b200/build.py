@@ -18,7 +18,7 @@ SOURCES = ["frame.cu", "api.cu", "noalloc.cu", "serve.cu", "mlp.cu", "spectral.c
            "world.cpp"]
 HEADERS = ["detmath.h", "dev_common.cuh", "dev_shade.cuh", "traverse.cuh", "frame.cuh", "scene_layout.h",
            "bvh_build.h", "spectral.h", "spectral.cuh", "spectral_fit.h", "persistent.cuh", "device_scope.h",
-           "spectral_tables.h", "spectral_data.h", "world.h"]
+           "spectral_tables.h", "spectral_data.h", "world.h", "traverse2.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-Xptxas", "-v"]
 

@@ -16,6 +16,7 @@
 #include "spectral.cuh"
 #include "spectral_fit.h"
 #include "traverse.cuh"
+#include "traverse2.cuh"
 #include "world.h"
 
 namespace {
@@ -62,6 +63,25 @@ struct DeviceScene {
   }
 };
 
+// The device copy of a world's two-level form (World::build_two_level),
+// used by the ray queries when the world has spawned instances.
+struct DeviceTwoLevel {
+  void *nodes = nullptr, *tris = nullptr, *tlas_nodes = nullptr, *tlas_leaves = nullptr, *insts = nullptr;
+  DevScene view{};  // nodes / tris: the BLAS pool
+  TwoLevel tl{};
+  uint64_t version = ~0ull;
+  bool valid = false;
+  void release() {
+    void** all[] = {&nodes, &tris, &tlas_nodes, &tlas_leaves, &insts};
+    for (void** p : all) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+    valid = false;
+    version = ~0ull;
+  }
+};
+
 struct Handle {
   FrameConfig cfg{};
   int device = 0;
@@ -103,6 +123,7 @@ struct Handle {
   bool spec_ready = false;
   // base scene, registered models and spawned instances (world actions)
   World world;
+  DeviceTwoLevel two_level;
   void spec_release() {
     if (spec_mats) cudaFree(spec_mats);
     if (spec_env) cudaFree(spec_env);
@@ -526,13 +547,59 @@ int world_sync(Handle* h) {
   return upload_scene(h, &d);
 }
 
+// The two-level form of a world with spawned instances (null without
+// instances: the flat scene is the world), rebuilt after a change.
+int two_level_sync(Handle* h, const TwoLevel** out) {
+  *out = nullptr;
+  if (h->world.instances.empty()) {
+    h->two_level.release();
+    return AP_OK;
+  }
+  DeviceTwoLevel& t = h->two_level;
+  if (t.valid && t.version == h->world.version) {
+    *out = &t.tl;
+    return AP_OK;
+  }
+  ap::DeviceScope device_scope(h->device);
+  cudaStreamSynchronize(h->stream);
+  t.release();
+  TwoLevelHost host;
+  std::string err;
+  if (!h->world.build_two_level((uint32_t)kTraversalStack, &host, &err)) return fail(h, AP_E_INVALID, err);
+  auto put = [&](void** dst, const void* src, size_t bytes, const char* what) {
+    int rc = check_cuda(h, cudaMalloc(dst, std::max<size_t>(bytes, 16)), what);
+    if (!rc && bytes) rc = check_cuda(h, cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), what);
+    return rc;
+  };
+  int rc = 0;
+  if ((rc = put(&t.nodes, host.nodes.data(), sizeof(WideNode) * host.nodes.size(), "BLAS nodes")) ||
+      (rc = put(&t.tris, host.tris.data(), sizeof(TriRec) * host.tris.size(), "BLAS triangles")) ||
+      (rc = put(&t.tlas_nodes, host.tlas_nodes.data(), sizeof(WideNode) * host.tlas_nodes.size(), "TLAS nodes")) ||
+      (rc = put(&t.tlas_leaves, host.tlas_leaves.data(), sizeof(TriRec) * host.tlas_leaves.size(), "TLAS leaves")) ||
+      (rc = put(&t.insts, host.insts.data(), sizeof(InstRec) * host.insts.size(), "instances"))) {
+    t.release();
+    return rc;
+  }
+  std::memset(&t.view, 0, sizeof(t.view));
+  t.view.nodes = static_cast<const uint4*>(t.nodes);
+  t.view.tris = static_cast<const float4*>(t.tris);
+  t.tl.tlas_nodes = static_cast<const uint4*>(t.tlas_nodes);
+  t.tl.tlas_leaves = static_cast<const float4*>(t.tlas_leaves);
+  t.tl.insts = static_cast<const InstRec*>(t.insts);
+  t.tl.num_insts = (uint32_t)host.insts.size();
+  t.version = h->world.version;
+  t.valid = true;
+  *out = &t.tl;
+  return AP_OK;
+}
+
 }  // namespace
 
 namespace ap {
 // Scene, stream and error slot of a handle, for entry points defined in other
 // translation units (noalloc.cu).  Returns AP_E_NO_SCENE when no scene is loaded.
-int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream, int* num_sms, int* device,
-                         std::string** err) {
+int handle_trace_context(void* hp, const DevScene** scene, const TwoLevel** two_level, cudaStream_t* stream,
+                         int* num_sms, int* device, std::string** err) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return AP_E_INVALID;
   *err = &h->err;
@@ -541,7 +608,8 @@ int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream,
     h->err = "no scene uploaded";
     return AP_E_NO_SCENE;
   }
-  *scene = &h->scene.view;
+  if (int rc = two_level_sync(h, two_level)) return rc;
+  *scene = *two_level ? &h->two_level.view : &h->scene.view;
   *stream = h->stream;
   *num_sms = h->num_sms;
   *device = h->device;
@@ -615,6 +683,7 @@ void ap_destroy(void* hp) {
   ap::DeviceScope device_scope(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   h->scene.release();
+  h->two_level.release();
   if (h->frame_mem) cudaFree(h->frame_mem);
   if (h->trace_mem) cudaFree(h->trace_mem);
   if (h->rc_mem) cudaFree(h->rc_mem);
@@ -690,6 +759,7 @@ int ap_scene_upload(void* hp, const ap_scene_desc* d) {
   h->world.base.assign(*d);
   h->world.instances.clear();
   h->world.dirty = false;
+  ++h->world.version;
   return upload_scene(h, d);
 }
 
@@ -701,6 +771,7 @@ int ap_model_register(void* hp, const char* asset_path, const ap_scene_desc* d) 
   int rc = validate_scene(h, d);
   if (rc) return rc;
   h->world.models[path].assign(*d);
+  ++h->world.version;
   for (const World::Instance& in : h->world.instances)
     if (in.path == path) h->world.dirty = true;
   return AP_OK;
@@ -800,6 +871,8 @@ int ap_trace_rays(void* hp, const float* origins_tmax, const float* dirs, uint32
   if (!origins_tmax || !dirs || !out4) return fail(h, AP_E_INVALID, "null buffer");
   if (n == 0) return AP_OK;
   ap::DeviceScope device_scope(h->device);
+  const TwoLevel* tl = nullptr;
+  if (int trc = two_level_sync(h, &tl)) return trc;
   size_t need = (size_t)n * 48 + 256;
   if (h->trace_bytes < need) {
     if (h->trace_mem) cudaFree(h->trace_mem);
@@ -815,7 +888,8 @@ int ap_trace_rays(void* hp, const float* origins_tmax, const float* dirs, uint32
   uint32_t* cursor = reinterpret_cast<uint32_t*>(p + (size_t)n * 48);
   cudaMemcpyAsync(o, origins_tmax, (size_t)n * 16, cudaMemcpyHostToDevice, h->stream);
   cudaMemcpyAsync(dd, dirs, (size_t)n * 16, cudaMemcpyHostToDevice, h->stream);
-  launch_trace_batch(h->scene.view, o, dd, n, any_hit, out, cursor, h->num_sms, h->stream);
+  launch_trace_batch(tl ? h->two_level.view : h->scene.view, o, dd, n, any_hit, out, cursor, h->num_sms, h->stream,
+                     tl);
   int rc = check_cuda(h, cudaGetLastError(), "trace launch");
   if (rc) return rc;
   cudaMemcpyAsync(out4, out, (size_t)n * 16, cudaMemcpyDeviceToHost, h->stream);

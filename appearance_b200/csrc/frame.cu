@@ -17,6 +17,7 @@
 #include "frame.cuh"
 #include "persistent.cuh"
 #include "traverse.cuh"
+#include "traverse2.cuh"
 
 namespace ap {
 
@@ -2040,6 +2041,25 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_batch(DevScen
       });
 }
 
+// The same batch over a two-level scene (traverse2.cuh).
+template <bool kAny>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_batch2(DevScene s, TwoLevel tl,
+                                                                         const float4* origins, const float4* dirs,
+                                                                         uint32_t n, uint4* out, uint32_t* cursor) {
+  persistent_trace2<kAny, false>(
+      s, tl, n, cursor,
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        const float4 a = origins[i], b = dirs[i];
+        o = f3(a.x, a.y, a.z);
+        d = f3(b.x, b.y, b.z);
+        tmax = a.w;
+      },
+      [&](uint32_t i, const Trav& t, const Visits&) {
+        if (kAny) out[i] = make_uint4(t.hit.tri != kNoHit ? 1u : 0u, 0u, 0u, 0u);
+        else out[i] = make_uint4(__float_as_uint(t.hit.t), __float_as_uint(t.hit.u), __float_as_uint(t.hit.v), t.hit.tri);
+      });
+}
+
 template <typename T>
 T* carve(char*& p, size_t count) {
   T* r = reinterpret_cast<T*>(p);
@@ -2510,8 +2530,13 @@ void encode_resolve_rgba8(const FrameBuffers& fb, uint32_t W, uint32_t H, uint32
 }
 
 void launch_trace_batch(const DevScene& scene, const float4* origins, const float4* dirs, uint32_t n, int any_hit,
-                        uint4* out, uint32_t* cursor, int num_sms, cudaStream_t st) {
+                        uint4* out, uint32_t* cursor, int num_sms, cudaStream_t st, const TwoLevel* tl) {
   cudaMemsetAsync(cursor, 0, 4, st);
+  if (tl) {
+    if (any_hit) k_trace_batch2<true><<<num_sms * kTraceMinBlocks, kBlock, 0, st>>>(scene, *tl, origins, dirs, n, out, cursor);
+    else k_trace_batch2<false><<<num_sms * kTraceMinBlocks, kBlock, 0, st>>>(scene, *tl, origins, dirs, n, out, cursor);
+    return;
+  }
   if (any_hit) k_trace_batch<true><<<num_sms * kTraceMinBlocks, kBlock, 0, st>>>(scene, origins, dirs, n, out, cursor);
   else k_trace_batch<false><<<num_sms * kTraceMinBlocks, kBlock, 0, st>>>(scene, origins, dirs, n, out, cursor);
 }

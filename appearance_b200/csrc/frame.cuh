@@ -163,7 +163,12 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
 void encode_resolve_rgba8(const FrameBuffers& fb, uint32_t W, uint32_t H, uint32_t spp, uint32_t accum_count,
                           cudaStream_t st);
 
+struct TwoLevel;
+// Closest or any hit of n rays (origin + tmax, direction): over `scene`, or
+// over the two-level scene `tl` (with `scene` holding its BLAS pool) when
+// given.
 void launch_trace_batch(const DevScene& scene, const float4* origins, const float4* dirs, uint32_t n,
-                        int any_hit, uint4* out, uint32_t* cursor, int num_sms, cudaStream_t stream);
+                        int any_hit, uint4* out, uint32_t* cursor, int num_sms, cudaStream_t stream,
+                        const TwoLevel* tl = nullptr);
 
 }  // namespace ap

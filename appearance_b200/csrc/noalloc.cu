@@ -38,8 +38,8 @@
 #include "frame.cuh"
 
 namespace ap {
-int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream, int* num_sms, int* device,
-                         std::string** err);
+int handle_trace_context(void* hp, const DevScene** scene, const TwoLevel** two_level, cudaStream_t* stream,
+                         int* num_sms, int* device, std::string** err);
 }
 
 namespace {
@@ -81,10 +81,11 @@ int cuda_fail(std::string* err, cudaError_t e, const char* what) {
 extern "C" int ap_trace_rays_static(void* handle, const float* origins_tmax, const float* dirs, uint32_t n,
                                     int any_hit, uint32_t* out4) {
   const ap::DevScene* scene = nullptr;
+  const ap::TwoLevel* two_level = nullptr;
   cudaStream_t stream = nullptr;
   int num_sms = 0, device = 0;
   std::string* err = nullptr;
-  int rc = ap::handle_trace_context(handle, &scene, &stream, &num_sms, &device, &err);
+  int rc = ap::handle_trace_context(handle, &scene, &two_level, &stream, &num_sms, &device, &err);
   if (rc != AP_OK) return rc;
   if (!origins_tmax || !dirs || !out4) {
     *err = "null buffer";
@@ -119,7 +120,8 @@ extern "C" int ap_trace_rays_static(void* handle, const float* origins_tmax, con
   if ((e = cudaMemcpyAsync(o, origins_tmax, (size_t)n * 16, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
       (e = cudaMemcpyAsync(d, dirs, (size_t)n * 16, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
     return fail_after_queue(e, "ray upload");
-  ap::launch_trace_batch(*scene, o, d, n, any_hit, hits, cursor, num_sms, stream);  // zeroes the cursor first
+  ap::launch_trace_batch(*scene, o, d, n, any_hit, hits, cursor, num_sms, stream,
+                         two_level);  // zeroes the cursor first
   if ((e = cudaGetLastError()) != cudaSuccess) return fail_after_queue(e, "trace launch");
   if ((e = cudaMemcpyAsync(out4, hits, (size_t)n * 16, cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
     return fail_after_queue(e, "hit readback");

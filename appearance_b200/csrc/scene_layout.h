@@ -79,6 +79,16 @@ struct EmissiveTri {
   float emission[3], pad3;
 };
 
+// Instance of a two-level scene (traverse2.cuh), 128 bytes: world-to-object
+// and object-to-world transforms (row-major 3x4), the root of its model's
+// BLAS in the node pool, its first global triangle id, its model.
+struct InstRec {
+  float w2o[12];
+  uint32_t blas_root, tri_base, model, pad0;
+  float o2w[12];
+  uint32_t pad1[4];
+};
+
 struct DevScene {
   const uint4* nodes;       // 5 per WideNode
   const float4* tris;       // 3 per TriRec

@@ -35,8 +35,8 @@
 #include "frame.cuh"
 
 namespace ap {
-int handle_trace_context(void* hp, const DevScene** scene, cudaStream_t* stream, int* num_sms, int* device,
-                         std::string** err);
+int handle_trace_context(void* hp, const DevScene** scene, const TwoLevel** two_level, cudaStream_t* stream,
+                         int* num_sms, int* device, std::string** err);
 size_t handle_scene_bytes(void* hp);
 }  // namespace ap
 
@@ -130,9 +130,10 @@ bool launch_job(Server* s, Job* j, Slot& sl) {
   const ap_job& d = j->desc;
   const DevScene* scene = nullptr;
   cudaStream_t unused_stream;
+  const TwoLevel* unused_two_level = nullptr;  // server scenes are flat uploads
   int sms = 0, dev = 0;
   std::string* err = nullptr;
-  ap::handle_trace_context(s->scenes[d.scene], &scene, &unused_stream, &sms, &dev, &err);
+  ap::handle_trace_context(s->scenes[d.scene], &scene, &unused_two_level, &unused_stream, &sms, &dev, &err);
   FrameConfig cfg = s->base;
   cfg.sample_count = d.spp;
   cfg.max_bounces = d.max_depth;

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/appearance_cuda.h"
+#include "scene_layout.h"
 
 namespace ap {
 
@@ -39,6 +40,23 @@ constexpr size_t kSpawnModelBytes = 64 + 16 + 256;  // Mat4, Uuid, asset path
 constexpr size_t kTransformModelBytes = 64 + 16;    // Mat4, Uuid
 constexpr size_t kDestroyModelBytes = 16;           // Uuid
 
+// The two-level form of a world (traverse2.cuh): one object-space BLAS per
+// model in a shared node / triangle pool (triangle records carry the model's
+// triangle index), a TLAS over the instances' world boxes (records carry the
+// instance index), and the instances: the base scene first (identity), then
+// every spawned instance in spawn order, so that global triangle ids are the
+// flattened world's.
+struct TwoLevelHost {
+  std::vector<WideNode> nodes, tlas_nodes;
+  std::vector<TriRec> tris, tlas_leaves;
+  std::vector<InstRec> insts;
+  uint32_t max_stack = 0;  // TLAS stack bound + the largest BLAS bound + 1
+};
+
+// World-to-object rows (row-major 3x4) of a column-major Mat4: its inverse
+// by cofactors in double, rounded to float.
+void inverse_rows(const float m[16], float w2o[12]);
+
 struct World {
   struct Instance {
     std::array<uint8_t, 16> uuid;
@@ -49,6 +67,7 @@ struct World {
   std::map<std::string, HostScene> models;
   std::vector<Instance> instances;  // spawn order
   bool dirty = false;
+  uint64_t version = 0;  // bumped by every change of the base scene, a model or an instance
 
   // Each returns AP_OK or an AP_E_* status with `err` set.
   int spawn(const uint8_t* bytes, size_t len, std::string* err);
@@ -61,6 +80,8 @@ struct World {
   // normals by its inverse transpose (renormalised); a model's materials are
   // appended once, the first time one of its instances is.
   void flatten(HostScene* out) const;
+  // The two-level form (false with `err` when a BVH would exceed `max_stack`).
+  bool build_two_level(uint32_t max_stack, TwoLevelHost* out, std::string* err) const;
 };
 
 }  // namespace ap

@@ -75,6 +75,11 @@ def lib():
         L.orc_spectral_new.argtypes = [P, P, P, P, F, F, F]
         L.orc_spectral_free.argtypes = [P]
         L.orc_spectral_render.argtypes = [P, P, P, U, U, U, U, U, ctypes.c_int, U, U, P]
+        L.orc_two_level_new.restype = P
+        L.orc_two_level_new.argtypes = [P, U, P, P, U]
+        L.orc_two_level_free.argtypes = [P]
+        L.orc_two_level_closest.argtypes = [P, P, P, U, F, U, P]
+        L.orc_two_level_any.argtypes = [P, P, P, U, F, U, P]
         L.orc_murmur3_x64_128.argtypes = [P, ctypes.c_size_t, ctypes.c_uint64, P]
         L.orc_zsobol.argtypes = [U, U, U, ctypes.c_uint64, U, U, U, P, U, P]
         L.orc_spectral_cmf.argtypes = [F, P]
@@ -207,6 +212,37 @@ class OracleSpectral:
     def __del__(self):
         if getattr(self, "ptr", None):
             lib().orc_spectral_free(self.ptr)
+            self.ptr = None
+
+
+class OracleTwoLevel:
+    """Queries over instances of models (oracle_twolevel.cpp): `models` are
+    model-space Scenes, `instances` (model index, column-major 4x4)."""
+
+    def __init__(self, models, instances):
+        self.models = [OracleScene(m) for m in models]
+        ptrs = (ctypes.c_void_p * len(self.models))(*[m.ptr for m in self.models])
+        im = np.ascontiguousarray([i for i, _ in instances], np.uint32)
+        mm = np.ascontiguousarray(np.stack([np.asarray(m, np.float32).reshape(16) for _, m in instances]))
+        self.ptr = lib().orc_two_level_new(ptrs, len(self.models), _p(im), _p(mm), len(instances))
+
+    def closest(self, origins, dirs, tmax=1e30, threads=0):
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(dirs, np.float32)
+        out = np.zeros((o.shape[0], 4), np.uint32)
+        lib().orc_two_level_closest(self.ptr, _p(o), _p(d), o.shape[0], tmax, threads or os.cpu_count(), _p(out))
+        return out
+
+    def any(self, origins, dirs, tmax, threads=0):
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(dirs, np.float32)
+        out = np.zeros(o.shape[0], np.uint8)
+        lib().orc_two_level_any(self.ptr, _p(o), _p(d), o.shape[0], tmax, threads or os.cpu_count(), _p(out))
+        return out
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().orc_two_level_free(self.ptr)
             self.ptr = None
 
 

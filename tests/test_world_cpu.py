@@ -117,3 +117,21 @@ def test_flatten_rule_moves_points_and_keeps_normals_unit():
     nref = model.normals.astype(np.float64) @ np.linalg.inv(m[:3, :3].astype(np.float64))
     nref /= np.linalg.norm(nref, axis=1, keepdims=True)
     np.testing.assert_allclose(n, nref, atol=1e-6)
+
+
+def test_two_level_oracle_with_identity_instances_equals_the_flat_oracle():
+    from oracle.oracle import OracleScene, OracleTwoLevel
+    a = scenes.cornell_box()
+    b = scenes.icosphere_field(seed=3, num_spheres=5, num_emissive=1, subdiv=1, box=0.8, env_size=None)
+    eye = np.eye(4, dtype=np.float32).reshape(16)
+    two = OracleTwoLevel([a, b], [(0, eye), (1, eye)])
+    flat = OracleScene(compose(a, b, [eye]))
+    rng = np.random.default_rng(2)
+    o = rng.uniform(-0.5, 1.5, (4000, 3)).astype(np.float32)
+    d = rng.normal(size=(4000, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    got = two.closest(o, d, 1000.0)
+    ref, _ = flat.closest(o, d, 1000.0)
+    assert np.array_equal(got, ref.view(np.uint32))
+    assert (got[:, 3] != 0xFFFFFFFF).mean() > 0.3
+    np.testing.assert_array_equal(two.any(o, d, 0.7), flat.any(o, d, np.full(len(o), 0.7, np.float32)))
