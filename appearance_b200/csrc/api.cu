@@ -67,12 +67,17 @@ struct DeviceScene {
 // used by the ray queries when the world has spawned instances.
 struct DeviceTwoLevel {
   void *nodes = nullptr, *tris = nullptr, *tlas_nodes = nullptr, *tlas_leaves = nullptr, *insts = nullptr;
-  DevScene view{};  // nodes / tris: the BLAS pool
+  void *positions = nullptr, *normals = nullptr, *indices = nullptr, *tri_mat = nullptr, *model_tri0 = nullptr,
+       *env = nullptr;
+  DevScene view{};  // nodes / tris: the BLAS pool; env: the base scene's environment
   TwoLevel tl{};
+  ModelGeo mg{};
+  std::vector<ap_material> materials;  // the models' materials, as tri_mat indexes them
   uint64_t version = ~0ull;
   bool valid = false;
   void release() {
-    void** all[] = {&nodes, &tris, &tlas_nodes, &tlas_leaves, &insts};
+    void** all[] = {&nodes, &tris, &tlas_nodes, &tlas_leaves, &insts, &positions, &normals, &indices, &tri_mat,
+                    &model_tri0, &env};
     for (void** p : all) {
       if (*p) cudaFree(*p);
       *p = nullptr;
@@ -121,6 +126,7 @@ struct Handle {
   size_t spec_out_bytes = 0;
   SpectralView spec{};
   bool spec_ready = false;
+  uint64_t spec_version = 0;  // the world the spectral tables were built for
   // base scene, registered models and spawned instances (world actions)
   World world;
   DeviceTwoLevel two_level;
@@ -576,13 +582,28 @@ int two_level_sync(Handle* h, const TwoLevel** out) {
       (rc = put(&t.tris, host.tris.data(), sizeof(TriRec) * host.tris.size(), "BLAS triangles")) ||
       (rc = put(&t.tlas_nodes, host.tlas_nodes.data(), sizeof(WideNode) * host.tlas_nodes.size(), "TLAS nodes")) ||
       (rc = put(&t.tlas_leaves, host.tlas_leaves.data(), sizeof(TriRec) * host.tlas_leaves.size(), "TLAS leaves")) ||
-      (rc = put(&t.insts, host.insts.data(), sizeof(InstRec) * host.insts.size(), "instances"))) {
+      (rc = put(&t.insts, host.insts.data(), sizeof(InstRec) * host.insts.size(), "instances")) ||
+      (rc = put(&t.positions, host.positions4.data(), sizeof(float) * host.positions4.size(), "model vertices")) ||
+      (rc = put(&t.normals, host.normals.data(), sizeof(float) * host.normals.size(), "model normals")) ||
+      (rc = put(&t.indices, host.indices.data(), sizeof(uint32_t) * host.indices.size(), "model indices")) ||
+      (rc = put(&t.tri_mat, host.tri_material.data(), sizeof(uint32_t) * host.tri_material.size(), "model materials")) ||
+      (rc = put(&t.model_tri0, host.model_tri0.data(), sizeof(uint32_t) * host.model_tri0.size(), "model table")) ||
+      (rc = put(&t.env, h->world.base.env.data(), sizeof(float) * h->world.base.env.size(), "environment"))) {
     t.release();
     return rc;
   }
   std::memset(&t.view, 0, sizeof(t.view));
   t.view.nodes = static_cast<const uint4*>(t.nodes);
   t.view.tris = static_cast<const float4*>(t.tris);
+  t.view.env = h->world.base.env_w ? static_cast<const float*>(t.env) : nullptr;
+  t.view.env_w = h->world.base.env_w;
+  t.view.env_h = h->world.base.env_h;
+  t.mg.positions = static_cast<const float4*>(t.positions);
+  t.mg.normals = static_cast<const float*>(t.normals);
+  t.mg.indices = static_cast<const uint32_t*>(t.indices);
+  t.mg.tri_mat = static_cast<const uint32_t*>(t.tri_mat);
+  t.mg.model_tri0 = static_cast<const uint32_t*>(t.model_tri0);
+  t.materials = host.materials;
   t.tl.tlas_nodes = static_cast<const uint4*>(t.tlas_nodes);
   t.tl.tlas_leaves = static_cast<const float4*>(t.tlas_leaves);
   t.tl.insts = static_cast<const InstRec*>(t.insts);
@@ -603,10 +624,12 @@ int handle_trace_context(void* hp, const DevScene** scene, const TwoLevel** two_
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return AP_E_INVALID;
   *err = &h->err;
-  if (int rc = world_sync(h)) return rc;
-  if (!h->scene.valid) {
-    h->err = "no scene uploaded";
-    return AP_E_NO_SCENE;
+  if (h->world.instances.empty()) {
+    if (int rc = world_sync(h)) return rc;
+    if (!h->scene.valid) {
+      h->err = "no scene uploaded";
+      return AP_E_NO_SCENE;
+    }
   }
   if (int rc = two_level_sync(h, two_level)) return rc;
   *scene = *two_level ? &h->two_level.view : &h->scene.view;
@@ -866,8 +889,10 @@ const float* ap_device_framebuffer(const void* hp) {
 int ap_trace_rays(void* hp, const float* origins_tmax, const float* dirs, uint32_t n, int any_hit, uint32_t* out4) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return AP_E_INVALID;
-  if (int wrc = world_sync(h)) return wrc;
-  if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  if (h->world.instances.empty()) {  // a world of instances is queried in its two-level form
+    if (int wrc = world_sync(h)) return wrc;
+    if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  }
   if (!origins_tmax || !dirs || !out4) return fail(h, AP_E_INVALID, "null buffer");
   if (n == 0) return AP_OK;
   ap::DeviceScope device_scope(h->device);
@@ -981,8 +1006,14 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
                       float env_scale) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h || !sun_dir3 || !sun_rgb3) return AP_E_INVALID;
-  if (int wrc = world_sync(h)) return wrc;
-  if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  const bool two = !h->world.instances.empty();  // a world of instances renders in its two-level form
+  const TwoLevel* tl = nullptr;
+  if (two) {
+    if (int trc = two_level_sync(h, &tl)) return trc;
+  } else {
+    if (int wrc = world_sync(h)) return wrc;
+    if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  }
   if (!(scene_radius > 0.0f) || !(sun_scale >= 0.0f) || !(env_scale >= 0.0f) ||
       !(sun_dir3[0] * sun_dir3[0] + sun_dir3[1] * sun_dir3[1] + sun_dir3[2] * sun_dir3[2] > 0.0f))
     return fail(h, AP_E_INVALID, "spectral setup: bad light parameters");
@@ -990,13 +1021,16 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
   cudaStreamSynchronize(h->stream);
   h->spec_release();
   const DeviceScene& sc = h->scene;
-  const uint32_t nm = (uint32_t)(sc.host_materials.size() / 26);
+  const float* mat26 = two ? reinterpret_cast<const float*>(h->two_level.materials.data()) : sc.host_materials.data();
+  const uint32_t nm = two ? (uint32_t)h->two_level.materials.size() : (uint32_t)(sc.host_materials.size() / 26);
   std::vector<spec::Material> mats(nm);
-  spec::upsample_materials(sc.host_materials.data(), nm, mats.data());
-  const size_t texels = sc.host_env.size() / 3;
+  spec::upsample_materials(mat26, nm, mats.data());
+  const std::vector<float>& env_rgb = two ? h->world.base.env : sc.host_env;
+  const uint32_t env_w = two ? h->world.base.env_w : sc.view.env_w, env_h = two ? h->world.base.env_h : sc.view.env_h;
+  const size_t texels = env_rgb.size() / 3;
   std::vector<float> env_pdf(texels);
   float env_integral = 0.0f;
-  if (texels) spectral_env_distribution(sc.host_env.data(), sc.view.env_w, sc.view.env_h, env_pdf.data(), &env_integral);
+  if (texels) spectral_env_distribution(env_rgb.data(), env_w, env_h, env_pdf.data(), &env_integral);
   int rc = check_cuda(h, cudaMalloc(&h->spec_mats, sizeof(spec::Material) * std::max<uint32_t>(nm, 1)), "spectral materials");
   if (!rc) rc = check_cuda(h, cudaMalloc(&h->spec_env, std::max<size_t>(sizeof(float) * texels, 16)), "spectral env");
   if (!rc) rc = check_cuda(h, cudaMemcpy(h->spec_mats, mats.data(), sizeof(spec::Material) * nm, cudaMemcpyHostToDevice),
@@ -1016,8 +1050,14 @@ int ap_spectral_setup(void* hp, const float* sun_dir3, const float* sun_rgb3, fl
   h->spec.mats = static_cast<const spec::Material*>(h->spec_mats);
   h->spec.env_pdf = static_cast<const float*>(h->spec_env);
   h->spec.env_pdf_integral = env_integral;
-  h->spec.env_w = texels ? sc.view.env_w : 0;
-  h->spec.env_h = texels ? sc.view.env_h : 0;
+  h->spec.env_w = texels ? env_w : 0;
+  h->spec.env_h = texels ? env_h : 0;
+  h->spec.two_level = two ? 1 : 0;
+  if (two) {
+    h->spec.tl = *tl;
+    h->spec.mg = h->two_level.mg;
+  }
+  h->spec_version = h->world.version;
   h->spec.env_scale = env_scale;
   h->spec.sun = spec::make_sun(sun_dir3, sun_rgb3, sun_scale, scene_radius);
   h->spec.illum_tab = static_cast<const float*>(h->spec_tab);
@@ -1032,9 +1072,17 @@ int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
                     uint64_t* visits6) {
   Handle* h = static_cast<Handle*>(hp);
   if (!h) return AP_E_INVALID;
-  if (int wrc = world_sync(h)) return wrc;
-  if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
-  if (!h->spec_ready) return fail(h, AP_E_INVALID, "spectral mode not set up (ap_spectral_setup)");
+  const bool two = !h->world.instances.empty();
+  const TwoLevel* tl = nullptr;
+  if (two) {
+    if (int trc = two_level_sync(h, &tl)) return trc;
+  } else {
+    if (int wrc = world_sync(h)) return wrc;
+    if (!h->scene.valid) return fail(h, AP_E_NO_SCENE, "no scene uploaded");
+  }
+  if (!h->spec_ready || h->spec_version != h->world.version)
+    return fail(h, AP_E_INVALID, "spectral mode not set up for this world (ap_spectral_setup)");
+  if (two && h->rc.cache) return fail(h, AP_E_UNSUPPORTED, "the radiance cache takes flat scenes (no spawned instances)");
   if (w == 0 || hgt == 0 || w > 65536 || row_start >= row_end || row_end > hgt || spp == 0 || max_depth == 0 ||
       max_depth > (uint32_t)kSpectralMaxDepth || (uint64_t)w * (row_end - row_start) > (1ull << 26))
     return fail(h, AP_E_INVALID, "spectral render: bad arguments");
@@ -1066,7 +1114,8 @@ int render_spectral(void* hp, uint32_t w, uint32_t hgt, uint32_t row_start, uint
   void* work = static_cast<char*>(h->spec_out) + need_a;
   const unsigned long long* counter = spectral_stats(work, P, rcp);
   cudaEventRecord(h->ev0, h->stream);
-  const int launches = launch_spectral(h->scene.view, h->spec, cam, w, hgt, row_start, row_end, spp, (int)max_depth,
+  const int launches = launch_spectral(two ? h->two_level.view : h->scene.view, h->spec, cam, w, hgt, row_start,
+                                       row_end, spp, (int)max_depth,
                                        seed, static_cast<float*>(h->spec_out), work, h->num_sms, visits6 != nullptr,
                                        rcp, h->stream, &h->fs);
   cudaEventRecord(h->ev1, h->stream);

@@ -57,6 +57,13 @@ APD float au_sample(const float* vals, float l) {
   return a + (b - a) * ((l - l0) / (l1 - l0));
 }
 
+// Scene access of the spectral integrator (spectral.h's Geo): the flat scene,
+// or (kTwo) a two-level world, whose shading data is the hit's instance (the
+// last whose first global triangle id is at most g), its model's triangle,
+// the vertices mapped to world space by the instance transform, and the
+// normals with the transform's inverse transpose (the transpose of the
+// world-to-object rows).
+template <bool kTwo>
 struct GpuGeo {
   const DevScene& s;
   const SpectralView& v;
@@ -71,25 +78,43 @@ struct GpuGeo {
     *i1 = in.first_vertex + s.indices[fi + 1];
     *i2 = in.first_vertex + s.indices[fi + 2];
   }
-  APD void tri(uint32_t g, spec::V3* p0, spec::V3* p1, spec::V3* p2) const {
-    uint32_t i0, i1, i2;
-    tri_index(g, &i0, &i1, &i2);
-    const float4 a = s.positions[i0], b = s.positions[i1], c = s.positions[i2];
-    *p0 = spec::v3(a.x, a.y, a.z);
-    *p1 = spec::v3(b.x, b.y, b.z);
-    *p2 = spec::v3(c.x, c.y, c.z);
-  }
-  APD void tri_normals(uint32_t g, spec::V3* n0, spec::V3* n1, spec::V3* n2) const {
-    uint32_t i0, i1, i2;
-    tri_index(g, &i0, &i1, &i2);
+  // world-space vertices and normals of triangle g, and its material
+  APD const spec::Material& fetch(uint32_t g, spec::TriGeo* tg) const {
+    if (kTwo) return fetch2(g, tg);
+    uint32_t vi[3];
+    tri_index(g, &vi[0], &vi[1], &vi[2]);
     const float* n = s.normals_f;
-    *n0 = spec::v3(n[3 * (size_t)i0], n[3 * (size_t)i0 + 1], n[3 * (size_t)i0 + 2]);
-    *n1 = spec::v3(n[3 * (size_t)i1], n[3 * (size_t)i1 + 1], n[3 * (size_t)i1 + 2]);
-    *n2 = spec::v3(n[3 * (size_t)i2], n[3 * (size_t)i2 + 1], n[3 * (size_t)i2 + 2]);
-  }
-  APD const spec::Material& material(uint32_t g) const {
+    for (int k = 0; k < 3; ++k) {
+      const float4 p = s.positions[vi[k]];
+      tg->p[k] = spec::v3(p.x, p.y, p.z);
+      tg->n[k] = spec::v3(n[3 * (size_t)vi[k]], n[3 * (size_t)vi[k] + 1], n[3 * (size_t)vi[k] + 2]);
+    }
+    tg->xform = false;
     const InstanceDev& in = s.instances[s.tri_instance[g]];
     return v.mats[in.material_idx + s.tri_material[in.first_index / 3 + (g - in.first_global_tri)]];
+  }
+  APD const spec::Material& fetch2(uint32_t g, spec::TriGeo* tg) const {
+    uint32_t lo = 0, hi = v.tl.num_insts;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (v.tl.insts[mid].tri_base <= g) lo = mid;
+      else hi = mid;
+    }
+    const InstRec& in = v.tl.insts[lo];
+    const uint32_t t = __ldg(&v.mg.model_tri0[in.model]) + (g - in.tri_base);
+    const float* m = in.o2w;
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t vi = __ldg(&v.mg.indices[3 * (size_t)t + k]);
+      const float4 p = v.mg.positions[vi];
+      tg->p[k] = spec::v3(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
+                          m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]);
+      const float* n = v.mg.normals + 3 * (size_t)vi;
+      tg->n[k] = spec::v3(n[0], n[1], n[2]);
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) tg->nm[3 * r + c] = in.w2o[4 * c + r];
+    tg->xform = true;
+    return v.mats[__ldg(&v.mg.tri_mat[t])];
   }
   APD void env_rgb(uint32_t x, uint32_t y, float c[3]) const {
     const float* p = s.env + 3 * ((size_t)y * env_w + x);
@@ -223,15 +248,22 @@ __global__ void __launch_bounds__(kBlock) k_sgen(SpecBuffers b, SpectralCamera c
   if (sample == 0) b.acc[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-template <bool kCount>
-__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s, SpecBuffers b, uint32_t round,
-                                                                     uint32_t P) {
+// The traversal loop of a scene: flat, or two-level when `tl` is given.
+template <bool kAny, bool kCount, bool kTwo, class Load, class Store>
+APD void trace_loop(const DevScene& s, const TwoLevel& tl, uint32_t count, uint32_t* cursor, Load load, Store store) {
+  if (kTwo) persistent_trace2<kAny, kCount>(s, tl, count, cursor, load, store);
+  else persistent_trace<kAny, kCount>(s, count, cursor, load, store);
+}
+
+template <bool kCount, bool kTwo>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s, TwoLevel tl, SpecBuffers b,
+                                                                     uint32_t round, uint32_t P) {
   const uint32_t count = round == 0 ? P : min(b.counters[4 * round], P);
   if (blockIdx.x == 0 && threadIdx.x == 0 && count) atomicAdd(&b.stats[0], (unsigned long long)count);
   const float4* qo = b.rq_o[round & 1];
   const float4* qd = b.rq_d[round & 1];
-  persistent_trace<false, kCount>(
-      s, count, &b.counters[4 * round + 1],
+  trace_loop<false, kCount, kTwo>(
+      s, tl, count, &b.counters[4 * round + 1],
       [&](uint32_t i, float3& o, float3& d, float& tmax) {
         const float4 a = qo[i], c = qd[i];
         o = f3(a.x, a.y, a.z);
@@ -251,6 +283,7 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sextend(DevScene s,
 #ifndef AP_SSHADE_MIN_BLOCKS
 #define AP_SSHADE_MIN_BLOCKS 8  // resident blocks per SM the shading kernel is register-capped for (measured)
 #endif
+template <bool kTwo>
 __global__ void __launch_bounds__(kBlock, AP_SSHADE_MIN_BLOCKS) k_sshade(DevScene s, SpectralView v, SpecBuffers b,
                                                                      uint32_t round, uint32_t P, int max_depth,
                                                                      uint32_t digits, uint64_t frame_seed) {
@@ -259,7 +292,7 @@ __global__ void __launch_bounds__(kBlock, AP_SSHADE_MIN_BLOCKS) k_sshade(DevScen
   const float4* qd = b.rq_d[round & 1];
   float4* no = b.rq_o[(round + 1) & 1];
   float4* nd = b.rq_d[(round + 1) & 1];
-  const GpuGeo g{s, v, v.env_w, v.env_h, v.env_scale, v.env_pdf_integral, v.sun};
+  const GpuGeo<kTwo> g{s, v, v.env_w, v.env_h, v.env_scale, v.env_pdf_integral, v.sun};
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const float4 ro = qo[i], rd = qd[i];
     const uint32_t owner = __float_as_uint(rd.w);
@@ -287,13 +320,13 @@ __global__ void __launch_bounds__(kBlock, AP_SSHADE_MIN_BLOCKS) k_sshade(DevScen
   }
 }
 
-template <bool kCount>
-__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sshadow(DevScene s, SpecBuffers b, uint32_t round,
-                                                                     uint32_t P) {
+template <bool kCount, bool kTwo>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_sshadow(DevScene s, TwoLevel tl, SpecBuffers b,
+                                                                     uint32_t round, uint32_t P) {
   const uint32_t count = min(b.counters[4 * round + 2], P);
   if (blockIdx.x == 0 && threadIdx.x == 0 && count) atomicAdd(&b.stats[3], (unsigned long long)count);
-  persistent_trace<true, kCount>(
-      s, count, &b.counters[4 * round + 3],
+  trace_loop<true, kCount, kTwo>(
+      s, tl, count, &b.counters[4 * round + 3],
       [&](uint32_t i, float3& o, float3& d, float& tmax) {
         const float4 a = b.sq_o[i], c = b.sq_d[i];
         o = f3(a.x, a.y, a.z);
@@ -518,6 +551,7 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
   if (rc) cudaMemsetAsync(b.rec, 0, sizeof(float4) * kSpecRecord * slots, st);  // no tags from an earlier call
   const uint32_t rounds = (uint32_t)max_depth + 1;
   const uint32_t digits = spec::zsobol_digits(W, H);
+  const bool two = v.two_level != 0;
   const int linear = (int)((P + kBlock - 1) / kBlock);
   const int persistent = num_sms * kTraceMinBlocks;
   const int shade = std::min(linear, num_sms * 16);
@@ -535,9 +569,15 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
       k_sgen<<<linear, kBlock, 0, sk>>>(bk, cam, W, H, row0, P, k, digits, (uint64_t)seed + k);
       ++launches;
       for (uint32_t r = 0; r < rounds; ++r) {
-        k_sextend<false><<<persistent, kBlock, 0, sk>>>(s, bk, r, P);
-        k_sshade<<<shade, kBlock, 0, sk>>>(s, v, bk, r, P, max_depth, digits, (uint64_t)seed + k);
-        k_sshadow<false><<<persistent, kBlock, 0, sk>>>(s, bk, r, P);
+        if (two) {
+          k_sextend<false, true><<<persistent, kBlock, 0, sk>>>(s, v.tl, bk, r, P);
+          k_sshade<true><<<shade, kBlock, 0, sk>>>(s, v, bk, r, P, max_depth, digits, (uint64_t)seed + k);
+          k_sshadow<false, true><<<persistent, kBlock, 0, sk>>>(s, v.tl, bk, r, P);
+        } else {
+          k_sextend<false, false><<<persistent, kBlock, 0, sk>>>(s, v.tl, bk, r, P);
+          k_sshade<false><<<shade, kBlock, 0, sk>>>(s, v, bk, r, P, max_depth, digits, (uint64_t)seed + k);
+          k_sshadow<false, false><<<persistent, kBlock, 0, sk>>>(s, v.tl, bk, r, P);
+        }
         launches += 3;
       }
       if (k > 0) cudaStreamWaitEvent(sk, fs->join, 0);  // the previous pass's accumulation
@@ -555,8 +595,13 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
     k_sgen<<<linear, kBlock, 0, st>>>(b, cam, W, H, row0, P, k, digits, (uint64_t)seed + k);
     ++launches;
     for (uint32_t r = 0; r < rounds; ++r) {
-      if (count_visits) k_sextend<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
-      else k_sextend<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+      if (two) {
+        if (count_visits) k_sextend<true, true><<<persistent, kBlock, 0, st>>>(s, v.tl, b, r, P);
+        else k_sextend<false, true><<<persistent, kBlock, 0, st>>>(s, v.tl, b, r, P);
+      } else {
+        if (count_visits) k_sextend<true, false><<<persistent, kBlock, 0, st>>>(s, v.tl, b, r, P);
+        else k_sextend<false, false><<<persistent, kBlock, 0, st>>>(s, v.tl, b, r, P);
+      }
       if (shadow_pending) {  // the previous round's shadow rays, traced beside this extension
         cudaEventRecord(fs->join, fs->side);
         cudaStreamWaitEvent(st, fs->join, 0);
@@ -566,17 +611,21 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
         k_svertex<<<shade, kBlock, 0, st>>>(s, b, *rc, r, P, k, seed);
         ++launches;
       }
-      k_sshade<<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth, digits, (uint64_t)seed + k);
+      if (two) k_sshade<true><<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth, digits, (uint64_t)seed + k);
+      else k_sshade<false><<<shade, kBlock, 0, st>>>(s, v, b, r, P, max_depth, digits, (uint64_t)seed + k);
       if (overlap && r + 1 < rounds) {
         // only the next shading pass reads what these rays add to L
         cudaEventRecord(fs->fork, st);
         cudaStreamWaitEvent(fs->side, fs->fork, 0);
-        k_sshadow<false><<<persistent, kBlock, 0, fs->side>>>(s, b, r, P);
+        if (two) k_sshadow<false, true><<<persistent, kBlock, 0, fs->side>>>(s, v.tl, b, r, P);
+        else k_sshadow<false, false><<<persistent, kBlock, 0, fs->side>>>(s, v.tl, b, r, P);
         shadow_pending = true;
       } else if (count_visits) {
-        k_sshadow<true><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+        if (two) k_sshadow<true, true><<<persistent, kBlock, 0, st>>>(s, v.tl, b, r, P);
+        else k_sshadow<true, false><<<persistent, kBlock, 0, st>>>(s, v.tl, b, r, P);
       } else {
-        k_sshadow<false><<<persistent, kBlock, 0, st>>>(s, b, r, P);
+        if (two) k_sshadow<false, true><<<persistent, kBlock, 0, st>>>(s, v.tl, b, r, P);
+        else k_sshadow<false, false><<<persistent, kBlock, 0, st>>>(s, v.tl, b, r, P);
       }
       launches += 3;
     }

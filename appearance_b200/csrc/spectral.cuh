@@ -5,6 +5,7 @@
 
 #include "scene_layout.h"
 #include "spectral.h"
+#include "traverse2.cuh"
 
 namespace ap {
 
@@ -14,8 +15,24 @@ namespace ap {
 // in the reference's x-major flattening, rows of env_w, and its integral; the
 // environment's RGB texels are the scene's), the distant light, and the
 // illuminant upsampling table.
+// The models of a two-level world, for shading (World::build_two_level):
+// model-space vertices (x, y, z, 0) and normals (3 floats), per model
+// triangle its vertex indices and its material, each model's first triangle.
+struct ModelGeo {
+  const float4* positions;
+  const float* normals;
+  const uint32_t* indices;
+  const uint32_t* tri_mat;
+  const uint32_t* model_tri0;
+};
+
 struct SpectralView {
   const spec::Material* mats;
+  // a two-level world (instances): traversal over tl, shading from mg; the
+  // DevScene passed with the view then holds the BLAS pool
+  int two_level;
+  TwoLevel tl;
+  ModelGeo mg;
   const float* env_pdf;  // env_w x env_h, or null with env_w = 0
   float env_pdf_integral;
   uint32_t env_w, env_h;

@@ -604,6 +604,16 @@ struct Hit {
   uint32_t tri;
 };
 
+// A hit triangle's data as a Geo fetches it: world-space vertices, its vertex
+// normals and, for an instance of a two-level scene, the 3x3 matrix that takes
+// the (object-space) normals to world space (the transform's inverse
+// transpose, geometry_resources.rs:258-261), row-major.
+struct TriGeo {
+  V3 p[3], n[3];
+  float nm[9];
+  bool xform;
+};
+
 // InfiniteLight::le (infinite_light.rs:69-82,145-148): the equirect uv of the
 // direction (unit_vector_to_panorama_coords, sampling/mod.rs:70-75), the
 // texture's clamped bilinear sample of its RGB (appearance-texture
@@ -690,12 +700,15 @@ SPHD bool path_vertex(const Geo& g, V3& o, V3& d, const Hit* h, const S4& lambda
     }
     return false;
   }
-  V3 p0, p1, p2, n0, n1, n2;
-  g.tri(h->tri, &p0, &p1, &p2);
-  g.tri_normals(h->tri, &n0, &n1, &n2);
-  const Material& m = g.material(h->tri);
+  TriGeo tg;
+  const Material& m = g.fetch(h->tri, &tg);
+  const V3 p0 = tg.p[0], p1 = tg.p[1], p2 = tg.p[2];
   const float bx = 1.0f - h->u - h->v;
-  const V3 n = normalize(n0 * bx + n1 * h->u + n2 * h->v);
+  V3 ni = tg.n[0] * bx + tg.n[1] * h->u + tg.n[2] * h->v;
+  if (tg.xform)
+    ni = v3(tg.nm[0] * ni.x + tg.nm[1] * ni.y + tg.nm[2] * ni.z, tg.nm[3] * ni.x + tg.nm[4] * ni.y + tg.nm[5] * ni.z,
+            tg.nm[6] * ni.x + tg.nm[7] * ni.y + tg.nm[8] * ni.z);
+  const V3 n = normalize(ni);
   const V3 hit = o + d * h->t;
   const V3 wo = -d;
   if (m.emit_scale > 0.0f && dot(cross(p1 - p0, p2 - p0), wo) > 0.0f) {

@@ -262,6 +262,22 @@ bool World::build_two_level(uint32_t max_stack, TwoLevelHost* out, std::string* 
     out->tris.insert(out->tris.end(), b.tris.begin(), b.tris.end());
     root[k] = node0;
     blas_stack = std::max(blas_stack, b.stats.max_stack);
+    // shading geometry: vertices, per-triangle vertex indices and materials
+    const HostScene& ms = *mods[k];
+    const uint32_t v0 = (uint32_t)(out->positions4.size() / 4), mat0 = (uint32_t)out->materials.size();
+    out->model_tri0.push_back((uint32_t)(out->indices.size() / 3));
+    for (size_t i = 0; i < ms.positions.size() / 3; ++i) {
+      for (int a = 0; a < 3; ++a) out->positions4.push_back(ms.positions[3 * i + a]);
+      out->positions4.push_back(0.0f);
+    }
+    out->normals.insert(out->normals.end(), ms.normals.begin(), ms.normals.end());
+    out->materials.insert(out->materials.end(), ms.materials.begin(), ms.materials.end());
+    for (const ap_mesh& me : ms.meshes)
+      for (uint32_t t = 0; t < me.num_indices / 3; ++t) {
+        const uint32_t g = me.first_index / 3 + t;
+        for (int c = 0; c < 3; ++c) out->indices.push_back(v0 + me.first_vertex + ms.indices[3 * (size_t)g + c]);
+        out->tri_material.push_back(mat0 + me.material_idx + ms.tri_material[g]);
+      }
     float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     for (size_t i = 0; i < tv.size(); i += 3)
       for (int a = 0; a < 3; ++a) {

@@ -51,6 +51,13 @@ struct TwoLevelHost {
   std::vector<TriRec> tris, tlas_leaves;
   std::vector<InstRec> insts;
   uint32_t max_stack = 0;  // TLAS stack bound + the largest BLAS bound + 1
+  // the models' geometry for shading, in model space: vertex positions
+  // (x, y, z, 0) and normals (3 floats), per model triangle its three vertex
+  // indices into those arrays and its material index into `materials`; each
+  // model's first triangle
+  std::vector<float> positions4, normals;
+  std::vector<uint32_t> indices, tri_material, model_tri0;
+  std::vector<ap_material> materials;
 };
 
 // World-to-object rows (row-major 3x4) of a column-major Mat4: its inverse
@@ -80,7 +87,8 @@ struct World {
   // normals by its inverse transpose (renormalised); a model's materials are
   // appended once, the first time one of its instances is.
   void flatten(HostScene* out) const;
-  // The two-level form (false with `err` when a BVH would exceed `max_stack`).
+  // The two-level form (false with `err` when a BVH would exceed `max_stack`);
+  // the base scene is model 0 with the identity instance when it has meshes.
   bool build_two_level(uint32_t max_stack, TwoLevelHost* out, std::string* err) const;
 };
 

@@ -72,7 +72,7 @@ def lib():
         L.orc_detmath.argtypes = [U, P, P, P, U]
         L.orc_resolve_rgba8.argtypes = [P, U, U, U, P, U, P]
         L.orc_spectral_new.restype = P
-        L.orc_spectral_new.argtypes = [P, P, P, P, F, F, F]
+        L.orc_spectral_new.argtypes = [P, P, P, P, F, F, F, P]
         L.orc_spectral_free.argtypes = [P]
         L.orc_spectral_render.argtypes = [P, P, P, U, U, U, U, U, ctypes.c_int, U, U, P]
         L.orc_two_level_new.restype = P
@@ -192,13 +192,15 @@ class OracleSpectral:
     arguments mean what they mean in PathTracer.spectral_setup / render_spectral."""
 
     def __init__(self, oscene: OracleScene, sun_dir=(0.0, -1.0, 0.2), sun_rgb=(1.0, 1.0, 0.95), sun_scale=100.0,
-                 scene_radius=1000.0, env_scale=1.0):
+                 scene_radius=1000.0, env_scale=1.0, two_level=None):
         self.scene = oscene
         self.n_mats = oscene._keep["mat"].shape[0]
         env = oscene._keep["env"]
         self.env_texels = 0 if env is None else env.shape[0] * env.shape[1]
+        self.two_level = two_level  # an OracleTwoLevel of the world `oscene` flattens
         self.ptr = lib().orc_spectral_new(oscene.ptr, _p(oscene._keep["nrm"]), _p(np.asarray(sun_dir, np.float32)),
-                                          _p(np.asarray(sun_rgb, np.float32)), sun_scale, scene_radius, env_scale)
+                                          _p(np.asarray(sun_rgb, np.float32)), sun_scale, scene_radius, env_scale,
+                                          None if two_level is None else two_level.ptr)
 
     def render(self, mats: np.ndarray, width: int, height: int, spp: int = 1, max_depth: int = 4, seed: int = 0,
                row0: int = 0, row1: int | None = None, threads: int = 0) -> np.ndarray:

@@ -57,6 +57,7 @@
 #include "../appearance_b200/csrc/spectral_data.h"
 #include "../appearance_b200/csrc/spectral_tables.h"
 #include "oracle_scene.h"
+#include "oracle_twolevel.h"
 
 namespace {
 
@@ -667,6 +668,10 @@ struct PiecewiseConstant1D {  // sampling/piecewise_constant.rs:21-49
 struct SpectralScene {
   const orc::Scene* scene;
   orc::OracleBvh bvh;
+  // a world of instances: hits come from its two-level form (object-space
+  // intersection, global triangle ids in the order of `scene`, the flattened
+  // world, whose data shades them)
+  const void* two_level = nullptr;
   std::vector<Vec3> normals;  // float vertex normals
   // per material: albedo coefficients, conductor and emission
   struct Mat {
@@ -755,8 +760,9 @@ Vec4 li(const SpectralScene& s, Vec3 ray_o, Vec3 ray_d, const Wavelengths& w, ZS
   bool specular_bounce = false;
   uint32_t depth = 0;
   while (true) {
-    const orc::Hit hit = s.bvh.closest(sc, orc::v3(ray_o.x, ray_o.y, ray_o.z), orc::v3(ray_d.x, ray_d.y, ray_d.z), 0.0f,
-                                       1e30f, nullptr, nullptr);
+    const orc::V3 ro = orc::v3(ray_o.x, ray_o.y, ray_o.z), rd = orc::v3(ray_d.x, ray_d.y, ray_d.z);
+    const orc::Hit hit = s.two_level ? orc::two_level_closest(s.two_level, ro, rd, 1e30f)
+                                     : s.bvh.closest(sc, ro, rd, 0.0f, 1e30f, nullptr, nullptr);
     if (hit.tri == 0xFFFFFFFFu) {
       const Vec4 le = env_le(s, ray_d, w);
       if (depth == 0 || specular_bounce) {
@@ -821,7 +827,8 @@ Vec4 li(const SpectralScene& s, Vec3 ray_o, Vec3 ray_d, const Wavelengths& w, ZS
           const Vec3 sd = normalize(wi);
           const Vec3 dd = hit_point - p;
           const float tmax = length(dd);
-          if (!s.bvh.any(sc, orc::v3(so.x, so.y, so.z), orc::v3(sd.x, sd.y, sd.z), 0.0f, tmax)) {
+          const orc::V3 qo = orc::v3(so.x, so.y, so.z), qd = orc::v3(sd.x, sd.y, sd.z);
+          if (!(s.two_level ? orc::two_level_any(s.two_level, qo, qd, tmax) : s.bvh.any(sc, qo, qd, 0.0f, tmax))) {
             const Vec4 ld = (li_l * f) / 1.0f;
             l = l + throughput * ld;
           }
@@ -878,13 +885,16 @@ Vec3 pixel_sample(const SpectralScene& s, const float* inv_view, const float* in
 extern "C" {
 
 // Spectral scene of an oracle scene (orc_scene_new) for the parameters of
-// ap_spectral_setup.  `normals` are the scene's float vertex normals.
+// ap_spectral_setup.  `normals` are the scene's float vertex normals.  With
+// `two_level` (orc_two_level_new, its instances in the order of the flattened
+// `scene`) rays are traced through the two-level form.
 void* orc_spectral_new(void* scene, const float* normals, const float* sun_dir3, const float* sun_rgb3, float sun_scale,
-                       float scene_radius, float env_scale) {
+                       float scene_radius, float env_scale, const void* two_level) {
   const orc::Scene* sc = (const orc::Scene*)scene;
   SpectralScene* s = new SpectralScene();
   s->scene = sc;
-  s->bvh.build(*sc);
+  s->two_level = two_level;
+  if (!two_level) s->bvh.build(*sc);
   s->normals.resize(sc->positions.size());
   for (size_t i = 0; i < s->normals.size(); ++i)
     s->normals[i] = {normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]};

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "oracle_scene.h"
+#include "oracle_twolevel.h"
 
 namespace {
 
@@ -124,6 +125,11 @@ void parallel(uint32_t n, uint32_t threads, F f) {
 }
 
 }  // namespace
+
+namespace orc {
+Hit two_level_closest(const void* p, V3 o, V3 d, float tmax) { return closest(*(const TwoLevel*)p, o, d, tmax); }
+bool two_level_any(const void* p, V3 o, V3 d, float tmax) { return any(*(const TwoLevel*)p, o, d, tmax); }
+}  // namespace orc
 
 extern "C" {
 

@@ -95,3 +95,51 @@ def test_instanced_city_matches_the_oracle():
     compare(pt, orc, o2, d2, 1e30, "city random rays")
     compare(pt, orc, o2, d2, 40.0, "city short rays")
     pt.close()
+
+
+def _spectral_pair(base, models, instances, mats, w, h, light, spp, depth, seed):
+    from oracle.oracle import OracleScene, OracleSpectral
+    from test_world_cpu import compose_many
+    pt = PathTracer(presets.PLAIN)
+    tl = world(pt, base, models, instances)
+    pt.set_camera_matrices(mats)
+    pt.spectral_setup(**light)
+    img = pt.render_spectral((w, h), spp=spp, max_depth=depth, seed=seed)
+    pt.close()
+    flat = compose_many(base, models, instances)
+    ref = OracleSpectral(OracleScene(flat), two_level=tl, **light).render(mats, w, h, spp=spp, max_depth=depth,
+                                                                         seed=seed)
+    return img, ref
+
+
+def test_spectral_over_instances_matches_the_oracle():
+    """The spectral mode over a world of instances (two-level traversal, normals
+    through the instance transforms) against the oracle tracing the same
+    two-level form and shading from the flattened world."""
+    from parity import assert_spectral_close
+    rng = np.random.default_rng(4)
+    base = scenes.cornell_box()
+    models = [scenes.icosphere_field(seed=s, num_spheres=3, num_emissive=1, subdiv=2, box=0.3, env_size=None)
+              for s in (6, 7)]
+    models[1].materials[:, 3] = 1.0  # gold
+    instances = [(int(rng.integers(0, 2)), random_transform(rng, 0.35)) for _ in range(12)]
+    for k, m in instances:
+        m[12:15] += 0.5  # inside the box
+    cam = scenes.cornell_camera()
+    w, h = 64, 48
+    mats = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], 0.01, 100.0, w, h, None)[0]
+    img, ref = _spectral_pair(base, models, instances, mats, w, h, dict(sun_scale=0.0, scene_radius=10.0), 2, 6, 3)
+    assert img.mean() > 0.0
+    assert_spectral_close(img, ref, "instances spp=2 depth=6")
+
+
+def test_spectral_instanced_city_matches_the_oracle():
+    from parity import assert_spectral_close
+    base, models, instances = scenes.city_instanced(env_size=(512, 256))
+    cam = scenes.city_camera()
+    w = h = 64
+    mats = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], 0.5, 5000.0, w, h, None)[0]
+    light = dict(sun_dir=(0.0, -1.0, 0.2), sun_rgb=(1.0, 1.0, 0.95), sun_scale=100.0, scene_radius=1500.0)
+    img, ref = _spectral_pair(base, models, instances, mats, w, h, light, 2, 16, 3)
+    assert img.mean() > 0.0
+    assert_spectral_close(img, ref, "instanced city 64x64 spp=2 depth=16")

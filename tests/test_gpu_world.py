@@ -3,13 +3,13 @@ Clear through ap_world_action, models from ap_model_register): the frames a
 handle renders after them equal, bit for bit, the frames of the same world
 uploaded in one piece (base scene plus the instances flattened with the rule
 restated in tests/test_world_cpu.py), and the spectral mode sees the same
-world."""
+world (in its two-level form)."""
 import numpy as np
 import pytest
 
 from appearance_b200 import PathTracer, gltf, presets, scenes
 from appearance_b200.renderer import RendererError
-from parity import assert_bits
+from parity import assert_bits, assert_spectral_close
 from test_world_cpu import compose
 
 pytestmark = pytest.mark.gpu
@@ -101,6 +101,10 @@ def test_spectral_mode_sees_spawned_instances(tmp_path):
     b.set_camera_matrices(mats)
     b.spectral_setup(**light)
     ref = b.render_spectral((W, H), spp=2, max_depth=4, seed=1)
-    assert_bits(img, ref, "spectral world")
+    # the world of instances renders through its two-level form (hits in
+    # object space, normals through the instance transform), the upload
+    # through the flattened world: the same estimator within the spectral
+    # tolerance
+    assert_spectral_close(img, ref, "spectral world")
     a.close()
     b.close()

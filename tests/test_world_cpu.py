@@ -135,3 +135,31 @@ def test_two_level_oracle_with_identity_instances_equals_the_flat_oracle():
     assert np.array_equal(got, ref.view(np.uint32))
     assert (got[:, 3] != 0xFFFFFFFF).mean() > 0.3
     np.testing.assert_array_equal(two.any(o, d, 0.7), flat.any(o, d, np.full(len(o), 0.7, np.float32)))
+
+
+def compose_many(base, models, instances):
+    """base + instances of several models (model index, column-major 4x4) in
+    World::flatten's layout (a model's materials appended at its first use)."""
+    pos, nrm, idx, tm, meshes = [base.positions], [base.normals], [base.indices], [base.tri_material], list(base.meshes)
+    mats = [base.materials]
+    mat_base = {}
+    nmat = base.materials.shape[0]
+    nv, nt = base.positions.shape[0], base.indices.shape[0]
+    for k, m16 in instances:
+        model = models[k]
+        if k not in mat_base:
+            mat_base[k] = nmat
+            mats.append(model.materials)
+            nmat += model.materials.shape[0]
+        p, n = flatten_instance(model, m16)
+        pos.append(p)
+        nrm.append(n)
+        idx.append(model.indices)
+        tm.append(model.tri_material)
+        for fv, cnt, fi, ni, mi, em in model.meshes:
+            meshes.append((fv + nv, cnt, fi + 3 * nt, ni, mi + mat_base[k], em))
+        nv += model.positions.shape[0]
+        nt += model.indices.shape[0]
+    return scenes.Scene(positions=np.concatenate(pos), normals=np.concatenate(nrm), indices=np.concatenate(idx),
+                        tri_material=np.concatenate(tm), meshes=np.asarray(meshes, np.uint32),
+                        materials=np.concatenate(mats).astype(np.float32), env=base.env, sun=base.sun)
