@@ -388,6 +388,63 @@ def city_instanced(seed: int = 0, lots: int = 64, extent: float = 2000.0, varian
     return b.finish(env, sun), models, instances
 
 
+def flatten_instance(model, m16):
+    """One instance in world space with the library's arithmetic (World::flatten,
+    csrc/world.cpp):
+    positions m * (p, 1) summed left to right in float32; normals by the
+    inverse transpose of the upper 3x3 (cofactors over the determinant in
+    double, rounded to float), renormalised in float32."""
+    m = np.asarray(m16, np.float32).reshape(16)
+    f = np.float32
+    x, y, z = (model.positions[:, k].astype(f) for k in range(3))
+    pos = np.stack([((m[r] * x + m[4 + r] * y) + m[8 + r] * z) + m[12 + r] for r in range(3)], 1).astype(f)
+    a = [[float(m[4 * c + r]) for r in range(3)] for c in range(3)]
+    det = (a[0][0] * (a[1][1] * a[2][2] - a[2][1] * a[1][2]) - a[1][0] * (a[0][1] * a[2][2] - a[2][1] * a[0][2])
+           + a[2][0] * (a[0][1] * a[1][2] - a[1][1] * a[0][2]))
+    nt = np.zeros((3, 3), f)
+    for r in range(3):
+        for k in range(3):
+            r1, r2, k1, k2 = (r + 1) % 3, (r + 2) % 3, (k + 1) % 3, (k + 2) % 3
+            nt[r, k] = f((a[k1][r1] * a[k2][r2] - a[k2][r1] * a[k1][r2]) / det)
+    nx, ny, nz = (model.normals[:, k].astype(f) for k in range(3))
+    n = np.stack([(nt[r, 0] * nx + nt[r, 1] * ny) + nt[r, 2] * nz for r in range(3)], 1).astype(f)
+    ln = np.sqrt((n[:, 0] * n[:, 0] + n[:, 1] * n[:, 1]) + n[:, 2] * n[:, 2]).astype(f)
+    s = np.where(ln > 0, f(1.0) / np.where(ln > 0, ln, f(1.0)), f(0.0)).astype(f)
+    return pos, (n * s[:, None]).astype(f)
+
+
+
+def flatten_world(base, models, instances):
+    """The world of a base scene and instances of models (model index,
+    column-major 4x4) as one Scene, in the layout of the library's World::flatten
+    (csrc/world.cpp): base first, then each instance's meshes in order, a
+    model's materials appended at its first use; the same float32 arithmetic,
+    so that the flattened upload equals the world the library builds."""
+    pos, nrm, idx, tm, meshes = [base.positions], [base.normals], [base.indices], [base.tri_material], list(base.meshes)
+    mats = [base.materials]
+    mat_base = {}
+    nmat = base.materials.shape[0]
+    nv, nt = base.positions.shape[0], base.indices.shape[0]
+    for k, m16 in instances:
+        model = models[k]
+        if k not in mat_base:
+            mat_base[k] = nmat
+            mats.append(model.materials)
+            nmat += model.materials.shape[0]
+        p, n = flatten_instance(model, m16)
+        pos.append(p)
+        nrm.append(n)
+        idx.append(model.indices)
+        tm.append(model.tri_material)
+        for fv, cnt, fi, ni, mi, em in model.meshes:
+            meshes.append((fv + nv, cnt, fi + 3 * nt, ni, mi + mat_base[k], em))
+        nv += model.positions.shape[0]
+        nt += model.indices.shape[0]
+    return Scene(positions=np.concatenate(pos), normals=np.concatenate(nrm), indices=np.concatenate(idx),
+                        tri_material=np.concatenate(tm), meshes=np.asarray(meshes, np.uint32),
+                        materials=np.concatenate(mats).astype(np.float32), env=base.env, sun=base.sun)
+
+
 def city_camera(extent: float = 2000.0):
     """Elevated view over the city towards its centre."""
     return dict(eye=(-0.42 * extent, 0.12 * extent, -0.42 * extent), target=(0.0, 20.0, 0.0), fov=50.0)

@@ -334,21 +334,30 @@ def cornell_config(cpu: bool) -> dict:
 
 
 def city_spectral_config(cpu: bool) -> dict:
-    """The large spectral configuration: the seeded 10.0M-triangle city (4096
-    buildings on a 2 km grid, 10k emissive window triangles, sky environment),
-    hero-wavelength paths (4 wavelengths in 360-830 nm, RGB-to-spectrum
-    albedos and emitters), depth 16, 4096x4096 at 64 spp: one warm-up image at
-    4 spp, then one timed image (device time); then the same in radiance-cache
-    mode (`cache`: paths ended at their first bounce's hit in the online-trained
-    cache, after 8 training passes).  The CPU oracle of the same integrator
-    renders 64 full-width rows at 1 spp beside it."""
-    from appearance_b200 import spectral_bench
+    """The large spectral configuration: the seeded instanced city (4096
+    instances of 64 box-building models on a 2 km grid, 10.0M world triangles,
+    emissive windows, sky environment) placed by world actions and traced
+    through the two-level BVH, hero-wavelength paths (4 wavelengths in 360-830
+    nm, RGB-to-spectrum albedos and emitters), depth 16, 4096x4096 at 64 spp:
+    one warm-up image at 4 spp, then one timed image (device time).  Beside
+    it the flat city (4096 distinct buildings, one world-space BVH) plain and
+    in radiance-cache mode (`cache`: paths ended at their first bounce's hit in
+    the online-trained cache, after 8 training passes).  The CPU oracle of the
+    same integrator renders 64 full-width rows of the instanced city at 1 spp."""
+    from appearance_b200 import scenes, spectral_bench
     kept = {}
-    res = spectral_bench.measure(cache=True, keep_scene=kept if cpu else None)
+    res = spectral_bench.measure(instanced=True, keep_scene=kept if cpu else None)
+    flat = spectral_bench.measure(instanced=False, cache=True)
+    res["flat_city"] = {k: flat[k] for k in ("value", "unit", "frame_ms", "rays_per_sample", "workload", "traversal")}
+    res["cache"] = flat["cache"]
     if cpu:
-        from oracle.oracle import OracleScene, OracleSpectral
+        from oracle.oracle import OracleScene, OracleSpectral, OracleTwoLevel
         rows, size, threads = 64, kept["size"], os.cpu_count()
-        osp = OracleSpectral(OracleScene(kept["scene"]), **kept["light"])
+        base, models, instances = kept["scene"]
+        eye = np.eye(4, dtype=np.float32).reshape(16)
+        tl = OracleTwoLevel([base] + list(models), [(0, eye)] + [(k + 1, m) for k, m in instances])
+        osp = OracleSpectral(OracleScene(scenes.flatten_world(base, models, instances)), two_level=tl,
+                             **kept["light"])
         r0 = size // 2 - rows // 2
         t0 = time.perf_counter()
         osp.render(kept["mats"], size, size, spp=1, max_depth=kept["depth"], seed=100, row0=r0, row1=r0 + rows,

@@ -60,49 +60,9 @@ def test_world_action_wire_sizes():
     assert struct.unpack("<16f", s[:64]) == tuple(np.eye(4, dtype=np.float32).reshape(16))
 
 
-def flatten_instance(model, m16):
-    """One instance in world space with the library's arithmetic (world.cpp):
-    positions m * (p, 1) summed left to right in float32; normals by the
-    inverse transpose of the upper 3x3 (cofactors over the determinant in
-    double, rounded to float), renormalised in float32."""
-    m = np.asarray(m16, np.float32).reshape(16)
-    f = np.float32
-    x, y, z = (model.positions[:, k].astype(f) for k in range(3))
-    pos = np.stack([((m[r] * x + m[4 + r] * y) + m[8 + r] * z) + m[12 + r] for r in range(3)], 1).astype(f)
-    a = [[float(m[4 * c + r]) for r in range(3)] for c in range(3)]
-    det = (a[0][0] * (a[1][1] * a[2][2] - a[2][1] * a[1][2]) - a[1][0] * (a[0][1] * a[2][2] - a[2][1] * a[0][2])
-           + a[2][0] * (a[0][1] * a[1][2] - a[1][1] * a[0][2]))
-    nt = np.zeros((3, 3), f)
-    for r in range(3):
-        for k in range(3):
-            r1, r2, k1, k2 = (r + 1) % 3, (r + 2) % 3, (k + 1) % 3, (k + 2) % 3
-            nt[r, k] = f((a[k1][r1] * a[k2][r2] - a[k2][r1] * a[k1][r2]) / det)
-    nx, ny, nz = (model.normals[:, k].astype(f) for k in range(3))
-    n = np.stack([(nt[r, 0] * nx + nt[r, 1] * ny) + nt[r, 2] * nz for r in range(3)], 1).astype(f)
-    ln = np.sqrt((n[:, 0] * n[:, 0] + n[:, 1] * n[:, 1]) + n[:, 2] * n[:, 2]).astype(f)
-    s = np.where(ln > 0, f(1.0) / np.where(ln > 0, ln, f(1.0)), f(0.0)).astype(f)
-    return pos, (n * s[:, None]).astype(f)
-
-
 def compose(base, model, transforms):
     """base + instances of `model`, as World::flatten lays them out."""
-    pos, nrm, idx, tm, meshes = [base.positions], [base.normals], [base.indices], [base.tri_material], list(base.meshes)
-    mats = [base.materials, model.materials]
-    mat0 = base.materials.shape[0]
-    nv, nt = base.positions.shape[0], base.indices.shape[0]
-    for m16 in transforms:
-        p, n = flatten_instance(model, m16)
-        pos.append(p)
-        nrm.append(n)
-        idx.append(model.indices)
-        tm.append(model.tri_material)
-        for fv, cnt, fi, ni, mi, em in model.meshes:
-            meshes.append((fv + nv, cnt, fi + 3 * nt, ni, mi + mat0, em))
-        nv += model.positions.shape[0]
-        nt += model.indices.shape[0]
-    return scenes.Scene(positions=np.concatenate(pos), normals=np.concatenate(nrm), indices=np.concatenate(idx),
-                        tri_material=np.concatenate(tm), meshes=np.asarray(meshes, np.uint32),
-                        materials=np.concatenate(mats).astype(np.float32), env=base.env, sun=base.sun)
+    return scenes.flatten_world(base, [model], [(0, m16) for m16 in transforms])
 
 
 def test_flatten_rule_moves_points_and_keeps_normals_unit():
@@ -110,7 +70,7 @@ def test_flatten_rule_moves_points_and_keeps_normals_unit():
     m = np.eye(4, dtype=np.float32)
     m[:3, :3] = [[0, -2, 0], [2, 0, 0], [0, 0, 3]]
     m[:3, 3] = [1, 2, 3]
-    p, n = flatten_instance(model, m.T.reshape(16))  # column-major
+    p, n = scenes.flatten_instance(model, m.T.reshape(16))  # column-major
     ref = model.positions.astype(np.float64) @ m[:3, :3].T.astype(np.float64) + m[:3, 3]
     np.testing.assert_allclose(p, ref, rtol=1e-6, atol=1e-5)
     np.testing.assert_allclose(np.linalg.norm(n, axis=1), 1.0, atol=1e-6)
@@ -137,29 +97,7 @@ def test_two_level_oracle_with_identity_instances_equals_the_flat_oracle():
     np.testing.assert_array_equal(two.any(o, d, 0.7), flat.any(o, d, np.full(len(o), 0.7, np.float32)))
 
 
+
+
 def compose_many(base, models, instances):
-    """base + instances of several models (model index, column-major 4x4) in
-    World::flatten's layout (a model's materials appended at its first use)."""
-    pos, nrm, idx, tm, meshes = [base.positions], [base.normals], [base.indices], [base.tri_material], list(base.meshes)
-    mats = [base.materials]
-    mat_base = {}
-    nmat = base.materials.shape[0]
-    nv, nt = base.positions.shape[0], base.indices.shape[0]
-    for k, m16 in instances:
-        model = models[k]
-        if k not in mat_base:
-            mat_base[k] = nmat
-            mats.append(model.materials)
-            nmat += model.materials.shape[0]
-        p, n = flatten_instance(model, m16)
-        pos.append(p)
-        nrm.append(n)
-        idx.append(model.indices)
-        tm.append(model.tri_material)
-        for fv, cnt, fi, ni, mi, em in model.meshes:
-            meshes.append((fv + nv, cnt, fi + 3 * nt, ni, mi + mat_base[k], em))
-        nv += model.positions.shape[0]
-        nt += model.indices.shape[0]
-    return scenes.Scene(positions=np.concatenate(pos), normals=np.concatenate(nrm), indices=np.concatenate(idx),
-                        tri_material=np.concatenate(tm), meshes=np.asarray(meshes, np.uint32),
-                        materials=np.concatenate(mats).astype(np.float32), env=base.env, sun=base.sun)
+    return scenes.flatten_world(base, models, instances)
