@@ -11,13 +11,14 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libappearance_cuda.so")
 
-AP_OK, AP_E_INVALID, AP_E_OOM, AP_E_CUDA, AP_E_TIMEOUT, AP_E_UNSUPPORTED, AP_E_NO_SCENE = range(7)
+AP_OK, AP_E_INVALID, AP_E_OOM, AP_E_CUDA, AP_E_TIMEOUT, AP_E_UNSUPPORTED, AP_E_NO_SCENE, AP_E_CANCELLED = range(8)
 
 EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error", "ap_set_config",
            "ap_world_action", "ap_scene_upload", "ap_model_register", "ap_set_camera_matrices", "ap_render_hdr", "ap_render_rgba8", "ap_render_device",
            "ap_device_framebuffer", "ap_trace_rays", "ap_trace_rays_static", "ap_read_buffer", "ap_profile_frame",
            "ap_bvh_stats", "ap_server_create", "ap_server_destroy", "ap_server_last_error", "ap_server_add_scene",
-           "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_stats",
+           "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_cancel",
+           "ap_server_stats",
            "ap_rc_create", "ap_rc_destroy", "ap_rc_last_error", "ap_rc_set_params", "ap_rc_get_params", "ap_rc_infer",
            "ap_rc_train", "ap_rc_attach", "ap_rc_wait_selftest", "ap_spectral_setup", "ap_render_spectral", "ap_profile_spectral"]
 
@@ -51,7 +52,7 @@ class FrameStats(ctypes.Structure):
 
 class Job(ctypes.Structure):
     _fields_ = [("scene", U32), ("width", U32), ("height", U32), ("spp", U32), ("max_depth", U32), ("seed", U32),
-                ("mats", F32 * 64)]
+                ("deadline_ms", U32), ("mats", F32 * 64)]
 
 
 class JobResult(ctypes.Structure):
@@ -108,6 +109,7 @@ def load() -> ctypes.CDLL:
     L.ap_server_submit.argtypes = [P, ctypes.POINTER(Job), P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]
     L.ap_server_query.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]
     L.ap_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(JobResult)]
+    L.ap_server_cancel.argtypes = [P, ctypes.c_uint64]
     L.ap_server_stats.argtypes = [P, P]
     L.ap_rc_create.restype = P
     L.ap_rc_create.argtypes = [ctypes.c_int, P, P, U32, ctypes.POINTER(ctypes.c_int)]

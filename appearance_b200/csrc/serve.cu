@@ -63,6 +63,7 @@ struct Job {
   std::string err;
   double gpu_ms = 0.0;
   int graph_mode = 0;  // 0 direct launches, 1 graph instantiated, 2 graph updated in place
+  bool cancelled = false;
 };
 
 struct Slot {
@@ -209,6 +210,10 @@ void dispatcher(Server* s) {
         j->rc = AP_E_CUDA;
         j->err = std::string("job: ") + cudaGetErrorString(e);
       }
+      if (j->rc == AP_OK && j->cancelled) {
+        j->rc = AP_E_CANCELLED;
+        j->err = "job cancelled while it ran";
+      }
       if (j->rc == AP_OK && !j->out_pinned)
         std::memcpy(j->out, sl.staging, (size_t)j->desc.width * j->desc.height * 12);
       if (j->dev) cudaFreeAsync(j->dev, sl.stream);
@@ -221,6 +226,22 @@ void dispatcher(Server* s) {
       sl.job = nullptr;
       sl.finished = false;
       s->cv_done.notify_all();
+    }
+    // queued jobs past their deadline complete without running
+    const Clock::time_point now = Clock::now();
+    for (auto it = s->pending.begin(); it != s->pending.end();) {
+      Job* j = *it;
+      if (j->desc.deadline_ms && ms_between(j->t_submit, now) >= (double)j->desc.deadline_ms) {
+        j->rc = AP_E_TIMEOUT;
+        j->err = "job deadline passed in the queue";
+        j->t_admit = j->t_done = now;
+        j->done = true;
+        s->completed++;
+        it = s->pending.erase(it);
+        s->cv_done.notify_all();
+      } else {
+        ++it;
+      }
     }
     // admissions, in arrival order
     while (!s->pending.empty()) {
@@ -289,7 +310,17 @@ void dispatcher(Server* s) {
     if (s->stop && s->pending.empty() && !inflight) break;
     bool ready = false;
     for (const Slot& sl : s->slots) ready = ready || (sl.job && sl.finished);
-    if (!ready) s->cv_work.wait(lk);
+    if (!ready) {
+      // sleep until a completion, a submission, or the nearest queued deadline
+      double wait_ms = -1.0;
+      for (const Job* j : s->pending)
+        if (j->desc.deadline_ms) {
+          const double left = (double)j->desc.deadline_ms - ms_between(j->t_submit, Clock::now());
+          wait_ms = wait_ms < 0.0 ? left : std::min(wait_ms, left);
+        }
+      if (wait_ms < 0.0) s->cv_work.wait(lk);
+      else if (wait_ms > 0.0) s->cv_work.wait_for(lk, std::chrono::duration<double, std::milli>(wait_ms));
+    }
   }
 }
 
@@ -476,6 +507,35 @@ int ap_server_wait(void* sp, uint64_t ticket, ap_job_result* res) {
   s->jobs.erase(it);
   delete j;
   return rc;
+}
+
+int ap_server_cancel(void* sp, uint64_t ticket) {
+  Server* s = static_cast<Server*>(sp);
+  if (!s) return AP_E_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) {
+      s->err = "unknown ticket";
+      return AP_E_INVALID;
+    }
+    Job* j = it->second;
+    if (j->done) return AP_OK;
+    auto q = std::find(s->pending.begin(), s->pending.end(), j);
+    if (q != s->pending.end()) {  // still queued: dropped
+      s->pending.erase(q);
+      j->rc = AP_E_CANCELLED;
+      j->err = "job cancelled before it started";
+      j->t_admit = j->t_done = Clock::now();
+      j->done = true;
+      s->completed++;
+      s->cv_done.notify_all();
+    } else {
+      j->cancelled = true;  // on the GPU: reported when its launches finish
+    }
+  }
+  s->cv_work.notify_one();
+  return AP_OK;
 }
 
 int ap_server_stats(void* sp, uint64_t* out8) {

@@ -77,11 +77,14 @@ class RenderServer:
         return int(_native.load().ap_server_job_bytes(width, height))
 
     def submit(self, scene: int, width: int, height: int, spp: int, max_depth: int, seed: int, mats,
-               out: np.ndarray | None = None) -> int:
+               out: np.ndarray | None = None, deadline_ms: int = 0) -> int:
         """Queues a job and returns its ticket.  `out` (float32, height x width x 3)
-        receives the result; page-locked memory avoids one host copy."""
+        receives the result; page-locked memory avoids one host copy.  A job
+        still queued `deadline_ms` after submission (0: no deadline) is not
+        started and its wait raises with AP_E_TIMEOUT."""
         j = _native.Job()
         j.scene, j.width, j.height, j.spp, j.max_depth, j.seed = scene, width, height, spp, max_depth, seed
+        j.deadline_ms = deadline_ms
         m = np.ascontiguousarray(mats, np.float32).reshape(64)
         for i in range(64):
             j.mats[i] = float(m[i])
@@ -106,6 +109,11 @@ class RenderServer:
         self._check(self._lib.ap_server_wait(self._s, ticket, ctypes.byref(r)))
         return out, dict(queued_ms=r.queued_ms, total_ms=r.total_ms, gpu_ms=r.gpu_ms, device_bytes=r.device_bytes,
                          graph_mode=r.graph_mode, slot=r.slot)
+
+    def cancel(self, ticket: int):
+        """ap_server_cancel: a queued job is dropped; one on the GPU finishes its
+        launches; either way its wait raises with AP_E_CANCELLED."""
+        self._check(self._lib.ap_server_cancel(self._s, ticket))
 
     def stats(self) -> dict:
         a = np.zeros(8, np.uint64)

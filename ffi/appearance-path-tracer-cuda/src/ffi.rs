@@ -12,6 +12,7 @@ pub const AP_E_CUDA: c_int = 3;
 pub const AP_E_TIMEOUT: c_int = 4;
 pub const AP_E_UNSUPPORTED: c_int = 5;
 pub const AP_E_NO_SCENE: c_int = 6;
+pub const AP_E_CANCELLED: c_int = 7;
 pub const AP_RC_NUM_PARAMS: u32 = 21696;
 
 #[repr(C)]
@@ -111,6 +112,7 @@ pub struct ApJob {
     pub spp: u32,
     pub max_depth: u32,
     pub seed: u32,
+    pub deadline_ms: u32,
     pub mats: [f32; 64],
 }
 
@@ -178,6 +180,7 @@ extern "C" {
                             ticket: *mut u64) -> c_int;
     pub fn ap_server_query(server: *mut c_void, ticket: u64, done: *mut c_int) -> c_int;
     pub fn ap_server_wait(server: *mut c_void, ticket: u64, result: *mut ApJobResult) -> c_int;
+    pub fn ap_server_cancel(server: *mut c_void, ticket: u64) -> c_int;
     pub fn ap_server_stats(server: *mut c_void, out8: *mut u64) -> c_int;
 
     // radiance cache

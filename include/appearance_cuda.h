@@ -36,7 +36,8 @@ enum {
   AP_E_CUDA = 3,        /* CUDA runtime error (message in ap_last_error) */
   AP_E_TIMEOUT = 4,     /* a bounded device wait ran out */
   AP_E_UNSUPPORTED = 5, /* valid request this library does not implement */
-  AP_E_NO_SCENE = 6     /* render before any geometry was uploaded */
+  AP_E_NO_SCENE = 6,    /* render before any geometry was uploaded */
+  AP_E_CANCELLED = 7    /* a serving job was cancelled (ap_server_cancel) */
 };
 
 /* PathTracerGpuConfig plus the literals the reference hard-codes in render()
@@ -291,6 +292,8 @@ typedef struct ap_job {
   uint32_t spp;             /* 1..4096 */
   uint32_t max_depth;       /* bounces, 1..64 */
   uint32_t seed;            /* frame index of the per-pixel PCG streams */
+  uint32_t deadline_ms;     /* 0: none; else a job still queued this long after submission is not
+                               started and completes with AP_E_TIMEOUT */
   float mats[64];           /* inv_view, inv_proj, view_proj, prev_view_proj (column-major) */
 } ap_job;
 
@@ -318,6 +321,12 @@ int ap_server_submit(void* server, const ap_job* job, float* out_rgb, size_t out
 int ap_server_query(void* server, uint64_t ticket, int* done);
 /* Blocks until the job is done; returns its status and releases the ticket. */
 int ap_server_wait(void* server, uint64_t ticket, ap_job_result* result);
+/* Cancels a job: a queued job is dropped without running; a job already on
+ * the GPU runs to the end of its launches (device work is not interrupted),
+ * and its output buffer may have been written.  Either way its wait returns
+ * AP_E_CANCELLED.  A finished job is left as it is (AP_OK); an unknown ticket
+ * is AP_E_INVALID. */
+int ap_server_cancel(void* server, uint64_t ticket);
 /* completed, in flight, queued, device bytes in use, peak device bytes, scene
  * bytes, graphs instantiated, graphs updated in place */
 int ap_server_stats(void* server, uint64_t* out8);

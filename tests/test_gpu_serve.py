@@ -91,3 +91,50 @@ def test_admission_respects_the_budget():
     with pytest.raises(RendererError):
         srv.wait(srv.submit(sid, 1024, 1024, 1, 1, 0, mats_for(0, 0, 1024, 1024)))
     srv.close()
+
+
+def test_faults_fail_their_own_job_only():
+    """Host-side fault injection on the serving loop (no GPU fault): a job
+    cancelled while queued, a job whose deadline passes in the queue, a job
+    naming an unknown scene, and a job too large for the device-memory budget
+    each fail with their own status, while the jobs around them complete with
+    the images they give alone."""
+    from appearance_b200 import _native
+    sc = small_scene(0)
+    srv = RenderServer(CFG, hbm_budget=2e9, max_inflight=1, use_graphs=False)
+    sid = srv.add_scene(sc)
+    w, h = 96, 64
+    m = mats_for(0, 2, w, h)
+    ref, _ = srv.wait(srv.submit(sid, w, h, 2, 3, 4, m))  # the image of the probe job alone
+    # one slot: a long job occupies it while the others queue behind
+    long_t = srv.submit(sid, 512, 512, 64, 3, 1, mats_for(0, 5, 512, 512))
+    dropped = srv.submit(sid, w, h, 2, 3, 4, m)
+    late = srv.submit(sid, w, h, 2, 3, 4, m, deadline_ms=1)
+    probe = srv.submit(sid, w, h, 2, 3, 4, m)
+    srv.cancel(dropped)
+    with pytest.raises(RendererError) as e:  # a corrupted scene id is refused at submission
+        srv.submit(sid + 7, w, h, 2, 3, 4, m)
+    assert e.value.code == _native.AP_E_INVALID
+    srv.wait(long_t)
+    with pytest.raises(RendererError) as e:
+        srv.wait(dropped)
+    assert e.value.code == _native.AP_E_CANCELLED
+    with pytest.raises(RendererError) as e:
+        srv.wait(late)
+    assert e.value.code == _native.AP_E_TIMEOUT
+    img, _ = srv.wait(probe)
+    assert same_bits(img, ref)
+    # a job larger than the whole budget fails alone; the next job still runs
+    big_w = big_h = 4096
+    assert RenderServer.job_bytes(big_w, big_h) > 2e9
+    big = srv.submit(sid, big_w, big_h, 1, 3, 4, mats_for(0, 1, big_w, big_h))
+    after = srv.submit(sid, w, h, 2, 3, 4, m)
+    with pytest.raises(RendererError) as e:
+        srv.wait(big)
+    assert e.value.code == _native.AP_E_OOM
+    img, _ = srv.wait(after)
+    assert same_bits(img, ref)
+    # cancelling a finished or unknown ticket
+    with pytest.raises(RendererError):
+        srv.cancel(123456789)
+    srv.close()
