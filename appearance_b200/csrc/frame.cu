@@ -310,6 +310,39 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_pair(DevScene
       });
 }
 
+// Persistent closest-hit traversal of two ray queues in one launch, each hit
+// going to its own queue's hit array (the closest-hit form of k_trace_pair).
+template <int Q0, int Q1, bool kCount>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_pair_closest(DevScene s, FrameBuffers fb, uint32_t cap,
+                                                                                uint4* h0, uint4* h1) {
+  const uint32_t n0 = min(fb.counters[kCounterQueueSize + Q0], cap);
+  const uint32_t count = n0 + min(fb.counters[kCounterQueueSize + Q1], cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fb.counters[3], count);
+  const float4 *o0 = fb.rq_o[Q0], *d0 = fb.rq_d[Q0], *o1 = fb.rq_o[Q1], *d1 = fb.rq_d[Q1];
+  persistent_trace<false, kCount>(
+      s, count, &fb.counters[kCounterQueueCursor + Q0],
+      [&](uint32_t i, float3& o, float3& d, float& tmax) {
+        const bool first = i < n0;
+        const uint32_t j = first ? i : i - n0;
+        const float4 a = (first ? o0 : o1)[j], b = (first ? d0 : d1)[j];
+        o = f3(a.x, a.y, a.z);
+        d = f3(b.x, b.y, b.z);
+        tmax = a.w;
+      },
+      [&](uint32_t i, const Trav& t, const Visits& vc) {
+        const bool first = i < n0;
+        const uint32_t j = first ? i : i - n0;
+        const uint32_t owner = __float_as_uint((first ? d0 : d1)[j].w);
+        (first ? h0 : h1)[owner] =
+            make_uint4(__float_as_uint(t.hit.t), __float_as_uint(t.hit.u), __float_as_uint(t.hit.v), t.hit.tri);
+        if (kCount) {
+          atomicAdd(&fb.visits[3 * K_TRACE_CLOSEST + 0], 1ull);
+          atomicAdd(&fb.visits[3 * K_TRACE_CLOSEST + 1], (unsigned long long)vc.nodes);
+          atomicAdd(&fb.visits[3 * K_TRACE_CLOSEST + 2], (unsigned long long)vc.tris);
+        }
+      });
+}
+
 // ---- trace.wgsl:62-262 as four stages around the secondary rays -------------
 //   A: hit attributes, emission, G-buffer, first NEE candidates (area + BSDF);
 //      queues the BSDF candidate ray            (Nee::sample_ris, nee.wgsl:131-197)
@@ -1547,6 +1580,323 @@ __global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_dsp_b(DevScene s, Fr
   push_ray(fb, Q_GI_SHADOW, there.ray, there.o, there.tmax, there.d, id);
 }
 
+// ---- unbiased ReSTIR GI spatial pass as wavefront stages ---------------------
+//
+// The same pass as k_spatial<true> with unbiased = 1 (restir_gi_spatial.wgsl:
+// 71-166), split at the rays of its target evaluations.  A target
+// (GiReservoir::phat, inline_path_tracer.wgsl:299-331) re-traces a closest-hit
+// ray toward the sample point and, at its hit, a shadow ray of a uniform light
+// sample (InlinePathTracer::trace with the approx() config, :51-256).  Per
+// neighbour i:
+//   k_gsp_a(i)  finishes neighbour i-1 (its Z, hence W), picks neighbour i
+//               and queues the re-trace of its sample's target here (Q_GI_CAND);
+//   closest-hit queue;
+//   k_gsp_b(i)  shades that hit and queues its shadow ray (Q_GI_SHADOW);
+//   any-hit queue;
+//   k_gsp_c(i)  combines; queues the re-traces of the combined sample's target
+//               here (Q_BSDF_CAND; none when it is known: the neighbour's own
+//               sample, or the memoised one) and at the neighbour (Q_GI_CAND);
+//   both closest-hit queues in one launch;
+//   k_gsp_d(i)  shades those hits and queues their shadow rays (Q_RIS_SHADOW,
+//               Q_GI_SHADOW);
+//   both any-hit queues in one launch.
+// k_gsp_a(nsamples) finishes the last neighbour and writes the history and the
+// payload's RNG.  The reservoir being built lives in out_a/out_b; the loop
+// state in the stage buffers:
+//   st_a {radius, rng, neighbour id, flags}   st_b memo {point.xyz, phat_rng}
+//   st_c {memoised target, throughput of the pending re-trace here (.yzw),
+//         later the neighbour's sample's target here if unoccluded (.y)}
+//   st_d {M of the pixel's reservoir, M of the neighbour's, target of the
+//         combined sample here (known, or if unoccluded), -}
+//   st_e {throughput of the re-trace at the neighbour}
+// The target of the combined sample at the neighbour only counts by its sign.
+// With a zero re-trace throughput it is not positive whatever the rays find
+// (the radiance is 0, or NaN from an infinite factor), so that re-trace is not
+// traced.
+enum : uint32_t {
+  GS_ACTIVE = 1u,      // neighbour passed the depth/normal test: its sample is combined
+  GS_N_SHADOW = 2u,    // neighbour's sample here: shadow ray queued
+  GS_C_RAY = 4u,       // combined sample here: re-trace queued (target not known)
+  GS_C_SHADOW = 8u,    // combined sample here: shadow ray queued
+  GS_CN_RAY = 16u,     // combined sample at the neighbour: re-trace queued
+  GS_CN_SHADOW = 32u,  // combined sample at the neighbour: shadow ray queued
+  GS_CN_POS = 64u,     // combined sample at the neighbour: target positive if unoccluded
+  GS_MEMO = 128u,      // st_b / st_c.x hold a memoised target
+};
+
+// First half of GiReservoir::phat at a surface (hit point, wo, light-sample
+// context cx, path throughput T): direction to the sample point, the
+// re-trace's origin and throughput.
+struct GiRetrace {
+  float3 wi, gi_origin, tr;
+};
+APD GiRetrace gi_retrace_begin(const DevScene& s, float3 point, const uint4 cx, float3 T, float3 hit, float3 wo) {
+  Bsdf b = load_bsdf(s.materials + cx.x);
+  Frame fr = ctx_frame(cx);
+  GiRetrace g;
+  g.wi = normalize(point - hit);
+  float sp = 0.0f;
+  float3 refl = disney_eval(b, fr, wo, g.wi, &sp);
+  float cos_in = dm::fabs_(dot(g.wi, fr.n));
+  float3 local = cos_in * refl;
+  g.gi_origin = hit + g.wi * 0.0001f;
+  g.tr = T * local;
+  return g;
+}
+APD GiRetrace gi_retrace_at(float3 point, float3 hit, float3 tr) {
+  GiRetrace g;
+  g.wi = normalize(point - hit);
+  g.gi_origin = hit + g.wi * 0.0001f;
+  g.tr = tr;
+  return g;
+}
+
+// Second half: the re-trace's closest hit `hr` shaded with a uniform light
+// sample drawn from the sample's own stream (prng), or the sky on a miss.
+// acc is the radiance when the shadow ray (if any) is unoccluded.
+struct GiShade {
+  float3 acc, o, d;
+  float tmax;
+  bool ray;
+};
+APD GiShade gi_retrace_hit(const DevScene& s, const uint4 hr, const GiRetrace& g, uint32_t prng) {
+  GiShade r;
+  r.acc = f3s(0.0f);
+  r.o = f3s(0.0f);
+  r.d = f3s(0.0f);
+  r.tmax = 0.0f;
+  r.ray = false;
+  if (hr.w != kNoHit) {
+    Hit h{__uint_as_float(hr.x), __uint_as_float(hr.y), __uint_as_float(hr.z), hr.w};
+    const MaterialDev* m;
+    Surface sf = surface(s, h, g.gi_origin, g.wi, &m);
+    Bsdf b = load_bsdf(m);
+    float pdf = 0.0f;
+    float r0 = rnd(prng), r1 = rnd(prng), r2 = rnd(prng), r3 = rnd(prng), r4 = rnd(prng);
+    LightSample ls = sample_uniform(s, r0, r1, r2, make_float2(r3, r4), &pdf);
+    float W = 1.0f / pdf;
+    if (W > 0.0f) {
+      LightEval ev = load_eval(s, ls, sf.hit_point);
+      float3 sdir = normalize(ev.point - sf.hit_point);
+      float sdist = dist(ev.point, sf.hit_point);
+      float ndl = dot(sdir, sf.n);
+      if (ndl > 0.0f) {
+        float sp = 0.0f;
+        float3 refl = disney_eval(b, sf.frame, -g.wi, sdir, &sp);
+        r.acc = f3s(0.0f) + g.tr * refl * ev.emission * ndl * W;
+        r.o = sf.hit_point + sf.n * 1e-4f;
+        r.d = sdir;
+        r.tmax = sdist - 1e-4f * 2.0f;
+        r.ray = true;
+      }
+    }
+  } else {
+    r.acc = f3s(0.0f) + g.tr * sky_radiance(s, g.wi, true);
+  }
+  return r;
+}
+
+APD float3 f3_bits(uint32_t x, uint32_t y, uint32_t z) { return f3(__uint_as_float(x), __uint_as_float(y), __uint_as_float(z)); }
+APD float3 primary_hit(const FrameBuffers& fb, uint32_t id, float pt) {
+  const float4 ray = fb.rays[id];
+  return ray_org(ray) + ray_dir(ray) * pt;
+}
+
+__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_a(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
+                                                uint32_t pass_count, uint32_t nsamples, uint32_t i,
+                                                const uint4* in_a, const uint4* in_b, uint4* out_a, uint4* out_b,
+                                                uint4* prev_a, uint4* prev_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  const uint32_t id = y * c.W + x;
+  uint4 pl = fb.payload[id];
+  const float pt = __uint_as_float(pl.z);
+  if (pt < 0.0f) return;
+  uint4 sa, sb, sc;
+  if (i == 0) {
+    sa = make_uint4(__float_as_uint(spatial_radius0(c)), pl.y, 0u, 0u);
+    sb = make_uint4(0u, 0u, 0u, 0u);
+    sc = make_uint4(0u, 0u, 0u, 0u);
+    out_a[id] = in_a[id];
+    out_b[id] = in_b[id];
+  } else {
+    sa = fb.st_a[id];
+    sb = fb.st_b[id];
+    sc = fb.st_c[id];
+    if (sa.w & GS_ACTIVE) {
+      // finish neighbour i-1: Z of the combined sample, then W
+      const uint4 sd = fb.st_d[id];
+      float zc = __uint_as_float(sd.z);
+      if ((sa.w & GS_C_SHADOW) && !fb.vis[Q_RIS_SHADOW][id]) zc = luma(f3s(0.0f));
+      GiRes cmb = gi_unpack(out_a[id], out_b[id]);
+      sb = gi_pack_b(cmb);  // memo: the combined sample and its target here
+      sc.x = __float_as_uint(zc);
+      sa.w |= GS_MEMO;
+      float z = 0.0f;
+      if (zc > 0.0f) z = z + __uint_as_float(sd.x);
+      const bool there = (sa.w & GS_CN_POS) && (!(sa.w & GS_CN_SHADOW) || fb.vis[Q_GI_SHADOW][id]);
+      if (there) z = z + __uint_as_float(sd.y);
+      if (cmb.phat > 0.0f && z * cmb.wsum > 0.0f) {
+        cmb.W = (1.0f / cmb.phat) * (1.0f / z * cmb.wsum);
+        out_a[id] = gi_pack_a(cmb);
+      }
+    }
+  }
+  sa.w &= GS_MEMO;
+  if (i == nsamples) {
+    if (pass_idx == pass_count - 1) {
+      prev_a[id] = out_a[id];
+      prev_b[id] = out_b[id];
+    }
+    pl.y = sa.y;
+    fb.payload[id] = pl;
+    return;
+  }
+  SpatialPixel sp;
+  spatial_pixel<true>(fb, c, x, y, pass_idx, pass_count, pt, sp);
+  float radius = __uint_as_float(sa.x);
+  const uint32_t nid = spatial_neighbour(c, sp, i, nsamples, radius);
+  bool want = false;
+  GiRetrace g;
+  g.wi = f3s(0.0f);
+  g.gi_origin = f3s(0.0f);
+  if (nid != id) {
+    if (spatial_similar(fb, c, sp, nid)) {
+      const GiRes nr = gi_unpack(in_a[nid], in_b[nid]);
+      g = gi_retrace_begin(s, nr.point, sp.cx, unpack_rgb9e5(pl.x), sp.hit, sp.wo);
+      want = true;
+      sa.w |= GS_ACTIVE;
+      sc.y = __float_as_uint(g.tr.x);
+      sc.z = __float_as_uint(g.tr.y);
+      sc.w = __float_as_uint(g.tr.z);
+    } else {
+      radius = dm::fmax(radius * 0.5f, 3.0f);
+    }
+  }
+  sa.x = __float_as_uint(radius);
+  sa.z = nid;
+  fb.st_a[id] = sa;
+  fb.st_b[id] = sb;
+  fb.st_c[id] = sc;
+  push_ray(fb, Q_GI_CAND, want, g.gi_origin + g.wi * 1e-4f, 1000.0f - 1e-4f * 2.0f, g.wi, id);
+}
+
+__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_b(DevScene s, FrameBuffers fb, Consts c, const uint4* in_a,
+                                                const uint4* in_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  const uint32_t id = y * c.W + x;
+  const float pt = __uint_as_float(fb.payload[id].z);
+  if (pt < 0.0f) return;
+  uint4 sa = fb.st_a[id];
+  if (!(sa.w & GS_ACTIVE)) return;
+  uint4 sc = fb.st_c[id];
+  const GiRes nr = gi_unpack(in_a[sa.z], in_b[sa.z]);
+  const GiRetrace g = gi_retrace_at(nr.point, primary_hit(fb, id, pt), f3_bits(sc.y, sc.z, sc.w));
+  const GiShade sh = gi_retrace_hit(s, fb.hit_gi[id], g, nr.phat_rng);
+  if (sh.ray) sa.w |= GS_N_SHADOW;
+  sc.y = __float_as_uint(luma(sh.acc));
+  fb.st_a[id] = sa;
+  fb.st_c[id] = sc;
+  push_ray(fb, Q_GI_SHADOW, sh.ray, sh.o, sh.tmax, sh.d, id);
+}
+
+__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_c(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
+                                                uint32_t pass_count, const uint4* in_a, const uint4* in_b,
+                                                uint4* out_a, uint4* out_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  const uint32_t id = y * c.W + x;
+  const uint4 pl = fb.payload[id];
+  const float pt = __uint_as_float(pl.z);
+  if (pt < 0.0f) return;
+  uint4 sa = fb.st_a[id];
+  if (!(sa.w & GS_ACTIVE)) return;
+  uint4 sc = fb.st_c[id];
+  const uint4 sb = fb.st_b[id];
+  const uint32_t nid = sa.z;
+  uint32_t rng = sa.y;
+  const GiRes rgi = gi_unpack(out_a[id], out_b[id]);
+  GiRes nr = gi_unpack(in_a[nid], in_b[nid]);
+  nr.phat = ((sa.w & GS_N_SHADOW) && !fb.vis[Q_GI_SHADOW][id]) ? luma(f3s(0.0f)) : __uint_as_float(sc.y);
+  const bool valid = nr.phat > 0.0f;
+  GiRes cmb = gi_new();
+  gi_update(cmb, rgi.phat * rgi.W * rgi.M, rng, rgi.point, rgi.phat, rgi.phat_rng);
+  gi_update(cmb, nr.phat * nr.W * nr.M, rng, nr.point, nr.phat, nr.phat_rng);
+  cmb.M = rgi.M + nr.M;
+  SpatialPixel sp;
+  spatial_pixel<true>(fb, c, x, y, pass_idx, pass_count, pt, sp);
+  float zc = 0.0f;
+  bool here = false;
+  GiRetrace gc;
+  gc.wi = f3s(0.0f);
+  gc.gi_origin = f3s(0.0f);
+  if (gi_same(cmb, nr)) {
+    zc = nr.phat;
+  } else if ((sa.w & GS_MEMO) && gi_same_key(cmb, f3_bits(sb.x, sb.y, sb.z), sb.w)) {
+    zc = __uint_as_float(sc.x);
+  } else {
+    gc = gi_retrace_begin(s, cmb.point, sp.cx, unpack_rgb9e5(pl.x), sp.hit, sp.wo);
+    here = true;
+    sa.w |= GS_C_RAY;
+    sc.y = __float_as_uint(gc.tr.x);
+    sc.z = __float_as_uint(gc.tr.y);
+    sc.w = __float_as_uint(gc.tr.z);
+  }
+  const uint4 nga = fb.gb_a[c.frame_idx & 1u][nid];
+  const float3 npos = f3_bits(nga.x, nga.y, nga.z);
+  const float3 nwo = -ray_dir(fb.rays[nid]);
+  const float3 nT = unpack_rgb9e5(fb.payload[nid].x);
+  const GiRetrace gn = gi_retrace_begin(s, cmb.point, fb.ctx[nid], nT, npos, nwo);
+  const bool there = !(gn.tr.x == 0.0f && gn.tr.y == 0.0f && gn.tr.z == 0.0f);
+  if (there) sa.w |= GS_CN_RAY;
+  float radius = __uint_as_float(sa.x);
+  if (!valid) radius = dm::fmax(radius * 0.5f, 3.0f);
+  sa.x = __float_as_uint(radius);
+  sa.y = rng;
+  out_a[id] = gi_pack_a(cmb);
+  out_b[id] = gi_pack_b(cmb);
+  fb.st_a[id] = sa;
+  fb.st_c[id] = sc;
+  fb.st_d[id] = make_uint4(__float_as_uint(rgi.M), __float_as_uint(nr.M), __float_as_uint(zc), 0u);
+  fb.st_e[id] = make_uint4(__float_as_uint(gn.tr.x), __float_as_uint(gn.tr.y), __float_as_uint(gn.tr.z), 0u);
+  push_ray(fb, Q_BSDF_CAND, here, gc.gi_origin + gc.wi * 1e-4f, 1000.0f - 1e-4f * 2.0f, gc.wi, id);
+  push_ray(fb, Q_GI_CAND, there, gn.gi_origin + gn.wi * 1e-4f, 1000.0f - 1e-4f * 2.0f, gn.wi, id);
+}
+
+__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_d(DevScene s, FrameBuffers fb, Consts c, const uint4* out_a,
+                                                const uint4* out_b) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= c.W || y >= c.H) return;
+  const uint32_t id = y * c.W + x;
+  const float pt = __uint_as_float(fb.payload[id].z);
+  if (pt < 0.0f) return;
+  uint4 sa = fb.st_a[id];
+  if (!(sa.w & GS_ACTIVE)) return;
+  const GiRes cmb = gi_unpack(out_a[id], out_b[id]);
+  GiShade hc = {}, hn = {};
+  if (sa.w & GS_C_RAY) {
+    const uint4 sc = fb.st_c[id];
+    uint4 sd = fb.st_d[id];
+    const GiRetrace g = gi_retrace_at(cmb.point, primary_hit(fb, id, pt), f3_bits(sc.y, sc.z, sc.w));
+    hc = gi_retrace_hit(s, fb.hit_bsdf[id], g, cmb.phat_rng);
+    if (hc.ray) sa.w |= GS_C_SHADOW;
+    sd.z = __float_as_uint(luma(hc.acc));
+    fb.st_d[id] = sd;
+  }
+  if (sa.w & GS_CN_RAY) {
+    const uint4 se = fb.st_e[id];
+    const uint4 nga = fb.gb_a[c.frame_idx & 1u][sa.z];
+    const GiRetrace g = gi_retrace_at(cmb.point, f3_bits(nga.x, nga.y, nga.z), f3_bits(se.x, se.y, se.z));
+    hn = gi_retrace_hit(s, fb.hit_gi[id], g, cmb.phat_rng);
+    if (hn.ray) sa.w |= GS_CN_SHADOW;
+    if (luma(hn.acc) > 0.0f) sa.w |= GS_CN_POS;
+  }
+  fb.st_a[id] = sa;
+  push_ray(fb, Q_RIS_SHADOW, hc.ray, hc.o, hc.tmax, hc.d, id);
+  push_ray(fb, Q_GI_SHADOW, hn.ray, hn.o, hn.tmax, hn.d, id);
+}
+
 // ---- radiance cache mode ------------------------------------------------------
 
 // Query of the cache at a path vertex: position, roughness, outgoing direction,
@@ -2095,7 +2445,7 @@ size_t frame_buffer_bytes(uint32_t W, uint32_t H) {
   for (int i = 0; i < 10; ++i) add(P * 16);  // ray queues (origin, direction) x 5
   add(P * 16); add(P * 16);                 // hit_bsdf, hit_gi
   for (int i = 0; i < 5; ++i) add(P);       // visibility
-  for (int i = 0; i < 4; ++i) add(P * 16);  // stage state
+  for (int i = 0; i < 5; ++i) add(P * 16);  // stage state
   add(64 * 4);                              // counters
   add(3 * K_NUM_KINDS * 8);                 // visit counters
   add(P * 12);                              // out rgb
@@ -2155,6 +2505,7 @@ void frame_buffers_carve(void* base, uint32_t W, uint32_t H, FrameBuffers* fb) {
   fb->st_b = carve<uint4>(p, P);
   fb->st_c = carve<uint4>(p, P);
   fb->st_d = carve<uint4>(p, P);
+  fb->st_e = carve<uint4>(p, P);
   fb->counters = carve<uint32_t>(p, 64);
   fb->visits = carve<unsigned long long>(p, 3 * K_NUM_KINDS);
   fb->atr_nd = reinterpret_cast<uint2*>(fb->rq_o[0]);
@@ -2206,6 +2557,15 @@ void trace_shadow_pair(bool counting, int blocks, cudaStream_t st, const DevScen
                        uint32_t cap) {
   if (counting) k_trace_pair<Q_RIS_SHADOW, Q_GI_SHADOW, true><<<blocks, kBlock, 0, st>>>(scene, fb, cap);
   else k_trace_pair<Q_RIS_SHADOW, Q_GI_SHADOW, false><<<blocks, kBlock, 0, st>>>(scene, fb, cap);
+}
+
+// The two closest-hit candidate queues (BSDF, GI) in one launch.
+void trace_candidate_pair(bool counting, int blocks, cudaStream_t st, const DevScene& scene, const FrameBuffers& fb,
+                          uint32_t cap) {
+  if (counting)
+    k_trace_pair_closest<Q_BSDF_CAND, Q_GI_CAND, true><<<blocks, kBlock, 0, st>>>(scene, fb, cap, fb.hit_bsdf, fb.hit_gi);
+  else
+    k_trace_pair_closest<Q_BSDF_CAND, Q_GI_CAND, false><<<blocks, kBlock, 0, st>>>(scene, fb, cap, fb.hit_bsdf, fb.hit_gi);
 }
 
 int frame_streams_create(FrameStreams* fs) {
@@ -2397,11 +2757,43 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
           }
           for (uint32_t k = 0; k < n; ++k) {
             bool odd = (k % 2) != 0;
-            k_spatial<true><<<g2, b2, 0, st>>>(scene, fb, c, k, n, cfg.gi_spatial_samples, cfg.gi_unbiased,
-                                               odd ? fb.gi_a : fb.gi_inter_a, odd ? fb.gi_b : fb.gi_inter_b,
-                                               odd ? fb.gi_inter_a : fb.gi_a, odd ? fb.gi_inter_b : fb.gi_b, pout_a,
-                                               pout_b);
-            mark(K_GI_SPATIAL);
+            const uint4* in_a = odd ? fb.gi_a : fb.gi_inter_a;
+            const uint4* in_b = odd ? fb.gi_b : fb.gi_inter_b;
+            uint4* out_a = odd ? fb.gi_inter_a : fb.gi_a;
+            uint4* out_b = odd ? fb.gi_inter_b : fb.gi_b;
+            if (!cfg.gi_unbiased) {
+              k_spatial<true><<<g2, b2, 0, st>>>(scene, fb, c, k, n, cfg.gi_spatial_samples, 0u, in_a, in_b, out_a,
+                                                 out_b, pout_a, pout_b);
+              mark(K_GI_SPATIAL);
+              continue;
+            }
+            // unbiased: wavefront stages, the targets' re-traces through the queues
+            const uint32_t ns = cfg.gi_spatial_samples;
+            for (uint32_t j = 0; j <= ns; ++j) {
+              cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+              mark(K_MEMSET);
+              k_gsp_a<<<g2, b2, 0, st>>>(scene, fb, c, k, n, ns, j, in_a, in_b, out_a, out_b, pout_a, pout_b);
+              mark(K_GI_SPATIAL);
+              if (j == ns) break;
+              trace_queue<false>(counting, persistent_blocks, st, scene, fb, Q_GI_CAND, P, fb.hit_gi, nullptr);
+              mark(K_TRACE_CLOSEST);
+              k_gsp_b<<<g2, b2, 0, st>>>(scene, fb, c, in_a, in_b);
+              mark(K_GI_SPATIAL);
+              trace_queue<true>(counting, persistent_blocks, st, scene, fb, Q_GI_SHADOW, P, nullptr, fb.vis[Q_GI_SHADOW]);
+              mark(K_TRACE_ANY);
+              cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+              mark(K_MEMSET);
+              k_gsp_c<<<g2, b2, 0, st>>>(scene, fb, c, k, n, in_a, in_b, out_a, out_b);
+              mark(K_GI_SPATIAL);
+              trace_candidate_pair(counting, persistent_blocks, st, scene, fb, P);
+              mark(K_TRACE_CLOSEST);
+              cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+              mark(K_MEMSET);
+              k_gsp_d<<<g2, b2, 0, st>>>(scene, fb, c, out_a, out_b);
+              mark(K_GI_SPATIAL);
+              trace_shadow_pair(counting, persistent_blocks, st, scene, fb, P);
+              mark(K_TRACE_ANY);
+            }
           }
           if (n > 0 && n % 2 == 0) {
             cudaMemcpyAsync(fb.gi_a, fb.gi_inter_a, (size_t)P * 16, cudaMemcpyDeviceToDevice, st);

@@ -53,7 +53,7 @@ struct FrameBuffers {
   uint4* hit_bsdf;     // closest hit of the NEE BSDF candidate ray, per path
   uint4* hit_gi;       // closest hit of the GI candidate ray, per path
   uint8_t* vis[5];     // any-hit queues: 1 = unoccluded, per path
-  uint4 *st_a, *st_b, *st_c, *st_d;  // per-path state between shading stages
+  uint4 *st_a, *st_b, *st_c, *st_d, *st_e;  // per-path state between shading stages
   uint32_t* counters;  // [0..1] path queue sizes, [2] extend cursor, [3] rays traced,
                        // [4..8] ray queue sizes, [9..13] ray queue cursors
   unsigned long long* visits;  // instrumented traversal: per kernel kind {rays, nodes, tris}
