@@ -68,7 +68,7 @@ struct DeviceScene {
 struct DeviceTwoLevel {
   void *nodes = nullptr, *tris = nullptr, *tlas_nodes = nullptr, *tlas_leaves = nullptr, *insts = nullptr;
   void *positions = nullptr, *normals = nullptr, *indices = nullptr, *tri_mat = nullptr, *model_tri0 = nullptr,
-       *env = nullptr;
+       *tri_inst = nullptr, *env = nullptr;
   DevScene view{};  // nodes / tris: the BLAS pool; env: the base scene's environment
   TwoLevel tl{};
   ModelGeo mg{};
@@ -77,7 +77,7 @@ struct DeviceTwoLevel {
   bool valid = false;
   void release() {
     void** all[] = {&nodes, &tris, &tlas_nodes, &tlas_leaves, &insts, &positions, &normals, &indices, &tri_mat,
-                    &model_tri0, &env};
+                    &model_tri0, &tri_inst, &env};
     for (void** p : all) {
       if (*p) cudaFree(*p);
       *p = nullptr;
@@ -588,6 +588,7 @@ int two_level_sync(Handle* h, const TwoLevel** out) {
       (rc = put(&t.indices, host.indices.data(), sizeof(uint32_t) * host.indices.size(), "model indices")) ||
       (rc = put(&t.tri_mat, host.tri_material.data(), sizeof(uint32_t) * host.tri_material.size(), "model materials")) ||
       (rc = put(&t.model_tri0, host.model_tri0.data(), sizeof(uint32_t) * host.model_tri0.size(), "model table")) ||
+      (rc = put(&t.tri_inst, host.tri_inst.data(), sizeof(uint32_t) * host.tri_inst.size(), "triangle instances")) ||
       (rc = put(&t.env, h->world.base.env.data(), sizeof(float) * h->world.base.env.size(), "environment"))) {
     t.release();
     return rc;
@@ -603,6 +604,7 @@ int two_level_sync(Handle* h, const TwoLevel** out) {
   t.mg.indices = static_cast<const uint32_t*>(t.indices);
   t.mg.tri_mat = static_cast<const uint32_t*>(t.tri_mat);
   t.mg.model_tri0 = static_cast<const uint32_t*>(t.model_tri0);
+  t.mg.tri_inst = static_cast<const uint32_t*>(t.tri_inst);
   t.materials = host.materials;
   t.tl.tlas_nodes = static_cast<const uint4*>(t.tlas_nodes);
   t.tl.tlas_leaves = static_cast<const float4*>(t.tlas_leaves);

@@ -94,13 +94,7 @@ struct GpuGeo {
     return v.mats[in.material_idx + s.tri_material[in.first_index / 3 + (g - in.first_global_tri)]];
   }
   APD const spec::Material& fetch2(uint32_t g, spec::TriGeo* tg) const {
-    uint32_t lo = 0, hi = v.tl.num_insts;
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (v.tl.insts[mid].tri_base <= g) lo = mid;
-      else hi = mid;
-    }
-    const InstRec& in = v.tl.insts[lo];
+    const InstRec& in = v.tl.insts[__ldg(&v.mg.tri_inst[g])];
     const uint32_t t = __ldg(&v.mg.model_tri0[in.model]) + (g - in.tri_base);
     const float* m = in.o2w;
     for (int k = 0; k < 3; ++k) {

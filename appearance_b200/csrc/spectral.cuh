@@ -17,13 +17,15 @@ namespace ap {
 // illuminant upsampling table.
 // The models of a two-level world, for shading (World::build_two_level):
 // model-space vertices (x, y, z, 0) and normals (3 floats), per model
-// triangle its vertex indices and its material, each model's first triangle.
+// triangle its vertex indices and its material, each model's first triangle,
+// and per global triangle id its instance.
 struct ModelGeo {
   const float4* positions;
   const float* normals;
   const uint32_t* indices;
   const uint32_t* tri_mat;
   const uint32_t* model_tri0;
+  const uint32_t* tri_inst;
 };
 
 struct SpectralView {

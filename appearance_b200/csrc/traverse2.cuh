@@ -102,57 +102,37 @@ APD void visit_node2(const uint4* nodes, Trav& t, uint2* stack, uint32_t* leaf_b
 }
 
 // Runs up to `budget` steps (a node of either level, one triangle, or one
-// instance entry); returns true when the ray is finished.
+// instance entry); returns true when the ray is finished.  Both levels' node
+// visits go through one call site (the level picks the node array and where
+// the leaf mask goes), so lanes of a warp at different levels share it.
 template <bool kAny, bool kCount>
 APD bool trav2_step(const DevScene& s, const TwoLevel& tl, Trav2& q, uint2* stack, int budget, Visits* vc) {
   Trav& t = q.t;
   for (int step = 0; step < budget; ++step) {
-    if (q.blas) {
-      if (t.tri_mask) {
-        const int j = __ffs(t.tri_mask) - 1;
-        t.tri_mask &= t.tri_mask - 1;
-        if (kCount) vc->tris++;
-        const float4* tp = s.tris + 3 * (size_t)(t.tri_base + j);
-        const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
-        float th, u, v;
-        const float lim = kAny ? t.tmax : t.hit.t;
-        if (intersect_tri(t.r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), 0.0f, lim, th, u, v)) {
-          const uint32_t gid = q.tri_base_id + __float_as_uint(a.w);
-          if (kAny) {
-            t.hit.tri = gid;
-            return true;
-          }
-          if (th < t.hit.t || gid < t.hit.tri) {
-            t.hit.t = th;
-            t.hit.u = u;
-            t.hit.v = v;
-            t.hit.tri = gid;
-          }
+    if (q.blas && t.tri_mask) {
+      const int j = __ffs(t.tri_mask) - 1;
+      t.tri_mask &= t.tri_mask - 1;
+      if (kCount) vc->tris++;
+      const float4* tp = s.tris + 3 * (size_t)(t.tri_base + j);
+      const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+      float th, u, v;
+      const float lim = kAny ? t.tmax : t.hit.t;
+      if (intersect_tri(t.r, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), 0.0f, lim, th, u, v)) {
+        const uint32_t gid = q.tri_base_id + __float_as_uint(a.w);
+        if (kAny) {
+          t.hit.tri = gid;
+          return true;
         }
-        continue;
-      }
-      if (t.have && !kAny && t.node_t > t.hit.t * kGrow) t.have = false;
-      if (!t.have) {
-        bool got = false;
-        while (t.sp > q.sp0) {
-          const uint2 e = stack[--t.sp];
-          if (kAny || __uint_as_float(e.y) <= t.hit.t * kGrow) {
-            t.node = e.x;
-            got = true;
-            break;
-          }
-        }
-        if (!got) {  // this instance is done: back to the world-space ray
-          q.blas = false;
-          t.r = ray_pre(q.wo, q.wd);
-          continue;
+        if (th < t.hit.t || gid < t.hit.tri) {
+          t.hit.t = th;
+          t.hit.u = u;
+          t.hit.v = v;
+          t.hit.tri = gid;
         }
       }
-      if (kCount) vc->nodes++;
-      visit_node2<kAny>(s.nodes, t, stack, &t.tri_base, &t.tri_mask);
       continue;
     }
-    if (q.inst_mask) {  // enter the next pending instance
+    if (!q.blas && q.inst_mask) {  // enter the next pending instance
       const int j = __ffs(q.inst_mask) - 1;
       q.inst_mask &= q.inst_mask - 1;
       const uint32_t ii = __float_as_uint(__ldg(tl.tlas_leaves + 3 * (size_t)(q.inst_base + j)).w);
@@ -171,10 +151,12 @@ APD bool trav2_step(const DevScene& s, const TwoLevel& tl, Trav2& q, uint2* stac
       t.tri_mask = 0;
       continue;
     }
+    // a node of the current level
     if (t.have && !kAny && t.node_t > t.hit.t * kGrow) t.have = false;
     if (!t.have) {
+      const int floor = q.blas ? q.sp0 : 0;
       bool got = false;
-      while (t.sp > 0) {
+      while (t.sp > floor) {
         const uint2 e = stack[--t.sp];
         if (kAny || __uint_as_float(e.y) <= t.hit.t * kGrow) {
           t.node = e.x;
@@ -182,10 +164,23 @@ APD bool trav2_step(const DevScene& s, const TwoLevel& tl, Trav2& q, uint2* stac
           break;
         }
       }
-      if (!got) return true;
+      if (!got) {
+        if (!q.blas) return true;
+        q.blas = false;  // this instance is done: back to the world-space ray
+        t.r = ray_pre(q.wo, q.wd);
+        continue;
+      }
     }
     if (kCount) vc->nodes++;
-    visit_node2<kAny>(tl.tlas_nodes, t, stack, &q.inst_base, &q.inst_mask);
+    uint32_t base, mask;
+    visit_node2<kAny>(q.blas ? s.nodes : tl.tlas_nodes, t, stack, &base, &mask);
+    if (q.blas) {
+      t.tri_base = base;
+      t.tri_mask = mask;
+    } else {
+      q.inst_base = base;
+      q.inst_mask = mask;
+    }
   }
   return false;
 }

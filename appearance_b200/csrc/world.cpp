@@ -306,6 +306,7 @@ bool World::build_two_level(uint32_t max_stack, TwoLevelHost* out, std::string* 
     r.model = k;
     out->insts.push_back(r);
     tri_base += mods[k]->num_tris();
+    out->tri_inst.resize(tri_base, (uint32_t)i);
     double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
     for (int corner = 0; corner < 8; ++corner) {
       const double p[3] = {box[6 * k + ((corner & 1) ? 3 : 0)], box[6 * k + 1 + ((corner & 2) ? 3 : 0)],

@@ -58,6 +58,8 @@ struct TwoLevelHost {
   std::vector<float> positions4, normals;
   std::vector<uint32_t> indices, tri_material, model_tri0;
   std::vector<ap_material> materials;
+  // per global triangle id, the instance it belongs to
+  std::vector<uint32_t> tri_inst;
 };
 
 // World-to-object rows (row-major 3x4) of a column-major Mat4: its inverse

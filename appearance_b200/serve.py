@@ -182,10 +182,70 @@ def summarise(jobs, results, wall):
                 mean_gpu_ms=statistics.mean(r["gpu_ms"] for r in results))
 
 
+def run_benchmark(n_jobs: int = 200, rates=(200.0,), scene_tris=(100000, 1000000, 2000000, 4000000),
+                  budget_gb: float = 150.0, slots: int = 4, graphs: bool = True, serial: bool = True,
+                  sustained_fraction: float = 0.0, seed: int = 0) -> dict:
+    """The serving benchmark: the same seeded job list submitted at each
+    Poisson rate in `rates` (jobs/s) to a concurrent server, and, with
+    `sustained_fraction` > 0, once more at that fraction of the job rate the
+    server completed at the first rate (a load it sustains, so that latency is
+    the loop's and not queueing); with `serial`, the list at the first rate to
+    a one-job-at-a-time server as well."""
+    import torch  # page-locked result buffers
+    t = time.perf_counter()
+    field = [scenes.icosphere_field(seed=k, num_spheres=max(1, round(n / TRIS_PER_SPHERE)),
+                                    num_emissive=max(1, round(n / TRIS_PER_SPHERE) // 16)) for k, n in enumerate(scene_tris)]
+    paths = [scenes.camera_spline(seed=k, frames=64) for k in range(len(scene_tris))]
+    gen_s = time.perf_counter() - t
+
+    def pinned(j):
+        return torch.empty((j["height"], j["width"], 3), dtype=torch.float32, pin_memory=True).numpy()
+
+    out = dict(workload=dict(jobs=n_jobs, rates=list(rates), scene_tris=[int(f.num_tris) for f in field],
+                             budget_gb=budget_gb, slots=slots, graphs=bool(graphs), depth=8, spp=SPPS,
+                             resolutions=RESOLUTIONS, res_probs=RES_PROBS, scene_gen_s=gen_s))
+    warm = [dict(j, arrival=0.0) for j in serving_jobs(8, 1.0, len(scene_tris), seed=seed + 99)]
+
+    def server(max_inflight, use_graphs):
+        srv = RenderServer(SERVE_CONFIG, hbm_budget=budget_gb * 1e9, max_inflight=max_inflight, use_graphs=use_graphs)
+        for f in field:
+            srv.add_scene(f)
+        run_jobs(srv, warm, paths, realtime=False, pinned=pinned)  # one job per class, untimed
+        return srv
+
+    t = time.perf_counter()
+    srv = server(slots, bool(graphs))
+    out["workload"]["scene_upload_s"] = time.perf_counter() - t
+    runs = []
+    for rate in rates:
+        jobs = serving_jobs(n_jobs, rate, len(scene_tris), seed=seed)
+        res, wall = run_jobs(srv, jobs, paths, realtime=True, pinned=pinned)
+        runs.append(dict(rate=rate, **summarise(jobs, res, wall)))
+    if sustained_fraction > 0:
+        first = runs[0]
+        rate = sustained_fraction * first["jobs"] / first["wall_s"]
+        jobs = serving_jobs(n_jobs, rate, len(scene_tris), seed=seed)
+        res, wall = run_jobs(srv, jobs, paths, realtime=True, pinned=pinned)
+        runs.append(dict(rate=rate, sustained=True, **summarise(jobs, res, wall)))
+    out["server"] = runs
+    out["stats"] = srv.stats()
+    srv.close()
+    if serial:
+        ser = server(1, False)
+        jobs = serving_jobs(n_jobs, rates[0], len(scene_tris), seed=seed)
+        res, wall = run_jobs(ser, jobs, paths, realtime=True, pinned=pinned)
+        out["serial"] = dict(rate=rates[0], **summarise(jobs, res, wall))
+        ser.close()
+        out["throughput_vs_serial"] = runs[0]["msamples_per_s"] / out["serial"]["msamples_per_s"]
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m appearance_b200.serve")
     ap.add_argument("--jobs", type=int, default=200)
     ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate (jobs/s)")
+    ap.add_argument("--sustained", type=float, default=0.6,
+                    help="also run at this fraction of the completion rate seen at --rate (0: off)")
     ap.add_argument("--scene-tris", default="100000,1000000,2000000,4000000")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--slots", type=int, default=4)
@@ -193,47 +253,8 @@ def main(argv=None):
     ap.add_argument("--serial", type=int, default=1, help="also run the jobs one at a time")
     ap.add_argument("--seed", type=int, default=0)
     a = ap.parse_args(argv)
-    tris = [int(x) for x in a.scene_tris.split(",")]
-    import torch  # page-locked result buffers
-    t = time.perf_counter()
-    field = [scenes.icosphere_field(seed=k, num_spheres=max(1, round(n / TRIS_PER_SPHERE)),
-                                    num_emissive=max(1, round(n / TRIS_PER_SPHERE) // 16)) for k, n in enumerate(tris)]
-    paths = [scenes.camera_spline(seed=k, frames=64) for k in range(len(tris))]
-    gen_s = time.perf_counter() - t
-    jobs = serving_jobs(a.jobs, a.rate, len(tris), seed=a.seed)
-    pool = {}
-
-    def pinned(j):
-        key = (j["width"], j["height"])
-        lst = pool.setdefault(key, [])
-        buf = torch.empty((j["height"], j["width"], 3), dtype=torch.float32, pin_memory=True)
-        lst.append(buf)
-        return buf.numpy()
-
-    out = dict(workload=dict(jobs=a.jobs, rate=a.rate, scene_tris=[int(f.num_tris) for f in field], budget_gb=a.budget_gb,
-                             slots=a.slots, graphs=bool(a.graphs), depth=8, spp=SPPS, resolutions=RESOLUTIONS,
-                             res_probs=RES_PROBS, scene_gen_s=gen_s))
-    srv = RenderServer(SERVE_CONFIG, hbm_budget=a.budget_gb * 1e9, max_inflight=a.slots, use_graphs=bool(a.graphs))
-    t = time.perf_counter()
-    for f in field:
-        srv.add_scene(f)
-    out["workload"]["scene_upload_s"] = time.perf_counter() - t
-    # warm-up: one job per (resolution, spp) class, not timed
-    warm = [dict(j, arrival=0.0) for j in serving_jobs(8, 1.0, len(tris), seed=a.seed + 99)]
-    run_jobs(srv, warm, paths, realtime=False, pinned=pinned)
-    res, wall = run_jobs(srv, jobs, paths, realtime=True, pinned=pinned)
-    out["server"] = summarise(jobs, res, wall)
-    out["server"]["stats"] = srv.stats()
-    srv.close()
-    if a.serial:
-        ser = RenderServer(SERVE_CONFIG, hbm_budget=a.budget_gb * 1e9, max_inflight=1, use_graphs=False)
-        for f in field:
-            ser.add_scene(f)
-        run_jobs(ser, warm, paths, realtime=False, pinned=pinned)
-        res, wall = run_jobs(ser, jobs, paths, realtime=True, pinned=pinned)
-        out["serial"] = summarise(jobs, res, wall)
-        ser.close()
-        out["throughput_vs_serial"] = out["server"]["msamples_per_s"] / out["serial"]["msamples_per_s"]
+    out = run_benchmark(a.jobs, (a.rate,), [int(x) for x in a.scene_tris.split(",")], a.budget_gb, a.slots,
+                        bool(a.graphs), bool(a.serial), a.sustained, a.seed)
     print(json.dumps(out), flush=True)
 
 

@@ -289,7 +289,8 @@ def main():
         if world == 1:  # the other configurations are single-GPU cases, measured on one GPU only
             cpu = bool(args.cpu_baseline)
             line["configs"] = {"cornell_512_16spp_depth5": cornell_config(cpu),
-                               "city_spectral_4096_64spp_depth16": city_spectral_config(cpu)}
+                               "city_spectral_4096_64spp_depth16": city_spectral_config(cpu),
+                               "serving_mixed_jobs": serving_config()}
         print(json.dumps(line), flush=True)
     pt.close()
     if world > 1:
@@ -331,6 +332,25 @@ def cornell_config(cpu: bool) -> dict:
                                "cores": os.cpu_count(), "kind": "port",
                                "sample": f"oracle, same scene and estimator at {cw}x{ch}, 16 spp, depth 5, 1 frame"}
     return out
+
+
+def serving_config() -> dict:
+    """The render-serving loop (ap_server_*): 96 seeded jobs of mixed
+    resolution (256^2 .. 1920x1080), spp (1 .. 64) and scene (resident
+    icosphere fields of 0.1M, 1M, 2M and 4M triangles), Poisson arrivals at
+    200 jobs/s (far above what one GPU completes: latency there is queueing),
+    then the same list at 60 % of the completion rate seen there (a load the
+    server sustains: latency is the loop's), and the 200 jobs/s list on a
+    one-job-at-a-time server.  Latency is submit -> result in host memory."""
+    from appearance_b200 import serve
+    r = serve.run_benchmark(n_jobs=96, rates=(200.0,), sustained_fraction=0.6, serial=True)
+    over, sus = r["server"][0], r["server"][1]
+    keep = ("rate", "jobs", "p50_ms", "p99_ms", "mean_ms", "msamples_per_s", "wall_s", "mean_queued_ms", "mean_gpu_ms")
+    return {"workload": "96 mixed jobs (4 resident scenes 0.1M-4M triangles, 256^2-1080p, 1-64 spp, depth 8)",
+            "unit": "Msamples/s", "value": over["msamples_per_s"],
+            "overload": {k: over[k] for k in keep}, "sustained": {k: sus[k] for k in keep},
+            "serial": {k: r["serial"][k] for k in keep}, "throughput_vs_serial": r["throughput_vs_serial"],
+            "server_stats": r["stats"]}
 
 
 def city_spectral_config(cpu: bool) -> dict:
