@@ -2055,7 +2055,10 @@ __global__ void k_firefly(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t cur,
 // the reference's buffer ping-pong, which the sky pixels of later frames read)
 // it writes the a-trous passes' records: oct30 normal + depth, and packed
 // radiance + variance.
-__global__ void k_svgf_temporal(FrameBuffers fb, Consts c, const uint32_t* demod, uint32_t* out_rad,
+// Register-capped for 6 blocks of 256 per SM: its reprojection gathers are
+// latency-bound, and the extra resident warps hide more of them than the few
+// spilled registers cost.
+__global__ void __launch_bounds__(256, 6) k_svgf_temporal(FrameBuffers fb, Consts c, const uint32_t* demod, uint32_t* out_rad,
                                 const float2* in_mom, float2* out_mom, int write_records) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;

@@ -71,8 +71,9 @@ struct Slot {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float* staging = nullptr;  // pinned, for callers whose output buffer is pageable
   size_t staging_bytes = 0;
-  cudaGraphExec_t exec = nullptr;
-  uint64_t exec_key = 0;
+  // instantiated frame graphs of this slot, one per launch sequence (shape
+  // key); a later job of the same key updates its graph in place
+  std::map<uint64_t, cudaGraphExec_t> execs;
   Job* job = nullptr;
   bool finished = false;  // set by the stream callback
 };
@@ -115,13 +116,14 @@ void CUDART_CB on_slot_done(void* p) {  // runs on a CUDA callback thread: no CU
 }
 
 uint64_t shape_key(const ap_job& j, const FrameConfig& cfg) {
+  // the frame's launch sequence depends on the sample and bounce counts only;
+  // resolution, scene, camera and buffers are node parameters, which an
+  // in-place update may change
+  (void)j;
   uint64_t k = 1469598103934665603ull;
   auto mix = [&](uint64_t v) { k = (k ^ v) * 1099511628211ull; };
-  mix(j.width);
-  mix(j.height);
   mix(cfg.sample_count);
   mix(cfg.max_bounces);
-  mix(j.scene);
   return k;
 }
 
@@ -164,21 +166,21 @@ bool launch_job(Server* s, Job* j, Slot& sl) {
     }
     if (e == cudaSuccess) {
       const uint64_t key = shape_key(d, cfg);
+      cudaGraphExec_t& exec = sl.execs[key];
       cudaGraphExecUpdateResultInfo info;
-      if (sl.exec && sl.exec_key == key && cudaGraphExecUpdate(sl.exec, g, &info) == cudaSuccess) {
+      if (exec && cudaGraphExecUpdate(exec, g, &info) == cudaSuccess) {
         j->graph_mode = 2;
         s->graph_updates++;
       } else {
         cudaGetLastError();  // a failed update leaves a recoverable error
-        if (sl.exec) cudaGraphExecDestroy(sl.exec);
-        sl.exec = nullptr;
-        e = cudaGraphInstantiate(&sl.exec, g, 0);
-        sl.exec_key = key;
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        e = cudaGraphInstantiate(&exec, g, 0);
         j->graph_mode = 1;
         s->graph_instantiations++;
       }
       cudaGraphDestroy(g);
-      if (e == cudaSuccess) e = cudaGraphLaunch(sl.exec, sl.stream);
+      if (e == cudaSuccess) e = cudaGraphLaunch(exec, sl.stream);
     }
   } else {
     encode_frame(*scene, fb, cfg, mats, d.width, d.height, d.seed, s->num_sms, sl.stream, nullptr);
@@ -402,7 +404,9 @@ void ap_server_destroy(void* sp) {
   ap::DeviceScope device_scope(s->device);
   for (Slot& sl : s->slots) {
     if (sl.stream) cudaStreamSynchronize(sl.stream);
-    if (sl.exec) cudaGraphExecDestroy(sl.exec);
+    for (auto& kv : sl.execs)
+      if (kv.second) cudaGraphExecDestroy(kv.second);
+    sl.execs.clear();
     if (sl.staging) cudaFreeHost(sl.staging);
     if (sl.ev0) cudaEventDestroy(sl.ev0);
     if (sl.ev1) cudaEventDestroy(sl.ev1);

@@ -109,14 +109,17 @@ APD bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float t
 // point outside the exact triangle by a few ulp of the vertex distances from
 // the origin.  Each slab is therefore widened by 2^-19 of (|p - o| + node
 // extent)/|d| and each interval by a relative 2^-21, so no child that holds a
-// triangle accepted inside [tmin, tmax] is culled.  For a zero direction
-// component the slab is all of t when the origin lies inside the child's
-// bounds decoded as p + q*s (rounded to nearest, which never shrinks the
-// conservatively quantised box), and empty otherwise.
+// triangle accepted inside [tmin, tmax] is culled.  The widening e is folded
+// into the per-node offsets once, fma(q, s/d, b - e) and fma(q, s/d, b + e)
+// with b = (p - o)/d: the one extra rounding (of b -+ e) is half an ulp of
+// |b| + e, far inside the 2^-19 margin, which is 16 ulp of |b| alone.  For a
+// zero direction component the slab is all of t when the origin lies inside
+// the child's bounds decoded as p + q*s (rounded to nearest, which never
+// shrinks the conservatively quantised box), and empty otherwise.
 struct NodeFrame {
   float px, py, pz, sxs, sys, szs;  // origin and scales of the quantisation grid
-  float ax, ay, az, bx, by, bz;     // slab = fma(q, a, b) per axis
-  float ex, ey, ez;                 // slab widening
+  float ax, ay, az;                 // slab = fma(q, a, b -+ e) per axis
+  float blx, bly, blz, bhx, bhy, bhz;  // b - e (near planes), b + e (far planes)
 };
 
 APD NodeFrame node_frame(const uint4 w0, const RayPre& r) {
@@ -130,13 +133,19 @@ APD NodeFrame node_frame(const uint4 w0, const RayPre& r) {
   f.ax = f.sxs * r.inv.x;
   f.ay = f.sys * r.inv.y;
   f.az = f.szs * r.inv.z;
-  f.bx = (f.px - r.o.x) * r.inv.x;
-  f.by = (f.py - r.o.y) * r.inv.y;
-  f.bz = (f.pz - r.o.z) * r.inv.z;
+  const float bx = (f.px - r.o.x) * r.inv.x;
+  const float by = (f.py - r.o.y) * r.inv.y;
+  const float bz = (f.pz - r.o.z) * r.inv.z;
   const float kSlack = 1.9073486e-06f;  // 2^-19
-  f.ex = (fabsf(f.bx) + 255.0f * fabsf(f.ax)) * kSlack;
-  f.ey = (fabsf(f.by) + 255.0f * fabsf(f.ay)) * kSlack;
-  f.ez = (fabsf(f.bz) + 255.0f * fabsf(f.az)) * kSlack;
+  const float ex = (fabsf(bx) + 255.0f * fabsf(f.ax)) * kSlack;
+  const float ey = (fabsf(by) + 255.0f * fabsf(f.ay)) * kSlack;
+  const float ez = (fabsf(bz) + 255.0f * fabsf(f.az)) * kSlack;
+  f.blx = bx - ex;
+  f.bhx = bx + ex;
+  f.bly = by - ey;
+  f.bhy = by + ey;
+  f.blz = bz - ez;
+  f.bhz = bz + ez;
   return f;
 }
 
@@ -185,13 +194,17 @@ APD float grow_down(float x) { return fmaf(-fabsf(x), kRelGrow, x); }
 
 // Entry distance of child i (a compile-time index after unrolling) or +inf
 // when its box is missed inside [tmin, tmax]; tmax_grown = tmax * kGrow.
+// kZero = false leaves out the zero-direction-component test, for rays
+// without one (the traversal loops pick the form once per node, so the
+// common case carries no per-child check).
+template <bool kZero = true>
 APD float child_entry(const NodeFrame& f, const NodePlanes& pl, const RayPre& r, int i, float tmin,
                       float tmax_grown) {
   const int k = i & 3, h = i >> 2;
-  float lx = fmaf(byte_at(pl.nx[h], k), f.ax, f.bx) - f.ex, hx = fmaf(byte_at(pl.fx[h], k), f.ax, f.bx) + f.ex;
-  float ly = fmaf(byte_at(pl.ny[h], k), f.ay, f.by) - f.ey, hy = fmaf(byte_at(pl.fy[h], k), f.ay, f.by) + f.ey;
-  float lz = fmaf(byte_at(pl.nz[h], k), f.az, f.bz) - f.ez, hz = fmaf(byte_at(pl.fz[h], k), f.az, f.bz) + f.ez;
-  if (r.zero_axes) {
+  float lx = fmaf(byte_at(pl.nx[h], k), f.ax, f.blx), hx = fmaf(byte_at(pl.fx[h], k), f.ax, f.bhx);
+  float ly = fmaf(byte_at(pl.ny[h], k), f.ay, f.bly), hy = fmaf(byte_at(pl.fy[h], k), f.ay, f.bhy);
+  float lz = fmaf(byte_at(pl.nz[h], k), f.az, f.blz), hz = fmaf(byte_at(pl.fz[h], k), f.az, f.bhz);
+  if (kZero && r.zero_axes) {
     const float inf = __uint_as_float(0x7f800000u);
     if (r.zero_axes & 1u) {
       bool in = r.o.x >= f.px + byte_at(pl.nx[h], k) * f.sxs && r.o.x <= f.px + byte_at(pl.fx[h], k) * f.sxs;
@@ -309,11 +322,19 @@ APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits*
     uint32_t tri_mask = 0;
     float best_t = __uint_as_float(0x7f800000u);
     uint32_t best_node = 0;
+    float tns[8];
+    if (t.r.zero_axes) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) tns[i] = child_entry<true>(f, pl, t.r, i, 0.0f, range_grown);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) tns[i] = child_entry<false>(f, pl, t.r, i, 0.0f, range_grown);
+    }
 #pragma unroll(kUnroll ? 8 : 1)
     for (int i = 0; i < 8; ++i) {
       const uint32_t meta = meta_of(w1, i);
       if (meta == 0u) continue;
-      const float tn = child_entry(f, pl, t.r, i, 0.0f, range_grown);
+      const float tn = tns[i];
       if (!(tn < __uint_as_float(0x7f800000u))) continue;
       if (meta & 0xe0u) {
         tri_mask |= (meta >> 5) << (meta & 0x1fu);  // unary count at the leaf's offset
@@ -357,15 +378,16 @@ APD uint32_t inline_children(const uint4 w0, const uint4 w2, const uint4 w3, con
   const float kSlack = 1.9073486e-06f;  // 2^-19
   float ex = (fabsf(bx) + 255.0f * fabsf(ax)) * kSlack, ey = (fabsf(by) + 255.0f * fabsf(ay)) * kSlack,
         ez = (fabsf(bz) + 255.0f * fabsf(az)) * kSlack;
+  const float blx = bx - ex, bhx = bx + ex, bly = by - ey, bhy = by + ey, blz = bz - ez, bhz = bz + ez;
   const NodePlanes pl = node_planes(w2, w3, w4, r.neg_axes);
   const float tmax_grown = tmax * kGrow;
   uint32_t mask = 0;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int k = i & 3, h = i >> 2;
-    float lx = fmaf(byte_at(pl.nx[h], k), ax, bx) - ex, hx = fmaf(byte_at(pl.fx[h], k), ax, bx) + ex;
-    float ly = fmaf(byte_at(pl.ny[h], k), ay, by) - ey, hy = fmaf(byte_at(pl.fy[h], k), ay, by) + ey;
-    float lz = fmaf(byte_at(pl.nz[h], k), az, bz) - ez, hz = fmaf(byte_at(pl.fz[h], k), az, bz) + ez;
+    float lx = fmaf(byte_at(pl.nx[h], k), ax, blx), hx = fmaf(byte_at(pl.fx[h], k), ax, bhx);
+    float ly = fmaf(byte_at(pl.ny[h], k), ay, bly), hy = fmaf(byte_at(pl.fy[h], k), ay, bhy);
+    float lz = fmaf(byte_at(pl.nz[h], k), az, blz), hz = fmaf(byte_at(pl.fz[h], k), az, bhz);
     if (r.zero_axes) {
       const float inf = __uint_as_float(0x7f800000u);
       if (r.zero_axes & 1u) {

@@ -75,11 +75,19 @@ APD void visit_node2(const uint4* nodes, Trav& t, uint2* stack, uint32_t* leaf_b
   float best_t = __uint_as_float(0x7f800000u);
   uint32_t best_node = 0;
   t.have = false;
+  float tns[8];
+  if (t.r.zero_axes) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) tns[i] = child_entry<true>(f, pl, t.r, i, 0.0f, range_grown);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) tns[i] = child_entry<false>(f, pl, t.r, i, 0.0f, range_grown);
+  }
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const uint32_t meta = meta_of(w1, i);
     if (meta == 0u) continue;
-    const float tn = child_entry(f, pl, t.r, i, 0.0f, range_grown);
+    const float tn = tns[i];
     if (!(tn < __uint_as_float(0x7f800000u))) continue;
     if (meta & 0xe0u) {
       mask |= (meta >> 5) << (meta & 0x1fu);

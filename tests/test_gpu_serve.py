@@ -69,6 +69,16 @@ def test_graph_updated_in_place_for_same_shape():
     modes = [srv.wait(srv.submit(sid, 48, 32, 2, 3, k, mats_for(0, k, 48, 32)))[1]["graph_mode"] for k in range(3)]
     assert modes == [1, 2, 2]
     assert srv.stats()["graphs_updated"] == 2
+    # another scene and resolution with the same samples and depth: the same
+    # launch sequence, updated in place, and the image of a graph-less run
+    sid1 = srv.add_scene(small_scene(1))
+    img, info = srv.wait(srv.submit(sid1, 64, 40, 2, 3, 7, mats_for(1, 7, 64, 40)))
+    assert info["graph_mode"] == 2
+    plain = RenderServer(CFG, hbm_budget=8e9, max_inflight=1, use_graphs=False)
+    pid = [plain.add_scene(small_scene(k)) for k in range(2)][1]
+    ref, _ = plain.wait(plain.submit(pid, 64, 40, 2, 3, 7, mats_for(1, 7, 64, 40)))
+    assert same_bits(img, ref)
+    plain.close()
     srv.close()
 
 
