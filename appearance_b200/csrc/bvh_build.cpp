@@ -1,6 +1,10 @@
 // Compressed 8-wide BVH build: binned-SAH binary tree, greedy collapse into
-// 8-wide nodes (largest-area child opened first), 8-bit conservative
-// quantisation of child boxes against a per-node origin and power-of-two scale.
+// 8-wide nodes (largest-area child opened first, down to single binary leaves
+// while a node has free slots: the traversal tests all 8 slots of a node
+// anyway, so a filled slot costs nothing and culls triangles at a finer
+// grain), 8-bit conservative quantisation of child boxes against a per-node
+// origin and power-of-two scale.  A child of at most 3 triangles that is not
+// opened becomes a leaf child.
 #include "bvh_build.h"
 
 #include <algorithm>
@@ -199,7 +203,7 @@ struct Collapser {
         double best = -1.0;
         for (size_t i = 0; i < kids.size(); ++i) {
           const BNode& c = bn[kids[i]];
-          if (c.leaf() || c.ntris <= 3) continue;
+          if (c.leaf()) continue;  // small subtrees split too while slots are free
           double a = c.box.area();
           if (a > best) { best = a; pick = (int)i; }
         }

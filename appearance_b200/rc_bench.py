@@ -108,18 +108,25 @@ def study(name, budget_ms, warm_frames, w=480, h=270):
         out[f"cache_prefix{prefix}_warmup_ms"] = train_ms
         pt.close()
         rc.close()
-    res = {"resolution": [w, h], "budget_ms": budget_ms, "reference": "4096 spp full depth, float64 accumulation"}
+    res = {"resolution": [w, h], "budget_ms": budget_ms, "warm_frames": warm_frames,
+           "reference": "4096 spp full depth, float64 accumulation"}
     e_plain = out["plain"][-1][1]
     res["plain"] = {"relmse_at_budget": e_plain, "frames_ms": out["plain"][-1][0]}
     for prefix in (2, 1):
         cur = out[f"cache_prefix{prefix}"]
         e = cur[-1][1]
         t_plain = time_to(out["plain"], e)
+        warm = out[f"cache_prefix{prefix}_warmup_ms"]
+        # equal total time: the plain curve at the cache's accumulation time
+        # plus its warm-up training
+        e_plain_eq = next((ep for tp, ep in out["plain"] if tp >= cur[-1][0] + warm), out["plain"][-1][1])
         res[f"cache_prefix{prefix}"] = {
-            "relmse_at_budget": e, "warmup_training_ms": out[f"cache_prefix{prefix}_warmup_ms"],
+            "relmse_at_budget": e, "warmup_training_ms": warm,
             "plain_time_to_same_relmse_ms": t_plain,
             "time_ratio_cache_over_plain": (cur[-1][0] / t_plain) if t_plain else None,
-            "relmse_ratio_at_equal_time": e / e_plain}
+            "time_ratio_with_warmup": ((cur[-1][0] + warm) / t_plain) if t_plain else None,
+            "relmse_ratio_at_equal_time": e / e_plain,
+            "relmse_ratio_at_equal_time_with_warmup": e / e_plain_eq}
     return res
 
 

@@ -290,7 +290,8 @@ def main():
             cpu = bool(args.cpu_baseline)
             line["configs"] = {"cornell_512_16spp_depth5": cornell_config(cpu),
                                "city_spectral_4096_64spp_depth16": city_spectral_config(cpu),
-                               "serving_mixed_jobs": serving_config()}
+                               "serving_mixed_jobs": serving_config(),
+                               "radiance_cache_cornell_480x270": radiance_cache_config()}
         print(json.dumps(line), flush=True)
     pt.close()
     if world > 1:
@@ -331,6 +332,21 @@ def cornell_config(cpu: bool) -> dict:
         out["cpu_baseline"] = {"value": cw * ch * cfg["sample_count"] / dt / 1e6, "unit": "Msamples/s",
                                "cores": os.cpu_count(), "kind": "port",
                                "sample": f"oracle, same scene and estimator at {cw}x{ch}, 16 spp, depth 5, 1 frame"}
+    return out
+
+
+def radiance_cache_config() -> dict:
+    """The radiance cache against the plain full-depth tracer (1 spp, depth 8)
+    on the Cornell box at 480x270: both accumulate frames from a fixed camera
+    for 400 ms of device time and are scored by relMSE against a 4096-spp
+    full-depth reference; the cache first trains online for 100 frames, and
+    the ratios with that warm-up included are reported beside those without."""
+    from appearance_b200 import rc_bench
+    r = rc_bench.study("cornell", budget_ms=400.0, warm_frames=100)
+    out = {"workload": "cornell box 480x270, 1 spp frames, depth 8, cache prefix 1 and 2 bounces",
+           "budget_ms": r["budget_ms"], "plain": r["plain"]}
+    for k in ("cache_prefix1", "cache_prefix2"):
+        out[k] = r[k]
     return out
 
 
