@@ -18,6 +18,7 @@ EXPORTS = ["ap_frame_config_default", "ap_create", "ap_destroy", "ap_last_error"
            "ap_device_framebuffer", "ap_trace_rays", "ap_trace_rays_static", "ap_read_buffer", "ap_profile_frame",
            "ap_bvh_stats", "ap_server_create", "ap_server_destroy", "ap_server_last_error", "ap_server_add_scene",
            "ap_server_job_bytes", "ap_server_submit", "ap_server_query", "ap_server_wait", "ap_server_cancel",
+           "ap_server_set_batching",
            "ap_server_stats",
            "ap_rc_create", "ap_rc_destroy", "ap_rc_last_error", "ap_rc_set_params", "ap_rc_get_params", "ap_rc_infer",
            "ap_rc_train", "ap_rc_attach", "ap_rc_wait_selftest", "ap_spectral_setup", "ap_render_spectral", "ap_profile_spectral"]
@@ -57,7 +58,8 @@ class Job(ctypes.Structure):
 
 class JobResult(ctypes.Structure):
     _fields_ = [("queued_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("gpu_ms", ctypes.c_double),
-                ("device_bytes", ctypes.c_uint64), ("graph_mode", U32), ("slot", U32)]
+                ("device_bytes", ctypes.c_uint64), ("graph_mode", U32), ("slot", U32), ("batch", U32),
+                ("pad", U32)]
 
 
 _lib = None
@@ -110,6 +112,7 @@ def load() -> ctypes.CDLL:
     L.ap_server_query.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]
     L.ap_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(JobResult)]
     L.ap_server_cancel.argtypes = [P, ctypes.c_uint64]
+    L.ap_server_set_batching.argtypes = [P, U32]
     L.ap_server_stats.argtypes = [P, P]
     L.ap_rc_create.restype = P
     L.ap_rc_create.argtypes = [ctypes.c_int, P, P, U32, ctypes.POINTER(ctypes.c_int)]

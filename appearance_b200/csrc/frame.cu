@@ -343,6 +343,115 @@ __global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_pair_closest(
       });
 }
 
+// ---- batches of frames: shared traversal launches (serving) -----------------
+
+// Block prologue of a batch traversal kernel: the frames' first ray indices
+// (start[nj] = the batch's ray count) and their BVHs, in shared memory.
+template <class CountOf>
+APD uint32_t batch_setup(const JobTrace* jobs, int nj, CountOf count_of, uint32_t* s_start, BvhView* s_bvh) {
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int j = 0; j < nj; ++j) {
+      s_start[j] = acc;
+      acc += count_of(jobs[j]);
+    }
+    s_start[nj] = acc;
+  }
+  if ((int)threadIdx.x < nj) s_bvh[threadIdx.x] = BvhView{jobs[threadIdx.x].nodes, jobs[threadIdx.x].tris};
+  __syncthreads();
+  return s_start[nj];
+}
+
+// k_extend over a batch: each frame's path queue (all its pixels at bounce 0).
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_extend_batch(const JobTrace* jobs, int nj, uint32_t bounce,
+                                                                          uint32_t qin) {
+  __shared__ uint32_t s_start[kMaxBatch + 1];
+  __shared__ BvhView s_bvh[kMaxBatch];
+  const uint32_t count = batch_setup(
+      jobs, nj, [&](const JobTrace& b) { return bounce == 0 ? b.P : min(b.counters[qin], b.P); }, s_start, s_bvh);
+  if (blockIdx.x == 0 && (int)threadIdx.x < nj)
+    atomicAdd(&jobs[threadIdx.x].counters[3], s_start[threadIdx.x + 1] - s_start[threadIdx.x]);
+  persistent_trace_batch<false>(
+      s_bvh, nj, s_start, count, &jobs[0].counters[2],
+      [&](int j, uint32_t i, float3& o, float3& d, float& tmax) {
+        const JobTrace& b = jobs[j];
+        const uint32_t id = bounce == 0 ? i : b.queue[qin][i];
+        const float4 r = b.rays[id];
+        d = ray_dir(r);
+        o = ray_org(r) + d * 1e-4f;
+        tmax = 1000.0f;
+      },
+      [&](int j, uint32_t i, const Trav& t) {
+        const JobTrace& b = jobs[j];
+        const uint32_t id = bounce == 0 ? i : b.queue[qin][i];
+        b.hits[id] = make_uint4(__float_as_uint(t.hit.t), __float_as_uint(t.hit.u), __float_as_uint(t.hit.v), t.hit.tri);
+      });
+}
+
+// k_trace_queue over a batch: queue q of every frame (closest hits of the
+// candidate queues to hit_bsdf / hit_gi, visibility of the shadow queues).
+template <bool kAny>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_queue_batch(const JobTrace* jobs, int nj, int q) {
+  __shared__ uint32_t s_start[kMaxBatch + 1];
+  __shared__ BvhView s_bvh[kMaxBatch];
+  const uint32_t count = batch_setup(
+      jobs, nj, [&](const JobTrace& b) { return min(b.counters[kCounterQueueSize + q], b.P); }, s_start, s_bvh);
+  if (blockIdx.x == 0 && (int)threadIdx.x < nj)
+    atomicAdd(&jobs[threadIdx.x].counters[3], s_start[threadIdx.x + 1] - s_start[threadIdx.x]);
+  persistent_trace_batch<kAny>(
+      s_bvh, nj, s_start, count, &jobs[0].counters[kCounterQueueCursor + q],
+      [&](int j, uint32_t i, float3& o, float3& d, float& tmax) {
+        const float4 a = jobs[j].rq_o[q][i], b = jobs[j].rq_d[q][i];
+        o = f3(a.x, a.y, a.z);
+        d = f3(b.x, b.y, b.z);
+        tmax = a.w;
+      },
+      [&](int j, uint32_t i, const Trav& t) {
+        const JobTrace& b = jobs[j];
+        const uint32_t owner = __float_as_uint(b.rq_d[q][i].w);
+        if (kAny) {
+          b.vis[q][owner] = t.hit.tri != kNoHit ? 0 : 1;
+        } else {
+          (q == Q_BSDF_CAND ? b.hit_bsdf : b.hit_gi)[owner] =
+              make_uint4(__float_as_uint(t.hit.t), __float_as_uint(t.hit.u), __float_as_uint(t.hit.v), t.hit.tri);
+        }
+      });
+}
+
+// k_trace_pair over a batch: the any-hit queues Q0 and Q1 of every frame.
+template <int Q0, int Q1>
+__global__ void __launch_bounds__(kBlock, kTraceMinBlocks) k_trace_pair_batch(const JobTrace* jobs, int nj) {
+  __shared__ uint32_t s_start[kMaxBatch + 1];
+  __shared__ BvhView s_bvh[kMaxBatch];
+  const uint32_t count = batch_setup(
+      jobs, nj,
+      [&](const JobTrace& b) {
+        return min(b.counters[kCounterQueueSize + Q0], b.P) + min(b.counters[kCounterQueueSize + Q1], b.P);
+      },
+      s_start, s_bvh);
+  if (blockIdx.x == 0 && (int)threadIdx.x < nj)
+    atomicAdd(&jobs[threadIdx.x].counters[3], s_start[threadIdx.x + 1] - s_start[threadIdx.x]);
+  persistent_trace_batch<true>(
+      s_bvh, nj, s_start, count, &jobs[0].counters[kCounterQueueCursor + Q0],
+      [&](int j, uint32_t i, float3& o, float3& d, float& tmax) {
+        const JobTrace& b = jobs[j];
+        const uint32_t n0 = min(b.counters[kCounterQueueSize + Q0], b.P);
+        const bool first = i < n0;
+        const float4 a = (first ? b.rq_o[Q0] : b.rq_o[Q1])[first ? i : i - n0];
+        const float4 e = (first ? b.rq_d[Q0] : b.rq_d[Q1])[first ? i : i - n0];
+        o = f3(a.x, a.y, a.z);
+        d = f3(e.x, e.y, e.z);
+        tmax = a.w;
+      },
+      [&](int j, uint32_t i, const Trav& t) {
+        const JobTrace& b = jobs[j];
+        const uint32_t n0 = min(b.counters[kCounterQueueSize + Q0], b.P);
+        const bool first = i < n0;
+        const uint32_t owner = __float_as_uint((first ? b.rq_d[Q0] : b.rq_d[Q1])[first ? i : i - n0].w);
+        (first ? b.vis[Q0] : b.vis[Q1])[owner] = t.hit.tri != kNoHit ? 0 : 1;
+      });
+}
+
 // ---- trace.wgsl:62-262 as four stages around the secondary rays -------------
 //   A: hit attributes, emission, G-buffer, first NEE candidates (area + BSDF);
 //      queues the BSDF candidate ray            (Nee::sample_ris, nee.wgsl:131-197)
@@ -2915,6 +3024,124 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
   mark(K_DEMODULATE);
   k_resolve<<<lb, 256, 0, st>>>(fb, P, (float)cfg.sample_count);
   mark(K_RESOLVE);
+  return launches;
+}
+
+JobTrace job_trace(const DevScene& scene, const FrameBuffers& fb, uint32_t P) {
+  JobTrace j{};
+  j.nodes = scene.nodes;
+  j.tris = scene.tris;
+  j.rays = fb.rays;
+  j.hits = fb.hits;
+  j.queue[0] = fb.queue[0];
+  j.queue[1] = fb.queue[1];
+  j.counters = fb.counters;
+  for (int q = 0; q < 5; ++q) {
+    j.rq_o[q] = fb.rq_o[q];
+    j.rq_d[q] = fb.rq_d[q];
+    j.vis[q] = fb.vis[q];
+  }
+  j.hit_bsdf = fb.hit_bsdf;
+  j.hit_gi = fb.hit_gi;
+  j.P = P;
+  return j;
+}
+
+bool batchable(const FrameConfig& cfg) {
+  return !cfg.restir_di && !cfg.restir_gi && !cfg.svgf && !cfg.taa && !cfg.firefly_filter;
+}
+
+// The plain-estimator launch sequence of encode_frame (same kernels, same
+// order per frame), with the traversal stages shared by the batch.
+int encode_batch_plain(const BatchFrame* fr, int nj, const FrameConfig& cfg, const JobTrace* d_jobs, int num_sms,
+                       cudaStream_t st) {
+  if (nj < 1 || nj > kMaxBatch || !batchable(cfg)) return -1;
+  int launches = 0;
+  const int persistent_blocks = num_sms * kTraceMinBlocks;
+  Consts cs[kMaxBatch];
+  int linear[kMaxBatch];
+  for (int j = 0; j < nj; ++j) {
+    const uint32_t P = fr[j].W * fr[j].H;
+    Consts& c = cs[j];
+    c = Consts{};
+    c.W = fr[j].W;
+    c.H = fr[j].H;
+    c.P = P;
+    c.frame_idx = fr[j].frame_idx;
+    c.sample = 0;
+    c.cfg = cfg;
+    linear[j] = (int)std::min<uint32_t>((P + kBlock - 1) / kBlock, (uint32_t)num_sms * 16u);
+    cudaMemsetAsync(fr[j].fb.radiance, 0, (size_t)P * 4, st);
+    cudaMemsetAsync(fr[j].fb.counters + 3, 0, 4, st);
+  }
+  auto each = [&](auto&& f) {
+    for (int j = 0; j < nj; ++j) f(j, fr[j].scene, fr[j].fb, cs[j]);
+  };
+  for (uint32_t sample = 0; sample < cfg.sample_count; ++sample) {
+    each([&](int j, const DevScene&, const FrameBuffers& fb, Consts& c) {
+      c.seed = c.frame_idx * cfg.sample_count + sample;
+      c.sample = sample;
+      dim3 b2(16, 16), g2((c.W + 15) / 16, (c.H + 15) / 16);
+      k_raygen<<<g2, b2, 0, st>>>(fb, c.W, c.H, fr[j].mats);
+      ++launches;
+    });
+    for (uint32_t i = 0; i < cfg.max_bounces; ++i) {
+      each([&](int, const DevScene&, const FrameBuffers& fb, Consts& c) {
+        c.bounce = i;
+        c.qin = i & 1u;
+        c.qout = (i + 1) & 1u;
+        cudaMemsetAsync(fb.counters + 2, 0, 4, st);
+      });
+      k_extend_batch<<<persistent_blocks, kBlock, 0, st>>>(d_jobs, nj, i, i & 1u);
+      ++launches;
+      each([&](int j, const DevScene& s, const FrameBuffers& fb, Consts& c) {
+        cudaMemsetAsync(fb.counters + kCounterQueueSize, 0, 10 * sizeof(uint32_t), st);
+        k_shade_a<<<linear[j], kBlock, 0, st>>>(s, fb, c, fr[j].mats);
+        ++launches;
+      });
+      k_trace_queue_batch<false><<<persistent_blocks, kBlock, 0, st>>>(d_jobs, nj, Q_BSDF_CAND);
+      ++launches;
+      each([&](int j, const DevScene& s, const FrameBuffers& fb, Consts& c) {
+        k_shade_b<<<linear[j], kBlock, 0, st>>>(s, fb, c);
+        k_shade_b2<<<linear[j], kBlock, 0, st>>>(s, fb, c);
+        launches += 2;
+      });
+      k_trace_queue_batch<false><<<persistent_blocks, kBlock, 0, st>>>(d_jobs, nj, Q_GI_CAND);
+      ++launches;
+      each([&](int j, const DevScene& s, const FrameBuffers& fb, Consts& c) {
+        k_shade_c<<<linear[j], kBlock, 0, st>>>(s, fb, c);
+        ++launches;
+      });
+      k_trace_pair_batch<Q_RIS_SHADOW, Q_GI_SHADOW><<<persistent_blocks, kBlock, 0, st>>>(d_jobs, nj);
+      ++launches;
+      each([&](int j, const DevScene& s, const FrameBuffers& fb, Consts& c) {
+        k_shade_d<<<linear[j], kBlock, 0, st>>>(fb, c);
+        k_apply_di_a<<<linear[j], kBlock, 0, st>>>(s, fb, c);
+        launches += 2;
+      });
+      k_trace_queue_batch<true><<<persistent_blocks, kBlock, 0, st>>>(d_jobs, nj, Q_DI_SHADOW);
+      ++launches;
+      each([&](int j, const DevScene& s, const FrameBuffers& fb, Consts& c) {
+        k_apply_di_b<<<linear[j], kBlock, 0, st>>>(fb, c);
+        ++launches;
+        if (i + 1 < cfg.max_bounces) {
+          cudaMemsetAsync(fb.counters + c.qout, 0, 4, st);
+          k_apply_gi<<<linear[j], kBlock, 0, st>>>(s, fb, c);
+          ++launches;
+        }
+      });
+    }
+  }
+  // demodulate -> remodulate -> resolve (no filter passes in the plain estimator)
+  each([&](int, const DevScene&, const FrameBuffers& fb, Consts& c) {
+    const uint32_t cur = c.frame_idx & 1u;
+    const int lb = (int)((c.P + 255) / 256);
+    uint32_t* dcur = fb.demod[cur];
+    k_demodulate<<<lb, 256, 0, st>>>(fb, c.P, cur, fb.radiance, dcur, 0);
+    k_demodulate<<<lb, 256, 0, st>>>(fb, c.P, cur, dcur, fb.radiance, 1);
+    k_resolve<<<lb, 256, 0, st>>>(fb, c.P, (float)cfg.sample_count);
+    launches += 3;
+  });
   return launches;
 }
 

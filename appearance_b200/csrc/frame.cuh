@@ -155,6 +155,50 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
                  uint32_t W, uint32_t H, uint32_t frame_idx, int num_sms, cudaStream_t stream,
                  FrameProfiler* prof = nullptr, const RcFrame* rc = nullptr, const FrameStreams* fs = nullptr);
 
+// ---- batches of frames sharing their traversal launches (serving) ----------
+//
+// Frames of the plain estimator (no reuse passes, denoising or radiance cache)
+// with the same sample and bounce counts have the same launch sequence; a
+// batch of up to kMaxBatch of them, each with its own scene, size, camera,
+// seed and frame state, runs as one sequence: the shading stages launch per
+// frame, and every traversal stage is one persistent launch over all the
+// frames' ray queues, each ray traced through its own frame's BVH.  A frame's
+// result is the one it has alone (its rays, random streams and queues are its
+// own; only which lane traces a ray changes).
+constexpr int kMaxBatch = 8;
+
+// What the batch traversal kernels read and write of one frame (a device
+// array of these is the kernels' argument).
+struct JobTrace {
+  const uint4* nodes;
+  const float4* tris;
+  const float4* rays;
+  uint4* hits;
+  const uint32_t* queue[2];
+  uint32_t* counters;
+  const float4* rq_o[5];
+  const float4* rq_d[5];
+  uint4* hit_bsdf;
+  uint4* hit_gi;
+  uint8_t* vis[5];
+  uint32_t P;
+};
+
+struct BatchFrame {
+  DevScene scene;
+  FrameBuffers fb;
+  Mats mats;
+  uint32_t W, H, frame_idx;
+};
+
+JobTrace job_trace(const DevScene& scene, const FrameBuffers& fb, uint32_t P);
+// Whether frames of `cfg` can share launches (the plain estimator).
+bool batchable(const FrameConfig& cfg);
+// Encodes the batch frames[0..nj) on `stream`; d_jobs holds job_trace() of
+// each frame, in the same order, in device memory.  Returns the kernels launched.
+int encode_batch_plain(const BatchFrame* frames, int nj, const FrameConfig& cfg, const JobTrace* d_jobs, int num_sms,
+                       cudaStream_t stream);
+
 // Closest / any hit for a batch of rays (parity tests and traversal bench).
 // rays: origin.xyz + tmax (float4), dirs: float4; out: t, u, v, tri bits.
 // The display resolve (resolve.wgsl:40-59): ACES-fit tonemap of radiance /

@@ -68,4 +68,53 @@ APD void persistent_trace(const DevScene& s, uint32_t count, uint32_t* cursor, L
   }
 }
 
+// persistent_trace over the rays of several independent jobs at once (a
+// batch of frames sharing one launch): the combined index range is split by
+// the jobs' first indices start[0..nj] (start[nj] = count); a lane that takes
+// ray i traces it through its own job's BVH.  load(job, i, o, d, tmax) and
+// store(job, i, trav) get the job and the ray's index within it.
+template <bool kAny, class Load, class Store>
+APD void persistent_trace_batch(const BvhView* bvh, int nj, const uint32_t* start, uint32_t count, uint32_t* cursor,
+                                Load load, Store store) {
+  const uint32_t lane = lane_id();
+  uint2 stack[kTraversalStack];
+  Trav t;
+  Visits vc;
+  BvhView view{nullptr, nullptr};
+  uint32_t cur = 0;
+  int job = 0;
+  bool active = false, exhausted = false;
+  while (true) {
+    if (!exhausted) {
+      const unsigned need = __ballot_sync(0xffffffffu, !active);
+      if (need) {
+        const int leader = __ffs(need) - 1;
+        uint32_t base = 0;
+        if ((int)lane == leader) base = atomicAdd(cursor, (uint32_t)__popc(need));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (base + (uint32_t)__popc(need) >= count) exhausted = true;
+        if (!active) {
+          const uint32_t idx = base + __popc(need & ((1u << lane) - 1u));
+          if (idx < count) {
+            job = 0;
+            while (job + 1 < nj && idx >= start[job + 1]) ++job;
+            cur = idx - start[job];
+            view = bvh[job];
+            float3 o, d;
+            float tmax;
+            load(job, cur, o, d, tmax);
+            trav_init(t, o, d, tmax);
+            active = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    if (active && trav_step<kAny, false, true>(view, t, stack, kStepBudget, &vc)) {
+      store(job, cur, t);
+      active = false;
+    }
+  }
+}
+
 }  // namespace ap

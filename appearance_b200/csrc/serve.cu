@@ -13,9 +13,13 @@
 // encode_frame as ap_render_*) on the slot's stream, optionally as a CUDA graph
 // captured once per job shape and updated in place for later jobs.  Jobs in
 // flight overlap on the device; a host callback on each stream wakes the
-// dispatcher when a job's result has reached host memory.  A job's result is
-// a function of its own inputs only (its seed, camera, scene and sizes), so it
-// is the same alone and in any mix.
+// dispatcher when a job's result has reached host memory.  With a plain
+// estimator configuration, jobs waiting with the same sample and bounce
+// counts are admitted together as one batch of up to kMaxBatch frames: the
+// batch runs as one launch sequence (encode_batch_plain) whose traversal
+// stages are single persistent launches over all its frames' ray queues.  A
+// job's result is a function of its own inputs only (its seed, camera, scene
+// and sizes), so it is the same alone, batched and in any mix.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -64,18 +68,23 @@ struct Job {
   double gpu_ms = 0.0;
   int graph_mode = 0;  // 0 direct launches, 1 graph instantiated, 2 graph updated in place
   bool cancelled = false;
+  int batch = 1;  // frames of the launch sequence the job ran in
+  float* staging = nullptr;  // its slot's pinned result buffer (pageable callers)
 };
 
 struct Slot {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  float* staging = nullptr;  // pinned, for callers whose output buffer is pageable
-  size_t staging_bytes = 0;
+  // pinned, per batch position, for callers whose output buffer is pageable
+  float* staging[kMaxBatch] = {};
+  size_t staging_bytes[kMaxBatch] = {};
+  JobTrace* h_table = nullptr;  // pinned: the batch's traversal table, copied to d_table in the stream
+  JobTrace* d_table = nullptr;
   // instantiated frame graphs of this slot, one per launch sequence (shape
   // key); a later job of the same key updates its graph in place
   std::map<uint64_t, cudaGraphExec_t> execs;
-  Job* job = nullptr;
-  bool finished = false;  // set by the stream callback
+  std::vector<Job*> jobs;  // the batch in flight; empty when the slot is free
+  bool finished = false;   // set by the stream callback
 };
 
 struct Server {
@@ -83,6 +92,7 @@ struct Server {
   int num_sms = 148;
   uint64_t budget = 0;
   int use_graphs = 0;
+  uint32_t max_batch = kMaxBatch;  // ap_server_set_batching
   FrameConfig base{};
   std::vector<void*> scenes;
   size_t scene_bytes = 0;
@@ -115,84 +125,120 @@ void CUDART_CB on_slot_done(void* p) {  // runs on a CUDA callback thread: no CU
   delete a;
 }
 
-uint64_t shape_key(const ap_job& j, const FrameConfig& cfg) {
-  // the frame's launch sequence depends on the sample and bounce counts only;
-  // resolution, scene, camera and buffers are node parameters, which an
-  // in-place update may change
-  (void)j;
+uint64_t shape_key(const FrameConfig& cfg, int batch) {
+  // the launch sequence depends on the sample and bounce counts and the batch
+  // size only; resolutions, scenes, cameras and buffers are node parameters,
+  // which an in-place update may change
   uint64_t k = 1469598103934665603ull;
   auto mix = [&](uint64_t v) { k = (k ^ v) * 1099511628211ull; };
   mix(cfg.sample_count);
   mix(cfg.max_bounces);
+  mix((uint64_t)batch);
   return k;
 }
 
-// Enqueues one admitted job on its slot's stream (dispatcher thread, no lock
-// held).  Returns false when nothing was enqueued (the job failed up front).
-bool launch_job(Server* s, Job* j, Slot& sl) {
-  const ap_job& d = j->desc;
-  const DevScene* scene = nullptr;
-  cudaStream_t unused_stream;
-  const TwoLevel* unused_two_level = nullptr;  // server scenes are flat uploads
-  int sms = 0, dev = 0;
-  std::string* err = nullptr;
-  ap::handle_trace_context(s->scenes[d.scene], &scene, &unused_two_level, &unused_stream, &sms, &dev, &err);
+// Jobs that may share a launch sequence.
+bool same_shape(const ap_job& a, const ap_job& b) { return a.spp == b.spp && a.max_depth == b.max_depth; }
+
+// Enqueues the admitted batch on the slot's stream (dispatcher thread, no
+// lock held).  The jobs enqueued go to `ok`; those whose frame state cannot be
+// allocated go to `failed` (rc set).  Returns false when nothing was enqueued.
+bool launch_batch(Server* s, Slot& sl, const std::vector<Job*>& batch, std::vector<Job*>* ok_out,
+                  std::vector<Job*>* failed) {
   FrameConfig cfg = s->base;
-  cfg.sample_count = d.spp;
-  cfg.max_bounces = d.max_depth;
-  const size_t out_bytes = (size_t)d.width * d.height * 12;
-  cudaError_t e = cudaMallocFromPoolAsync(&j->dev, j->bytes, s->pool, sl.stream);
-  if (e != cudaSuccess) {
-    j->rc = e == cudaErrorMemoryAllocation ? AP_E_OOM : AP_E_CUDA;
-    j->err = std::string("job frame state: ") + cudaGetErrorString(e);
-    j->dev = nullptr;
-    cudaGetLastError();
-    return false;
+  cfg.sample_count = batch[0]->desc.spp;
+  cfg.max_bounces = batch[0]->desc.max_depth;
+  std::vector<Job*>& ok = *ok_out;
+  BatchFrame frames[kMaxBatch];
+  for (Job* j : batch) {
+    const ap_job& d = j->desc;
+    cudaError_t e = cudaMallocFromPoolAsync(&j->dev, j->bytes, s->pool, sl.stream);
+    if (e != cudaSuccess) {
+      j->rc = e == cudaErrorMemoryAllocation ? AP_E_OOM : AP_E_CUDA;
+      j->err = std::string("job frame state: ") + cudaGetErrorString(e);
+      j->dev = nullptr;
+      cudaGetLastError();
+      failed->push_back(j);
+      continue;
+    }
+    cudaMemsetAsync(j->dev, 0, j->bytes, sl.stream);  // a job starts from a fresh frame sequence
+    const DevScene* scene = nullptr;
+    cudaStream_t unused_stream;
+    const TwoLevel* unused_two_level = nullptr;  // server scenes are flat uploads
+    int sms = 0, dev = 0;
+    std::string* err = nullptr;
+    ap::handle_trace_context(s->scenes[d.scene], &scene, &unused_two_level, &unused_stream, &sms, &dev, &err);
+    BatchFrame& f = frames[ok.size()];
+    f.scene = *scene;
+    frame_buffers_carve(j->dev, d.width, d.height, &f.fb);
+    std::memcpy(&f.mats, d.mats, sizeof(Mats));
+    f.W = d.width;
+    f.H = d.height;
+    f.frame_idx = d.seed;
+    ok.push_back(j);
   }
-  cudaMemsetAsync(j->dev, 0, j->bytes, sl.stream);  // a job starts from a fresh frame sequence
-  FrameBuffers fb{};
-  frame_buffers_carve(j->dev, d.width, d.height, &fb);
-  Mats mats;
-  std::memcpy(&mats, d.mats, sizeof(Mats));
-  float* dst = j->out_pinned ? j->out : sl.staging;
+  const int nj = (int)ok.size();
+  if (nj == 0) return false;
+  const bool batched = nj > 1;
+  for (int k = 0; k < nj; ++k) {
+    sl.h_table[k] = job_trace(frames[k].scene, frames[k].fb, frames[k].W * frames[k].H);
+    ok[k]->batch = nj;
+  }
+  auto encode = [&]() {
+    if (batched) {
+      cudaMemcpyAsync(sl.d_table, sl.h_table, sizeof(JobTrace) * nj, cudaMemcpyHostToDevice, sl.stream);
+      encode_batch_plain(frames, nj, cfg, sl.d_table, s->num_sms, sl.stream);
+    } else {
+      const BatchFrame& f = frames[0];
+      encode_frame(f.scene, f.fb, cfg, f.mats, f.W, f.H, f.frame_idx, s->num_sms, sl.stream, nullptr);
+    }
+    for (int k = 0; k < nj; ++k) {
+      Job* j = ok[k];
+      float* dst = j->out_pinned ? j->out : j->staging;
+      cudaMemcpyAsync(dst, frames[k].fb.out_rgb, (size_t)frames[k].W * frames[k].H * 12, cudaMemcpyDeviceToHost,
+                      sl.stream);
+    }
+  };
+  cudaError_t e = cudaSuccess;
+  int mode = 0;
   cudaEventRecord(sl.ev0, sl.stream);
   if (s->use_graphs) {
     cudaGraph_t g = nullptr;
     e = cudaStreamBeginCapture(sl.stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      encode_frame(*scene, fb, cfg, mats, d.width, d.height, d.seed, s->num_sms, sl.stream, nullptr);
-      cudaMemcpyAsync(dst, fb.out_rgb, out_bytes, cudaMemcpyDeviceToHost, sl.stream);
+      encode();
       e = cudaStreamEndCapture(sl.stream, &g);
     }
     if (e == cudaSuccess) {
-      const uint64_t key = shape_key(d, cfg);
-      cudaGraphExec_t& exec = sl.execs[key];
+      cudaGraphExec_t& exec = sl.execs[shape_key(cfg, nj)];
       cudaGraphExecUpdateResultInfo info;
       if (exec && cudaGraphExecUpdate(exec, g, &info) == cudaSuccess) {
-        j->graph_mode = 2;
+        mode = 2;
         s->graph_updates++;
       } else {
         cudaGetLastError();  // a failed update leaves a recoverable error
         if (exec) cudaGraphExecDestroy(exec);
         exec = nullptr;
         e = cudaGraphInstantiate(&exec, g, 0);
-        j->graph_mode = 1;
+        mode = 1;
         s->graph_instantiations++;
       }
       cudaGraphDestroy(g);
       if (e == cudaSuccess) e = cudaGraphLaunch(exec, sl.stream);
     }
   } else {
-    encode_frame(*scene, fb, cfg, mats, d.width, d.height, d.seed, s->num_sms, sl.stream, nullptr);
-    cudaMemcpyAsync(dst, fb.out_rgb, out_bytes, cudaMemcpyDeviceToHost, sl.stream);
+    encode();
     e = cudaGetLastError();
   }
   cudaEventRecord(sl.ev1, sl.stream);
-  if (e != cudaSuccess) {
-    j->rc = AP_E_CUDA;
-    j->err = std::string("job launch: ") + cudaGetErrorString(e);
+  for (Job* j : ok) {
+    j->graph_mode = mode;
+    if (e != cudaSuccess) {
+      j->rc = AP_E_CUDA;
+      j->err = std::string("job launch: ") + cudaGetErrorString(e);
+    }
   }
-  cudaLaunchHostFunc(sl.stream, on_slot_done, new CallbackArg{s, j->slot});
+  cudaLaunchHostFunc(sl.stream, on_slot_done, new CallbackArg{s, (int)(&sl - &s->slots[0])});
   return true;
 }
 
@@ -203,29 +249,31 @@ void dispatcher(Server* s) {
     // completions
     for (size_t i = 0; i < s->slots.size(); ++i) {
       Slot& sl = s->slots[i];
-      if (!sl.job || !sl.finished) continue;
-      Job* j = sl.job;
+      if (sl.jobs.empty() || !sl.finished) continue;
       cudaError_t e = cudaEventSynchronize(sl.ev1);  // already complete: returns at once
       float ms = 0.0f;
       if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, sl.ev0, sl.ev1);
-      if (e != cudaSuccess && j->rc == AP_OK) {
-        j->rc = AP_E_CUDA;
-        j->err = std::string("job: ") + cudaGetErrorString(e);
+      for (size_t k = 0; k < sl.jobs.size(); ++k) {
+        Job* j = sl.jobs[k];
+        if (e != cudaSuccess && j->rc == AP_OK) {
+          j->rc = AP_E_CUDA;
+          j->err = std::string("job: ") + cudaGetErrorString(e);
+        }
+        if (j->rc == AP_OK && j->cancelled) {
+          j->rc = AP_E_CANCELLED;
+          j->err = "job cancelled while it ran";
+        }
+        if (j->rc == AP_OK && !j->out_pinned)
+          std::memcpy(j->out, j->staging, (size_t)j->desc.width * j->desc.height * 12);
+        if (j->dev) cudaFreeAsync(j->dev, sl.stream);
+        j->dev = nullptr;
+        s->in_use -= j->bytes;
+        j->gpu_ms = ms;
+        j->t_done = Clock::now();
+        j->done = true;
+        s->completed++;
       }
-      if (j->rc == AP_OK && j->cancelled) {
-        j->rc = AP_E_CANCELLED;
-        j->err = "job cancelled while it ran";
-      }
-      if (j->rc == AP_OK && !j->out_pinned)
-        std::memcpy(j->out, sl.staging, (size_t)j->desc.width * j->desc.height * 12);
-      if (j->dev) cudaFreeAsync(j->dev, sl.stream);
-      j->dev = nullptr;
-      s->in_use -= j->bytes;
-      j->gpu_ms = ms;
-      j->t_done = Clock::now();
-      j->done = true;
-      s->completed++;
-      sl.job = nullptr;
+      sl.jobs.clear();
       sl.finished = false;
       s->cv_done.notify_all();
     }
@@ -245,11 +293,12 @@ void dispatcher(Server* s) {
         ++it;
       }
     }
-    // admissions, in arrival order
+    // admissions, in arrival order; a batch takes the head job and the later
+    // queued jobs of the same shape that fit the budget
     while (!s->pending.empty()) {
       int free_slot = -1;
       for (size_t i = 0; i < s->slots.size(); ++i)
-        if (!s->slots[i].job) {
+        if (s->slots[i].jobs.empty()) {
           free_slot = (int)i;
           break;
         }
@@ -269,49 +318,76 @@ void dispatcher(Server* s) {
         break;  // wait for memory to free up
       }
       s->pending.pop_front();
-      Slot& sl = s->slots[free_slot];
-      const size_t out_bytes = (size_t)j->desc.width * j->desc.height * 12;
-      if (!j->out_pinned && sl.staging_bytes < out_bytes) {
-        lk.unlock();
-        if (sl.staging) cudaFreeHost(sl.staging);
-        sl.staging = nullptr;
-        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&sl.staging), out_bytes, cudaHostAllocDefault);
-        lk.lock();
-        sl.staging_bytes = e == cudaSuccess ? out_bytes : 0;
-        if (e != cudaSuccess) {
-          sl.staging = nullptr;
-          j->rc = AP_E_OOM;
-          j->err = "pinned staging buffer";
-          j->t_admit = j->t_done = Clock::now();
-          j->done = true;
-          s->completed++;
-          s->cv_done.notify_all();
-          continue;
+      std::vector<Job*> batch{j};
+      size_t bytes = j->bytes;
+      if (batchable(s->base) && s->max_batch > 1) {
+        for (auto it = s->pending.begin(); it != s->pending.end() && batch.size() < s->max_batch;) {
+          Job* o = *it;
+          if (same_shape(o->desc, j->desc) && s->scene_bytes + s->in_use + bytes + o->bytes <= s->budget) {
+            batch.push_back(o);
+            bytes += o->bytes;
+            it = s->pending.erase(it);
+          } else {
+            ++it;
+          }
         }
       }
-      j->slot = free_slot;
-      j->t_admit = Clock::now();
-      s->in_use += j->bytes;
+      Slot& sl = s->slots[free_slot];
+      std::vector<Job*> admitted;
+      for (size_t k = 0; k < batch.size(); ++k) {
+        Job* b = batch[k];
+        const size_t out_bytes = (size_t)b->desc.width * b->desc.height * 12;
+        if (!b->out_pinned && sl.staging_bytes[k] < out_bytes) {
+          lk.unlock();
+          if (sl.staging[k]) cudaFreeHost(sl.staging[k]);
+          sl.staging[k] = nullptr;
+          cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&sl.staging[k]), out_bytes, cudaHostAllocDefault);
+          lk.lock();
+          sl.staging_bytes[k] = e == cudaSuccess ? out_bytes : 0;
+          if (e != cudaSuccess) {
+            sl.staging[k] = nullptr;
+            b->rc = AP_E_OOM;
+            b->err = "pinned staging buffer";
+            b->t_admit = b->t_done = Clock::now();
+            b->done = true;
+            s->completed++;
+            s->cv_done.notify_all();
+            continue;
+          }
+        }
+        b->staging = sl.staging[k];  // buffer k of the slot is this job's alone
+        admitted.push_back(b);
+      }
+      if (admitted.empty()) continue;
+      const std::vector<Job*>& launched = admitted;
+      const Clock::time_point t_admit = Clock::now();
+      for (Job* b : launched) {
+        b->slot = free_slot;
+        b->t_admit = t_admit;
+        s->in_use += b->bytes;
+      }
       s->peak = std::max(s->peak, s->scene_bytes + s->in_use);
-      sl.job = j;
+      sl.jobs = launched;
       sl.finished = false;
       lk.unlock();
-      const bool enqueued = launch_job(s, j, sl);
+      std::vector<Job*> enq, failed;
+      const bool enqueued = launch_batch(s, sl, launched, &enq, &failed);
       lk.lock();
-      if (!enqueued) {
-        s->in_use -= j->bytes;
-        j->t_done = Clock::now();
-        j->done = true;
+      sl.jobs = enq;
+      for (Job* b : failed) {
+        s->in_use -= b->bytes;
+        b->t_done = Clock::now();
+        b->done = true;
         s->completed++;
-        sl.job = nullptr;
-        s->cv_done.notify_all();
       }
+      if (!enqueued) sl.jobs.clear();
+      if (!failed.empty() || !enqueued) s->cv_done.notify_all();
     }
     bool inflight = false;
-    for (const Slot& sl : s->slots) inflight = inflight || sl.job;
+    for (const Slot& sl : s->slots) inflight = inflight || !sl.jobs.empty();
     if (s->stop && s->pending.empty() && !inflight) break;
     bool ready = false;
-    for (const Slot& sl : s->slots) ready = ready || (sl.job && sl.finished);
+    for (const Slot& sl : s->slots) ready = ready || (!sl.jobs.empty() && sl.finished);
     if (!ready) {
       // sleep until a completion, a submission, or the nearest queued deadline
       double wait_ms = -1.0;
@@ -374,7 +450,10 @@ void* ap_server_create(const ap_frame_config* cfg, int device, uint64_t hbm_budg
   for (Slot& sl : s->slots) {
     if (!ok) break;
     ok = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) == cudaSuccess &&
-         cudaEventCreate(&sl.ev0) == cudaSuccess && cudaEventCreate(&sl.ev1) == cudaSuccess;
+         cudaEventCreate(&sl.ev0) == cudaSuccess && cudaEventCreate(&sl.ev1) == cudaSuccess &&
+         cudaHostAlloc(reinterpret_cast<void**>(&sl.h_table), sizeof(JobTrace) * kMaxBatch, cudaHostAllocDefault) ==
+             cudaSuccess &&
+         cudaMalloc(&sl.d_table, sizeof(JobTrace) * kMaxBatch) == cudaSuccess;
   }
   if (!ok) {
     cudaGetLastError();
@@ -383,6 +462,8 @@ void* ap_server_create(const ap_frame_config* cfg, int device, uint64_t hbm_budg
       if (t.stream) cudaStreamDestroy(t.stream);
       if (t.ev0) cudaEventDestroy(t.ev0);
       if (t.ev1) cudaEventDestroy(t.ev1);
+      if (t.h_table) cudaFreeHost(t.h_table);
+      if (t.d_table) cudaFree(t.d_table);
     }
     if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
@@ -407,7 +488,10 @@ void ap_server_destroy(void* sp) {
     for (auto& kv : sl.execs)
       if (kv.second) cudaGraphExecDestroy(kv.second);
     sl.execs.clear();
-    if (sl.staging) cudaFreeHost(sl.staging);
+    for (float* p : sl.staging)
+      if (p) cudaFreeHost(p);
+    if (sl.h_table) cudaFreeHost(sl.h_table);
+    if (sl.d_table) cudaFree(sl.d_table);
     if (sl.ev0) cudaEventDestroy(sl.ev0);
     if (sl.ev1) cudaEventDestroy(sl.ev1);
     if (sl.stream) cudaStreamDestroy(sl.stream);
@@ -505,6 +589,8 @@ int ap_server_wait(void* sp, uint64_t ticket, ap_job_result* res) {
     res->device_bytes = j->bytes;
     res->graph_mode = (uint32_t)j->graph_mode;
     res->slot = (uint32_t)j->slot;
+    res->batch = (uint32_t)j->batch;
+    res->pad = 0;
   }
   int rc = j->rc;
   if (rc != AP_OK) s->err = j->err;
@@ -542,12 +628,23 @@ int ap_server_cancel(void* sp, uint64_t ticket) {
   return AP_OK;
 }
 
+int ap_server_set_batching(void* sp, uint32_t max_batch) {
+  Server* s = static_cast<Server*>(sp);
+  if (!s || max_batch == 0 || max_batch > (uint32_t)kMaxBatch) return AP_E_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->max_batch = max_batch;
+  }
+  s->cv_work.notify_one();
+  return AP_OK;
+}
+
 int ap_server_stats(void* sp, uint64_t* out8) {
   Server* s = static_cast<Server*>(sp);
   if (!s || !out8) return AP_E_INVALID;
   std::lock_guard<std::mutex> lk(s->mu);
   uint64_t inflight = 0;
-  for (const Slot& sl : s->slots) inflight += sl.job ? 1 : 0;
+  for (const Slot& sl : s->slots) inflight += sl.jobs.size();
   out8[0] = s->completed;
   out8[1] = inflight;
   out8[2] = s->pending.size();

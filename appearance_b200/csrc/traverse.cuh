@@ -273,8 +273,15 @@ APD void trav_init(Trav& t, float3 o, float3 d, float tmax) {
 
 // Runs up to `budget` steps; returns true when the ray is finished.  kUnroll
 // unrolls the 8 child tests.
-template <bool kAny, bool kCount, bool kUnroll = false>
-APD bool trav_step(const DevScene& s, Trav& t, uint2* stack, int budget, Visits* vc) {
+// The scene S is a DevScene or any view with the same `nodes` and `tris`
+// (the only fields the traversal reads), such as BvhView.
+struct BvhView {
+  const uint4* nodes;
+  const float4* tris;
+};
+
+template <bool kAny, bool kCount, bool kUnroll = false, class S>
+APD bool trav_step(const S& s, Trav& t, uint2* stack, int budget, Visits* vc) {
   for (int step = 0; step < budget; ++step) {
     if (t.tri_mask) {
       const int j = __ffs(t.tri_mask) - 1;

@@ -108,7 +108,12 @@ class RenderServer:
         out = self._outs.pop(ticket)
         self._check(self._lib.ap_server_wait(self._s, ticket, ctypes.byref(r)))
         return out, dict(queued_ms=r.queued_ms, total_ms=r.total_ms, gpu_ms=r.gpu_ms, device_bytes=r.device_bytes,
-                         graph_mode=r.graph_mode, slot=r.slot)
+                         graph_mode=r.graph_mode, slot=r.slot, batch=r.batch)
+
+    def set_batching(self, max_batch: int):
+        """ap_server_set_batching: the largest batch of same-shape jobs admitted
+        together (1 runs every job on its own)."""
+        self._check(self._lib.ap_server_set_batching(self._s, max_batch))
 
     def cancel(self, ticket: int):
         """ap_server_cancel: a queued job is dropped; one on the GPU finishes its
@@ -174,11 +179,13 @@ def run_jobs(server: RenderServer, jobs, paths, realtime: bool = True, pinned=No
 
 def summarise(jobs, results, wall):
     lat = sorted(r["total_ms"] for r in results)
+    batches = [r.get("batch", 1) for r in results]
     samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
     q = lambda p: lat[min(len(lat) - 1, int(round(p * (len(lat) - 1))))]
     return dict(jobs=len(jobs), p50_ms=q(0.5), p99_ms=q(0.99), mean_ms=statistics.mean(lat),
                 msamples_per_s=samples / wall / 1e6, wall_s=wall,
                 mean_queued_ms=statistics.mean(r["queued_ms"] for r in results),
+                mean_batch=statistics.mean(batches), batched_jobs=sum(1 for b in batches if b > 1),
                 mean_gpu_ms=statistics.mean(r["gpu_ms"] for r in results))
 
 
@@ -206,8 +213,9 @@ def run_benchmark(n_jobs: int = 200, rates=(200.0,), scene_tris=(100000, 1000000
                              resolutions=RESOLUTIONS, res_probs=RES_PROBS, scene_gen_s=gen_s))
     warm = [dict(j, arrival=0.0) for j in serving_jobs(8, 1.0, len(scene_tris), seed=seed + 99)]
 
-    def server(max_inflight, use_graphs):
+    def server(max_inflight, use_graphs, max_batch=8):
         srv = RenderServer(SERVE_CONFIG, hbm_budget=budget_gb * 1e9, max_inflight=max_inflight, use_graphs=use_graphs)
+        srv.set_batching(max_batch)
         for f in field:
             srv.add_scene(f)
         run_jobs(srv, warm, paths, realtime=False, pinned=pinned)  # one job per class, untimed
@@ -231,7 +239,7 @@ def run_benchmark(n_jobs: int = 200, rates=(200.0,), scene_tris=(100000, 1000000
     out["stats"] = srv.stats()
     srv.close()
     if serial:
-        ser = server(1, False)
+        ser = server(1, False, max_batch=1)
         jobs = serving_jobs(n_jobs, rates[0], len(scene_tris), seed=seed)
         res, wall = run_jobs(ser, jobs, paths, realtime=True, pinned=pinned)
         out["serial"] = dict(rate=rates[0], **summarise(jobs, res, wall))

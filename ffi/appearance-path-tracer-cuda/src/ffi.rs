@@ -125,6 +125,8 @@ pub struct ApJobResult {
     pub device_bytes: u64,
     pub graph_mode: u32,
     pub slot: u32,
+    pub batch: u32,
+    pub pad: u32,
 }
 
 extern "C" {
@@ -181,6 +183,7 @@ extern "C" {
     pub fn ap_server_query(server: *mut c_void, ticket: u64, done: *mut c_int) -> c_int;
     pub fn ap_server_wait(server: *mut c_void, ticket: u64, result: *mut ApJobResult) -> c_int;
     pub fn ap_server_cancel(server: *mut c_void, ticket: u64) -> c_int;
+    pub fn ap_server_set_batching(server: *mut c_void, max_batch: u32) -> c_int;
     pub fn ap_server_stats(server: *mut c_void, out8: *mut u64) -> c_int;
 
     // radiance cache

@@ -282,9 +282,15 @@ int ap_profile_spectral(void* handle, uint32_t w, uint32_t h, uint32_t row_start
  * concurrently, one stream each.  A job renders `spp` samples per pixel with
  * `max_depth` bounces using the server's frame configuration otherwise, from
  * a fresh frame sequence with PCG frame index `seed`; its result is the same
- * alone and in any mix of jobs.  use_graphs != 0 launches each job as a CUDA
- * graph (captured per job, updated in place when a slot's previous job had
- * the same shape).  The server's dispatcher thread and CUDA callbacks do the
+ * alone and in any mix of jobs.  With a plain-estimator configuration
+ * (restir_di, restir_gi, svgf, taa and firefly_filter all 0), queued jobs of
+ * the same spp and max_depth are admitted together, up to 8
+ * (ap_server_set_batching), and run as one launch sequence whose traversal
+ * stages are shared persistent launches over all their ray queues; each
+ * job's result is still its alone result.  use_graphs != 0 launches each
+ * slot's work as a CUDA graph (captured per launch, updated in place when the
+ * slot ran a launch sequence of the same shape before: same spp, depth and
+ * batch size).  The server's dispatcher thread and CUDA callbacks do the
  * work; all entry points are thread-safe. */
 typedef struct ap_job {
   uint32_t scene;           /* id from ap_server_add_scene */
@@ -304,6 +310,8 @@ typedef struct ap_job_result {
   uint64_t device_bytes;    /* frame state held while it ran */
   uint32_t graph_mode;      /* 0 direct launches, 1 graph instantiated, 2 graph updated in place */
   uint32_t slot;
+  uint32_t batch;           /* jobs of the launch sequence it ran in (1: alone) */
+  uint32_t pad;
 } ap_job_result;
 
 void* ap_server_create(const ap_frame_config* cfg, int device, uint64_t hbm_budget, uint32_t max_inflight,
@@ -327,6 +335,9 @@ int ap_server_wait(void* server, uint64_t ticket, ap_job_result* result);
  * AP_E_CANCELLED.  A finished job is left as it is (AP_OK); an unknown ticket
  * is AP_E_INVALID. */
 int ap_server_cancel(void* server, uint64_t ticket);
+/* Largest batch of jobs admitted together (1..8, default 8; 1 runs every job
+ * on its own).  Takes effect at the next admission. */
+int ap_server_set_batching(void* server, uint32_t max_batch);
 /* completed, in flight, queued, device bytes in use, peak device bytes, scene
  * bytes, graphs instantiated, graphs updated in place */
 int ap_server_stats(void* server, uint64_t* out8);

@@ -148,3 +148,39 @@ def test_faults_fail_their_own_job_only():
     with pytest.raises(RendererError):
         srv.cancel(123456789)
     srv.close()
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_batched_jobs_equal_their_alone_results(graphs):
+    """Jobs of the same spp and depth queued together run as one launch
+    sequence (shared traversal launches over all their ray queues); each
+    result is bit for bit the one the job has on a server that runs every job
+    on its own.  The batch mixes scenes, sizes (one of a single pixel),
+    cameras and seeds."""
+    scs = [small_scene(0), small_scene(1)]
+    jobs = [(0, 64, 48, 11), (1, 40, 30, 12), (0, 1, 1, 13), (1, 96, 20, 14), (0, 33, 65, 15), (1, 64, 48, 16)]
+    spp, depth = 2, 3
+    alone = RenderServer(CFG, hbm_budget=8e9, max_inflight=1, use_graphs=False)
+    alone.set_batching(1)
+    ids = [alone.add_scene(s) for s in scs]
+    refs = []
+    for sc, w, h, seed in jobs:
+        img, info = alone.wait(alone.submit(ids[sc], w, h, spp, depth, seed, mats_for(sc, seed % 16, w, h)))
+        assert info["batch"] == 1
+        refs.append(img)
+    alone.close()
+    srv = RenderServer(CFG, hbm_budget=8e9, max_inflight=1, use_graphs=graphs)
+    ids = [srv.add_scene(s) for s in scs]
+    # a long job first holds the only slot, so the others queue up and are admitted together
+    blocker = srv.submit(ids[0], 256, 256, 16, depth, 1, mats_for(0, 1, 256, 256))
+    tickets = [srv.submit(ids[sc], w, h, spp, depth, seed, mats_for(sc, seed % 16, w, h)) for sc, w, h, seed in jobs]
+    srv.wait(blocker)
+    batches = []
+    for t, ref in zip(tickets, refs):
+        img, info = srv.wait(t)
+        assert same_bits(img, ref)
+        batches.append(info["batch"])
+    assert max(batches) > 1, batches
+    st = srv.stats()
+    assert st["in_flight"] == 0 and st["queued"] == 0
+    srv.close()
