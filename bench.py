@@ -383,9 +383,16 @@ def city_spectral_config(cpu: bool) -> dict:
     from appearance_b200 import scenes, spectral_bench
     kept = {}
     res = spectral_bench.measure(instanced=True, keep_scene=kept if cpu else None)
-    flat = spectral_bench.measure(instanced=False, cache=True)
+    flat = spectral_bench.measure(instanced=False, cache=True, quality=True, ref_spp=1024)
     res["flat_city"] = {k: flat[k] for k in ("value", "unit", "frame_ms", "rays_per_sample", "workload", "traversal")}
-    res["cache"] = flat["cache"]
+    res["cache"] = dict(flat["cache"])
+    # relMSE of the 1024x1024 centre crop against a 1024-spp plain render of it;
+    # the plain time to the cache's relMSE assumes relMSE ~ 1/spp (variance)
+    e_plain, e_cache = flat["quality"]["relmse_crop"], flat["cache"]["relmse_crop"]
+    t_plain_eq = flat["frame_ms"] * e_plain / e_cache
+    res["cache"].update(relmse_plain=e_plain, relmse_cache=e_cache, reference_spp=1024,
+                        plain_time_to_cache_relmse_ms=t_plain_eq,
+                        time_ratio=(flat["cache"]["frame_ms"] + flat["cache"]["warmup_ms"]) / t_plain_eq)
     if cpu:
         from oracle.oracle import OracleScene, OracleSpectral, OracleTwoLevel
         rows, size, threads = 64, kept["size"], os.cpu_count()
