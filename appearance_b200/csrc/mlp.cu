@@ -16,10 +16,10 @@
 // thread issues tcgen05.mma (M=128, N=64 or 16, K=16 per instruction) with the
 // FP32 accumulator in tensor memory; every warp reads its 32 rows back with
 // tcgen05.ld, applies ReLU, rounds to FP16 and writes the next layer's
-// operand.  Training (k_rc_encode_batch, k_sgemm, k_rc_loss, k_rc_adam) runs
-// on the CUDA cores in FP32 on the same FP16-rounded weights and activations,
-// layer by layer as tiled GEMMs over the batch: 2^16 samples per step is about
-// 7 GFLOP, small beside the frame.
+// operand.  Training (k_rc_train_tc) runs forward and backward on the tensor
+// cores in one kernel per step, tile by tile with the weight-gradient sums in
+// tensor memory; k_rc_adam updates the FP32 master weights and repacks the
+// FP16 operands (forward and transposed).
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -53,6 +53,13 @@ constexpr int kPackW2 = kPackW1 + kHid * kHid;
 constexpr int kPackW3 = kPackW2 + kHid * kHid;
 constexpr int kPackW4 = kPackW3 + kHid * kHid;
 constexpr int kPackHalves = kPackW4 + kOutPad * kHid;  // 22528 halves = 45056 bytes
+// Transposed copies for the backward pass (W_l^T as the B operand of
+// dH_l = dZ_l W_l: rows = the layer's inputs, K = its outputs), W1..W4; W4^T's
+// K is padded to 16 (outputs 3..15 zero).
+constexpr int kPackT1 = kPackHalves;
+constexpr int kPackT4 = kPackT1 + 3 * kHid * kHid;
+constexpr int kPackTHalves = 3 * kHid * kHid + kHid * kOutPad;  // 13312 halves = 26624 bytes
+constexpr int kPackAllHalves = kPackHalves + kPackTHalves;
 constexpr int kTile = 128;                             // queries per CTA tile (MMA M)
 constexpr int kSmemWeights = kPackHalves * 2;
 constexpr int kSmemAct = kTile * kIn * 2;              // 36864: A0, then the two hidden buffers
@@ -302,151 +309,310 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
 }
 
-// ---- training (CUDA cores, FP32 on FP16-rounded weights and activations) ----
+// ---- training on the tensor cores -------------------------------------------
 //
-// Per sample: h0 = encode (FP16-rounded), h_{l+1} = fp16(relu(W_l h_l)) for
-// l = 0..3, y = W4 h4, prediction exp(y).  Relative L2 loss (the prediction in
-// the denominator held constant), averaged over samples and channels:
-//   L = mean (exp(y) - t)^2 / (exp(y)^2 + 0.01).
-// Backward: d4 = dL/dy, d_l = (W_{l+1}^T d_{l+1}) * [h_{l+1} > 0], and the
-// weight gradients dW_l = sum_s d_l h_l^T.  The batch is processed layer by
-// layer as tiled GEMMs over all samples (activations H_l and gradients D_l
-// stored row-major per sample); the sample count comes from device memory.
+// k_rc_train_tc: one CTA of 128 threads takes whole 128-sample tiles.  Per
+// tile it runs the forward layers as k_rc_infer does, keeping each hidden
+// activation (the next layer's operand) and its transpose (an operand of the
+// weight gradient), then the loss and its gradient per sample, then the
+// backward layers:
+//   dH_l = dZ_l W_l       M = 128 samples, N = the layer's inputs, K = its
+//                         outputs (B = the packed W_l^T);
+//   dW_l += dZ_l^T H_l    M = 128 rows, N = the layer's inputs, K = the tile's
+//                         128 samples;
+//   dZ_{l-1} = dH_l * [H_l > 0].
+// Tensor-core operands are FP16.  A gradient value x enters as two FP16
+// numbers, hi = fp16(x) and lo = fp16(x - hi), about 21 significant bits
+// together: dH_l takes two MMAs (hi, then lo, into one accumulator), and the
+// A operand of dW_l stacks the 64 outputs' hi rows over their lo rows, the two
+// halves of the sum being added when it is read out.  The activations H_l are
+// FP16 values already (the model rounds them).  So the products and their
+// FP32 sums keep the precision of an FP32 backward pass.  The weight-gradient
+// sums stay in tensor memory over all of the CTA's tiles and reach the
+// gradient with one atomic add per element at the end.  The per-sample loss
+// gradient enters without the mean's 1 / (3n), which is applied to the sums
+// (the FP16 operands stay clear of underflow); a value beyond the FP16 range
+// (65504) is clamped there.
+constexpr int kTrainR = kPackAllHalves * 2;           // A0, H_l ping-pong, dY and dZ rows, H0^T
+constexpr int kTrainHT = kTrainR + kTile * kIn * 2;   // H1^T .. H4^T, kHid x kTile each
+constexpr int kTrainHTBytes = kHid * kTile * 2;
+constexpr int kTrainDZT = kTrainHT + 4 * kTrainHTBytes;  // [dZ^T hi; dZ^T lo], 128 x kTile
+constexpr int kTrainBar = kTrainDZT + 2 * kHid * kTile * 2;
+constexpr int kSmemTrain = kTrainBar + 16;
+static_assert(kSmemTrain <= 227 * 1024, "training shared memory");
+// tensor-memory columns: the layer accumulator, then the weight-gradient sums
+constexpr uint32_t kColLayer = 0, kColDW4 = 64, kColDW3 = 128, kColDW2 = 192, kColDW1 = 256, kColDW0 = 320;
 
-// Encodes the batch: H0[s] = fp16-rounded features.
-__global__ void k_rc_encode_batch(const float4* __restrict__ queries, const uint32_t* __restrict__ n_dev, uint32_t cap,
-                                  RcBounds bounds, float* __restrict__ h0) {
-  const uint32_t n = min(*n_dev, cap);
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  float q[kQueryFloats];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    float4 v = queries[4 * (size_t)s + i];
-    q[4 * i] = v.x; q[4 * i + 1] = v.y; q[4 * i + 2] = v.z; q[4 * i + 3] = v.w;
-  }
-  float* row = h0 + (size_t)s * kIn;
-  rc_encode(q, bounds, [&](int k, float x) { row[k] = h16(x); });
+APD void split_half(float x, __half* hi, __half* lo) {
+  x = fminf(fmaxf(x, -65504.0f), 65504.0f);
+  const __half h = __float2half_rn(x);
+  *hi = h;
+  *lo = __float2half_rn(x - __half2float(h));
 }
 
-enum { EPI_RELU_H16 = 0, EPI_MASK = 1, EPI_ATOMIC = 2 };
+// `steps` MMAs of K = 16 over K-major operands (stride byte offsets sbo_a,
+// sbo_b between 8-row groups); the first overwrites the accumulator unless acc.
+APD void mma_steps(uint32_t d, uint32_t a, uint32_t sbo_a, uint32_t b, uint32_t sbo_b, int steps, uint32_t idesc,
+                   bool acc) {
+  for (int ks = 0; ks < steps; ++ks)
+    mma_f16(d, smem_desc(a + ks * 256, 128, sbo_a), smem_desc(b + ks * 256, 128, sbo_b), idesc,
+            (acc || ks > 0) ? 1u : 0u);
+}
 
-// C(m, n) = sum_k A(m, k) B(k, n) over 64 x 64 tiles, 256 threads of 4 x 4
-// outputs, K staged 16 at a time in shared memory.  A(m, k) is A[m*lda + k]
-// (kAT false) or A[k*lda + m]; B(k, n) is B[k*ldb + n] (kBT false) or
-// B[n*ldb + k].  Rows m of sample-indexed operands stop at the device count
-// (kRowsAreSamples); for the weight gradients K runs over samples, split into
-// chunks along gridDim.z and summed with atomics (EPI_ATOMIC).  Epilogues:
-// fp16(relu) for hidden layers, the ReLU mask `aux` > 0 for backward
-// gradients, atomic accumulation for weight gradients.
-template <bool kAT, bool kBT, int kEpi>
-__global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, const float* __restrict__ A, int lda,
-                                               const float* __restrict__ B, int ldb, float* __restrict__ C, int ldc,
-                                               const float* __restrict__ aux, int ldaux, const uint32_t* __restrict__ n_dev,
-                                               uint32_t cap, int kchunk) {
-  __shared__ float As[16][64 + 4];
-  __shared__ float Bs[16][64 + 4];
-  const uint32_t n = min(*n_dev, cap);
-  if (kEpi != EPI_ATOMIC) M = min(M, (int)n);  // rows are samples
-  else K = min(K, (int)n);                      // the reduction runs over samples
-  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-  const int kb = kEpi == EPI_ATOMIC ? blockIdx.z * kchunk : 0;
-  const int ke = kEpi == EPI_ATOMIC ? min(K, kb + kchunk) : K;
-  if (m0 >= M || kb >= ke) return;
-  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-  float acc[4][4] = {};
-  for (int k0 = kb; k0 < ke; k0 += 16) {
+// Shared-memory operands written by all threads, handed to the tensor core.
+APD void operands_ready() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Thread 0 commits the MMAs it issued; all wait for them (bounded).  Returns
+// false on every thread when the wait ran out.
+APD bool mmas_done(uint32_t bar, uint32_t& phase, int t) {
+  if (t == 0) mma_commit(bar);
+  const bool bad = !mbar_wait(bar, phase);
+  phase ^= 1u;
+  const bool any_bad = __syncthreads_or(bad);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  return !any_bad;
+}
+
+// The 64 columns of the layer accumulator in this thread's row.
+APD void layer_row(uint32_t lane_addr, float* v) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int e = t * 4 + j;  // 1024 elements of each tile
-      const int kk = e >> 6, mm = e & 63;  // A tile as [k][m]
-      const int gk = k0 + kk, gm = m0 + mm, gn = n0 + mm;
-      float av = 0.0f, bv = 0.0f;
-      if (gk < ke && gm < M) av = kAT ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
-      if (gk < ke && gn < N) bv = kBT ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
-      As[kk][mm] = av;
-      Bs[kk][mm] = bv;
+  for (int c = 0; c < kHid; c += 16) tmem_ld16(lane_addr + kColLayer + c, v + c);
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+APD void store_row8h(__half* base, int row, int k0, int K, const __half* h) {
+  *reinterpret_cast<uint4*>(base + core_offset(row, k0, K)) = *reinterpret_cast<const uint4*>(h);
+}
+
+// Forward epilogue of a hidden layer: H = fp16(relu(acc)) as the next layer's
+// A operand (row t of `next`) and into column t of its transpose `ht`.
+APD void train_fwd_epilogue(uint32_t lane_addr, __half* next, __half* ht, int t) {
+  float v[kHid];
+  layer_row(lane_addr, v);
+#pragma unroll
+  for (int k = 0; k < kHid; k += 8) {
+    __align__(16) __half h[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      h[i] = __float2half_rn(fmaxf(v[k + i], 0.0f));
+      ht[core_offset(k + i, t, kTile)] = h[i];
     }
-    __syncthreads();
+    store_row8h(next, t, k, kHid, h);
+  }
+}
+
+// Backward epilogue: dZ = dH * [H > 0] from the layer accumulator and the
+// mask of ht (H's transpose); hi / lo rows into dz_hi / dz_lo (when given) and
+// columns into [dZ^T hi; dZ^T lo].
+APD void train_bwd_epilogue(uint32_t lane_addr, const __half* ht, __half* dz_hi, __half* dz_lo, __half* dzt, int t) {
+  float v[kHid];
+  layer_row(lane_addr, v);
 #pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      float a[4], b[4];
+  for (int k = 0; k < kHid; k += 8) {
+    __align__(16) __half hi[8];
+    __align__(16) __half lo[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int c = k + i;
+      const float x = __half2float(ht[core_offset(c, t, kTile)]) > 0.0f ? v[c] : 0.0f;
+      split_half(x, &hi[i], &lo[i]);
+      dzt[core_offset(c, t, kTile)] = hi[i];
+      dzt[core_offset(kHid + c, t, kTile)] = lo[i];
+    }
+    if (dz_hi) {
+      store_row8h(dz_hi, t, k, kHid, hi);
+      store_row8h(dz_lo, t, k, kHid, lo);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTile, 1) k_rc_train_tc(const uint4* __restrict__ packed,
+                                                          const float4* __restrict__ queries,
+                                                          const float* __restrict__ targets,
+                                                          const uint32_t* __restrict__ n_dev, uint32_t cap,
+                                                          RcBounds bounds, float* __restrict__ grad,
+                                                          float* __restrict__ loss_sum, uint32_t* __restrict__ err) {
+  const uint32_t n = min(*n_dev, cap);
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int t = threadIdx.x, warp = t >> 5;
+  for (int i = t; i < kPackAllHalves / 8; i += kTile) reinterpret_cast<uint4*>(smem)[i] = packed[i];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTrainBar);
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(smem + kTrainBar + 8);
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_holder;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t bar_a = smem_u32(bar);
+  const uint32_t w_a = smem_u32(smem), r_a = smem_u32(smem + kTrainR), dzt_a = smem_u32(smem + kTrainDZT);
+  __half* r = reinterpret_cast<__half*>(smem + kTrainR);
+  __half* p0 = r;                // H1, H3, dZ hi rows
+  __half* p1 = r + kTile * kHid;  // H2, H4, dZ lo rows
+  __half* dzt = reinterpret_cast<__half*>(smem + kTrainDZT);
+  __half* ht[4];
+  uint32_t ht_a[4];
+  for (int l = 0; l < 4; ++l) {
+    ht[l] = reinterpret_cast<__half*>(smem + kTrainHT + l * kTrainHTBytes);
+    ht_a[l] = smem_u32(ht[l]);
+  }
+  const uint32_t p0_a = r_a, p1_a = r_a + kTile * kHid * 2;
+  const uint32_t sbo64 = (kHid / 8) * 128, sbo144 = (kIn / 8) * 128, sbo16 = (kOutPad / 8) * 128,
+                 sbo_s = (kTile / 8) * 128;
+  const uint32_t id64 = mma_idesc(kTile, kHid), id16 = mma_idesc(kTile, kOutPad), id144 = mma_idesc(kTile, kIn);
+  const uint32_t wt_a[5] = {0u, w_a + kPackT1 * 2, w_a + (kPackT1 + kHid * kHid) * 2,
+                            w_a + (kPackT1 + 2 * kHid * kHid) * 2, w_a + kPackT4 * 2};
+  uint32_t phase = 0;
+  bool ok = true, first = true;
+  float loss = 0.0f;
+  const uint32_t tiles = (n + kTile - 1) / kTile;
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    const uint32_t row = tile * kTile + t;
+    float q[kQueryFloats];
+    if (row < n) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        a[i] = As[kk][ty * 4 + i];
-        b[i] = Bs[kk][tx * 4 + i];
+        const float4 v = queries[4 * (size_t)row + i];
+        q[4 * i] = v.x; q[4 * i + 1] = v.y; q[4 * i + 2] = v.z; q[4 * i + 3] = v.w;
       }
+      rc_encode(q, bounds, [&](int k, float x) { r[core_offset(t, k, kIn)] = __float2half_rn(x); });
+    } else {
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+      for (int k = 0; k < kIn; k += 8) *reinterpret_cast<uint4*>(r + core_offset(t, k, kIn)) = make_uint4(0, 0, 0, 0);
     }
-    __syncthreads();
-  }
+    // forward: H1 .. H4
+    operands_ready();
+    if (t == 0) mma_steps(tmem + kColLayer, r_a, sbo144, w_a + kPackW0 * 2, sbo144, kIn / 16, id64, false);
+    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    train_fwd_epilogue(lane_addr, p0, ht[0], t);
+    operands_ready();
+    if (t == 0) mma_steps(tmem + kColLayer, p0_a, sbo64, w_a + kPackW1 * 2, sbo64, kHid / 16, id64, false);
+    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    train_fwd_epilogue(lane_addr, p1, ht[1], t);
+    operands_ready();
+    if (t == 0) mma_steps(tmem + kColLayer, p1_a, sbo64, w_a + kPackW2 * 2, sbo64, kHid / 16, id64, false);
+    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    train_fwd_epilogue(lane_addr, p0, ht[2], t);
+    operands_ready();
+    if (t == 0) mma_steps(tmem + kColLayer, p0_a, sbo64, w_a + kPackW3 * 2, sbo64, kHid / 16, id64, false);
+    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    train_fwd_epilogue(lane_addr, p1, ht[3], t);
+    operands_ready();
+    if (t == 0) mma_steps(tmem + kColLayer, p1_a, sbo64, w_a + kPackW4 * 2, sbo64, kHid / 16, id16, false);
+    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    // output layer: loss and its gradient per sample (without the 1 / (3n))
+    {
+      float v[16];
+      tmem_ld16(lane_addr + kColLayer, v);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      __align__(16) __half hi[16];
+      __align__(16) __half lo[16];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int gm = m0 + ty * 4 + i;
-    if (gm >= M) continue;
+      for (int c = 0; c < 16; ++c) {
+        hi[c] = __float2half_rn(0.0f);
+        lo[c] = hi[c];
+      }
+      if (row < n) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int gn = n0 + tx * 4 + j;
-      if (gn >= N) continue;
-      float* c = C + (size_t)gm * ldc + gn;
-      if (kEpi == EPI_RELU_H16) *c = h16(fmaxf(acc[i][j], 0.0f));
-      else if (kEpi == EPI_MASK) *c = aux[(size_t)gm * ldaux + gn] > 0.0f ? acc[i][j] : 0.0f;
-      else atomicAdd(c, acc[i][j]);
+        for (int c = 0; c < kOut; ++c) {
+          const float p = dm::exp_(v[c]), tg = targets[3 * (size_t)row + c];
+          const float den = p * p + 0.01f;
+          loss += (p - tg) * (p - tg) / den;
+          split_half(2.0f * (p - tg) / den * p, &hi[c], &lo[c]);
+        }
+      }
+      store_row8h(p0, t, 0, kOutPad, hi);      // dY hi rows: [128 x 16]
+      store_row8h(p0, t, 8, kOutPad, hi + 8);
+      __half* dy_lo = p0 + kTile * kOutPad;    // dY lo rows
+      store_row8h(dy_lo, t, 0, kOutPad, lo);
+      store_row8h(dy_lo, t, 8, kOutPad, lo + 8);
+      for (int i = t; i < 2 * kHid * kTile / 8; i += kTile) reinterpret_cast<uint4*>(dzt)[i] = make_uint4(0, 0, 0, 0);
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < kOut; ++c) {
+        dzt[core_offset(c, t, kTile)] = hi[c];
+        dzt[core_offset(kHid + c, t, kTile)] = lo[c];
+      }
     }
+    // backward: layer 4, then 3 .. 1
+    operands_ready();
+    if (t == 0) {
+      mma_steps(tmem + kColDW4, dzt_a, sbo_s, ht_a[3], sbo_s, kTile / 16, id64, !first);
+      mma_steps(tmem + kColLayer, p0_a, sbo16, wt_a[4], sbo16, 1, id64, false);
+      mma_steps(tmem + kColLayer, p0_a + kTile * kOutPad * 2, sbo16, wt_a[4], sbo16, 1, id64, true);
+    }
+    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    train_bwd_epilogue(lane_addr, ht[3], p0, p1, dzt, t);  // dZ3
+    const uint32_t dw_col[4] = {kColDW0, kColDW1, kColDW2, kColDW3};
+    for (int l = 3; l >= 1; --l) {
+      operands_ready();
+      if (t == 0) {
+        mma_steps(tmem + dw_col[l], dzt_a, sbo_s, ht_a[l - 1], sbo_s, kTile / 16, id64, !first);
+        mma_steps(tmem + kColLayer, p0_a, sbo64, wt_a[l], sbo64, kHid / 16, id64, false);
+        mma_steps(tmem + kColLayer, p1_a, sbo64, wt_a[l], sbo64, kHid / 16, id64, true);
+      }
+      if (!(ok = mmas_done(bar_a, phase, t))) break;
+      // dZ_{l-1}; the last one (dZ0) only as the weight-gradient operand
+      train_bwd_epilogue(lane_addr, ht[l - 1], l > 1 ? p0 : nullptr, l > 1 ? p1 : nullptr, dzt, t);
+    }
+    if (!ok) break;
+    // H0^T (the encoding, re-computed) for dW0 = dZ0^T H0
+    if (row < n) rc_encode(q, bounds, [&](int k, float x) { r[core_offset(k, t, kTile)] = __float2half_rn(x); });
+    else
+      for (int k = 0; k < kIn; ++k) r[core_offset(k, t, kTile)] = __float2half_rn(0.0f);
+    operands_ready();
+    if (t == 0) mma_steps(tmem + kColDW0, dzt_a, sbo_s, r_a, sbo_s, kTile / 16, id144, !first);
+    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    first = false;
   }
-}
-
-// Output layer, loss and the first two gradients per sample: y = W4 h4,
-// d4 = dL/dy (through exp), d3 = (W4^T d4) * [h4 > 0].
-__global__ void __launch_bounds__(128) k_rc_loss(const float* __restrict__ wf, const float* __restrict__ h4,
-                                                 const float* __restrict__ targets, const uint32_t* __restrict__ n_dev,
-                                                 uint32_t cap, float* __restrict__ d4, float* __restrict__ d3,
-                                                 float* __restrict__ loss_sum) {
-  __shared__ float w4[kOut * kHid];
-  for (int i = threadIdx.x; i < kOut * kHid; i += blockDim.x) w4[i] = wf[kOffW4 + i];
-  __syncthreads();
-  const uint32_t n = min(*n_dev, cap);
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  float loss = 0.0f;
-  if (s < n) {
-    const float* h = h4 + (size_t)s * kHid;
-    float hv[kHid];
-#pragma unroll
-    for (int i = 0; i < kHid; ++i) hv[i] = h[i];
-    float dy[kOut];
+  // weight-gradient sums -> gradient: rows 0..63 (hi) plus rows 64..127 (lo)
+  if (ok && !first) {
+    float* lo_rows = reinterpret_cast<float*>(smem + kTrainR);  // 64 rows x 16 columns
+    const int out_rows[5] = {kHid, kHid, kHid, kHid, kOut};
+    const int width[5] = {kIn, kHid, kHid, kHid, kHid};
+    const int woff[5] = {kOffW0, kOffW1, kOffW2, kOffW3, kOffW4};
+    const uint32_t col[5] = {kColDW0, kColDW1, kColDW2, kColDW3, kColDW4};
     const float inv_count = 1.0f / (3.0f * (float)n);
-#pragma unroll
-    for (int c = 0; c < kOut; ++c) {
-      float z = 0.0f;
-#pragma unroll
-      for (int i = 0; i < kHid; ++i) z = fmaf(w4[c * kHid + i], hv[i], z);
-      const float p = dm::exp_(z), tg = targets[3 * (size_t)s + c];
-      const float den = p * p + 0.01f;
-      loss += (p - tg) * (p - tg) / den;
-      dy[c] = 2.0f * (p - tg) / den * p * inv_count;
-      d4[4 * (size_t)s + c] = dy[c];
-    }
-    d4[4 * (size_t)s + 3] = 0.0f;
-#pragma unroll
-    for (int i = 0; i < kHid; ++i) {
-      float a = 0.0f;
-#pragma unroll
-      for (int c = 0; c < kOut; ++c) a = fmaf(w4[c * kHid + i], dy[c], a);
-      d3[(size_t)s * kHid + i] = hv[i] > 0.0f ? a : 0.0f;
-    }
+    for (int l = 0; l < 5; ++l)
+      for (int c0 = 0; c0 < width[l]; c0 += 16) {
+        float v[16];
+        tmem_ld16(lane_addr + col[l] + c0, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (t >= kHid)
+          for (int i = 0; i < 16; ++i) lo_rows[(t - kHid) * 16 + i] = v[i];
+        __syncthreads();
+        if (t < out_rows[l])
+          for (int i = 0; i < 16; ++i)
+            atomicAdd(grad + woff[l] + t * width[l] + c0 + i, (v[i] + lo_rows[t * 16 + i]) * inv_count);
+        __syncthreads();
+      }
   }
   for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(loss_sum, loss);
+  if ((t & 31) == 0 && loss != 0.0f) atomicAdd(loss_sum, loss);
+  if (!ok && t == 0) atomicExch(err, 1u);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
-// Adam on the FP32 master weights, then the FP16-rounded FP32 copy used by
-// training and the packed FP16 tensor-core operands.
+// Adam on the FP32 master weights, then the packed FP16 tensor-core operands
+// (forward, and transposed for the backward pass).
 __global__ void k_rc_adam(float* __restrict__ master, float* __restrict__ m1, float* __restrict__ m2,
                           const float* __restrict__ grad, float lr, float b1, float b2, float eps, float c1, float c2,
-                          int update, float* __restrict__ wf, __half* __restrict__ packed) {
+                          int update, __half* __restrict__ packed) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= kNumParams) return;
   float w = master[p];
@@ -460,12 +626,17 @@ __global__ void k_rc_adam(float* __restrict__ master, float* __restrict__ m1, fl
     master[p] = w;
   }
   const __half hw = __float2half_rn(w);
-  wf[p] = __half2float(hw);
   int row, k, K, base;
   if (p < kOffW1) { row = p / kIn; k = p % kIn; K = kIn; base = kPackW0; }
   else if (p < kOffW4) { int q = p - kOffW1; int l = q / (kHid * kHid); q %= kHid * kHid; row = q / kHid; k = q % kHid; K = kHid; base = kPackW1 + l * kHid * kHid; }
   else { int q = p - kOffW4; row = q / kHid; k = q % kHid; K = kHid; base = kPackW4; }
   packed[base + core_offset(row, k, K)] = hw;
+  if (p >= kOffW1 && p < kOffW4) {  // W_l^T: row = input k, K index = output row
+    const int l = (p - kOffW1) / (kHid * kHid);
+    packed[kPackT1 + l * kHid * kHid + core_offset(k, row, kHid)] = hw;
+  } else if (p >= kOffW4) {
+    packed[kPackT4 + core_offset(k, row, kOutPad)] = hw;
+  }
 }
 
 struct Cache {
@@ -473,13 +644,13 @@ struct Cache {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   RcBounds bounds{};
-  float *master = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr, *wf = nullptr, *loss = nullptr;
+  float *master = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr, *loss = nullptr;
   uint32_t* count = nullptr;  // sample count of host-submitted batches
   __half* packed = nullptr;
   uint32_t* err = nullptr;
   int step = 0;
   // batch buffers
-  float *h = nullptr, *d = nullptr, *targets = nullptr;
+  float* targets = nullptr;
   float4* queries = nullptr;
   float* out = nullptr;
   uint32_t cap = 0;
@@ -499,14 +670,12 @@ int cuda_ok(Cache* c, cudaError_t e, const char* what) {
 
 int ensure_batch(Cache* c, uint32_t n) {
   if (n <= c->cap) return AP_OK;
-  cudaFree(c->h); cudaFree(c->d); cudaFree(c->targets); cudaFree(c->queries); cudaFree(c->out);
-  c->h = c->d = c->targets = c->out = nullptr;
+  cudaFree(c->targets); cudaFree(c->queries); cudaFree(c->out);
+  c->targets = c->out = nullptr;
   c->queries = nullptr;
   c->cap = 0;
   int rc;
-  if ((rc = cuda_ok(c, cudaMalloc(&c->h, (size_t)n * (kIn + 4 * kHid) * 4), "batch")) ||
-      (rc = cuda_ok(c, cudaMalloc(&c->d, (size_t)n * (4 * kHid + 4) * 4), "batch")) ||
-      (rc = cuda_ok(c, cudaMalloc(&c->targets, (size_t)n * 12), "batch")) ||
+  if ((rc = cuda_ok(c, cudaMalloc(&c->targets, (size_t)n * 12), "batch")) ||
       (rc = cuda_ok(c, cudaMalloc(&c->queries, (size_t)n * 64), "batch")) ||
       (rc = cuda_ok(c, cudaMalloc(&c->out, (size_t)n * 12), "batch")))
     return rc;
@@ -517,7 +686,7 @@ int ensure_batch(Cache* c, uint32_t n) {
 // Refreshes the FP16 copies from the master weights (no update).
 void repack(Cache* c) {
   k_rc_adam<<<(kNumParams + 255) / 256, 256, 0, c->stream>>>(c->master, c->m1, c->m2, c->grad, 0.0f, 0.9f, 0.999f, 1e-8f,
-                                                               1.0f, 1.0f, 0, c->wf, c->packed);
+                                                               1.0f, 1.0f, 0, c->packed);
 }
 
 }  // namespace
@@ -563,34 +732,16 @@ int rc_train_device(void* cp, const float4* queries, const float* targets, const
   }
   cudaMemsetAsync(c->grad, 0, kNumParams * 4, st);
   cudaMemsetAsync(c->loss, 0, 4, st);
-  const size_t S = cap;
-  float* H[5] = {c->h, c->h + S * kIn, c->h + S * (kIn + kHid), c->h + S * (kIn + 2 * kHid), c->h + S * (kIn + 3 * kHid)};
-  float* D[5] = {c->d, c->d + S * kHid, c->d + S * 2 * kHid, c->d + S * 3 * kHid, c->d + S * 4 * kHid};
-  const int woff[5] = {kOffW0, kOffW1, kOffW2, kOffW3, kOffW4};
-  const int width[5] = {kIn, kHid, kHid, kHid, kHid};
-  const int mt = (int)((cap + 63) / 64);
-  k_rc_encode_batch<<<(cap + 127) / 128, 128, 0, st>>>(queries, n_dev, cap, c->bounds, H[0]);
-  for (int l = 0; l < 4; ++l)  // H_{l+1} = fp16(relu(H_l W_l^T))
-    k_sgemm<false, true, EPI_RELU_H16><<<dim3(1, mt, 1), 256, 0, st>>>((int)cap, kHid, width[l], H[l], width[l],
-                                                                      c->wf + woff[l], width[l], H[l + 1], kHid, nullptr, 0,
-                                                                      n_dev, cap, 0);
-  k_rc_loss<<<(cap + 127) / 128, 128, 0, st>>>(c->wf, H[4], targets, n_dev, cap, D[4], D[3], c->loss);
-  for (int l = 2; l >= 0; --l)  // D_l = (D_{l+1} W_{l+1}) * [H_{l+1} > 0]
-    k_sgemm<false, false, EPI_MASK><<<dim3(1, mt, 1), 256, 0, st>>>((int)cap, kHid, kHid, D[l + 1], kHid,
-                                                                   c->wf + woff[l + 1], kHid, D[l], kHid, H[l + 1], kHid,
-                                                                   n_dev, cap, 0);
-  const int kchunk = 512, splits = (int)((cap + kchunk - 1) / kchunk);
-  for (int l = 0; l < 5; ++l) {  // dW_l = D_l^T H_l (sum over samples)
-    const int M = l == 4 ? kOut : kHid, N = width[l], lda = l == 4 ? 4 : kHid;
-    k_sgemm<true, false, EPI_ATOMIC><<<dim3((N + 63) / 64, 1, splits), 256, 0, st>>>(
-        M, N, (int)cap, D[l], lda, H[l], N, c->grad + woff[l], N, nullptr, 0, n_dev, cap, kchunk);
-  }
+  const int tiles = (int)((cap + kTile - 1) / kTile);
+  const int grid = tiles < c->num_sms ? tiles : c->num_sms;
+  k_rc_train_tc<<<grid, kTile, kSmemTrain, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, targets, n_dev,
+                                                  cap, c->bounds, c->grad, c->loss, c->err);
   if (update) {
     c->step += 1;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.0f - (float)std::pow(0.9, c->step), c2 = 1.0f - (float)std::pow(0.999, c->step);
     k_rc_adam<<<(kNumParams + 255) / 256, 256, 0, st>>>(c->master, c->m1, c->m2, c->grad, lr, b1, b2, 1e-8f, c1, c2, 1,
-                                                        c->wf, c->packed);
+                                                        c->packed);
   }
   rc = cuda_ok(c, cudaGetLastError(), "radiance cache training");
   if (rc && !c->pending) c->pending = rc;
@@ -626,13 +777,14 @@ void* ap_rc_create(int device, const float* scene_lo, const float* scene_hi, uin
       (rc = ap::cuda_ok(c, cudaMalloc(&c->m1, ap::kNumParams * 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->m2, ap::kNumParams * 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->grad, ap::kNumParams * 4), "params")) ||
-      (rc = ap::cuda_ok(c, cudaMalloc(&c->wf, ap::kNumParams * 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->loss, 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->err, 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->count, 4), "params")) ||
-      (rc = ap::cuda_ok(c, cudaMalloc(&c->packed, ap::kPackHalves * 2), "params")) ||
+      (rc = ap::cuda_ok(c, cudaMalloc(&c->packed, ap::kPackAllHalves * 2), "params")) ||
       (rc = ap::cuda_ok(c, cudaFuncSetAttribute(ap::k_rc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                ap::kSmemInfer), "smem"))) {
+                                                ap::kSmemInfer), "smem")) ||
+      (rc = ap::cuda_ok(c, cudaFuncSetAttribute(ap::k_rc_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                ap::kSmemTrain), "smem"))) {
     if (err) *err = rc;
     ap_rc_destroy(c);
     return nullptr;
@@ -660,7 +812,7 @@ void ap_rc_destroy(void* cp) {
   if (!c) return;
   ap::DeviceScope device_scope(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->wf, c->loss, c->err, c->count, c->packed, c->h, c->d, c->targets,
+  void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->loss, c->err, c->count, c->packed, c->targets,
                   c->queries, c->out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -696,7 +848,7 @@ int ap_rc_set_params(void* cp, const float* params, uint32_t count) {
     return rc;
   cudaMemsetAsync(c->m1, 0, ap::kNumParams * 4, c->stream);
   cudaMemsetAsync(c->m2, 0, ap::kNumParams * 4, c->stream);
-  cudaMemsetAsync(c->packed, 0, ap::kPackHalves * 2, c->stream);
+  cudaMemsetAsync(c->packed, 0, ap::kPackAllHalves * 2, c->stream);
   c->step = 0;
   ap::repack(c);
   return ap::cuda_ok(c, cudaStreamSynchronize(c->stream), "params");
