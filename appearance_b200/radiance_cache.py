@@ -70,3 +70,45 @@ class RadianceCache:
         self._check(self._lib.ap_rc_train(self._c, _p(q), _p(t), q.shape[0], lr, 1 if update else 0,
                                           ctypes.byref(loss), None if g is None else _p(g)))
         return loss.value, g
+
+
+def random_queries(n: int, seed: int, lo=(-1.0, -1.0, -1.0), hi=(11.0, 11.0, 11.0)) -> np.ndarray:
+    """n seeded query records (16 floats each): positions uniform in the box,
+    roughness in [0.05, 1], unit directions, albedos in [0, 1]."""
+    rng = np.random.default_rng(seed)
+    q = np.zeros((n, QUERY_FLOATS), np.float32)
+    q[:, 0:3] = rng.uniform(lo, hi, (n, 3))
+    q[:, 3] = rng.uniform(0.05, 1.0, n)
+    d = rng.normal(size=(n, 3))
+    q[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    q[:, 8:14] = rng.uniform(0.0, 1.0, (n, 6))
+    return q
+
+
+def _bench_cli(argv=None):
+    """Runs inference over --infer queries (--infer-calls times) and --steps
+    training steps of --train samples on seeded random queries: the fixed
+    command that profiler captures of the cache's kernels run."""
+    import argparse
+
+    ap = argparse.ArgumentParser(prog="python -m appearance_b200.radiance_cache")
+    ap.add_argument("--infer", type=int, default=1 << 19)
+    ap.add_argument("--infer-calls", type=int, default=3)
+    ap.add_argument("--train", type=int, default=1 << 16)
+    ap.add_argument("--steps", type=int, default=4)
+    a = ap.parse_args(argv)
+    lo, hi = np.array([-1.0] * 3, np.float32), np.array([11.0] * 3, np.float32)
+    rc = RadianceCache(lo, hi, seed=3)
+    q = random_queries(a.infer, 77)
+    for _ in range(a.infer_calls):
+        rc.infer(q)
+    qt = random_queries(a.train, 5)
+    t = np.random.default_rng(8).uniform(0.0, 3.0, (a.train, 3)).astype(np.float32)
+    for _ in range(a.steps):
+        loss, _ = rc.train(qt, t, lr=1e-3)
+        print(f"train loss {loss:.6f}", flush=True)
+    rc.close()
+
+
+if __name__ == "__main__":
+    _bench_cli()
