@@ -11,12 +11,12 @@
 // roughness, diffuse albedo (3), specular albedo (3).
 //
 // Inference (k_rc_infer) runs on the 5th-generation tensor cores: one CTA of
-// 128 threads holds all weights in shared memory in the K-major core-matrix
-// layout, encodes 128 queries into shared memory, and for each layer one
-// thread issues tcgen05.mma (M=128, N=64 or 16, K=16 per instruction) with the
-// FP32 accumulator in tensor memory; every warp reads its 32 rows back with
-// tcgen05.ld, applies ReLU, rounds to FP16 and writes the next layer's
-// operand.  Training (k_rc_train_tc) runs forward and backward on the tensor
+// 256 threads (two per query row) holds all weights in shared memory in the
+// K-major core-matrix layout, encodes 128 queries into shared memory, and for
+// each layer one thread issues tcgen05.mma (M=128, N=64 or 16, K=16 per
+// instruction) with the FP32 accumulator in tensor memory; the warps read
+// their rows back with tcgen05.ld (each thread half of a row's columns),
+// apply ReLU, round to FP16 and write the next layer's operand.  Training (k_rc_train_tc) runs forward and backward on the tensor
 // cores in one kernel per step, tile by tile with the weight-gradient sums in
 // tensor memory; k_rc_adam updates the FP32 master weights and repacks the
 // FP16 operands (forward and transposed).
@@ -80,10 +80,34 @@ struct RcBounds {
 // double-angle recurrence from o = 0.  Each one-blob bin i holds
 // exp(-0.5 c_i^2), c_i = (v - (i + 0.5)/32) * 32; only the 13 bins around the
 // peak are evaluated (written after zeroing all 32): farther bins are below
-// half the smallest FP16 subnormal, so their FP16 value is 0 either way.
-template <class Sink>
-APD void rc_encode(const float* q, const RcBounds& b, Sink sink) {
+// half the smallest FP16 subnormal, so their FP16 value is 0 either way.  The
+// elementary functions are the deterministic ones the oracle's encoding uses,
+// so the FP16 features match it bit for bit (hardware-rate functions flip
+// enough FP16 roundings to move the weight gradients by ~1e-3).
+// rc_encode_part<0> writes the position features and the material tail
+// (80 features), rc_encode_part<1> the two one-blobs (64), so that two
+// threads can share one query's encoding; rc_encode writes all of them.
+template <int kPart, class Sink>
+APD void rc_encode_part(const float* q, const RcBounds& b, Sink sink) {
   const float kPi = 3.14159265358979323846f;
+  if (kPart == 1) {
+    const float v[2] = {dm::acos_(dm::clamp(q[6], -1.0f, 1.0f)) * (1.0f / kPi),
+                        dm::atan2_(q[5], q[4]) * (0.5f / kPi) + 0.5f};
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) sink(72 + 32 * j + i, 0.0f);
+      const int b0 = min(max((int)floorf(v[j] * 32.0f), 0), 31);
+#pragma unroll
+      for (int w = -6; w <= 6; ++w) {
+        const int i = b0 + w;
+        if (i < 0 || i > 31) continue;
+        const float ci = (v[j] - ((float)i + 0.5f) * (1.0f / 32.0f)) * 32.0f;
+        sink(72 + 32 * j + i, dm::exp_(-0.5f * ci * ci));
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const float x = (q[a] - b.lo[a]) * b.inv[a];
@@ -98,21 +122,6 @@ APD void rc_encode(const float* q, const RcBounds& b, Sink sink) {
       c = c2;
     }
   }
-  const float v[2] = {dm::acos_(dm::clamp(q[6], -1.0f, 1.0f)) * (1.0f / kPi),
-                      dm::atan2_(q[5], q[4]) * (0.5f / kPi) + 0.5f};
-#pragma unroll
-  for (int j = 0; j < 2; ++j) {
-#pragma unroll
-    for (int i = 0; i < 32; ++i) sink(72 + 32 * j + i, 0.0f);
-    const int b0 = min(max((int)floorf(v[j] * 32.0f), 0), 31);
-#pragma unroll
-    for (int w = -6; w <= 6; ++w) {
-      const int i = b0 + w;
-      if (i < 0 || i > 31) continue;
-      const float ci = (v[j] - ((float)i + 0.5f) * (1.0f / 32.0f)) * 32.0f;
-      sink(72 + 32 * j + i, dm::exp_(-0.5f * ci * ci));
-    }
-  }
   sink(136, q[3]);
   sink(137, q[8]);
   sink(138, q[9]);
@@ -121,6 +130,12 @@ APD void rc_encode(const float* q, const RcBounds& b, Sink sink) {
   sink(141, q[12]);
   sink(142, q[13]);
   sink(143, 0.0f);
+}
+
+template <class Sink>
+APD void rc_encode(const float* q, const RcBounds& b, Sink sink) {
+  rc_encode_part<0>(q, b, sink);
+  rc_encode_part<1>(q, b, sink);
 }
 
 APD float h16(float x) { return __half2float(__float2half_rn(x)); }
@@ -208,10 +223,13 @@ APD void store_row8(__half* base, int row, int k0, int K, const float* v) {
 // from tensor memory.  Hidden layers write fp16(relu(.)) as the next layer's
 // A operand; the last writes exp() of the 3 outputs.  Returns false (on every
 // thread) when the MMA completion wait timed out.
+// Two threads share each query row: `half` 0 takes the first half of a hidden
+// layer's columns (and the outputs), half 1 the second; their warps read the
+// same tensor-memory lane quarter.
 template <int K, int N, bool kLast>
-APD bool rc_layer(uint32_t tmem, uint32_t bar, uint32_t& phase, uint32_t a_base, uint32_t b_base, __half* dst, int t,
-                  uint32_t row, uint32_t n, float* out) {
-  if (t == 0) {
+APD bool rc_layer(uint32_t tmem, uint32_t bar, uint32_t& phase, uint32_t a_base, uint32_t b_base, __half* dst, int tid,
+                  int t, int half, uint32_t row, uint32_t n, float* out) {
+  if (tid == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     constexpr uint32_t sbo = (uint32_t)(K / 8) * 128;
 #pragma unroll
@@ -224,22 +242,27 @@ APD bool rc_layer(uint32_t tmem, uint32_t bar, uint32_t& phase, uint32_t a_base,
   phase ^= 1u;
   if (__syncthreads_or(bad)) return false;
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t taddr = tmem + ((uint32_t)((t >> 5) * 32) << 16);
-  float v[N];
-#pragma unroll
-  for (int c = 0; c < N; c += 16) tmem_ld16(taddr + c, v + c);
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  const uint32_t taddr = tmem + ((uint32_t)(((tid >> 5) & 3) * 32) << 16);
   if (!kLast) {
+    constexpr int kCols = N / 2;
+    float v[kCols];
 #pragma unroll
-    for (int k = 0; k < N; k += 8) {
+    for (int c = 0; c < kCols; c += 16) tmem_ld16(taddr + half * kCols + c, v + c);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < kCols; k += 8) {
       float r[8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) r[i] = fmaxf(v[k + i], 0.0f);
-      store_row8(dst, t, k, N, r);
+      store_row8(dst, t, half * kCols + k, N, r);
     }
-  } else if (row < n) {
+  } else if (half == 0) {
+    float v[16];
+    tmem_ld16(taddr, v);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (row < n)
 #pragma unroll
-    for (int c = 0; c < kOut; ++c) out[3 * (size_t)row + c] = dm::exp_(v[c]);
+      for (int c = 0; c < kOut; ++c) out[3 * (size_t)row + c] = dm::exp_(v[c]);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -247,7 +270,7 @@ APD bool rc_layer(uint32_t tmem, uint32_t bar, uint32_t& phase, uint32_t a_base,
   return true;
 }
 
-__global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__ packed, const float4* __restrict__ queries,
+__global__ void __launch_bounds__(2 * kTile, 1) k_rc_infer(const uint4* __restrict__ packed, const float4* __restrict__ queries,
                                                        uint32_t n, RcBounds bounds, float* __restrict__ out,
                                                        uint32_t* __restrict__ err, const uint32_t* __restrict__ n_dev) {
   if (n_dev) n = min(n, *n_dev);  // a query count produced on the device (at most n)
@@ -256,9 +279,10 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__
   __half* act = reinterpret_cast<__half*>(smem + kSmemWeights);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kSmemWeights + kSmemAct);
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(smem + kSmemWeights + kSmemAct + 8);
-  const int t = threadIdx.x, warp = t >> 5;
-  for (int i = t; i < kSmemWeights / 16; i += kTile) reinterpret_cast<uint4*>(smem)[i] = packed[i];
-  if (t == 0) {
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int t = tid & (kTile - 1), half = tid >> 7;  // the query row, and which half of it
+  for (int i = tid; i < kSmemWeights / 16; i += 2 * kTile) reinterpret_cast<uint4*>(smem)[i] = packed[i];
+  if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -289,21 +313,23 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__
           float4 v = queries[4 * (size_t)row + i];
           q[4 * i] = v.x; q[4 * i + 1] = v.y; q[4 * i + 2] = v.z; q[4 * i + 3] = v.w;
         }
-        rc_encode(q, bounds, [&](int k, float x) { act[core_offset(t, k, kIn)] = __float2half_rn(x); });
-      } else {
+        auto sink = [&](int k, float x) { act[core_offset(t, k, kIn)] = __float2half_rn(x); };
+        if (half == 0) rc_encode_part<0>(q, bounds, sink);
+        else rc_encode_part<1>(q, bounds, sink);
+      } else if (half == 0) {
 #pragma unroll
         for (int k = 0; k < kIn; k += 8) *reinterpret_cast<uint4*>(act + core_offset(t, k, kIn)) = make_uint4(0, 0, 0, 0);
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    ok = rc_layer<kIn, kHid, false>(tmem, bar_a, phase, act_a, w_a + kPackW0 * 2, h0, t, row, n, out) &&
-         rc_layer<kHid, kHid, false>(tmem, bar_a, phase, h0_a, w_a + kPackW1 * 2, h1, t, row, n, out) &&
-         rc_layer<kHid, kHid, false>(tmem, bar_a, phase, h1_a, w_a + kPackW2 * 2, h0, t, row, n, out) &&
-         rc_layer<kHid, kHid, false>(tmem, bar_a, phase, h0_a, w_a + kPackW3 * 2, h1, t, row, n, out) &&
-         rc_layer<kHid, kOutPad, true>(tmem, bar_a, phase, h1_a, w_a + kPackW4 * 2, nullptr, t, row, n, out);
+    ok = rc_layer<kIn, kHid, false>(tmem, bar_a, phase, act_a, w_a + kPackW0 * 2, h0, tid, t, half, row, n, out) &&
+         rc_layer<kHid, kHid, false>(tmem, bar_a, phase, h0_a, w_a + kPackW1 * 2, h1, tid, t, half, row, n, out) &&
+         rc_layer<kHid, kHid, false>(tmem, bar_a, phase, h1_a, w_a + kPackW2 * 2, h0, tid, t, half, row, n, out) &&
+         rc_layer<kHid, kHid, false>(tmem, bar_a, phase, h0_a, w_a + kPackW3 * 2, h1, tid, t, half, row, n, out) &&
+         rc_layer<kHid, kOutPad, true>(tmem, bar_a, phase, h1_a, w_a + kPackW4 * 2, nullptr, tid, t, half, row, n, out);
   }
-  if (!ok && t == 0) atomicExch(err, 1u);
+  if (!ok && tid == 0) atomicExch(err, 1u);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
@@ -311,11 +337,11 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_infer(const uint4* __restrict__
 
 // ---- training on the tensor cores -------------------------------------------
 //
-// k_rc_train_tc: one CTA of 128 threads takes whole 128-sample tiles.  Per
-// tile it runs the forward layers as k_rc_infer does, keeping each hidden
-// activation (the next layer's operand) and its transpose (an operand of the
-// weight gradient), then the loss and its gradient per sample, then the
-// backward layers:
+// k_rc_train_tc: one CTA of 256 threads (two per sample row) takes whole
+// 128-sample tiles.  Per tile it runs the forward layers as k_rc_infer does,
+// keeping each hidden activation (the next layer's operand) and its
+// transpose (an operand of the weight gradient), then the loss and its
+// gradient per sample, then the backward layers:
 //   dH_l = dZ_l W_l       M = 128 samples, N = the layer's inputs, K = its
 //                         outputs (B = the packed W_l^T);
 //   dW_l += dZ_l^T H_l    M = 128 rows, N = the layer's inputs, K = the tile's
@@ -378,10 +404,16 @@ APD bool mmas_done(uint32_t bar, uint32_t& phase, int t) {
   return !any_bad;
 }
 
-// The 64 columns of the layer accumulator in this thread's row.
-APD void layer_row(uint32_t lane_addr, float* v) {
+// Two threads share each sample row: `half` 0 takes the first 32 columns of
+// a 64-wide layer, half 1 the other 32 (their warps read the same tensor-
+// memory lane quarter).
+constexpr int kTrainThreads = 2 * kTile;
+constexpr int kHalfCols = kHid / 2;
+
+// This thread's 32 columns of the layer accumulator, in its row.
+APD void layer_row(uint32_t lane_addr, int half, float* v) {
 #pragma unroll
-  for (int c = 0; c < kHid; c += 16) tmem_ld16(lane_addr + kColLayer + c, v + c);
+  for (int c = 0; c < kHalfCols; c += 16) tmem_ld16(lane_addr + kColLayer + half * kHalfCols + c, v + c);
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
@@ -391,35 +423,37 @@ APD void store_row8h(__half* base, int row, int k0, int K, const __half* h) {
 
 // Forward epilogue of a hidden layer: H = fp16(relu(acc)) as the next layer's
 // A operand (row t of `next`) and into column t of its transpose `ht`.
-APD void train_fwd_epilogue(uint32_t lane_addr, __half* next, __half* ht, int t) {
-  float v[kHid];
-  layer_row(lane_addr, v);
+APD void train_fwd_epilogue(uint32_t lane_addr, __half* next, __half* ht, int t, int half) {
+  float v[kHalfCols];
+  layer_row(lane_addr, half, v);
 #pragma unroll
-  for (int k = 0; k < kHid; k += 8) {
+  for (int k = 0; k < kHalfCols; k += 8) {
     __align__(16) __half h[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       h[i] = __float2half_rn(fmaxf(v[k + i], 0.0f));
-      ht[core_offset(k + i, t, kTile)] = h[i];
+      ht[core_offset(half * kHalfCols + k + i, t, kTile)] = h[i];
     }
-    store_row8h(next, t, k, kHid, h);
+    store_row8h(next, t, half * kHalfCols + k, kHid, h);
   }
 }
 
 // Backward epilogue: dZ = dH * [H > 0] from the layer accumulator and the
 // mask of ht (H's transpose); hi / lo rows into dz_hi / dz_lo (when given) and
 // columns into [dZ^T hi; dZ^T lo].
-APD void train_bwd_epilogue(uint32_t lane_addr, const __half* ht, __half* dz_hi, __half* dz_lo, __half* dzt, int t) {
-  float v[kHid];
-  layer_row(lane_addr, v);
+APD void train_bwd_epilogue(uint32_t lane_addr, const __half* ht, __half* dz_hi, __half* dz_lo, __half* dzt, int t,
+                               int half) {
+  float v[kHalfCols];
+  layer_row(lane_addr, half, v);
 #pragma unroll
-  for (int k = 0; k < kHid; k += 8) {
+  for (int k0 = 0; k0 < kHalfCols; k0 += 8) {
+    const int k = half * kHalfCols + k0;
     __align__(16) __half hi[8];
     __align__(16) __half lo[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       const int c = k + i;
-      const float x = __half2float(ht[core_offset(c, t, kTile)]) > 0.0f ? v[c] : 0.0f;
+      const float x = __half2float(ht[core_offset(c, t, kTile)]) > 0.0f ? v[k0 + i] : 0.0f;
       split_half(x, &hi[i], &lo[i]);
       dzt[core_offset(c, t, kTile)] = hi[i];
       dzt[core_offset(kHid + c, t, kTile)] = lo[i];
@@ -431,7 +465,7 @@ APD void train_bwd_epilogue(uint32_t lane_addr, const __half* ht, __half* dz_hi,
   }
 }
 
-__global__ void __launch_bounds__(kTile, 1) k_rc_train_tc(const uint4* __restrict__ packed,
+__global__ void __launch_bounds__(kTrainThreads, 1) k_rc_train_tc(const uint4* __restrict__ packed,
                                                           const float4* __restrict__ queries,
                                                           const float* __restrict__ targets,
                                                           const uint32_t* __restrict__ n_dev, uint32_t cap,
@@ -439,11 +473,12 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_train_tc(const uint4* __restric
                                                           float* __restrict__ loss_sum, uint32_t* __restrict__ err) {
   const uint32_t n = min(*n_dev, cap);
   extern __shared__ __align__(1024) unsigned char smem[];
-  const int t = threadIdx.x, warp = t >> 5;
-  for (int i = t; i < kPackAllHalves / 8; i += kTile) reinterpret_cast<uint4*>(smem)[i] = packed[i];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int t = tid & (kTile - 1), half = tid >> 7;  // the sample row, and which half of it
+  for (int i = tid; i < kPackAllHalves / 8; i += kTrainThreads) reinterpret_cast<uint4*>(smem)[i] = packed[i];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTrainBar);
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(smem + kTrainBar + 8);
-  if (t == 0) {
+  if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -456,7 +491,7 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_train_tc(const uint4* __restric
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_holder;
-  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const uint32_t bar_a = smem_u32(bar);
   const uint32_t w_a = smem_u32(smem), r_a = smem_u32(smem + kTrainR), dzt_a = smem_u32(smem + kTrainDZT);
   __half* r = reinterpret_cast<__half*>(smem + kTrainR);
@@ -488,33 +523,37 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_train_tc(const uint4* __restric
         const float4 v = queries[4 * (size_t)row + i];
         q[4 * i] = v.x; q[4 * i + 1] = v.y; q[4 * i + 2] = v.z; q[4 * i + 3] = v.w;
       }
-      rc_encode(q, bounds, [&](int k, float x) { r[core_offset(t, k, kIn)] = __float2half_rn(x); });
-    } else {
+      auto sink = [&](int k, float x) { r[core_offset(t, k, kIn)] = __float2half_rn(x); };
+      if (half == 0) rc_encode_part<0>(q, bounds, sink);
+      else rc_encode_part<1>(q, bounds, sink);
+    } else if (half == 0) {
 #pragma unroll
       for (int k = 0; k < kIn; k += 8) *reinterpret_cast<uint4*>(r + core_offset(t, k, kIn)) = make_uint4(0, 0, 0, 0);
     }
     // forward: H1 .. H4
     operands_ready();
-    if (t == 0) mma_steps(tmem + kColLayer, r_a, sbo144, w_a + kPackW0 * 2, sbo144, kIn / 16, id64, false);
-    if (!(ok = mmas_done(bar_a, phase, t))) break;
-    train_fwd_epilogue(lane_addr, p0, ht[0], t);
+    if (tid == 0) mma_steps(tmem + kColLayer, r_a, sbo144, w_a + kPackW0 * 2, sbo144, kIn / 16, id64, false);
+    if (!(ok = mmas_done(bar_a, phase, tid))) break;
+    train_fwd_epilogue(lane_addr, p0, ht[0], t, half);
     operands_ready();
-    if (t == 0) mma_steps(tmem + kColLayer, p0_a, sbo64, w_a + kPackW1 * 2, sbo64, kHid / 16, id64, false);
-    if (!(ok = mmas_done(bar_a, phase, t))) break;
-    train_fwd_epilogue(lane_addr, p1, ht[1], t);
+    if (tid == 0) mma_steps(tmem + kColLayer, p0_a, sbo64, w_a + kPackW1 * 2, sbo64, kHid / 16, id64, false);
+    if (!(ok = mmas_done(bar_a, phase, tid))) break;
+    train_fwd_epilogue(lane_addr, p1, ht[1], t, half);
     operands_ready();
-    if (t == 0) mma_steps(tmem + kColLayer, p1_a, sbo64, w_a + kPackW2 * 2, sbo64, kHid / 16, id64, false);
-    if (!(ok = mmas_done(bar_a, phase, t))) break;
-    train_fwd_epilogue(lane_addr, p0, ht[2], t);
+    if (tid == 0) mma_steps(tmem + kColLayer, p1_a, sbo64, w_a + kPackW2 * 2, sbo64, kHid / 16, id64, false);
+    if (!(ok = mmas_done(bar_a, phase, tid))) break;
+    train_fwd_epilogue(lane_addr, p0, ht[2], t, half);
     operands_ready();
-    if (t == 0) mma_steps(tmem + kColLayer, p0_a, sbo64, w_a + kPackW3 * 2, sbo64, kHid / 16, id64, false);
-    if (!(ok = mmas_done(bar_a, phase, t))) break;
-    train_fwd_epilogue(lane_addr, p1, ht[3], t);
+    if (tid == 0) mma_steps(tmem + kColLayer, p0_a, sbo64, w_a + kPackW3 * 2, sbo64, kHid / 16, id64, false);
+    if (!(ok = mmas_done(bar_a, phase, tid))) break;
+    train_fwd_epilogue(lane_addr, p1, ht[3], t, half);
     operands_ready();
-    if (t == 0) mma_steps(tmem + kColLayer, p1_a, sbo64, w_a + kPackW4 * 2, sbo64, kHid / 16, id16, false);
-    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    if (tid == 0) mma_steps(tmem + kColLayer, p1_a, sbo64, w_a + kPackW4 * 2, sbo64, kHid / 16, id16, false);
+    if (!(ok = mmas_done(bar_a, phase, tid))) break;
     // output layer: loss and its gradient per sample (without the 1 / (3n))
-    {
+    for (int i = tid; i < 2 * kHid * kTile / 8; i += kTrainThreads) reinterpret_cast<uint4*>(dzt)[i] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    if (half == 0) {
       float v[16];
       tmem_ld16(lane_addr + kColLayer, v);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
@@ -539,8 +578,6 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_train_tc(const uint4* __restric
       __half* dy_lo = p0 + kTile * kOutPad;    // dY lo rows
       store_row8h(dy_lo, t, 0, kOutPad, lo);
       store_row8h(dy_lo, t, 8, kOutPad, lo + 8);
-      for (int i = t; i < 2 * kHid * kTile / 8; i += kTile) reinterpret_cast<uint4*>(dzt)[i] = make_uint4(0, 0, 0, 0);
-      __syncthreads();
 #pragma unroll
       for (int c = 0; c < kOut; ++c) {
         dzt[core_offset(c, t, kTile)] = hi[c];
@@ -549,52 +586,60 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_train_tc(const uint4* __restric
     }
     // backward: layer 4, then 3 .. 1
     operands_ready();
-    if (t == 0) {
+    if (tid == 0) {
       mma_steps(tmem + kColDW4, dzt_a, sbo_s, ht_a[3], sbo_s, kTile / 16, id64, !first);
       mma_steps(tmem + kColLayer, p0_a, sbo16, wt_a[4], sbo16, 1, id64, false);
       mma_steps(tmem + kColLayer, p0_a + kTile * kOutPad * 2, sbo16, wt_a[4], sbo16, 1, id64, true);
     }
-    if (!(ok = mmas_done(bar_a, phase, t))) break;
-    train_bwd_epilogue(lane_addr, ht[3], p0, p1, dzt, t);  // dZ3
+    if (!(ok = mmas_done(bar_a, phase, tid))) break;
+    train_bwd_epilogue(lane_addr, ht[3], p0, p1, dzt, t, half);  // dZ3
     const uint32_t dw_col[4] = {kColDW0, kColDW1, kColDW2, kColDW3};
     for (int l = 3; l >= 1; --l) {
       operands_ready();
-      if (t == 0) {
+      if (tid == 0) {
         mma_steps(tmem + dw_col[l], dzt_a, sbo_s, ht_a[l - 1], sbo_s, kTile / 16, id64, !first);
         mma_steps(tmem + kColLayer, p0_a, sbo64, wt_a[l], sbo64, kHid / 16, id64, false);
         mma_steps(tmem + kColLayer, p1_a, sbo64, wt_a[l], sbo64, kHid / 16, id64, true);
       }
-      if (!(ok = mmas_done(bar_a, phase, t))) break;
+      if (!(ok = mmas_done(bar_a, phase, tid))) break;
       // dZ_{l-1}; the last one (dZ0) only as the weight-gradient operand
-      train_bwd_epilogue(lane_addr, ht[l - 1], l > 1 ? p0 : nullptr, l > 1 ? p1 : nullptr, dzt, t);
+      train_bwd_epilogue(lane_addr, ht[l - 1], l > 1 ? p0 : nullptr, l > 1 ? p1 : nullptr, dzt, t, half);
     }
     if (!ok) break;
     // H0^T (the encoding, re-computed) for dW0 = dZ0^T H0
-    if (row < n) rc_encode(q, bounds, [&](int k, float x) { r[core_offset(k, t, kTile)] = __float2half_rn(x); });
-    else
+    if (row < n) {
+      auto sink = [&](int k, float x) { r[core_offset(k, t, kTile)] = __float2half_rn(x); };
+      if (half == 0) rc_encode_part<0>(q, bounds, sink);
+      else rc_encode_part<1>(q, bounds, sink);
+    } else if (half == 0) {
       for (int k = 0; k < kIn; ++k) r[core_offset(k, t, kTile)] = __float2half_rn(0.0f);
+    }
     operands_ready();
-    if (t == 0) mma_steps(tmem + kColDW0, dzt_a, sbo_s, r_a, sbo_s, kTile / 16, id144, !first);
-    if (!(ok = mmas_done(bar_a, phase, t))) break;
+    if (tid == 0) mma_steps(tmem + kColDW0, dzt_a, sbo_s, r_a, sbo_s, kTile / 16, id144, !first);
+    if (!(ok = mmas_done(bar_a, phase, tid))) break;
     first = false;
   }
   // weight-gradient sums -> gradient: rows 0..63 (hi) plus rows 64..127 (lo)
   if (ok && !first) {
-    float* lo_rows = reinterpret_cast<float*>(smem + kTrainR);  // 64 rows x 16 columns
+    float* lo_rows = reinterpret_cast<float*>(smem + kTrainR) + half * kHid * 16;  // 64 rows x 16 columns per half
     const int out_rows[5] = {kHid, kHid, kHid, kHid, kOut};
     const int width[5] = {kIn, kHid, kHid, kHid, kHid};
     const int woff[5] = {kOffW0, kOffW1, kOffW2, kOffW3, kOffW4};
     const uint32_t col[5] = {kColDW0, kColDW1, kColDW2, kColDW3, kColDW4};
     const float inv_count = 1.0f / (3.0f * (float)n);
     for (int l = 0; l < 5; ++l)
-      for (int c0 = 0; c0 < width[l]; c0 += 16) {
+      for (int cc = 0; cc < width[l]; cc += 32) {
+        const int c0 = cc + 16 * half;  // each half reads its own 16 columns
+        const bool mine = c0 < width[l];
         float v[16];
-        tmem_ld16(lane_addr + col[l] + c0, v);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (t >= kHid)
-          for (int i = 0; i < 16; ++i) lo_rows[(t - kHid) * 16 + i] = v[i];
+        if (mine) {
+          tmem_ld16(lane_addr + col[l] + c0, v);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (t >= kHid)
+            for (int i = 0; i < 16; ++i) lo_rows[(t - kHid) * 16 + i] = v[i];
+        }
         __syncthreads();
-        if (t < out_rows[l])
+        if (mine && t < out_rows[l])
           for (int i = 0; i < 16; ++i)
             atomicAdd(grad + woff[l] + t * width[l] + c0 + i, (v[i] + lo_rows[t * 16 + i]) * inv_count);
         __syncthreads();
@@ -602,7 +647,7 @@ __global__ void __launch_bounds__(kTile, 1) k_rc_train_tc(const uint4* __restric
   }
   for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
   if ((t & 31) == 0 && loss != 0.0f) atomicAdd(loss_sum, loss);
-  if (!ok && t == 0) atomicExch(err, 1u);
+  if (!ok && tid == 0) atomicExch(err, 1u);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
@@ -697,7 +742,7 @@ int rc_infer_device(void* cp, const float4* queries, uint32_t n, float* out, cud
   if (n == 0) return AP_OK;
   const int tiles = (int)((n + kTile - 1) / kTile);
   const int grid = tiles < 2 * c->num_sms ? tiles : 2 * c->num_sms;
-  k_rc_infer<<<grid, kTile, kSmemInfer, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, n, c->bounds, out, c->err,
+  k_rc_infer<<<grid, 2 * kTile, kSmemInfer, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, n, c->bounds, out, c->err,
                                                n_dev);
   const int rc = cuda_ok(c, cudaGetLastError(), "radiance cache inference");
   if (rc && !c->pending) c->pending = rc;
@@ -734,7 +779,7 @@ int rc_train_device(void* cp, const float4* queries, const float* targets, const
   cudaMemsetAsync(c->loss, 0, 4, st);
   const int tiles = (int)((cap + kTile - 1) / kTile);
   const int grid = tiles < c->num_sms ? tiles : c->num_sms;
-  k_rc_train_tc<<<grid, kTile, kSmemTrain, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, targets, n_dev,
+  k_rc_train_tc<<<grid, kTrainThreads, kSmemTrain, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, targets, n_dev,
                                                   cap, c->bounds, c->grad, c->loss, c->err);
   if (update) {
     c->step += 1;
