@@ -31,7 +31,7 @@ struct RayPre {
   int kx, ky, kz;
   float sx, sy, sz;
   float3 inv;          // box-test reciprocal direction (0 where the component is 0)
-  uint32_t zero_axes;  // bit k: direction component k is +-0
+  uint32_t zero_axes;  // bit k < 3: direction component k is +-0; bit 3: some component is below 2^-64
   uint32_t neg_axes;   // bit k: direction component k is negative (the far plane is entered first)
 };
 
@@ -57,6 +57,10 @@ APD RayPre ray_pre(float3 o, float3 d) {
   r.sy = comp(d, ky) / dz;
   r.sz = 1.0f / dz;
   r.zero_axes = (d.x == 0.0f ? 1u : 0u) | (d.y == 0.0f ? 2u : 0u) | (d.z == 0.0f ? 4u : 0u);
+  // bit 3: a component below 2^-64 in magnitude (zero included), for which
+  // the box test takes its exact form
+  const float kTiny = 5.42101086e-20f;  // 2^-64
+  if (!(ax >= kTiny && ay >= kTiny && az >= kTiny)) r.zero_axes |= 8u;
   r.inv = f3(d.x == 0.0f ? 0.0f : 1.0f / d.x, d.y == 0.0f ? 0.0f : 1.0f / d.y, d.z == 0.0f ? 0.0f : 1.0f / d.z);
   r.neg_axes = (r.inv.x < 0.0f ? 1u : 0u) | (r.inv.y < 0.0f ? 2u : 0u) | (r.inv.z < 0.0f ? 4u : 0u);
   return r;
@@ -116,6 +120,21 @@ APD bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float t
 // zero direction component the slab is all of t when the origin lies inside
 // the child's bounds decoded as p + q*s (rounded to nearest, which never
 // shrinks the conservatively quantised box), and empty otherwise.
+//
+// Two forms of that test.  The exact form (NodeFrame, child_entry) decodes
+// each plane byte as the float q.  The fast form (NodeFrameQ,
+// child_entry_q), taken by rays whose direction components are all at least
+// 2^-64 in magnitude (ray_pre sets bit 3 of zero_axes otherwise), decodes it
+// with one byte permute as Q = 1 + q 2^-15 (q under the exponent of 1.0 at
+// mantissa bits 15..8) and computes the slab as fma(Q, A, c) with A = 2^15 a,
+// a = s/d (exact: a power-of-two multiple, finite for |1/d| <= 2^64 and any
+// node scale below 2^49), and c = (b -+ e) - A, since Q A = A + q a exactly
+// inside the fma.  The rounding of c adds at most half an ulp of
+// |b| + e + 2^15 |a|: 2^-24 |b|, inside the 2^-19 margin, plus 2^-9 |a|, which
+// a further widening of 2^-8 |a| (1/256 of a quantum) covers.  The fast form
+// pairs the near and far planes in packed fp32 fmas (fma.rn.f32x2, the same
+// rounding per lane as a scalar fma).  Boxes of either form hold every
+// triangle the test accepts, so both give the same hits.
 struct NodeFrame {
   float px, py, pz, sxs, sys, szs;  // origin and scales of the quantisation grid
   float ax, ay, az;                 // slab = fma(q, a, b -+ e) per axis
@@ -149,6 +168,35 @@ APD NodeFrame node_frame(const uint4 w0, const RayPre& r) {
   return f;
 }
 
+// The fast form's per-node terms, paired for the packed fmas: (A_x, A_y) and
+// (A_z, A_z) multiply (near x, near y), (far x, far y) and (near z, far z).
+struct NodeFrameQ {
+  float2 axy, azz;
+  float2 cn_xy, cf_xy, c_z;  // c of the near x/y planes, the far x/y planes, near and far z
+};
+
+APD NodeFrameQ node_frame_q(const uint4 w0, const RayPre& r) {
+  NodeFrameQ f;
+  const float ax = __uint_as_float((w0.w & 0xffu) << 23) * r.inv.x;
+  const float ay = __uint_as_float(((w0.w >> 8) & 0xffu) << 23) * r.inv.y;
+  const float az = __uint_as_float(((w0.w >> 16) & 0xffu) << 23) * r.inv.z;
+  const float bx = (__uint_as_float(w0.x) - r.o.x) * r.inv.x;
+  const float by = (__uint_as_float(w0.y) - r.o.y) * r.inv.y;
+  const float bz = (__uint_as_float(w0.z) - r.o.z) * r.inv.z;
+  const float kSlack = 1.9073486e-06f;                 // 2^-19 of |b|
+  const float kSlackA = 255.0f * 1.9073486e-06f + 0.00390625f;  // 2^-19 of the extent + 2^-8 of a quantum
+  const float ex = fmaf(fabsf(ax), kSlackA, fabsf(bx) * kSlack);
+  const float ey = fmaf(fabsf(ay), kSlackA, fabsf(by) * kSlack);
+  const float ez = fmaf(fabsf(az), kSlackA, fabsf(bz) * kSlack);
+  const float Ax = ax * 32768.0f, Ay = ay * 32768.0f, Az = az * 32768.0f;
+  f.axy = make_float2(Ax, Ay);
+  f.azz = make_float2(Az, Az);
+  f.cn_xy = make_float2((bx - ex) - Ax, (by - ey) - Ay);
+  f.cf_xy = make_float2((bx + ex) - Ax, (by + ey) - Ay);
+  f.c_z = make_float2((bz - ez) - Az, (bz + ez) - Az);
+  return f;
+}
+
 constexpr float kGrow = 1.0f + 4.8e-7f;  // relative 2^-21
 
 // Byte k of `word` as a float.  Exact: the byte is placed under the exponent
@@ -156,6 +204,22 @@ constexpr float kGrow = 1.0f + 4.8e-7f;  // relative 2^-21
 // this keeps the 48 conversions of a node off the conversion pipe.
 APD float byte_at(uint32_t word, int k) {
   return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
+}
+
+// Byte k of `word` as 1 + byte * 2^-15 (0x3F80bb00), one byte permute.
+APD float byte_q15(uint32_t word, int k) {
+  return __uint_as_float(__byte_perm(word, 0x3F800000u, 0x7604u | ((uint32_t)k << 4)));
+}
+
+// Packed fp32 fma (sm_100): a * b + c per lane, each rounded as fmaf.
+APD float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
 }
 
 // A node's quantised child planes ordered by the ray's octant: per axis the
@@ -192,39 +256,64 @@ constexpr float kRelGrow = 4.76837158e-07f;  // 2^-21
 APD float grow_up(float x) { return fmaf(fabsf(x), kRelGrow, x); }
 APD float grow_down(float x) { return fmaf(-fabsf(x), kRelGrow, x); }
 
-// Entry distance of child i (a compile-time index after unrolling) or +inf
-// when its box is missed inside [tmin, tmax]; tmax_grown = tmax * kGrow.
-// kZero = false leaves out the zero-direction-component test, for rays
-// without one (the traversal loops pick the form once per node, so the
-// common case carries no per-child check).
-template <bool kZero = true>
+// Entry distance from the six slab values, or +inf when the box is missed
+// inside [tmin, tmax]; tmax_grown = tmax * kGrow.
+APD float slab_entry(float lx, float hx, float ly, float hy, float lz, float hz, float tmin, float tmax_grown) {
+  const float tn = grow_down(fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin)));
+  const float tf = grow_up(fminf(fminf(hx, hy), hz));
+  return (tn <= tf && tn <= tmax_grown) ? tn : __uint_as_float(0x7f800000u);
+}
+
+// Entry distance of child i (a compile-time index after unrolling), exact
+// form, with the zero-direction-component test.
 APD float child_entry(const NodeFrame& f, const NodePlanes& pl, const RayPre& r, int i, float tmin,
                       float tmax_grown) {
   const int k = i & 3, h = i >> 2;
   float lx = fmaf(byte_at(pl.nx[h], k), f.ax, f.blx), hx = fmaf(byte_at(pl.fx[h], k), f.ax, f.bhx);
   float ly = fmaf(byte_at(pl.ny[h], k), f.ay, f.bly), hy = fmaf(byte_at(pl.fy[h], k), f.ay, f.bhy);
   float lz = fmaf(byte_at(pl.nz[h], k), f.az, f.blz), hz = fmaf(byte_at(pl.fz[h], k), f.az, f.bhz);
-  if (kZero && r.zero_axes) {
-    const float inf = __uint_as_float(0x7f800000u);
-    if (r.zero_axes & 1u) {
-      bool in = r.o.x >= f.px + byte_at(pl.nx[h], k) * f.sxs && r.o.x <= f.px + byte_at(pl.fx[h], k) * f.sxs;
-      lx = in ? -inf : inf;
-      hx = in ? inf : -inf;
-    }
-    if (r.zero_axes & 2u) {
-      bool in = r.o.y >= f.py + byte_at(pl.ny[h], k) * f.sys && r.o.y <= f.py + byte_at(pl.fy[h], k) * f.sys;
-      ly = in ? -inf : inf;
-      hy = in ? inf : -inf;
-    }
-    if (r.zero_axes & 4u) {
-      bool in = r.o.z >= f.pz + byte_at(pl.nz[h], k) * f.szs && r.o.z <= f.pz + byte_at(pl.fz[h], k) * f.szs;
-      lz = in ? -inf : inf;
-      hz = in ? inf : -inf;
-    }
+  const float inf = __uint_as_float(0x7f800000u);
+  if (r.zero_axes & 1u) {
+    bool in = r.o.x >= f.px + byte_at(pl.nx[h], k) * f.sxs && r.o.x <= f.px + byte_at(pl.fx[h], k) * f.sxs;
+    lx = in ? -inf : inf;
+    hx = in ? inf : -inf;
   }
-  const float tn = grow_down(fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin)));
-  const float tf = grow_up(fminf(fminf(hx, hy), hz));
-  return (tn <= tf && tn <= tmax_grown) ? tn : __uint_as_float(0x7f800000u);
+  if (r.zero_axes & 2u) {
+    bool in = r.o.y >= f.py + byte_at(pl.ny[h], k) * f.sys && r.o.y <= f.py + byte_at(pl.fy[h], k) * f.sys;
+    ly = in ? -inf : inf;
+    hy = in ? inf : -inf;
+  }
+  if (r.zero_axes & 4u) {
+    bool in = r.o.z >= f.pz + byte_at(pl.nz[h], k) * f.szs && r.o.z <= f.pz + byte_at(pl.fz[h], k) * f.szs;
+    lz = in ? -inf : inf;
+    hz = in ? inf : -inf;
+  }
+  return slab_entry(lx, hx, ly, hy, lz, hz, tmin, tmax_grown);
+}
+
+// Entry distance of child i, fast form (no zero or tiny direction component).
+APD float child_entry_q(const NodeFrameQ& f, const NodePlanes& pl, int i, float tmin, float tmax_grown) {
+  const int k = i & 3, h = i >> 2;
+  const float2 n = fma2(make_float2(byte_q15(pl.nx[h], k), byte_q15(pl.ny[h], k)), f.axy, f.cn_xy);
+  const float2 x = fma2(make_float2(byte_q15(pl.fx[h], k), byte_q15(pl.fy[h], k)), f.axy, f.cf_xy);
+  const float2 z = fma2(make_float2(byte_q15(pl.nz[h], k), byte_q15(pl.fz[h], k)), f.azz, f.c_z);
+  return slab_entry(n.x, x.x, n.y, x.y, z.x, z.y, tmin, tmax_grown);
+}
+
+// Entry distances of a node's 8 children (+inf where missed), the form picked
+// once per node.
+APD void child_entries(const uint4 w0, const uint4 w2, const uint4 w3, const uint4 w4, const RayPre& r, float tmin,
+                       float tmax_grown, float tns[8]) {
+  const NodePlanes pl = node_planes(w2, w3, w4, r.neg_axes);
+  if (r.zero_axes) {
+    const NodeFrame f = node_frame(w0, r);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) tns[i] = child_entry(f, pl, r, i, tmin, tmax_grown);
+  } else {
+    const NodeFrameQ f = node_frame_q(w0, r);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) tns[i] = child_entry_q(f, pl, i, tmin, tmax_grown);
+  }
 }
 
 APD uint32_t meta_of(const uint4 w1, int i) { return ((i < 4 ? w1.z : w1.w) >> (8 * (i & 3))) & 0xffu; }
@@ -323,20 +412,12 @@ APD bool trav_step(const S& s, Trav& t, uint2* stack, int budget, Visits* vc) {
     if (kCount) vc->nodes++;
     const uint4* np = s.nodes + 5 * (size_t)t.node;
     const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-    const NodeFrame f = node_frame(w0, t.r);
-    const NodePlanes pl = node_planes(w2, w3, w4, t.r.neg_axes);
     const float range_grown = (kAny ? t.tmax : t.hit.t) * kGrow;
     uint32_t tri_mask = 0;
     float best_t = __uint_as_float(0x7f800000u);
     uint32_t best_node = 0;
     float tns[8];
-    if (t.r.zero_axes) {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) tns[i] = child_entry<true>(f, pl, t.r, i, 0.0f, range_grown);
-    } else {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) tns[i] = child_entry<false>(f, pl, t.r, i, 0.0f, range_grown);
-    }
+    child_entries(w0, w2, w3, w4, t.r, 0.0f, range_grown, tns);
 #pragma unroll(kUnroll ? 8 : 1)
     for (int i = 0; i < 8; ++i) {
       const uint32_t meta = meta_of(w1, i);
@@ -366,60 +447,21 @@ APD bool trav_step(const S& s, Trav& t, uint2* stack, int budget, Visits* vc) {
 }
 
 // ---- Loop-form traversal for rays traced inline in the large resampling
-// kernels.  Same box test (child_entry's arithmetic, all 8 children in one
-// unrolled pass), same culling and tie rules as trav_step, hence the same
-// results; the loop form has no resumable state, which keeps these kernels'
-// code and local memory small.  Returns the hit mask; tnear[] gets the entry
-// distance of each hit child.
+// kernels.  Same box test (child_entries), same culling and tie rules as
+// trav_step, hence the same results; the loop form has no resumable state,
+// which keeps these kernels' code and local memory small.  Returns the hit
+// mask; tnear[] gets the entry distance of each hit child.
 template <bool kClosest>
 APD uint32_t inline_children(const uint4 w0, const uint4 w2, const uint4 w3, const uint4 w4,
                            const RayPre& r, float tmin, float tmax, float tnear[8]) {
-  float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
-  float sxs = __uint_as_float((w0.w & 0xffu) << 23);
-  float sys = __uint_as_float(((w0.w >> 8) & 0xffu) << 23);
-  float szs = __uint_as_float(((w0.w >> 16) & 0xffu) << 23);
-  float ax = sxs * r.inv.x, ay = sys * r.inv.y, az = szs * r.inv.z;
-  float bx = (px - r.o.x) * r.inv.x, by = (py - r.o.y) * r.inv.y, bz = (pz - r.o.z) * r.inv.z;
-  // slab slack: 2^-19 of the node's distance scale from the origin, |p - o| plus
-  // the node extent (255 quanta), along the axis
-  const float kSlack = 1.9073486e-06f;  // 2^-19
-  float ex = (fabsf(bx) + 255.0f * fabsf(ax)) * kSlack, ey = (fabsf(by) + 255.0f * fabsf(ay)) * kSlack,
-        ez = (fabsf(bz) + 255.0f * fabsf(az)) * kSlack;
-  const float blx = bx - ex, bhx = bx + ex, bly = by - ey, bhy = by + ey, blz = bz - ez, bhz = bz + ez;
-  const NodePlanes pl = node_planes(w2, w3, w4, r.neg_axes);
-  const float tmax_grown = tmax * kGrow;
+  child_entries(w0, w2, w3, w4, r, tmin, tmax * kGrow, tnear);
   uint32_t mask = 0;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int k = i & 3, h = i >> 2;
-    float lx = fmaf(byte_at(pl.nx[h], k), ax, blx), hx = fmaf(byte_at(pl.fx[h], k), ax, bhx);
-    float ly = fmaf(byte_at(pl.ny[h], k), ay, bly), hy = fmaf(byte_at(pl.fy[h], k), ay, bhy);
-    float lz = fmaf(byte_at(pl.nz[h], k), az, blz), hz = fmaf(byte_at(pl.fz[h], k), az, bhz);
-    if (r.zero_axes) {
-      const float inf = __uint_as_float(0x7f800000u);
-      if (r.zero_axes & 1u) {
-        bool in = r.o.x >= px + byte_at(pl.nx[h], k) * sxs && r.o.x <= px + byte_at(pl.fx[h], k) * sxs;
-        lx = in ? -inf : inf;
-        hx = in ? inf : -inf;
-      }
-      if (r.zero_axes & 2u) {
-        bool in = r.o.y >= py + byte_at(pl.ny[h], k) * sys && r.o.y <= py + byte_at(pl.fy[h], k) * sys;
-        ly = in ? -inf : inf;
-        hy = in ? inf : -inf;
-      }
-      if (r.zero_axes & 4u) {
-        bool in = r.o.z >= pz + byte_at(pl.nz[h], k) * szs && r.o.z <= pz + byte_at(pl.fz[h], k) * szs;
-        lz = in ? -inf : inf;
-        hz = in ? inf : -inf;
-      }
-    }
-    const float tn = grow_down(fmaxf(fmaxf(lx, ly), fmaxf(lz, tmin)));
-    const float tf = grow_up(fminf(fminf(hx, hy), hz));
-    tnear[i] = tn;
-    if (tn <= tf && tn <= tmax_grown) mask |= 1u << i;
-  }
+  for (int i = 0; i < 8; ++i)
+    if (tnear[i] < __uint_as_float(0x7f800000u)) mask |= 1u << i;
   return mask;
 }
+
 // Closest hit in [0, tmax] (returns false on miss).  Tie rule: smaller t, then
 // smaller global triangle id.
 template <bool kCount = false>

@@ -68,21 +68,13 @@ template <bool kAny>
 APD void visit_node2(const uint4* nodes, Trav& t, uint2* stack, uint32_t* leaf_base, uint32_t* leaf_mask) {
   const uint4* np = nodes + 5 * (size_t)t.node;
   const uint4 w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-  const NodeFrame f = node_frame(w0, t.r);
-  const NodePlanes pl = node_planes(w2, w3, w4, t.r.neg_axes);
   const float range_grown = (kAny ? t.tmax : t.hit.t) * kGrow;
   uint32_t mask = 0;
   float best_t = __uint_as_float(0x7f800000u);
   uint32_t best_node = 0;
   t.have = false;
   float tns[8];
-  if (t.r.zero_axes) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) tns[i] = child_entry<true>(f, pl, t.r, i, 0.0f, range_grown);
-  } else {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) tns[i] = child_entry<false>(f, pl, t.r, i, 0.0f, range_grown);
-  }
+  child_entries(w0, w2, w3, w4, t.r, 0.0f, range_grown, tns);
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const uint32_t meta = meta_of(w1, i);
