@@ -132,9 +132,16 @@ APD bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float t
 // inside the fma.  The rounding of c adds at most half an ulp of
 // |b| + e + 2^15 |a|: 2^-24 |b|, inside the 2^-19 margin, plus 2^-9 |a|, which
 // a further widening of 2^-8 |a| (1/256 of a quantum) covers.  The fast form
-// pairs the near and far planes in packed fp32 fmas (fma.rn.f32x2, the same
-// rounding per lane as a scalar fma).  Boxes of either form hold every
-// triangle the test accepts, so both give the same hits.
+// also folds the interval ends' relative 2^-21 widening into the per-node
+// slack: every slab value is at most |b| + 255 |a| (+ e) in magnitude, so a
+// slack of 1.5 * 2^-19 (|b| + 255 |a|) lowers each near slab (raises each far
+// one) by more than 2^-21 of its value on top of the 2^-19 margin, and the
+// entry and exit need no per-child widening (checked against exact plane
+// distances over random nodes and rays: the margin left is at least the exact
+// form's 2^-19 slack plus its 2^-21 interval widening).  It pairs the near and
+// far planes in packed fp32 fmas (fma.rn.f32x2, the same rounding per lane as a
+// scalar fma).  Boxes of either form hold every triangle the test accepts, so
+// both give the same hits.
 struct NodeFrame {
   float px, py, pz, sxs, sys, szs;  // origin and scales of the quantisation grid
   float ax, ay, az;                 // slab = fma(q, a, b -+ e) per axis
@@ -183,8 +190,8 @@ APD NodeFrameQ node_frame_q(const uint4 w0, const RayPre& r) {
   const float bx = (__uint_as_float(w0.x) - r.o.x) * r.inv.x;
   const float by = (__uint_as_float(w0.y) - r.o.y) * r.inv.y;
   const float bz = (__uint_as_float(w0.z) - r.o.z) * r.inv.z;
-  const float kSlack = 1.9073486e-06f;                 // 2^-19 of |b|
-  const float kSlackA = 255.0f * 1.9073486e-06f + 0.00390625f;  // 2^-19 of the extent + 2^-8 of a quantum
+  const float kSlack = 2.86102295e-06f;                 // 1.5 * 2^-19 of |b|
+  const float kSlackA = 255.0f * 2.86102295e-06f + 0.00390625f;  // 1.5 * 2^-19 of the extent + 2^-8 of a quantum
   const float ex = fmaf(fabsf(ax), kSlackA, fabsf(bx) * kSlack);
   const float ey = fmaf(fabsf(ay), kSlackA, fabsf(by) * kSlack);
   const float ez = fmaf(fabsf(az), kSlackA, fabsf(bz) * kSlack);
@@ -291,13 +298,16 @@ APD float child_entry(const NodeFrame& f, const NodePlanes& pl, const RayPre& r,
   return slab_entry(lx, hx, ly, hy, lz, hz, tmin, tmax_grown);
 }
 
-// Entry distance of child i, fast form (no zero or tiny direction component).
+// Entry distance of child i, fast form (no zero or tiny direction component;
+// the interval widening is in the slack).
 APD float child_entry_q(const NodeFrameQ& f, const NodePlanes& pl, int i, float tmin, float tmax_grown) {
   const int k = i & 3, h = i >> 2;
   const float2 n = fma2(make_float2(byte_q15(pl.nx[h], k), byte_q15(pl.ny[h], k)), f.axy, f.cn_xy);
   const float2 x = fma2(make_float2(byte_q15(pl.fx[h], k), byte_q15(pl.fy[h], k)), f.axy, f.cf_xy);
   const float2 z = fma2(make_float2(byte_q15(pl.nz[h], k), byte_q15(pl.fz[h], k)), f.azz, f.c_z);
-  return slab_entry(n.x, x.x, n.y, x.y, z.x, z.y, tmin, tmax_grown);
+  const float tn = fmaxf(fmaxf(n.x, n.y), fmaxf(z.x, tmin));
+  const float tf = fminf(fminf(x.x, x.y), z.y);
+  return (tn <= tf && tn <= tmax_grown) ? tn : __uint_as_float(0x7f800000u);
 }
 
 // Entry distances of a node's 8 children (+inf where missed), the form picked
