@@ -2167,7 +2167,10 @@ __global__ void k_firefly(FrameBuffers fb, uint32_t W, uint32_t H, uint32_t cur,
 // Register-capped for 6 blocks of 256 per SM: its reprojection gathers are
 // latency-bound, and the extra resident warps hide more of them than the few
 // spilled registers cost.
-__global__ void __launch_bounds__(256, 6) k_svgf_temporal(FrameBuffers fb, Consts c, const uint32_t* demod, uint32_t* out_rad,
+#ifndef AP_SVGF_MIN_BLOCKS
+#define AP_SVGF_MIN_BLOCKS 6
+#endif
+__global__ void __launch_bounds__(256, AP_SVGF_MIN_BLOCKS) k_svgf_temporal(FrameBuffers fb, Consts c, const uint32_t* demod, uint32_t* out_rad,
                                 const float2* in_mom, float2* out_mom, int write_records) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
@@ -2187,23 +2190,31 @@ __global__ void __launch_bounds__(256, 6) k_svgf_temporal(FrameBuffers fb, Const
   float3 trad = f3s(0.0f);
   float tmx = 0.0f, tmy = 0.0f;
   uint32_t count = 0;
-  float2 pp;
-  if (prev_point(fb, cur, x, y, c.W, c.H, &pp)) {
+  // the previous point from this pixel's velocity (prev_point's arithmetic on
+  // the G-buffer texel already read)
+  const float ppx = (float)x - ((float)c.W * __uint_as_float(gbv.z));
+  const float ppy = (float)y - ((float)c.H * __uint_as_float(gbv.w));
+  if (ppx >= 0.0f && ppy >= 0.0f && ppx <= (float)(c.W - 1) && ppy <= (float)(c.H - 1)) {
+    const float2 pp = make_float2(ppx, ppy);
+    uint32_t ix = dm::f2u(floorf(pp.x)), iy = dm::f2u(floorf(pp.y));
+    float fx = dm::fract(pp.x), fy = dm::fract(pp.y);
+    uint32_t x1 = min(ix + 1, c.W - 1), y1 = min(iy + 1, c.H - 1);
+    uint32_t i00 = iy * c.W + ix, i10 = iy * c.W + x1, i01 = y1 * c.W + ix, i11 = y1 * c.W + x1;
+    // the history taps share the previous G-buffer taps' positions: all of
+    // them are read before the validity test, in one round trip
+    const uint32_t h00 = fb.svgf_hist[i00], h10 = fb.svgf_hist[i10], h01 = fb.svgf_hist[i01], h11 = fb.svgf_hist[i11];
+    const float2 m00 = in_mom[i00], m10 = in_mom[i10], m01 = in_mom[i01], m11 = in_mom[i11];
+    const uint32_t prev_count = fb.svgf_count[id];
     GT pg = sample_prev_gbuffer(fb.gb_a[cur ^ 1u], fb.gb_b[cur ^ 1u], c.W, c.H, pp);
     if (history_valid(g, pg)) {
-      uint32_t ix = dm::f2u(floorf(pp.x)), iy = dm::f2u(floorf(pp.y));
-      float fx = dm::fract(pp.x), fy = dm::fract(pp.y);
-      uint32_t x1 = min(ix + 1, c.W - 1), y1 = min(iy + 1, c.H - 1);
-      uint32_t i00 = iy * c.W + ix, i10 = iy * c.W + x1, i01 = y1 * c.W + ix, i11 = y1 * c.W + x1;
-      float3 c0 = mix3(unpack_rgb9e5(fb.svgf_hist[i00]), unpack_rgb9e5(fb.svgf_hist[i10]), fx);
-      float3 c1 = mix3(unpack_rgb9e5(fb.svgf_hist[i01]), unpack_rgb9e5(fb.svgf_hist[i11]), fx);
+      float3 c0 = mix3(unpack_rgb9e5(h00), unpack_rgb9e5(h10), fx);
+      float3 c1 = mix3(unpack_rgb9e5(h01), unpack_rgb9e5(h11), fx);
       trad = mix3(c0, c1, fy);
-      float2 m00 = in_mom[i00], m10 = in_mom[i10], m01 = in_mom[i01], m11 = in_mom[i11];
       float m0x = mixf(m00.x, m10.x, fx), m0y = mixf(m00.y, m10.y, fx);
       float m1x = mixf(m01.x, m11.x, fx), m1y = mixf(m01.y, m11.y, fx);
       tmx = mixf(m0x, m1x, fy);
       tmy = mixf(m0y, m1y, fy);
-      count = min(fb.svgf_count[id] + 1u, c.cfg.svgf_max_history);
+      count = min(prev_count + 1u, c.cfg.svgf_max_history);
     }
   }
   float alpha = 1.0f / (1.0f + (float)count);
@@ -2333,7 +2344,8 @@ __global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uin
 
 // taa.wgsl:67-171.  A 16x16 block stages the 18x18 neighbourhood of the
 // pre-TAA frame `src` in shared memory (unpacked once, clamped at zero, with
-// its luma); the 3x3 filter and the colour-box statistics read it from there.
+// the filter's 1 / (1 + luma)); the 3x3 filter and the colour-box statistics
+// read it from there.
 // Weights and the history clip use hardware division and square root.  Sky
 // pixels keep `src`'s value (the reference leaves them untouched).
 APD float mitchell(float x_, float B, float C) {
@@ -2349,25 +2361,53 @@ constexpr int kTaaTile = 16;
 constexpr int kTaaSpan = kTaaTile + 2;
 __global__ void __launch_bounds__(256) k_taa(FrameBuffers fb, Consts c, const uint32_t* src, uint32_t* dst,
                                              const uint32_t* prevb) {
-  __shared__ float4 s_c[kTaaSpan * kTaaSpan];  // max(colour, 0), luma; w < 0 outside the image
+  __shared__ float4 s_c[kTaaSpan * kTaaSpan];  // max(colour, 0), 1 / (1 + luma); w < 0 outside the image
   const int x0 = blockIdx.x * kTaaTile, y0 = blockIdx.y * kTaaTile;
   const int tid = threadIdx.y * kTaaTile + threadIdx.x;
+  const uint32_t x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  const bool in_image = x < c.W && y < c.H;
+  const uint32_t id = in_image ? y * c.W + x : 0u;
+  const uint32_t cur = c.frame_idx & 1u;
+  // This pixel's depth, colour and velocity, then its history taps and the
+  // previous depth, are read before the neighbourhood is staged, so that their
+  // round trips overlap the staging loads.
+  float cdepth = 0.0f;
+  uint32_t csrc = 0u, hp[4] = {0u, 0u, 0u, 0u}, pid = id;
+  float tx = 0.0f, ty = 0.0f, pdepth = 0.0f;
+  bool bilinear = false;
+  if (in_image) {
+    cdepth = __uint_as_float(fb.gb_a[cur][id].w);
+    csrc = src[id];
+    float2 pp;
+    bilinear = prev_point(fb, cur, x, y, c.W, c.H, &pp);
+    if (cdepth != 0.0f) {
+      if (bilinear) {
+        uint32_t fx = dm::f2u(floorf(pp.x)), fy = dm::f2u(floorf(pp.y));
+        uint32_t cxp = dm::f2u(ceilf(pp.x)), cyp = dm::f2u(ceilf(pp.y));
+        pid = fy * c.W + fx;
+        hp[0] = prevb[min(fy, c.H - 1) * c.W + min(fx, c.W - 1)];
+        hp[1] = prevb[min(cyp, c.H - 1) * c.W + min(fx, c.W - 1)];
+        hp[2] = prevb[min(fy, c.H - 1) * c.W + min(cxp, c.W - 1)];
+        hp[3] = prevb[min(cyp, c.H - 1) * c.W + min(cxp, c.W - 1)];
+        tx = dm::fract(pp.x);
+        ty = dm::fract(pp.y);
+      } else {
+        hp[0] = prevb[id];
+      }
+      pdepth = __uint_as_float(fb.gb_a[cur ^ 1u][pid].w);
+    }
+  }
   for (int k = tid; k < kTaaSpan * kTaaSpan; k += kTaaTile * kTaaTile) {
     const int px = x0 + k % kTaaSpan - 1, py = y0 + k / kTaaSpan - 1;
     float4 v = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
     if (px >= 0 && py >= 0 && px < (int)c.W && py < (int)c.H) {
       const float3 sc = vmax(unpack_rgb9e5(src[(uint32_t)py * c.W + (uint32_t)px]), f3s(0.0f));
-      v = make_float4(sc.x, sc.y, sc.z, luma(sc));
+      v = make_float4(sc.x, sc.y, sc.z, __frcp_rn(1.0f + luma(sc)));
     }
     s_c[k] = v;
   }
   __syncthreads();
-  const uint32_t x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-  if (x >= c.W || y >= c.H) return;
-  const uint32_t id = y * c.W + x;
-  const uint32_t cur = c.frame_idx & 1u;
-  const float cdepth = __uint_as_float(fb.gb_a[cur][id].w);
-  const uint32_t csrc = src[id];
+  if (!in_image) return;
   if (cdepth == 0.0f) {
     dst[id] = csrc;
     return;
@@ -2386,8 +2426,7 @@ __global__ void __launch_bounds__(256) k_taa(FrameBuffers fb, Consts c, const ui
       const float4 v = s_c[cs + dy * kTaaSpan + dx];
       if (v.w < 0.0f) continue;
       const float3 sc = f3(v.x, v.y, v.z);
-      const float w = (mitchell((float)dx, 0.33f, 0.33f) * mitchell((float)dy, 0.33f, 0.33f)) *
-                      __frcp_rn(1.0f + v.w);
+      const float w = (mitchell((float)dx, 0.33f, 0.33f) * mitchell((float)dy, 0.33f, 0.33f)) * v.w;
       rec = rec + sc * w;
       wsum = wsum + w;
       m1 = m1 + sc;
@@ -2396,27 +2435,15 @@ __global__ void __launch_bounds__(256) k_taa(FrameBuffers fb, Consts c, const ui
     }
   rec = rec * __frcp_rn(fmaxf(wsum, 1e-5f));
   float3 hist;
-  uint32_t pid;
-  float2 pp;
-  if (prev_point(fb, cur, x, y, c.W, c.H, &pp)) {
-    uint32_t fx = dm::f2u(floorf(pp.x)), fy = dm::f2u(floorf(pp.y));
-    uint32_t cxp = dm::f2u(ceilf(pp.x)), cyp = dm::f2u(ceilf(pp.y));
-    pid = fy * c.W + fx;
-    uint32_t i00 = min(fy, c.H - 1) * c.W + min(fx, c.W - 1);
-    uint32_t i10 = min(cyp, c.H - 1) * c.W + min(fx, c.W - 1);
-    uint32_t i01 = min(fy, c.H - 1) * c.W + min(cxp, c.W - 1);
-    uint32_t i11 = min(cyp, c.H - 1) * c.W + min(cxp, c.W - 1);
-    float3 h00 = unpack_rgb9e5(prevb[i00]), h10 = unpack_rgb9e5(prevb[i10]);
-    float3 h01 = unpack_rgb9e5(prevb[i01]), h11 = unpack_rgb9e5(prevb[i11]);
-    float tx = dm::fract(pp.x), ty = dm::fract(pp.y);
+  if (bilinear) {
+    float3 h00 = unpack_rgb9e5(hp[0]), h10 = unpack_rgb9e5(hp[1]);
+    float3 h01 = unpack_rgb9e5(hp[2]), h11 = unpack_rgb9e5(hp[3]);
     float3 a = h00 * (1.0f - tx) + h10 * tx;
     float3 b = h01 * (1.0f - tx) + h11 * tx;
     hist = a * (1.0f - ty) + b * ty;
   } else {
-    hist = unpack_rgb9e5(prevb[id]);
-    pid = id;
+    hist = unpack_rgb9e5(hp[0]);
   }
-  float pdepth = __uint_as_float(fb.gb_a[cur ^ 1u][pid].w);
   float cdcs = depth_cs(cdepth, 0.001f, 10000.0f), pdcs = depth_cs(pdepth, 0.001f, 10000.0f);
   bool vdd = (dm::fabs_(cdcs - pdcs) / cdcs) < 0.1f;
   const float inv_cnt = __frcp_rn(cnt);
