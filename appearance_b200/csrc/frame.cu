@@ -2239,11 +2239,13 @@ __global__ void __launch_bounds__(256, AP_SVGF_MIN_BLOCKS) k_svgf_temporal(Frame
 // every step.  Pixels outside the image are staged as sky (depth 0), which
 // the taps skip as the reference skips both.
 //
-// Arithmetic: the two exponential weights are one hardware exp of the summed
-// exponents and pow(., 128) is seven squarings; sums use fused multiply-adds.
-// The result therefore differs from the reference's literal expressions in
-// the last bits of the weights; after RGB9E5 packing (9-bit mantissas) most
-// pixels are bit-identical and the rest differ by a rounding step.
+// Arithmetic: the tap weight, pow(n.n', 128) times the two exponential
+// weights times the kernel weight, is one hardware base-2 exponential of
+// 128 log2(n.n') (hardware log2) plus the summed exponents in base 2; sums use
+// fused multiply-adds.  The result therefore differs from the reference's
+// literal expressions in the last bits of the weights; after RGB9E5 packing
+// (9-bit mantissas) most pixels are bit-identical and the rest differ by a
+// rounding step.
 //
 // Stores: the next pass's record (packed radiance, variance); pass 0 the
 // history radiance of the next frame's temporal pass (svgf_hist); the last
@@ -2251,6 +2253,13 @@ __global__ void __launch_bounds__(256, AP_SVGF_MIN_BLOCKS) k_svgf_temporal(Frame
 // ping-pong stores it there (sky pixels of the next frame read it); the final
 // pass writes the filtered frame, and for sky pixels, which no pass writes in
 // the reference, the value the reference's final buffer still holds.
+// Hardware base-2 exponential (ex2.approx.ftz.f32).
+APD float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 constexpr int kAtrousTile = 16;
 constexpr int kAtrousSpan = kAtrousTile + 4;
 enum : uint32_t { ATR_HIST = 1u, ATR_STATE = 2u, ATR_FINAL = 4u, ATR_NEXT = 8u };
@@ -2307,9 +2316,11 @@ __global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uin
   float wsum = 1.0f;
   // exp(-dd^2 / (2 PHI_DEPTH^2)) * exp(-ld / max(PHI_LUMA sqrt(var), 1e-8)),
   // PHI_DEPTH 0.1, PHI_LUMA 4, PHI_NORMAL 128 (svgf_atrous.wgsl:7-9)
-  const float inv_lum = 1.0f / fmaxf(4.0f * sqrtf(vsum), 1e-8f);
-  const float depth_k = 1.0f / (2.0f * 0.1f * 0.1f);
-  const float KW[3] = {3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
+  // in base 2: w = 2^(128 log2(d) - |dl| log2(e) / lum - dd^2 log2(e) / (2 PHI_DEPTH^2) + log2(K))
+  const float kLog2e = 1.44269504f;
+  const float inv_lum2 = kLog2e / fmaxf(4.0f * sqrtf(vsum), 1e-8f);
+  const float depth_k2 = kLog2e / (2.0f * 0.1f * 0.1f);
+  const float LOG2_KW[3] = {-1.41503751f, -2.0f, -4.0f};  // log2 of 3/8, 1/4, 1/16
 #pragma unroll
   for (int dy = -2; dy <= 2; ++dy)
 #pragma unroll
@@ -2321,11 +2332,13 @@ __global__ void __launch_bounds__(256) k_atrous(FrameBuffers fb, uint32_t W, uin
       const float svar = s_var[k];
       float d = __fmaf_rn(cnd.x, snd.x, __fmaf_rn(cnd.y, snd.y, __fmul_rn(cnd.z, snd.z)));
       d = fmaxf(d, 0.0f);
-      d = d * d; d = d * d; d = d * d; d = d * d; d = d * d; d = d * d; d = d * d;  // ^128
       const float dd = cnd.w - snd.w;
-      const float e = __fmaf_rn(-fabsf(crad.w - srad.w), inv_lum, -(dd * dd) * depth_k);
-      float w = d * __expf(e) * (KW[dx < 0 ? -dx : dx] * KW[dy < 0 ? -dy : dy]);
-      w = snd.w == 0.0f ? 0.0f : w;  // sky neighbour or outside the image: skipped
+      const float lk = LOG2_KW[dx < 0 ? -dx : dx] + LOG2_KW[dy < 0 ? -dy : dy];
+      float e = __fmaf_rn(-(dd * dd), depth_k2, lk);
+      e = __fmaf_rn(-fabsf(crad.w - srad.w), inv_lum2, e);
+      // a sky neighbour or one outside the image is staged with a zero
+      // normal and zero radiance and variance: d = 0 gives w = 0 exactly
+      const float w = ex2_approx(__fmaf_rn(128.0f, __log2f(d), e));
       rsum.x = __fmaf_rn(srad.x, w, rsum.x);
       rsum.y = __fmaf_rn(srad.y, w, rsum.y);
       rsum.z = __fmaf_rn(srad.z, w, rsum.z);
