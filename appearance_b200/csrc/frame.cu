@@ -1811,7 +1811,13 @@ APD float3 primary_hit(const FrameBuffers& fb, uint32_t id, float pt) {
   return ray_org(ray) + ray_dir(ray) * pt;
 }
 
-__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_a(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
+#ifndef AP_GSP_MIN_BLOCKS
+// resident blocks of 256 per SM the GI spatial stages are register-capped for
+// (1080p benchmark frame, CUDA events: 2, 3, 4, 5, 6 blocks gave 5.5, 4.4,
+// 4.0, 4.0, 4.0 ms for the 21 stage launches)
+#define AP_GSP_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, AP_GSP_MIN_BLOCKS) k_gsp_a(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
                                                 uint32_t pass_count, uint32_t nsamples, uint32_t i,
                                                 const uint4* in_a, const uint4* in_b, uint4* out_a, uint4* out_b,
                                                 uint4* prev_a, uint4* prev_b) {
@@ -1890,7 +1896,7 @@ __global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_a(DevScene s, Fr
   push_ray(fb, Q_GI_CAND, want, g.gi_origin + g.wi * 1e-4f, 1000.0f - 1e-4f * 2.0f, g.wi, id);
 }
 
-__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_b(DevScene s, FrameBuffers fb, Consts c, const uint4* in_a,
+__global__ void __launch_bounds__(256, AP_GSP_MIN_BLOCKS) k_gsp_b(DevScene s, FrameBuffers fb, Consts c, const uint4* in_a,
                                                 const uint4* in_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
@@ -1910,7 +1916,7 @@ __global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_b(DevScene s, Fr
   push_ray(fb, Q_GI_SHADOW, sh.ray, sh.o, sh.tmax, sh.d, id);
 }
 
-__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_c(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
+__global__ void __launch_bounds__(256, AP_GSP_MIN_BLOCKS) k_gsp_c(DevScene s, FrameBuffers fb, Consts c, uint32_t pass_idx,
                                                 uint32_t pass_count, const uint4* in_a, const uint4* in_b,
                                                 uint4* out_a, uint4* out_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1973,7 +1979,7 @@ __global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_c(DevScene s, Fr
   push_ray(fb, Q_GI_CAND, there, gn.gi_origin + gn.wi * 1e-4f, 1000.0f - 1e-4f * 2.0f, gn.wi, id);
 }
 
-__global__ void __launch_bounds__(256, AP_DSP_MIN_BLOCKS) k_gsp_d(DevScene s, FrameBuffers fb, Consts c, const uint4* out_a,
+__global__ void __launch_bounds__(256, AP_GSP_MIN_BLOCKS) k_gsp_d(DevScene s, FrameBuffers fb, Consts c, const uint4* out_a,
                                                 const uint4* out_b) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= c.W || y >= c.H) return;
