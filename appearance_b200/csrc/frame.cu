@@ -484,6 +484,13 @@ APD const uint4* stage_lights(const DevScene& s, uint4* sm) {
   return sm;
 }
 
+// The full evaluation kept out of line in the RIS candidate loop, where only
+// transmissive materials take it, so the loop's code stays small (the first
+// candidate, evaluated without a context, keeps it inline); same arithmetic.
+__device__ __noinline__ float3 disney_eval_outlined(const Bsdf& b, const Frame& fr, float3 wo, float3 wi, float* sp) {
+  return disney_eval(b, fr, wo, wi, sp);
+}
+
 // `ctx` (the shading point's DisneyCtx, or null) saves the per-candidate
 // evaluation its wo-only terms; transmissive materials evaluate in full.
 APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& fr, const Bsdf& b, uint32_t& rng,
@@ -500,8 +507,9 @@ APD void area_candidate(const DevScene& s, float3 hit, float3 wo, const Frame& f
   const bool lit = ev->emission.x != 0.0f || ev->emission.y != 0.0f || ev->emission.z != 0.0f;
   if (wdn > 0.0f && *pdf > 0.0f && lit) {
     float sp = 0.0f;
-    float3 refl = (ctx && b.transmission <= 0.5f) ? disney_eval_ctx(b, *ctx, fr, wo, wi, &sp)
-                                                  : disney_eval(b, fr, wo, wi, &sp);
+    float3 refl = !ctx ? disney_eval(b, fr, wo, wi, &sp)
+                       : (b.transmission <= 0.5f ? disney_eval_ctx(b, *ctx, fr, wo, wi, &sp)
+                                                 : disney_eval_outlined(b, fr, wo, wi, &sp));
     if (sp > 0.0f) *phat = luma(refl * wdn * ev->emission);
   }
 }
