@@ -41,6 +41,25 @@ APD float3 reflect(float3 i, float3 n) { return i - (2.0f * dot(n, i)) * n; }
 APD float luma(float3 c) { return dot(c, f3(0.2126f, 0.7152f, 0.0722f)); }
 APD float sqr(float x) { return x * x; }
 
+// Exclusive prefix of `flag` over the block's threads in thread order, and
+// the block's total.  Every thread of the block calls it, once per kernel
+// (blockDim.x a multiple of 32, at most 1024).
+APD uint32_t block_prefix(bool flag, uint32_t* total) {
+  __shared__ uint32_t s_warp[32];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned b = __ballot_sync(0xffffffffu, flag);
+  if (lane == 0) s_warp[warp] = (uint32_t)__popc(b);
+  __syncthreads();
+  uint32_t off = 0, tot = 0;
+  for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) {
+    const uint32_t c = s_warp[w];
+    off += w < warp ? c : 0u;
+    tot += c;
+  }
+  *total = tot;
+  return off + (uint32_t)__popc(b & ((1u << lane) - 1u));
+}
+
 // Column-major 3x3: columns c0, c1, c2.
 struct Mat3 {
   float3 c0, c1, c2;

@@ -2097,17 +2097,31 @@ __global__ void k_rc_count(RcFrame rc, uint32_t slots, float last_tag) {
   if ((threadIdx.x & 31) == 0 && b) atomicAdd(&rc.counts[0], (uint32_t)__popc(b));
 }
 
-__global__ void k_rc_batch(FrameBuffers fb, RcFrame rc, uint32_t slots, uint32_t frame_idx, float last_tag) {
-  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= slots) return;
-  const float4* r = rc.rec + 6 * (size_t)k;
-  if (r[5].w != last_tag) return;
+// A record of the last sample goes into the training batch with probability
+// batch / candidates, drawn from its slot index and the frame index.
+APD bool rc_kept(const RcFrame& rc, uint32_t k, uint32_t slots, uint32_t frame_idx, float last_tag) {
+  if (k >= slots || rc.rec[6 * (size_t)k + 5].w != last_tag) return false;
   const uint32_t cand = rc.counts[0];
   const float keep = cand <= rc.batch ? 1.0f : (float)rc.batch / (float)cand;
   const float u = (float)(pcg_hash(k ^ xor_shift(frame_idx * 0x9E3779B9u)) >> 8) * (1.0f / 16777216.0f);
-  if (u >= keep) return;
-  const uint32_t slot = atomicAdd(&rc.counts[1], 1u);
-  if (slot >= rc.batch) return;
+  return u < keep;
+}
+
+// Records kept per block of 256 slots (count_scan turns them into the
+// blocks' first batch slots, so the batch is in record order).
+__global__ void k_rc_keep(RcFrame rc, uint32_t slots, uint32_t frame_idx, float last_tag) {
+  uint32_t tot;
+  block_prefix(rc_kept(rc, blockIdx.x * blockDim.x + threadIdx.x, slots, frame_idx, last_tag), &tot);
+  if (threadIdx.x == 0) rc.bcount[blockIdx.x] = tot;
+}
+
+__global__ void k_rc_batch(FrameBuffers fb, RcFrame rc, uint32_t slots, uint32_t frame_idx, float last_tag) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool kept = rc_kept(rc, k, slots, frame_idx, last_tag);
+  uint32_t tot;
+  const uint32_t slot = rc.bcount[blockIdx.x] + block_prefix(kept, &tot);
+  if (!kept || slot >= rc.batch) return;
+  const float4* r = rc.rec + 6 * (size_t)k;
   const uint32_t pixel = (k / kRcMaxBounces) * rc.stride + (frame_idx * 7u + 3u) % rc.stride;
   const float3 t = rc_target(r, unpack_rgb9e5(fb.radiance[pixel]));
   float4* q = rc.bq + 4 * (size_t)slot;
@@ -2686,7 +2700,7 @@ size_t rc_frame_bytes(uint32_t W, uint32_t H, uint32_t stride, uint32_t batch) {
   const size_t P = (size_t)W * H, slots = ((P + stride - 1) / stride) * kRcMaxBounces;
   auto a = [](size_t b) { return ((b + 255) / 256) * 256; };
   return a(P * 64) + a(P * 16) + a(P * 4) + a(P * 12) + a(slots * 96) + a((size_t)batch * 64) + a((size_t)batch * 12) +
-         a(12);
+         a(12) + a(4 * ((slots + 255) / 256));
 }
 
 void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_t batch, RcFrame* rc) {
@@ -2700,6 +2714,34 @@ void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_
   rc->bq = carve<float4>(p, 4 * (size_t)batch);
   rc->bt = carve<float>(p, 3 * (size_t)batch);
   rc->counts = carve<uint32_t>(p, 3);
+  rc->bcount = carve<uint32_t>(p, (slots + 255) / 256);
+}
+
+__global__ void __launch_bounds__(1024) k_count_scan(uint32_t* c, uint32_t n, uint32_t* total, uint32_t cap) {
+  __shared__ uint32_t s[1024];
+  const uint32_t t = threadIdx.x, per = (n + 1023u) / 1024u;
+  const uint32_t b0 = min(t * per, n), b1 = min(b0 + per, n);
+  uint32_t sum = 0;
+  for (uint32_t i = b0; i < b1; ++i) sum += c[i];
+  s[t] = sum;
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024u; off <<= 1) {  // inclusive scan of the per-thread sums
+    const uint32_t v = t >= off ? s[t - off] : 0u;
+    __syncthreads();
+    s[t] += v;
+    __syncthreads();
+  }
+  uint32_t run = t ? s[t - 1] : 0u;
+  for (uint32_t i = b0; i < b1; ++i) {
+    const uint32_t v = c[i];
+    c[i] = run;
+    run += v;
+  }
+  if (t == 1023u) *total = min(s[1023], cap);
+}
+
+void count_scan(uint32_t* counts, uint32_t n, uint32_t* total, uint32_t cap, cudaStream_t st) {
+  k_count_scan<<<1, 1024, 0, st>>>(counts, n, total, cap);
 }
 
 const char* kernel_kind_name(int k) {
@@ -3009,8 +3051,11 @@ int encode_frame(const DevScene& scene, const FrameBuffers& fb, const FrameConfi
     // training targets of the last sample's suffix vertices (the radiance of
     // the training pixels is final here), one Adam step
     const float last_tag = (float)cfg.sample_count;
-    k_rc_count<<<(rc_slots + 255) / 256, 256, 0, st>>>(*rc, rc_slots, last_tag);
-    k_rc_batch<<<(rc_slots + 255) / 256, 256, 0, st>>>(fb, *rc, rc_slots, frame_idx, last_tag);
+    const uint32_t nb = (rc_slots + 255) / 256;
+    k_rc_count<<<nb, 256, 0, st>>>(*rc, rc_slots, last_tag);
+    k_rc_keep<<<nb, 256, 0, st>>>(*rc, rc_slots, frame_idx, last_tag);
+    count_scan(rc->bcount, nb, rc->counts + 1, rc->batch, st);
+    k_rc_batch<<<nb, 256, 0, st>>>(fb, *rc, rc_slots, frame_idx, last_tag);
     mark(K_RC);
     {
       rc_train_device(rc->cache, rc->bq, rc->bt, rc->counts + 1, rc->batch, rc->lr, 1, st);

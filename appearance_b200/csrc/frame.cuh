@@ -122,10 +122,14 @@ struct RcFrame {
   float4* bq = nullptr;      // training batch queries (batch x 4)
   float* bt = nullptr;       // training batch targets (batch x 3)
   uint32_t* counts = nullptr;  // [0] candidate records, [1] batch entries, [2] retired paths of the sample
+  uint32_t* bcount = nullptr;  // per 256 record slots: records kept for the batch, then their first batch slot
 };
 constexpr uint32_t kRcMaxBounces = 8;        // record slots per training pixel
 constexpr uint32_t kRcRetired = 0xFFFFFFFEu;  // hit id of a path retired into the cache
 size_t rc_frame_bytes(uint32_t W, uint32_t H, uint32_t stride, uint32_t batch);
+// In place: counts[0..n) -> their exclusive prefix sums; *total = min(sum, cap).
+// Assembles training batches in record order (one block, any n).
+void count_scan(uint32_t* counts, uint32_t n, uint32_t* total, uint32_t cap, cudaStream_t st);
 void rc_frame_carve(void* base, uint32_t W, uint32_t H, uint32_t stride, uint32_t batch, RcFrame* rc);
 
 // mlp.cu: inference over n queries, and one training step on a device-assembled batch

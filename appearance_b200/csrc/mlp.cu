@@ -18,7 +18,8 @@
 // their rows back with tcgen05.ld (each thread half of a row's columns),
 // apply ReLU, round to FP16 and write the next layer's operand.  Training (k_rc_train_tc) runs forward and backward on the tensor
 // cores in one kernel per step, tile by tile with the weight-gradient sums in
-// tensor memory; k_rc_adam updates the FP32 master weights and repacks the
+// tensor memory, one gradient row per CTA; k_rc_grad_sum adds the rows in a
+// fixed order and k_rc_adam updates the FP32 master weights and repacks the
 // FP16 operands (forward and transposed).
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -354,8 +355,9 @@ __global__ void __launch_bounds__(2 * kTile, 1) k_rc_infer(const uint4* __restri
 // halves of the sum being added when it is read out.  The activations H_l are
 // FP16 values already (the model rounds them).  So the products and their
 // FP32 sums keep the precision of an FP32 backward pass.  The weight-gradient
-// sums stay in tensor memory over all of the CTA's tiles and reach the
-// gradient with one atomic add per element at the end.  The per-sample loss
+// sums stay in tensor memory over all of the CTA's tiles and are stored to the
+// CTA's own gradient row at the end; k_rc_grad_sum adds the rows in a fixed
+// order, so a step's gradient is reproducible bit for bit.  The per-sample loss
 // gradient enters without the mean's 1 / (3n), which is applied to the sums
 // (the FP16 operands stay clear of underflow); a value beyond the FP16 range
 // (65504) is clamped there.
@@ -469,8 +471,8 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_rc_train_tc(const uint4* _
                                                           const float4* __restrict__ queries,
                                                           const float* __restrict__ targets,
                                                           const uint32_t* __restrict__ n_dev, uint32_t cap,
-                                                          RcBounds bounds, float* __restrict__ grad,
-                                                          float* __restrict__ loss_sum, uint32_t* __restrict__ err) {
+                                                          RcBounds bounds, float* __restrict__ parts,
+                                                          float* __restrict__ loss_parts, uint32_t* __restrict__ err) {
   const uint32_t n = min(*n_dev, cap);
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -619,7 +621,11 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_rc_train_tc(const uint4* _
     if (!(ok = mmas_done(bar_a, phase, tid))) break;
     first = false;
   }
-  // weight-gradient sums -> gradient: rows 0..63 (hi) plus rows 64..127 (lo)
+  // weight-gradient sums -> this CTA's gradient row: rows 0..63 (hi) plus
+  // rows 64..127 (lo); k_rc_grad_sum adds the CTAs' rows in a fixed order
+  float* row = parts + (size_t)blockIdx.x * kNumParams;
+  if (!(ok && !first))
+    for (int p = tid; p < kNumParams; p += kTrainThreads) row[p] = 0.0f;
   if (ok && !first) {
     float* lo_rows = reinterpret_cast<float*>(smem + kTrainR) + half * kHid * 16;  // 64 rows x 16 columns per half
     const int out_rows[5] = {kHid, kHid, kHid, kHid, kOut};
@@ -640,17 +646,49 @@ __global__ void __launch_bounds__(kTrainThreads, 1) k_rc_train_tc(const uint4* _
         }
         __syncthreads();
         if (mine && t < out_rows[l])
-          for (int i = 0; i < 16; ++i)
-            atomicAdd(grad + woff[l] + t * width[l] + c0 + i, (v[i] + lo_rows[t * 16 + i]) * inv_count);
+          for (int i = 0; i < 16; ++i) row[woff[l] + t * width[l] + c0 + i] = (v[i] + lo_rows[t * 16 + i]) * inv_count;
         __syncthreads();
       }
   }
+  __shared__ float s_loss[kTrainThreads / 32];
   for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
-  if ((t & 31) == 0 && loss != 0.0f) atomicAdd(loss_sum, loss);
+  if ((tid & 31) == 0) s_loss[warp] = loss;
+  __syncthreads();
+  if (tid == 0) {
+    float l = 0.0f;
+    for (int w = 0; w < kTrainThreads / 32; ++w) l += s_loss[w];
+    loss_parts[blockIdx.x] = l;
+  }
   if (!ok && tid == 0) atomicExch(err, 1u);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}
+
+// Gradient and loss of a training step: the sum of the CTAs' rows in a fixed
+// order (row r to group r % 8, each group in row order, then the groups in
+// order), so a step's gradient does not depend on which CTA finished first.
+constexpr int kSumParams = 32, kSumGroups = 8;
+__global__ void k_rc_grad_sum(const float* __restrict__ parts, int rows, float* __restrict__ grad,
+                              const float* __restrict__ loss_parts, float* __restrict__ loss) {
+  __shared__ float s[kSumGroups][kSumParams];
+  const int pl = threadIdx.x % kSumParams, g = threadIdx.x / kSumParams;
+  const int p = blockIdx.x * kSumParams + pl;
+  float acc = 0.0f;
+  if (p < kNumParams)
+    for (int r = g; r < rows; r += kSumGroups) acc += parts[(size_t)r * kNumParams + p];
+  s[g][pl] = acc;
+  __syncthreads();
+  if (g == 0 && p < kNumParams) {
+    float t = 0.0f;
+    for (int k = 0; k < kSumGroups; ++k) t += s[k][pl];
+    grad[p] = t;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    float l = 0.0f;
+    for (int r = 0; r < rows; ++r) l += loss_parts[r];
+    *loss = l;
+  }
 }
 
 // Adam on the FP32 master weights, then the packed FP16 tensor-core operands
@@ -690,6 +728,7 @@ struct Cache {
   cudaStream_t stream = nullptr;
   RcBounds bounds{};
   float *master = nullptr, *m1 = nullptr, *m2 = nullptr, *grad = nullptr, *loss = nullptr;
+  float *parts = nullptr, *loss_parts = nullptr;  // per-CTA gradient rows and losses of a training step
   uint32_t* count = nullptr;  // sample count of host-submitted batches
   __half* packed = nullptr;
   uint32_t* err = nullptr;
@@ -775,12 +814,12 @@ int rc_train_device(void* cp, const float4* queries, const float* targets, const
     if (!c->pending) c->pending = rc;
     return rc;
   }
-  cudaMemsetAsync(c->grad, 0, kNumParams * 4, st);
-  cudaMemsetAsync(c->loss, 0, 4, st);
   const int tiles = (int)((cap + kTile - 1) / kTile);
   const int grid = tiles < c->num_sms ? tiles : c->num_sms;
   k_rc_train_tc<<<grid, kTrainThreads, kSmemTrain, st>>>(reinterpret_cast<const uint4*>(c->packed), queries, targets, n_dev,
-                                                  cap, c->bounds, c->grad, c->loss, c->err);
+                                                  cap, c->bounds, c->parts, c->loss_parts, c->err);
+  k_rc_grad_sum<<<(kNumParams + kSumParams - 1) / kSumParams, kSumParams * kSumGroups, 0, st>>>(
+      c->parts, grid, c->grad, c->loss_parts, c->loss);
   if (update) {
     c->step += 1;
     const float b1 = 0.9f, b2 = 0.999f;
@@ -823,6 +862,8 @@ void* ap_rc_create(int device, const float* scene_lo, const float* scene_hi, uin
       (rc = ap::cuda_ok(c, cudaMalloc(&c->m2, ap::kNumParams * 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->grad, ap::kNumParams * 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->loss, 4), "params")) ||
+      (rc = ap::cuda_ok(c, cudaMalloc(&c->parts, (size_t)c->num_sms * ap::kNumParams * 4), "gradient rows")) ||
+      (rc = ap::cuda_ok(c, cudaMalloc(&c->loss_parts, (size_t)c->num_sms * 4), "gradient rows")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->err, 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->count, 4), "params")) ||
       (rc = ap::cuda_ok(c, cudaMalloc(&c->packed, ap::kPackAllHalves * 2), "params")) ||
@@ -857,8 +898,8 @@ void ap_rc_destroy(void* cp) {
   if (!c) return;
   ap::DeviceScope device_scope(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->loss, c->err, c->count, c->packed, c->targets,
-                  c->queries, c->out};
+  void* ptrs[] = {c->master, c->m1, c->m2, c->grad, c->loss, c->parts, c->loss_parts, c->err, c->count, c->packed,
+                  c->targets, c->queries, c->out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);

@@ -151,6 +151,7 @@ struct SpecBuffers {
   float4* bq;       // training batch queries
   float* bt;        // training batch targets (RGB)
   uint32_t* ccount; // [0] candidate records, [1] batch entries, [2] retired paths of the pass
+  uint32_t* cbcount;  // per 256 record slots: records kept for the batch, then their first batch slot
 };
 
 constexpr uint32_t kSpecRecord = 7;  // float4 per recorded vertex
@@ -184,7 +185,7 @@ size_t carve(void* base, uint32_t P, const SpectralCache* rc, SpecBuffers* b) {
   b->stats = static_cast<unsigned long long*>(take(6 * sizeof(unsigned long long)));
   b->cq = b->cT = b->rec = b->bq = nullptr;
   b->cout = b->bt = nullptr;
-  b->ccount = b->cown = nullptr;
+  b->ccount = b->cown = b->cbcount = nullptr;
   if (rc) {
     const size_t slots = ((size_t)P / rc->stride + 1) * kRcMaxBounces;
     b->cq = static_cast<float4*>(take(4 * f4));
@@ -195,6 +196,7 @@ size_t carve(void* base, uint32_t P, const SpectralCache* rc, SpecBuffers* b) {
     b->bq = static_cast<float4*>(take(sizeof(float4) * 4 * (size_t)rc->batch));
     b->bt = static_cast<float*>(take(sizeof(float) * 3 * (size_t)rc->batch));
     b->ccount = static_cast<uint32_t*>(take(3 * sizeof(uint32_t)));
+    b->cbcount = static_cast<uint32_t*>(take(sizeof(uint32_t) * ((slots + 255) / 256)));
   }
   return off;
 }
@@ -423,20 +425,33 @@ __global__ void k_scount(SpecBuffers b, SpectralCache rc, uint32_t slots, float 
 // Keeps each of this pass's records with probability batch / count; its
 // target is the RGB of the path's radiance after the vertex divided by the
 // throughput at the vertex, per wavelength (clamped at 0).
-__global__ void k_sbatch(SpecBuffers b, SpectralCache rc, uint32_t slots, float tag, uint32_t pass, uint32_t seed,
-                         uint32_t P) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= slots) return;
-  const float4* r = b.rec + (size_t)k * kSpecRecord;
-  if (r[6].x != tag) return;
+APD bool s_kept(const SpecBuffers& b, const SpectralCache& rc, uint32_t k, uint32_t slots, float tag, uint32_t pass,
+                uint32_t seed, uint32_t P) {
+  if (k >= slots || b.rec[(size_t)k * kSpecRecord + 6].x != tag) return false;
   const uint32_t cand = b.ccount[0];
   const float keep = cand <= rc.batch ? 1.0f : (float)rc.batch / (float)cand;
   const float u = (float)(spec::pcg(k * 2654435761u ^ spec::pcg(pass + seed * 7919u)) >> 8) * (1.0f / 16777216.0f);
-  if (u >= keep) return;
+  return u < keep && (k / kRcMaxBounces) * rc.stride + (pass * 7u + 3u + seed) % rc.stride < P;
+}
+
+// Records kept per block of 256 slots (count_scan turns them into the blocks'
+// first batch slots, so the batch is in record order).
+__global__ void k_skeep(SpecBuffers b, SpectralCache rc, uint32_t slots, float tag, uint32_t pass, uint32_t seed,
+                        uint32_t P) {
+  uint32_t tot;
+  block_prefix(s_kept(b, rc, blockIdx.x * blockDim.x + threadIdx.x, slots, tag, pass, seed, P), &tot);
+  if (threadIdx.x == 0) b.cbcount[blockIdx.x] = tot;
+}
+
+__global__ void k_sbatch(SpecBuffers b, SpectralCache rc, uint32_t slots, float tag, uint32_t pass, uint32_t seed,
+                         uint32_t P) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool kept = s_kept(b, rc, k, slots, tag, pass, seed, P);
+  uint32_t tot;
+  const uint32_t slot = b.cbcount[blockIdx.x] + block_prefix(kept, &tot);
+  if (!kept || slot >= rc.batch) return;
+  const float4* r = b.rec + (size_t)k * kSpecRecord;
   const uint32_t p = (k / kRcMaxBounces) * rc.stride + (pass * 7u + 3u + seed) % rc.stride;
-  if (p >= P) return;
-  const uint32_t slot = atomicAdd(&b.ccount[1], 1u);
-  if (slot >= rc.batch) return;
   const spec::S4 Lend = s4of(b.L[p]), Lv = s4of(r[5]), T = s4of(r[4]);
   spec::S4 dl;
   for (int j = 0; j < 4; ++j) dl.v[j] = T.v[j] > 0.0f ? dm::fmax(Lend.v[j] - Lv.v[j], 0.0f) / T.v[j] : 0.0f;
@@ -632,9 +647,11 @@ int launch_spectral(const DevScene& s, const SpectralView& v, const SpectralCame
         const int sb = (int)((slots + 255) / 256);
         cudaMemsetAsync(b.ccount, 0, 2 * sizeof(uint32_t), st);
         k_scount<<<sb, 256, 0, st>>>(b, *rc, slots, tag);
+        k_skeep<<<sb, 256, 0, st>>>(b, *rc, slots, tag, k, seed, P);
+        count_scan(b.cbcount, (uint32_t)sb, b.ccount + 1, rc->batch, st);
         k_sbatch<<<sb, 256, 0, st>>>(b, *rc, slots, tag, k, seed, P);
         rc_train_device(rc->cache, b.bq, b.bt, b.ccount + 1, rc->batch, rc->lr, 1, st);
-        launches += 3;
+        launches += 6;
       }
     }
     k_saccum<<<linear, kBlock, 0, st>>>(b, P, k + 1 == spp, 1.0f / (float)spp, out);

@@ -81,9 +81,9 @@ def test_ray_queries_between_cached_frames_leave_the_cache_state_intact():
         pt = PathTracer(cfg)
         pt.upload_scene(sc)
         pt.set_camera_matrices(mats)
-        # lr 0: the weights stay put (the split-K gradient sums are not
-        # bit-reproducible), while every frame-side cache buffer is still used
-        pt.attach_radiance_cache(rc, prefix_bounces=1, train_stride=4, train_batch=4096, lr=0.0)
+        # training on: the batch and the gradient sums are assembled in a fixed
+        # order, so the whole sequence is reproducible bit for bit
+        pt.attach_radiance_cache(rc, prefix_bounces=1, train_stride=4, train_batch=4096, lr=5e-3)
         frames = [pt.render((W, H))]
         if with_query:
             pt.trace_rays(o[:16], d[:16], 100.0)
@@ -96,3 +96,47 @@ def test_ray_queries_between_cached_frames_leave_the_cache_state_intact():
     a, b = run(False), run(True)
     for i, (x, y) in enumerate(zip(a, b)):
         assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), f"frame {i} differs"
+
+
+def test_online_training_is_reproducible():
+    """Two runs of the same cached frame sequence from the same initial
+    network give the same frames and the same trained weights, bit for bit:
+    the training batch takes its records in slot order (a prefix-sum
+    compaction) and each step's gradient is the CTAs' rows added in a fixed
+    order.  The spectral mode's training, over several sample passes, too."""
+    sc = scenes.cornell_box()
+    cam = scenes.cornell_camera()
+    mats, _ = scenes.camera_matrices(cam["eye"], cam["target"], cam["fov"], cam["near"], cam["far"], W, H, None)
+
+    def frames_run():
+        rc = RadianceCache([-0.05, -0.05, -0.05], [1.05, 1.05, 1.05], seed=4)
+        pt = PathTracer(dict(presets.PLAIN, max_bounces=8, sample_count=2))
+        pt.upload_scene(sc)
+        pt.set_camera_matrices(mats)
+        pt.attach_radiance_cache(rc, prefix_bounces=1, train_stride=4, train_batch=4096, lr=5e-3)
+        out = [pt.render((W, H)) for _ in range(12)]
+        params = rc.params()
+        pt.close()
+        rc.close()
+        return out, params
+
+    def spectral_run():
+        rc = RadianceCache([-0.05, -0.05, -0.05], [1.05, 1.05, 1.05], seed=5)
+        pt = PathTracer(presets.PLAIN)
+        pt.upload_scene(sc)
+        pt.set_camera_matrices(mats)
+        pt.spectral_setup(sun_scale=0.0, scene_radius=10.0)
+        pt.attach_radiance_cache(rc, prefix_bounces=1, train_stride=4, train_batch=8192, lr=5e-3)
+        img = pt.render_spectral((W, H), spp=8, max_depth=8, seed=1)
+        params = rc.params()
+        pt.close()
+        rc.close()
+        return img, params
+
+    (fa, pa), (fb, pb) = frames_run(), frames_run()
+    for i, (x, y) in enumerate(zip(fa, fb)):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), f"frame {i} differs"
+    assert np.array_equal(pa.view(np.uint32), pb.view(np.uint32)), "trained weights differ"
+    (ia, qa), (ib, qb) = spectral_run(), spectral_run()
+    assert np.array_equal(ia.view(np.uint32), ib.view(np.uint32)), "spectral image differs"
+    assert np.array_equal(qa.view(np.uint32), qb.view(np.uint32)), "spectral-trained weights differ"
