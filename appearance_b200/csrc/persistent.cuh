@@ -31,6 +31,7 @@ constexpr int kTraceMinBlocks = AP_TRACE_MIN_BLOCKS;
 
 template <bool kAny, bool kCount, class Load, class Store>
 APD void persistent_trace(const DevScene& s, uint32_t count, uint32_t* cursor, Load load, Store store) {
+  if (count == 0) return;  // an empty queue: no warp needs the cursor
   const uint32_t lane = lane_id();
   uint2 stack[kTraversalStack];
   Trav t;
@@ -76,6 +77,7 @@ APD void persistent_trace(const DevScene& s, uint32_t count, uint32_t* cursor, L
 template <bool kAny, class Load, class Store>
 APD void persistent_trace_batch(const BvhView* bvh, int nj, const uint32_t* start, uint32_t count, uint32_t* cursor,
                                 Load load, Store store) {
+  if (count == 0) return;  // an empty queue: no warp needs the cursor
   const uint32_t lane = lane_id();
   uint2 stack[kTraversalStack];
   Trav t;

@@ -189,6 +189,7 @@ APD bool trav2_step(const DevScene& s, const TwoLevel& tl, Trav2& q, uint2* stac
 template <bool kAny, bool kCount, class Load, class Store>
 APD void persistent_trace2(const DevScene& s, const TwoLevel& tl, uint32_t count, uint32_t* cursor, Load load,
                            Store store) {
+  if (count == 0) return;  // an empty queue: no warp needs the cursor
   const uint32_t lane = lane_id();
   uint2 stack[kTraversalStack];
   Trav2 t;
