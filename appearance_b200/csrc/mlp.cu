@@ -85,44 +85,55 @@ struct RcBounds {
 // elementary functions are the deterministic ones the oracle's encoding uses,
 // so the FP16 features match it bit for bit (hardware-rate functions flip
 // enough FP16 roundings to move the weight gradients by ~1e-3).
-// rc_encode_part<0> writes the position features and the material tail
-// (80 features), rc_encode_part<1> the two one-blobs (64), so that two
-// threads can share one query's encoding; rc_encode writes all of them.
+// The two threads of a query row share its encoding, balanced by their
+// elementary functions: rc_encode_part<0> writes the x and y position
+// features and the polar-angle one-blob (two sincos, one acos, 13 exps),
+// rc_encode_part<1> the z position features, the azimuth one-blob and the
+// material tail (one sincos, one atan2, 13 exps); rc_encode writes all of them.
+template <class Sink>
+APD void rc_encode_axis(const float* q, const RcBounds& b, int a, Sink& sink) {
+  const float kPi = 3.14159265358979323846f;
+  const float x = (q[a] - b.lo[a]) * b.inv[a];
+  float s, c;
+  dm::sincos_(x * kPi, &s, &c);
+#pragma unroll
+  for (int o = 0; o < 12; ++o) {
+    sink(a * 24 + 2 * o, s);
+    sink(a * 24 + 2 * o + 1, c);
+    const float s2 = 2.0f * s * c, c2 = 1.0f - 2.0f * s * s;
+    s = s2;
+    c = c2;
+  }
+}
+
+// One-blob j of the direction: 0 the polar angle / pi, 1 the azimuth / (2 pi) + 1/2.
+template <int j, class Sink>
+APD void rc_encode_blob(const float* q, Sink& sink) {
+  const float kPi = 3.14159265358979323846f;
+  const float v = j == 0 ? dm::acos_(dm::clamp(q[6], -1.0f, 1.0f)) * (1.0f / kPi)
+                         : dm::atan2_(q[5], q[4]) * (0.5f / kPi) + 0.5f;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) sink(72 + 32 * j + i, 0.0f);
+  const int b0 = min(max((int)floorf(v * 32.0f), 0), 31);
+#pragma unroll
+  for (int w = -6; w <= 6; ++w) {
+    const int i = b0 + w;
+    if (i < 0 || i > 31) continue;
+    const float ci = (v - ((float)i + 0.5f) * (1.0f / 32.0f)) * 32.0f;
+    sink(72 + 32 * j + i, dm::exp_(-0.5f * ci * ci));
+  }
+}
+
 template <int kPart, class Sink>
 APD void rc_encode_part(const float* q, const RcBounds& b, Sink sink) {
-  const float kPi = 3.14159265358979323846f;
-  if (kPart == 1) {
-    const float v[2] = {dm::acos_(dm::clamp(q[6], -1.0f, 1.0f)) * (1.0f / kPi),
-                        dm::atan2_(q[5], q[4]) * (0.5f / kPi) + 0.5f};
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-#pragma unroll
-      for (int i = 0; i < 32; ++i) sink(72 + 32 * j + i, 0.0f);
-      const int b0 = min(max((int)floorf(v[j] * 32.0f), 0), 31);
-#pragma unroll
-      for (int w = -6; w <= 6; ++w) {
-        const int i = b0 + w;
-        if (i < 0 || i > 31) continue;
-        const float ci = (v[j] - ((float)i + 0.5f) * (1.0f / 32.0f)) * 32.0f;
-        sink(72 + 32 * j + i, dm::exp_(-0.5f * ci * ci));
-      }
-    }
+  if (kPart == 0) {
+    rc_encode_axis(q, b, 0, sink);
+    rc_encode_axis(q, b, 1, sink);
+    rc_encode_blob<0>(q, sink);
     return;
   }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float x = (q[a] - b.lo[a]) * b.inv[a];
-    float s, c;
-    dm::sincos_(x * kPi, &s, &c);
-#pragma unroll
-    for (int o = 0; o < 12; ++o) {
-      sink(a * 24 + 2 * o, s);
-      sink(a * 24 + 2 * o + 1, c);
-      const float s2 = 2.0f * s * c, c2 = 1.0f - 2.0f * s * s;
-      s = s2;
-      c = c2;
-    }
-  }
+  rc_encode_axis(q, b, 2, sink);
+  rc_encode_blob<1>(q, sink);
   sink(136, q[3]);
   sink(137, q[8]);
   sink(138, q[9]);
