@@ -15,16 +15,18 @@ APD uint32_t lane_id() {
 // Persistent traversal with per-lane refill: a lane that finishes its ray
 // takes the next one through a warp-aggregated atomic on `cursor`, so warps
 // stay full until the batch drains.  Lanes check for a refill every
-// kStepBudget steps (the best of 8, 16, 32 measured on the benchmark
-// scene).  load(i, o, d, tmax) fetches ray i,
-// store(i, trav, visits) writes its result.  The traversal kernels run with
-// the child tests unrolled and are register-capped for 6 resident blocks of
-// kBlock threads per SM (the best of the measured 1..8 on the benchmark scene).
+// kStepBudget steps.  load(i, o, d, tmax) fetches ray i, store(i, trav,
+// visits) writes its result.  The traversal kernels run with the child tests
+// unrolled and are register-capped for kTraceMinBlocks resident blocks of
+// kBlock threads per SM.  Measured on the 1080p benchmark frame with the packed
+// box test (CUDA events, frame time): 5, 6, 7, 8 blocks with an 8-step refill
+// 42.9, 41.1, 39.8, 39.6 ms; 7 blocks with 6 and 10 steps 39.6, 40.2 ms; 8
+// blocks with 6 steps 39.3-39.5 ms.
 #ifndef AP_TRACE_MIN_BLOCKS
-#define AP_TRACE_MIN_BLOCKS 6
+#define AP_TRACE_MIN_BLOCKS 8
 #endif
 #ifndef AP_STEP_BUDGET
-#define AP_STEP_BUDGET 8
+#define AP_STEP_BUDGET 6
 #endif
 constexpr int kStepBudget = AP_STEP_BUDGET;
 constexpr int kTraceMinBlocks = AP_TRACE_MIN_BLOCKS;
